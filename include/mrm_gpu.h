@@ -1,0 +1,207 @@
+/*
+ * mrm_gpu.h -- C ABI of the B200 grain-dynamics path.
+ *
+ * Drop-in for the per-timestep body of mrm's llg() loop: push_m and the
+ * get_field calls it makes (src/llg.f90:212-285, :1195-1271), i.e. the
+ * stochastic LLG integrator plus the effective-field assembly
+ * (src/field.f90:160-273, :326-436), the demag FFT convolution
+ * (src/demag.f90:33-135, src/fftw.f90:37-93) and the magnetostatic tensor
+ * (src/tensor.f90:82-216, src/tensor_element.f90:13-102,219-261).
+ *
+ * Conventions follow the reference's data layout (src/data.f90:91-104):
+ *   - per-grain vectors are AoS (3,N) like the Fortran m(1+in:3+in,:),
+ *     h(3,:), uni_axis(3,:), hk(2,:) arrays, passed as contiguous doubles;
+ *   - CSR index arrays are the Fortran (0:N) arrays (N+1 cumulative counts
+ *     starting at 0); neighbour / cell coordinates are 1-based as in Fortran;
+ *   - the real-space tensor is Fortran n2d(nx,ny,9,n_lay,n_lay) (observation
+ *     layer 4th, source layer 5th), including the 1/(dx dy dz nx ny)
+ *     normalisation of tensor.f90:183;
+ *   - every function returns an int status (0 = MRM_OK), mapped to the
+ *     reference's logical ok_p by the Fortran shim; mrm_gpu_last_error()
+ *     gives the message.  Device-side failures come back as status codes,
+ *     never as traps.
+ * Ownership: the caller owns every host array; the library copies on
+ * upload/download and keeps no host pointer.  A handle is not thread-safe
+ * (neither were the FFTW plans it replaces, src/demag.f90:256).
+ */
+#ifndef MRM_GPU_H
+#define MRM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MRM_MAX_LAYERS 8
+
+enum {
+  MRM_OK = 0,
+  MRM_ERR_ARG = 1,          /* invalid argument / size */
+  MRM_ERR_CUDA = 2,         /* CUDA runtime error */
+  MRM_ERR_UNSUPPORTED = 3,  /* valid reference input this path does not cover */
+  MRM_ERR_STATE = 4,        /* call order (e.g. stepping before upload) */
+  MRM_ERR_NOMEM = 5,        /* device memory exhausted */
+  MRM_ERR_DEVICE = 6        /* kernel-reported error status */
+};
+
+enum { MRM_PERIODIC = 0, MRM_OPEN = 1 };
+enum { MRM_FP32 = 0, MRM_FP64 = 1 };
+
+/* Geometry of one medium (src/data.f90:87-89 + the demag namelist,
+ * src/input.f90:221-246).  boundary MRM_PERIODIC reproduces the reference's
+ * periodic tensor with num_images image pairs (tensor.f90:6,96-97);
+ * MRM_OPEN zero-pads the FFT grid to the next power of two >= 2n in each
+ * direction and builds the tensor on it without images. */
+typedef struct mrm_geom {
+  int32_t nx, ny, n_lay;
+  int32_t boundary;
+  int32_t num_images;
+  int32_t precision; /* MRM_FP32: FP32 state/field/FFT, FP64 tensor + reductions;
+                        MRM_FP64: everything FP64 */
+  double dx, dy;     /* cm */
+  double dz[MRM_MAX_LAYERS];
+  double il_space[MRM_MAX_LAYERS];
+  double space_to_sul, sul_mu, head_mu, fly_height; /* tensor.f90:9 image settings */
+} mrm_geom;
+
+/* Per-call results, FP64 (llg.f90:217-237 reductions, push_llg errmx/errmx1/mmag,
+ * plot.f90:192-273 M(H) row).  Values describe the state after the last step:
+ * mave/mvar/have are the volume-weighted <m>, var(m), <h> the reference's loop
+ * computes at the top of its next iteration; mms_l is plot_mh's Ms*V-weighted
+ * m; nup_l counts grains with m.h_dir > 0 (N+). */
+typedef struct mrm_gpu_stats {
+  double t;
+  int64_t step;
+  double mave[3], mvar[3], have[3];
+  double errmx;  /* sqrt(max |m x H|^2/Ms^2) of the last stage */
+  double errmx1; /* max |dm|^2 of the last stage */
+  double mmag;   /* sum over layers of sum |m| ms_scale V / sum V */
+  double energy; /* sum V * energy density of the last field evaluation (erg) */
+  double mave_l[MRM_MAX_LAYERS][3], mvar_l[MRM_MAX_LAYERS][3];
+  double have_l[MRM_MAX_LAYERS][3], mms_l[MRM_MAX_LAYERS][3];
+  double vol_l[MRM_MAX_LAYERS], msvol_l[MRM_MAX_LAYERS];
+  int64_t nup_l[MRM_MAX_LAYERS];
+} mrm_gpu_stats;
+
+typedef struct mrm_gpu mrm_gpu;     /* one medium realisation (a "run") */
+typedef struct mrm_batch mrm_batch; /* many runs advanced by one launch sequence */
+
+/* ---------------- plain single-run path (the drop-in) ---------------- */
+
+/* Allocates a run on `device` (replaces start_demag/init_demag set-up,
+ * src/demag.f90:184-286, and the data_m allocations). */
+int mrm_gpu_create(const mrm_geom* geom, int device, mrm_gpu** out);
+int mrm_gpu_destroy(mrm_gpu* h);
+const char* mrm_gpu_last_error(const mrm_gpu* h);
+
+/* Static grain data of one layer (0-based `layer`; Fortran layer k -> k-1).
+ * Arrays as data_s/field_ss: ms(N), grain_vol(N), uni_axis(3,N), hk(2,N),
+ * hk_scale/ms_scale/alpha_scale(N); alpha, gamma, floor_ms scalars;
+ * grain2gridindex(0:N), grain2grid(2,ncell) (field.f90:22-23); intralayer
+ * exchange hxgrainindex(0:N), hxgrain(nnz), hx(nnz) (field.f90:28-29), or
+ * NULL for none.  This path requires one cell per grain on the nx*ny grid
+ * (grains are nodes, construct_grain.f90:160-189) and returns
+ * MRM_ERR_UNSUPPORTED for multi-cell grains. */
+int mrm_gpu_upload_layer(mrm_gpu* h, int layer, int n_grains, const double* ms,
+                         const double* grain_vol, const double* uni_axis, const double* hk,
+                         const double* hk_scale, const double* ms_scale,
+                         const double* alpha_scale, double alpha, double gamma, double floor_ms,
+                         const int32_t* grain2gridindex, const int32_t* grain2grid,
+                         const int32_t* hxgrainindex, const int32_t* hxgrain, const double* hx);
+
+/* Interlayer exchange CSR of `layer`: side 0 = uhx (couples to layer-1),
+ * side 1 = lhx (couples to layer+1) (field.f90:211-220, :326-348). */
+int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* index,
+                              const int32_t* grain, const double* coef);
+
+/* Builds the FP64 tensor on the device (calculate_tensor + the once-per-run
+ * FFT of demag.f90:259-267, in FP64) and keeps its spectrum resident. */
+int mrm_gpu_build_tensor(mrm_gpu* h);
+/* Uses a tensor computed by the host (calculate_tensor's n2d or mrm_N.dat)
+ * for an FFT grid of nx_fft x ny_fft (must equal the handle's FFT grid). */
+int mrm_gpu_upload_tensor(mrm_gpu* h, const double* n2d, int nx_fft, int ny_fft);
+/* Copies the device-built real-space tensor back (for the tensor cache file). */
+int mrm_gpu_download_tensor(mrm_gpu* h, double* n2d);
+/* FFT grid of the handle (nx_fft, ny_fft). */
+int mrm_gpu_fft_grid(const mrm_gpu* h, int* nx_fft, int* ny_fft);
+/* Diagnostic of the packed tensor spectrum: largest dropped (wrong-parity)
+ * part and largest kept value, FP64. */
+int mrm_gpu_tensor_residual(const mrm_gpu* h, double* resid, double* kept);
+/* demag_p of the demag namelist (src/input.f90:228); default on. */
+int mrm_gpu_set_demag(mrm_gpu* h, int on);
+
+/* Uniform applied field of `layer` with a linear time ramp:
+ * h_app(t) = ((s_end-s_start)*clamp((t-t_start)/(t_end-t_start),0,1)+s_start)*scale*hdir
+ * (set_fld / get_appl, src/applied.f90:263-317,871-883). */
+int mrm_gpu_set_uniform_field(mrm_gpu* h, int layer, const double hdir[3], double t_start,
+                              double t_end, double s_start, double s_end, double scale);
+
+/* Thermal (Brown) field of `layer` at `temperature` K (get_thermal,
+ * field.f90:397-436).  The normals come from a counter-based Philox4x64-10
+ * stream keyed by `seed` (statistical, not bitwise, equivalence with the
+ * reference's MT19937 stream, random.f90:231-249). */
+int mrm_gpu_set_thermal(mrm_gpu* h, int layer, int on, double temperature, uint64_t seed);
+
+/* m(3,N) of `layer` (the active half m(1+in:3+in,:)) */
+int mrm_gpu_set_state(mrm_gpu* h, int layer, const double* m);
+int mrm_gpu_get_state(mrm_gpu* h, int layer, double* m);
+/* h(3,N): the last non-thermal total field (field.f90:201) */
+int mrm_gpu_get_field(mrm_gpu* h, int layer, double* hfield);
+/* time and step counter (the Philox counter) of the handle */
+int mrm_gpu_set_time(mrm_gpu* h, double t, int64_t step);
+int mrm_gpu_get_time(const mrm_gpu* h, double* t, int64_t* step);
+
+/* Evaluates get_field(t) (no thermal) on the current state; h_demag(3,N) of
+ * `layer` is returned if hdemag != NULL, the total field via get_field. */
+int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag);
+
+/* Advances nsteps fixed-dt steps of llg_type (-3 Heun; src/llg.f90:1122-1139,
+ * :1195-1271).  Replaces nsteps iterations of the llg() loop body for a
+ * fixed-step run (fixed_dt_p, conv_torque = conv_angle = 0).  `out` (may be
+ * NULL) receives the reductions of the last step. */
+int mrm_gpu_step(mrm_gpu* h, int nsteps, double dt, int llg_type, mrm_gpu_stats* out);
+
+/* Enqueues nsteps like mrm_gpu_step without waiting for them; the stats of
+ * the last enqueued step are read later with mrm_gpu_read_stats (which waits). */
+int mrm_gpu_enqueue_steps(mrm_gpu* h, int nsteps, double dt, int llg_type);
+int mrm_gpu_read_stats(mrm_gpu* h, mrm_gpu_stats* out);
+/* The cudaStream_t (as void*) the handle launches on, for event timing. */
+int mrm_gpu_stream(const mrm_gpu* h, void** stream);
+/* Advances `reps` Heun steps launching each kernel bracketed by CUDA events
+ * on the handle's stream; ms_out[4] = mean ms of row(predictor), column,
+ * row(corrector), column launches (the demag column launches are 0 when
+ * demag is off). */
+int mrm_gpu_profile(mrm_gpu* h, int reps, double dt, double* ms_out);
+
+/* ---------------- batched / served form ---------------- */
+
+/* A batch owns a device stream and advances all its active runs with one
+ * launch sequence per Heun stage (one task table over every run's rows and
+ * spectral columns), captured in CUDA graphs. */
+int mrm_batch_create(int precision, int device, mrm_batch** out);
+int mrm_batch_destroy(mrm_batch* b);
+const char* mrm_batch_last_error(const mrm_batch* b);
+/* Creates a run inside the batch (same precision/device); configure it with
+ * the mrm_gpu_* upload/set functions; it is freed by mrm_batch_remove. */
+int mrm_batch_add(mrm_batch* b, const mrm_geom* geom, mrm_gpu** run);
+int mrm_batch_remove(mrm_batch* b, mrm_gpu* run);
+/* per-run time step and step budget: the run advances while step < step_end */
+int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active);
+/* Advances every active run by up to nsteps Heun steps (llg_type -3). */
+int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type);
+/* Stats of each listed run after its last step in the preceding mrm_batch_step. */
+int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats* out);
+/* Enqueues like mrm_batch_step without waiting (stats via mrm_batch_stats). */
+int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type);
+int mrm_batch_stream(const mrm_batch* b, void** stream);
+/* Device bytes a run of this geometry holds (admission by HBM footprint). */
+int64_t mrm_run_footprint(const mrm_geom* geom);
+/* Free / total device memory in bytes. */
+int mrm_device_memory(int device, int64_t* free_bytes, int64_t* total_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MRM_GPU_H */

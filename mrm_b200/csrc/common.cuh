@@ -1,0 +1,99 @@
+// common.cuh -- device types shared by the grain-dynamics kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MRM_HD __host__ __device__ __forceinline__
+#define MRM_D __device__ __forceinline__
+
+namespace mrm {
+
+constexpr int kMaxLayers = 8;
+constexpr int kTwLog = 12;                 // twiddle table covers FFT lengths <= 4096
+constexpr int kTwN = 1 << kTwLog;
+constexpr int kNPart = 20;                 // doubles per row-task stats record
+
+template <typename R>
+struct alignas(2 * sizeof(R)) Cx {
+  R x, y;
+};
+
+template <typename R>
+struct alignas(4 * sizeof(R)) V4 {
+  R x, y, z, w;
+};
+
+template <typename R>
+MRM_HD Cx<R> cmul(Cx<R> a, Cx<R> b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename R>
+MRM_HD Cx<R> cadd(Cx<R> a, Cx<R> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename R>
+MRM_HD Cx<R> csub(Cx<R> a, Cx<R> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename R>
+MRM_HD Cx<R> cconj(Cx<R> a) { return {a.x, -a.y}; }
+template <typename R>
+MRM_HD Cx<R> cscale(Cx<R> a, R s) { return {a.x * s, a.y * s}; }
+// multiply by i*s (s = +1 or -1)
+template <typename R>
+MRM_HD Cx<R> cmul_i(Cx<R> a, R s) { return {-s * a.y, s * a.x}; }
+
+// Per-layer device view of one run.  State vectors are float4/double4
+// "SoA of 4-vectors": (x,y,z,unused) per grain for one 16/32-byte load.
+template <typename R>
+struct LayerDev {
+  V4<R>* m;         // m_n (state at step boundaries)
+  V4<R>* mp;        // Heun predictor m*
+  V4<R>* dm;        // predictor increment d1
+  V4<R>* hf;        // last non-thermal total field (get_field output)
+  V4<R>* hd;        // demag field of the last evaluation-only pass
+  const V4<R>* pa;  // {kx, ky, kz, Hk1*hk_scale}
+  const V4<R>* pb;  // {Ms*ms_scale, Hk2*hk_scale, alpha*alpha_scale, sigma0}
+  const V4<double>* pv;  // {vol, ms_scale, ms, 0} (FP64, reductions)
+  const int* xidx;  // intralayer exchange CSR (0-based), coef includes ms_scale(nbr)
+  const int* xnbr;
+  const R* xcoef;
+  const int* uidx;  // interlayer: couples to layer-1
+  const int* unbr;
+  const R* ucoef;
+  const int* lidx;  // interlayer: couples to layer+1
+  const int* lnbr;
+  const R* lcoef;
+  double hdir[3];
+  double t_start, t_end, s_start, s_end, scale;
+  double temperature;
+  double gamma;
+  int thermal;
+  int n;
+};
+
+// Device descriptor of one run (one medium realisation).
+template <typename R>
+struct RunDev {
+  int nx, ny, nl;
+  int px, py, lgpx, lgpy;  // FFT grid (px = 2^lgpx)
+  int demag;
+  int ncomp;               // tensor components stored per pair (9)
+  double dt;
+  double t_base;           // time at step index step_base
+  long long step_base;
+  long long step;          // current step index (advanced by the advance kernel)
+  long long step_end;      // the run advances while step < step_end
+  unsigned long long seed;
+  int active;
+  int row_task0, nrow_tasks;  // range of this run's row tasks (stats partials)
+  Cx<R>* spec;             // [nl][3][ny][px/2+1] half spectra of M (forward) / H (inverse)
+  const R* tens;           // [px/2+1][nl*nl][ncomp][py/2+1] tensor spectrum (real or imag part)
+  LayerDev<R> L[kMaxLayers];
+};
+
+// Tensor component parity (c = 3*field + source): the spectrum is purely
+// imaginary for xz, yz, zx, zy and odd in ky for xy, yx, yz, zy.
+constexpr int kImagMask = (1 << 2) | (1 << 5) | (1 << 6) | (1 << 7);
+constexpr int kOddMask = (1 << 1) | (1 << 3) | (1 << 5) | (1 << 7);
+
+// row task: (run, layer, first row, number of rows); column task: (run, first column, ncols, 0)
+using Task = int4;
+
+}  // namespace mrm

@@ -1,0 +1,472 @@
+// kernels.cuh -- fused per-step kernels of the grain-dynamics path (sm_100a).
+//
+// One Heun step (src/llg.f90:1195-1271, llg_type = -3) is four launches:
+//   row<PRED>  : inverse row FFT of H^(m_n) -> H_demag, field assembly
+//                (field.f90:197-225), Philox thermal field (field.f90:397-436),
+//                Heun predictor (llg.f90:1122-1139, iter = 2), forward row FFT
+//                of Ms*m* (data.f90:322-390 scatter + demag.f90:113-116)
+//   col        : column FFT, tensor multiply (demag.f90:117-121), inverse
+//                column FFT, all in shared memory
+//   row<CORR>  : same with the corrector (iter = 1) at t+dt on m*, thermal
+//                regenerated from the same counter; optional FP64 reductions
+//                (llg.f90:217-237, push_llg errmx/errmx1/mmag)
+//   col
+// The spectrum buffer always holds H^(m) of the state it follows, so a step
+// starts from it without a separate demag pass.
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+#include "philox.cuh"
+
+namespace mrm {
+
+enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
+enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4 };
+
+template <typename R>
+MRM_D void cross3(R ax, R ay, R az, R bx, R by, R bz, R& cx, R& cy, R& cz) {
+  cx = ay * bz - az * by;
+  cy = az * bx - ax * bz;
+  cz = ax * by - ay * bx;
+}
+
+template <typename R>
+MRM_D double ramp(const LayerDev<R>& L, double t) {
+  // applied.f90:871-872 (linear ramp of the time scale) with set_fld's folded scale
+  double u = (t - L.t_start) / (L.t_end - L.t_start);
+  u = fmax(0.0, fmin(1.0, u));
+  return ((L.s_end - L.s_start) * u + L.s_start) * L.scale;
+}
+
+// CSR neighbour sum  sum_j c_j m_j  (field.f90:350-363 / :326-348)
+template <typename R>
+MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
+                   const R* __restrict__ cf, const V4<R>* __restrict__ mb, int n, R& hx, R& hy,
+                   R& hz) {
+  const int q0 = __ldg(idx + n), q1 = __ldg(idx + n + 1);
+  for (int q = q0; q < q1; ++q) {
+    const int j = __ldg(nbr + q);
+    const R c = __ldg(cf + q);
+    const V4<R> mj = mb[j];
+    hx += c * mj.x;
+    hy += c * mj.y;
+    hz += c * mj.z;
+  }
+}
+
+// block reduction of the stats record (sums except [kMaxTq], [kMaxD2] which are maxima)
+constexpr int kSlotV = 0, kSlotM = 1, kSlotM2 = 4, kSlotH = 7, kSlotWM = 10, kSlotW = 13,
+              kSlotNup = 14, kSlotMaxTq = 15, kSlotMaxD2 = 16, kSlotMmag = 17, kSlotE = 18;
+
+MRM_D void block_reduce_record(double* rec, double* sred /* [32][kNPart] */, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int s = 0; s < kNPart; ++s) {
+    double v = rec[s];
+    const bool mx = (s == kSlotMaxTq || s == kSlotMaxD2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = mx ? fmax(v, w) : v + w;
+    }
+    if (lane == 0) sred[warp * kNPart + s] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNPart) {
+    const int s = threadIdx.x;
+    const bool mx = (s == kSlotMaxTq || s == kSlotMaxD2);
+    double v = sred[s];
+    for (int w = 1; w < nw; ++w) v = mx ? fmax(v, sred[w * kNPart + s]) : v + sred[w * kNPart + s];
+    out[s] = v;
+  }
+}
+
+template <int STAGE, bool STATS>
+__host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STATS) ? 32 * kNPart : 1; }
+
+template <typename R, int STAGE, bool STATS>
+__global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ runs,
+                                                  const Task* __restrict__ tasks,
+                                                  const Cx<R>* __restrict__ tw, int istep,
+                                                  int flags, double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Task tk = tasks[blockIdx.x];
+  const RunDev<R>& rd = runs[tk.x];
+  if (!rd.active) return;
+  const long long step = rd.step + istep;
+  if (!(flags & kFlagForce) && step >= rd.step_end) return;
+
+  const int l = tk.y, row0 = tk.z, nrows = tk.w;
+  const int nx = rd.nx, ny = rd.ny;
+  const int lgM = rd.lgpx - 1, M = 1 << lgM, ph = M + 1;
+  const int nseq = nrows * 3;
+  const LayerDev<R>& L = rd.L[l];
+  const bool demag = rd.demag != 0;
+
+  Cx<R>* bufA = reinterpret_cast<Cx<R>*>(smem_raw);
+  Cx<R>* bufB = bufA + nseq * M;
+  __shared__ double sred[stats_slots<STAGE, STATS>()];
+
+  // ---------------- inverse row transform: H^ rows -> H_demag ----------------
+  Cx<R>* Z = bufA;  // holds x[2n] + i x[2n+1] of each sequence after the inverse
+  if (STAGE != kInit && demag) {
+    for (int idx = threadIdx.x; idx < nseq * M; idx += blockDim.x) {
+      const int s = idx >> lgM, k = idx & (M - 1);
+      const int row = s / 3, comp = s - 3 * row;
+      const Cx<R>* X = rd.spec + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
+      Cx<R> xk = X[k], xmk = X[M - k];
+      if (k == 0) { xk.y = 0; xmk.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
+      const Cx<R> e = cadd(xk, cconj(xmk));
+      const Cx<R> o = csub(xk, cconj(xmk));
+      const Cx<R> w = cconj(twiddle(tw, k, rd.lgpx));  // e^{+2 pi i k / px}
+      bufA[s * M + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
+    }
+    __syncthreads();
+    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, M, tw);
+  }
+  Cx<R>* W = (Z == bufA) ? bufB : bufA;  // real outputs of this stage (forward input)
+  const R* hdr = reinterpret_cast<const R*>(Z);
+  R* outr = reinterpret_cast<R*>(W);
+
+  // ---------------- per-grain field + integrator stage ----------------
+  const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
+  const double t_stage = (STAGE == kCorr) ? t_now + rd.dt : t_now;
+  const double sc = ramp(L, t_stage);
+  const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
+  const R dt = (R)rd.dt;
+  const R gamma = (R)L.gamma;
+  const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
+  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
+  constexpr bool stats = (STAGE == kCorr) && STATS;
+  const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
+
+  double rec[stats ? kNPart : 1];
+#pragma unroll
+  for (int s = 0; s < (stats ? kNPart : 1); ++s) rec[s] = 0.0;
+
+  const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;  // state the field is evaluated on
+  const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
+  const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
+
+  const int two_m = 2 * M;
+  for (int idx = threadIdx.x; idx < nrows * nx; idx += blockDim.x) {
+    const int row = idx / nx, i = idx - row * nx;
+    const int n = (row0 + row) * nx + i;
+    const V4<R> pb = L.pb[n];
+    const R mse = pb.x;  // Ms * ms_scale
+    if (STAGE == kInit) {
+      const V4<R> m = L.m[n];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) outr[(row * 3 + c) * two_m + i] = mse * (c == 0 ? m.x : c == 1 ? m.y : m.z);
+      continue;
+    }
+    const V4<R> mf = mfield[n];
+    R hdx = 0, hdy = 0, hdz = 0;
+    if (demag) {
+      hdx = hdr[(row * 3 + 0) * two_m + i];
+      hdy = hdr[(row * 3 + 1) * two_m + i];
+      hdz = hdr[(row * 3 + 2) * two_m + i];
+    }
+    // h = h_app + h_demag + H_uni + H_ex (+ interlayer)   (field.f90:201,211-220)
+    R hx = hax + hdx, hy = hay + hdy, hz = haz + hdz;
+    const V4<R> pa = L.pa[n];
+    R e_k = 0;
+    {
+      // get_uni_hk (field.f90:366-375); pa.w = Hk1*hk_scale, pb.y = Hk2*hk_scale
+      const R hks = mf.x * pa.x + mf.y * pa.y + mf.z * pa.z;
+      const R yy = (R)1 - hks * hks;
+      const R f = hks * (pa.w + pb.y * yy);
+      hx += f * pa.x;
+      hy += f * pa.y;
+      hz += f * pa.z;
+      e_k = (R)0.5 * yy * (pa.w + (R)0.5 * pb.y * yy) * mse;
+    }
+    R ex = 0, ey = 0, ez = 0;
+    if (L.xidx) csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
+    R vx = 0, vy = 0, vz = 0;
+    if (L.uidx && Lu) csr_sum<R>(L.uidx, L.unbr, L.ucoef, (STAGE == kCorr) ? Lu->mp : Lu->m, n, vx, vy, vz);
+    if (L.lidx && Ll) csr_sum<R>(L.lidx, L.lnbr, L.lcoef, (STAGE == kCorr) ? Ll->mp : Ll->m, n, vx, vy, vz);
+    hx += ex + vx;
+    hy += ey + vy;
+    hz += ez + vz;
+    if (store_field) {
+      L.hf[n] = V4<R>{hx, hy, hz, (R)0};
+    }
+    if (STAGE == kEval) {
+      L.hd[n] = V4<R>{hdx, hdy, hdz, (R)0};
+      continue;
+    }
+
+    // thermal field / sqrt(dt) (llg.f90:1083), Philox normals regenerated in the corrector
+    R htx = 0, hty = 0, htz = 0;
+    if (thermal) {
+      R g[3];
+      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step,
+                      (unsigned long long)n, g);
+      const R s = pb.w * tfac;
+      htx = s * g[0];
+      hty = s * g[1];
+      htz = s * g[2];
+    }
+    const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
+    V4<R> mn;
+    R dx = 0, dy = 0, dz = 0, tq2 = 0;
+    if (mse > (R)0) {
+      const R a = pb.z;  // alpha * alpha_scale
+      const R s11 = -gamma * dt / ((R)1 + a * a);
+      R tx, ty, tz, ux, uy, uz;
+      cross3(mf.x, mf.y, mf.z, fx, fy, fz, tx, ty, tz);
+      cross3(mf.x, mf.y, mf.z, tx, ty, tz, ux, uy, uz);
+      dx = s11 * (tx + a * ux);
+      dy = s11 * (ty + a * uy);
+      dz = s11 * (tz + a * uz);
+      tq2 = tx * tx + ty * ty + tz * tz;
+      V4<R> m0;
+      if (STAGE == kPred) {
+        L.dm[n] = V4<R>{dx, dy, dz, (R)0};
+        m0 = mf;
+      } else {
+        const V4<R> d1 = L.dm[n];
+        dx = (R)0.5 * (dx + d1.x);
+        dy = (R)0.5 * (dy + d1.y);
+        dz = (R)0.5 * (dz + d1.z);
+        m0 = L.m[n];
+      }
+      mn.x = m0.x + dx;
+      mn.y = m0.y + dy;
+      mn.z = m0.z + dz;
+      const R y = mn.x * mn.x + mn.y * mn.y + mn.z * mn.z;
+      if (y > (R)0) {
+        const R r = (R)1 / sqrt(y);
+        mn.x *= r;
+        mn.y *= r;
+        mn.z *= r;
+      }
+    } else {
+      // ms_scale <= 0: m along the (non-thermal) field (llg.f90:1140-1148)
+      const R y = sqrt(hx * hx + hy * hy + hz * hz);
+      if (y > (R)0) {
+        mn.x = hx / y; mn.y = hy / y; mn.z = hz / y;
+      } else {
+        mn = (STAGE == kCorr) ? L.m[n] : mf;
+      }
+    }
+    mn.w = (R)0;
+    if (STAGE == kPred) L.mp[n] = mn;
+    else L.m[n] = mn;
+    outr[(row * 3 + 0) * two_m + i] = mse * mn.x;
+    outr[(row * 3 + 1) * two_m + i] = mse * mn.y;
+    outr[(row * 3 + 2) * two_m + i] = mse * mn.z;
+
+    if constexpr (stats) {
+      const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 0}
+      const double v = pv.x, w = pv.z * pv.y * v;
+      const double mx = mn.x, my = mn.y, mz = mn.z;
+      rec[kSlotV] += v;
+      rec[kSlotM + 0] += v * mx;
+      rec[kSlotM + 1] += v * my;
+      rec[kSlotM + 2] += v * mz;
+      rec[kSlotM2 + 0] += v * mx * mx;
+      rec[kSlotM2 + 1] += v * my * my;
+      rec[kSlotM2 + 2] += v * mz * mz;
+      rec[kSlotH + 0] += v * (double)hx;
+      rec[kSlotH + 1] += v * (double)hy;
+      rec[kSlotH + 2] += v * (double)hz;
+      rec[kSlotWM + 0] += w * mx;
+      rec[kSlotWM + 1] += w * my;
+      rec[kSlotWM + 2] += w * mz;
+      rec[kSlotW] += w;
+      if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += 1.0;
+      const double ms2 = pv.z * pv.z;
+      rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / ms2);
+      rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
+      rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+      // energy at the evaluated state (field.f90:200, :360, :374, :339)
+      const double e_d = -((double)mf.x * ((double)hdx + hax) + (double)mf.y * ((double)hdy + hay) +
+                           (double)mf.z * ((double)hdz + haz)) * (double)mse;
+      const double e_x = -((double)(ex + vx) * mf.x + (double)(ey + vy) * mf.y +
+                           (double)(ez + vz) * mf.z) * (double)mse;
+      rec[kSlotE] += (e_d + (double)e_k + e_x) * v;
+    }
+  }
+  if constexpr (stats) {
+    block_reduce_record(rec, sred, part + (size_t)blockIdx.x * kNPart);
+  }
+  if (STAGE == kEval || !demag) return;
+
+  // ---------------- forward row transform of Ms*m -> spectrum rows ----------------
+  if (nx < two_m) {
+    const int pad = two_m - nx;
+    for (int idx = threadIdx.x; idx < nseq * pad; idx += blockDim.x) {
+      const int s = idx / pad, i = nx + (idx - s * pad);
+      outr[s * two_m + i] = (R)0;
+    }
+  }
+  __syncthreads();
+  Cx<R>* scratch = (W == bufA) ? bufB : bufA;
+  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, M, tw);
+  for (int idx = threadIdx.x; idx < nseq * ph; idx += blockDim.x) {
+    const int s = idx / ph, k = idx - s * ph;
+    const int row = s / 3, comp = s - 3 * row;
+    const Cx<R> yk = Y[s * M + (k & (M - 1))];
+    const Cx<R> ymk = cconj(Y[s * M + ((M - k) & (M - 1))]);
+    const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
+    const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
+    // X[k] = e - i w^k o,  w = e^{-2 pi i / px}
+    const Cx<R> wo = cmul(twiddle(tw, k & (two_m - 1), rd.lgpx), o);
+    const Cx<R> xk = csub(e, cmul_i(wo, (R)1));
+    rd.spec[((size_t)(l * 3 + comp) * ny + row0 + row) * ph + k] = xk;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) col_kernel(const RunDev<R>* __restrict__ runs,
+                                                  const Task* __restrict__ tasks,
+                                                  const Cx<R>* __restrict__ tw, int istep,
+                                                  int flags) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Task tk = tasks[blockIdx.x];
+  const RunDev<R>& rd = runs[tk.x];
+  if (!rd.active || !rd.demag) return;
+  if (!(flags & kFlagForce) && rd.step + istep >= rd.step_end) return;
+  const int k0 = tk.y, nc = tk.z;
+  const int nl = rd.nl, ny = rd.ny, py = rd.py, lgpy = rd.lgpy;
+  const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1;
+  const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
+  Cx<R>* A = reinterpret_cast<Cx<R>*>(smem_raw);
+  Cx<R>* B = A + nseq * py;
+
+  // load columns (rows >= ny are the zero padding)
+  for (int idx = threadIdx.x; idx < nseq * py; idx += blockDim.x) {
+    const int c = idx % nc;
+    const int rest = idx / nc;
+    const int j = rest % py;
+    const int lc = rest / py;  // layer*3 + comp
+    Cx<R> v = {(R)0, (R)0};
+    if (j < ny) v = rd.spec[((size_t)lc * ny + j) * ph + k0 + c];
+    A[(c * nl * 3 + lc) * py + j] = v;
+  }
+  __syncthreads();
+  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, py, tw);
+  Cx<R>* G = (F == A) ? B : A;
+
+  // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
+  const int npair = nl * nl;
+  for (int idx = threadIdx.x; idx < nc * py; idx += blockDim.x) {
+    const int c = idx / py, ky = idx - c * py;
+    const bool upper = ky > (py >> 1);
+    const int kyh = upper ? py - ky : ky;
+    const R* T = rd.tens + (size_t)(k0 + c) * npair * rd.ncomp * pyh;
+    for (int ko = 0; ko < nl; ++ko) {
+      Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
+      for (int ks = 0; ks < nl; ++ks) {
+        const R* Tp = T + (size_t)(ks * nl + ko) * rd.ncomp * pyh;
+        Cx<R> xm[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) xm[b] = F[((c * nl + ks) * 3 + b) * py + ky];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const int cc = 3 * a + b;
+            R v = __ldg(Tp + cc * pyh + kyh);
+            if (((kOddMask >> cc) & 1) && upper) v = -v;
+            if ((kImagMask >> cc) & 1) h[a] = cadd(h[a], cmul_i(cscale(xm[b], v), (R)1));
+            else h[a] = cadd(h[a], cscale(xm[b], v));
+          }
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) G[((c * nl + ko) * 3 + a) * py + ky] = h[a];
+    }
+  }
+  __syncthreads();
+  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, py, tw);
+
+  for (int idx = threadIdx.x; idx < nseq * ny; idx += blockDim.x) {
+    const int c = idx % nc;
+    const int rest = idx / nc;
+    const int j = rest % ny;
+    const int lc = rest / ny;
+    rd.spec[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * py + j];
+  }
+}
+
+// Advances every active run's step counter after a captured chunk of k steps.
+template <typename R>
+__global__ void advance_kernel(RunDev<R>* runs, int nruns, int k) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  RunDev<R>& rd = runs[r];
+  if (!rd.active) return;
+  long long left = rd.step_end - rd.step;
+  if (left < 0) left = 0;
+  rd.step += (left < k) ? left : k;
+}
+
+// FP64 reduction of the per-task stats records of each run into mrm_gpu_stats
+// (layout mirrored by StatsDev), in a fixed order (deterministic).
+struct StatsDev {
+  double t;
+  long long step;
+  double mave[3], mvar[3], have[3];
+  double errmx, errmx1, mmag, energy;
+  double mave_l[kMaxLayers][3], mvar_l[kMaxLayers][3], have_l[kMaxLayers][3], mms_l[kMaxLayers][3];
+  double vol_l[kMaxLayers], msvol_l[kMaxLayers];
+  long long nup_l[kMaxLayers];
+};
+
+template <typename R>
+__global__ void finalize_stats_kernel(const RunDev<R>* __restrict__ runs, const Task* __restrict__ tasks,
+                                      const double* __restrict__ part, StatsDev* __restrict__ out,
+                                      int nruns) {
+  const int r = blockIdx.x;
+  if (r >= nruns || threadIdx.x != 0) return;
+  const RunDev<R>& rd = runs[r];
+  StatsDev& st = out[r];
+  if (!rd.active) return;
+  double acc[kMaxLayers][kNPart];
+  for (int l = 0; l < kMaxLayers; ++l)
+    for (int s = 0; s < kNPart; ++s) acc[l][s] = 0.0;
+  for (int q = rd.row_task0; q < rd.row_task0 + rd.nrow_tasks; ++q) {
+    const int l = tasks[q].y;
+    const double* p = part + (size_t)q * kNPart;
+    for (int s = 0; s < kNPart; ++s)
+      acc[l][s] = (s == kSlotMaxTq || s == kSlotMaxD2) ? fmax(acc[l][s], p[s]) : acc[l][s] + p[s];
+  }
+  st.step = rd.step;
+  st.t = rd.t_base + (double)(rd.step - rd.step_base) * rd.dt;
+  double vt = 0, mt = 0, m1 = 0, mmag = 0, en = 0;
+  for (int a = 0; a < 3; ++a) { st.mave[a] = 0; st.mvar[a] = 0; st.have[a] = 0; }
+  for (int l = 0; l < rd.nl; ++l) vt += acc[l][kSlotV];
+  for (int l = 0; l < kMaxLayers; ++l) {
+    const double V = acc[l][kSlotV];
+    for (int a = 0; a < 3; ++a) {
+      const double mean = (l < rd.nl && V > 0) ? acc[l][kSlotM + a] / V : 0.0;
+      st.mave_l[l][a] = mean;
+      st.mvar_l[l][a] = (l < rd.nl && V > 0) ? acc[l][kSlotM2 + a] / V - mean * mean : 0.0;
+      st.have_l[l][a] = (l < rd.nl && V > 0) ? acc[l][kSlotH + a] / V : 0.0;
+      const double W = acc[l][kSlotW];
+      st.mms_l[l][a] = acc[l][kSlotWM + a] * W / (W * W + 1e-300);
+    }
+    st.vol_l[l] = V;
+    st.msvol_l[l] = acc[l][kSlotW];
+    st.nup_l[l] = (long long)acc[l][kSlotNup];
+    if (l < rd.nl && V > 0) {
+      for (int a = 0; a < 3; ++a) {
+        st.mave[a] += V * st.mave_l[l][a] / vt;
+        st.mvar[a] += V * st.mvar_l[l][a] / vt;
+        st.have[a] += V * st.have_l[l][a] / vt;
+      }
+      mmag += acc[l][kSlotMmag] / V;
+    }
+    mt = fmax(mt, acc[l][kSlotMaxTq]);
+    m1 = fmax(m1, acc[l][kSlotMaxD2]);
+    en += acc[l][kSlotE];
+  }
+  st.errmx = sqrt(mt);
+  st.errmx1 = m1;
+  st.mmag = mmag;
+  st.energy = en;
+}
+
+}  // namespace mrm

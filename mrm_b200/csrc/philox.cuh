@@ -1,0 +1,68 @@
+// philox.cuh -- counter-based thermal-noise stream.
+//
+// Philox4x64-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11) with the Box-Muller transform.  Counter =
+// (grain, step, layer, 0), key = (seed, 0x6d726d): the predictor and the
+// corrector of one Heun step regenerate the same three normals instead of
+// storing them (the reference reuses hthm, src/llg.f90:1262-1266).
+#pragma once
+#include "common.cuh"
+
+namespace mrm {
+
+MRM_D void philox4x64_10(unsigned long long c[4], unsigned long long k0, unsigned long long k1) {
+  const unsigned long long M0 = 0xD2E7470EE14C6C93ull, M1 = 0xCA5A826395121157ull;
+  const unsigned long long W0 = 0x9E3779B97F4A7C15ull, W1 = 0xBB67AE8584CAA73Bull;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    unsigned long long hi0 = __umul64hi(M0, c[0]), lo0 = M0 * c[0];
+    unsigned long long hi1 = __umul64hi(M1, c[2]), lo1 = M1 * c[2];
+    unsigned long long n0 = hi1 ^ c[1] ^ k0;
+    unsigned long long n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += W0;
+    k1 += W1;
+  }
+}
+
+// Three standard normals of grain `grain` at step `step` in stream `layer`.
+MRM_D void thermal_normals(unsigned long long seed, unsigned long long layer,
+                           unsigned long long step, unsigned long long grain, double n[3]) {
+  unsigned long long c[4] = {grain, step, layer, 0ull};
+  philox4x64_10(c, seed, 0x6d726dull);
+  const double s53 = 1.0 / 9007199254740992.0;
+  double u0 = ((double)(c[0] >> 11) + 0.5) * s53;
+  double u1 = ((double)(c[1] >> 11) + 0.5) * s53;
+  double u2 = ((double)(c[2] >> 11) + 0.5) * s53;
+  double u3 = ((double)(c[3] >> 11) + 0.5) * s53;
+  double ra = sqrt(-2.0 * log(u0));
+  double rb = sqrt(-2.0 * log(u2));
+  double s, co;
+  sincospi(2.0 * u1, &s, &co);
+  n[0] = ra * co;
+  n[1] = ra * s;
+  n[2] = rb * cospi(2.0 * u3);
+}
+
+MRM_D void thermal_normals(unsigned long long seed, unsigned long long layer,
+                           unsigned long long step, unsigned long long grain, float n[3]) {
+  unsigned long long c[4] = {grain, step, layer, 0ull};
+  philox4x64_10(c, seed, 0x6d726dull);
+  const float s24 = 1.0f / 16777216.0f;
+  float u0 = ((float)(unsigned)(c[0] >> 40) + 0.5f) * s24;
+  float u1 = ((float)(unsigned)(c[1] >> 40) + 0.5f) * s24;
+  float u2 = ((float)(unsigned)(c[2] >> 40) + 0.5f) * s24;
+  float u3 = ((float)(unsigned)(c[3] >> 40) + 0.5f) * s24;
+  float ra = sqrtf(-2.0f * logf(u0));
+  float rb = sqrtf(-2.0f * logf(u2));
+  float s, co;
+  sincospif(2.0f * u1, &s, &co);
+  n[0] = ra * co;
+  n[1] = ra * s;
+  n[2] = rb * cospif(2.0f * u3);
+}
+
+}  // namespace mrm

@@ -1,0 +1,192 @@
+"""Host-side mirror of the reference's LLG/field interface on the GPU path.
+
+`GpuSim` plays the role the Fortran modules play in the reference:
+`construct_field`/`file_grain` hand over the per-layer arrays
+(upload_layer), `init_demag` builds the tensor (build_tensor),
+`set_fld`/`uniform_fld` set the applied-field schedule, `start_field` the
+thermal seeds, and `llg()` advances fixed-dt steps (step).  Every call goes
+through the C ABI of include/mrm_gpu.h; the class only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import MrmError, f64, fptr, i32, iptr
+
+
+def geom_of(medium, precision: int) -> _lib.Geom:
+    g = _lib.Geom()
+    g.nx, g.ny, g.n_lay = medium.nx, medium.ny, medium.n_lay
+    g.boundary = medium.boundary
+    g.num_images = medium.images
+    g.precision = precision
+    g.dx, g.dy = medium.dx, medium.dy
+    for l in range(medium.n_lay):
+        g.dz[l] = medium.dz[l]
+        g.il_space[l] = medium.il_space[l]
+    g.space_to_sul = medium.space_to_sul
+    g.sul_mu = medium.sul_mu
+    g.head_mu = medium.head_mu
+    g.fly_height = medium.fly_height
+    return g
+
+
+class _RunMixin:
+    """C-ABI calls shared by the plain handle and batched runs."""
+
+    h: C.c_void_p
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = _lib.load().mrm_gpu_last_error(self.h)
+            raise MrmError(rc, (msg or b"").decode())
+
+    def upload_medium(self, medium, thermal_seed: int = 1):
+        L = _lib.load()
+        self.medium = medium
+        for l, lay in enumerate(medium.layers):
+            arrs = [f64(lay.ms), f64(lay.vol), f64(lay.axis), f64(lay.hk), f64(lay.hk_scale),
+                    f64(lay.ms_scale), f64(lay.alpha_scale)]
+            g2ci, g2c = i32(lay.g2c_index), i32(lay.g2c)
+            hxi, hxg, hx = i32(lay.hx_index), i32(lay.hx_grain), f64(lay.hx)
+            self._check(L.mrm_gpu_upload_layer(self.h, l, lay.N, *[fptr(a) for a in arrs], lay.alpha,
+                                               lay.gamma, lay.floor_ms, iptr(g2ci), iptr(g2c),
+                                               iptr(hxi), iptr(hxg), fptr(hx)))
+        for l, lay in enumerate(medium.layers):
+            for side, cpl in ((0, lay.uhx), (1, lay.lhx)):
+                if cpl is not None:
+                    idx, gr, cf = i32(cpl[0]), i32(cpl[1]), f64(cpl[2])
+                    self._check(L.mrm_gpu_upload_interlayer(self.h, l, side, iptr(idx), iptr(gr), fptr(cf)))
+            self.set_uniform_field(l, lay.hdir, lay.t_start, lay.t_end, lay.s_start, lay.s_end, lay.scale)
+            self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
+        if medium.m0 is not None:
+            for l, m in enumerate(medium.m0):
+                self.set_state(l, m)
+
+    def build_tensor(self):
+        self._check(_lib.load().mrm_gpu_build_tensor(self.h))
+
+    def upload_tensor(self, n2d: np.ndarray):
+        n2d = f64(n2d)
+        px, py = self.fft_grid()
+        self._check(_lib.load().mrm_gpu_upload_tensor(self.h, fptr(n2d), px, py))
+
+    def download_tensor(self) -> np.ndarray:
+        px, py = self.fft_grid()
+        nl = self.medium.n_lay
+        out = np.zeros((nl, nl, 9, py, px))
+        self._check(_lib.load().mrm_gpu_download_tensor(self.h, fptr(out)))
+        return out
+
+    def fft_grid(self):
+        a, b = C.c_int(), C.c_int()
+        self._check(_lib.load().mrm_gpu_fft_grid(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def tensor_residual(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(_lib.load().mrm_gpu_tensor_residual(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_demag(self, on: bool):
+        self._check(_lib.load().mrm_gpu_set_demag(self.h, 1 if on else 0))
+
+    def set_uniform_field(self, layer, hdir, t_start, t_end, s_start, s_end, scale=1.0):
+        d = f64(hdir)
+        self._check(_lib.load().mrm_gpu_set_uniform_field(self.h, layer, fptr(d), t_start, t_end,
+                                                          s_start, s_end, scale))
+
+    def set_thermal(self, layer, on, temperature, seed):
+        self._check(_lib.load().mrm_gpu_set_thermal(self.h, layer, 1 if on else 0,
+                                                    float(temperature), int(seed)))
+
+    def set_state(self, layer: int, m: np.ndarray):
+        mm = f64(m)
+        self._check(_lib.load().mrm_gpu_set_state(self.h, layer, fptr(mm)))
+
+    def get_state(self, layer: int) -> np.ndarray:
+        out = np.zeros((self.medium.layers[layer].N, 3))
+        self._check(_lib.load().mrm_gpu_get_state(self.h, layer, fptr(out)))
+        return out
+
+    def get_field(self, layer: int) -> np.ndarray:
+        out = np.zeros((self.medium.layers[layer].N, 3))
+        self._check(_lib.load().mrm_gpu_get_field(self.h, layer, fptr(out)))
+        return out
+
+    def set_time(self, t: float, step: int = 0):
+        self._check(_lib.load().mrm_gpu_set_time(self.h, t, step))
+
+    def get_time(self):
+        t, s = C.c_double(), C.c_int64()
+        self._check(_lib.load().mrm_gpu_get_time(self.h, C.byref(t), C.byref(s)))
+        return t.value, s.value
+
+    def eval_field(self, t: float, layer: int = 0) -> np.ndarray:
+        """get_field(t) on the current state; returns H_demag of `layer`."""
+        out = np.zeros((self.medium.layers[layer].N, 3))
+        self._check(_lib.load().mrm_gpu_eval_field(self.h, t, layer, fptr(out)))
+        return out
+
+
+class GpuSim(_RunMixin):
+    """Plain single-run handle (the drop-in for llg()'s loop body)."""
+
+    def __init__(self, medium, precision: int = _lib.FP32, device: int = 0, demag: bool = True,
+                 thermal_seed: int = 1, tensor: Optional[np.ndarray] = None):
+        L = _lib.load()
+        self.medium = medium
+        self.precision = precision
+        g = geom_of(medium, precision)
+        h = C.c_void_p()
+        rc = L.mrm_gpu_create(C.byref(g), device, C.byref(h))
+        if rc != 0:
+            raise MrmError(rc, (L.mrm_gpu_last_error(None) or b"").decode())
+        self.h = h
+        self.upload_medium(medium, thermal_seed)
+        if demag:
+            if tensor is None:
+                self.build_tensor()
+            else:
+                self.upload_tensor(tensor)
+        else:
+            self.set_demag(False)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().mrm_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def enqueue(self, nsteps: int, dt: float, llg_type: int = -3):
+        self._check(_lib.load().mrm_gpu_enqueue_steps(self.h, int(nsteps), float(dt), int(llg_type)))
+
+    def stats(self):
+        st = np.zeros(1, _lib.STATS_DTYPE)
+        self._check(_lib.load().mrm_gpu_read_stats(self.h, st.ctypes.data))
+        return st[0]
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(_lib.load().mrm_gpu_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def profile(self, reps: int, dt: float) -> np.ndarray:
+        out = np.zeros(4)
+        self._check(_lib.load().mrm_gpu_profile(self.h, int(reps), float(dt), fptr(out)))
+        return out
+
+    def step(self, nsteps: int, dt: float, llg_type: int = -3, stats: bool = True):
+        st = np.zeros(1, _lib.STATS_DTYPE) if stats else None
+        self._check(_lib.load().mrm_gpu_step(self.h, int(nsteps), float(dt), int(llg_type),
+                                             st.ctypes.data if stats else None))
+        return st[0] if stats else None

@@ -1,0 +1,243 @@
+"""Synthetic granular media in the reference's data layout.
+
+The reference builds media with its GEN_GRAIN command
+(src/grain.f90:97-165 -> src/construct_grain.f90).  That setup is not on the
+hot path; this module produces the same *kind* of arrays, in the same
+conventions, so they can be handed to the GPU path (and to the CPU oracle in
+the tests) exactly as the Fortran host would hand over its own arrays:
+
+* grains are nodes: one grain per cell of an nx*ny grid, grain n (1-based)
+  at cell (i, j) with n = i + nx*(j-1) (src/construct_grain.f90:160-189);
+* grain2gridindex(0:N) / grain2grid(2, ncell) CSR, 1-based (data.f90:100-101);
+* Hk magnitude hk(1,n) = |1 + k_sigma*N(0,1)| * Hk  ("k_sigma < 0" Gaussian,
+  src/construct_grain.f90:1494-1506);
+* easy axis uniform in cos(theta) inside a cone k_ang around +z with uniform
+  azimuth (hk_uniform_p, :1672-1697; rotate, transform.f90:22-47);
+* nearest-neighbour intralayer exchange CSR hxgrainindex(0:N), hxgrain(nnz)
+  (1-based) and hx(nnz) in Oe, neighbours sorted by grain number
+  (:1276-1317), with periodic wrap (iwrp, :1441-1455).  hx = L*ex/(Ms*A)
+  (:1364); here the per-neighbour field `hex_oe` is given directly, i.e.
+  ex = hex_oe*Ms*A/L.
+* interlayer (vertical) exchange for columnar two-layer media: grain n of
+  layer l couples to grain n of the adjacent layer with a field `hint_oe`
+  (the reference's uhx/lhx CSR, :1006-1155).
+
+Random draws use numpy's PCG64 (seeded), not the reference's MT streams: the
+media are inputs, identical for the GPU path and the oracle.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Layer:
+    nx: int
+    ny: int
+    ms: np.ndarray            # (N,) emu/cc
+    vol: np.ndarray           # (N,) cm^3
+    axis: np.ndarray          # (N,3) unit easy axis
+    hk: np.ndarray            # (N,2) Oe: Hk1, Hk2
+    hk_scale: np.ndarray      # (N,)
+    ms_scale: np.ndarray      # (N,)
+    alpha_scale: np.ndarray   # (N,)
+    alpha: float
+    gamma: float
+    floor_ms: float
+    g2c_index: np.ndarray     # (N+1,) int32 cumulative (Fortran 0:N)
+    g2c: np.ndarray           # (ncell,2) int32, 1-based (i,j)
+    hx_index: Optional[np.ndarray]  # (N+1,) int32
+    hx_grain: Optional[np.ndarray]  # (nnz,) int32 1-based
+    hx: Optional[np.ndarray]        # (nnz,) Oe
+    uhx: Optional[tuple] = None     # (index, grain, coef) coupling to layer l-1
+    lhx: Optional[tuple] = None     # (index, grain, coef) coupling to layer l+1
+    # schedule / thermal
+    hdir: tuple = (0.0, 0.0, 1.0)
+    t_start: float = -1e22
+    t_end: float = 1e22
+    s_start: float = 1.0
+    s_end: float = 1.0
+    scale: float = 1.0
+    temperature: float = 0.0
+    thermal: bool = False
+
+    @property
+    def N(self) -> int:
+        return int(self.ms.shape[0])
+
+
+@dataclasses.dataclass
+class Medium:
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    dz: List[float]
+    il_space: List[float]
+    layers: List[Layer]
+    boundary: int = 1          # 0 periodic (reference), 1 open / zero-padded 2x
+    images: int = 2
+    space_to_sul: float = 0.0
+    sul_mu: float = 1.0
+    head_mu: float = 1.0
+    fly_height: float = 0.0
+    m0: Optional[List[np.ndarray]] = None   # initial m per layer (N,3)
+
+    @property
+    def n_lay(self) -> int:
+        return len(self.layers)
+
+    @property
+    def n_grains(self) -> int:
+        return sum(l.N for l in self.layers)
+
+
+def lattice_maps(nx: int, ny: int):
+    """grains-as-nodes grain<->cell CSR (construct_grain.f90:182-189)."""
+    n = nx * ny
+    idx = np.arange(n + 1, dtype=np.int32)
+    jj, ii = np.divmod(np.arange(n), nx)
+    g2c = np.stack([ii + 1, jj + 1], axis=1).astype(np.int32)
+    return idx, g2c
+
+
+def lattice_exchange(nx: int, ny: int, hex_oe):
+    """4-neighbour periodic exchange CSR, neighbours sorted by grain number.
+
+    hex_oe: scalar or (N,) per-grain field per unit shared edge fraction.
+    Shared edges that wrap onto the same neighbour twice accumulate
+    (construct_grain.f90:1298-1316).
+    """
+    n = nx * ny
+    hexa = np.broadcast_to(np.asarray(hex_oe, dtype=np.float64), (n,))
+    index = np.zeros(n + 1, dtype=np.int32)
+    grains: list = []
+    coefs: list = []
+    if nx >= 3 and ny >= 3:
+        g = np.arange(n)
+        j, i = np.divmod(g, nx)
+        nb = np.stack([
+            i + nx * ((j - 1) % ny),        # (i, j-1)   shared length dx
+            (i - 1) % nx + nx * j,          # (i-1, j)   shared length dy
+            (i + 1) % nx + nx * j,          # (i+1, j)   shared length dy
+            i + nx * ((j + 1) % ny),        # (i, j+1)   shared length dx
+        ], axis=1)
+        order = np.argsort(nb, axis=1, kind="stable")
+        nbs = np.take_along_axis(nb, order, axis=1)
+        index[1:] = 4 * np.arange(1, n + 1)
+        hx_grain = (nbs + 1).astype(np.int32).reshape(-1)
+        hx = np.repeat(hexa, 4)
+        return index, hx_grain, hx.astype(np.float64)
+    for g in range(n):
+        j, i = divmod(g, nx)
+        acc = {}
+        for nbg in (i + nx * ((j - 1) % ny), (i - 1) % nx + nx * j,
+                    (i + 1) % nx + nx * j, i + nx * ((j + 1) % ny)):
+            if nbg != g:
+                acc[nbg] = acc.get(nbg, 0.0) + 1.0
+        for k in sorted(acc):
+            grains.append(k + 1)
+            coefs.append(acc[k] * hexa[g])
+        index[g + 1] = len(grains)
+    return index, np.asarray(grains, np.int32), np.asarray(coefs, np.float64)
+
+
+def easy_axes(rng: np.random.Generator, n: int, k_ang_deg: float) -> np.ndarray:
+    """uniform-in-cos(theta) cone around +z, uniform azimuth (construct_grain.f90:1672-1697)."""
+    tsig = abs(k_ang_deg) * math.pi / 180.0
+    phi = 2.0 * math.pi * rng.random(n)
+    if tsig == 0.0:
+        theta = np.zeros(n)
+    else:
+        u = rng.random(n)
+        theta = np.arccos(np.minimum(1.0, np.maximum(math.cos(tsig), 1.0 - u * (1.0 - math.cos(tsig)))))
+    # rotate(phi_n=0, theta_n=0, phi, theta) (transform.f90:22-47)
+    st = np.sin(theta)
+    return np.stack([np.cos(phi) * st, np.sin(phi) * st, np.cos(theta)], axis=1)
+
+
+def hk_magnitudes(rng: np.random.Generator, n: int, hk: float, k_sigma: float) -> np.ndarray:
+    """|1 + k_sigma*N(0,1)| * hk for k_sigma<0 (Gaussian), exp(k_sigma*N) for k_sigma>0."""
+    x = 1.0 + abs(k_sigma) * rng.standard_normal(n)
+    if k_sigma > 0:
+        x = np.exp(x - 1.0)
+    return np.abs(x) * hk
+
+
+def make_layer(rng, nx, ny, dx, dy, dz, ms, hk, k_sigma, k_ang_deg, hex_oe, alpha,
+               gamma=1.76e7, hk2=0.0) -> Layer:
+    n = nx * ny
+    g2c_index, g2c = lattice_maps(nx, ny)
+    hkm = hk_magnitudes(rng, n, hk, k_sigma)
+    hkarr = np.stack([hkm, np.full(n, 0.0) + hk2 * hkm / max(hk, 1e-300)], axis=1)
+    axis = easy_axes(rng, n, k_ang_deg)
+    if hex_oe != 0.0:
+        hx_index, hx_grain, hx = lattice_exchange(nx, ny, hex_oe)
+    else:
+        hx_index = hx_grain = hx = None
+    return Layer(
+        nx=nx, ny=ny,
+        ms=np.full(n, float(ms)), vol=np.full(n, dx * dy * dz),
+        axis=axis, hk=hkarr,
+        hk_scale=np.ones(n), ms_scale=np.ones(n), alpha_scale=np.ones(n),
+        alpha=float(alpha), gamma=float(gamma), floor_ms=0.01,
+        g2c_index=g2c_index, g2c=g2c,
+        hx_index=hx_index, hx_grain=hx_grain, hx=hx,
+    )
+
+
+def columnar_coupling(n: int, coef_oe: float):
+    idx = np.arange(n + 1, dtype=np.int32)
+    grain = np.arange(1, n + 1, dtype=np.int32)
+    return idx, grain, np.full(n, float(coef_oe))
+
+
+def mh_medium(side: int, *, pitch_nm: float = 8.0, thickness_nm: float = 10.0, ms: float = 700.0,
+              hk: float = 15000.0, k_sigma: float = -0.05, k_ang_deg: float = 3.0,
+              hex_oe: float = 500.0, alpha: float = 0.1, h_max: float = 20000.0,
+              angle_deg: float = 10.0, ramp_s: float = 2e-9, temperature: float = 0.0,
+              boundary: int = 1, seed: int = 1, ny: Optional[int] = None) -> Medium:
+    """Single-layer M(H) medium (the 4,096- and 65,536-grain workloads).
+
+    Uniform field along (sin a, 0, cos a) ramped linearly from +h_max to
+    -h_max over ramp_s (applied.f90:871-883); m starts along +z.
+    """
+    nx = side
+    ny = side if ny is None else ny
+    rng = np.random.default_rng(seed)
+    dx = dy = pitch_nm * 1e-7
+    dz = thickness_nm * 1e-7
+    lay = make_layer(rng, nx, ny, dx, dy, dz, ms, hk, k_sigma, k_ang_deg, hex_oe, alpha)
+    a = math.radians(angle_deg)
+    lay.hdir = (math.sin(a), 0.0, math.cos(a))
+    lay.t_start, lay.t_end, lay.s_start, lay.s_end, lay.scale = 0.0, ramp_s, h_max, -h_max, 1.0
+    lay.temperature = float(temperature)
+    lay.thermal = temperature > 0.0
+    m0 = np.zeros((lay.N, 3))
+    m0[:, 2] = 1.0
+    return Medium(nx=nx, ny=ny, dx=dx, dy=dy, dz=[dz], il_space=[0.0], layers=[lay],
+                  boundary=boundary, m0=[m0])
+
+
+def two_layer_medium(nx: int = 1024, ny: int = 256, *, pitch_nm: float = 7.0, seed: int = 1,
+                     temperature: float = 300.0, hint_oe: float = 2000.0, hex_oe: float = 500.0,
+                     alpha: float = 0.1, boundary: int = 1) -> Medium:
+    """Exchange-coupled hard/soft recording bilayer (the two-layer write workload)."""
+    rng = np.random.default_rng(seed)
+    dx = dy = pitch_nm * 1e-7
+    hard = make_layer(rng, nx, ny, dx, dy, 8e-7, 800.0, 18000.0, -0.05, 3.0, hex_oe, alpha)
+    soft = make_layer(rng, nx, ny, dx, dy, 4e-7, 900.0, 6000.0, -0.05, 3.0, hex_oe, alpha)
+    n = nx * ny
+    # layer 1 is the top layer (nearest the head), layer 2 below it (tensor.f90:149-200)
+    hard.lhx = columnar_coupling(n, hint_oe)
+    soft.uhx = columnar_coupling(n, hint_oe)
+    for lay in (hard, soft):
+        lay.temperature = float(temperature)
+        lay.thermal = temperature > 0.0
+    m0 = [np.tile([0.0, 0.0, 1.0], (n, 1)), np.tile([0.0, 0.0, 1.0], (n, 1))]
+    return Medium(nx=nx, ny=ny, dx=dx, dy=dy, dz=[8e-7, 4e-7], il_space=[0.0, 0.0],
+                  layers=[hard, soft], boundary=boundary, m0=m0)

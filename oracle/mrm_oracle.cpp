@@ -1,0 +1,1143 @@
+// mrm_oracle.cpp -- TEST INFRASTRUCTURE, not product code.
+//
+// CPU restatement (FP64, OpenMP) of the reference's per-timestep grain dynamics
+// (com-entonos/mrm), used only as the checker: by tests/, by
+// __graft_entry__.smoke() and by bench.py's cpu_baseline / --impl reference leg.
+// The product path (mrm_b200/libmrm_gpu.so) never links or calls this file.
+//
+// Parity status: the reference is Fortran + FFTW and cannot be compiled in this
+// environment (no Fortran compiler, no FFTW), so this restatement is pinned by
+//   * numpy's independent MT19937 (tempering/twist of random.f90) and
+//     numpy's independent Philox4x64-10 (the GPU thermal stream),
+//   * closed-form physics (Stoner-Wohlfarth switching, Larmor precession,
+//     demag sum rules and tensor symmetries),
+//   * a direct FP64 O(N^2) demag summation against the FFT convolution,
+//   * numpy's pocketfft for the unnormalised r2c/c2r semantics of fftw.f90.
+// It is NOT pinned against outputs of the reference binary ("parity unpinned").
+//
+// Each routine cites the reference file:line it restates (paths relative to the
+// reference project root).
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using cd = std::complex<double>;
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// MT19937 with the reference's 1998-style seeding: src/random.f90:9-10,166-213
+// ---------------------------------------------------------------------------
+struct MT {
+  uint32_t mt[624];
+  int mti;
+  int iset;
+  double gset;
+};
+
+static void mt_create(MT* s, int seed) {
+  // random.f90:173-181: iseed=4357+|seed|; mt(0)=iseed; mt(i)=69069*mt(i-1) (32-bit wrap)
+  int32_t iseed = 4357 + std::abs(seed);
+  s->mt[0] = (uint32_t)iseed;
+  for (int i = 1; i < 624; ++i) s->mt[i] = 69069u * s->mt[i - 1];
+  s->iset = 0;
+  s->mti = 624;
+  s->gset = 0.0;
+}
+
+static uint32_t mt_next_u32(MT* s) {
+  // random.f90:191-207 (twist with UMASK/LMASK/MATA, tempering TMASKB/TMASKC)
+  const uint32_t UM = 0x80000000u, LM = 0x7fffffffu, MATA = 0x9908b0dfu;
+  const int N = 624, M = 397;
+  if (s->mti >= N) {
+    uint32_t j;
+    for (int i = 0; i < N - M; ++i) {
+      j = (s->mt[i] & UM) | (s->mt[i + 1] & LM);
+      s->mt[i] = s->mt[i + M] ^ (j >> 1) ^ ((j & 1u) ? MATA : 0u);
+    }
+    for (int i = N - M; i < N - 1; ++i) {
+      j = (s->mt[i] & UM) | (s->mt[i + 1] & LM);
+      s->mt[i] = s->mt[i + M - N] ^ (j >> 1) ^ ((j & 1u) ? MATA : 0u);
+    }
+    j = (s->mt[N - 1] & UM) | (s->mt[0] & LM);
+    s->mt[N - 1] = s->mt[M - 1] ^ (j >> 1) ^ ((j & 1u) ? MATA : 0u);
+    s->mti = 0;
+  }
+  uint32_t y = s->mt[s->mti++];
+  y ^= (y >> 11);
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= (y >> 18);
+  return y;
+}
+
+static double mt_uniform(MT* s) {
+  // random.f90:208-212: unsigned value / 2^32, in [0,1)
+  return (double)mt_next_u32(s) / 4294967296.0;
+}
+
+static double mt_normal(MT* s) {
+  // random.f90:215-229: polar Box-Muller with a cached second deviate
+  if (s->iset != 0) {
+    s->iset = 0;
+    return s->gset;
+  }
+  double v1, v2, rsq;
+  v1 = 2.0 * mt_uniform(s) - 1.0;
+  v2 = 2.0 * mt_uniform(s) - 1.0;
+  rsq = v1 * v1 + v2 * v2;
+  while (rsq >= 1.0 || rsq == 0.0) {
+    v1 = 2.0 * mt_uniform(s) - 1.0;
+    v2 = 2.0 * mt_uniform(s) - 1.0;
+    rsq = v1 * v1 + v2 * v2;
+  }
+  double f = std::sqrt(-2.0 * std::log(rsq) / rsq);
+  s->gset = v1 * f;
+  s->iset = 1;
+  return v2 * f;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x64-10 (Salmon et al., SC'11) + Box-Muller: the counter-based thermal
+// stream of the GPU path (the reference draws MT serially instead).  The same
+// definition lives in mrm_b200/csrc/philox.cuh; numpy.random.Philox pins it.
+// ---------------------------------------------------------------------------
+static inline void mulhilo64(uint64_t a, uint64_t b, uint64_t* hi, uint64_t* lo) {
+  unsigned __int128 p = (unsigned __int128)a * b;
+  *hi = (uint64_t)(p >> 64);
+  *lo = (uint64_t)p;
+}
+
+static void philox4x64(const uint64_t ctr_in[4], const uint64_t key_in[2], uint64_t out[4]) {
+  const uint64_t M0 = 0xD2E7470EE14C6C93ull, M1 = 0xCA5A826395121157ull;
+  const uint64_t W0 = 0x9E3779B97F4A7C15ull, W1 = 0xBB67AE8584CAA73Bull;
+  uint64_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+  uint64_t k0 = key_in[0], k1 = key_in[1];
+  for (int r = 0; r < 10; ++r) {
+    uint64_t hi0, lo0, hi1, lo1;
+    mulhilo64(M0, c0, &hi0, &lo0);
+    mulhilo64(M1, c2, &hi1, &lo1);
+    uint64_t n0 = hi1 ^ c1 ^ k0;
+    uint64_t n1 = lo1;
+    uint64_t n2 = hi0 ^ c3 ^ k1;
+    uint64_t n3 = lo0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += W0; k1 += W1;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// Thermal normals of one grain at one Heun step: counter (grain, step, stream, 0),
+// key (seed, 0x6d726d).  u = ((x>>11)+0.5)/2^53, Box-Muller pairs (u0,u1),(u2,u3).
+static void philox_normal3(uint64_t seed, uint64_t stream, uint64_t step, uint64_t grain,
+                           double n[3]) {
+  uint64_t ctr[4] = {grain, step, stream, 0ull};
+  uint64_t key[2] = {seed, 0x6d726dull};
+  uint64_t r[4];
+  philox4x64(ctr, key, r);
+  const double s53 = 1.0 / 9007199254740992.0;
+  double u0 = ((double)(r[0] >> 11) + 0.5) * s53;
+  double u1 = ((double)(r[1] >> 11) + 0.5) * s53;
+  double u2 = ((double)(r[2] >> 11) + 0.5) * s53;
+  const double twopi = 6.283185307179586476925286766559;
+  double ra = std::sqrt(-2.0 * std::log(u0));
+  double rb = std::sqrt(-2.0 * std::log(u2));
+  double u3 = ((double)(r[3] >> 11) + 0.5) * s53;
+  n[0] = ra * std::cos(twopi * u1);
+  n[1] = ra * std::sin(twopi * u1);
+  n[2] = rb * std::cos(twopi * u3);
+}
+
+// ---------------------------------------------------------------------------
+// Magnetostatic tensor: src/tensor_element.f90:13-102 (volume_averaged_n),
+// :219-261 (plane_to_plane), src/tensor.f90:82-216 (calculate_tensor).
+// ---------------------------------------------------------------------------
+static inline double fsign(double a, double b) { return std::copysign(std::fabs(a), b); }
+
+static inline double g1(double x, double y, double z, double d) {
+  // tensor_element.f90:78-87
+  double r = x * y * z * std::atan(y * z / fsign(std::max(1.0e-300, std::fabs(x) * d), x));
+  r += 0.5 * y * (z * z - x * x) * std::log(std::max(1.0e-300, d - y));
+  r += 0.5 * z * (y * y - x * x) * std::log(std::max(1.0e-300, d - z));
+  r += (y * y + z * z - 2.0 * x * x) * d / 6.0;
+  return r;
+}
+
+static inline double g2(double z, double x, double y, double d) {
+  // tensor_element.f90:89-100 (argument order g2(z,x,y,d) as in the reference)
+  double r = -x * y * z * std::log(std::max(1.0e-300, d + z));
+  r += y * (y * y - 3.0 * z * z) * std::log(std::max(1.0e-300, d + x)) / 6.0;
+  r += x * (x * x - 3.0 * z * z) * std::log(std::max(1.0e-300, d + y)) / 6.0;
+  r += 0.5 * x * x * z * std::atan(y * z / fsign(std::max(1.0e-300, std::fabs(x) * d), x));
+  r += 0.5 * y * y * z * std::atan(x * z / fsign(std::max(1.0e-300, std::fabs(y) * d), y));
+  r += z * z * z * std::atan(x * y / fsign(std::max(1.0e-300, std::fabs(z) * d), z)) / 6.0;
+  r += x * y * d / 3.0;
+  return r;
+}
+
+// n(a,b) -= t(a,b); n stored row-major n[a*3+b] with a = first Fortran index.
+static void volume_averaged_n(double rx, double ry, double rz, double xs, double ys, double zs,
+                              double xo, double yo, double zo, double n[9]) {
+  (void)yo;
+  // tensor_element.f90:31: dyo uses xo (reference quirk, harmless for dx=dy)
+  const double dxo[2] = {-0.5 * xo, 0.5 * xo}, dyo[2] = {-0.5 * xo, 0.5 * xo},
+               dzo[2] = {-0.5 * zo, 0.5 * zo};
+  const double dxs[2] = {-0.5 * xs, 0.5 * xs}, dys[2] = {-0.5 * ys, 0.5 * ys},
+               dzs[2] = {-0.5 * zs, 0.5 * zs};
+  double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i6 = 1; i6 <= 2; ++i6)
+    for (int i5 = 1; i5 <= 2; ++i5)
+      for (int i4 = 1; i4 <= 2; ++i4)
+        for (int i3 = 1; i3 <= 2; ++i3) {
+          double dx = -rx + dxo[i3 - 1] - dxs[i6 - 1];
+          for (int i2 = 1; i2 <= 2; ++i2) {
+            double dy = -ry + dyo[i2 - 1] - dys[i5 - 1];
+            for (int i1 = 1; i1 <= 2; ++i1) {
+              double dz = -rz + dzo[i1 - 1] - dzs[i4 - 1];
+              double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+              if (d != 0.0) {
+                double sgn = ((i1 + i2 + i3 + i4 + i5 + i6 - 1) % 2 == 0) ? 1.0 : -1.0;
+                t[0] += sgn * g1(dx, dy, dz, d);  // t(1,1)
+                t[4] += sgn * g1(dy, dz, dx, d);  // t(2,2)
+                t[8] += sgn * g1(dz, dx, dy, d);  // t(3,3)
+                double x = sgn * g2(dx, dy, dz, d);
+                t[7] += x;  // t(3,2)
+                t[5] += x;  // t(2,3)
+                x = sgn * g2(dy, dz, dx, d);
+                t[6] += x;  // t(3,1)
+                t[2] += x;  // t(1,3)
+                x = sgn * g2(dz, dx, dy, d);
+                t[3] += x;  // t(2,1)
+                t[1] += x;  // t(1,2)
+              }
+            }
+          }
+        }
+  for (int k = 0; k < 9; ++k) n[k] -= t[k];
+}
+
+// plane_to_plane: out[((a*3+b)*ny + j)*nx + i] = t(a,b) at FFT index (i,j)
+static void plane_to_plane(int nx, int ny, double dx, double dy, double dz, double dzo, double rz,
+                           int n_imgxi, int n_imgyi, double* out) {
+  const int n_imgx = std::max(0, n_imgxi);
+  const int n_imgy = std::max(0, n_imgxi);  // tensor_element.f90:230 (uses the x count)
+  (void)n_imgyi;
+  std::fill(out, out + (size_t)9 * nx * ny, 0.0);
+  const int jlo = -ny / 2, jhi = ny / 2, ilo = -nx / 2, ihi = nx / 2;
+  const int nj = jhi - jlo + 1, ni = ihi - ilo + 1;
+  // compute each offset's t in parallel, then accumulate serially in the
+  // reference's loop order (two offsets can share one FFT slot for even n)
+  std::vector<double> tt((size_t)nj * ni * 9);
+#pragma omp parallel for schedule(dynamic, 4) collapse(2)
+  for (int jj = 0; jj < nj; ++jj)
+    for (int ii = 0; ii < ni; ++ii) {
+      int j = jlo + jj, i = ilo + ii;
+      int yp0 = -n_imgy * (1 - std::max(0, j / ((ny + 1) / 2)));
+      int yp1 = n_imgy * (1 + std::min(0, j / ((ny + 1) / 2)));
+      int xp0 = -n_imgx * (1 - std::max(0, i / ((nx + 1) / 2)));
+      int xp1 = n_imgx * (1 + std::min(0, i / ((nx + 1) / 2)));
+      double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int ny_img = yp0; ny_img <= yp1; ++ny_img)
+        for (int nx_img = xp0; nx_img <= xp1; ++nx_img) {
+          double rx = (double)i * dx + (double)nx_img * dx * (double)nx;
+          double ry = (double)j * dy + (double)ny_img * dy * (double)ny;
+          volume_averaged_n(rx, ry, rz, dx, dy, dz, dx, dy, dzo, t);
+        }
+      std::memcpy(&tt[((size_t)jj * ni + ii) * 9], t, sizeof(t));
+    }
+  for (int jj = 0; jj < nj; ++jj)
+    for (int ii = 0; ii < ni; ++ii) {
+      int j = jlo + jj, i = ilo + ii;
+      int fi = ((nx - i) % nx + nx) % nx, fj = ((ny - j) % ny + ny) % ny;
+      const double* t = &tt[((size_t)jj * ni + ii) * 9];
+      for (int c = 0; c < 9; ++c) out[((size_t)c * ny + fj) * nx + fi] += t[c];
+    }
+}
+
+// calculate_tensor (tensor.f90:82-216).  n2d layout = Fortran n2d(nx,ny,9,ko,ks):
+// n2d[(((ks*nl + ko)*9 + c)*ny + j)*nx + i], c = 3*(field comp) + (source comp).
+static void calculate_tensor(int nx, int ny, int nl, double dx, double dy, const double* dz,
+                             const double* il_space, int imx, int imy, double space_to_sul,
+                             double sul_mu, double head_mu, double fly_height, double* n2d) {
+  std::fill(n2d, n2d + (size_t)nx * ny * 9 * nl * nl, 0.0);
+  bool sul_p = (sul_mu > 1.0), head_p = (head_mu > 1.0);  // tensor.f90:20,105,111
+  double mus = 0.0, mush = 0.0;
+  if (sul_p) mus = std::max(0.0, (std::max(1.0, sul_mu) - 1.0) / (std::max(1.0, sul_mu) + 1.0));
+  if (head_p) mush = std::max(0.0, (std::max(1.0, head_mu) - 1.0) / (std::max(1.0, head_mu) + 1.0));
+  std::vector<double> hdz(nl);
+  hdz[0] = fly_height;
+  for (int ks = 1; ks < nl; ++ks) hdz[ks] = hdz[ks - 1] + dz[ks - 1] + il_space[ks];
+  for (int k = 0; k < nl; ++k) hdz[k] += 0.5 * dz[k];
+  std::vector<double> nn((size_t)9 * nx * ny);
+  const size_t plane = (size_t)nx * ny;
+  double zsb = space_to_sul;
+  for (int ks = nl - 1; ks >= 0; --ks) {
+    double zst = zsb + dz[ks];
+    double zob = space_to_sul;
+    for (int ko = nl - 1; ko >= 0; --ko) {
+      double zot = zob + dz[ko];
+      double* dst = n2d + ((size_t)ks * nl + ko) * 9 * plane;
+      // nn(:,:,a,b) -> n2d(:,:,3*(b-1)+a): dst[c=3*b+a] = t(a,b)
+      plane_to_plane(nx, ny, dx, dy, dz[ks], dz[ko], 0.5 * (zst - zot + zsb - zob), imx, imy,
+                     nn.data());
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          for (size_t p = 0; p < plane; ++p) dst[(3 * b + a) * plane + p] = nn[(a * 3 + b) * plane + p];
+      if (sul_p) {
+        plane_to_plane(nx, ny, dx, dy, dz[ks], dz[ko], 0.5 * (-zst - zot - zsb - zob), imx, imy,
+                       nn.data());
+        for (int a = 0; a < 3; ++a) {
+          double f = (a < 2) ? -mus : mus;  // tensor.f90:167
+          for (int b = 0; b < 3; ++b)
+            for (size_t p = 0; p < plane; ++p) dst[(3 * b + a) * plane + p] += f * nn[(a * 3 + b) * plane + p];
+        }
+      }
+      if (head_p) {
+        plane_to_plane(nx, ny, dx, dy, dz[ks], dz[ko], hdz[ks] + hdz[ko], imx, imy, nn.data());
+        for (int a = 0; a < 3; ++a) {
+          double f = (a < 2) ? -mush : mush;  // tensor.f90:177
+          for (int b = 0; b < 3; ++b)
+            for (size_t p = 0; p < plane; ++p) dst[(3 * b + a) * plane + p] += f * nn[(a * 3 + b) * plane + p];
+        }
+      }
+      double norm = 1.0 / (dx * dy * dz[ko] * (double)nx * (double)ny);  // tensor.f90:183
+      for (size_t p = 0; p < 9 * plane; ++p) dst[p] *= norm;
+      zob = zot + il_space[ko];
+    }
+    zsb = zst + il_space[ks];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FFT with FFTW's unnormalised r2c / c2r semantics (fftw.f90:37-93).
+// Radix-2 iterative for powers of two, direct DFT otherwise (test sizes only).
+// ---------------------------------------------------------------------------
+struct FFT1 {
+  int n = 0;
+  bool pow2 = true;
+  std::vector<cd> tw;  // e^{-2 pi i k/n}
+  std::vector<int> rev;
+  void init(int n_) {
+    n = n_;
+    pow2 = (n > 0) && ((n & (n - 1)) == 0);
+    tw.resize(n);
+    for (int k = 0; k < n; ++k) {
+      double a = -2.0 * M_PI * (double)k / (double)n;
+      tw[k] = cd(std::cos(a), std::sin(a));
+    }
+    if (pow2) {
+      rev.resize(n);
+      int lg = 0;
+      while ((1 << lg) < n) ++lg;
+      for (int i = 0; i < n; ++i) {
+        int r = 0;
+        for (int b = 0; b < lg; ++b)
+          if (i & (1 << b)) r |= 1 << (lg - 1 - b);
+        rev[i] = r;
+      }
+    }
+  }
+  // in-place, sign -1 (forward) or +1 (backward), unnormalised
+  void run(cd* a, int sign, cd* scratch) const {
+    if (pow2) {
+      for (int i = 0; i < n; ++i)
+        if (i < rev[i]) std::swap(a[i], a[rev[i]]);
+      for (int len = 2; len <= n; len <<= 1) {
+        int half = len >> 1, step = n / len;
+        for (int i = 0; i < n; i += len)
+          for (int k = 0; k < half; ++k) {
+            cd w = tw[k * step];
+            if (sign > 0) w = std::conj(w);
+            cd u = a[i + k], v = a[i + k + half] * w;
+            a[i + k] = u + v;
+            a[i + k + half] = u - v;
+          }
+      }
+    } else {
+      for (int k = 0; k < n; ++k) {
+        cd s = 0;
+        for (int j = 0; j < n; ++j) {
+          cd w = tw[(size_t)((long long)j * k % n)];
+          if (sign > 0) w = std::conj(w);
+          s += a[j] * w;
+        }
+        scratch[k] = s;
+      }
+      for (int k = 0; k < n; ++k) a[k] = scratch[k];
+    }
+  }
+};
+
+struct FFT2 {
+  int nx = 0, ny = 0, nh = 0;  // nh = nx/2+1
+  FFT1 fx, fy;
+  void init(int nx_, int ny_) {
+    nx = nx_; ny = ny_; nh = nx / 2 + 1;
+    fx.init(nx); fy.init(ny);
+  }
+  // r[ny][nx] -> c[ny][nh]
+  void r2c(const double* r, cd* c) const {
+#pragma omp parallel
+    {
+      std::vector<cd> row(nx), scr(std::max(nx, ny));
+#pragma omp for
+      for (int j = 0; j < ny; ++j) {
+        for (int i = 0; i < nx; ++i) row[i] = cd(r[(size_t)j * nx + i], 0.0);
+        fx.run(row.data(), -1, scr.data());
+        for (int k = 0; k < nh; ++k) c[(size_t)j * nh + k] = row[k];
+      }
+    }
+#pragma omp parallel
+    {
+      std::vector<cd> col(ny), scr(std::max(nx, ny));
+#pragma omp for
+      for (int k = 0; k < nh; ++k) {
+        for (int j = 0; j < ny; ++j) col[j] = c[(size_t)j * nh + k];
+        fy.run(col.data(), -1, scr.data());
+        for (int j = 0; j < ny; ++j) c[(size_t)j * nh + k] = col[j];
+      }
+    }
+  }
+  // c[ny][nh] (Hermitian half) -> r[ny][nx], unnormalised; c is destroyed
+  void c2r(cd* c, double* r) const {
+#pragma omp parallel
+    {
+      std::vector<cd> col(ny), scr(std::max(nx, ny));
+#pragma omp for
+      for (int k = 0; k < nh; ++k) {
+        for (int j = 0; j < ny; ++j) col[j] = c[(size_t)j * nh + k];
+        fy.run(col.data(), +1, scr.data());
+        for (int j = 0; j < ny; ++j) c[(size_t)j * nh + k] = col[j];
+      }
+    }
+#pragma omp parallel
+    {
+      std::vector<cd> row(nx), scr(std::max(nx, ny));
+#pragma omp for
+      for (int j = 0; j < ny; ++j) {
+        for (int k = 0; k < nh; ++k) row[k] = c[(size_t)j * nh + k];
+        for (int k = nh; k < nx; ++k) row[k] = std::conj(c[(size_t)j * nh + (nx - k)]);
+        // FFTW c2r ignores the imaginary parts of the self-conjugate bins
+        row[0] = cd(row[0].real(), 0.0);
+        if (nx % 2 == 0) row[nx / 2] = cd(row[nx / 2].real(), 0.0);
+        fx.run(row.data(), +1, scr.data());
+        for (int i = 0; i < nx; ++i) r[(size_t)j * nx + i] = row[i].real();
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Simulation state (data_s src/data.f90:91-104, field_ss src/field.f90:15-35,
+// llg_s src/llg.f90:16-25), restricted to the LLG path.
+// ---------------------------------------------------------------------------
+struct Layer {
+  int N = 0;
+  std::vector<double> ms, vol, axis, hk, hk_scale, ms_scale, alpha_scale;
+  double alpha = 1.0, gamma = 1.76e7, floor_ms = 0.01;
+  std::vector<int> hx_idx, hx_nbr;  // CSR: hx_idx[N+1] cumulative, hx_nbr 0-based
+  std::vector<double> hx;
+  std::vector<int> uhx_idx, uhx_nbr, lhx_idx, lhx_nbr;  // interlayer (upper = layer-1)
+  std::vector<double> uhx, lhx;
+  std::vector<int> g2c_idx, g2c_i, g2c_j;  // grain -> cells (0-based i,j)
+  std::vector<double> m[2], dm, h, hthm, hdemag, happ;
+  // schedule: uniform field x linear ramp (applied.f90:863-883)
+  double hdir[3] = {0, 0, 0};
+  double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
+  double temperature = 0.0;
+  bool thermal = false;
+  MT rng;
+};
+
+struct Stats {
+  double t;
+  long long step;
+  double mave[3], mvar[3], have[3];
+  double errmx, errmx1, mmag, energy;
+  double mave_l[8][3], mvar_l[8][3], have_l[8][3], mms_l[8][3];
+  double vol_l[8], msvol_l[8];
+  long long nup_l[8];
+};
+
+struct Sim {
+  int nx, ny, nl;
+  int boundary;  // 0 periodic (reference), 1 open (zero-padded 2x)
+  int images;
+  double dx, dy;
+  std::vector<double> dz, il_space;
+  double space_to_sul = 0, sul_mu = 1, head_mu = 1, fly_height = 0;
+  int px, py, ph;  // FFT grid and half width
+  FFT2 fft;
+  std::vector<cd> nhat;  // [ks][ko][9][py][ph]
+  bool demag_on = true;
+  std::vector<Layer> L;
+  int in = 0;          // which m buffer is current (llg.f90 `in` toggle, 0 or 1)
+  double t = 0.0;
+  long long step = 0;
+  int rng_mode = 0;  // 0: MT per layer (reference), 1: Philox (GPU stream)
+  uint64_t seed = 1;
+  // scratch
+  std::vector<double> grid;
+  std::vector<cd> spec;
+  Stats last{};
+};
+
+// ----- tensor spectrum (demag.f90:255-267, computed here in FP64) -----
+static void build_spectrum(Sim* s, const double* n2d_real) {
+  const int nl = s->nl;
+  const size_t plane = (size_t)s->px * s->py, hplane = (size_t)s->ph * s->py;
+  s->nhat.assign((size_t)nl * nl * 9 * hplane, cd(0, 0));
+  for (int p = 0; p < nl * nl * 9; ++p) s->fft.r2c(n2d_real + p * plane, &s->nhat[p * hplane]);
+}
+
+// grain -> cell scatter of Ms*ms_scale*m (data.f90:322-390)
+static void scatter_m(Sim* s, int buf, std::vector<double>& grid) {
+  const size_t plane = (size_t)s->px * s->py;
+  grid.assign((size_t)s->nl * 3 * plane, 0.0);
+  for (int l = 0; l < s->nl; ++l) {
+    Layer& Ly = s->L[l];
+    const double* m = Ly.m[buf].data();
+    for (int n = 0; n < Ly.N; ++n) {
+      double f = Ly.ms[n] * Ly.ms_scale[n];
+      for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
+        size_t cell = (size_t)Ly.g2c_j[q] * s->px + Ly.g2c_i[q];
+        for (int a = 0; a < 3; ++a) grid[((size_t)l * 3 + a) * plane + cell] = f * m[3 * n + a];
+      }
+    }
+  }
+}
+
+// get_demag (demag.f90:33-135) + get_magnetostatic gather (field.f90:438-470)
+static void demag_from_grid(Sim* s, std::vector<double>& grid) {
+  const int nl = s->nl;
+  const size_t plane = (size_t)s->px * s->py, hplane = (size_t)s->ph * s->py;
+  std::vector<cd> X((size_t)nl * 3 * hplane), H((size_t)nl * 3 * hplane, cd(0, 0));
+  for (int p = 0; p < nl * 3; ++p) s->fft.r2c(&grid[p * plane], &X[p * hplane]);
+  for (int ks = 0; ks < nl; ++ks)
+    for (int ko = 0; ko < nl; ++ko) {
+      const cd* N = &s->nhat[((size_t)ks * nl + ko) * 9 * hplane];
+      for (int a = 0; a < 3; ++a) {
+        cd* Ha = &H[((size_t)ko * 3 + a) * hplane];
+        for (int b = 0; b < 3; ++b) {
+          const cd* Nab = N + (size_t)(3 * a + b) * hplane;
+          const cd* Xb = &X[((size_t)ks * 3 + b) * hplane];
+          for (size_t q = 0; q < hplane; ++q) Ha[q] += Nab[q] * Xb[q];
+        }
+      }
+    }
+  for (int p = 0; p < nl * 3; ++p) s->fft.c2r(&H[p * hplane], &grid[p * plane]);
+}
+
+static void gather_demag(Sim* s, const std::vector<double>& grid) {
+  const size_t plane = (size_t)s->px * s->py;
+  for (int l = 0; l < s->nl; ++l) {
+    Layer& Ly = s->L[l];
+    for (int n = 0; n < Ly.N; ++n) {
+      double y[3] = {0, 0, 0};
+      for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
+        size_t cell = (size_t)Ly.g2c_j[q] * s->px + Ly.g2c_i[q];
+        for (int a = 0; a < 3; ++a) y[a] += grid[((size_t)l * 3 + a) * plane + cell];
+      }
+      double cnt = (double)(Ly.g2c_idx[n + 1] - Ly.g2c_idx[n]);
+      for (int a = 0; a < 3; ++a) Ly.hdemag[3 * n + a] = y[a] / cnt;
+    }
+  }
+}
+
+static void compute_demag(Sim* s, int buf) {
+  if (!s->demag_on) {
+    for (auto& Ly : s->L) std::fill(Ly.hdemag.begin(), Ly.hdemag.end(), 0.0);
+    return;
+  }
+  scatter_m(s, buf, s->grid);
+  demag_from_grid(s, s->grid);
+  gather_demag(s, s->grid);
+}
+
+// applied field: linear ramp x uniform direction (applied.f90:871-883, set_fld :309-317)
+static double ramp_scale(const Layer& Ly, double t) {
+  double u = (t - Ly.t_start) / (Ly.t_end - Ly.t_start);
+  u = std::max(0.0, std::min(1.0, u));
+  return ((Ly.s_end - Ly.s_start) * u + Ly.s_start) * Ly.scale;
+}
+
+// get_field (field.f90:160-273) for the LLG path; energy per grain summed into *energy
+static void get_field(Sim* s, double t, int buf, double* energy) {
+  compute_demag(s, buf);
+  double e_tot = 0.0;
+  for (int l = 0; l < s->nl; ++l) {
+    Layer& Ly = s->L[l];
+    double sc = ramp_scale(Ly, t);
+    const double* m = Ly.m[buf].data();
+    double el = 0.0;
+#pragma omp parallel for reduction(+ : el)
+    for (int n = 0; n < Ly.N; ++n) {
+      double ha[3] = {sc * Ly.hdir[0], sc * Ly.hdir[1], sc * Ly.hdir[2]};
+      for (int a = 0; a < 3; ++a) Ly.happ[3 * n + a] = ha[a];
+      const double* mn = m + 3 * n;
+      const double* hd = &Ly.hdemag[3 * n];
+      double en = -(mn[0] * (hd[0] + ha[0]) + mn[1] * (hd[1] + ha[1]) + mn[2] * (hd[2] + ha[2])) *
+                  Ly.ms[n] * Ly.ms_scale[n];
+      double h[3] = {ha[0] + hd[0], ha[1] + hd[1], ha[2] + hd[2]};
+      // get_uni_hk field.f90:366-375
+      if (Ly.hk_scale[n] > 0.0) {
+        const double* k = &Ly.axis[3 * n];
+        double hks = mn[0] * k[0] + mn[1] * k[1] + mn[2] * k[2];
+        double yy = 1.0 - hks * hks;
+        double f = hks * (Ly.hk[2 * n] + Ly.hk[2 * n + 1] * yy) * Ly.hk_scale[n];
+        for (int a = 0; a < 3; ++a) h[a] += f * k[a];
+        en += 0.5 * yy * (Ly.hk[2 * n] + 0.5 * Ly.hk[2 * n + 1] * yy) * Ly.hk_scale[n] * Ly.ms[n] *
+              Ly.ms_scale[n];
+      }
+      // get_intralayer_hx field.f90:350-363
+      if (!Ly.hx_idx.empty()) {
+        double hx[3] = {0, 0, 0};
+        for (int q = Ly.hx_idx[n]; q < Ly.hx_idx[n + 1]; ++q) {
+          int j = Ly.hx_nbr[q];
+          double c = Ly.hx[q] * Ly.ms_scale[j];
+          for (int a = 0; a < 3; ++a) hx[a] += c * m[3 * j + a];
+        }
+        en += -(hx[0] * mn[0] + hx[1] * mn[1] + hx[2] * mn[2]) * Ly.ms[n] * Ly.ms_scale[n];
+        for (int a = 0; a < 3; ++a) h[a] += hx[a];
+      }
+      // get_interlayer_hx field.f90:326-348 (upper = layer l-1, lower = layer l+1)
+      for (int side = 0; side < 2; ++side) {
+        const std::vector<int>& idx = side == 0 ? Ly.uhx_idx : Ly.lhx_idx;
+        const std::vector<int>& nbr = side == 0 ? Ly.uhx_nbr : Ly.lhx_nbr;
+        const std::vector<double>& cf = side == 0 ? Ly.uhx : Ly.lhx;
+        if (idx.empty()) continue;
+        const Layer& Q = s->L[side == 0 ? l - 1 : l + 1];
+        const double* mq = Q.m[buf].data();
+        double hv[3] = {0, 0, 0};
+        for (int q = idx[n]; q < idx[n + 1]; ++q) {
+          int j = nbr[q];
+          double c = cf[q] * Q.ms_scale[j];
+          for (int a = 0; a < 3; ++a) hv[a] += c * mq[3 * j + a];
+        }
+        en += -(hv[0] * mn[0] + hv[1] * mn[1] + hv[2] * mn[2]) * Ly.ms_scale[n] * Ly.ms[n];
+        for (int a = 0; a < 3; ++a) h[a] += hv[a];
+      }
+      for (int a = 0; a < 3; ++a) Ly.h[3 * n + a] = h[a];
+      el += en * Ly.vol[n];
+    }
+    e_tot += el;
+  }
+  if (energy) *energy = e_tot;
+}
+
+// get_thermal (field.f90:397-436), LLG branch (mag == 1, ms_scale > 0)
+static void get_thermal(Sim* s) {
+  const double kB = 1.380662e-16;
+  for (int l = 0; l < s->nl; ++l) {
+    Layer& Ly = s->L[l];
+    if (!Ly.thermal) {
+      std::fill(Ly.hthm.begin(), Ly.hthm.end(), 0.0);
+      continue;
+    }
+    double tsigma = std::sqrt(2.0 * kB * Ly.alpha / Ly.gamma);
+    for (int n = 0; n < Ly.N; ++n) {
+      double x = 0.0;
+      if (Ly.ms_scale[n] > 0.0)
+        x = Ly.alpha_scale[n] * Ly.temperature /
+            (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, Ly.ms_scale[n]));
+      x = std::sqrt(x) * tsigma;
+      double r[3];
+      if (s->rng_mode == 0) {
+        // random_normal3d (random.f90:231-249)
+        for (int a = 0; a < 3; ++a) r[a] = mt_normal(&Ly.rng);
+      } else {
+        philox_normal3(s->seed, (uint64_t)l, (uint64_t)s->step, (uint64_t)n, r);
+      }
+      for (int a = 0; a < 3; ++a) Ly.hthm[3 * n + a] = x * r[a];
+    }
+  }
+}
+
+static inline void cross(const double* a, const double* b, double* c) {
+  // transform.f90:16-20
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// push_llg (llg.f90:1066-1155): one stage for one layer.
+// Heun (type -3) branch :1122-1139, Boris/semi-implicit (|type|=2) :1109-1118.
+static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l,
+                     double* errmx1_l, double* mmag1) {
+  Layer& Ly = s->L[l];
+  const int id = s->in;  // current buffer; next buffer = 1-id
+  const double scale1 = -0.5 * Ly.gamma * dt;
+  double em = 0.0, em1 = 0.0, mm = 0.0;
+  const double sdt0 = std::sqrt(dt0);
+#pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
+  for (int n = 0; n < Ly.N; ++n) {
+    double h[3];
+    for (int a = 0; a < 3; ++a) h[a] = Ly.hthm[3 * n + a] / sdt0 + Ly.h[3 * n + a];
+    double* mnext = &Ly.m[1 - id][3 * n];
+    const double* mcur = &Ly.m[id][3 * n];
+    if (Ly.ms_scale[n] > 0.0) {
+      double m[3] = {mcur[0], mcur[1], mcur[2]};
+      double t[3], d[3], y;
+      const double ms2 = Ly.ms[n] * Ly.ms[n];
+      if (std::abs(type) < 3) {
+        cross(m, h, t);
+        y = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+        if (y > em * ms2) em = y / ms2;
+        double scale2 = Ly.alpha_scale[n] * Ly.alpha;
+        // |type| == 2: semi-implicit (Boris) push, llg.f90:1115-1118
+        double o[3] = {scale1 * h[0] - scale2 * m[0], scale1 * h[1] - scale2 * m[1],
+                       scale1 * h[2] - scale2 * m[2]};
+        double mo[3];
+        cross(m, o, mo);
+        double tt[3] = {m[0] + mo[0], m[1] + mo[1], m[2] + mo[2]};
+        double yy = 2.0 / (1.0 + o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+        double to[3];
+        cross(tt, o, to);
+        for (int a = 0; a < 3; ++a) d[a] = yy * to[a];
+        em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int a = 0; a < 3; ++a) mnext[a] = m[a] + d[a];
+      } else {
+        double scale2 = Ly.alpha_scale[n] * Ly.alpha;
+        double scale11 = 2.0 * scale1 / (1.0 + scale2 * scale2);
+        if (iter == 1)
+          for (int a = 0; a < 3; ++a) m[a] = mnext[a];  // second (corrector) stage
+        cross(m, h, t);
+        double mt[3];
+        cross(m, t, mt);
+        for (int a = 0; a < 3; ++a) d[a] = scale11 * (t[a] + scale2 * mt[a]);
+        if (iter == 1) {
+          for (int a = 0; a < 3; ++a) d[a] = 0.5 * (d[a] + Ly.dm[3 * n + a]);
+        } else {
+          for (int a = 0; a < 3; ++a) Ly.dm[3 * n + a] = d[a];
+        }
+        y = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+        if (y > em * ms2) em = y / ms2;
+        em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int a = 0; a < 3; ++a) mnext[a] = mcur[a] + d[a];
+        y = mnext[0] * mnext[0] + mnext[1] * mnext[1] + mnext[2] * mnext[2];
+        if (y > 0.0) {
+          double r = std::sqrt(y);
+          for (int a = 0; a < 3; ++a) mnext[a] /= r;
+        }
+      }
+    } else {
+      // ms_scale <= 0: m along h (llg.f90:1140-1148)
+      double hh[3] = {Ly.h[3 * n], Ly.h[3 * n + 1], Ly.h[3 * n + 2]};
+      double y = std::sqrt(hh[0] * hh[0] + hh[1] * hh[1] + hh[2] * hh[2]);
+      if (y > 0.0)
+        for (int a = 0; a < 3; ++a) mnext[a] = hh[a] / y;
+      else
+        for (int a = 0; a < 3; ++a) mnext[a] = mcur[a];
+    }
+    mm += std::sqrt(mnext[0] * mnext[0] + mnext[1] * mnext[1] + mnext[2] * mnext[2]) *
+          Ly.ms_scale[n] * Ly.vol[n];
+  }
+  *errmx_l = em;
+  *errmx1_l = em1;
+  *mmag1 = mm;
+}
+
+static void compute_stats(Sim* s, double errmx, double errmx1, double mmag, double energy) {
+  Stats& st = s->last;
+  std::memset(&st, 0, sizeof(st));
+  st.t = s->t;
+  st.step = s->step;
+  double vtot = 0.0;
+  for (int l = 0; l < s->nl; ++l) {
+    Layer& Ly = s->L[l];
+    const double* m = Ly.m[s->in].data();
+    double V = 0, Mw = 0, sm[3] = {0, 0, 0}, sh[3] = {0, 0, 0}, sms[3] = {0, 0, 0};
+    long long nup = 0;
+    double hd[3] = {Ly.hdir[0], Ly.hdir[1], Ly.hdir[2]};
+    for (int n = 0; n < Ly.N; ++n) {
+      double v = Ly.vol[n];
+      V += v;
+      double w = Ly.ms[n] * Ly.ms_scale[n] * v;
+      Mw += w;
+      for (int a = 0; a < 3; ++a) {
+        sm[a] += v * m[3 * n + a];
+        sh[a] += v * Ly.h[3 * n + a];
+        sms[a] += w * m[3 * n + a];
+      }
+      if (m[3 * n] * hd[0] + m[3 * n + 1] * hd[1] + m[3 * n + 2] * hd[2] > 0.0) ++nup;
+    }
+    double mv[3] = {0, 0, 0};
+    for (int n = 0; n < Ly.N; ++n)
+      for (int a = 0; a < 3; ++a) {
+        double dd = m[3 * n + a] - sm[a] / V;
+        mv[a] += Ly.vol[n] * dd * dd;
+      }
+    for (int a = 0; a < 3; ++a) {
+      st.mave_l[l][a] = sm[a] / V;
+      st.mvar_l[l][a] = mv[a] / V;
+      st.have_l[l][a] = sh[a] / V;
+      st.mms_l[l][a] = sms[a] * Mw / (Mw * Mw + 1e-300);
+    }
+    st.vol_l[l] = V;
+    st.msvol_l[l] = Mw;
+    st.nup_l[l] = nup;
+    vtot += V;
+  }
+  for (int l = 0; l < s->nl; ++l)
+    for (int a = 0; a < 3; ++a) {
+      st.mave[a] += st.vol_l[l] * st.mave_l[l][a] / vtot;
+      st.mvar[a] += st.vol_l[l] * st.mvar_l[l][a] / vtot;
+      st.have[a] += st.vol_l[l] * st.have_l[l][a] / vtot;
+    }
+  st.errmx = errmx;
+  st.errmx1 = errmx1;
+  st.mmag = mmag;
+  st.energy = energy;
+}
+
+// One pass of the llg() loop body (llg.f90:240-269) with push_m (llg.f90:1195-1271)
+// at fixed dt (fixed_dt_p: max_dmdt = 1, no retries).
+static void heun_or_boris_step(Sim* s, double dt, int type) {
+  const int nl = s->nl;
+  double energy = 0.0;
+  // get_fields(t): field + thermal at the current state (llg.f90:363-365)
+  get_field(s, s->t, s->in, &energy);
+  get_thermal(s);
+  double dt_s = 1.0;
+  int iter = 1;
+  if (type < 0) {
+    iter = 2;
+    if (type > -3) dt_s = 0.5;
+  }
+  double errmx = 0, errmx1 = 0, mmag = 0;
+  while (iter > 0) {
+    errmx = 0; errmx1 = 0; mmag = 0;
+    for (int l = 0; l < nl; ++l) {
+      double e0, e1, m1;
+      push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
+      double vs = 0;
+      for (int n = 0; n < s->L[l].N; ++n) vs += s->L[l].vol[n];
+      mmag += m1 / vs;
+      errmx = std::max(errmx, std::sqrt(e0));
+      errmx1 = std::max(errmx1, e1);
+    }
+    iter -= 1;
+    if (iter > 0) {
+      // llg.f90:1262-1266: field at t+dt*dt_s on the predicted state, thermal reused
+      s->in = 1 - s->in;
+      get_field(s, s->t + dt * dt_s, s->in, &energy);
+      s->in = 1 - s->in;
+      dt_s = 1.0;
+    }
+  }
+  s->in = 1 - s->in;  // llg.f90:1269
+  s->t += dt;
+  s->step += 1;
+  compute_stats(s, errmx, errmx1, mmag, energy);
+}
+
+}  // namespace orc
+
+// ===========================================================================
+// C ABI for ctypes (tests / bench cpu leg only)
+// ===========================================================================
+using namespace orc;
+
+extern "C" {
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int orc_get_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// ---- RNG probes ----
+void orc_mt_u32(int seed, int n, uint32_t* out) {
+  MT s;
+  mt_create(&s, seed);
+  for (int i = 0; i < n; ++i) out[i] = mt_next_u32(&s);
+}
+void orc_mt_state(int seed, uint32_t* out624) {
+  MT s;
+  mt_create(&s, seed);
+  std::memcpy(out624, s.mt, sizeof(s.mt));
+}
+void orc_mt_normals(int seed, int n, double* out) {
+  MT s;
+  mt_create(&s, seed);
+  for (int i = 0; i < n; ++i) out[i] = mt_normal(&s);
+}
+void orc_philox4x64(const uint64_t* ctr, const uint64_t* key, uint64_t* out) {
+  philox4x64(ctr, key, out);
+}
+void orc_philox_normal3(uint64_t seed, uint64_t stream, uint64_t step, uint64_t grain, double* out) {
+  philox_normal3(seed, stream, step, grain, out);
+}
+
+// ---- tensor ----
+void orc_volume_averaged_n(double rx, double ry, double rz, double xs, double ys, double zs,
+                           double xo, double yo, double zo, double* n9) {
+  volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo, n9);
+}
+void orc_calculate_tensor(int nx, int ny, int nl, double dx, double dy, const double* dz,
+                          const double* il_space, int imx, int imy, double space_to_sul,
+                          double sul_mu, double head_mu, double fly_height, double* n2d) {
+  calculate_tensor(nx, ny, nl, dx, dy, dz, il_space, imx, imy, space_to_sul, sul_mu, head_mu,
+                   fly_height, n2d);
+}
+
+// ---- FFT probes (row-major [ny][nx] real, [ny][nx/2+1] complex interleaved) ----
+void orc_fft_r2c(int nx, int ny, const double* r, double* c) {
+  FFT2 f;
+  f.init(nx, ny);
+  f.r2c(r, reinterpret_cast<cd*>(c));
+}
+void orc_fft_c2r(int nx, int ny, const double* c_in, double* r) {
+  FFT2 f;
+  f.init(nx, ny);
+  std::vector<cd> c(reinterpret_cast<const cd*>(c_in),
+                    reinterpret_cast<const cd*>(c_in) + (size_t)ny * (nx / 2 + 1));
+  f.c2r(c.data(), r);
+}
+
+// Direct FP64 circular convolution with the real-space tensor n2d (reference layout):
+// H_a(o) = P * sum_s sum_b n2d[ks][ko][3a+b][(o-s) mod P] M_b(s), for a list of
+// observation cells `obs` (pairs i,j) on layer ko.  M grids [nl][3][py][px].
+void orc_demag_direct(int px, int py, int nl, const double* n2d, const double* mgrid, int nobs,
+                      const int* obs_ij, int ko, double* hout) {
+  const size_t plane = (size_t)px * py;
+  const double P = (double)px * py;
+#pragma omp parallel for schedule(static)
+  for (int q = 0; q < nobs; ++q) {
+    int oi = obs_ij[2 * q], oj = obs_ij[2 * q + 1];
+    double h[3] = {0, 0, 0};
+    for (int ks = 0; ks < nl; ++ks) {
+      const double* N = n2d + ((size_t)ks * nl + ko) * 9 * plane;
+      for (int sj = 0; sj < py; ++sj) {
+        int dj = ((oj - sj) % py + py) % py;
+        for (int si = 0; si < px; ++si) {
+          size_t sc = (size_t)sj * px + si;
+          double m0 = mgrid[((size_t)ks * 3 + 0) * plane + sc];
+          double m1 = mgrid[((size_t)ks * 3 + 1) * plane + sc];
+          double m2 = mgrid[((size_t)ks * 3 + 2) * plane + sc];
+          if (m0 == 0.0 && m1 == 0.0 && m2 == 0.0) continue;
+          int di = ((oi - si) % px + px) % px;
+          size_t off = (size_t)dj * px + di;
+          for (int a = 0; a < 3; ++a)
+            h[a] += N[(3 * a + 0) * plane + off] * m0 + N[(3 * a + 1) * plane + off] * m1 +
+                    N[(3 * a + 2) * plane + off] * m2;
+        }
+      }
+    }
+    for (int a = 0; a < 3; ++a) hout[3 * q + a] = h[a] * P;
+  }
+}
+
+// ---- simulation handle ----
+void* orc_create(int nx, int ny, int nl, int boundary, int images, double dx, double dy,
+                 const double* dz, const double* il_space, double space_to_sul, double sul_mu,
+                 double head_mu, double fly_height, int demag_on) {
+  Sim* s = new Sim();
+  s->nx = nx; s->ny = ny; s->nl = nl;
+  s->boundary = boundary; s->images = images;
+  s->dx = dx; s->dy = dy;
+  s->dz.assign(dz, dz + nl);
+  s->il_space.assign(il_space, il_space + nl);
+  s->space_to_sul = space_to_sul; s->sul_mu = sul_mu; s->head_mu = head_mu;
+  s->fly_height = fly_height;
+  s->px = boundary == 1 ? 2 * nx : nx;
+  s->py = boundary == 1 ? 2 * ny : ny;
+  s->ph = s->px / 2 + 1;
+  s->fft.init(s->px, s->py);
+  s->demag_on = demag_on != 0;
+  s->L.resize(nl);
+  return s;
+}
+
+void orc_destroy(void* h) { delete static_cast<Sim*>(h); }
+
+// Real-space tensor of the FFT grid (reference layout, with normalisation), FP64.
+// Periodic: calculate_tensor on (nx,ny) with the handle's images; open: on the
+// padded grid (2nx,2ny) with no images.
+void orc_build_tensor(void* h, double* n2d_out) {
+  Sim* s = static_cast<Sim*>(h);
+  int im = s->boundary == 1 ? 0 : s->images;
+  std::vector<double> n2d((size_t)s->px * s->py * 9 * s->nl * s->nl);
+  calculate_tensor(s->px, s->py, s->nl, s->dx, s->dy, s->dz.data(), s->il_space.data(), im, im,
+                   s->space_to_sul, s->sul_mu, s->head_mu, s->fly_height, n2d.data());
+  build_spectrum(s, n2d.data());
+  if (n2d_out) std::memcpy(n2d_out, n2d.data(), n2d.size() * sizeof(double));
+}
+
+void orc_set_tensor(void* h, const double* n2d) {
+  Sim* s = static_cast<Sim*>(h);
+  build_spectrum(s, n2d);
+}
+
+int orc_upload_layer(void* h, int l, int N, const double* ms, const double* vol,
+                     const double* axis, const double* hk, const double* hk_scale,
+                     const double* ms_scale, const double* alpha_scale, double alpha, double gamma,
+                     double floor_ms, const int* g2c_index, const int* g2c /* 2 per cell, 1-based */,
+                     const int* hx_index, const int* hx_grain /*1-based*/, const double* hx) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.N = N;
+  Ly.ms.assign(ms, ms + N);
+  Ly.vol.assign(vol, vol + N);
+  Ly.axis.assign(axis, axis + 3 * N);
+  Ly.hk.assign(hk, hk + 2 * N);
+  Ly.hk_scale.assign(hk_scale, hk_scale + N);
+  Ly.ms_scale.assign(ms_scale, ms_scale + N);
+  Ly.alpha_scale.assign(alpha_scale, alpha_scale + N);
+  Ly.alpha = alpha; Ly.gamma = gamma; Ly.floor_ms = floor_ms;
+  Ly.g2c_idx.assign(g2c_index, g2c_index + N + 1);
+  int nc = g2c_index[N];
+  Ly.g2c_i.resize(nc);
+  Ly.g2c_j.resize(nc);
+  for (int q = 0; q < nc; ++q) {
+    Ly.g2c_i[q] = g2c[2 * q] - 1;
+    Ly.g2c_j[q] = g2c[2 * q + 1] - 1;
+  }
+  if (hx_index) {
+    Ly.hx_idx.assign(hx_index, hx_index + N + 1);
+    int nnz = hx_index[N];
+    Ly.hx_nbr.resize(nnz);
+    for (int q = 0; q < nnz; ++q) Ly.hx_nbr[q] = hx_grain[q] - 1;
+    Ly.hx.assign(hx, hx + nnz);
+  } else {
+    Ly.hx_idx.clear(); Ly.hx_nbr.clear(); Ly.hx.clear();
+  }
+  for (int b = 0; b < 2; ++b) Ly.m[b].assign(3 * N, 0.0);
+  Ly.dm.assign(3 * N, 0.0);
+  Ly.h.assign(3 * N, 0.0);
+  Ly.hthm.assign(3 * N, 0.0);
+  Ly.hdemag.assign(3 * N, 0.0);
+  Ly.happ.assign(3 * N, 0.0);
+  return 0;
+}
+
+// side 0: upper (couples to layer l-1, uhx), side 1: lower (couples to layer l+1, lhx)
+int orc_upload_interlayer(void* h, int l, int side, const int* index, const int* grain,
+                          const double* coef) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  int N = Ly.N;
+  std::vector<int>& idx = side == 0 ? Ly.uhx_idx : Ly.lhx_idx;
+  std::vector<int>& nbr = side == 0 ? Ly.uhx_nbr : Ly.lhx_nbr;
+  std::vector<double>& cf = side == 0 ? Ly.uhx : Ly.lhx;
+  idx.assign(index, index + N + 1);
+  int nnz = index[N];
+  nbr.resize(nnz);
+  for (int q = 0; q < nnz; ++q) nbr[q] = grain[q] - 1;
+  cf.assign(coef, coef + nnz);
+  return 0;
+}
+
+int orc_set_uniform_field(void* h, int l, const double* dir, double t_start, double t_end,
+                          double s_start, double s_end, double scale) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  for (int a = 0; a < 3; ++a) Ly.hdir[a] = dir[a];
+  Ly.t_start = t_start; Ly.t_end = t_end; Ly.s_start = s_start; Ly.s_end = s_end; Ly.scale = scale;
+  // set_fld :309-312 folds a constant scale
+  if (Ly.s_start == Ly.s_end) {
+    Ly.scale *= Ly.s_start;
+    Ly.s_start = 1.0; Ly.s_end = 1.0;
+  }
+  return 0;
+}
+
+// rng_mode 0: MT19937 per layer seeded like input.f90:190-206 / field.f90:712-733;
+// rng_mode 1: Philox stream (seed) shared with the GPU path.
+int orc_set_thermal(void* h, int l, int on, double temperature, int rng_mode, long long seed) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.thermal = on != 0;
+  Ly.temperature = temperature;
+  s->rng_mode = rng_mode;
+  if (rng_mode == 0) mt_create(&Ly.rng, (int)seed);
+  else s->seed = (uint64_t)seed;
+  return 0;
+}
+
+int orc_set_state(void* h, int l, const double* m) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  std::memcpy(Ly.m[s->in].data(), m, sizeof(double) * 3 * Ly.N);
+  std::memcpy(Ly.m[1 - s->in].data(), m, sizeof(double) * 3 * Ly.N);
+  return 0;
+}
+
+int orc_get_state(void* h, int l, double* m) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  std::memcpy(m, s->L[l].m[s->in].data(), sizeof(double) * 3 * s->L[l].N);
+  return 0;
+}
+
+int orc_get_field(void* h, int l, double* out) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  std::memcpy(out, s->L[l].h.data(), sizeof(double) * 3 * s->L[l].N);
+  return 0;
+}
+
+int orc_get_demag(void* h, int l, double* out) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  std::memcpy(out, s->L[l].hdemag.data(), sizeof(double) * 3 * s->L[l].N);
+  return 0;
+}
+
+void orc_set_time(void* h, double t, long long step) {
+  Sim* s = static_cast<Sim*>(h);
+  s->t = t;
+  s->step = step;
+}
+
+// evaluate the (non-thermal) field of the current state at time t (get_field)
+void orc_eval_field(void* h, double t) {
+  Sim* s = static_cast<Sim*>(h);
+  double e;
+  get_field(s, t, s->in, &e);
+}
+
+// nsteps fixed-dt steps of llg type (-3 Heun, 2 Boris, -2 Boris midpoint).
+// stats_out: mirrors mrm_gpu_stats (see include/mrm_gpu.h) for the last step.
+// traj: optional [nsteps][nl][3] vol-weighted <m> after each step.
+int orc_step(void* h, int nsteps, double dt, int type, double* stats_out, double* traj) {
+  Sim* s = static_cast<Sim*>(h);
+  if (!(type == -3 || type == 2 || type == -2)) return 2;
+  for (int k = 0; k < nsteps; ++k) {
+    heun_or_boris_step(s, dt, type);
+    if (traj)
+      for (int l = 0; l < s->nl; ++l)
+        for (int a = 0; a < 3; ++a) traj[((size_t)k * s->nl + l) * 3 + a] = s->last.mave_l[l][a];
+  }
+  if (stats_out) std::memcpy(stats_out, &s->last, sizeof(Stats));
+  return 0;
+}
+
+int orc_stats_size(void) { return (int)sizeof(Stats); }
+
+}  // extern "C"

@@ -1,0 +1,270 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this
+module.  It loads oracle/liboracle.so (built by oracle/Makefile) and mirrors
+the GPU host API closely enough that a parity test can drive both with the
+same media and schedule.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+MAX_LAYERS = 8
+STATS_DTYPE = np.dtype([
+    ("t", "f8"), ("step", "i8"),
+    ("mave", "f8", 3), ("mvar", "f8", 3), ("have", "f8", 3),
+    ("errmx", "f8"), ("errmx1", "f8"), ("mmag", "f8"), ("energy", "f8"),
+    ("mave_l", "f8", (MAX_LAYERS, 3)), ("mvar_l", "f8", (MAX_LAYERS, 3)),
+    ("have_l", "f8", (MAX_LAYERS, 3)), ("mms_l", "f8", (MAX_LAYERS, 3)),
+    ("vol_l", "f8", MAX_LAYERS), ("msvol_l", "f8", MAX_LAYERS), ("nup_l", "i8", MAX_LAYERS),
+])
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "liboracle.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        d, i, u64, vp = C.c_double, C.c_int, C.c_uint64, C.c_void_p
+        P = C.POINTER
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [i, i, i, i, i, d, d, P(d), P(d), d, d, d, d, i]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_build_tensor.argtypes = [vp, P(d)]
+        L.orc_set_tensor.argtypes = [vp, P(d)]
+        L.orc_upload_layer.argtypes = [vp, i, i, P(d), P(d), P(d), P(d), P(d), P(d), P(d), d, d, d,
+                                       P(i), P(i), P(i), P(i), P(d)]
+        L.orc_upload_interlayer.argtypes = [vp, i, i, P(i), P(i), P(d)]
+        L.orc_set_uniform_field.argtypes = [vp, i, P(d), d, d, d, d, d]
+        L.orc_set_thermal.argtypes = [vp, i, i, d, i, C.c_longlong]
+        L.orc_set_state.argtypes = [vp, i, P(d)]
+        L.orc_get_state.argtypes = [vp, i, P(d)]
+        L.orc_get_field.argtypes = [vp, i, P(d)]
+        L.orc_get_demag.argtypes = [vp, i, P(d)]
+        L.orc_set_time.argtypes = [vp, d, C.c_longlong]
+        L.orc_eval_field.argtypes = [vp, d]
+        L.orc_step.argtypes = [vp, i, d, i, vp, vp]
+        L.orc_mt_u32.argtypes = [i, i, P(C.c_uint32)]
+        L.orc_mt_state.argtypes = [i, P(C.c_uint32)]
+        L.orc_mt_normals.argtypes = [i, i, P(d)]
+        L.orc_philox4x64.argtypes = [P(u64), P(u64), P(u64)]
+        L.orc_philox_normal3.argtypes = [u64, u64, u64, u64, P(d)]
+        L.orc_volume_averaged_n.argtypes = [d] * 9 + [P(d)]
+        L.orc_calculate_tensor.argtypes = [i, i, i, d, d, P(d), P(d), i, i, d, d, d, d, P(d)]
+        L.orc_fft_r2c.argtypes = [i, i, P(d), P(d)]
+        L.orc_fft_c2r.argtypes = [i, i, P(d), P(d)]
+        L.orc_demag_direct.argtypes = [i, i, i, P(d), P(d), i, P(i), i, P(d)]
+        L.orc_set_threads.argtypes = [i]
+        L.orc_get_threads.restype = i
+        L.orc_stats_size.restype = i
+        assert L.orc_stats_size() == STATS_DTYPE.itemsize, "Stats layout mismatch"
+        _LIB = L
+    return _LIB
+
+
+def _p(a, ct=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---------------- probes ----------------
+def mt_u32(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.uint32)
+    lib().orc_mt_u32(seed, n, _p(out, C.c_uint32))
+    return out
+
+
+def mt_state(seed: int) -> np.ndarray:
+    out = np.zeros(624, np.uint32)
+    lib().orc_mt_state(seed, _p(out, C.c_uint32))
+    return out
+
+
+def mt_normals(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    lib().orc_mt_normals(seed, n, _p(out))
+    return out
+
+
+def philox4x64(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, np.uint64)
+    k = np.ascontiguousarray(key, np.uint64)
+    out = np.zeros(4, np.uint64)
+    lib().orc_philox4x64(_p(c, C.c_uint64), _p(k, C.c_uint64), _p(out, C.c_uint64))
+    return out
+
+
+def philox_normal3(seed, stream, step, grain) -> np.ndarray:
+    out = np.zeros(3)
+    lib().orc_philox_normal3(seed, stream, step, grain, _p(out))
+    return out
+
+
+def volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo) -> np.ndarray:
+    n = np.zeros(9)
+    lib().orc_volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo, _p(n))
+    return n.reshape(3, 3)
+
+
+def calculate_tensor(nx, ny, dx, dy, dz, il_space, images, space_to_sul=0.0, sul_mu=1.0,
+                     head_mu=1.0, fly_height=0.0) -> np.ndarray:
+    """Real-space tensor, reference layout [ks][ko][9][ny][nx]."""
+    nl = len(dz)
+    out = np.zeros((nl, nl, 9, ny, nx))
+    dzv, ilv = f64(dz), f64(il_space)
+    lib().orc_calculate_tensor(nx, ny, nl, dx, dy, _p(dzv), _p(ilv), images, images, space_to_sul,
+                               sul_mu, head_mu, fly_height, _p(out))
+    return out
+
+
+def fft_r2c(r: np.ndarray) -> np.ndarray:
+    ny, nx = r.shape
+    r = f64(r)
+    c = np.zeros((ny, nx // 2 + 1), np.complex128)
+    lib().orc_fft_r2c(nx, ny, _p(r), c.ctypes.data_as(C.POINTER(C.c_double)))
+    return c
+
+
+def fft_c2r(c: np.ndarray, nx: int) -> np.ndarray:
+    ny = c.shape[0]
+    c = np.ascontiguousarray(c, np.complex128)
+    r = np.zeros((ny, nx))
+    lib().orc_fft_c2r(nx, ny, c.ctypes.data_as(C.POINTER(C.c_double)), _p(r))
+    return r
+
+
+def demag_direct(n2d: np.ndarray, mgrid: np.ndarray, obs_ij: np.ndarray, ko: int) -> np.ndarray:
+    """Direct FP64 convolution at observation cells; n2d [nl][nl][9][py][px], mgrid [nl][3][py][px]."""
+    nl, _, _, py, px = n2d.shape
+    n2d = f64(n2d)
+    mg = f64(mgrid)
+    obs = i32(obs_ij)
+    out = np.zeros((obs.shape[0], 3))
+    lib().orc_demag_direct(px, py, nl, _p(n2d), _p(mg), obs.shape[0], _p(obs, C.c_int), ko, _p(out))
+    return out
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+class OracleSim:
+    """CPU restatement driven like the GPU handle (mrm_b200.GpuSim)."""
+
+    def __init__(self, medium, demag: bool = True, rng_mode: int = 1, seed: int = 1,
+                 tensor: np.ndarray | None = None):
+        L = lib()
+        self.medium = medium
+        dz = f64(medium.dz)
+        il = f64(medium.il_space)
+        self.h = L.orc_create(medium.nx, medium.ny, medium.n_lay, medium.boundary, medium.images,
+                              medium.dx, medium.dy, _p(dz), _p(il), medium.space_to_sul,
+                              medium.sul_mu, medium.head_mu, medium.fly_height, 1 if demag else 0)
+        self._keep = []
+        for l, lay in enumerate(medium.layers):
+            arrs = [f64(lay.ms), f64(lay.vol), f64(lay.axis), f64(lay.hk), f64(lay.hk_scale),
+                    f64(lay.ms_scale), f64(lay.alpha_scale)]
+            g2ci, g2c = i32(lay.g2c_index), i32(lay.g2c)
+            if lay.hx_index is not None:
+                hxi, hxg, hx = i32(lay.hx_index), i32(lay.hx_grain), f64(lay.hx)
+                hxa = (_p(hxi, C.c_int), _p(hxg, C.c_int), _p(hx))
+            else:
+                hxa = (None, None, None)
+            rc = L.orc_upload_layer(self.h, l, lay.N, *[_p(a) for a in arrs], lay.alpha, lay.gamma,
+                                    lay.floor_ms, _p(g2ci, C.c_int), _p(g2c, C.c_int), *hxa)
+            assert rc == 0
+            d = f64(lay.hdir)
+            L.orc_set_uniform_field(self.h, l, _p(d), lay.t_start, lay.t_end, lay.s_start,
+                                    lay.s_end, lay.scale)
+            L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
+        for l, lay in enumerate(medium.layers):
+            for side, cpl in ((0, lay.uhx), (1, lay.lhx)):
+                if cpl is not None:
+                    idx, gr, cf = i32(cpl[0]), i32(cpl[1]), f64(cpl[2])
+                    L.orc_upload_interlayer(self.h, l, side, _p(idx, C.c_int), _p(gr, C.c_int), _p(cf))
+        px = medium.nx * (2 if medium.boundary == 1 else 1)
+        py = medium.ny * (2 if medium.boundary == 1 else 1)
+        self.px, self.py = px, py
+        if demag:
+            if tensor is None:
+                self.n2d = np.zeros((medium.n_lay, medium.n_lay, 9, py, px))
+                L.orc_build_tensor(self.h, _p(self.n2d))
+            else:
+                self.n2d = f64(tensor)
+                L.orc_set_tensor(self.h, _p(self.n2d))
+        if medium.m0 is not None:
+            for l, m in enumerate(medium.m0):
+                self.set_state(l, m)
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, layer: int, m: np.ndarray):
+        mm = f64(m)
+        lib().orc_set_state(self.h, layer, _p(mm))
+
+    def get_state(self, layer: int) -> np.ndarray:
+        n = self.medium.layers[layer].N
+        out = np.zeros((n, 3))
+        lib().orc_get_state(self.h, layer, _p(out))
+        return out
+
+    def get_field(self, layer: int) -> np.ndarray:
+        n = self.medium.layers[layer].N
+        out = np.zeros((n, 3))
+        lib().orc_get_field(self.h, layer, _p(out))
+        return out
+
+    def get_demag(self, layer: int) -> np.ndarray:
+        n = self.medium.layers[layer].N
+        out = np.zeros((n, 3))
+        lib().orc_get_demag(self.h, layer, _p(out))
+        return out
+
+    def set_time(self, t: float, step: int = 0):
+        lib().orc_set_time(self.h, t, step)
+
+    def eval_field(self, t: float):
+        lib().orc_eval_field(self.h, t)
+
+    def step(self, nsteps: int, dt: float, llg_type: int = -3, traj: bool = False):
+        st = np.zeros(1, STATS_DTYPE)
+        tr = np.zeros((nsteps, self.medium.n_lay, 3)) if traj else None
+        rc = lib().orc_step(self.h, nsteps, dt, llg_type, st.ctypes.data,
+                            tr.ctypes.data if traj else None)
+        if rc != 0:
+            raise RuntimeError(f"orc_step failed rc={rc}")
+        return (st[0], tr) if traj else st[0]
