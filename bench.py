@@ -192,13 +192,19 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global HEUN_PER_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--heun", type=int, default=HEUN_PER_STEP,
+                    help="Heun steps per bench step (profiling runs use a small value)")
+    ap.add_argument("--timing-only", action="store_true",
+                    help="skip the e2e and per-kernel legs (profiling runs)")
     args = ap.parse_args()
+    HEUN_PER_STEP = args.heun
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -261,6 +267,14 @@ def main():
         dev_ms = float(tt.item())
     heun_total = HEUN_PER_STEP * args.steps
     value = world * n * heun_total / (dev_ms * 1e-3)
+
+    if args.timing_only:
+        if rank == 0:
+            print(json.dumps({"timing_only": True, "value": value, "ms_per_step": dev_ms / args.steps}))
+        sim.close()
+        if dist:
+            dist.destroy_process_group()
+        return
 
     # end-to-end through the C ABI with host buffers: upload m, step, read stats + m
     m_host = torch.from_numpy(np.ascontiguousarray(med.m0[0])).pin_memory()
