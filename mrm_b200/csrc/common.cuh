@@ -60,6 +60,9 @@ struct LayerDev {
   const int* lidx;  // interlayer: couples to layer+1
   const int* lnbr;
   const R* lcoef;
+  const V4<R>* xst;  // lattice form of the intralayer exchange: coef of (j-1, i-1, i+1, j+1)
+  const R* ucol;     // columnar form of the interlayer coupling (grain n <-> grain n)
+  const R* lcol;
   double hdir[3];
   double t_start, t_end, s_start, s_end, scale;
   double temperature;
@@ -84,7 +87,8 @@ struct RunDev {
   int active;
   int row_task0, nrow_tasks;  // range of this run's row tasks (stats partials)
   Cx<R>* spec;             // [nl][3][ny][px/2+1] half spectra of M (forward) / H (inverse)
-  const R* tens;           // [px/2+1][nl*nl][ncomp][py/2+1] tensor spectrum (real or imag part)
+  const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][py/2+1] reals,
+                           // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];
 };
 

@@ -2,14 +2,21 @@
 //
 // Replaces the FFTW r2c/c2r plans of src/fftw.f90:37-93 (unnormalised,
 // forward sign -1).  A batch of `nb` complex sequences of length n = 2^lgn,
-// sequence b at buf + b*stride, is transformed with radix-8 passes and one
-// final radix-4 or radix-2 pass (Stockham autosort: natural-order output,
-// ping-pong between two shared buffers, one __syncthreads per pass).
-// Twiddles come from one FP64-accurate table of e^{-2 pi i k / 4096}.
+// sequence b at buf + b*stride, is transformed with radix-16 passes and one
+// radix-8/4/2 pass for the remainder (Stockham autosort: natural-order
+// output, ping-pong between two shared buffers, one __syncthreads per pass).
+// Intermediate passes use a padded layout (one spare slot per 16 elements)
+// so the stride-R stores of the early passes hit distinct banks; the input of
+// the first pass and the output of the last pass are unpadded.  `stride`
+// must be >= fft_stride(n).  Twiddles come from one FP64-accurate table of
+// e^{-2 pi i k / 4096}.
 #pragma once
 #include "common.cuh"
 
 namespace mrm {
+
+MRM_HD int fft_stride(int n) { return n + (n >> 4) + 1; }
+MRM_D int padi(int i) { return i + (i >> 4); }
 
 template <typename R, int S>
 MRM_D void dft2(Cx<R>* v) {
@@ -37,7 +44,7 @@ MRM_D void dft8(Cx<R>* v) {
   dft4<R, S>(o0, o1, o2, o3);
   const R h = (R)0.70710678118654752440084436210485;
   // w8^k = e^{S*2*pi*i*k/8}
-  Cx<R> w1 = {h, (R)S * h}, w3 = {-h, (R)S * h};
+  const Cx<R> w1 = {h, (R)S * h}, w3 = {-h, (R)S * h};
   o1 = cmul(o1, w1);
   o2 = cmul_i(o2, (R)S);
   o3 = cmul(o3, w3);
@@ -51,9 +58,46 @@ MRM_D void dft8(Cx<R>* v) {
   v[7] = csub(e3, o3);
 }
 
+// 16-point DFT as 4 x 4 (radix-4 over stride 4, twiddles w16^(k1 n2), radix-4)
+template <typename R, int S>
+MRM_D void dft16(Cx<R>* v) {
+  const R c1 = (R)0.92387953251128675612818318939679;  // cos(pi/8)
+  const R s1 = (R)0.38268343236508977172845998403040;  // sin(pi/8)
+  const R h = (R)0.70710678118654752440084436210485;
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4<R, S>(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+  // after this, v[n2 + 4*k1] holds the k1-th output of column n2; twiddle w16^(k1*n2)
+  const Cx<R> w1 = {c1, (R)S * s1}, w2 = {h, (R)S * h}, w3 = {s1, (R)S * c1};
+  const Cx<R> w6 = {-h, (R)S * h}, w9 = {-c1, (R)S * (-s1)};
+  // k1=1: n2=1..3 -> w^1, w^2, w^3 ; k1=2 -> w^2, w^4, w^6 ; k1=3 -> w^3, w^6, w^9
+  v[5] = cmul(v[5], w1);
+  v[6] = cmul(v[6], w2);
+  v[7] = cmul(v[7], w3);
+  v[9] = cmul(v[9], w2);
+  v[10] = cmul_i(v[10], (R)S);
+  v[11] = cmul(v[11], w6);
+  v[13] = cmul(v[13], w3);
+  v[14] = cmul(v[14], w6);
+  v[15] = cmul(v[15], w9);
+  Cx<R> t[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    Cx<R> a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
+    dft4<R, S>(a0, a1, a2, a3);
+    // output index k = k1 + 4*k2
+    t[k1] = a0;
+    t[k1 + 4] = a1;
+    t[k1 + 8] = a2;
+    t[k1 + 12] = a3;
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = t[k];
+}
+
+// One Stockham pass.  PIN / POUT: input / output use the padded layout.
 template <typename R, int RADIX, int LGR, int S>
 MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, int lgn, int nb,
-                         int stride, int lgNs, const Cx<R>* __restrict__ tw) {
+                         int stride, int lgNs, bool pin, bool pout, const Cx<R>* __restrict__ tw) {
   const int lgnR = lgn - LGR;
   const int nR = 1 << lgnR;
   const int Ns = 1 << lgNs;
@@ -64,7 +108,10 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
     Cx<R>* dst = out + b * stride;
     Cx<R> v[RADIX];
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) v[r] = src[j + r * nR];
+    for (int r = 0; r < RADIX; ++r) {
+      const int i = j + r * nR;
+      v[r] = src[pin ? padi(i) : i];
+    }
     const int k = j & (Ns - 1);
     if (lgNs > 0) {
       const int sh = kTwLog - lgNs - LGR;
@@ -75,36 +122,46 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
         v[r] = cmul(v[r], w);
       }
     }
-    if (RADIX == 8) dft8<R, S>(v);
+    if (RADIX == 16) dft16<R, S>(v);
+    else if (RADIX == 8) dft8<R, S>(v);
     else if (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
     else dft2<R, S>(v);
     const int idxD = ((j >> lgNs) << (lgNs + LGR)) + k;
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) dst[idxD + r * Ns] = v[r];
+    for (int r = 0; r < RADIX; ++r) {
+      const int i = idxD + r * Ns;
+      dst[pout ? padi(i) : i] = v[r];
+    }
   }
 }
 
-// Transforms nb sequences held in `a`; `b` is scratch of the same size.
-// Returns the buffer that holds the result.  The caller must __syncthreads()
-// before the call (data in `a` complete); on return the result is complete.
+// Transforms nb sequences held (unpadded) in `a`; `b` is scratch of the same
+// size.  Returns the buffer holding the (unpadded) result.  The caller must
+// __syncthreads() before the call; on return the result is complete.
 template <typename R, int S>
 MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
                        const Cx<R>* __restrict__ tw) {
   int lgNs = 0;
   int rem = lgn;
-  while (rem >= 3) {
-    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, tw);
+  // pass list: radix-16 while >= 4 bits remain, then one 8/4/2 pass
+  const int n16 = rem >> 2;
+  const int tail = rem & 3;
+  const int npass = n16 + (tail ? 1 : 0);
+  int p = 0;
+  for (int q = 0; q < n16; ++q, ++p) {
+    stockham_pass<R, 16, 4, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw);
     __syncthreads();
     Cx<R>* t = a; a = b; b = t;
-    lgNs += 3;
-    rem -= 3;
+    lgNs += 4;
   }
-  if (rem == 2) {
-    stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, tw);
-    __syncthreads();
-    Cx<R>* t = a; a = b; b = t;
-  } else if (rem == 1) {
-    stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, tw);
+  if (tail == 3) {
+    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+  } else if (tail == 2) {
+    stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+  } else if (tail == 1) {
+    stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+  }
+  if (tail) {
     __syncthreads();
     Cx<R>* t = a; a = b; b = t;
   }

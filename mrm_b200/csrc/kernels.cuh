@@ -13,6 +13,11 @@
 //   col
 // The spectrum buffer always holds H^(m) of the state it follows, so a step
 // starts from it without a separate demag pass.
+//
+// Latency layout: every per-grain global load (state, parameters, lattice
+// neighbours, columnar interlayer partner) is issued at the top of the row
+// kernel, before the inverse FFT, so its latency overlaps the shared-memory
+// passes; the column kernel batches its strided loads the same way.
 #pragma once
 #include "common.cuh"
 #include "fft.cuh"
@@ -54,41 +59,52 @@ MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
   }
 }
 
-// block reduction of the stats record (sums except [kMaxTq], [kMaxD2] which are maxima)
+// stats record slots (sums except the two maxima)
 constexpr int kSlotV = 0, kSlotM = 1, kSlotM2 = 4, kSlotH = 7, kSlotWM = 10, kSlotW = 13,
               kSlotNup = 14, kSlotMaxTq = 15, kSlotMaxD2 = 16, kSlotMmag = 17, kSlotE = 18;
+MRM_HD constexpr bool slot_is_max(int s) { return s == kSlotMaxTq || s == kSlotMaxD2; }
 
 MRM_D void block_reduce_record(double* rec, double* sred /* [32][kNPart] */, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int s = 0; s < kNPart; ++s) {
     double v = rec[s];
-    const bool mx = (s == kSlotMaxTq || s == kSlotMaxD2);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       double w = __shfl_xor_sync(0xffffffffu, v, o);
-      v = mx ? fmax(v, w) : v + w;
+      v = slot_is_max(s) ? fmax(v, w) : v + w;
     }
     if (lane == 0) sred[warp * kNPart + s] = v;
   }
   __syncthreads();
   if (threadIdx.x < kNPart) {
     const int s = threadIdx.x;
-    const bool mx = (s == kSlotMaxTq || s == kSlotMaxD2);
     double v = sred[s];
-    for (int w = 1; w < nw; ++w) v = mx ? fmax(v, sred[w * kNPart + s]) : v + sred[w * kNPart + s];
+    for (int w = 1; w < nw; ++w) v = slot_is_max(s) ? fmax(v, sred[w * kNPart + s]) : v + sred[w * kNPart + s];
     out[s] = v;
   }
 }
 
+// Per-grain inputs gathered at the top of the row kernel.
+template <typename R>
+struct GrainIn {
+  V4<R> mf;      // state the field is evaluated on (m_n, or m* in the corrector)
+  V4<R> pa, pb;  // parameters
+  V4<R> cst;     // lattice exchange coefficients (j-1, i-1, i+1, j+1)
+  V4<R> nb[4];   // lattice neighbours
+  V4<R> dm, m0;  // corrector: predictor increment and m_n
+  V4<R> vu, vl;  // columnar interlayer partners
+  R cu, cl;
+};
+
 template <int STAGE, bool STATS>
 __host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STATS) ? 32 * kNPart : 1; }
 
-template <typename R, int STAGE, bool STATS>
-__global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ runs,
-                                                  const Task* __restrict__ tasks,
-                                                  const Cx<R>* __restrict__ tw, int istep,
-                                                  int flags, double* __restrict__ part) {
+template <typename R, int STAGE, bool STATS, int GPT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict__ runs,
+                                                    const Task* __restrict__ tasks,
+                                                    const Cx<R>* __restrict__ tw, int istep,
+                                                    int flags, double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
@@ -99,34 +115,97 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
   const int l = tk.y, row0 = tk.z, nrows = tk.w;
   const int nx = rd.nx, ny = rd.ny;
   const int lgM = rd.lgpx - 1, M = 1 << lgM, ph = M + 1;
+  const int cs = fft_stride(M);  // complex stride of one sequence in shared memory
   const int nseq = nrows * 3;
+  const int ngr = nrows * nx;
   const LayerDev<R>& L = rd.L[l];
   const bool demag = rd.demag != 0;
+  constexpr bool stats = (STAGE == kCorr) && STATS;
 
   Cx<R>* bufA = reinterpret_cast<Cx<R>*>(smem_raw);
-  Cx<R>* bufB = bufA + nseq * M;
+  Cx<R>* bufB = bufA + nseq * cs;
   __shared__ double sred[stats_slots<STAGE, STATS>()];
 
+  // ---------------- prefetch per-grain inputs ----------------
+  const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
+  const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
+  const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
+  const bool stencil = L.xst != nullptr;
+  GrainIn<R> g[GPT];
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    const int idx = threadIdx.x + q * BLOCK;
+    if (idx >= ngr) continue;
+    const int row = idx / nx, i = idx - row * nx, j = row0 + row;
+    const int n = j * nx + i;
+    g[q].pb = L.pb[n];
+    if (STAGE == kInit) {
+      g[q].mf = L.m[n];
+      continue;
+    }
+    g[q].mf = mfield[n];
+    g[q].pa = L.pa[n];
+    if (stencil) {
+      g[q].cst = L.xst[n];
+      const int jm = (j == 0 ? ny - 1 : j - 1), jp = (j == ny - 1 ? 0 : j + 1);
+      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
+      g[q].nb[0] = mfield[jm * nx + i];
+      g[q].nb[1] = mfield[j * nx + im];
+      g[q].nb[2] = mfield[j * nx + ip];
+      g[q].nb[3] = mfield[jp * nx + i];
+    }
+    if (STAGE == kCorr) {
+      g[q].dm = L.dm[n];
+      g[q].m0 = L.m[n];
+    }
+    if (L.ucol && Lu) {
+      g[q].cu = L.ucol[n];
+      g[q].vu = ((STAGE == kCorr) ? Lu->mp : Lu->m)[n];
+    }
+    if (L.lcol && Ll) {
+      g[q].cl = L.lcol[n];
+      g[q].vl = ((STAGE == kCorr) ? Ll->mp : Ll->m)[n];
+    }
+  }
+
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
-  Cx<R>* Z = bufA;  // holds x[2n] + i x[2n+1] of each sequence after the inverse
+  Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
   if (STAGE != kInit && demag) {
-    for (int idx = threadIdx.x; idx < nseq * M; idx += blockDim.x) {
-      const int s = idx >> lgM, k = idx & (M - 1);
-      const int row = s / 3, comp = s - 3 * row;
-      const Cx<R>* X = rd.spec + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
-      Cx<R> xk = X[k], xmk = X[M - k];
-      if (k == 0) { xk.y = 0; xmk.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
-      const Cx<R> e = cadd(xk, cconj(xmk));
-      const Cx<R> o = csub(xk, cconj(xmk));
-      const Cx<R> w = cconj(twiddle(tw, k, rd.lgpx));  // e^{+2 pi i k / px}
-      bufA[s * M + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
+    const int tot = nseq * M;
+    for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
+      Cx<R> xk[4], xm[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * BLOCK;
+        if (idx < tot) {
+          const int s = idx >> lgM, k = idx & (M - 1);
+          const int row = s / 3, comp = s - 3 * row;
+          const Cx<R>* X = rd.spec + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
+          xk[u] = X[k];
+          xm[u] = X[M - k];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * BLOCK;
+        if (idx < tot) {
+          const int s = idx >> lgM, k = idx & (M - 1);
+          Cx<R> a = xk[u], b = xm[u];
+          if (k == 0) { a.y = 0; b.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
+          const Cx<R> e = cadd(a, cconj(b));
+          const Cx<R> o = csub(a, cconj(b));
+          const Cx<R> w = cconj(twiddle(tw, k, rd.lgpx));  // e^{+2 pi i k / px}
+          bufA[s * cs + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
+        }
+      }
     }
     __syncthreads();
-    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, M, tw);
+    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, cs, tw);
   }
   Cx<R>* W = (Z == bufA) ? bufB : bufA;  // real outputs of this stage (forward input)
   const R* hdr = reinterpret_cast<const R*>(Z);
   R* outr = reinterpret_cast<R*>(W);
+  const int rs = 2 * cs;  // real stride of one sequence
 
   // ---------------- per-grain field + integrator stage ----------------
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
@@ -137,40 +216,37 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
   const R gamma = (R)L.gamma;
   const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
   const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
-  constexpr bool stats = (STAGE == kCorr) && STATS;
   const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
 
   double rec[stats ? kNPart : 1];
 #pragma unroll
   for (int s = 0; s < (stats ? kNPart : 1); ++s) rec[s] = 0.0;
 
-  const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;  // state the field is evaluated on
-  const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
-  const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
-
-  const int two_m = 2 * M;
-  for (int idx = threadIdx.x; idx < nrows * nx; idx += blockDim.x) {
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    const int idx = threadIdx.x + q * BLOCK;
+    if (idx >= ngr) continue;
     const int row = idx / nx, i = idx - row * nx;
     const int n = (row0 + row) * nx + i;
-    const V4<R> pb = L.pb[n];
-    const R mse = pb.x;  // Ms * ms_scale
+    const GrainIn<R>& G = g[q];
+    const R mse = G.pb.x;  // Ms * ms_scale
     if (STAGE == kInit) {
-      const V4<R> m = L.m[n];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) outr[(row * 3 + c) * two_m + i] = mse * (c == 0 ? m.x : c == 1 ? m.y : m.z);
+      outr[(row * 3 + 0) * rs + i] = mse * G.mf.x;
+      outr[(row * 3 + 1) * rs + i] = mse * G.mf.y;
+      outr[(row * 3 + 2) * rs + i] = mse * G.mf.z;
       continue;
     }
-    const V4<R> mf = mfield[n];
+    const V4<R> mf = G.mf;
     R hdx = 0, hdy = 0, hdz = 0;
     if (demag) {
-      hdx = hdr[(row * 3 + 0) * two_m + i];
-      hdy = hdr[(row * 3 + 1) * two_m + i];
-      hdz = hdr[(row * 3 + 2) * two_m + i];
+      hdx = hdr[(row * 3 + 0) * rs + i];
+      hdy = hdr[(row * 3 + 1) * rs + i];
+      hdz = hdr[(row * 3 + 2) * rs + i];
     }
     // h = h_app + h_demag + H_uni + H_ex (+ interlayer)   (field.f90:201,211-220)
     R hx = hax + hdx, hy = hay + hdy, hz = haz + hdz;
-    const V4<R> pa = L.pa[n];
-    R e_k = 0;
+    const V4<R> pa = G.pa, pb = G.pb;
+    R e_k;
     {
       // get_uni_hk (field.f90:366-375); pa.w = Hk1*hk_scale, pb.y = Hk2*hk_scale
       const R hks = mf.x * pa.x + mf.y * pa.y + mf.z * pa.z;
@@ -182,16 +258,28 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
       e_k = (R)0.5 * yy * (pa.w + (R)0.5 * pb.y * yy) * mse;
     }
     R ex = 0, ey = 0, ez = 0;
-    if (L.xidx) csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
+    if (stencil) {
+      ex = G.cst.x * G.nb[0].x + G.cst.y * G.nb[1].x + G.cst.z * G.nb[2].x + G.cst.w * G.nb[3].x;
+      ey = G.cst.x * G.nb[0].y + G.cst.y * G.nb[1].y + G.cst.z * G.nb[2].y + G.cst.w * G.nb[3].y;
+      ez = G.cst.x * G.nb[0].z + G.cst.y * G.nb[1].z + G.cst.z * G.nb[2].z + G.cst.w * G.nb[3].z;
+    } else if (L.xidx) {
+      csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
+    }
     R vx = 0, vy = 0, vz = 0;
-    if (L.uidx && Lu) csr_sum<R>(L.uidx, L.unbr, L.ucoef, (STAGE == kCorr) ? Lu->mp : Lu->m, n, vx, vy, vz);
-    if (L.lidx && Ll) csr_sum<R>(L.lidx, L.lnbr, L.lcoef, (STAGE == kCorr) ? Ll->mp : Ll->m, n, vx, vy, vz);
+    if (L.ucol && Lu) {
+      vx += G.cu * G.vu.x; vy += G.cu * G.vu.y; vz += G.cu * G.vu.z;
+    } else if (L.uidx && Lu) {
+      csr_sum<R>(L.uidx, L.unbr, L.ucoef, (STAGE == kCorr) ? Lu->mp : Lu->m, n, vx, vy, vz);
+    }
+    if (L.lcol && Ll) {
+      vx += G.cl * G.vl.x; vy += G.cl * G.vl.y; vz += G.cl * G.vl.z;
+    } else if (L.lidx && Ll) {
+      csr_sum<R>(L.lidx, L.lnbr, L.lcoef, (STAGE == kCorr) ? Ll->mp : Ll->m, n, vx, vy, vz);
+    }
     hx += ex + vx;
     hy += ey + vy;
     hz += ez + vz;
-    if (store_field) {
-      L.hf[n] = V4<R>{hx, hy, hz, (R)0};
-    }
+    if (store_field) L.hf[n] = V4<R>{hx, hy, hz, (R)0};
     if (STAGE == kEval) {
       L.hd[n] = V4<R>{hdx, hdy, hdz, (R)0};
       continue;
@@ -200,13 +288,13 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
     // thermal field / sqrt(dt) (llg.f90:1083), Philox normals regenerated in the corrector
     R htx = 0, hty = 0, htz = 0;
     if (thermal) {
-      R g[3];
+      R gn[3];
       thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step,
-                      (unsigned long long)n, g);
+                      (unsigned long long)n, gn);
       const R s = pb.w * tfac;
-      htx = s * g[0];
-      hty = s * g[1];
-      htz = s * g[2];
+      htx = s * gn[0];
+      hty = s * gn[1];
+      htz = s * gn[2];
     }
     const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
     V4<R> mn;
@@ -226,11 +314,10 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
         L.dm[n] = V4<R>{dx, dy, dz, (R)0};
         m0 = mf;
       } else {
-        const V4<R> d1 = L.dm[n];
-        dx = (R)0.5 * (dx + d1.x);
-        dy = (R)0.5 * (dy + d1.y);
-        dz = (R)0.5 * (dz + d1.z);
-        m0 = L.m[n];
+        dx = (R)0.5 * (dx + G.dm.x);
+        dy = (R)0.5 * (dy + G.dm.y);
+        dz = (R)0.5 * (dz + G.dm.z);
+        m0 = G.m0;
       }
       mn.x = m0.x + dx;
       mn.y = m0.y + dy;
@@ -248,15 +335,15 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
       if (y > (R)0) {
         mn.x = hx / y; mn.y = hy / y; mn.z = hz / y;
       } else {
-        mn = (STAGE == kCorr) ? L.m[n] : mf;
+        mn = (STAGE == kCorr) ? G.m0 : mf;
       }
     }
     mn.w = (R)0;
     if (STAGE == kPred) L.mp[n] = mn;
     else L.m[n] = mn;
-    outr[(row * 3 + 0) * two_m + i] = mse * mn.x;
-    outr[(row * 3 + 1) * two_m + i] = mse * mn.y;
-    outr[(row * 3 + 2) * two_m + i] = mse * mn.z;
+    outr[(row * 3 + 0) * rs + i] = mse * mn.x;
+    outr[(row * 3 + 1) * rs + i] = mse * mn.y;
+    outr[(row * 3 + 2) * rs + i] = mse * mn.z;
 
     if constexpr (stats) {
       const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 0}
@@ -277,8 +364,7 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
       rec[kSlotWM + 2] += w * mz;
       rec[kSlotW] += w;
       if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += 1.0;
-      const double ms2 = pv.z * pv.z;
-      rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / ms2);
+      rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / (pv.z * pv.z));
       rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
       rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
       // energy at the evaluated state (field.f90:200, :360, :374, :339)
@@ -295,35 +381,40 @@ __global__ void __launch_bounds__(256) row_kernel(const RunDev<R>* __restrict__ 
   if (STAGE == kEval || !demag) return;
 
   // ---------------- forward row transform of Ms*m -> spectrum rows ----------------
+  const int two_m = 2 * M;
   if (nx < two_m) {
     const int pad = two_m - nx;
-    for (int idx = threadIdx.x; idx < nseq * pad; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < nseq * pad; idx += BLOCK) {
       const int s = idx / pad, i = nx + (idx - s * pad);
-      outr[s * two_m + i] = (R)0;
+      outr[s * rs + i] = (R)0;
     }
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
-  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, M, tw);
-  for (int idx = threadIdx.x; idx < nseq * ph; idx += blockDim.x) {
+  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, cs, tw);
+  for (int idx = threadIdx.x; idx < nseq * ph; idx += BLOCK) {
     const int s = idx / ph, k = idx - s * ph;
     const int row = s / 3, comp = s - 3 * row;
-    const Cx<R> yk = Y[s * M + (k & (M - 1))];
-    const Cx<R> ymk = cconj(Y[s * M + ((M - k) & (M - 1))]);
+    const Cx<R> yk = Y[s * cs + (k & (M - 1))];
+    const Cx<R> ymk = cconj(Y[s * cs + ((M - k) & (M - 1))]);
     const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
     const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
     // X[k] = e - i w^k o,  w = e^{-2 pi i / px}
     const Cx<R> wo = cmul(twiddle(tw, k & (two_m - 1), rd.lgpx), o);
-    const Cx<R> xk = csub(e, cmul_i(wo, (R)1));
-    rd.spec[((size_t)(l * 3 + comp) * ny + row0 + row) * ph + k] = xk;
+    rd.spec[((size_t)(l * 3 + comp) * ny + row0 + row) * ph + k] = csub(e, cmul_i(wo, (R)1));
   }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) col_kernel(const RunDev<R>* __restrict__ runs,
-                                                  const Task* __restrict__ tasks,
-                                                  const Cx<R>* __restrict__ tw, int istep,
-                                                  int flags) {
+// Column kernel: per spectral column k, forward FFT along y of the 3*nl
+// half-spectra, H^_a = sum_b N^_ab M^_b, inverse FFT, written back in place.
+// PACKED: tensor stored as one real per (k, 0<=ky<=py/2) and component (the
+// parity of each component restores the rest); otherwise the full complex
+// tensor spectrum [k][pair][9][py] is used (FP64 runs).
+template <typename R, bool PACKED, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict__ runs,
+                                                    const Task* __restrict__ tasks,
+                                                    const Cx<R>* __restrict__ tw, int istep,
+                                                    int flags) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
@@ -332,62 +423,90 @@ __global__ void __launch_bounds__(256) col_kernel(const RunDev<R>* __restrict__ 
   const int k0 = tk.y, nc = tk.z;
   const int nl = rd.nl, ny = rd.ny, py = rd.py, lgpy = rd.lgpy;
   const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1;
+  const int cs = fft_stride(py);
   const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
   Cx<R>* A = reinterpret_cast<Cx<R>*>(smem_raw);
-  Cx<R>* B = A + nseq * py;
+  Cx<R>* B = A + nseq * cs;
 
-  // load columns (rows >= ny are the zero padding)
-  for (int idx = threadIdx.x; idx < nseq * py; idx += blockDim.x) {
-    const int c = idx % nc;
-    const int rest = idx / nc;
-    const int j = rest % py;
-    const int lc = rest / py;  // layer*3 + comp
-    Cx<R> v = {(R)0, (R)0};
-    if (j < ny) v = rd.spec[((size_t)lc * ny + j) * ph + k0 + c];
-    A[(c * nl * 3 + lc) * py + j] = v;
+  // batched strided loads of the columns (rows >= ny are the zero padding)
+  const int tot = nseq * py;
+  for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
+    Cx<R> v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * BLOCK;
+      v[u] = Cx<R>{(R)0, (R)0};
+      if (idx < tot) {
+        const int c = idx % nc, rest = idx / nc;
+        const int j = rest % py, lc = rest / py;
+        if (j < ny) v[u] = rd.spec[((size_t)lc * ny + j) * ph + k0 + c];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * BLOCK;
+      if (idx < tot) {
+        const int c = idx % nc, rest = idx / nc;
+        const int j = rest % py, lc = rest / py;
+        A[(c * nl * 3 + lc) * cs + j] = v[u];
+      }
+    }
   }
   __syncthreads();
-  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, py, tw);
+  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, cs, tw);
   Cx<R>* G = (F == A) ? B : A;
 
   // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
   const int npair = nl * nl;
-  for (int idx = threadIdx.x; idx < nc * py; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK) {
     const int c = idx / py, ky = idx - c * py;
-    const bool upper = ky > (py >> 1);
-    const int kyh = upper ? py - ky : ky;
-    const R* T = rd.tens + (size_t)(k0 + c) * npair * rd.ncomp * pyh;
     for (int ko = 0; ko < nl; ++ko) {
       Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
       for (int ks = 0; ks < nl; ++ks) {
-        const R* Tp = T + (size_t)(ks * nl + ko) * rd.ncomp * pyh;
         Cx<R> xm[3];
 #pragma unroll
-        for (int b = 0; b < 3; ++b) xm[b] = F[((c * nl + ks) * 3 + b) * py + ky];
+        for (int b = 0; b < 3; ++b) xm[b] = F[((c * nl + ks) * 3 + b) * cs + ky];
+        if constexpr (PACKED) {
+          const bool upper = ky > (py >> 1);
+          const int kyh = upper ? py - ky : ky;
+          const R* Tp = rd.tens + ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * pyh;
+          R tv[9];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+          for (int cc = 0; cc < 9; ++cc) tv[cc] = __ldg(Tp + cc * pyh + kyh);
 #pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const int cc = 3 * a + b;
-            R v = __ldg(Tp + cc * pyh + kyh);
-            if (((kOddMask >> cc) & 1) && upper) v = -v;
-            if ((kImagMask >> cc) & 1) h[a] = cadd(h[a], cmul_i(cscale(xm[b], v), (R)1));
-            else h[a] = cadd(h[a], cscale(xm[b], v));
-          }
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+              const int cc = 3 * a + b;
+              R v = tv[cc];
+              if (((kOddMask >> cc) & 1) && upper) v = -v;
+              if ((kImagMask >> cc) & 1) h[a] = cadd(h[a], cmul_i(cscale(xm[b], v), (R)1));
+              else h[a] = cadd(h[a], cscale(xm[b], v));
+            }
+        } else {
+          const Cx<R>* Tc = reinterpret_cast<const Cx<R>*>(rd.tens) +
+                            ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * py;
+          Cx<R> tv[9];
+#pragma unroll
+          for (int cc = 0; cc < 9; ++cc) tv[cc] = Tc[cc * py + ky];
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) h[a] = cadd(h[a], cmul(tv[3 * a + b], xm[b]));
+        }
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) G[((c * nl + ko) * 3 + a) * py + ky] = h[a];
+      for (int a = 0; a < 3; ++a) G[((c * nl + ko) * 3 + a) * cs + ky] = h[a];
     }
   }
   __syncthreads();
-  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, py, tw);
+  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, cs, tw);
 
-  for (int idx = threadIdx.x; idx < nseq * ny; idx += blockDim.x) {
-    const int c = idx % nc;
-    const int rest = idx / nc;
-    const int j = rest % ny;
-    const int lc = rest / ny;
-    rd.spec[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * py + j];
+  const int tot2 = nseq * ny;
+  for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
+    const int c = idx % nc, rest = idx / nc;
+    const int j = rest % ny, lc = rest / ny;
+    rd.spec[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
   }
 }
 
@@ -403,8 +522,7 @@ __global__ void advance_kernel(RunDev<R>* runs, int nruns, int k) {
   rd.step += (left < k) ? left : k;
 }
 
-// FP64 reduction of the per-task stats records of each run into mrm_gpu_stats
-// (layout mirrored by StatsDev), in a fixed order (deterministic).
+// mrm_gpu_stats layout
 struct StatsDev {
   double t;
   long long step;
@@ -415,53 +533,64 @@ struct StatsDev {
   long long nup_l[kMaxLayers];
 };
 
+// FP64 reduction of each run's per-task stats records into StatsDev; one
+// 256-thread block per run, fixed reduction order (deterministic).
 template <typename R>
-__global__ void finalize_stats_kernel(const RunDev<R>* __restrict__ runs, const Task* __restrict__ tasks,
-                                      const double* __restrict__ part, StatsDev* __restrict__ out,
-                                      int nruns) {
+__global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __restrict__ runs,
+                                                             const Task* __restrict__ tasks,
+                                                             const double* __restrict__ part,
+                                                             StatsDev* __restrict__ out, int nruns) {
+  __shared__ double sred[32 * kNPart];
+  __shared__ double acc[kMaxLayers][kNPart];
   const int r = blockIdx.x;
-  if (r >= nruns || threadIdx.x != 0) return;
+  if (r >= nruns) return;
   const RunDev<R>& rd = runs[r];
-  StatsDev& st = out[r];
   if (!rd.active) return;
-  double acc[kMaxLayers][kNPart];
-  for (int l = 0; l < kMaxLayers; ++l)
-    for (int s = 0; s < kNPart; ++s) acc[l][s] = 0.0;
-  for (int q = rd.row_task0; q < rd.row_task0 + rd.nrow_tasks; ++q) {
-    const int l = tasks[q].y;
-    const double* p = part + (size_t)q * kNPart;
-    for (int s = 0; s < kNPart; ++s)
-      acc[l][s] = (s == kSlotMaxTq || s == kSlotMaxD2) ? fmax(acc[l][s], p[s]) : acc[l][s] + p[s];
+  for (int l = 0; l < rd.nl; ++l) {
+    double rec[kNPart];
+#pragma unroll
+    for (int s = 0; s < kNPart; ++s) rec[s] = 0.0;
+    for (int q = rd.row_task0 + threadIdx.x; q < rd.row_task0 + rd.nrow_tasks; q += blockDim.x) {
+      if (tasks[q].y != l) continue;
+      const double* p = part + (size_t)q * kNPart;
+#pragma unroll
+      for (int s = 0; s < kNPart; ++s) rec[s] = slot_is_max(s) ? fmax(rec[s], p[s]) : rec[s] + p[s];
+    }
+    block_reduce_record(rec, sred, acc[l]);
+    __syncthreads();
   }
+  if (threadIdx.x != 0) return;
+  StatsDev& st = out[r];
   st.step = rd.step;
   st.t = rd.t_base + (double)(rd.step - rd.step_base) * rd.dt;
   double vt = 0, mt = 0, m1 = 0, mmag = 0, en = 0;
   for (int a = 0; a < 3; ++a) { st.mave[a] = 0; st.mvar[a] = 0; st.have[a] = 0; }
   for (int l = 0; l < rd.nl; ++l) vt += acc[l][kSlotV];
   for (int l = 0; l < kMaxLayers; ++l) {
-    const double V = acc[l][kSlotV];
+    const bool on = l < rd.nl;
+    const double V = on ? acc[l][kSlotV] : 0.0;
     for (int a = 0; a < 3; ++a) {
-      const double mean = (l < rd.nl && V > 0) ? acc[l][kSlotM + a] / V : 0.0;
+      const double mean = (on && V > 0) ? acc[l][kSlotM + a] / V : 0.0;
       st.mave_l[l][a] = mean;
-      st.mvar_l[l][a] = (l < rd.nl && V > 0) ? acc[l][kSlotM2 + a] / V - mean * mean : 0.0;
-      st.have_l[l][a] = (l < rd.nl && V > 0) ? acc[l][kSlotH + a] / V : 0.0;
-      const double W = acc[l][kSlotW];
-      st.mms_l[l][a] = acc[l][kSlotWM + a] * W / (W * W + 1e-300);
+      st.mvar_l[l][a] = (on && V > 0) ? acc[l][kSlotM2 + a] / V - mean * mean : 0.0;
+      st.have_l[l][a] = (on && V > 0) ? acc[l][kSlotH + a] / V : 0.0;
+      const double W = on ? acc[l][kSlotW] : 0.0;
+      st.mms_l[l][a] = on ? acc[l][kSlotWM + a] * W / (W * W + 1e-300) : 0.0;
     }
     st.vol_l[l] = V;
-    st.msvol_l[l] = acc[l][kSlotW];
-    st.nup_l[l] = (long long)acc[l][kSlotNup];
-    if (l < rd.nl && V > 0) {
+    st.msvol_l[l] = on ? acc[l][kSlotW] : 0.0;
+    st.nup_l[l] = on ? (long long)acc[l][kSlotNup] : 0;
+    if (on && V > 0) {
       for (int a = 0; a < 3; ++a) {
         st.mave[a] += V * st.mave_l[l][a] / vt;
         st.mvar[a] += V * st.mvar_l[l][a] / vt;
         st.have[a] += V * st.have_l[l][a] / vt;
       }
       mmag += acc[l][kSlotMmag] / V;
+      mt = fmax(mt, acc[l][kSlotMaxTq]);
+      m1 = fmax(m1, acc[l][kSlotMaxD2]);
+      en += acc[l][kSlotE];
     }
-    mt = fmax(mt, acc[l][kSlotMaxTq]);
-    m1 = fmax(m1, acc[l][kSlotMaxD2]);
-    en += acc[l][kSlotE];
   }
   st.errmx = sqrt(mt);
   st.errmx1 = m1;

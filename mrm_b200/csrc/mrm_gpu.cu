@@ -47,6 +47,9 @@ struct LayerBufs {
   void* ucoef = nullptr;
   int *lidx = nullptr, *lnbr = nullptr;
   void* lcoef = nullptr;
+  void* xst = nullptr;   // V4<R> lattice exchange coefficients (null: CSR form)
+  void* ucol = nullptr;  // R columnar interlayer coefficients (null: CSR form)
+  void* lcol = nullptr;
   double hdir[3] = {0, 0, 0};
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
   double temperature = 0.0, gamma = 1.76e7;
@@ -92,6 +95,7 @@ struct Engine {
   Task* d_ctasks = nullptr;
   int nrt = 0, nct = 0, rt_cap = 0, ct_cap = 0;
   size_t smem_row = 0, smem_col = 0;
+  int rowcfg = 0;
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -100,7 +104,7 @@ struct Engine {
   void* d_tw = nullptr;  // Cx<R>[kTwN]
   bool tables_dirty = true;
   bool desc_dirty = true;
-  std::map<int, cudaGraphExec_t> graphs;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (steps, with stats)
   std::string err;
   bool init_done = false;
 };
@@ -206,16 +210,31 @@ void fft_grid(const mrm_geom& g, int* px, int* py) {
   }
 }
 
-int rows_per_task(const mrm_gpu* r) { return std::max(1, std::min(r->g.ny, kBlock / std::max(1, r->g.nx))); }
+int rows_per_task(const mrm_gpu* r) {
+  if (r->g.nx >= kBlock) return 1;
+  return std::max(1, std::min(r->g.ny, kBlock / std::max(1, r->g.nx)));
+}
 int cols_per_task(const mrm_gpu* r) {
   int ph = r->px / 2 + 1;
   return std::max(1, std::min(ph, 2048 / (3 * r->nl * r->py)));
 }
+size_t cx_bytes(int prec) { return 2 * relem(prec); }
 size_t row_smem(const mrm_gpu* r, int prec) {
-  return 2ull * rows_per_task(r) * 3 * (r->px / 2) * 2 * relem(prec);
+  return 2ull * rows_per_task(r) * 3 * fft_stride(r->px / 2) * cx_bytes(prec);
 }
 size_t col_smem(const mrm_gpu* r, int prec) {
-  return 2ull * cols_per_task(r) * r->nl * 3 * r->py * 2 * relem(prec);
+  return 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py) * cx_bytes(prec);
+}
+// row-kernel shape: grains per thread x block size
+int row_config(int max_grains) {
+  if (max_grains <= 256) return 0;   // GPT 1, 256 threads
+  if (max_grains <= 512) return 1;   // GPT 2, 256 threads
+  return 2;                          // GPT 2, 512 threads (<= 1024 grains)
+}
+size_t tensor_bytes(const mrm_gpu* r) {
+  const size_t ph = r->px / 2 + 1, npair = (size_t)r->nl * r->nl;
+  if (r->g.precision == MRM_FP64) return ph * npair * 9 * r->py * 2 * sizeof(double);
+  return ph * npair * 9 * (r->py / 2 + 1) * sizeof(float);
 }
 
 int validate_geom(const mrm_geom* g, std::string* errp) {
@@ -230,6 +249,8 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
   if (!(g->dx > 0 && g->dy > 0)) return set_err(errp, MRM_ERR_ARG, "dx, dy must be > 0");
   for (int l = 0; l < g->n_lay; ++l)
     if (!(g->dz[l] > 0)) return set_err(errp, MRM_ERR_ARG, "dz[%d] must be > 0", l);
+  if (g->nx > 1024)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "rows of more than 1024 grains are not supported (nx=%d)", g->nx);
   if (g->boundary == MRM_PERIODIC && (!is_pow2(g->nx) || !is_pow2(g->ny)))
     return set_err(errp, MRM_ERR_UNSUPPORTED,
                    "periodic demag needs power-of-two nx, ny on this path (got %d x %d)", g->nx, g->ny);
@@ -293,6 +314,9 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.lidx = b.lidx;
     o.lnbr = b.lnbr;
     o.lcoef = static_cast<const R*>(b.lcoef);
+    o.xst = static_cast<const V4<R>*>(b.xst);
+    o.ucol = static_cast<const R*>(b.ucol);
+    o.lcol = static_cast<const R*>(b.lcol);
     for (int a = 0; a < 3; ++a) o.hdir[a] = b.hdir[a];
     o.t_start = b.t_start;
     o.t_end = b.t_end;
@@ -341,6 +365,7 @@ int build_tables(Engine* e) {
   std::string* errp = &e->err;
   std::vector<Task> rt, ct;
   size_t srow = 0, scol = 0;
+  int maxg = 1;
   for (size_t i = 0; i < e->runs.size(); ++i) {
     mrm_gpu* r = e->runs[i];
     r->slot = (int)i;
@@ -349,6 +374,7 @@ int build_tables(Engine* e) {
     for (int l = 0; l < r->nl; ++l)
       for (int j = 0; j < r->g.ny; j += rpt) rt.push_back(make_int4((int)i, l, j, std::min(rpt, r->g.ny - j)));
     r->nrow_tasks = (int)rt.size() - r->row_task0;
+    maxg = std::max(maxg, rpt * r->g.nx);
     srow = std::max(srow, row_smem(r, e->prec));
     if (r->demag && r->tensor_ready) {
       const int cpt = cols_per_task(r), ph = r->px / 2 + 1;
@@ -391,6 +417,7 @@ int build_tables(Engine* e) {
   if (e->nct) CK(cudaMemcpyAsync(e->d_ctasks, ct.data(), sizeof(Task) * e->nct, cudaMemcpyHostToDevice, e->st));
   e->smem_row = srow;
   e->smem_col = scol;
+  e->rowcfg = row_config(maxg);
   clear_graphs(e);
   e->tables_dirty = false;
   e->desc_dirty = true;
@@ -409,58 +436,75 @@ int raise_smem(K* kern, size_t bytes, std::string* errp) {
   return MRM_OK;
 }
 
+template <typename R, int GPT, int BLK>
+int set_row_attrs(size_t rs, std::string* errp) {
+  int rc = 0;
+  rc |= raise_smem(row_kernel<R, kInit, false, GPT, BLK>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kPred, false, GPT, BLK>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kCorr, false, GPT, BLK>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kCorr, true, GPT, BLK>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kEval, false, GPT, BLK>, rs, errp);
+  return rc;
+}
+
 template <typename R>
 int set_smem_attrs(Engine* e) {
   std::string* errp = &e->err;
   const size_t rs = std::max<size_t>(e->smem_row, 16), cs = std::max<size_t>(e->smem_col, 16);
   int rc = 0;
-  rc |= raise_smem(row_kernel<R, kInit, false>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kPred, false>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, false>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, true>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kEval, false>, rs, errp);
-  rc |= raise_smem(col_kernel<R>, cs, errp);
+  if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256>(rs, errp);
+  else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256>(rs, errp);
+  else rc |= set_row_attrs<R, 2, 512>(rs, errp);
+  rc |= raise_smem(col_kernel<R, true, kBlock>, cs, errp);
+  rc |= raise_smem(col_kernel<R, false, kBlock>, cs, errp);
   return rc ? MRM_ERR_CUDA : MRM_OK;
 }
 
-template <typename R>
-void launch_row(Engine* e, int stage, int istep, int flags) {
+template <typename R, int GPT, int BLK>
+void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
   const RunDev<R>* runs = static_cast<const RunDev<R>*>(e->d_runs);
   const Cx<R>* tw = static_cast<const Cx<R>*>(e->d_tw);
-  if (!e->nrt) return;
-  const dim3 g(e->nrt), b(kBlock);
+  const dim3 g(e->nrt), b(BLK);
   const size_t sm = e->smem_row;
   switch (stage) {
     case kInit:
-      row_kernel<R, kInit, false><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      row_kernel<R, kInit, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kPred:
-      row_kernel<R, kPred, false><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      row_kernel<R, kPred, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kCorr:
       if (flags & kFlagStats)
-        row_kernel<R, kCorr, true><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        row_kernel<R, kCorr, true, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
       else
-        row_kernel<R, kCorr, false><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        row_kernel<R, kCorr, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     default:
-      row_kernel<R, kEval, false><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      row_kernel<R, kEval, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
   }
 }
 
 template <typename R>
-void launch_col(Engine* e, int istep, int flags) {
-  if (!e->nct) return;
-  col_kernel<R><<<e->nct, kBlock, e->smem_col, e->st>>>(static_cast<const RunDev<R>*>(e->d_runs),
-                                                       e->d_ctasks, static_cast<const Cx<R>*>(e->d_tw),
-                                                       istep, flags);
+void launch_row(Engine* e, int stage, int istep, int flags) {
+  if (!e->nrt) return;
+  if (e->rowcfg == 0) launch_row_cfg<R, 1, 256>(e, stage, istep, flags);
+  else if (e->rowcfg == 1) launch_row_cfg<R, 2, 256>(e, stage, istep, flags);
+  else launch_row_cfg<R, 2, 512>(e, stage, istep, flags);
 }
 
 template <typename R>
-void enqueue_steps(Engine* e, int k) {
+void launch_col(Engine* e, int istep, int flags) {
+  if (!e->nct) return;
+  constexpr bool packed = sizeof(R) == sizeof(float);
+  col_kernel<R, packed, kBlock><<<e->nct, kBlock, e->smem_col, e->st>>>(
+      static_cast<const RunDev<R>*>(e->d_runs), e->d_ctasks, static_cast<const Cx<R>*>(e->d_tw), istep, flags);
+}
+
+template <typename R>
+void enqueue_steps(Engine* e, int k, bool stats) {
   for (int i = 0; i < k; ++i) {
-    const int last = (i == k - 1) ? (kFlagStats | kFlagStoreField) : 0;
+    const int last = (stats && i == k - 1) ? (kFlagStats | kFlagStoreField) : 0;
     launch_row<R>(e, kPred, i, 0);
     launch_col<R>(e, i, 0);
     launch_row<R>(e, kCorr, i, last);
@@ -468,8 +512,9 @@ void enqueue_steps(Engine* e, int k) {
   }
   const int nr = (int)e->runs.size();
   advance_kernel<R><<<(nr + 127) / 128, 128, 0, e->st>>>(static_cast<RunDev<R>*>(e->d_runs), nr, k);
-  finalize_stats_kernel<R><<<nr, 32, 0, e->st>>>(static_cast<const RunDev<R>*>(e->d_runs), e->d_rtasks,
-                                                 e->d_part, e->d_stats, nr);
+  if (stats)
+    finalize_stats_kernel<R><<<nr, 256, 0, e->st>>>(static_cast<const RunDev<R>*>(e->d_runs), e->d_rtasks,
+                                                    e->d_part, e->d_stats, nr);
 }
 
 template <typename R>
@@ -508,18 +553,20 @@ int run_steps(Engine* e, int nsteps) {
   int left = nsteps;
   while (left > 0) {
     const int k = std::min(left, kGraphSteps);
-    auto it = e->graphs.find(k);
+    const bool stats = (left == k);  // reductions only on the call's last step
+    auto key = std::make_pair(k, stats ? 1 : 0);
+    auto it = e->graphs.find(key);
     if (it == e->graphs.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-      enqueue_steps<R>(e, k);
+      enqueue_steps<R>(e, k, stats);
       cudaError_t ce = cudaStreamEndCapture(e->st, &g);
       if (ce != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
       cudaGraphExec_t ge;
       ce = cudaGraphInstantiate(&ge, g, 0);
       cudaGraphDestroy(g);
       if (ce != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-      it = e->graphs.emplace(k, ge).first;
+      it = e->graphs.emplace(key, ge).first;
     }
     CK(cudaGraphLaunch(it->second, e->st));
     left -= k;
@@ -556,7 +603,8 @@ int run_alloc(mrm_gpu* r) {
   const int ph = r->px / 2 + 1, pyh = r->py / 2 + 1;
   int rc = dmalloc(errp, &r->spec, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
   if (rc) return rc;
-  rc = dmalloc(errp, &r->tens, (size_t)ph * r->nl * r->nl * 9 * pyh * re);
+  (void)pyh;
+  rc = dmalloc(errp, &r->tens, tensor_bytes(r));
   if (rc) return rc;
   const size_t n = (size_t)r->g.nx * r->g.ny;
   for (int l = 0; l < r->nl; ++l) {
@@ -582,6 +630,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
+    dfree(b.xst); dfree(b.ucol); dfree(b.lcol);
   }
 }
 
@@ -591,7 +640,8 @@ int64_t footprint(const mrm_geom& g) {
   const size_t re = g.precision == MRM_FP64 ? 8 : 4;
   const int64_t n = (int64_t)g.nx * g.ny, nl = g.n_lay;
   const int64_t ph = px / 2 + 1, pyh = py / 2 + 1;
-  int64_t b = nl * 3 * g.ny * ph * 2 * re + ph * nl * nl * 9 * pyh * re;
+  int64_t b = nl * 3 * g.ny * ph * 2 * re;
+  b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * pyh * 4;
   b += nl * n * (7 * 4 * re + 4 * 8);
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
   if (nl > 1) b += 2 * nl * ((n + 1) * 4 + n * (4 + re));
@@ -714,9 +764,34 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
   auto& hc = host_cache()[r];
   hc.resize(MRM_MAX_LAYERS);
   hc[l].ms_scale.assign(ms_scale, ms_scale + n);
+  dfree(b.xst);
   if (hxi && hxg && hx) {
     int rc = upload_csr<R>(r, n, hxi, hxg, hx, ms_scale, n, &b.xidx, &b.xnbr, &b.xcoef);
     if (rc) return rc;
+    // lattice form: every entry is one of the 4 periodic nearest neighbours, each
+    // at most once (construct_grain.f90:1281, iwrp) -> per-grain coefficients
+    bool lattice = nx >= 3 && ny >= 3;
+    std::vector<R> st(lattice ? 4 * (size_t)n : 0, (R)0);
+    for (int gi = 0; lattice && gi < n; ++gi) {
+      const int i = gi % nx, j = gi / nx;
+      const int nbrs[4] = {((j + ny - 1) % ny) * nx + i, j * nx + (i + nx - 1) % nx,
+                           j * nx + (i + 1) % nx, ((j + 1) % ny) * nx + i};
+      bool used[4] = {false, false, false, false};
+      for (int q = hxi[gi]; q < hxi[gi + 1]; ++q) {
+        const int nb = hxg[q] - 1;
+        int d = -1;
+        for (int k = 0; k < 4; ++k)
+          if (nbrs[k] == nb && !used[k]) { d = k; break; }
+        if (d < 0) { lattice = false; break; }
+        used[d] = true;
+        st[4 * (size_t)gi + d] = (R)(hx[q] * ms_scale[nb]);
+      }
+    }
+    if (lattice) {
+      int rc2 = dmalloc(errp, &b.xst, sizeof(R) * 4 * (size_t)n);
+      if (rc2) return rc2;
+      CK(cudaMemcpy(b.xst, st.data(), sizeof(R) * 4 * (size_t)n, cudaMemcpyHostToDevice));
+    }
   } else {
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
   }
@@ -811,13 +886,15 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   unsigned long long* d_mx = nullptr;
   rc = dmalloc(errp, (void**)&d_mx, 2 * sizeof(unsigned long long));
   if (rc) return rc;
-  const long long total = (long long)ph * npair * 9 * pyh;
-  if (e->prec == MRM_FP64)
-    pack_tensor_kernel<double><<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
-        static_cast<const Cx<double>*>(d_spec), static_cast<double*>(r->tens), npair, r->py, ph, d_mx, d_mx + 1);
-  else
+  if (e->prec == MRM_FP64) {
+    const long long total = (long long)ph * npair * 9 * r->py;
+    pack_tensor_full_kernel<<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
+        static_cast<const Cx<double>*>(d_spec), static_cast<Cx<double>*>(r->tens), npair, r->py, ph, d_mx, d_mx + 1);
+  } else {
+    const long long total = (long long)ph * npair * 9 * pyh;
     pack_tensor_kernel<float><<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
         static_cast<const Cx<double>*>(d_spec), static_cast<float*>(r->tens), npair, r->py, ph, d_mx, d_mx + 1);
+  }
   CK(cudaGetLastError());
   unsigned long long hm[2];
   CK(cudaMemcpyAsync(hm, d_mx, sizeof(hm), cudaMemcpyDeviceToHost, e->st));
@@ -924,6 +1001,7 @@ int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* in
   if ((int)hc.size() <= other || hc[other].ms_scale.empty())
     return set_err(&h->err, MRM_ERR_STATE, "upload layer %d before its interlayer coupling", other);
   if (!index || !grain || !coef) return set_err(&h->err, MRM_ERR_ARG, "NULL interlayer array");
+  std::string* errp = &h->err;
   cudaSetDevice(h->eng->dev);
   cudaStreamSynchronize(h->eng->st);
   LayerBufs& b = h->L[layer];
@@ -936,6 +1014,25 @@ int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* in
     rc = side == 0 ? upload_csr<float>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.uidx, &b.unbr, &b.ucoef)
                    : upload_csr<float>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.lidx, &b.lnbr, &b.lcoef);
   if (rc) return rc;
+  // columnar form: grain n couples to grain n of the other layer only
+  void** col = side == 0 ? &b.ucol : &b.lcol;
+  dfree(*col);
+  bool columnar = h->L[other].n == n;
+  for (int g = 0; columnar && g < n; ++g)
+    columnar = (index[g + 1] - index[g] == 1) && (grain[index[g]] == g + 1);
+  if (columnar) {
+    const size_t re = relem(h->g.precision);
+    std::vector<double> cf(n);
+    for (int g = 0; g < n; ++g) cf[g] = coef[index[g]] * hc[other].ms_scale[g];
+    rc = dmalloc(errp, col, re * n);
+    if (rc) return rc;
+    if (h->g.precision == MRM_FP64) {
+      CK(cudaMemcpy(*col, cf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(cf.begin(), cf.end());
+      CK(cudaMemcpy(*col, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    }
+  }
   h->eng->desc_dirty = true;
   return MRM_OK;
 }

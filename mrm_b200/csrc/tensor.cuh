@@ -185,8 +185,42 @@ __global__ void __launch_bounds__(256) c2c_cols_f64(Cx<double>* __restrict__ dat
   for (int j = threadIdx.x; j < py; j += blockDim.x) base[(long long)j * ph] = Y[j];
 }
 
-// spectrum [pair][9][py][ph] (FP64) -> tens[k][pair][c][kyh] (R); the discarded
-// parts (the wrong-parity residue) are tracked in *resid as max |discarded|.
+// block-wide max of two non-negative doubles, one atomicMax per block
+__device__ __forceinline__ void block_max2(double a, double b, unsigned long long* ga,
+                                           unsigned long long* gb) {
+  __shared__ double sa[32], sb[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { sa[warp] = a; sb[warp] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x + 31) / 32; ++w) { a = fmax(a, sa[w]); b = fmax(b, sb[w]); }
+    atomicMax(ga, (unsigned long long)__double_as_longlong(a));
+    atomicMax(gb, (unsigned long long)__double_as_longlong(b));
+  }
+}
+
+// parity-violating part of one spectral value (and its ky mirror) and the kept part
+__device__ __forceinline__ void parity_parts(const Cx<double>* S, int c, int kyh, int k, int py, int ph,
+                                             double* keep, double* disc) {
+  const Cx<double> v = S[(long long)kyh * ph + k];
+  const bool imag = (kImagMask >> c) & 1;
+  const bool odd = (kOddMask >> c) & 1;
+  *keep = imag ? v.y : v.x;
+  double d = imag ? fabs(v.x) : fabs(v.y);
+  if (kyh > 0 && kyh < py - kyh) {
+    const Cx<double> u = S[(long long)(py - kyh) * ph + k];
+    const double um = imag ? u.y : u.x;
+    d = fmax(d, fabs(um - (odd ? -*keep : *keep)));
+  }
+  *disc = d;
+}
+
+// spectrum [pair][9][py][ph] (FP64) -> tens[k][pair][c][kyh] (R): one real per
+// component and 0 <= ky <= py/2 (FP32 runs); tracks the dropped residue.
 template <typename R>
 __global__ void pack_tensor_kernel(const Cx<double>* __restrict__ spec, R* __restrict__ tens,
                                    int npair, int py, int ph, unsigned long long* resid,
@@ -194,28 +228,39 @@ __global__ void pack_tensor_kernel(const Cx<double>* __restrict__ spec, R* __res
   const int pyh = py / 2 + 1;
   const long long total = (long long)ph * npair * 9 * pyh;
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= total) return;
-  const int kyh = (int)(gid % pyh);
-  long long r = gid / pyh;
-  const int c = (int)(r % 9);
-  r /= 9;
-  const int pair = (int)(r % npair);
-  const int k = (int)(r / npair);
-  const Cx<double>* S = spec + ((long long)pair * 9 + c) * py * ph;
-  const Cx<double> v = S[(long long)kyh * ph + k];
-  const bool imag = (kImagMask >> c) & 1;
-  const bool odd = (kOddMask >> c) & 1;
-  const double keep = imag ? v.y : v.x;
-  double disc = imag ? fabs(v.x) : fabs(v.y);
-  // mirror bin: N(k, py-ky) must equal +-N(k, ky)
-  if (kyh > 0 && kyh < py - kyh) {
-    const Cx<double> u = S[(long long)(py - kyh) * ph + k];
-    const double um = imag ? u.y : u.x;
-    disc = fmax(disc, fabs(um - (odd ? -keep : keep)));
+  double keep = 0.0, disc = 0.0;
+  if (gid < total) {
+    const int kyh = (int)(gid % pyh);
+    long long r = gid / pyh;
+    const int c = (int)(r % 9);
+    r /= 9;
+    const int pair = (int)(r % npair);
+    const int k = (int)(r / npair);
+    parity_parts(spec + ((long long)pair * 9 + c) * py * ph, c, kyh, k, py, ph, &keep, &disc);
+    tens[gid] = (R)keep;
   }
-  tens[gid] = (R)keep;
-  atomicMax(resid, (unsigned long long)__double_as_longlong(disc));
-  atomicMax(kept, (unsigned long long)__double_as_longlong(fabs(keep)));
+  block_max2(disc, fabs(keep), resid, kept);
+}
+
+// spectrum [pair][9][py][ph] -> tens[k][pair][c][ky] complex, unchanged (FP64 runs)
+__global__ void pack_tensor_full_kernel(const Cx<double>* __restrict__ spec, Cx<double>* __restrict__ tens,
+                                        int npair, int py, int ph, unsigned long long* resid,
+                                        unsigned long long* kept) {
+  const long long total = (long long)ph * npair * 9 * py;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double keep = 0.0, disc = 0.0;
+  if (gid < total) {
+    const int ky = (int)(gid % py);
+    long long r = gid / py;
+    const int c = (int)(r % 9);
+    r /= 9;
+    const int pair = (int)(r % npair);
+    const int k = (int)(r / npair);
+    const Cx<double>* S = spec + ((long long)pair * 9 + c) * py * ph;
+    tens[gid] = S[(long long)ky * ph + k];
+    if (ky <= py / 2) parity_parts(S, c, ky, k, py, ph, &keep, &disc);
+  }
+  block_max2(disc, fabs(keep), resid, kept);
 }
 
 }  // namespace mrm
