@@ -877,7 +877,8 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   CK(cudaMemcpy(d_tw64, tw.data(), sizeof(double) * 2 * kTwN, cudaMemcpyHostToDevice));
   const Cx<double>* tw64 = static_cast<const Cx<double>*>(d_tw64);
   const int M = r->px / 2;
-  size_t s1 = 2 * M * sizeof(Cx<double>), s2 = 2 * r->py * sizeof(Cx<double>);
+  // two shared buffers of one padded-stride sequence each (fft.cuh)
+  size_t s1 = 2 * (size_t)fft_stride(M) * sizeof(Cx<double>), s2 = 2 * (size_t)fft_stride(r->py) * sizeof(Cx<double>);
   if (raise_smem(r2c_rows_f64, s1, errp) || raise_smem(c2c_cols_f64, s2, errp)) return MRM_ERR_CUDA;
   r2c_rows_f64<<<planes * r->py, 256, s1, e->st>>>(d_n2d, static_cast<Cx<double>*>(d_spec), r->lgpx, r->py, tw64);
   CK(cudaGetLastError());

@@ -155,12 +155,13 @@ __global__ void __launch_bounds__(256) r2c_rows_f64(const double* __restrict__ i
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lgM = lgpx - 1, M = 1 << lgM, ph = M + 1, px = 2 * M;
   const long long row = blockIdx.x;  // p*py + j
+  const int cs = fft_stride(M);
   Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
-  Cx<double>* B = A + M;
+  Cx<double>* B = A + cs;
   const double* src = in + row * px;
   for (int k = threadIdx.x; k < M; k += blockDim.x) A[k] = Cx<double>{src[2 * k], src[2 * k + 1]};
   __syncthreads();
-  Cx<double>* Y = block_fft<double, -1>(A, B, lgM, 1, M, tw);
+  Cx<double>* Y = block_fft<double, -1>(A, B, lgM, 1, cs, tw);
   for (int k = threadIdx.x; k < ph; k += blockDim.x) {
     const Cx<double> yk = Y[k & (M - 1)], ymk = cconj(Y[(M - k) & (M - 1)]);
     const Cx<double> e = cscale(cadd(yk, ymk), 0.5), o = cscale(csub(yk, ymk), 0.5);
@@ -176,12 +177,13 @@ __global__ void __launch_bounds__(256) c2c_cols_f64(Cx<double>* __restrict__ dat
   const int py = 1 << lgpy;
   const long long p = blockIdx.x / ph;
   const int k = blockIdx.x - (int)(p * ph);
+  const int cs = fft_stride(py);
   Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
-  Cx<double>* B = A + py;
+  Cx<double>* B = A + cs;
   Cx<double>* base = data + p * (long long)py * ph + k;
   for (int j = threadIdx.x; j < py; j += blockDim.x) A[j] = base[(long long)j * ph];
   __syncthreads();
-  Cx<double>* Y = block_fft<double, -1>(A, B, lgpy, 1, py, tw);
+  Cx<double>* Y = block_fft<double, -1>(A, B, lgpy, 1, cs, tw);
   for (int j = threadIdx.x; j < py; j += blockDim.x) base[(long long)j * ph] = Y[j];
 }
 
