@@ -69,7 +69,9 @@ def test_device_tensor_matches_oracle(oracle, gpulib, boundary):
     # 64-corner sums (tensor_element.f90:78-100); periodic images amplify it
     assert np.abs(T - orc.n2d).max() < 2e-8 * scale
     resid, kept = gpu.tensor_residual()
-    assert resid < 1e-8 * kept
+    # wrong-parity residue of the spectrum: rounding for open boundaries; the
+    # periodic image sums carry ~1e-7-relative antisymmetric cancellation noise
+    assert resid < (1e-6 if boundary == 0 else 1e-9) * kept
     # the device-built tensor gives the same demag as the oracle's
     m = random_m(med.layers[0].N, 9)
     orc.set_state(0, m)
