@@ -48,6 +48,7 @@ struct LayerDev {
   V4<R>* dm;        // predictor increment d1
   V4<R>* hf;        // last non-thermal total field (get_field output)
   V4<R>* hd;        // demag field of the last evaluation-only pass
+  V4<R>* ht;        // thermal field / sqrt(dt) of the current step (predictor -> corrector)
   const V4<R>* pa;  // {kx, ky, kz, Hk1*hk_scale}
   const V4<R>* pb;  // {Ms*ms_scale, Hk2*hk_scale, alpha*alpha_scale, sigma0}
   const V4<double>* pv;  // {vol, ms_scale, ms, 0} (FP64, reductions)

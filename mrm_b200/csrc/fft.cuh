@@ -8,8 +8,8 @@
 // Intermediate passes use a padded layout (one spare slot per 16 elements)
 // so the stride-R stores of the early passes hit distinct banks; the input of
 // the first pass and the output of the last pass are unpadded.  `stride`
-// must be >= fft_stride(n).  Twiddles come from one FP64-accurate table of
-// e^{-2 pi i k / 4096}.
+// must be >= fft_stride(n).  Twiddles come from a table tw[k] = e^{-2 pi i k / 2^lgtw}
+// (FP64-accurate values) with 2^lgtw >= n, normally staged in shared memory.
 #pragma once
 #include "common.cuh"
 
@@ -97,7 +97,8 @@ MRM_D void dft16(Cx<R>* v) {
 // One Stockham pass.  PIN / POUT: input / output use the padded layout.
 template <typename R, int RADIX, int LGR, int S>
 MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, int lgn, int nb,
-                         int stride, int lgNs, bool pin, bool pout, const Cx<R>* __restrict__ tw) {
+                         int stride, int lgNs, bool pin, bool pout, const Cx<R>* __restrict__ tw,
+                         int lgtw) {
   const int lgnR = lgn - LGR;
   const int nR = 1 << lgnR;
   const int Ns = 1 << lgNs;
@@ -114,7 +115,7 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
     }
     const int k = j & (Ns - 1);
     if (lgNs > 0) {
-      const int sh = kTwLog - lgNs - LGR;
+      const int sh = lgtw - lgNs - LGR;
 #pragma unroll
       for (int r = 1; r < RADIX; ++r) {
         Cx<R> w = tw[(r * k) << sh];
@@ -140,7 +141,7 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
 // __syncthreads() before the call; on return the result is complete.
 template <typename R, int S>
 MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
-                       const Cx<R>* __restrict__ tw) {
+                       const Cx<R>* __restrict__ tw, int lgtw) {
   int lgNs = 0;
   int rem = lgn;
   // pass list: radix-16 while >= 4 bits remain, then one 8/4/2 pass
@@ -149,17 +150,17 @@ MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
   const int npass = n16 + (tail ? 1 : 0);
   int p = 0;
   for (int q = 0; q < n16; ++q, ++p) {
-    stockham_pass<R, 16, 4, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw);
+    stockham_pass<R, 16, 4, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw, lgtw);
     __syncthreads();
     Cx<R>* t = a; a = b; b = t;
     lgNs += 4;
   }
   if (tail == 3) {
-    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
   } else if (tail == 2) {
-    stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+    stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
   } else if (tail == 1) {
-    stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw);
+    stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
   }
   if (tail) {
     __syncthreads();
@@ -168,10 +169,22 @@ MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
   return a;
 }
 
-// e^{-2 pi i k / 2^lg} from the 4096-entry table
+// e^{-2 pi i k / 2^lg} from the 4096-entry global table
 template <typename R>
 MRM_D Cx<R> twiddle(const Cx<R>* __restrict__ tw, int k, int lg) {
   return tw[k << (kTwLog - lg)];
 }
+
+// Stages tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, from the global table.
+template <typename R>
+MRM_D void stage_twiddles(Cx<R>* __restrict__ tw_s, const Cx<R>* __restrict__ tw, int lg) {
+  const int n = 1 << lg;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) tw_s[k] = tw[k << (kTwLog - lg)];
+}
+
+// programmatic dependent launch (sm_90+): let the next kernel in the stream
+// start its independent prologue / wait for the previous kernel's results
+MRM_D void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+MRM_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 }  // namespace mrm

@@ -94,6 +94,7 @@ struct GrainIn {
   V4<R> nb[4];   // lattice neighbours
   V4<R> dm, m0;  // corrector: predictor increment and m_n
   V4<R> vu, vl;  // columnar interlayer partners
+  V4<R> ht;      // thermal field / sqrt(dt)
   R cu, cl;
 };
 
@@ -106,15 +107,14 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags, double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_launch_dependents();
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
-  if (!rd.active) return;
-  const long long step = rd.step + istep;
-  if (!(flags & kFlagForce) && step >= rd.step_end) return;
+  if (!rd.active) return;  // host-set, constant within a captured graph
 
   const int l = tk.y, row0 = tk.z, nrows = tk.w;
   const int nx = rd.nx, ny = rd.ny;
-  const int lgM = rd.lgpx - 1, M = 1 << lgM, ph = M + 1;
+  const int lgpx = rd.lgpx, lgM = lgpx - 1, M = 1 << lgM, ph = M + 1;
   const int cs = fft_stride(M);  // complex stride of one sequence in shared memory
   const int nseq = nrows * 3;
   const int ngr = nrows * nx;
@@ -122,31 +122,52 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
   const bool demag = rd.demag != 0;
   constexpr bool stats = (STAGE == kCorr) && STATS;
 
-  Cx<R>* bufA = reinterpret_cast<Cx<R>*>(smem_raw);
+  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // e^{-2 pi i k/px}, k < px
+  Cx<R>* bufA = tws + (1 << lgpx);
   Cx<R>* bufB = bufA + nseq * cs;
   __shared__ double sred[stats_slots<STAGE, STATS>()];
 
-  // ---------------- prefetch per-grain inputs ----------------
+  // ---------------- static inputs (not written by the previous kernel) ----------------
+  if (demag) stage_twiddles(tws, tw, lgpx);
   const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
   const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
   const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
   const bool stencil = L.xst != nullptr;
+  const bool ucol = L.ucol && Lu, lcol = L.lcol && Ll;
+  const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
   GrainIn<R> g[GPT];
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    const int idx = threadIdx.x + q * BLOCK;
+    if (idx >= ngr) continue;
+    const int row = idx / nx, i = idx - row * nx;
+    const int n = (row0 + row) * nx + i;
+    g[q].pb = L.pb[n];
+    if (STAGE == kInit) continue;
+    g[q].pa = L.pa[n];
+    if (stencil) g[q].cst = L.xst[n];
+    if (ucol) g[q].cu = L.ucol[n];
+    if (lcol) g[q].cl = L.lcol[n];
+  }
+
+  // ---------------- wait for the previous kernel's results ----------------
+  pdl_wait();
+  const long long step = rd.step + istep;
+  if (!(flags & kFlagForce) && step >= rd.step_end) return;
+
+  // ---------------- dynamic per-grain inputs ----------------
 #pragma unroll
   for (int q = 0; q < GPT; ++q) {
     const int idx = threadIdx.x + q * BLOCK;
     if (idx >= ngr) continue;
     const int row = idx / nx, i = idx - row * nx, j = row0 + row;
     const int n = j * nx + i;
-    g[q].pb = L.pb[n];
     if (STAGE == kInit) {
       g[q].mf = L.m[n];
       continue;
     }
     g[q].mf = mfield[n];
-    g[q].pa = L.pa[n];
     if (stencil) {
-      g[q].cst = L.xst[n];
       const int jm = (j == 0 ? ny - 1 : j - 1), jp = (j == ny - 1 ? 0 : j + 1);
       const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
       g[q].nb[0] = mfield[jm * nx + i];
@@ -157,14 +178,26 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
     if (STAGE == kCorr) {
       g[q].dm = L.dm[n];
       g[q].m0 = L.m[n];
+      if (thermal) g[q].ht = L.ht[n];
     }
-    if (L.ucol && Lu) {
-      g[q].cu = L.ucol[n];
-      g[q].vu = ((STAGE == kCorr) ? Lu->mp : Lu->m)[n];
-    }
-    if (L.lcol && Ll) {
-      g[q].cl = L.lcol[n];
-      g[q].vl = ((STAGE == kCorr) ? Ll->mp : Ll->m)[n];
+    if (ucol) g[q].vu = ((STAGE == kCorr) ? Lu->mp : Lu->m)[n];
+    if (lcol) g[q].vl = ((STAGE == kCorr) ? Ll->mp : Ll->m)[n];
+  }
+  // predictor: Philox thermal normals while the loads above are in flight
+  // (llg.f90:1083 h = H + hthm/sqrt(dt); the corrector reuses them, :1262-1266)
+  if (STAGE == kPred && thermal) {
+    const R tfac = (R)sqrt(L.temperature / rd.dt);
+#pragma unroll
+    for (int q = 0; q < GPT; ++q) {
+      const int idx = threadIdx.x + q * BLOCK;
+      if (idx >= ngr) continue;
+      const int row = idx / nx, i = idx - row * nx;
+      const int n = (row0 + row) * nx + i;
+      R gn[3];
+      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step,
+                      (unsigned long long)n, gn);
+      const R s = g[q].pb.w * tfac;
+      g[q].ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
     }
   }
 
@@ -194,13 +227,13 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
           if (k == 0) { a.y = 0; b.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
           const Cx<R> e = cadd(a, cconj(b));
           const Cx<R> o = csub(a, cconj(b));
-          const Cx<R> w = cconj(twiddle(tw, k, rd.lgpx));  // e^{+2 pi i k / px}
+          const Cx<R> w = cconj(tws[k]);  // e^{+2 pi i k / px}
           bufA[s * cs + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
         }
       }
     }
     __syncthreads();
-    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, cs, tw);
+    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, cs, tws, lgpx);
   }
   Cx<R>* W = (Z == bufA) ? bufB : bufA;  // real outputs of this stage (forward input)
   const R* hdr = reinterpret_cast<const R*>(Z);
@@ -214,8 +247,6 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
   const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
-  const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
-  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
   const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
 
   double rec[stats ? kNPart : 1];
@@ -266,12 +297,12 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
       csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
     }
     R vx = 0, vy = 0, vz = 0;
-    if (L.ucol && Lu) {
+    if (ucol) {
       vx += G.cu * G.vu.x; vy += G.cu * G.vu.y; vz += G.cu * G.vu.z;
     } else if (L.uidx && Lu) {
       csr_sum<R>(L.uidx, L.unbr, L.ucoef, (STAGE == kCorr) ? Lu->mp : Lu->m, n, vx, vy, vz);
     }
-    if (L.lcol && Ll) {
+    if (lcol) {
       vx += G.cl * G.vl.x; vy += G.cl * G.vl.y; vz += G.cl * G.vl.z;
     } else if (L.lidx && Ll) {
       csr_sum<R>(L.lidx, L.lnbr, L.lcoef, (STAGE == kCorr) ? Ll->mp : Ll->m, n, vx, vy, vz);
@@ -285,16 +316,13 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
       continue;
     }
 
-    // thermal field / sqrt(dt) (llg.f90:1083), Philox normals regenerated in the corrector
+    // thermal field / sqrt(dt) (llg.f90:1083): drawn by the predictor, reused by the corrector
     R htx = 0, hty = 0, htz = 0;
     if (thermal) {
-      R gn[3];
-      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step,
-                      (unsigned long long)n, gn);
-      const R s = pb.w * tfac;
-      htx = s * gn[0];
-      hty = s * gn[1];
-      htz = s * gn[2];
+      htx = G.ht.x;
+      hty = G.ht.y;
+      htz = G.ht.z;
+      if (STAGE == kPred) L.ht[n] = G.ht;
     }
     const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
     V4<R> mn;
@@ -391,7 +419,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
-  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, cs, tw);
+  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, cs, tws, lgpx);
   for (int idx = threadIdx.x; idx < nseq * ph; idx += BLOCK) {
     const int s = idx / ph, k = idx - s * ph;
     const int row = s / 3, comp = s - 3 * row;
@@ -400,7 +428,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
     const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
     const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
     // X[k] = e - i w^k o,  w = e^{-2 pi i / px}
-    const Cx<R> wo = cmul(twiddle(tw, k & (two_m - 1), rd.lgpx), o);
+    const Cx<R> wo = cmul(tws[k & (two_m - 1)], o);
     rd.spec[((size_t)(l * 3 + comp) * ny + row0 + row) * ph + k] = csub(e, cmul_i(wo, (R)1));
   }
 }
@@ -416,17 +444,39 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_launch_dependents();
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
   if (!rd.active || !rd.demag) return;
-  if (!(flags & kFlagForce) && rd.step + istep >= rd.step_end) return;
   const int k0 = tk.y, nc = tk.z;
   const int nl = rd.nl, ny = rd.ny, py = rd.py, lgpy = rd.lgpy;
   const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1;
   const int cs = fft_stride(py);
   const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
-  Cx<R>* A = reinterpret_cast<Cx<R>*>(smem_raw);
+  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // e^{-2 pi i k/py}, k < py
+  Cx<R>* A = tws + py;
   Cx<R>* B = A + nseq * cs;
+
+  // static inputs: twiddles and (single layer pair) the tensor values of this thread's bins
+  stage_twiddles(tws, tw, lgpy);
+  constexpr int kPre = 2;
+  const bool pre = PACKED && nl == 1 && nc * py <= kPre * BLOCK;
+  R tpre[kPre][9];
+  if (pre) {
+#pragma unroll
+    for (int e = 0; e < kPre; ++e) {
+      const int idx = threadIdx.x + e * BLOCK;
+      if (idx < nc * py) {
+        const int c = idx / py, ky = idx - c * py;
+        const int kyh = ky > (py >> 1) ? py - ky : ky;
+        const R* Tp = rd.tens + (size_t)(k0 + c) * 9 * pyh;
+#pragma unroll
+        for (int cc = 0; cc < 9; ++cc) tpre[e][cc] = __ldg(Tp + cc * pyh + kyh);
+      }
+    }
+  }
+  pdl_wait();
+  if (!(flags & kFlagForce) && rd.step + istep >= rd.step_end) return;
 
   // batched strided loads of the columns (rows >= ny are the zero padding)
   const int tot = nseq * py;
@@ -453,12 +503,13 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
     }
   }
   __syncthreads();
-  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, cs, tw);
+  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, cs, tws, lgpy);
   Cx<R>* G = (F == A) ? B : A;
 
   // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
   const int npair = nl * nl;
-  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK) {
+  int e = 0;
+  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK, ++e) {
     const int c = idx / py, ky = idx - c * py;
     for (int ko = 0; ko < nl; ++ko) {
       Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
@@ -471,8 +522,14 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
           const int kyh = upper ? py - ky : ky;
           const R* Tp = rd.tens + ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * pyh;
           R tv[9];
+          if (pre) {
+            // e < kPre here: `pre` implies at most kPre bins per thread
 #pragma unroll
-          for (int cc = 0; cc < 9; ++cc) tv[cc] = __ldg(Tp + cc * pyh + kyh);
+            for (int cc = 0; cc < 9; ++cc) tv[cc] = (e == 0) ? tpre[0][cc] : tpre[kPre - 1][cc];
+          } else {
+#pragma unroll
+            for (int cc = 0; cc < 9; ++cc) tv[cc] = __ldg(Tp + cc * pyh + kyh);
+          }
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -500,7 +557,7 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
     }
   }
   __syncthreads();
-  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, cs, tw);
+  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, cs, tws, lgpy);
 
   const int tot2 = nseq * ny;
   for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
@@ -513,6 +570,8 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
 // Advances every active run's step counter after a captured chunk of k steps.
 template <typename R>
 __global__ void advance_kernel(RunDev<R>* runs, int nruns, int k) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nruns) return;
   RunDev<R>& rd = runs[r];
@@ -542,6 +601,8 @@ __global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __
                                                              StatsDev* __restrict__ out, int nruns) {
   __shared__ double sred[32 * kNPart];
   __shared__ double acc[kMaxLayers][kNPart];
+  pdl_launch_dependents();
+  pdl_wait();
   const int r = blockIdx.x;
   if (r >= nruns) return;
   const RunDev<R>& rd = runs[r];

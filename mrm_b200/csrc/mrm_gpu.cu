@@ -39,7 +39,7 @@ bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 struct LayerBufs {
   int n = 0;
   bool uploaded = false;
-  void *m = nullptr, *mp = nullptr, *dm = nullptr, *hf = nullptr, *hd = nullptr, *pa = nullptr, *pb = nullptr;
+  void *m = nullptr, *mp = nullptr, *dm = nullptr, *hf = nullptr, *hd = nullptr, *ht = nullptr, *pa = nullptr, *pb = nullptr;
   void* pv = nullptr;
   int *xidx = nullptr, *xnbr = nullptr;
   void* xcoef = nullptr;
@@ -219,11 +219,12 @@ int cols_per_task(const mrm_gpu* r) {
   return std::max(1, std::min(ph, 2048 / (3 * r->nl * r->py)));
 }
 size_t cx_bytes(int prec) { return 2 * relem(prec); }
+// shared memory: twiddle table of the transform length + two padded ping-pong buffers
 size_t row_smem(const mrm_gpu* r, int prec) {
-  return 2ull * rows_per_task(r) * 3 * fft_stride(r->px / 2) * cx_bytes(prec);
+  return ((size_t)r->px + 2ull * rows_per_task(r) * 3 * fft_stride(r->px / 2)) * cx_bytes(prec);
 }
 size_t col_smem(const mrm_gpu* r, int prec) {
-  return 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py) * cx_bytes(prec);
+  return ((size_t)r->py + 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py)) * cx_bytes(prec);
 }
 // row-kernel shape: grains per thread x block size
 int row_config(int max_grains) {
@@ -302,6 +303,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.dm = static_cast<V4<R>*>(b.dm);
     o.hf = static_cast<V4<R>*>(b.hf);
     o.hd = static_cast<V4<R>*>(b.hd);
+    o.ht = static_cast<V4<R>*>(b.ht);
     o.pa = static_cast<const V4<R>*>(b.pa);
     o.pb = static_cast<const V4<R>*>(b.pb);
     o.pv = static_cast<const V4<double>*>(b.pv);
@@ -436,6 +438,25 @@ int raise_smem(K* kern, size_t bytes, std::string* errp) {
   return MRM_OK;
 }
 
+// Launch with programmatic stream serialization: the kernel may start while its
+// predecessor drains; it runs its independent prologue and then waits
+// (griddepcontrol.wait) for the predecessor's results.
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <typename R, int GPT, int BLK>
 int set_row_attrs(size_t rs, std::string* errp) {
   int rc = 0;
@@ -468,19 +489,19 @@ void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
   const size_t sm = e->smem_row;
   switch (stage) {
     case kInit:
-      row_kernel<R, kInit, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kInit, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kPred:
-      row_kernel<R, kPred, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kPred, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kCorr:
       if (flags & kFlagStats)
-        row_kernel<R, kCorr, true, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        launch_pdl(row_kernel<R, kCorr, true, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       else
-        row_kernel<R, kCorr, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        launch_pdl(row_kernel<R, kCorr, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     default:
-      row_kernel<R, kEval, false, GPT, BLK><<<g, b, sm, e->st>>>(runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kEval, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
   }
 }
@@ -497,8 +518,9 @@ template <typename R>
 void launch_col(Engine* e, int istep, int flags) {
   if (!e->nct) return;
   constexpr bool packed = sizeof(R) == sizeof(float);
-  col_kernel<R, packed, kBlock><<<e->nct, kBlock, e->smem_col, e->st>>>(
-      static_cast<const RunDev<R>*>(e->d_runs), e->d_ctasks, static_cast<const Cx<R>*>(e->d_tw), istep, flags);
+  launch_pdl(col_kernel<R, packed, kBlock>, dim3(e->nct), dim3(kBlock), e->smem_col, e->st,
+             static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_ctasks,
+             static_cast<const Cx<R>*>(e->d_tw), istep, flags);
 }
 
 template <typename R>
@@ -511,10 +533,12 @@ void enqueue_steps(Engine* e, int k, bool stats) {
     launch_col<R>(e, i, 0);
   }
   const int nr = (int)e->runs.size();
-  advance_kernel<R><<<(nr + 127) / 128, 128, 0, e->st>>>(static_cast<RunDev<R>*>(e->d_runs), nr, k);
+  launch_pdl(advance_kernel<R>, dim3((nr + 127) / 128), dim3(128), 0, e->st,
+             static_cast<RunDev<R>*>(e->d_runs), nr, k);
   if (stats)
-    finalize_stats_kernel<R><<<nr, 256, 0, e->st>>>(static_cast<const RunDev<R>*>(e->d_runs), e->d_rtasks,
-                                                    e->d_part, e->d_stats, nr);
+    launch_pdl(finalize_stats_kernel<R>, dim3(nr), dim3(256), 0, e->st,
+               static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_rtasks,
+               (const double*)e->d_part, e->d_stats, nr);
 }
 
 template <typename R>
@@ -610,7 +634,7 @@ int run_alloc(mrm_gpu* r) {
   for (int l = 0; l < r->nl; ++l) {
     LayerBufs& b = r->L[l];
     b.n = (int)n;
-    void** v4s[] = {&b.m, &b.mp, &b.dm, &b.hf, &b.hd, &b.pa, &b.pb};
+    void** v4s[] = {&b.m, &b.mp, &b.dm, &b.hf, &b.hd, &b.ht, &b.pa, &b.pb};
     for (void** p : v4s) {
       rc = dmalloc(errp, p, n * 4 * re);
       if (rc) return rc;
@@ -626,7 +650,7 @@ void run_free(mrm_gpu* r) {
   dfree(r->tens);
   for (int l = 0; l < MRM_MAX_LAYERS; ++l) {
     LayerBufs& b = r->L[l];
-    dfree(b.m); dfree(b.mp); dfree(b.dm); dfree(b.hf); dfree(b.hd); dfree(b.pa); dfree(b.pb); dfree(b.pv);
+    dfree(b.m); dfree(b.mp); dfree(b.dm); dfree(b.hf); dfree(b.hd); dfree(b.ht); dfree(b.pa); dfree(b.pb); dfree(b.pv);
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
@@ -642,7 +666,7 @@ int64_t footprint(const mrm_geom& g) {
   const int64_t ph = px / 2 + 1, pyh = py / 2 + 1;
   int64_t b = nl * 3 * g.ny * ph * 2 * re;
   b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * pyh * 4;
-  b += nl * n * (7 * 4 * re + 4 * 8);
+  b += nl * n * (8 * 4 * re + 4 * 8);
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
   if (nl > 1) b += 2 * nl * ((n + 1) * 4 + n * (4 + re));
   return b;

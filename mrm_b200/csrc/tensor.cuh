@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) r2c_rows_f64(const double* __restrict__ i
   const double* src = in + row * px;
   for (int k = threadIdx.x; k < M; k += blockDim.x) A[k] = Cx<double>{src[2 * k], src[2 * k + 1]};
   __syncthreads();
-  Cx<double>* Y = block_fft<double, -1>(A, B, lgM, 1, cs, tw);
+  Cx<double>* Y = block_fft<double, -1>(A, B, lgM, 1, cs, tw, kTwLog);
   for (int k = threadIdx.x; k < ph; k += blockDim.x) {
     const Cx<double> yk = Y[k & (M - 1)], ymk = cconj(Y[(M - k) & (M - 1)]);
     const Cx<double> e = cscale(cadd(yk, ymk), 0.5), o = cscale(csub(yk, ymk), 0.5);
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) c2c_cols_f64(Cx<double>* __restrict__ dat
   Cx<double>* base = data + p * (long long)py * ph + k;
   for (int j = threadIdx.x; j < py; j += blockDim.x) A[j] = base[(long long)j * ph];
   __syncthreads();
-  Cx<double>* Y = block_fft<double, -1>(A, B, lgpy, 1, cs, tw);
+  Cx<double>* Y = block_fft<double, -1>(A, B, lgpy, 1, cs, tw, kTwLog);
   for (int j = threadIdx.x; j < py; j += blockDim.x) base[(long long)j * ph] = Y[j];
 }
 
