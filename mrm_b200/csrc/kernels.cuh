@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
   Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
   if (STAGE != kInit && demag) {
+    __syncthreads();  // staged twiddles visible to every thread
     const int tot = nseq * M;
     for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
       Cx<R> xk[4], xm[4];
