@@ -87,7 +87,8 @@ struct RunDev {
   unsigned long long seed;
   int active;
   int row_task0, nrow_tasks;  // range of this run's row tasks (stats partials)
-  Cx<R>* spec;             // [nl][3][ny][px/2+1] half spectra of M (forward) / H (inverse)
+  Cx<R>* spech;            // H^ half spectra, row-major [nl][3][ny][px/2+1] (column kernel -> row kernel)
+  Cx<R>* specx;            // M^ half spectra, column-major [nl][3][px/2+1][ny] (row kernel -> column kernel)
   const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][py/2+1] reals,
                            // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];

@@ -58,7 +58,8 @@ MRM_D void dft8(Cx<R>* v) {
   v[7] = csub(e3, o3);
 }
 
-// 16-point DFT as 4 x 4 (radix-4 over stride 4, twiddles w16^(k1 n2), radix-4)
+// 16-point DFT as 4 x 4 (radix-4 over stride 4, twiddles w16^(k1 n2), radix-4);
+// the outputs are left in digit-reversed order (see dft16_out)
 template <typename R, int S>
 MRM_D void dft16(Cx<R>* v) {
   const R c1 = (R)0.92387953251128675612818318939679;  // cos(pi/8)
@@ -79,20 +80,13 @@ MRM_D void dft16(Cx<R>* v) {
   v[13] = cmul(v[13], w3);
   v[14] = cmul(v[14], w6);
   v[15] = cmul(v[15], w9);
-  Cx<R> t[16];
 #pragma unroll
-  for (int k1 = 0; k1 < 4; ++k1) {
-    Cx<R> a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
-    dft4<R, S>(a0, a1, a2, a3);
-    // output index k = k1 + 4*k2
-    t[k1] = a0;
-    t[k1 + 4] = a1;
-    t[k1 + 8] = a2;
-    t[k1 + 12] = a3;
-  }
-#pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = t[k];
+  for (int k1 = 0; k1 < 4; ++k1) dft4<R, S>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+  // v[4*k1 + k2] now holds output k = k1 + 4*k2 (digit-reversed); dft16_out maps it back
 }
+
+// output index of v[q] after dft16
+MRM_HD constexpr int dft16_out(int q) { return (q >> 2) + 4 * (q & 3); }
 
 // One Stockham pass.  PIN / POUT: input / output use the padded layout.
 template <typename R, int RADIX, int LGR, int S>
@@ -129,11 +123,46 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
     else dft2<R, S>(v);
     const int idxD = ((j >> lgNs) << (lgNs + LGR)) + k;
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) {
+    for (int q = 0; q < RADIX; ++q) {
+      const int r = (RADIX == 16) ? dft16_out(q) : q;
       const int i = idxD + r * Ns;
-      dst[pout ? padi(i) : i] = v[r];
+      dst[pout ? padi(i) : i] = v[q];
     }
   }
+}
+
+// Radix plan: the largest radix R in {16, 8, 4} whose passes keep at least
+// half the block busy (nb * n / R >= BLOCK / 2); small batches use radix 4
+// so that more threads share each pass.
+MRM_D int fft_radix(int lgn, int nb, int block) {
+  const int n = 1 << lgn;
+  if ((nb * n) / 16 >= block / 2 && lgn >= 4) return 16;
+  if ((nb * n) / 8 >= block / 2 && lgn >= 3) return 8;
+  return 4;
+}
+
+template <typename R, int RADIX, int LGR, int S>
+MRM_D Cx<R>* fft_passes(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
+                        const Cx<R>* __restrict__ tw, int lgtw) {
+  int lgNs = 0;
+  const int nfull = lgn / LGR;
+  const int tail = lgn - nfull * LGR;  // 0..LGR-1 remaining bits
+  const int npass = nfull + (tail ? 1 : 0);
+  int p = 0;
+  for (int q = 0; q < nfull; ++q, ++p) {
+    stockham_pass<R, RADIX, LGR, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw, lgtw);
+    __syncthreads();
+    Cx<R>* t = a; a = b; b = t;
+    lgNs += LGR;
+  }
+  if (tail) {
+    if (tail == 3) stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
+    else if (tail == 2) stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
+    else stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
+    __syncthreads();
+    Cx<R>* t = a; a = b; b = t;
+  }
+  return a;
 }
 
 // Transforms nb sequences held (unpadded) in `a`; `b` is scratch of the same
@@ -142,31 +171,10 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
 template <typename R, int S>
 MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
                        const Cx<R>* __restrict__ tw, int lgtw) {
-  int lgNs = 0;
-  int rem = lgn;
-  // pass list: radix-16 while >= 4 bits remain, then one 8/4/2 pass
-  const int n16 = rem >> 2;
-  const int tail = rem & 3;
-  const int npass = n16 + (tail ? 1 : 0);
-  int p = 0;
-  for (int q = 0; q < n16; ++q, ++p) {
-    stockham_pass<R, 16, 4, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw, lgtw);
-    __syncthreads();
-    Cx<R>* t = a; a = b; b = t;
-    lgNs += 4;
-  }
-  if (tail == 3) {
-    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
-  } else if (tail == 2) {
-    stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
-  } else if (tail == 1) {
-    stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
-  }
-  if (tail) {
-    __syncthreads();
-    Cx<R>* t = a; a = b; b = t;
-  }
-  return a;
+  const int radix = fft_radix(lgn, nb, blockDim.x);
+  if (radix == 16) return fft_passes<R, 16, 4, S>(a, b, lgn, nb, stride, tw, lgtw);
+  if (radix == 8) return fft_passes<R, 8, 3, S>(a, b, lgn, nb, stride, tw, lgtw);
+  return fft_passes<R, 4, 2, S>(a, b, lgn, nb, stride, tw, lgtw);
 }
 
 // e^{-2 pi i k / 2^lg} from the 4096-entry global table
@@ -175,11 +183,23 @@ MRM_D Cx<R> twiddle(const Cx<R>* __restrict__ tw, int k, int lg) {
   return tw[k << (kTwLog - lg)];
 }
 
-// Stages tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, from the global table.
-template <typename R>
-MRM_D void stage_twiddles(Cx<R>* __restrict__ tw_s, const Cx<R>* __restrict__ tw, int lg) {
+// Fills tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, with sincospi (accurate to
+// about one ulp; no memory round trip).
+MRM_D void make_twiddles(Cx<float>* __restrict__ tw_s, int lg) {
   const int n = 1 << lg;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) tw_s[k] = tw[k << (kTwLog - lg)];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float s, c;
+    sincospif(-2.0f * (float)k / (float)n, &s, &c);
+    tw_s[k] = Cx<float>{c, s};
+  }
+}
+MRM_D void make_twiddles(Cx<double>* __restrict__ tw_s, int lg) {
+  const int n = 1 << lg;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * (double)k / (double)n, &s, &c);
+    tw_s[k] = Cx<double>{c, s};
+  }
 }
 
 // programmatic dependent launch (sm_90+): let the next kernel in the stream

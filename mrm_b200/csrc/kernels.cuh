@@ -101,8 +101,11 @@ struct GrainIn {
 template <int STAGE, bool STATS>
 __host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STATS) ? 32 * kNPart : 1; }
 
+template <typename R>
+__host__ __device__ constexpr int min_blocks() { return sizeof(R) == sizeof(float) ? 2 : 1; }
+
 template <typename R, int STAGE, bool STATS, int GPT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict__ runs,
+__global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDev<R>* __restrict__ runs,
                                                     const Task* __restrict__ tasks,
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags, double* __restrict__ part) {
@@ -128,7 +131,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
   __shared__ double sred[stats_slots<STAGE, STATS>()];
 
   // ---------------- static inputs (not written by the previous kernel) ----------------
-  if (demag) stage_twiddles(tws, tw, lgpx);
+  if (demag) make_twiddles(tws, lgpx);
   const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
   const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
   const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
@@ -150,10 +153,32 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
     if (lcol) g[q].cl = L.lcol[n];
   }
 
+  // predictor: Philox thermal normals (llg.f90:1083 h = H + hthm/sqrt(dt); the
+  // corrector reuses them, :1262-1266), drawn for the step counter read before
+  // the wait and redrawn only if the previous kernel advanced it meanwhile
+  const long long step_guess = rd.step + istep;
+  auto draw = [&](long long st) {
+    const R tfac = (R)sqrt(L.temperature / rd.dt);
+#pragma unroll
+    for (int q = 0; q < GPT; ++q) {
+      const int idx = threadIdx.x + q * BLOCK;
+      if (idx >= ngr) continue;
+      const int row = idx / nx, i = idx - row * nx;
+      const int n = (row0 + row) * nx + i;
+      R gn[3];
+      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)st,
+                      (unsigned long long)n, gn);
+      const R s = g[q].pb.w * tfac;
+      g[q].ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
+    }
+  };
+  if (STAGE == kPred && thermal) draw(step_guess);
+
   // ---------------- wait for the previous kernel's results ----------------
   pdl_wait();
-  const long long step = rd.step + istep;
+  const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
   if (!(flags & kFlagForce) && step >= rd.step_end) return;
+  if (STAGE == kPred && thermal && step != step_guess) draw(step);
 
   // ---------------- dynamic per-grain inputs ----------------
 #pragma unroll
@@ -183,23 +208,6 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
     if (ucol) g[q].vu = ((STAGE == kCorr) ? Lu->mp : Lu->m)[n];
     if (lcol) g[q].vl = ((STAGE == kCorr) ? Ll->mp : Ll->m)[n];
   }
-  // predictor: Philox thermal normals while the loads above are in flight
-  // (llg.f90:1083 h = H + hthm/sqrt(dt); the corrector reuses them, :1262-1266)
-  if (STAGE == kPred && thermal) {
-    const R tfac = (R)sqrt(L.temperature / rd.dt);
-#pragma unroll
-    for (int q = 0; q < GPT; ++q) {
-      const int idx = threadIdx.x + q * BLOCK;
-      if (idx >= ngr) continue;
-      const int row = idx / nx, i = idx - row * nx;
-      const int n = (row0 + row) * nx + i;
-      R gn[3];
-      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step,
-                      (unsigned long long)n, gn);
-      const R s = g[q].pb.w * tfac;
-      g[q].ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
-    }
-  }
 
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
   Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
@@ -214,7 +222,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
         if (idx < tot) {
           const int s = idx >> lgM, k = idx & (M - 1);
           const int row = s / 3, comp = s - 3 * row;
-          const Cx<R>* X = rd.spec + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
+          const Cx<R>* X = rd.spech + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
           xk[u] = X[k];
           xm[u] = X[M - k];
         }
@@ -430,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
     const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
     // X[k] = e - i w^k o,  w = e^{-2 pi i / px}
     const Cx<R> wo = cmul(tws[k & (two_m - 1)], o);
-    rd.spec[((size_t)(l * 3 + comp) * ny + row0 + row) * ph + k] = csub(e, cmul_i(wo, (R)1));
+    rd.specx[((size_t)(l * 3 + comp) * ph + k) * ny + row0 + row] = csub(e, cmul_i(wo, (R)1));
   }
 }
 
@@ -439,8 +447,13 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(const RunDev<R>* __restrict_
 // PACKED: tensor stored as one real per (k, 0<=ky<=py/2) and component (the
 // parity of each component restores the rest); otherwise the full complex
 // tensor spectrum [k][pair][9][py] is used (FP64 runs).
+// packed tensor slice of a column task staged in shared memory up to this size
+constexpr int kTensSliceBytes = 48 * 1024;
+template <typename R>
+MRM_HD bool tens_slice_fits(int reals) { return (size_t)reals * sizeof(R) <= (size_t)kTensSliceBytes; }
+
 template <typename R, bool PACKED, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict__ runs,
+__global__ void __launch_bounds__(BLOCK, min_blocks<R>()) col_kernel(const RunDev<R>* __restrict__ runs,
                                                     const Task* __restrict__ tasks,
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags) {
@@ -458,28 +471,20 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
   Cx<R>* A = tws + py;
   Cx<R>* B = A + nseq * cs;
 
-  // static inputs: twiddles and (single layer pair) the tensor values of this thread's bins
-  stage_twiddles(tws, tw, lgpy);
-  constexpr int kPre = 2;
-  const bool pre = PACKED && nl == 1 && nc * py <= kPre * BLOCK;
-  R tpre[kPre][9];
-  if (pre) {
-#pragma unroll
-    for (int e = 0; e < kPre; ++e) {
-      const int idx = threadIdx.x + e * BLOCK;
-      if (idx < nc * py) {
-        const int c = idx / py, ky = idx - c * py;
-        const int kyh = ky > (py >> 1) ? py - ky : ky;
-        const R* Tp = rd.tens + (size_t)(k0 + c) * 9 * pyh;
-#pragma unroll
-        for (int cc = 0; cc < 9; ++cc) tpre[e][cc] = __ldg(Tp + cc * pyh + kyh);
-      }
-    }
+  // static inputs: twiddles and this task's packed tensor slice (when it fits)
+  make_twiddles(tws, lgpy);
+  const int npair = nl * nl;
+  const int tslice = nc * npair * 9 * pyh;  // reals
+  const bool tsm = PACKED && tens_slice_fits<R>(tslice);
+  R* Ts = reinterpret_cast<R*>(B + nseq * cs);
+  if (tsm) {
+    const R* src = rd.tens + (size_t)k0 * npair * 9 * pyh;  // columns k0.. are contiguous
+    for (int q = threadIdx.x; q < tslice; q += BLOCK) Ts[q] = __ldg(src + q);
   }
   pdl_wait();
   if (!(flags & kFlagForce) && rd.step + istep >= rd.step_end) return;
 
-  // batched strided loads of the columns (rows >= ny are the zero padding)
+  // batched, coalesced loads of the columns (column-major M^; rows >= ny are the zero padding)
   const int tot = nseq * py;
   for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
     Cx<R> v[4];
@@ -488,19 +493,15 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
       const int idx = base + u * BLOCK;
       v[u] = Cx<R>{(R)0, (R)0};
       if (idx < tot) {
-        const int c = idx % nc, rest = idx / nc;
-        const int j = rest % py, lc = rest / py;
-        if (j < ny) v[u] = rd.spec[((size_t)lc * ny + j) * ph + k0 + c];
+        const int j = idx & (py - 1), s = idx >> lgpy;  // s = c*nl*3 + lc
+        const int c = s / (nl * 3), lc = s - c * nl * 3;
+        if (j < ny) v[u] = rd.specx[((size_t)lc * ph + k0 + c) * ny + j];
       }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int idx = base + u * BLOCK;
-      if (idx < tot) {
-        const int c = idx % nc, rest = idx / nc;
-        const int j = rest % py, lc = rest / py;
-        A[(c * nl * 3 + lc) * cs + j] = v[u];
-      }
+      if (idx < tot) A[(idx >> lgpy) * cs + (idx & (py - 1))] = v[u];
     }
   }
   __syncthreads();
@@ -508,9 +509,7 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
   Cx<R>* G = (F == A) ? B : A;
 
   // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
-  const int npair = nl * nl;
-  int e = 0;
-  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK, ++e) {
+  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK) {
     const int c = idx / py, ky = idx - c * py;
     for (int ko = 0; ko < nl; ++ko) {
       Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
@@ -521,16 +520,11 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
         if constexpr (PACKED) {
           const bool upper = ky > (py >> 1);
           const int kyh = upper ? py - ky : ky;
-          const R* Tp = rd.tens + ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * pyh;
+          const size_t off = ((size_t)c * npair + ks * nl + ko) * 9 * pyh;
+          const R* Tp = tsm ? Ts + off : rd.tens + (size_t)k0 * npair * 9 * pyh + off;
           R tv[9];
-          if (pre) {
-            // e < kPre here: `pre` implies at most kPre bins per thread
 #pragma unroll
-            for (int cc = 0; cc < 9; ++cc) tv[cc] = (e == 0) ? tpre[0][cc] : tpre[kPre - 1][cc];
-          } else {
-#pragma unroll
-            for (int cc = 0; cc < 9; ++cc) tv[cc] = __ldg(Tp + cc * pyh + kyh);
-          }
+          for (int cc = 0; cc < 9; ++cc) tv[cc] = Tp[cc * pyh + kyh];
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -564,7 +558,7 @@ __global__ void __launch_bounds__(BLOCK) col_kernel(const RunDev<R>* __restrict_
   for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
     const int c = idx % nc, rest = idx / nc;
     const int j = rest % ny, lc = rest / ny;
-    rd.spec[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
+    rd.spech[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
   }
 }
 

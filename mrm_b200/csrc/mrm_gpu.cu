@@ -66,7 +66,8 @@ struct mrm_gpu {
   mrm_geom g{};
   int px = 0, py = 0, lgpx = 0, lgpy = 0, nl = 0;
   LayerBufs L[MRM_MAX_LAYERS];
-  void* spec = nullptr;
+  void* spech = nullptr;
+  void* specx = nullptr;
   void* tens = nullptr;
   bool tensor_ready = false;
   bool demag = true;
@@ -214,9 +215,10 @@ int rows_per_task(const mrm_gpu* r) {
   if (r->g.nx >= kBlock) return 1;
   return std::max(1, std::min(r->g.ny, kBlock / std::max(1, r->g.nx)));
 }
+// columns per column task: enough sequences for one radix-16 butterfly per thread
 int cols_per_task(const mrm_gpu* r) {
   int ph = r->px / 2 + 1;
-  return std::max(1, std::min(ph, 2048 / (3 * r->nl * r->py)));
+  return std::max(1, std::min(ph, kBlock * 16 / (3 * r->nl * r->py)));
 }
 size_t cx_bytes(int prec) { return 2 * relem(prec); }
 // shared memory: twiddle table of the transform length + two padded ping-pong buffers
@@ -224,7 +226,12 @@ size_t row_smem(const mrm_gpu* r, int prec) {
   return ((size_t)r->px + 2ull * rows_per_task(r) * 3 * fft_stride(r->px / 2)) * cx_bytes(prec);
 }
 size_t col_smem(const mrm_gpu* r, int prec) {
-  return ((size_t)r->py + 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py)) * cx_bytes(prec);
+  size_t b = ((size_t)r->py + 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py)) * cx_bytes(prec);
+  if (prec == MRM_FP32) {  // packed tensor slice (kernels.cuh: tens_slice_fits)
+    const int reals = cols_per_task(r) * r->nl * r->nl * 9 * (r->py / 2 + 1);
+    if (tens_slice_fits<float>(reals)) b += (size_t)reals * sizeof(float);
+  }
+  return b;
 }
 // row-kernel shape: grains per thread x block size
 int row_config(int max_grains) {
@@ -293,7 +300,8 @@ RunDev<R> make_desc(const mrm_gpu* r) {
   d.active = r->active ? 1 : 0;
   d.row_task0 = r->row_task0;
   d.nrow_tasks = r->nrow_tasks;
-  d.spec = static_cast<Cx<R>*>(r->spec);
+  d.spech = static_cast<Cx<R>*>(r->spech);
+  d.specx = static_cast<Cx<R>*>(r->specx);
   d.tens = static_cast<const R*>(r->tens);
   for (int l = 0; l < r->nl; ++l) {
     const LayerBufs& b = r->L[l];
@@ -625,7 +633,9 @@ int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
   const int ph = r->px / 2 + 1, pyh = r->py / 2 + 1;
-  int rc = dmalloc(errp, &r->spec, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
+  int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
+  if (rc) return rc;
+  rc = dmalloc(errp, &r->specx, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
   if (rc) return rc;
   (void)pyh;
   rc = dmalloc(errp, &r->tens, tensor_bytes(r));
@@ -646,7 +656,8 @@ int run_alloc(mrm_gpu* r) {
 }
 
 void run_free(mrm_gpu* r) {
-  dfree(r->spec);
+  dfree(r->spech);
+  dfree(r->specx);
   dfree(r->tens);
   for (int l = 0; l < MRM_MAX_LAYERS; ++l) {
     LayerBufs& b = r->L[l];
@@ -664,7 +675,7 @@ int64_t footprint(const mrm_geom& g) {
   const size_t re = g.precision == MRM_FP64 ? 8 : 4;
   const int64_t n = (int64_t)g.nx * g.ny, nl = g.n_lay;
   const int64_t ph = px / 2 + 1, pyh = py / 2 + 1;
-  int64_t b = nl * 3 * g.ny * ph * 2 * re;
+  int64_t b = 2 * nl * 3 * g.ny * ph * 2 * re;
   b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * pyh * 4;
   b += nl * n * (8 * 4 * re + 4 * 8);
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
