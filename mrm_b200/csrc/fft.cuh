@@ -183,6 +183,13 @@ MRM_D Cx<R> twiddle(const Cx<R>* __restrict__ tw, int k, int lg) {
   return tw[k << (kTwLog - lg)];
 }
 
+// Stages tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, from the global table.
+template <typename R>
+MRM_D void stage_twiddles(Cx<R>* __restrict__ tw_s, const Cx<R>* __restrict__ tw, int lg) {
+  const int n = 1 << lg;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) tw_s[k] = tw[k << (kTwLog - lg)];
+}
+
 // Fills tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, with sincospi (accurate to
 // about one ulp; no memory round trip).
 MRM_D void make_twiddles(Cx<float>* __restrict__ tw_s, int lg) {

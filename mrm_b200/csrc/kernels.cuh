@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDe
   __shared__ double sred[stats_slots<STAGE, STATS>()];
 
   // ---------------- static inputs (not written by the previous kernel) ----------------
-  if (demag) make_twiddles(tws, lgpx);
+  if (demag) stage_twiddles(tws, tw, lgpx);
   const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
   const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
   const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) col_kernel(const RunDe
   Cx<R>* B = A + nseq * cs;
 
   // static inputs: twiddles and this task's packed tensor slice (when it fits)
-  make_twiddles(tws, lgpy);
+  stage_twiddles(tws, tw, lgpy);
   const int npair = nl * nl;
   const int tslice = nc * npair * 9 * pyh;  // reals
   const bool tsm = PACKED && tens_slice_fits<R>(tslice);
