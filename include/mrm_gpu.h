@@ -123,6 +123,10 @@ int mrm_gpu_build_tensor(mrm_gpu* h);
 int mrm_gpu_upload_tensor(mrm_gpu* h, const double* n2d, int nx_fft, int ny_fft);
 /* Copies the device-built real-space tensor back (for the tensor cache file). */
 int mrm_gpu_download_tensor(mrm_gpu* h, double* n2d);
+/* Copies the resident tensor spectrum of `src` into `dst` (same device, FFT
+ * grid, layer stack and precision): runs of one geometry share a tensor
+ * without rebuilding it. */
+int mrm_gpu_copy_tensor(mrm_gpu* dst, const mrm_gpu* src);
 /* FFT grid of the handle (nx_fft, ny_fft). */
 int mrm_gpu_fft_grid(const mrm_gpu* h, int* nx_fft, int* ny_fft);
 /* Diagnostic of the packed tensor spectrum: largest dropped (wrong-parity)
@@ -136,6 +140,15 @@ int mrm_gpu_set_demag(mrm_gpu* h, int on);
  * (set_fld / get_appl, src/applied.f90:263-317,871-883). */
 int mrm_gpu_set_uniform_field(mrm_gpu* h, int layer, const double hdir[3], double t_start,
                               double t_end, double s_start, double s_end, double scale);
+
+/* Uniform applied field of `layer` with a time function (set_fld with func1,
+ * applied.f90:263-297,328-377,866-869):
+ * h_app(t) = (amp*f(t) + dc)*scale*hdir, f = 1 sin(t*gamma+phase),
+ * 2 cos(t*gamma+phase), 3 exp(t*gamma+phase), 4 STE (trapezoidal square wave
+ * of period gamma and rise time param), 5 NEW (exponential pulse train). */
+int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int func, double amp,
+                               double gamma, double phase, double param, double duty,
+                               double moddepth, double dc, double scale);
 
 /* Thermal (Brown) field of `layer` at `temperature` K (get_thermal,
  * field.f90:397-436).  The normals come from a counter-based Philox4x64-10
@@ -190,11 +203,17 @@ int mrm_batch_remove(mrm_batch* b, mrm_gpu* run);
 int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active);
 /* Advances every active run by up to nsteps Heun steps (llg_type -3). */
 int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type);
-/* Stats of each listed run after its last step in the preceding mrm_batch_step. */
+/* Stats of each listed run at its last executed step that ended an
+ * mrm_batch_step / mrm_batch_enqueue call (a run whose budget ends inside a
+ * call keeps the stats of its previous call: schedule calls so that budgets
+ * end on call boundaries). */
 int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats* out);
 /* Enqueues like mrm_batch_step without waiting (stats via mrm_batch_stats). */
 int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type);
 int mrm_batch_stream(const mrm_batch* b, void** stream);
+/* Resident blocks per SM of the row and column kernels of this batch (0 if
+ * no step was taken yet): out[0] = row, out[1] = column. */
+int mrm_batch_occupancy(mrm_batch* b, int* out2);
 /* Device bytes a run of this geometry holds (admission by HBM footprint). */
 int64_t mrm_run_footprint(const mrm_geom* geom);
 /* Free / total device memory in bytes. */

@@ -32,7 +32,8 @@ EXPORTS = [
     "mrm_gpu_step", "mrm_gpu_enqueue_steps", "mrm_gpu_read_stats", "mrm_gpu_stream", "mrm_gpu_profile",
     "mrm_batch_enqueue", "mrm_batch_stream", "mrm_batch_create", "mrm_batch_destroy", "mrm_batch_last_error",
     "mrm_batch_add", "mrm_batch_remove", "mrm_batch_set_run", "mrm_batch_step", "mrm_batch_stats",
-    "mrm_run_footprint", "mrm_device_memory",
+    "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
+    "mrm_gpu_set_field_function",
 ]
 
 
@@ -114,6 +115,9 @@ def load(path: str = LIB_PATH):
         "mrm_batch_step": ([vp, i, i], i),
         "mrm_batch_stats": ([vp, i, P(vp), vp], i),
         "mrm_run_footprint": ([P(Geom)], i64),
+        "mrm_gpu_copy_tensor": ([vp, vp], i),
+        "mrm_gpu_set_field_function": ([vp, i, pd, i, d, d, d, d, d, d, d, d], i),
+        "mrm_batch_occupancy": ([vp, P(i)], i),
         "mrm_device_memory": ([i, P(i64), P(i64)], i),
     }
     for name, (args, res) in sig.items():

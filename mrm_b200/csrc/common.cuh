@@ -66,6 +66,8 @@ struct LayerDev {
   const R* lcol;
   double hdir[3];
   double t_start, t_end, s_start, s_end, scale;
+  int func;  // 0 linear ramp; 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW (applied.f90:328-377)
+  double amp, fgamma, phase, param, duty, moddepth, dc;
   double temperature;
   double gamma;
   int thermal;
@@ -86,6 +88,7 @@ struct RunDev {
   long long step_end;      // the run advances while step < step_end
   unsigned long long seed;
   int active;
+  int stats_ok;            // set by the advance kernel: the chunk's last step was executed
   int row_task0, nrow_tasks;  // range of this run's row tasks (stats partials)
   Cx<R>* spech;            // H^ half spectra, row-major [nl][3][ny][px/2+1] (column kernel -> row kernel)
   Cx<R>* specx;            // M^ half spectra, column-major [nl][3][px/2+1][ny] (row kernel -> column kernel)

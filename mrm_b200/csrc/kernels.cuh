@@ -35,9 +35,44 @@ MRM_D void cross3(R ax, R ay, R az, R bx, R by, R bz, R& cx, R& cy, R& cz) {
   cz = ax * by - ay * bx;
 }
 
+// funct (applied.f90:328-377); Fortran mod(x,g) = x - int(x/g)*g = fmod
+MRM_D double funct(int f, double t, double g, double phase, double param, double duty,
+                   double moddepth) {
+  if (f == 1) return sin(t * g + phase);
+  if (f == 2) return cos(t * g + phase);
+  if (f == 3) return exp(t * g + phase);
+  if (f == 5) {  // NEW
+    double x = g / param;
+    const double y = exp(duty * x), w = exp(x);
+    x = t + phase;
+    if (x < 0.0) x = x + g * (1.0 + (double)(long long)fabs(x / g));
+    x = fmod(x, g);
+    if (x > duty * g) {
+      x = exp((g - x) / param);
+      return 1.0 - moddepth + x * (y - 1.0) * moddepth / (w - 1.0);
+    }
+    x = exp(-x / param);
+    return 1.0 + x * (y - w) * moddepth / (w - 1.0);
+  }
+  if (f == 4) {  // STE: trapezoidal square wave of period g, rise time param
+    double x = t + phase;
+    if (x < 0.0) x = x + g * (1.0 + (double)(long long)fabs(x / g));
+    x = fmod(x, g);
+    if (x < 0.5 * param) return 2.0 * x / param;
+    if (x < 0.5 * (g - param)) return 1.0;
+    if (x < 0.5 * (g + param)) return (g - 2.0 * x) / param;
+    if (x < g - 0.5 * param) return -1.0;
+    return 2.0 * (x - g) / param;
+  }
+  return 0.0;
+}
+
+// time scale of a layer's uniform field (applied.f90:866-883; set_fld folds
+// a constant ramp into `scale`, :309-312)
 template <typename R>
 MRM_D double ramp(const LayerDev<R>& L, double t) {
-  // applied.f90:871-872 (linear ramp of the time scale) with set_fld's folded scale
+  if (L.func != 0)
+    return (L.amp * funct(L.func, t, L.fgamma, L.phase, L.param, L.duty, L.moddepth) + L.dc) * L.scale;
   double u = (t - L.t_start) / (L.t_end - L.t_start);
   u = fmax(0.0, fmin(1.0, u));
   return ((L.s_end - L.s_start) * u + L.s_start) * L.scale;
@@ -573,6 +608,7 @@ __global__ void advance_kernel(RunDev<R>* runs, int nruns, int k) {
   if (!rd.active) return;
   long long left = rd.step_end - rd.step;
   if (left < 0) left = 0;
+  rd.stats_ok = left >= k ? 1 : 0;
   rd.step += (left < k) ? left : k;
 }
 
@@ -601,7 +637,7 @@ __global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __
   const int r = blockIdx.x;
   if (r >= nruns) return;
   const RunDev<R>& rd = runs[r];
-  if (!rd.active) return;
+  if (!rd.active || !rd.stats_ok) return;  // keep the stats of the run's last stats step
   for (int l = 0; l < rd.nl; ++l) {
     double rec[kNPart];
 #pragma unroll

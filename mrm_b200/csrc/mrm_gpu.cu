@@ -52,6 +52,8 @@ struct LayerBufs {
   void* lcol = nullptr;
   double hdir[3] = {0, 0, 0};
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
+  int func = 0;
+  double amp = 0, fgamma = 0, phase = 0, param = 0, duty = 0, moddepth = 0, dc = 0;
   double temperature = 0.0, gamma = 1.76e7;
   int thermal = 0;
 };
@@ -333,6 +335,14 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.s_start = b.s_start;
     o.s_end = b.s_end;
     o.scale = b.scale;
+    o.func = b.func;
+    o.amp = b.amp;
+    o.fgamma = b.fgamma;
+    o.phase = b.phase;
+    o.param = b.param;
+    o.duty = b.duty;
+    o.moddepth = b.moddepth;
+    o.dc = b.dc;
     o.temperature = b.temperature;
     o.gamma = b.gamma;
     o.thermal = b.thermal;
@@ -1120,6 +1130,32 @@ int mrm_gpu_download_tensor(mrm_gpu* h, double* n2d) {
   return rc;
 }
 
+int mrm_gpu_copy_tensor(mrm_gpu* dst, const mrm_gpu* src) {
+  if (!dst || !src) return MRM_ERR_ARG;
+  std::string* errp = &dst->err;
+  if (!src->tensor_ready) return set_err(errp, MRM_ERR_STATE, "source run has no tensor");
+  if (dst->px != src->px || dst->py != src->py || dst->nl != src->nl ||
+      dst->g.precision != src->g.precision || dst->eng->dev != src->eng->dev)
+    return set_err(errp, MRM_ERR_ARG, "tensor geometry differs");
+  for (int l = 0; l < dst->nl; ++l)
+    if (dst->g.dz[l] != src->g.dz[l] || dst->g.il_space[l] != src->g.il_space[l])
+      return set_err(errp, MRM_ERR_ARG, "layer stack differs");
+  if (dst->g.dx != src->g.dx || dst->g.dy != src->g.dy || dst->g.boundary != src->g.boundary ||
+      dst->g.num_images != src->g.num_images)
+    return set_err(errp, MRM_ERR_ARG, "cell size or boundary differs");
+  CK(cudaSetDevice(dst->eng->dev));
+  CK(cudaStreamSynchronize(src->eng->st));
+  CK(cudaMemcpyAsync(dst->tens, src->tens, tensor_bytes(dst), cudaMemcpyDeviceToDevice, dst->eng->st));
+  CK(cudaStreamSynchronize(dst->eng->st));
+  dst->tensor_ready = true;
+  dst->tensor_resid = src->tensor_resid;
+  dst->tensor_kept = src->tensor_kept;
+  dst->spec_valid = false;
+  dst->eng->tables_dirty = true;
+  dst->eng->desc_dirty = true;
+  return MRM_OK;
+}
+
 int mrm_gpu_fft_grid(const mrm_gpu* h, int* nx_fft, int* ny_fft) {
   if (!h) return MRM_ERR_ARG;
   if (nx_fft) *nx_fft = h->px;
@@ -1155,11 +1191,35 @@ int mrm_gpu_set_uniform_field(mrm_gpu* h, int layer, const double hdir[3], doubl
   b.s_start = s_start;
   b.s_end = s_end;
   b.scale = scale;
+  b.func = 0;
   if (b.s_start == b.s_end) {  // applied.f90:309-312
     b.scale *= b.s_start;
     b.s_start = 1.0;
     b.s_end = 1.0;
   }
+  h->eng->desc_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int func, double amp,
+                               double gamma, double phase, double param, double duty,
+                               double moddepth, double dc, double scale) {
+  if (!h || !hdir) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  if (func < 1 || func > 5) return set_err(&h->err, MRM_ERR_ARG, "unknown time function %d", func);
+  if ((func == 4 || func == 5) && !(gamma > 0 && param > 0))
+    return set_err(&h->err, MRM_ERR_ARG, "STE/NEW need a period and a time constant > 0");
+  LayerBufs& b = h->L[layer];
+  for (int a = 0; a < 3; ++a) b.hdir[a] = hdir[a];
+  b.func = func;
+  b.amp = amp;
+  b.fgamma = gamma;
+  b.phase = phase;
+  b.param = param;
+  b.duty = std::max(0.0, std::min(1.0, duty));          // applied.f90:276-277
+  b.moddepth = std::max(0.0, std::min(1.0, moddepth));
+  b.dc = dc;
+  b.scale = scale;
   h->eng->desc_dirty = true;
   return MRM_OK;
 }
@@ -1522,6 +1582,33 @@ int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats
     std::memcpy(&out[i], e->h_stats + runs[i]->slot, sizeof(StatsDev));
   }
   return MRM_OK;
+}
+
+}  // extern "C"
+
+template <typename R>
+static int occ_t(Engine* e, int* out2) {
+  std::string* errp = &e->err;
+  int a = 0, b = 0;
+  if (e->rowcfg == 0)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256>, 256, e->smem_row));
+  else if (e->rowcfg == 1)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 256>, 256, e->smem_row));
+  else
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 512>, 512, e->smem_row));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, col_kernel<R, sizeof(R) == 4, kBlock>, kBlock, e->smem_col));
+  out2[0] = a;
+  out2[1] = b;
+  return MRM_OK;
+}
+
+extern "C" {
+
+int mrm_batch_occupancy(mrm_batch* b, int* out2) {
+  if (!b || !out2) return MRM_ERR_ARG;
+  Engine* e = &b->eng;
+  cudaSetDevice(e->dev);
+  return e->prec == MRM_FP64 ? occ_t<double>(e, out2) : occ_t<float>(e, out2);
 }
 
 int64_t mrm_run_footprint(const mrm_geom* geom) {

@@ -61,7 +61,12 @@ class _RunMixin:
                 if cpl is not None:
                     idx, gr, cf = i32(cpl[0]), i32(cpl[1]), f64(cpl[2])
                     self._check(L.mrm_gpu_upload_interlayer(self.h, l, side, iptr(idx), iptr(gr), fptr(cf)))
-            self.set_uniform_field(l, lay.hdir, lay.t_start, lay.t_end, lay.s_start, lay.s_end, lay.scale)
+            if getattr(lay, "func", 0):
+                self.set_field_function(l, lay.hdir, lay.func, lay.amp, lay.fgamma, lay.phase,
+                                        lay.param, lay.duty, lay.moddepth, lay.dc, lay.scale)
+            else:
+                self.set_uniform_field(l, lay.hdir, lay.t_start, lay.t_end, lay.s_start, lay.s_end,
+                                       lay.scale)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
         if medium.m0 is not None:
             for l, m in enumerate(medium.m0):
@@ -99,6 +104,13 @@ class _RunMixin:
         d = f64(hdir)
         self._check(_lib.load().mrm_gpu_set_uniform_field(self.h, layer, fptr(d), t_start, t_end,
                                                           s_start, s_end, scale))
+
+    def set_field_function(self, layer, hdir, func, amp, gamma, phase=0.0, param=0.0, duty=0.0,
+                           moddepth=0.0, dc=0.0, scale=1.0):
+        d = f64(hdir)
+        self._check(_lib.load().mrm_gpu_set_field_function(self.h, layer, fptr(d), int(func), amp,
+                                                           gamma, phase, param, duty, moddepth,
+                                                           dc, scale))
 
     def set_thermal(self, layer, on, temperature, seed):
         self._check(_lib.load().mrm_gpu_set_thermal(self.h, layer, 1 if on else 0,

@@ -64,6 +64,16 @@ class Layer:
     scale: float = 1.0
     temperature: float = 0.0
     thermal: bool = False
+    # time function of the uniform field (applied.f90:328-377): 0 = linear ramp,
+    # 1 SIN, 2 COS, 3 EXP, 4 STE (trapezoidal square wave), 5 NEW
+    func: int = 0
+    amp: float = 0.0
+    fgamma: float = 0.0
+    phase: float = 0.0
+    param: float = 0.0
+    duty: float = 0.0
+    moddepth: float = 0.0
+    dc: float = 0.0
 
     @property
     def N(self) -> int:

@@ -1,0 +1,211 @@
+"""Served form: continuous batching of M(H)-loop and write-pattern requests.
+
+Requests arrive over time (`Request.arrival`, seconds after the stream
+start).  The server keeps one Batch resident on the GPU and loops:
+
+1. move requests whose arrival time has passed into the admission queue;
+2. admit queued requests first-come-first-served while their device
+   footprint (state, parameters, spectra, tensor) fits the HBM budget; a
+   request's tensor spectrum is copied device-to-device from a per-geometry
+   template instead of being rebuilt;
+3. advance every active run by K Heun steps in one launch sequence, with
+   K = min(chunk, the smallest remaining budget), so that budgets end on
+   call boundaries and each run's reductions describe its own last step;
+4. record each run's M(H) sample (time, applied field, m.h), retire finished
+   runs (result + latency = finish - arrival) and free their memory.
+
+Requests that arrive while others are on the GPU are admitted as soon as
+memory frees up and join the next launch; a run's trajectory does not depend
+on its neighbours (each run's kernels read only its own data), which the
+tests check bit for bit against the same request run alone.
+"""
+from __future__ import annotations
+
+import collections
+import math
+import time
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+
+from . import _lib
+from .workloads import DT, Request
+
+
+class _Active:
+    __slots__ = ("req", "run", "fp", "admitted", "remaining", "samples")
+
+    def __init__(self, req, run, fp, admitted):
+        self.req = req
+        self.run = run
+        self.fp = fp
+        self.admitted = admitted
+        self.remaining = req.steps
+        self.samples = []
+
+
+def applied_field(req: Request, t: float) -> float:
+    """Signed magnitude of the request's uniform field along its direction."""
+    if req.kind == "mh":
+        u = min(1.0, max(0.0, t / (req.steps * DT)))
+        return 20000.0 - 40000.0 * u
+    return 12000.0  # write: STE amplitude; the sign follows the square wave
+
+
+def coercivity(h, mh):
+    h, mh = np.asarray(h, float), np.asarray(mh, float)
+    hc = mr = None
+    for k in range(1, len(h)):
+        if hc is None and mh[k - 1] > 0 >= mh[k]:
+            hc = -(h[k - 1] + (h[k] - h[k - 1]) * mh[k - 1] / (mh[k - 1] - mh[k]))
+        if mr is None and h[k - 1] > 0 >= h[k]:
+            mr = mh[k - 1] + (mh[k] - mh[k - 1]) * h[k - 1] / (h[k - 1] - h[k])
+    return hc, mr
+
+
+class Server:
+    """Continuous-batching scheduler over a Batch-like backend.
+
+    backend: object with add(medium, dt, steps, thermal_seed, tensor_from) ->
+    run, remove(run), step(k), stats(runs), footprint(medium) -> bytes,
+    memory() -> (free, total); defaults to the GPU Batch.
+    """
+
+    def __init__(self, backend=None, precision: int = _lib.FP32, device: int = 0,
+                 hbm_fraction: float = 0.8, hbm_budget: Optional[int] = None, chunk: int = 500,
+                 max_active: int = 4096, keep_state: bool = False,
+                 clock: Callable[[], float] = time.perf_counter,
+                 sleep: Callable[[float], None] = time.sleep):
+        if backend is None:
+            backend = GpuBackend(precision, device)
+        self.be = backend
+        free, total = backend.memory()
+        self.budget = hbm_budget if hbm_budget is not None else int(free * hbm_fraction)
+        self.chunk = int(chunk)
+        self.max_active = int(max_active)
+        self.keep_state = keep_state
+        self.clock = clock
+        self.sleep = sleep
+        self.used = 0
+        self.templates: Dict[tuple, object] = {}
+
+    def _admit(self, req: Request, med, fp: int, now: float):
+        key = (req.side, req.side)
+        tmpl = self.templates.get(key)
+        run = self.be.add(med, DT, req.steps, req.seed, tmpl)
+        if tmpl is None:
+            self.templates[key] = self.be.make_template(run)
+        return _Active(req, run, fp, now)
+
+    def run(self, requests: List[Request]) -> dict:
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        queue = collections.deque()
+        active: List[_Active] = []
+        results = []
+        t0 = self.clock()
+        calls = 0
+        while pending or queue or active:
+            now = self.clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            # admission, first come first served, by device footprint
+            while queue and len(active) < self.max_active:
+                req = queue[0]
+                med = req.medium()
+                fp = self.be.footprint(med)
+                if active and self.used + fp > self.budget:
+                    break
+                queue.popleft()
+                a = self._admit(req, med, fp, self.clock() - t0)
+                self.used += a.fp
+                active.append(a)
+            if not active:
+                if pending:
+                    self.sleep(max(0.0, min(pending[0].arrival - (self.clock() - t0), 0.01)))
+                continue
+            # one launch sequence for every active run; budgets end on call boundaries
+            k = min(self.chunk, min(a.remaining for a in active))
+            self.be.step(k)
+            calls += 1
+            st = self.be.stats([a.run for a in active])
+            done_t = self.clock() - t0
+            finished = []
+            for a, s in zip(active, st):
+                a.remaining -= k
+                mh = float(np.asarray(s["mms_l"][0]) @ self.be.hdir(a.run))
+                a.samples.append((float(s["t"]), applied_field(a.req, float(s["t"])), mh,
+                                  float(s["mave"][2])))
+                if a.remaining <= 0:
+                    finished.append((a, s))
+            for a, s in finished:
+                ts = np.array(a.samples)
+                res = {"rid": a.req.rid, "kind": a.req.kind, "grains": a.req.grains,
+                       "steps": a.req.steps, "arrival": a.req.arrival, "admitted": a.admitted,
+                       "finished": done_t, "latency": done_t - a.req.arrival,
+                       "final_mave": np.asarray(s["mave"]).tolist(), "step": int(s["step"]),
+                       "samples": len(a.samples)}
+                if a.req.kind == "mh":
+                    hc, mr = coercivity(ts[:, 1], ts[:, 2])
+                    res["hc"], res["mr"] = hc, mr
+                if self.keep_state:
+                    res["m"] = self.be.get_state(a.run)
+                results.append(res)
+                self.be.remove(a.run)
+                self.used -= a.fp
+                active.remove(a)
+        wall = self.clock() - t0
+        lat = np.array([r["latency"] for r in results]) if results else np.zeros(1)
+        gs = sum(r["grains"] * r["steps"] for r in results)
+        return {"results": sorted(results, key=lambda r: r["rid"]), "wall_s": wall,
+                "grain_steps": gs, "grain_steps_per_s": gs / wall if wall > 0 else 0.0,
+                "p50_latency_s": float(np.percentile(lat, 50)),
+                "p99_latency_s": float(np.percentile(lat, 99)), "calls": calls}
+
+
+class GpuBackend:
+    """The GPU Batch behind the server."""
+
+    def __init__(self, precision: int, device: int):
+        from .batch import Batch, device_memory, footprint
+        self._Batch = Batch
+        self._fp = footprint
+        self._mem = device_memory
+        self.precision = precision
+        self.device = device
+        self.batch = Batch(precision, device)
+        self.lib_batch = Batch(precision, device)  # per-geometry tensor templates (never stepped)
+
+    def memory(self):
+        return self._mem(self.device)
+
+    def footprint(self, medium) -> int:
+        return self._fp(medium, self.precision)
+
+    def add(self, medium, dt, steps, seed, template):
+        run = self.batch.add(medium, dt=dt, steps=steps, thermal_seed=seed, tensor_from=template)
+        run._hdir = np.array(medium.layers[0].hdir, float)
+        return run
+
+    def make_template(self, run):
+        t = self.lib_batch.add(run.medium, dt=DT, steps=0, demag=True, tensor_from=run)
+        t.set_run(DT, 0, active=False)
+        return t
+
+    def hdir(self, run):
+        return run._hdir
+
+    def remove(self, run):
+        self.batch.remove(run)
+
+    def step(self, k: int):
+        self.batch.step(k)
+
+    def stats(self, runs):
+        return self.batch.stats(runs)
+
+    def get_state(self, run):
+        return run.get_state(0)
+
+    def close(self):
+        self.batch.close()
+        self.lib_batch.close()

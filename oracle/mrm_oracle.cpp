@@ -454,6 +454,9 @@ struct Layer {
   // schedule: uniform field x linear ramp (applied.f90:863-883)
   double hdir[3] = {0, 0, 0};
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
+  // time function (applied.f90:328-377): 0 none (linear ramp), 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW
+  int func = 0;
+  double amp = 0, fgamma = 0, phase = 0, param = 0, duty = 0, moddepth = 0, dc = 0;
   double temperature = 0.0;
   bool thermal = false;
   MT rng;
@@ -564,8 +567,42 @@ static void compute_demag(Sim* s, int buf) {
   gather_demag(s, s->grid);
 }
 
-// applied field: linear ramp x uniform direction (applied.f90:871-883, set_fld :309-317)
+// funct (applied.f90:328-377); Fortran mod(x,g) = x - int(x/g)*g
+static double funct(int f, double t, double g, double phase, double param, double duty,
+                    double moddepth) {
+  if (f == 1) return std::sin(t * g + phase);
+  if (f == 2) return std::cos(t * g + phase);
+  if (f == 3) return std::exp(t * g + phase);
+  if (f == 5) {  // NEW
+    double x = g / param;
+    const double y = std::exp(duty * x), w = std::exp(x);
+    x = t + phase;
+    if (x < 0.0) x = x + g * (1.0 + (double)(long long)std::fabs(x / g));
+    x = std::fmod(x, g);
+    if (x > duty * g) {
+      x = std::exp((g - x) / param);
+      return 1.0 - moddepth + x * (y - 1.0) * moddepth / (w - 1.0);
+    }
+    x = std::exp(-x / param);
+    return 1.0 + x * (y - w) * moddepth / (w - 1.0);
+  }
+  if (f == 4) {  // STE
+    double x = t + phase;
+    if (x < 0.0) x = x + g * (1.0 + (double)(long long)std::fabs(x / g));
+    x = std::fmod(x, g);
+    if (x < 0.5 * param) return 2.0 * x / param;
+    if (x < 0.5 * (g - param)) return 1.0;
+    if (x < 0.5 * (g + param)) return (g - 2.0 * x) / param;
+    if (x < g - 0.5 * param) return -1.0;
+    return 2.0 * (x - g) / param;
+  }
+  return 0.0;
+}
+
+// applied field scale of one uniform field (applied.f90:866-883, set_fld :289-317)
 static double ramp_scale(const Layer& Ly, double t) {
+  if (Ly.func != 0)
+    return (Ly.amp * funct(Ly.func, t, Ly.fgamma, Ly.phase, Ly.param, Ly.duty, Ly.moddepth) + Ly.dc) * Ly.scale;
   double u = (t - Ly.t_start) / (Ly.t_end - Ly.t_start);
   u = std::max(0.0, std::min(1.0, u));
   return ((Ly.s_end - Ly.s_start) * u + Ly.s_start) * Ly.scale;
@@ -1062,6 +1099,20 @@ int orc_set_uniform_field(void* h, int l, const double* dir, double t_start, dou
     Ly.scale *= Ly.s_start;
     Ly.s_start = 1.0; Ly.s_end = 1.0;
   }
+  return 0;
+}
+
+// uniform field with a time function: scale(t) = (amp*funct(t)+dc)*scale (applied.f90:867-869)
+int orc_set_field_function(void* h, int l, const double* dir, int func, double amp, double g,
+                           double phase, double param, double duty, double moddepth, double dc,
+                           double scale) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  for (int a = 0; a < 3; ++a) Ly.hdir[a] = dir[a];
+  Ly.func = func; Ly.amp = amp; Ly.fgamma = g; Ly.phase = phase; Ly.param = param;
+  Ly.duty = std::max(0.0, std::min(1.0, duty)); Ly.moddepth = std::max(0.0, std::min(1.0, moddepth));
+  Ly.dc = dc; Ly.scale = scale;
   return 0;
 }
 

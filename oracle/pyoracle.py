@@ -51,6 +51,7 @@ def lib():
         L.orc_upload_interlayer.argtypes = [vp, i, i, P(i), P(i), P(d)]
         L.orc_set_uniform_field.argtypes = [vp, i, P(d), d, d, d, d, d]
         L.orc_set_thermal.argtypes = [vp, i, i, d, i, C.c_longlong]
+        L.orc_set_field_function.argtypes = [vp, i, P(d), i, d, d, d, d, d, d, d, d]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
         L.orc_get_field.argtypes = [vp, i, P(d)]
@@ -199,8 +200,12 @@ class OracleSim:
                                     lay.floor_ms, _p(g2ci, C.c_int), _p(g2c, C.c_int), *hxa)
             assert rc == 0
             d = f64(lay.hdir)
-            L.orc_set_uniform_field(self.h, l, _p(d), lay.t_start, lay.t_end, lay.s_start,
-                                    lay.s_end, lay.scale)
+            if getattr(lay, "func", 0):
+                L.orc_set_field_function(self.h, l, _p(d), lay.func, lay.amp, lay.fgamma, lay.phase,
+                                         lay.param, lay.duty, lay.moddepth, lay.dc, lay.scale)
+            else:
+                L.orc_set_uniform_field(self.h, l, _p(d), lay.t_start, lay.t_end, lay.s_start,
+                                        lay.s_end, lay.scale)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
         for l, lay in enumerate(medium.layers):
             for side, cpl in ((0, lay.uhx), (1, lay.lhx)):

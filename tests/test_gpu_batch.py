@@ -1,0 +1,83 @@
+"""Batched and served forms against the plain single-run path (bitwise)."""
+import math
+
+import numpy as np
+import pytest
+
+from mrm_b200 import FP32, FP64, GpuSim, media
+from mrm_b200.batch import Batch
+from mrm_b200.serve import Server
+from mrm_b200.workloads import Request
+
+pytestmark = pytest.mark.gpu
+
+
+def _media():
+    a = media.mh_medium(16, seed=21, temperature=0.0, ramp_s=1e-10)
+    b = media.mh_medium(32, seed=22, temperature=300.0, ramp_s=1e-10)
+    c = media.mh_medium(24, seed=23, temperature=250.0)
+    lay = c.layers[0]
+    lay.func, lay.amp, lay.fgamma, lay.param, lay.scale = 4, 12000.0, 2e-11, 1e-12, 1.0
+    lay.hdir = (math.sin(0.3), 0.0, -math.cos(0.3))
+    return [a, b, c]
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_batch_matches_alone(gpulib, precision):
+    meds = _media()
+    n = 150
+    alone = []
+    for i, m in enumerate(meds):
+        g = GpuSim(m, precision=precision, thermal_seed=5 + i)
+        s = g.step(n, 1e-13)
+        alone.append((g.get_state(0), s))
+        g.close()
+    b = Batch(precision)
+    runs = [b.add(m, dt=1e-13, steps=n, thermal_seed=5 + i) for i, m in enumerate(meds)]
+    b.step(n)
+    st = b.stats(runs)
+    for r, s, (m_alone, s_alone) in zip(runs, st, alone):
+        assert np.array_equal(r.get_state(0), m_alone)
+        assert s["step"] == n and np.array_equal(s["mave"], s_alone["mave"])
+    b.close()
+
+
+def test_batch_step_budgets(gpulib):
+    meds = _media()
+    budgets = [40, 100, 64]
+    b = Batch(FP64)
+    runs = [b.add(m, dt=1e-13, steps=k, thermal_seed=9) for m, k in zip(meds, budgets)]
+    b.step(100)
+    for r, m, k in zip(runs, meds, budgets):
+        g = GpuSim(m, precision=FP64, thermal_seed=9)
+        g.step(k, 1e-13)
+        assert np.array_equal(r.get_state(0), g.get_state(0))
+        assert r.get_time()[1] == k
+        g.close()
+    b.close()
+
+
+def test_tensor_copy_matches_build(gpulib):
+    m = media.mh_medium(32, seed=4)
+    b = Batch(FP32)
+    r1 = b.add(m, steps=50)
+    r2 = b.add(m, steps=50, tensor_from=r1)
+    b.step(50)
+    assert np.array_equal(r1.get_state(0), r2.get_state(0))
+    b.close()
+
+
+def test_served_results_equal_alone(gpulib):
+    reqs = [Request(0, 0.0, "mh", 32, 300.0, 300, 31), Request(1, 0.0, "write", 64, 260.0, 500, 32),
+            Request(2, 0.0, "mh", 32, 340.0, 700, 33), Request(3, 0.05, "mh", 64, 300.0, 200, 34),
+            Request(4, 0.05, "write", 32, 290.0, 450, 35)]
+    srv = Server(precision=FP32, chunk=128, keep_state=True)
+    out = srv.run(reqs)
+    assert len(out["results"]) == len(reqs)
+    for r in out["results"]:
+        q = reqs[r["rid"]]
+        g = GpuSim(q.medium(), precision=FP32, thermal_seed=q.seed)
+        g.step(q.steps, 1e-13)
+        assert np.array_equal(r["m"], g.get_state(0)), q
+        g.close()
+    srv.be.close()
