@@ -131,6 +131,90 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
   }
 }
 
+// One Stockham pass with every size known at compile time (LGN: log2 length,
+// LGR: log2 radix, LGNS: log2 of the current sub-transform length, TWL: log2
+// of the twiddle table length, PIN/POUT: padded input/output layout).
+template <typename R, int LGN, int LGR, int LGNS, int TWL, bool PIN, bool POUT, int S>
+MRM_D void stockham_pass_c(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, int nb,
+                           const Cx<R>* __restrict__ tw) {
+  constexpr int RADIX = 1 << LGR;
+  constexpr int LGNR = LGN - LGR;
+  constexpr int NR = 1 << LGNR;
+  constexpr int NS = 1 << LGNS;
+  constexpr int STRIDE = (1 << LGN) + ((1 << LGN) >> 4) + 1;  // fft_stride(n)
+  const int total = nb << LGNR;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int b = q >> LGNR, j = q & (NR - 1);
+    const Cx<R>* src = in + b * STRIDE;
+    Cx<R>* dst = out + b * STRIDE;
+    Cx<R> v[RADIX];
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) {
+      const int i = j + r * NR;
+      v[r] = src[PIN ? i + (i >> 4) : i];
+    }
+    const int k = j & (NS - 1);
+    if constexpr (LGNS > 0) {
+#pragma unroll
+      for (int r = 1; r < RADIX; ++r) {
+        Cx<R> w = tw[(k * r) << (TWL - LGNS - LGR)];
+        if (S > 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if constexpr (RADIX == 16) dft16<R, S>(v);
+    else if constexpr (RADIX == 8) dft8<R, S>(v);
+    else if constexpr (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
+    else dft2<R, S>(v);
+    const int idxD = ((j >> LGNS) << (LGNS + LGR)) + k;
+#pragma unroll
+    for (int q2 = 0; q2 < RADIX; ++q2) {
+      const int r = (RADIX == 16) ? dft16_out(q2) : q2;
+      const int i = idxD + r * NS;
+      dst[POUT ? i + (i >> 4) : i] = v[q2];
+    }
+  }
+}
+
+// Radix-8 Stockham plan of length 2^LGN unrolled at compile time (the final
+// pass takes the 1, 2 or 3 remaining bits).  Pass P reads layout PIN = (P>0),
+// writes POUT = (P < last).
+template <typename R, int LGN, int TWL, int S, int P, int LGNS>
+MRM_D Cx<R>* fft_c_from(Cx<R>* a, Cx<R>* b, int nb, const Cx<R>* __restrict__ tw) {
+  constexpr int REM = LGN - LGNS;
+  if constexpr (REM <= 0) {
+    return a;
+  } else {
+    constexpr int LGR = REM >= 3 ? 3 : REM;
+    constexpr bool LAST = (REM - LGR) == 0;
+    stockham_pass_c<R, LGN, LGR, LGNS, TWL, (P > 0), !LAST, S>(a, b, nb, tw);
+    __syncthreads();
+    return fft_c_from<R, LGN, TWL, S, P + 1, LGNS + LGR>(b, a, nb, tw);
+  }
+}
+
+// Transforms nb sequences held (unpadded) in `a`, sequence stride
+// fft_stride(n); `b` is scratch of the same size.  Returns the buffer holding
+// the (unpadded) result.  The caller must __syncthreads() before the call.
+// TWOFF: the twiddle table has length 2^(lgn + TWOFF).
+template <typename R, int S, int TWOFF>
+MRM_D Cx<R>* block_fft_c(Cx<R>* a, Cx<R>* b, int lgn, int nb, const Cx<R>* __restrict__ tw) {
+  switch (lgn) {
+    case 1: return fft_c_from<R, 1, 1 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 2: return fft_c_from<R, 2, 2 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 3: return fft_c_from<R, 3, 3 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 4: return fft_c_from<R, 4, 4 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 5: return fft_c_from<R, 5, 5 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 6: return fft_c_from<R, 6, 6 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 7: return fft_c_from<R, 7, 7 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 8: return fft_c_from<R, 8, 8 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 9: return fft_c_from<R, 9, 9 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 10: return fft_c_from<R, 10, 10 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    case 11: return fft_c_from<R, 11, 11 + TWOFF, S, 0, 0>(a, b, nb, tw);
+    default: return fft_c_from<R, 12, 12, S, 0, 0>(a, b, nb, tw);  // TWOFF = 0 at the 4096 limit
+  }
+}
+
 // Radix plan: the largest radix R in {16, 8, 4} whose passes keep at least
 // half the block busy (nb * n / R >= BLOCK / 2); small batches use radix 4
 // so that more threads share each pass.

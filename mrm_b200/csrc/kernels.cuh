@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDe
       }
     }
     __syncthreads();
-    Z = block_fft<R, +1>(bufA, bufB, lgM, nseq, cs, tws, lgpx);
+    Z = block_fft_c<R, +1, 1>(bufA, bufB, lgM, nseq, tws);
   }
   Cx<R>* W = (Z == bufA) ? bufB : bufA;  // real outputs of this stage (forward input)
   const R* hdr = reinterpret_cast<const R*>(Z);
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDe
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
-  Cx<R>* Y = block_fft<R, -1>(W, scratch, lgM, nseq, cs, tws, lgpx);
+  Cx<R>* Y = block_fft_c<R, -1, 1>(W, scratch, lgM, nseq, tws);
   for (int idx = threadIdx.x; idx < nseq * ph; idx += BLOCK) {
     const int s = idx / ph, k = idx - s * ph;
     const int row = s / 3, comp = s - 3 * row;
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) col_kernel(const RunDe
     }
   }
   __syncthreads();
-  Cx<R>* F = block_fft<R, -1>(A, B, lgpy, nseq, cs, tws, lgpy);
+  Cx<R>* F = block_fft_c<R, -1, 0>(A, B, lgpy, nseq, tws);
   Cx<R>* G = (F == A) ? B : A;
 
   // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) col_kernel(const RunDe
     }
   }
   __syncthreads();
-  Cx<R>* Hs = block_fft<R, +1>(G, F, lgpy, nseq, cs, tws, lgpy);
+  Cx<R>* Hs = block_fft_c<R, +1, 0>(G, F, lgpy, nseq, tws);
 
   const int tot2 = nseq * ny;
   for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
