@@ -138,9 +138,16 @@ __host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STAT
 
 template <typename R>
 __host__ __device__ constexpr int min_blocks() { return sizeof(R) == sizeof(float) ? 2 : 1; }
+// PREF: gather every per-grain input into registers before the inverse FFT
+// (latency-bound runs with few blocks per SM); otherwise load at use and run
+// four 256-thread blocks per SM (throughput-bound batches).
+template <typename R, bool PREF>
+__host__ __device__ constexpr int row_min_blocks() {
+  return PREF ? min_blocks<R>() : (sizeof(R) == sizeof(float) ? 4 : 2);
+}
 
-template <typename R, int STAGE, bool STATS, int GPT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDev<R>* __restrict__ runs,
+template <typename R, int STAGE, bool STATS, int GPT, int BLOCK, bool PREF>
+__global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(const RunDev<R>* __restrict__ runs,
                                                     const Task* __restrict__ tasks,
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags, double* __restrict__ part) {
@@ -173,75 +180,92 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDe
   const bool stencil = L.xst != nullptr;
   const bool ucol = L.ucol && Lu, lcol = L.lcol && Ll;
   const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
-  GrainIn<R> g[GPT];
+  const V4<R>* __restrict__ mother_u = Lu ? ((STAGE == kCorr) ? Lu->mp : Lu->m) : nullptr;
+  const V4<R>* __restrict__ mother_l = Ll ? ((STAGE == kCorr) ? Ll->mp : Ll->m) : nullptr;
+  // inputs that the previous kernel does not write
+  auto load_static = [&](GrainIn<R>& G, int n) {
+    G.pb = L.pb[n];
+    if (STAGE == kInit) return;
+    G.pa = L.pa[n];
+    if (stencil) G.cst = L.xst[n];
+    if (ucol) G.cu = L.ucol[n];
+    if (lcol) G.cl = L.lcol[n];
+  };
+  // inputs written by the previous kernels of this step
+  auto load_dynamic = [&](GrainIn<R>& G, int n, int i, int j) {
+    if (STAGE == kInit) {
+      G.mf = L.m[n];
+      return;
+    }
+    G.mf = mfield[n];
+    if (stencil) {
+      const int jm = (j == 0 ? ny - 1 : j - 1), jp = (j == ny - 1 ? 0 : j + 1);
+      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
+      G.nb[0] = mfield[jm * nx + i];
+      G.nb[1] = mfield[j * nx + im];
+      G.nb[2] = mfield[j * nx + ip];
+      G.nb[3] = mfield[jp * nx + i];
+    }
+    if (STAGE == kCorr) {
+      G.dm = L.dm[n];
+      G.m0 = L.m[n];
+      if (thermal) G.ht = L.ht[n];
+    }
+    if (ucol) G.vu = mother_u[n];
+    if (lcol) G.vl = mother_l[n];
+  };
+  GrainIn<R> g[PREF ? GPT : 1];
+  if constexpr (PREF) {
 #pragma unroll
-  for (int q = 0; q < GPT; ++q) {
-    const int idx = threadIdx.x + q * BLOCK;
-    if (idx >= ngr) continue;
-    const int row = idx / nx, i = idx - row * nx;
-    const int n = (row0 + row) * nx + i;
-    g[q].pb = L.pb[n];
-    if (STAGE == kInit) continue;
-    g[q].pa = L.pa[n];
-    if (stencil) g[q].cst = L.xst[n];
-    if (ucol) g[q].cu = L.ucol[n];
-    if (lcol) g[q].cl = L.lcol[n];
+    for (int q = 0; q < GPT; ++q) {
+      const int idx = threadIdx.x + q * BLOCK;
+      if (idx >= ngr) continue;
+      const int row = idx / nx, i = idx - row * nx;
+      load_static(g[q], (row0 + row) * nx + i);
+    }
   }
 
   // predictor: Philox thermal normals (llg.f90:1083 h = H + hthm/sqrt(dt); the
   // corrector reuses them, :1262-1266), drawn for the step counter read before
   // the wait and redrawn only if the previous kernel advanced it meanwhile
   const long long step_guess = rd.step + istep;
+  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
+  auto draw_one = [&](GrainIn<R>& G, int n, long long st) {
+    R gn[3];
+    thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)st, (unsigned long long)n, gn);
+    const R s = G.pb.w * tfac;
+    G.ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
+  };
   auto draw = [&](long long st) {
-    const R tfac = (R)sqrt(L.temperature / rd.dt);
 #pragma unroll
     for (int q = 0; q < GPT; ++q) {
       const int idx = threadIdx.x + q * BLOCK;
       if (idx >= ngr) continue;
       const int row = idx / nx, i = idx - row * nx;
-      const int n = (row0 + row) * nx + i;
-      R gn[3];
-      thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)st,
-                      (unsigned long long)n, gn);
-      const R s = g[q].pb.w * tfac;
-      g[q].ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
+      draw_one(g[q], (row0 + row) * nx + i, st);
     }
   };
-  if (STAGE == kPred && thermal) draw(step_guess);
+  if constexpr (PREF) {
+    if (STAGE == kPred && thermal) draw(step_guess);
+  }
 
   // ---------------- wait for the previous kernel's results ----------------
   pdl_wait();
   const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
   if (!(flags & kFlagForce) && step >= rd.step_end) return;
-  if (STAGE == kPred && thermal && step != step_guess) draw(step);
+  if constexpr (PREF) {
+    if (STAGE == kPred && thermal && step != step_guess) draw(step);
+  }
 
   // ---------------- dynamic per-grain inputs ----------------
+  if constexpr (PREF) {
 #pragma unroll
-  for (int q = 0; q < GPT; ++q) {
-    const int idx = threadIdx.x + q * BLOCK;
-    if (idx >= ngr) continue;
-    const int row = idx / nx, i = idx - row * nx, j = row0 + row;
-    const int n = j * nx + i;
-    if (STAGE == kInit) {
-      g[q].mf = L.m[n];
-      continue;
+    for (int q = 0; q < GPT; ++q) {
+      const int idx = threadIdx.x + q * BLOCK;
+      if (idx >= ngr) continue;
+      const int row = idx / nx, i = idx - row * nx, j = row0 + row;
+      load_dynamic(g[q], j * nx + i, i, j);
     }
-    g[q].mf = mfield[n];
-    if (stencil) {
-      const int jm = (j == 0 ? ny - 1 : j - 1), jp = (j == ny - 1 ? 0 : j + 1);
-      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
-      g[q].nb[0] = mfield[jm * nx + i];
-      g[q].nb[1] = mfield[j * nx + im];
-      g[q].nb[2] = mfield[j * nx + ip];
-      g[q].nb[3] = mfield[jp * nx + i];
-    }
-    if (STAGE == kCorr) {
-      g[q].dm = L.dm[n];
-      g[q].m0 = L.m[n];
-      if (thermal) g[q].ht = L.ht[n];
-    }
-    if (ucol) g[q].vu = ((STAGE == kCorr) ? Lu->mp : Lu->m)[n];
-    if (lcol) g[q].vl = ((STAGE == kCorr) ? Ll->mp : Ll->m)[n];
   }
 
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
@@ -303,7 +327,12 @@ __global__ void __launch_bounds__(BLOCK, min_blocks<R>()) row_kernel(const RunDe
     if (idx >= ngr) continue;
     const int row = idx / nx, i = idx - row * nx;
     const int n = (row0 + row) * nx + i;
-    const GrainIn<R>& G = g[q];
+    GrainIn<R>& G = g[PREF ? q : 0];
+    if constexpr (!PREF) {
+      load_static(G, n);
+      load_dynamic(G, n, i, row0 + row);
+      if (STAGE == kPred && thermal) draw_one(G, n, step);
+    }
     const R mse = G.pb.x;  // Ms * ms_scale
     if (STAGE == kInit) {
       outr[(row * 3 + 0) * rs + i] = mse * G.mf.x;
@@ -488,7 +517,7 @@ template <typename R>
 MRM_HD bool tens_slice_fits(int reals) { return (size_t)reals * sizeof(R) <= (size_t)kTensSliceBytes; }
 
 template <typename R, bool PACKED, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, min_blocks<R>()) col_kernel(const RunDev<R>* __restrict__ runs,
+__global__ void __launch_bounds__(BLOCK, PACKED ? 3 : 1) col_kernel(const RunDev<R>* __restrict__ runs,
                                                     const Task* __restrict__ tasks,
                                                     const Cx<R>* __restrict__ tw, int istep,
                                                     int flags) {

@@ -99,6 +99,7 @@ struct Engine {
   int nrt = 0, nct = 0, rt_cap = 0, ct_cap = 0;
   size_t smem_row = 0, smem_col = 0;
   int rowcfg = 0;
+  bool pref = true;  // row kernel gathers grain inputs up front (few blocks per SM)
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -438,6 +439,10 @@ int build_tables(Engine* e) {
   e->smem_row = srow;
   e->smem_col = scol;
   e->rowcfg = row_config(maxg);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->dev);
+  // enough row blocks to fill four per SM: the throughput variant wins
+  e->pref = !(e->prec == MRM_FP32 && e->rowcfg <= 1 && e->nrt >= 4 * nsm);
   clear_graphs(e);
   e->tables_dirty = false;
   e->desc_dirty = true;
@@ -475,14 +480,14 @@ void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cuda
   cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
-template <typename R, int GPT, int BLK>
+template <typename R, int GPT, int BLK, bool PREF>
 int set_row_attrs(size_t rs, std::string* errp) {
   int rc = 0;
-  rc |= raise_smem(row_kernel<R, kInit, false, GPT, BLK>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kPred, false, GPT, BLK>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, false, GPT, BLK>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, true, GPT, BLK>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kEval, false, GPT, BLK>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kInit, false, GPT, BLK, PREF>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kPred, false, GPT, BLK, PREF>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kCorr, false, GPT, BLK, PREF>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kCorr, true, GPT, BLK, PREF>, rs, errp);
+  rc |= raise_smem(row_kernel<R, kEval, false, GPT, BLK, PREF>, rs, errp);
   return rc;
 }
 
@@ -491,15 +496,19 @@ int set_smem_attrs(Engine* e) {
   std::string* errp = &e->err;
   const size_t rs = std::max<size_t>(e->smem_row, 16), cs = std::max<size_t>(e->smem_col, 16);
   int rc = 0;
-  if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256>(rs, errp);
-  else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256>(rs, errp);
-  else rc |= set_row_attrs<R, 2, 512>(rs, errp);
+  if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256, true>(rs, errp);
+  else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256, true>(rs, errp);
+  else rc |= set_row_attrs<R, 2, 512, true>(rs, errp);
+  if constexpr (sizeof(R) == sizeof(float)) {
+    if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256, false>(rs, errp);
+    else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256, false>(rs, errp);
+  }
   rc |= raise_smem(col_kernel<R, true, kBlock>, cs, errp);
   rc |= raise_smem(col_kernel<R, false, kBlock>, cs, errp);
   return rc ? MRM_ERR_CUDA : MRM_OK;
 }
 
-template <typename R, int GPT, int BLK>
+template <typename R, int GPT, int BLK, bool PREF>
 void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
   const RunDev<R>* runs = static_cast<const RunDev<R>*>(e->d_runs);
   const Cx<R>* tw = static_cast<const Cx<R>*>(e->d_tw);
@@ -507,19 +516,19 @@ void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
   const size_t sm = e->smem_row;
   switch (stage) {
     case kInit:
-      launch_pdl(row_kernel<R, kInit, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kInit, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kPred:
-      launch_pdl(row_kernel<R, kPred, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kPred, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     case kCorr:
       if (flags & kFlagStats)
-        launch_pdl(row_kernel<R, kCorr, true, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        launch_pdl(row_kernel<R, kCorr, true, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       else
-        launch_pdl(row_kernel<R, kCorr, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
+        launch_pdl(row_kernel<R, kCorr, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
     default:
-      launch_pdl(row_kernel<R, kEval, false, GPT, BLK>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
+      launch_pdl(row_kernel<R, kEval, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
       break;
   }
 }
@@ -527,9 +536,16 @@ void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
 template <typename R>
 void launch_row(Engine* e, int stage, int istep, int flags) {
   if (!e->nrt) return;
-  if (e->rowcfg == 0) launch_row_cfg<R, 1, 256>(e, stage, istep, flags);
-  else if (e->rowcfg == 1) launch_row_cfg<R, 2, 256>(e, stage, istep, flags);
-  else launch_row_cfg<R, 2, 512>(e, stage, istep, flags);
+  if constexpr (sizeof(R) == sizeof(float)) {
+    if (!e->pref) {
+      if (e->rowcfg == 0) launch_row_cfg<R, 1, 256, false>(e, stage, istep, flags);
+      else launch_row_cfg<R, 2, 256, false>(e, stage, istep, flags);
+      return;
+    }
+  }
+  if (e->rowcfg == 0) launch_row_cfg<R, 1, 256, true>(e, stage, istep, flags);
+  else if (e->rowcfg == 1) launch_row_cfg<R, 2, 256, true>(e, stage, istep, flags);
+  else launch_row_cfg<R, 2, 512, true>(e, stage, istep, flags);
 }
 
 template <typename R>
@@ -1590,12 +1606,14 @@ template <typename R>
 static int occ_t(Engine* e, int* out2) {
   std::string* errp = &e->err;
   int a = 0, b = 0;
-  if (e->rowcfg == 0)
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256>, 256, e->smem_row));
+  if (e->rowcfg == 0 && !e->pref && sizeof(R) == sizeof(float))
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256, false>, 256, e->smem_row));
+  else if (e->rowcfg == 0)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256, true>, 256, e->smem_row));
   else if (e->rowcfg == 1)
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 256>, 256, e->smem_row));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 256, true>, 256, e->smem_row));
   else
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 512>, 512, e->smem_row));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 512, true>, 512, e->smem_row));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, col_kernel<R, sizeof(R) == 4, kBlock>, kBlock, e->smem_col));
   out2[0] = a;
   out2[1] = b;
