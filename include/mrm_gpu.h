@@ -219,6 +219,26 @@ int64_t mrm_run_footprint(const mrm_geom* geom);
 /* Free / total device memory in bytes. */
 int mrm_device_memory(int device, int64_t* free_bytes, int64_t* total_bytes);
 
+/* Allocation-free demag evaluation.  No counterpart in the reference (its
+ * get_demag, src/demag.f90:33-135, works on module arrays allocated in
+ * init_demag); it exists for hosts that must not allocate device memory
+ * while they run, e.g. under a stream-ordered pool or a caching allocator.
+ *   h       an MRM_FP32 handle with every layer uploaded and a tensor built or
+ *           uploaded (its tensor, parameters and twiddles are read, nothing of
+ *           the handle is written);
+ *   m       device pointer, n_lay x n_grains x 3 floats (each layer's m(3,n));
+ *   hdemag  device pointer, same shape: the demagnetising field (Oe);
+ *   stream  cudaStream_t to enqueue on (NULL: the handle's stream); the call
+ *           returns once the work is enqueued.
+ * Scratch is one static 16 MiB device array per device; a grid whose
+ * descriptor, tasks, three float4 grain arrays and two half spectra exceed it
+ * returns MRM_ERR_UNSUPPORTED.  Nothing in the scratch needs to start at zero.
+ * The first call on a device sets up (scratch address, kernel loading and
+ * shared-memory limits) and must not be made during a stream capture.  Calls
+ * whose work overlaps on the device (different streams, other threads) share
+ * the scratch and race: serialise them. */
+int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1640,6 +1641,228 @@ int mrm_device_memory(int device, int64_t* free_bytes, int64_t* total_bytes) {
   if (cudaMemGetInfo(&f, &t) != cudaSuccess) return MRM_ERR_CUDA;
   if (free_bytes) *free_bytes = (int64_t)f;
   if (total_bytes) *total_bytes = (int64_t)t;
+  return MRM_OK;
+}
+
+}  // extern "C"
+
+// ---------------- allocation-free demag evaluation ----------------
+//
+// mrm_gpu_demag_noalloc evaluates the demagnetising field of a caller's device
+// magnetisation with the handle's tensor, using the same four kernels as
+// mrm_gpu_eval_field (Ms*m -> forward row FFT, column FFT x tensor x inverse,
+// inverse row FFT), but with every buffer of its own -- run descriptor, task
+// tables, packed magnetisation, fields and both half spectra -- carved out of
+// one file-scope device array instead of the handle's allocations.  The call
+// itself allocates nothing (no cudaMalloc/cudaFree, no pinned host memory, no
+// graph): callers running under a stream-ordered pool or a framework's
+// caching allocator, or a Fortran host that must not grow device memory inside
+// its time loop, can evaluate fields of trial states without an allocation.
+namespace {
+
+constexpr size_t kNoAllocBytes = 16u << 20;  // 16 MiB of scratch per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDev = 64;
+struct NoAllocDev {
+  unsigned char* base = nullptr;
+  bool ready = false;
+};
+NoAllocDev g_noalloc_dev[kNoAllocMaxDev];
+std::mutex g_noalloc_mu;
+
+static_assert(sizeof(RunDev<float>) <= 4000, "run descriptor must fit in a kernel parameter block");
+
+struct NoAllocLayout {
+  size_t desc = 0, rtask = 0, ctask = 0, m = 0, hd = 0, hf = 0, specx = 0, spech = 0, total = 0;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+NoAllocLayout noalloc_layout(const mrm_gpu* r, int nrt, int nct) {
+  NoAllocLayout o;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  const size_t n = (size_t)r->g.nx * r->g.ny, ph = r->px / 2 + 1;
+  const size_t grains = (size_t)r->nl * n * sizeof(V4<float>);
+  const size_t spec = (size_t)r->nl * 3 * r->g.ny * ph * sizeof(Cx<float>);
+  o.desc = take(sizeof(RunDev<float>));
+  o.rtask = take(sizeof(Task) * nrt);
+  o.ctask = take(sizeof(Task) * nct);
+  o.m = take(grains);
+  o.hd = take(grains);
+  o.hf = take(grains);
+  o.specx = take(spec);
+  o.spech = take(spec);
+  o.total = off;
+  return o;
+}
+
+// Writes the run descriptor and both task tables, and packs m (n_lay x n x 3
+// floats) into the float4 layout of the row kernel.
+__global__ void noalloc_pack_kernel(RunDev<float> d, RunDev<float>* __restrict__ desc,
+                                    Task* __restrict__ rt, int nrt, int rpt, Task* __restrict__ ct,
+                                    int nct, int cpt, const float* __restrict__ m_in,
+                                    V4<float>* __restrict__ m_out, long long ntot) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *desc = d;
+  if (i < nrt) {
+    const int per = (d.ny + rpt - 1) / rpt;
+    const int l = (int)i / per, j = ((int)i - l * per) * rpt;
+    rt[i] = make_int4(0, l, j, min(rpt, d.ny - j));
+  }
+  if (i < nct) {
+    const int k = (int)i * cpt, ph = d.px / 2 + 1;
+    ct[i] = make_int4(0, k, min(cpt, ph - k), 0);
+  }
+  if (i < ntot) m_out[i] = V4<float>{m_in[3 * i], m_in[3 * i + 1], m_in[3 * i + 2], 0.f};
+}
+
+__global__ void noalloc_unpack_kernel(const V4<float>* __restrict__ hd, float* __restrict__ out,
+                                      long long ntot) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntot) return;
+  const V4<float> v = hd[i];
+  out[3 * i] = v.x;
+  out[3 * i + 1] = v.y;
+  out[3 * i + 2] = v.z;
+}
+
+// Loads a kernel (CUDA lazy loading would otherwise load it, and allocate its
+// code, at its first launch) and lets it use all opt-in shared memory.  The
+// raise_smem record is lifted to the same value so that no engine lowers it.
+template <typename K>
+int noalloc_prepare(K* kern, int optin, std::string* errp) {
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, kern));
+  const size_t dyn = (size_t)optin - fa.sharedSizeBytes;
+  int rc = raise_smem(kern, dyn, errp);
+  if (rc) return rc;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  return MRM_OK;
+}
+
+template <int GPT, int BLK>
+int noalloc_prepare_rows(int optin, std::string* errp) {
+  int rc = noalloc_prepare(row_kernel<float, kInit, false, GPT, BLK, true>, optin, errp);
+  if (!rc) rc = noalloc_prepare(row_kernel<float, kEval, false, GPT, BLK, true>, optin, errp);
+  return rc;
+}
+
+// Once per device, with that device current: the scratch address and the
+// kernels' attributes.  Runs inside the first call on the device.
+int noalloc_setup(int dev, std::string* errp, unsigned char** base) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDev& s = g_noalloc_dev[dev];
+  if (s.ready) {
+    *base = s.base;
+    return MRM_OK;
+  }
+  void* p = nullptr;
+  CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  int rc = noalloc_prepare_rows<1, 256>(optin, errp);
+  if (!rc) rc = noalloc_prepare_rows<2, 256>(optin, errp);
+  if (!rc) rc = noalloc_prepare_rows<2, 512>(optin, errp);
+  if (!rc) rc = noalloc_prepare(col_kernel<float, true, kBlock>, optin, errp);
+  if (rc) return rc;
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, noalloc_pack_kernel));
+  CK(cudaFuncGetAttributes(&fa, noalloc_unpack_kernel));
+  s.base = static_cast<unsigned char*>(p);
+  s.ready = true;
+  *base = s.base;
+  return MRM_OK;
+}
+
+// kInit follows the pack kernel with a plain launch: it reads the descriptor
+// and tasks before its dependency wait, so it must not overlap their writer.
+// kEval follows the column kernel with programmatic serialization, as in the
+// engine.
+template <int GPT, int BLK>
+void noalloc_rows(int stage, int nrt, size_t smem, cudaStream_t st, const RunDev<float>* runs,
+                  const Task* tasks, const Cx<float>* tw) {
+  if (stage == kInit)
+    row_kernel<float, kInit, false, GPT, BLK, true><<<nrt, BLK, smem, st>>>(runs, tasks, tw, 0, kFlagForce, nullptr);
+  else
+    launch_pdl(row_kernel<float, kEval, false, GPT, BLK, true>, dim3(nrt), dim3(BLK), smem, st, runs, tasks, tw, 0,
+               kFlagForce | kFlagStoreField, (double*)nullptr);
+}
+
+void noalloc_rows_cfg(int cfg, int stage, int nrt, size_t smem, cudaStream_t st, const RunDev<float>* runs,
+                      const Task* tasks, const Cx<float>* tw) {
+  if (cfg == 0) noalloc_rows<1, 256>(stage, nrt, smem, st, runs, tasks, tw);
+  else if (cfg == 1) noalloc_rows<2, 256>(stage, nrt, smem, st, runs, tasks, tw);
+  else noalloc_rows<2, 512>(stage, nrt, smem, st, runs, tasks, tw);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* stream) {
+  if (!h) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  if (!m || !hdemag) return set_err(errp, MRM_ERR_ARG, "m and hdemag must be device pointers");
+  if (h->g.precision != MRM_FP32)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
+  const int nl = h->nl, ny = h->g.ny, ph = h->px / 2 + 1;
+  const int rpt = rows_per_task(h), nrt = nl * ((ny + rpt - 1) / rpt);
+  const int cpt = cols_per_task(h), nct = (ph + cpt - 1) / cpt;
+  const NoAllocLayout lay = noalloc_layout(h, nrt, nct);
+  if (lay.total > kNoAllocBytes)
+    return set_err(errp, MRM_ERR_UNSUPPORTED,
+                   "%d x %d x %d grains (FFT grid %d x %d) need %zu bytes of scratch; the allocation-free "
+                   "demag evaluation has %zu",
+                   h->g.nx, ny, nl, h->px, h->py, lay.total, kNoAllocBytes);
+  for (int l = 0; l < nl; ++l)
+    if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
+  if (!h->tensor_ready) return set_err(errp, MRM_ERR_STATE, "build or upload the tensor first");
+  Engine* e = h->eng;
+  if (e->dev < 0 || e->dev >= kNoAllocMaxDev)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "device %d above the supported %d", e->dev, kNoAllocMaxDev);
+  CK(cudaSetDevice(e->dev));
+  unsigned char* base = nullptr;
+  int rc = noalloc_setup(e->dev, errp, &base);
+  if (rc) return rc;
+
+  const long long n = (long long)h->g.nx * ny, ntot = n * nl;
+  RunDev<float> d = make_desc<float>(h);
+  d.active = 1;
+  d.demag = 1;
+  d.row_task0 = 0;
+  d.nrow_tasks = nrt;
+  d.specx = reinterpret_cast<Cx<float>*>(base + lay.specx);
+  d.spech = reinterpret_cast<Cx<float>*>(base + lay.spech);
+  V4<float>* sm = reinterpret_cast<V4<float>*>(base + lay.m);
+  V4<float>* shd = reinterpret_cast<V4<float>*>(base + lay.hd);
+  V4<float>* shf = reinterpret_cast<V4<float>*>(base + lay.hf);
+  for (int l = 0; l < nl; ++l) {
+    d.L[l].m = sm + l * n;
+    d.L[l].hd = shd + l * n;
+    d.L[l].hf = shf + l * n;
+  }
+  RunDev<float>* desc = reinterpret_cast<RunDev<float>*>(base + lay.desc);
+  Task* rt = reinterpret_cast<Task*>(base + lay.rtask);
+  Task* ct = reinterpret_cast<Task*>(base + lay.ctask);
+  const Cx<float>* tw = static_cast<const Cx<float>*>(e->d_tw);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e->st;
+  const long long work = std::max<long long>(ntot, std::max(nrt, nct));
+  const int cfg = row_config(rpt * h->g.nx);
+
+  noalloc_pack_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(d, desc, rt, nrt, rpt, ct, nct, cpt, m, sm,
+                                                                      ntot);
+  noalloc_rows_cfg(cfg, kInit, nrt, row_smem(h, MRM_FP32), st, desc, rt, tw);
+  launch_pdl(col_kernel<float, true, kBlock>, dim3(nct), dim3(kBlock), col_smem(h, MRM_FP32), st,
+             (const RunDev<float>*)desc, (const Task*)ct, tw, 0, (int)kFlagForce);
+  noalloc_rows_cfg(cfg, kEval, nrt, row_smem(h, MRM_FP32), st, desc, rt, tw);
+  noalloc_unpack_kernel<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(shd, hdemag, ntot);
+  CK(cudaGetLastError());
   return MRM_OK;
 }
 
