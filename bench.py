@@ -1,21 +1,34 @@
 """Benchmark of the per-timestep grain dynamics on B200.
 
-Workload (one GPU): the 65,536-grain medium -- 256 x 256 grains-as-nodes at
-8 nm pitch, 10 nm thick, Ms 700 emu/cc, Hk 15 kOe sigma 5 %, easy axes within
-3 deg, nearest-neighbour exchange 0.5 kOe, alpha 0.1, T = 300 K Philox thermal
-field, FP32 state/field/FFT with FP64 tensor and FP64 reductions, demag as a
-512 x 512 zero-padded FFT convolution, uniform field ramped +20 kOe -> -20 kOe
-at 10 deg off normal over 2 ns, Heun dt = 0.1 ps.  Synthetic media (seeded).
+Headline workload (one GPU): the batched form over B (default 32) independent
+realisations of the 65,536-grain medium -- 256 x 256 grains-as-nodes at 8 nm
+pitch, 10 nm thick, Ms 700 emu/cc, Hk 15 kOe sigma 5 %, easy axes within 3 deg,
+nearest-neighbour exchange 0.5 kOe, alpha 0.1, T = 300 K Philox thermal field
+(one seed per realisation), FP32 state/field/FFT with FP64 tensor and FP64
+reductions, demag as a 512 x 512 zero-padded FFT convolution, uniform field
+ramped +20 kOe -> -20 kOe at 10 deg off normal over 2 ns, Heun dt = 0.1 ps --
+advanced by one graph-captured launch sequence per Heun stage.  Synthetic
+media (seeded).  One bench step = HEUN_PER_STEP (100) Heun steps of every
+realisation; K = 200 timed bench steps = the full 20,000-step, 2 ns run.
 
-One bench step = HEUN_PER_STEP (1,000) Heun steps of that run; K timed bench
-steps = K * 1,000 Heun steps (K = 20 is the full 20,000-step run).
+Beside the headline (sub-objects of the same JSON line):
+  plain    the same medium as one plain single run (the drop-in; the
+           denominator of the batched/plain ratio), full 2 ns ramp, L2 flushed
+           between timed chunks; its coercivity against an FP64 run of the
+           same medium and seed;
+  mix      64 realisations with grain counts log-uniform in [1,024, 65,536],
+           Hk sigma in [3 %, 10 %], 5,000 Heun steps each, one batch;
+  served   a bounded sample of the Poisson request stream (200 req/s, M(H)
+           and write requests of 1,024..262,144 grains, 2,000..20,000 steps):
+           aggregate grain-steps/s and p50/p99 latency.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---gpus N > 1 runs under torch.distributed.run: one replica per GPU (the path
-does not shard: independent media realisations), value = sum of grain-steps
-over ranks / max rank time.  --impl reference times the CPU port of the
-reference algorithm (oracle/, OpenMP, all host cores) on a bounded sample.
+--gpus N > 1 runs under torch.distributed.run: one replica of the headline
+batch per GPU (the path does not shard: independent media realisations),
+value = grain-steps of all ranks / max rank time; the sub-objects run on rank
+0 only.  --impl reference times the CPU port of the reference algorithm
+(oracle/, OpenMP, all host cores) on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -35,18 +48,21 @@ sys.path.insert(0, ROOT)
 
 METRIC = "grain-steps/s (1 B200) batched/served vs plain GPU at <=1% Hc err; p50/p99 latency"
 UNIT = "grain-steps/s"
-HEUN_PER_STEP = 1000
+HEUN_PER_STEP = 100
 SIDE = 256
 DT = 1e-13
-WORKLOAD = "65,536-grain M(H) ramp, T=300 K, FP32, 512x512 zero-padded FFT demag, Heun 0.1 ps"
+RAMP_STEPS = 20000  # 2 ns at 0.1 ps
+WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
+            "512x512 zero-padded FFT demag, Heun 0.1 ps")
 
-# DRAM traffic per launch of the dominant kernel from the ncu capture summarised
-# in profiles/ (None until a capture exists for the current kernel version).
-NCU_TRAFFIC_BYTES = None
+# DRAM traffic per launch of the dominant kernel (bytes per grain of the
+# launch, from the ncu capture summarised in profiles/; None: no capture of the
+# current kernel version)
+NCU_TRAFFIC_BYTES_PER_GRAIN = None
 
 
 def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4) -> dict:
-    """Bytes each kernel must move at minimum with this path's data layout.
+    """Bytes each kernel must move at minimum with this path's data layout, per run.
 
     row predictor: H^ rows in + M^ rows out (2 * 3 ny (px/2+1) complex), per grain
       m, pa, pb (3 x 16 B), exchange CSR (4 B index + 4 x (4 B nbr + 4 B coef)),
@@ -132,6 +148,10 @@ def make_medium(seed: int = 1):
     return media.mh_medium(SIDE, boundary=1, temperature=300.0, seed=seed)
 
 
+def applied(t: float) -> float:
+    return 20000.0 - 40000.0 * min(1.0, max(0.0, t / (RAMP_STEPS * DT)))
+
+
 def coercivity(h, mh):
     """Hc, Mr from a descending M(H) branch by linear interpolation of the sign changes."""
     h, mh = np.asarray(h), np.asarray(mh)
@@ -144,19 +164,25 @@ def coercivity(h, mh):
     return hc, mr
 
 
-def cpu_baseline_sample(threads: int, nsteps: int = 12, warm: int = 2):
+def cpu_baseline_sample(threads: int, min_s: float = 10.0, chunk: int = 25, max_steps: int = 2000):
     """Oracle port (FP64, OpenMP) timed on a bounded sample of the same workload."""
     from oracle import pyoracle
+    pyoracle.build()
     pyoracle.set_threads(threads)
     med = make_medium()
     sim = pyoracle.OracleSim(med, rng_mode=1, seed=1)
-    sim.step(warm, DT)
-    t0 = time.perf_counter()
-    sim.step(nsteps, DT)
+    sim.step(2, DT)
+    done, t0 = 0, time.perf_counter()
+    while done < max_steps:
+        sim.step(chunk, DT)
+        done += chunk
+        if time.perf_counter() - t0 >= min_s:
+            break
     el = time.perf_counter() - t0
     n = med.n_grains
-    return {"value": n * nsteps / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{nsteps} Heun steps of the {n}-grain workload (FP64 oracle, OpenMP, after {warm} warm-up steps; tensor build excluded)"}
+    return {"value": n * done / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{done} Heun steps of one {n}-grain realisation in {el:.1f} s (FP64 oracle, "
+                      f"OpenMP, after 2 warm-up steps; tensor build excluded)"}
 
 
 def run_reference(args, rank, world):
@@ -168,7 +194,7 @@ def run_reference(args, rank, world):
     pyoracle.set_threads(threads)
     med = make_medium()
     sim = pyoracle.OracleSim(med, rng_mode=1, seed=1)
-    per = 4  # Heun steps per bench step: bounded sample
+    per = 4  # Heun steps of one realisation per bench step: a bounded sample
     for _ in range(args.warmup):
         sim.step(per, DT)
     t0 = time.perf_counter()
@@ -182,29 +208,203 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded media)",
-        "config": {"workload": WORKLOAD + f"; CPU sample of {per} Heun steps per bench step",
+        "config": {"workload": WORKLOAD.format(b=args.batch) +
+                   f"; CPU sample: {per} Heun steps of one realisation per bench step",
                    "grains": n, "heun_steps_per_bench_step": per},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{per} Heun steps x {args.steps} bench steps of the {n}-grain workload"},
+                         "sample": f"{per} Heun steps x {args.steps} bench steps of one {n}-grain realisation"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+def launches_per_bench_step(heun: int, stats: bool = True) -> int:
+    """Kernels per call of `heun` Heun steps: 4 per step, one advance per graph of
+    <= 16 steps, one stats finalisation per call."""
+    return 4 * heun + math.ceil(heun / 16) + (1 if stats else 0)
+
+
+def batched_leg(args, torch, local, rank, dist):
+    """Headline: B realisations of the 65,536-grain medium in one batch."""
+    from mrm_b200 import FP32, STATS_DTYPE
+    from mrm_b200.batch import Batch
+
+    b = Batch(FP32, local)
+    meds = [make_medium(seed=1 + rank * args.batch + i) for i in range(args.batch)]
+    runs = []
+    for i, med in enumerate(meds):
+        runs.append(b.add(med, dt=DT, thermal_seed=1 + rank * args.batch + i,
+                          tensor_from=runs[0] if runs else None))
+    n = meds[0].n_grains
+    ext = torch.cuda.ExternalStream(b.stream(), device=local)
+    hdirs = [np.array(m.layers[0].hdir) for m in meds]
+
+    def reset():
+        for r, med in zip(runs, meds):
+            r.set_state(0, med.m0[0])
+            r.set_time(0.0, 0)
+
+    for _ in range(args.warmup):
+        b.step(args.heun)
+    reset()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    hs, mhs = [], []
+    for k in range(args.steps):
+        ev[k][0].record(ext)
+        b.enqueue(args.heun)
+        ev[k][1].record(ext)
+        st = b.stats(runs)  # waits; outside the event pair
+        hs.append(applied(float(st[0]["t"])))
+        mhs.append([float(st[i]["mms_l"][0] @ hdirs[i]) for i in range(len(runs))])
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dev_ms = sum(a.elapsed_time(c) for a, c in ev)
+    if dist:
+        tt = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms = float(tt.item())
+    mh = np.array(mhs)
+    hcs = [coercivity(hs, mh[:, i])[0] for i in range(len(runs))]
+    hcs = [h for h in hcs if h is not None]
+
+    # end to end through the public API with host buffers: each bench step uploads
+    # every realisation's m, advances the batch and reads back its stats and m
+    reset()
+    m_host = [torch.from_numpy(np.ascontiguousarray(med.m0[0])).pin_memory().numpy() for med in meds]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    k_e2e = max(1, min(args.steps, args.e2e_steps))
+    t0 = time.perf_counter()
+    for k in range(k_e2e):
+        for r, m in zip(runs, m_host):
+            r.set_state(0, m)
+        b.step(args.heun)
+        st = b.stats(runs)
+        for i, r in enumerate(runs):
+            m_host[i][:] = r.get_state(0)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = sum(m.nbytes for m in m_host)
+    d2h = sum(m.nbytes for m in m_host) + len(runs) * STATS_DTYPE.itemsize
+
+    # per-kernel CUDA-event timing on the batch's stream
+    prof = b.profile(20)
+    px, py = runs[0].fft_grid()
+    occ = b.occupancy()
+    b.close()
+    return {"n": n, "runs": len(runs), "dev_ms": dev_ms, "clocks": clk, "hcs": hcs,
+            "e2e_s": e2e_s, "k_e2e": k_e2e, "h2d": h2d, "d2h": d2h, "prof": prof, "fft": (px, py),
+            "occupancy": occ, "samples": len(hs)}
+
+
+def plain_leg(torch, local, precision, heun_chunk=100, total=RAMP_STEPS, flush_l2=True):
+    """One plain single run of the 65,536-grain medium over the full ramp."""
+    from mrm_b200 import GpuSim
+    med = make_medium(seed=1)
+    sim = GpuSim(med, precision=precision, device=local, thermal_seed=1)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.step(3 * heun_chunk, DT, stats=False)  # warm-up: graphs, clocks
+    sim.set_time(0.0, 0)
+    sim.set_state(0, med.m0[0])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    hdir = np.array(med.layers[0].hdir)
+    nchunks = total // heun_chunk
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(nchunks)]
+    hs, mhs = [], []
+    torch.cuda.synchronize()
+    for k in range(nchunks):
+        if flush_l2:
+            flush.fill_(float(k))  # 256 MB > 126 MB L2
+            torch.cuda.synchronize()
+        ev[k][0].record(ext)
+        sim.enqueue(heun_chunk, DT)
+        ev[k][1].record(ext)
+        st = sim.stats()
+        hs.append(applied(float(st["t"])))
+        mhs.append(float(st["mms_l"][0] @ hdir))
+    torch.cuda.synchronize()
+    dev_ms = sum(a.elapsed_time(c) for a, c in ev)
+    prof = sim.profile(50, DT)
+    sim.close()
+    del flush
+    hc, mr = coercivity(hs, mhs)
+    n = med.n_grains
+    return {"value": n * nchunks * heun_chunk / (dev_ms * 1e-3), "us_per_heun_step":
+            1e3 * dev_ms / (nchunks * heun_chunk), "hc_oe": hc, "mr": mr, "prof": prof}
+
+
+def mix_leg(torch, local, steps=5000, nreal=64):
+    from mrm_b200 import FP32
+    from mrm_b200.batch import Batch
+    from mrm_b200.workloads import batched_media
+    meds = batched_media(nreal, steps=steps)
+    b = Batch(FP32, local)
+    for i, med in enumerate(meds):
+        b.add(med, dt=DT, steps=steps, thermal_seed=100 + i)
+    ext = torch.cuda.ExternalStream(b.stream(), device=local)
+    b.step(16)  # warm-up: task tables, attributes, first graph
+    for r, med in zip(b.runs, meds):
+        r.set_state(0, med.m0[0])
+        r.set_time(0.0, 0)
+        r.set_run(DT, steps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    b.enqueue(steps)
+    e1.record(ext)
+    b.stats()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    grains = sum(m.n_grains for m in meds)
+    b.close()
+    return {"workload": f"{nreal} realisations, grain counts log-uniform 1,024..65,536 (side a multiple "
+                        f"of 32), Hk sigma 3..10 %, T=300 K, FP32, {steps} Heun steps each",
+            "grains": grains, "value": grains * steps / (ms * 1e-3), "unit": UNIT, "device_ms": ms}
+
+
+def served_leg(local, nreq):
+    from mrm_b200 import FP32
+    from mrm_b200.serve import GpuBackend, Server
+    from mrm_b200.workloads import served_requests
+    reqs = served_requests(nreq)
+    be = GpuBackend(FP32, local)
+    srv = Server(backend=be)
+    out = srv.run(reqs)
+    be.close()
+    return {"workload": f"first {nreq} requests of the seeded Poisson stream (200 req/s, M(H) and STE "
+                        "write requests, 1,024..262,144 grains, T 250..350 K, 2,000..20,000 Heun steps)",
+            "requests": nreq, "value": out["grain_steps_per_s"], "unit": UNIT,
+            "p50_latency_s": out["p50_latency_s"], "p99_latency_s": out["p99_latency_s"],
+            "wall_s": out["wall_s"], "launch_calls": out["calls"]}
+
+
 def main():
-    global HEUN_PER_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=RAMP_STEPS // HEUN_PER_STEP)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=32, help="realisations in the headline batch")
+    ap.add_argument("--heun", type=int, default=HEUN_PER_STEP, help="Heun steps per bench step")
+    ap.add_argument("--e2e-steps", type=int, default=50, help="bench steps of the end-to-end leg")
+    ap.add_argument("--served", type=int, default=48, help="requests of the served sample (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--heun", type=int, default=HEUN_PER_STEP,
-                    help="Heun steps per bench step (profiling runs use a small value)")
-    ap.add_argument("--timing-only", action="store_true",
-                    help="skip the e2e and per-kernel legs (profiling runs)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the headline batch (profiling runs)")
     args = ap.parse_args()
-    HEUN_PER_STEP = args.heun
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -216,130 +416,80 @@ def main():
 
     import torch
     dist = None
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    from mrm_b200 import FP32, GpuSim, build
+    from mrm_b200 import FP32, FP64, build
     build.build()
 
-    med = make_medium(seed=1 + rank)
-    n = med.n_grains
-    sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1 + rank)
-    px, py = sim.fft_grid()
-    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
-
-    # warm-up (untimed), then restart the run from t = 0 for the timed region
-    for _ in range(args.warmup):
-        sim.step(HEUN_PER_STEP, DT, stats=False)
-    sim.set_time(0.0, 0)
-    sim.set_state(0, med.m0[0])
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    clocks = ClockSampler(local)
+    B = batched_leg(args, torch, local, rank, dist)
     if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    hs, mhs = [], []
-    hdir = np.array(med.layers[0].hdir)
-    for k in range(args.steps):
-        flush.fill_(float(k))  # L2 flush between timed iterations (256 MB > 126 MB L2)
-        torch.cuda.synchronize()
-        ev[k][0].record(ext)
-        sim.enqueue(HEUN_PER_STEP, DT)
-        ev[k][1].record(ext)
-        st = sim.stats()  # waits; outside the event pair
-        t = st["t"]
-        hs.append(20000.0 - 40000.0 * min(1.0, t / 2e-9))
-        mhs.append(float(st["mms_l"][0] @ hdir))
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if dist:
-        tt = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms = float(tt.item())
-    heun_total = HEUN_PER_STEP * args.steps
-    value = world * n * heun_total / (dev_ms * 1e-3)
-
-    if args.timing_only:
-        if rank == 0:
-            print(json.dumps({"timing_only": True, "value": value, "ms_per_step": dev_ms / args.steps}))
-        sim.close()
-        if dist:
-            dist.destroy_process_group()
+        dist.destroy_process_group()  # the sub-objects run on rank 0 alone
+    if rank != 0:
         return
-
-    # end-to-end through the C ABI with host buffers: upload m, step, read stats + m
-    m_host = torch.from_numpy(np.ascontiguousarray(med.m0[0])).pin_memory()
-    m_out = np.zeros_like(med.m0[0])
-    sim.set_time(0.0, 0)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        sim.set_state(0, m_host.numpy())
-        sim.step(HEUN_PER_STEP, DT, stats=True)
-        m_out[:] = sim.get_state(0)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e_value = world * n * heun_total / e2e_s
-    h2d = m_host.numel() * 8
-    d2h = m_out.size * 8 + np.dtype(__import__("mrm_b200").STATS_DTYPE).itemsize
-
-    # per-kernel CUDA-event timing on the launching stream (roofline of the dominant kernel)
-    prof = sim.profile(50, DT)
-    names = ["row_pred", "col", "row_corr", "col"]
-    ab = algorithmic_bytes(med.nx, med.ny, px, py)
+    n, nb = B["n"], B["runs"]
+    value = world * nb * n * args.heun * args.steps / (B["dev_ms"] * 1e-3)
+    e2e_value = world * nb * n * args.heun * B["k_e2e"] / B["e2e_s"]
+    px, py = B["fft"]
+    ab = {k: v * nb for k, v in algorithmic_bytes(SIDE, SIDE, px, py).items()}
+    prof = B["prof"]
     per_kernel = {"row_pred": prof[0], "col": 0.5 * (prof[1] + prof[3]), "row_corr": prof[2]}
-    dom = max(per_kernel, key=per_kernel.get)
+    launches_per_heun = {"row_pred": 1, "col": 2, "row_corr": 1}
+    # dominant kernel: the largest share of a Heun step's device time
+    dom = max(per_kernel, key=lambda k: per_kernel[k] * launches_per_heun[k])
     peak, peak_kind = measured_peaks()
     achieved = ab[dom] / (per_kernel[dom] * 1e-3) / 1e9
-    sim.close()
-
-    if rank != 0:
-        if dist:
-            dist.destroy_process_group()
-        return
-    hc, mr = coercivity(hs, mhs)
-    n_chunks = math.ceil(HEUN_PER_STEP / 16)
-    launches = args.steps * (4 * HEUN_PER_STEP + 2 * n_chunks)
+    hc_mean = float(np.mean(B["hcs"])) if B["hcs"] else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": B["dev_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded media, random-init grain properties)",
-        "config": {"workload": WORKLOAD, "grains": n, "fft_grid": [px, py],
-                   "heun_steps_per_bench_step": HEUN_PER_STEP, "form": "plain single run per GPU",
+        "config": {"workload": WORKLOAD.format(b=nb), "realisations_per_gpu": nb, "grains_per_realisation": n,
+                   "fft_grid": [px, py], "heun_steps_per_bench_step": args.heun,
+                   "form": "batched: one launch sequence per Heun stage over every realisation",
                    "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MB write) between timed bench steps"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
+                   "l2": f"inputs larger than L2 ({nb} realisations, ~{nb * 17} MB resident)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B["h2d"], "d2h_bytes_per_step": B["d2h"],
+                "bench_steps": B["k_e2e"]},
+        "gpu_launches": args.steps * launches_per_bench_step(args.heun),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes": ab[dom], "avg_launch_ms": per_kernel[dom],
-                     "traffic": NCU_TRAFFIC_BYTES,
-                     "per_kernel_ms": per_kernel},
-        "physics": {"Hc_Oe": hc, "Mr": mr, "m_h_samples": len(hs)},
+                     "traffic": (NCU_TRAFFIC_BYTES_PER_GRAIN * nb * n
+                                 if NCU_TRAFFIC_BYTES_PER_GRAIN is not None else None),
+                     "per_kernel_ms": per_kernel, "launches_per_heun_step": launches_per_heun,
+                     "per_kernel_frac": {k: ab[k] / (v * 1e-3) / 1e9 / peak for k, v in per_kernel.items()},
+                     "occupancy_blocks_per_sm": {"row": B["occupancy"][0], "col": B["occupancy"][1]}},
+        "physics": {"hc_mean_oe": hc_mean,
+                    "hc_std_oe": float(np.std(B["hcs"])) if B["hcs"] else None,
+                    "hc_realisations": len(B["hcs"]), "m_h_samples": B["samples"]},
     }
-    if clk:
-        line["clocks"] = clk
-    if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
+    if B["clocks"]:
+        line["clocks"] = B["clocks"]
+    if not args.headline_only:
+        p32 = plain_leg(torch, local, FP32)
+        p64 = plain_leg(torch, local, FP64, flush_l2=False)
+        hc_err = (abs(p32["hc_oe"] - p64["hc_oe"]) / abs(p64["hc_oe"])
+                  if p32["hc_oe"] and p64["hc_oe"] else None)
+        line["plain"] = {"workload": "one 65,536-grain realisation (seed 1), full 2 ns ramp, FP32",
+                         "value": p32["value"], "unit": UNIT, "us_per_heun_step": p32["us_per_heun_step"],
+                         "batched_over_plain": value / world / p32["value"],
+                         "per_kernel_ms": {"row_pred": p32["prof"][0], "col": 0.5 * (p32["prof"][1] + p32["prof"][3]),
+                                           "row_corr": p32["prof"][2]},
+                         "l2": "flushed (256 MB write) between timed 100-step chunks"}
+        line["physics"].update({"hc_fp32_oe": p32["hc_oe"], "hc_fp64_oe": p64["hc_oe"], "hc_rel_err_fp32_vs_fp64": hc_err,
+                                "mr_fp32": p32["mr"], "mr_fp64": p64["mr"],
+                                "fp64_us_per_heun_step": p64["us_per_heun_step"]})
+        line["mix"] = mix_leg(torch, local)
+        if args.served > 0:
+            line["served"] = served_leg(local, args.served)
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

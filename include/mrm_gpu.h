@@ -211,6 +211,10 @@ int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats
 /* Enqueues like mrm_batch_step without waiting (stats via mrm_batch_stats). */
 int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type);
 int mrm_batch_stream(const mrm_batch* b, void** stream);
+/* Per-kernel timing of one Heun step of every active run (CUDA events on the
+ * batch's stream, averaged over reps steps, which are taken):
+ * ms_out[4] = predictor row, column, corrector row, column kernel. */
+int mrm_batch_profile(mrm_batch* b, int reps, double* ms_out);
 /* Resident blocks per SM of the row and column kernels of this batch (0 if
  * no step was taken yet): out[0] = row, out[1] = column. */
 int mrm_batch_occupancy(mrm_batch* b, int* out2);

@@ -33,7 +33,7 @@ EXPORTS = [
     "mrm_batch_enqueue", "mrm_batch_stream", "mrm_batch_create", "mrm_batch_destroy", "mrm_batch_last_error",
     "mrm_batch_add", "mrm_batch_remove", "mrm_batch_set_run", "mrm_batch_step", "mrm_batch_stats",
     "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
-    "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc",
+    "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile",
 ]
 
 
@@ -120,6 +120,7 @@ def load(path: str = LIB_PATH):
         "mrm_batch_occupancy": ([vp, P(i)], i),
         "mrm_device_memory": ([i, P(i64), P(i64)], i),
         "mrm_gpu_demag_noalloc": ([vp, vp, vp, vp], i),
+        "mrm_batch_profile": ([vp, i, pd], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -94,6 +94,12 @@ class Batch:
         self._check(_lib.load().mrm_batch_stream(self.b, C.byref(s)))
         return s.value or 0
 
+    def profile(self, reps: int) -> np.ndarray:
+        """Per-kernel ms of one Heun step (predictor row, column, corrector row, column)."""
+        out = np.zeros(4)
+        self._check(_lib.load().mrm_batch_profile(self.b, int(reps), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     def occupancy(self):
         o = (C.c_int * 2)()
         self._check(_lib.load().mrm_batch_occupancy(self.b, o))

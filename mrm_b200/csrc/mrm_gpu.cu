@@ -1432,8 +1432,7 @@ int mrm_gpu_stream(const mrm_gpu* h, void** stream) {
 }  // extern "C"
 
 template <typename R>
-static int profile_t(mrm_gpu* h, int reps, double* ms_out) {
-  Engine* e = h->eng;
+static int profile_t(Engine* e, int reps, double* ms_out) {
   std::string* errp = &e->err;
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
@@ -1474,7 +1473,7 @@ int mrm_gpu_profile(mrm_gpu* h, int reps, double dt, double* ms_out) {
   if (!h || !ms_out || reps < 1) return MRM_ERR_ARG;
   int rc = plain_prepare(h, reps, dt, -3);
   if (rc) return rc;
-  rc = h->eng->prec == MRM_FP64 ? profile_t<double>(h, reps, ms_out) : profile_t<float>(h, reps, ms_out);
+  rc = h->eng->prec == MRM_FP64 ? profile_t<double>(h->eng, reps, ms_out) : profile_t<float>(h->eng, reps, ms_out);
   if (rc) h->err = h->eng->err;
   return rc;
 }
@@ -1576,6 +1575,12 @@ int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type) {
   std::string* errp = &b->eng.err;
   CK(cudaStreamSynchronize(b->eng.st));
   return MRM_OK;
+}
+
+int mrm_batch_profile(mrm_batch* b, int reps, double* ms_out) {
+  if (!b || !ms_out || reps < 1) return MRM_ERR_ARG;
+  Engine* e = &b->eng;
+  return e->prec == MRM_FP64 ? profile_t<double>(e, reps, ms_out) : profile_t<float>(e, reps, ms_out);
 }
 
 int mrm_batch_stream(const mrm_batch* b, void** stream) {
