@@ -303,10 +303,11 @@ def batched_leg(args, torch, local, rank, dist):
     prof = b.profile(20)
     px, py = runs[0].fft_grid()
     occ = b.occupancy()
+    shape = runs[0].get_shape()
     b.close()
     return {"n": n, "runs": len(runs), "dev_ms": dev_ms, "clocks": clk, "hcs": hcs,
             "e2e_s": e2e_s, "k_e2e": k_e2e, "h2d": h2d, "d2h": d2h, "prof": prof, "fft": (px, py),
-            "occupancy": occ, "samples": len(hs)}
+            "occupancy": occ, "shape": shape, "samples": len(hs)}
 
 
 def plain_leg(torch, local, precision, heun_chunk=100, total=RAMP_STEPS, flush_l2=True):
@@ -463,7 +464,8 @@ def main():
                                  if NCU_TRAFFIC_BYTES_PER_GRAIN is not None else None),
                      "per_kernel_ms": per_kernel, "launches_per_heun_step": launches_per_heun,
                      "per_kernel_frac": {k: ab[k] / (v * 1e-3) / 1e9 / peak for k, v in per_kernel.items()},
-                     "occupancy_blocks_per_sm": {"row": B["occupancy"][0], "col": B["occupancy"][1]}},
+                     "occupancy_blocks_per_sm": {"row": B["occupancy"][0], "col": B["occupancy"][1]},
+                     "kernel_shapes": {"row": B["shape"][0], "col": B["shape"][1], "cols_per_task": B["shape"][2]}},
         "physics": {"hc_mean_oe": hc_mean,
                     "hc_std_oe": float(np.std(B["hcs"])) if B["hcs"] else None,
                     "hc_realisations": len(B["hcs"]), "m_h_samples": B["samples"]},

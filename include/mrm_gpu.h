@@ -181,6 +181,27 @@ int mrm_gpu_enqueue_steps(mrm_gpu* h, int nsteps, double dt, int llg_type);
 int mrm_gpu_read_stats(mrm_gpu* h, mrm_gpu_stats* out);
 /* The cudaStream_t (as void*) the handle launches on, for event timing. */
 int mrm_gpu_stream(const mrm_gpu* h, void** stream);
+
+/* Kernel shapes of the engine a handle runs in (a batch run: the batch's).
+ * row_shape / col_shape index the compiled row / column kernel shapes
+ * (rows per block, threads, resident blocks; threads and resident blocks of
+ * the column kernel) and cols_per_task > 0 fixes the spectral columns per
+ * column task; a negative shape returns to the automatic choice.  Results do
+ * not depend on the shape.  Automatic: with autotuning on (the default), the
+ * first step after the set of runs changes times every compiled shape on the
+ * runs themselves (their state is restored) and keeps the fastest, cached per
+ * grid size, layer count and grain-count magnitude; with it off, a size
+ * heuristic.  mrm_gpu_get_shape: out3 = {row shape, column shape, columns per
+ * task (0: default)} of the last step. */
+int mrm_gpu_set_shape(mrm_gpu* h, int row_shape, int col_shape, int cols_per_task);
+int mrm_gpu_set_autotune(mrm_gpu* h, int on);
+int mrm_gpu_get_shape(const mrm_gpu* h, int* out3);
+/* Waits for the handle's stream and reads (and clears) the device error flag
+ * its kernels raise instead of trapping (bulk-copy waits that ran out, a
+ * kernel shape outside its compiled range); MRM_ERR_DEVICE with the details
+ * in mrm_gpu_last_error() if it was set.  The stepping calls do this at every
+ * synchronisation. */
+int mrm_gpu_check_device(mrm_gpu* h);
 /* Advances `reps` Heun steps launching each kernel bracketed by CUDA events
  * on the handle's stream; ms_out[4] = mean ms of row(predictor), column,
  * row(corrector), column launches (the demag column launches are 0 when

@@ -1,9 +1,13 @@
 """Builds mrm_b200/libmrm_gpu.so (sm_100a) in-tree with nvcc.
 
-    python -m mrm_b200.build
+    python -m mrm_b200.build [--force] [-v]
+
+Every translation unit compiles in its own nvcc process (in parallel), then
+one nvcc call links the shared library.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import os
 import shutil
 import subprocess
@@ -12,10 +16,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmrm_gpu.so")
-SOURCES = ["csrc/mrm_gpu.cu"]
-HEADERS = ["csrc/common.cuh", "csrc/fft.cuh", "csrc/kernels.cuh", "csrc/philox.cuh",
-           "csrc/tensor.cuh", "../include/mrm_gpu.h"]
+OBJ = os.path.join(HERE, "_build")
+SOURCES = (["csrc/mrm_gpu.cu", "csrc/k_col.cu"] + [f"csrc/k_row_f32_v{v}.cu" for v in range(5)] +
+           [f"csrc/k_row_f64_v{v}.cu" for v in range(3)])
+HEADERS = ["csrc/common.cuh", "csrc/fft.cuh", "csrc/kernels.cuh", "csrc/philox.cuh", "csrc/tensor.cuh",
+           "csrc/tma.cuh", "csrc/launch.h", "csrc/k_row.inc", "../include/mrm_gpu.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
 def nvcc() -> str:
@@ -25,21 +32,48 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def _mtime(rel: str) -> float:
+    return os.path.getmtime(os.path.join(HERE, rel))
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(os.path.join(HERE, s)) <= t for s in SOURCES + HEADERS)
+    return all(_mtime(s) <= t for s in SOURCES + HEADERS)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-o", LIB + ".tmp", *[os.path.join(HERE, s) for s in SOURCES]]
+def _obj(src: str) -> str:
+    return os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
+
+
+def _compile(src: str, verbose: bool) -> str:
+    out = _obj(src)
+    cmd = [nvcc(), *FLAGS, "-c", os.path.join(HERE, src), "-o", out + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+    if verbose and r.stderr:
+        print(r.stderr, file=sys.stderr)
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJ, exist_ok=True)
+    newest_header = max(_mtime(h) for h in HEADERS)
+    todo = [s for s in SOURCES
+            if force or not os.path.exists(_obj(s))
+            or os.path.getmtime(_obj(s)) < max(_mtime(s), newest_header)]
+    jobs = jobs or max(1, min(len(todo) or 1, os.cpu_count() or 1))
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        list(ex.map(lambda s: _compile(s, verbose), todo))
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *[_obj(s) for s in SOURCES]]
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB

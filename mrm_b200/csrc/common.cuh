@@ -9,7 +9,7 @@
 namespace mrm {
 
 constexpr int kMaxLayers = 8;
-constexpr int kTwLog = 12;                 // twiddle table covers FFT lengths <= 4096
+constexpr int kTwLog = 12;                 // FFT lengths <= 4096
 constexpr int kTwN = 1 << kTwLog;
 constexpr int kNPart = 20;                 // doubles per row-task stats record
 
@@ -90,9 +90,12 @@ struct RunDev {
   int active;
   int stats_ok;            // set by the advance kernel: the chunk's last step was executed
   int row_task0, nrow_tasks;  // range of this run's row tasks (stats partials)
-  Cx<R>* spech;            // H^ half spectra, row-major [nl][3][ny][px/2+1] (column kernel -> row kernel)
-  Cx<R>* specx;            // M^ half spectra, column-major [nl][3][px/2+1][ny] (row kernel -> column kernel)
-  const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][py/2+1] reals,
+  int phs, nys, pyhs;      // padded strides: spectrum row (px/2+1 -> even), spectrum column
+                           // (ny -> even), packed tensor row (py/2+1 -> multiple of 4)
+  int tw_row, tw_col;      // offsets of this grid's twiddle blocks in the global table (fft.cuh)
+  Cx<R>* spech;            // H^ half spectra, row-major [nl][3][ny][phs] (column kernel -> row kernel)
+  Cx<R>* specx;            // M^ half spectra, column-major [nl][3][px/2+1][nys] (row kernel -> column kernel)
+  const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][pyhs] reals,
                            // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];
 };

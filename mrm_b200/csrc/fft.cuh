@@ -1,22 +1,67 @@
-// fft.cuh -- block-cooperative Stockham FFT in shared memory (sm_100a).
+// fft.cuh -- block-cooperative Stockham FFTs in shared memory (sm_100a).
 //
 // Replaces the FFTW r2c/c2r plans of src/fftw.f90:37-93 (unnormalised,
-// forward sign -1).  A batch of `nb` complex sequences of length n = 2^lgn,
-// sequence b at buf + b*stride, is transformed with radix-16 passes and one
-// radix-8/4/2 pass for the remainder (Stockham autosort: natural-order
-// output, ping-pong between two shared buffers, one __syncthreads per pass).
-// Intermediate passes use a padded layout (one spare slot per 16 elements)
-// so the stride-R stores of the early passes hit distinct banks; the input of
-// the first pass and the output of the last pass are unpadded.  `stride`
-// must be >= fft_stride(n).  Twiddles come from a table tw[k] = e^{-2 pi i k / 2^lgtw}
-// (FP64-accurate values) with 2^lgtw >= n, normally staged in shared memory.
+// forward sign -1).  Two forms:
+//
+//  * the hot-path form (block_fft_c): every length, pass, stride and twiddle
+//    offset is a compile-time constant.  A batch of nb complex sequences of
+//    length n = 2^lgn, sequence b at buf + b*seq_stride(n), is transformed by
+//    radix-8 passes plus one radix-2/4 pass for the remaining bits (Stockham
+//    autosort: natural-order result, ping-pong between two buffers, one
+//    __syncthreads per pass).  Intermediate passes use the swizzled layout
+//    swz(i) = i ^ ((i >> 3) & 15), a permutation inside each group of 16
+//    elements under which the stride-8 stores of the first pass, the runs of
+//    8 of the second and the contiguous loads all touch distinct banks; the
+//    input of the first pass and the output of the last are natural order.
+//    Each pass reads its twiddles from its own table, entry (r-1)*Ns + k =
+//    e^{-2 pi i k r / (Ns R)}, so a warp reads consecutive entries.
+//  * the run-time form (block_fft): sizes at run time, padded layout, twiddles
+//    from the 4096-entry table; used by the once-per-run FP64 tensor FFT.
 #pragma once
 #include "common.cuh"
 
 namespace mrm {
 
-MRM_HD int fft_stride(int n) { return n + (n >> 4) + 1; }
-MRM_D int padi(int i) { return i + (i >> 4); }
+// ---------------- hot-path form ----------------
+
+MRM_HD constexpr int swz(int i) { return i ^ ((i >> 3) & 15); }
+// complex stride of one sequence of length n in the hot-path buffers (even,
+// so that every sequence starts 16-byte aligned in FP32)
+MRM_HD constexpr int seq_stride(int n) { return n == 64 ? n + 8 : n + 2; }
+
+// radix plan of length 2^lgn: passes of 3 bits, the last takes the remaining 1..3
+MRM_HD constexpr int pass_lgr(int lgn, int lgns) { return (lgn - lgns) >= 3 ? 3 : lgn - lgns; }
+// twiddles of all passes of a length-2^lgn transform
+MRM_HD constexpr int pass_tw_count(int lgn) {
+  int total = 0, lgns = 0;
+  while (lgns < lgn) {
+    const int lgr = pass_lgr(lgn, lgns);
+    if (lgns > 0) total += ((1 << lgr) - 1) << lgns;
+    lgns += lgr;
+  }
+  return total;
+}
+MRM_HD constexpr int even_up(int x) { return (x + 1) & ~1; }
+// Row-kernel twiddle block for an FFT grid of 2^lgpx columns (real transform
+// of length px through a complex one of length M = px/2): the post/pre-
+// processing twiddles e^{-2 pi i k/px}, k <= M (padded to even), then the
+// pass tables of the length-M transform.
+MRM_HD constexpr int row_tw_post(int lgpx) { return even_up((1 << (lgpx - 1)) + 1); }
+MRM_HD constexpr int row_tw_count(int lgpx) { return row_tw_post(lgpx) + even_up(pass_tw_count(lgpx - 1)); }
+// Column-kernel twiddle block for 2^lgpy rows: the pass tables of that length.
+MRM_HD constexpr int col_tw_count(int lgpy) { return even_up(pass_tw_count(lgpy)); }
+// offsets of the blocks in the global table: row blocks for lg = 1..kTwLog, then column blocks
+MRM_HD constexpr int row_tw_off(int lgpx) {
+  int o = 0;
+  for (int l = 1; l < lgpx; ++l) o += row_tw_count(l);
+  return o;
+}
+MRM_HD constexpr int col_tw_off(int lgpy) {
+  int o = row_tw_off(kTwLog + 1);
+  for (int l = 1; l < lgpy; ++l) o += col_tw_count(l);
+  return o;
+}
+MRM_HD constexpr int tw_table_size() { return col_tw_off(kTwLog + 1); }
 
 template <typename R, int S>
 MRM_D void dft2(Cx<R>* v) {
@@ -58,35 +103,106 @@ MRM_D void dft8(Cx<R>* v) {
   v[7] = csub(e3, o3);
 }
 
-// 16-point DFT as 4 x 4 (radix-4 over stride 4, twiddles w16^(k1 n2), radix-4);
-// the outputs are left in digit-reversed order (see dft16_out)
-template <typename R, int S>
-MRM_D void dft16(Cx<R>* v) {
-  const R c1 = (R)0.92387953251128675612818318939679;  // cos(pi/8)
-  const R s1 = (R)0.38268343236508977172845998403040;  // sin(pi/8)
-  const R h = (R)0.70710678118654752440084436210485;
+// One Stockham pass with every size known at compile time.  LGN: log2
+// length; LGR: log2 radix; LGNS: log2 of the sub-transform length so far;
+// OFF: offset of this pass's table in the pass tables; PIN/POUT: swizzled
+// input/output; NBMAX: upper bound of nb (0: none, run-time loop); BLOCK:
+// threads of the block.
+template <typename R, int LGN, int LGR, int LGNS, int OFF, bool PIN, bool POUT, int S, int NBMAX, int BLOCK>
+MRM_D void stockham_pass_c(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, int nb,
+                           const Cx<R>* __restrict__ twp) {
+  constexpr int RADIX = 1 << LGR;
+  constexpr int LGNR = LGN - LGR;
+  constexpr int NR = 1 << LGNR;
+  constexpr int NS = 1 << LGNS;
+  constexpr int STRIDE = seq_stride(1 << LGN);
+  const int total = nb << LGNR;
+  auto body = [&](int q) {
+    const int b = q >> LGNR, j = q & (NR - 1);
+    const Cx<R>* src = in + b * STRIDE;
+    Cx<R>* dst = out + b * STRIDE;
+    Cx<R> v[RADIX];
 #pragma unroll
-  for (int n2 = 0; n2 < 4; ++n2) dft4<R, S>(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
-  // after this, v[n2 + 4*k1] holds the k1-th output of column n2; twiddle w16^(k1*n2)
-  const Cx<R> w1 = {c1, (R)S * s1}, w2 = {h, (R)S * h}, w3 = {s1, (R)S * c1};
-  const Cx<R> w6 = {-h, (R)S * h}, w9 = {-c1, (R)S * (-s1)};
-  // k1=1: n2=1..3 -> w^1, w^2, w^3 ; k1=2 -> w^2, w^4, w^6 ; k1=3 -> w^3, w^6, w^9
-  v[5] = cmul(v[5], w1);
-  v[6] = cmul(v[6], w2);
-  v[7] = cmul(v[7], w3);
-  v[9] = cmul(v[9], w2);
-  v[10] = cmul_i(v[10], (R)S);
-  v[11] = cmul(v[11], w6);
-  v[13] = cmul(v[13], w3);
-  v[14] = cmul(v[14], w6);
-  v[15] = cmul(v[15], w9);
+    for (int r = 0; r < RADIX; ++r) {
+      const int i = j + r * NR;
+      v[r] = src[PIN ? swz(i) : i];
+    }
+    const int k = j & (NS - 1);
+    if constexpr (LGNS > 0) {
 #pragma unroll
-  for (int k1 = 0; k1 < 4; ++k1) dft4<R, S>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
-  // v[4*k1 + k2] now holds output k = k1 + 4*k2 (digit-reversed); dft16_out maps it back
+      for (int r = 1; r < RADIX; ++r) {
+        Cx<R> w = twp[OFF + (r - 1) * NS + k];
+        if (S > 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if constexpr (RADIX == 8) dft8<R, S>(v);
+    else if constexpr (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
+    else dft2<R, S>(v);
+    const int idxD = ((j >> LGNS) << (LGNS + LGR)) + k;
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) {
+      const int i = idxD + r * NS;
+      dst[POUT ? swz(i) : i] = v[r];
+    }
+  };
+  constexpr int ITERS = NBMAX > 0 ? ((NBMAX << LGNR) + BLOCK - 1) / BLOCK : 0;
+  if constexpr (NBMAX > 0 && ITERS <= 2) {
+#pragma unroll
+    for (int it = 0; it < ITERS; ++it) {
+      const int q = threadIdx.x + it * BLOCK;
+      if (q < total) body(q);
+    }
+  } else {
+#pragma unroll 1
+    for (int q = threadIdx.x; q < total; q += BLOCK) body(q);
+  }
 }
 
-// output index of v[q] after dft16
-MRM_HD constexpr int dft16_out(int q) { return (q >> 2) + 4 * (q & 3); }
+// Radix-8 plan of length 2^LGN unrolled at compile time.  Pass P reads the
+// swizzled layout when P > 0 and writes it unless it is the last pass.
+template <typename R, int LGN, int S, int P, int LGNS, int OFF, int NBMAX, int BLOCK>
+MRM_D Cx<R>* fft_c_from(Cx<R>* a, Cx<R>* b, int nb, const Cx<R>* __restrict__ twp) {
+  constexpr int REM = LGN - LGNS;
+  if constexpr (REM <= 0) {
+    return a;
+  } else {
+    constexpr int LGR = REM >= 3 ? 3 : REM;
+    constexpr bool LAST = (REM - LGR) == 0;
+    stockham_pass_c<R, LGN, LGR, LGNS, OFF, (P > 0), !LAST, S, NBMAX, BLOCK>(a, b, nb, twp);
+    __syncthreads();
+    constexpr int NEXT_OFF = OFF + (LGNS > 0 ? ((1 << LGR) - 1) << LGNS : 0);
+    return fft_c_from<R, LGN, S, P + 1, LGNS + LGR, NEXT_OFF, NBMAX, BLOCK>(b, a, nb, twp);
+  }
+}
+
+// Transforms nb sequences held (natural order) in `a`, sequence stride
+// seq_stride(n); `b` is scratch of the same size; twp: the pass tables of
+// length 2^lgn.  Returns the buffer holding the (natural-order) result.  The
+// caller must __syncthreads() before the call.  Lengths above 2^LGMAX are
+// not compiled in (the caller checks lgn <= LGMAX).
+template <typename R, int S, int NBMAX, int BLOCK, int LGMAX = 12>
+MRM_D Cx<R>* block_fft_c(Cx<R>* a, Cx<R>* b, int lgn, int nb, const Cx<R>* __restrict__ twp) {
+  switch (lgn) {
+    case 1: return fft_c_from<R, 1, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 2: return fft_c_from<R, 2, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 3: return fft_c_from<R, 3, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 4: return fft_c_from<R, 4, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 5: return fft_c_from<R, 5, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 6: return fft_c_from<R, 6, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp);
+    case 7: if constexpr (LGMAX >= 7) return fft_c_from<R, 7, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+    case 8: if constexpr (LGMAX >= 8) return fft_c_from<R, 8, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+    case 9: if constexpr (LGMAX >= 9) return fft_c_from<R, 9, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+    case 10: if constexpr (LGMAX >= 10) return fft_c_from<R, 10, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+    case 11: if constexpr (LGMAX >= 11) return fft_c_from<R, 11, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+    default: if constexpr (LGMAX >= 12) return fft_c_from<R, 12, S, 0, 0, 0, NBMAX, BLOCK>(a, b, nb, twp); else return a;
+  }
+}
+
+// ---------------- run-time form (tensor FFT) ----------------
+
+MRM_HD int pad_stride(int n) { return n + (n >> 4) + 1; }
+MRM_D int padi(int i) { return i + (i >> 4); }
 
 // One Stockham pass.  PIN / POUT: input / output use the padded layout.
 template <typename R, int RADIX, int LGR, int S>
@@ -117,131 +233,38 @@ MRM_D void stockham_pass(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, 
         v[r] = cmul(v[r], w);
       }
     }
-    if (RADIX == 16) dft16<R, S>(v);
-    else if (RADIX == 8) dft8<R, S>(v);
+    if (RADIX == 8) dft8<R, S>(v);
     else if (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
     else dft2<R, S>(v);
     const int idxD = ((j >> lgNs) << (lgNs + LGR)) + k;
 #pragma unroll
-    for (int q = 0; q < RADIX; ++q) {
-      const int r = (RADIX == 16) ? dft16_out(q) : q;
-      const int i = idxD + r * Ns;
-      dst[pout ? padi(i) : i] = v[q];
-    }
-  }
-}
-
-// One Stockham pass with every size known at compile time (LGN: log2 length,
-// LGR: log2 radix, LGNS: log2 of the current sub-transform length, TWL: log2
-// of the twiddle table length, PIN/POUT: padded input/output layout).
-template <typename R, int LGN, int LGR, int LGNS, int TWL, bool PIN, bool POUT, int S>
-MRM_D void stockham_pass_c(const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out, int nb,
-                           const Cx<R>* __restrict__ tw) {
-  constexpr int RADIX = 1 << LGR;
-  constexpr int LGNR = LGN - LGR;
-  constexpr int NR = 1 << LGNR;
-  constexpr int NS = 1 << LGNS;
-  constexpr int STRIDE = (1 << LGN) + ((1 << LGN) >> 4) + 1;  // fft_stride(n)
-  const int total = nb << LGNR;
-  for (int q = threadIdx.x; q < total; q += blockDim.x) {
-    const int b = q >> LGNR, j = q & (NR - 1);
-    const Cx<R>* src = in + b * STRIDE;
-    Cx<R>* dst = out + b * STRIDE;
-    Cx<R> v[RADIX];
-#pragma unroll
-    for (int r = 0; r < RADIX; ++r) {
-      const int i = j + r * NR;
-      v[r] = src[PIN ? i + (i >> 4) : i];
-    }
-    const int k = j & (NS - 1);
-    if constexpr (LGNS > 0) {
-#pragma unroll
-      for (int r = 1; r < RADIX; ++r) {
-        Cx<R> w = tw[(k * r) << (TWL - LGNS - LGR)];
-        if (S > 0) w.y = -w.y;
-        v[r] = cmul(v[r], w);
-      }
-    }
-    if constexpr (RADIX == 16) dft16<R, S>(v);
-    else if constexpr (RADIX == 8) dft8<R, S>(v);
-    else if constexpr (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
-    else dft2<R, S>(v);
-    const int idxD = ((j >> LGNS) << (LGNS + LGR)) + k;
-#pragma unroll
     for (int q2 = 0; q2 < RADIX; ++q2) {
-      const int r = (RADIX == 16) ? dft16_out(q2) : q2;
-      const int i = idxD + r * NS;
-      dst[POUT ? i + (i >> 4) : i] = v[q2];
+      const int i = idxD + q2 * Ns;
+      dst[pout ? padi(i) : i] = v[q2];
     }
   }
 }
 
-// Radix-8 Stockham plan of length 2^LGN unrolled at compile time (the final
-// pass takes the 1, 2 or 3 remaining bits).  Pass P reads layout PIN = (P>0),
-// writes POUT = (P < last).
-template <typename R, int LGN, int TWL, int S, int P, int LGNS>
-MRM_D Cx<R>* fft_c_from(Cx<R>* a, Cx<R>* b, int nb, const Cx<R>* __restrict__ tw) {
-  constexpr int REM = LGN - LGNS;
-  if constexpr (REM <= 0) {
-    return a;
-  } else {
-    constexpr int LGR = REM >= 3 ? 3 : REM;
-    constexpr bool LAST = (REM - LGR) == 0;
-    stockham_pass_c<R, LGN, LGR, LGNS, TWL, (P > 0), !LAST, S>(a, b, nb, tw);
-    __syncthreads();
-    return fft_c_from<R, LGN, TWL, S, P + 1, LGNS + LGR>(b, a, nb, tw);
-  }
-}
-
-// Transforms nb sequences held (unpadded) in `a`, sequence stride
-// fft_stride(n); `b` is scratch of the same size.  Returns the buffer holding
-// the (unpadded) result.  The caller must __syncthreads() before the call.
-// TWOFF: the twiddle table has length 2^(lgn + TWOFF).
-template <typename R, int S, int TWOFF>
-MRM_D Cx<R>* block_fft_c(Cx<R>* a, Cx<R>* b, int lgn, int nb, const Cx<R>* __restrict__ tw) {
-  switch (lgn) {
-    case 1: return fft_c_from<R, 1, 1 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 2: return fft_c_from<R, 2, 2 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 3: return fft_c_from<R, 3, 3 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 4: return fft_c_from<R, 4, 4 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 5: return fft_c_from<R, 5, 5 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 6: return fft_c_from<R, 6, 6 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 7: return fft_c_from<R, 7, 7 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 8: return fft_c_from<R, 8, 8 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 9: return fft_c_from<R, 9, 9 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 10: return fft_c_from<R, 10, 10 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    case 11: return fft_c_from<R, 11, 11 + TWOFF, S, 0, 0>(a, b, nb, tw);
-    default: return fft_c_from<R, 12, 12, S, 0, 0>(a, b, nb, tw);  // TWOFF = 0 at the 4096 limit
-  }
-}
-
-// Radix plan: the largest radix R in {16, 8, 4} whose passes keep at least
-// half the block busy (nb * n / R >= BLOCK / 2); small batches use radix 4
-// so that more threads share each pass.
-MRM_D int fft_radix(int lgn, int nb, int block) {
-  const int n = 1 << lgn;
-  if ((nb * n) / 16 >= block / 2 && lgn >= 4) return 16;
-  if ((nb * n) / 8 >= block / 2 && lgn >= 3) return 8;
-  return 4;
-}
-
-template <typename R, int RADIX, int LGR, int S>
-MRM_D Cx<R>* fft_passes(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
-                        const Cx<R>* __restrict__ tw, int lgtw) {
+// Transforms nb sequences held (unpadded) in `a` with radix-8 passes and a
+// radix-2/4 tail; `b` is scratch of the same size; stride >= pad_stride(n);
+// tw: e^{-2 pi i k / 2^lgtw}.  Returns the buffer holding the (unpadded)
+// result.  The caller must __syncthreads() before the call.
+template <typename R, int S>
+MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
+                       const Cx<R>* __restrict__ tw, int lgtw) {
   int lgNs = 0;
-  const int nfull = lgn / LGR;
-  const int tail = lgn - nfull * LGR;  // 0..LGR-1 remaining bits
+  const int nfull = lgn / 3;
+  const int tail = lgn - nfull * 3;
   const int npass = nfull + (tail ? 1 : 0);
   int p = 0;
   for (int q = 0; q < nfull; ++q, ++p) {
-    stockham_pass<R, RADIX, LGR, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw, lgtw);
+    stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, p < npass - 1, tw, lgtw);
     __syncthreads();
     Cx<R>* t = a; a = b; b = t;
-    lgNs += LGR;
+    lgNs += 3;
   }
   if (tail) {
-    if (tail == 3) stockham_pass<R, 8, 3, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
-    else if (tail == 2) stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
+    if (tail == 2) stockham_pass<R, 4, 2, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
     else stockham_pass<R, 2, 1, S>(a, b, lgn, nb, stride, lgNs, p > 0, false, tw, lgtw);
     __syncthreads();
     Cx<R>* t = a; a = b; b = t;
@@ -249,48 +272,10 @@ MRM_D Cx<R>* fft_passes(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
   return a;
 }
 
-// Transforms nb sequences held (unpadded) in `a`; `b` is scratch of the same
-// size.  Returns the buffer holding the (unpadded) result.  The caller must
-// __syncthreads() before the call; on return the result is complete.
-template <typename R, int S>
-MRM_D Cx<R>* block_fft(Cx<R>* a, Cx<R>* b, int lgn, int nb, int stride,
-                       const Cx<R>* __restrict__ tw, int lgtw) {
-  const int radix = fft_radix(lgn, nb, blockDim.x);
-  if (radix == 16) return fft_passes<R, 16, 4, S>(a, b, lgn, nb, stride, tw, lgtw);
-  if (radix == 8) return fft_passes<R, 8, 3, S>(a, b, lgn, nb, stride, tw, lgtw);
-  return fft_passes<R, 4, 2, S>(a, b, lgn, nb, stride, tw, lgtw);
-}
-
-// e^{-2 pi i k / 2^lg} from the 4096-entry global table
+// e^{-2 pi i k / 2^lg} from the 4096-entry table of the run-time form
 template <typename R>
 MRM_D Cx<R> twiddle(const Cx<R>* __restrict__ tw, int k, int lg) {
   return tw[k << (kTwLog - lg)];
-}
-
-// Stages tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, from the global table.
-template <typename R>
-MRM_D void stage_twiddles(Cx<R>* __restrict__ tw_s, const Cx<R>* __restrict__ tw, int lg) {
-  const int n = 1 << lg;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) tw_s[k] = tw[k << (kTwLog - lg)];
-}
-
-// Fills tw_s[k] = e^{-2 pi i k / 2^lg}, k < 2^lg, with sincospi (accurate to
-// about one ulp; no memory round trip).
-MRM_D void make_twiddles(Cx<float>* __restrict__ tw_s, int lg) {
-  const int n = 1 << lg;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    float s, c;
-    sincospif(-2.0f * (float)k / (float)n, &s, &c);
-    tw_s[k] = Cx<float>{c, s};
-  }
-}
-MRM_D void make_twiddles(Cx<double>* __restrict__ tw_s, int lg) {
-  const int n = 1 << lg;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    double s, c;
-    sincospi(-2.0 * (double)k / (double)n, &s, &c);
-    tw_s[k] = Cx<double>{c, s};
-  }
 }
 
 // programmatic dependent launch (sm_90+): let the next kernel in the stream

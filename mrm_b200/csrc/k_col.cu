@@ -1,0 +1,195 @@
+// k_col.cu -- column kernels (FP32 packed tensor, FP64 complex tensor), their
+// launch wrappers, and the dispatch over the row shapes compiled in k_row_*.cu.
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace mrm {
+namespace {
+
+template <typename R, int V>
+struct ColV {
+  static constexpr ColVariant s = col_variant<R>(V);
+  static constexpr bool packed = sizeof(R) == sizeof(float);
+  static constexpr auto fn() { return col_kernel<R, packed, s.block, s.minb>; }
+};
+
+template <typename R>
+const void* col_fn_any(int v) {
+  switch (v) {
+    case 0: return (const void*)ColV<R, 0>::fn();
+    case 1: return (const void*)ColV<R, 1 < col_variant_count<R>() ? 1 : 0>::fn();
+    default: return (const void*)ColV<R, 2 < col_variant_count<R>() ? 2 : 0>::fn();
+  }
+}
+
+template <typename R, int V>
+cudaError_t col_launch_v(const ColLaunch& a, int istep, int flags) {
+  return launch_kernel(ColV<R, V>::fn(), dim3(a.ntasks), dim3(ColV<R, V>::s.block), a.smem, a.st, a.pdl,
+                       static_cast<const RunDev<R>*>(a.runs), a.tasks, static_cast<const Cx<R>*>(a.tw), istep,
+                       flags, a.err);
+}
+
+template <typename R>
+cudaError_t col_launch_any(int v, const ColLaunch& a, int istep, int flags) {
+  if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;
+  switch (v) {
+    case 0: return col_launch_v<R, 0>(a, istep, flags);
+    case 1: return col_launch_v<R, 1 < col_variant_count<R>() ? 1 : 0>(a, istep, flags);
+    default: return col_launch_v<R, 2 < col_variant_count<R>() ? 2 : 0>(a, istep, flags);
+  }
+}
+
+}  // namespace
+
+cudaError_t allow_smem(const void* kern, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> cur;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& c = cur[std::make_pair(dev, kern)];
+  if (bytes <= c) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) c = bytes;
+  return e;
+}
+
+// ---------------- row shapes (kernels in k_row_*.cu) ----------------
+template <typename R>
+static const RowOps* row_ops_of(int v) {
+  if (v < 0 || v >= row_variant_count<R>()) return nullptr;
+  if constexpr (sizeof(R) == sizeof(float)) {
+    switch (v) {
+      case 0: return &row_ops<float, 0>();
+      case 1: return &row_ops<float, 1>();
+      case 2: return &row_ops<float, 2>();
+      case 3: return &row_ops<float, 3>();
+      default: return &row_ops<float, 4>();
+    }
+  } else {
+    switch (v) {
+      case 0: return &row_ops<double, 0>();
+      case 1: return &row_ops<double, 1>();
+      default: return &row_ops<double, 2>();
+    }
+  }
+}
+static int stage_slot(int stage, bool stats) {
+  return stage == kInit ? 0 : stage == kPred ? 1 : stage == kCorr ? (stats ? 3 : 2) : 4;
+}
+
+template <typename R>
+static cudaError_t launch_row_any(int v, int stage, bool stats, const RowLaunch& a, int istep, int flags) {
+  const RowOps* o = row_ops_of<R>(v);
+  return o ? o->launch(stage, stats, a, istep, flags) : cudaErrorInvalidValue;
+}
+template <typename R>
+static cudaError_t row_allow_any(int v, const size_t* smem5) {
+  const RowOps* o = row_ops_of<R>(v);
+  if (!o) return cudaErrorInvalidValue;
+  for (int q = 0; q < 5; ++q) {
+    cudaError_t e = allow_smem(o->fn[q], smem5[q]);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+template <typename R>
+static cudaError_t row_occ_any(int v, int stage, size_t smem, int* blocks) {
+  const RowOps* o = row_ops_of<R>(v);
+  if (!o) return cudaErrorInvalidValue;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn[stage_slot(stage, false)],
+                                                       row_variant<R>(v).block, smem);
+}
+template <typename R>
+static cudaError_t row_load_any(int v) {
+  const RowOps* o = row_ops_of<R>(v);
+  if (!o) return cudaErrorInvalidValue;
+  for (int q = 0; q < 5; ++q) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[q]);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+template <typename R>
+static cudaError_t row_static_any(int v, int stage, bool stats, size_t* bytes) {
+  const RowOps* o = row_ops_of<R>(v);
+  if (!o) return cudaErrorInvalidValue;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[stage_slot(stage, stats)]);
+  if (e == cudaSuccess) *bytes = fa.sharedSizeBytes;
+  return e;
+}
+
+template <>
+cudaError_t launch_row<float>(int v, int stage, bool stats, const RowLaunch& a, int istep, int flags) {
+  return launch_row_any<float>(v, stage, stats, a, istep, flags);
+}
+template <>
+cudaError_t launch_row<double>(int v, int stage, bool stats, const RowLaunch& a, int istep, int flags) {
+  return launch_row_any<double>(v, stage, stats, a, istep, flags);
+}
+template <>
+cudaError_t row_allow_smem<float>(int v, const size_t* smem5) { return row_allow_any<float>(v, smem5); }
+template <>
+cudaError_t row_allow_smem<double>(int v, const size_t* smem5) { return row_allow_any<double>(v, smem5); }
+template <>
+cudaError_t row_occupancy<float>(int v, int stage, size_t smem, int* b) { return row_occ_any<float>(v, stage, smem, b); }
+template <>
+cudaError_t row_occupancy<double>(int v, int stage, size_t smem, int* b) { return row_occ_any<double>(v, stage, smem, b); }
+template <>
+cudaError_t row_load<float>(int v) { return row_load_any<float>(v); }
+template <>
+cudaError_t row_load<double>(int v) { return row_load_any<double>(v); }
+template <>
+cudaError_t row_static_smem<float>(int v, int stage, bool stats, size_t* b) { return row_static_any<float>(v, stage, stats, b); }
+template <>
+cudaError_t row_static_smem<double>(int v, int stage, bool stats, size_t* b) { return row_static_any<double>(v, stage, stats, b); }
+
+// ---------------- column shapes ----------------
+template <>
+cudaError_t launch_col<float>(int v, const ColLaunch& a, int istep, int flags) {
+  return col_launch_any<float>(v, a, istep, flags);
+}
+template <>
+cudaError_t launch_col<double>(int v, const ColLaunch& a, int istep, int flags) {
+  return col_launch_any<double>(v, a, istep, flags);
+}
+
+template <typename R>
+static cudaError_t col_allow_any(int v, size_t smem) {
+  if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;
+  return allow_smem(col_fn_any<R>(v), smem);
+}
+template <>
+cudaError_t col_allow_smem<float>(int v, size_t smem) { return col_allow_any<float>(v, smem); }
+template <>
+cudaError_t col_allow_smem<double>(int v, size_t smem) { return col_allow_any<double>(v, smem); }
+
+template <typename R>
+static cudaError_t col_occ_any(int v, size_t smem, int* blocks) {
+  if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, col_fn_any<R>(v), col_variant<R>(v).block, smem);
+}
+template <>
+cudaError_t col_occupancy<float>(int v, size_t smem, int* blocks) { return col_occ_any<float>(v, smem, blocks); }
+template <>
+cudaError_t col_occupancy<double>(int v, size_t smem, int* blocks) { return col_occ_any<double>(v, smem, blocks); }
+
+template <typename R>
+static cudaError_t col_load_any(int v) {
+  if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;
+  cudaFuncAttributes fa;
+  return cudaFuncGetAttributes(&fa, col_fn_any<R>(v));
+}
+template <>
+cudaError_t col_load<float>(int v) { return col_load_any<float>(v); }
+template <>
+cudaError_t col_load<double>(int v) { return col_load_any<double>(v); }
+
+}  // namespace mrm

@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "philox.cuh"
+#include "tma.cuh"
 
 namespace mrm {
 
@@ -120,236 +121,302 @@ MRM_D void block_reduce_record(double* rec, double* sred /* [32][kNPart] */, dou
   }
 }
 
-// Per-grain inputs gathered at the top of the row kernel.
-template <typename R>
-struct GrainIn {
-  V4<R> mf;      // state the field is evaluated on (m_n, or m* in the corrector)
-  V4<R> pa, pb;  // parameters
-  V4<R> cst;     // lattice exchange coefficients (j-1, i-1, i+1, j+1)
-  V4<R> nb[4];   // lattice neighbours
-  V4<R> dm, m0;  // corrector: predictor increment and m_n
-  V4<R> vu, vl;  // columnar interlayer partners
-  V4<R> ht;      // thermal field / sqrt(dt)
-  R cu, cl;
-};
-
 template <int STAGE, bool STATS>
 __host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STATS) ? 32 * kNPart : 1; }
 
+// ---------------- grain-row staging plan ----------------
+//
+// The row kernel copies the grain rows it works on into shared memory with
+// bulk copies issued by one thread: static rows (parameters, lattice
+// coefficients) before the dependency wait, the state rows after it.  The
+// field's rows carry a one-row halo on each side for the lattice stencil.
+// Everything is staged when it fits in the launch's staging capacity,
+// otherwise the block reads the same arrays from global memory.
+struct RowStage {
+  int pb, pa, xst, ucol, lcol;  // static rows (byte offsets, -1: not used)
+  int mf, m0, dm, ht, vu, vl;   // dynamic rows
+  int halo;                     // rows of halo on each side of mf (0 or 1)
+  int bytes;                    // total
+};
+
+// R-valued rows can be staged when a row is a whole number of 16-byte units
 template <typename R>
-__host__ __device__ constexpr int min_blocks() { return sizeof(R) == sizeof(float) ? 2 : 1; }
-// PREF: gather every per-grain input into registers before the inverse FFT
-// (latency-bound runs with few blocks per SM); otherwise load at use and run
-// four 256-thread blocks per SM (throughput-bound batches).
-template <typename R, bool PREF>
-__host__ __device__ constexpr int row_min_blocks() {
-  return PREF ? min_blocks<R>() : (sizeof(R) == sizeof(float) ? 4 : 2);
+MRM_HD bool rows_16b(int nx) { return ((long long)nx * (long long)sizeof(R)) % 16 == 0; }
+
+template <typename R>
+MRM_HD RowStage row_stage_plan(int stage, int nx, int nrows, bool stencil, bool ucol, bool lcol,
+                               bool thermal) {
+  RowStage p{-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, 0, 0};
+  const int v4row = nx * (int)sizeof(V4<R>);
+  const int rrow = nx * (int)sizeof(R);
+  int off = 0;
+  auto take = [&](int bytes) {
+    const int at = off;
+    off += bytes;
+    return at;
+  };
+  p.pb = take(nrows * v4row);
+  if (stage != kInit) {
+    p.pa = take(nrows * v4row);
+    if (stencil) p.xst = take(nrows * v4row);
+    if (ucol && rows_16b<R>(nx)) p.ucol = take(nrows * rrow);
+    if (lcol && rows_16b<R>(nx)) p.lcol = take(nrows * rrow);
+  }
+  p.halo = (stage != kInit && stencil) ? 1 : 0;
+  p.mf = take((nrows + 2 * p.halo) * v4row);
+  if (stage == kCorr) {
+    p.m0 = take(nrows * v4row);
+    p.dm = take(nrows * v4row);
+    if (thermal) p.ht = take(nrows * v4row);
+  }
+  if (stage != kInit) {
+    if (ucol) p.vu = take(nrows * v4row);
+    if (lcol) p.vl = take(nrows * v4row);
+  }
+  p.bytes = off;
+  return p;
 }
 
-template <typename R, int STAGE, bool STATS, int GPT, int BLOCK, bool PREF>
-__global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(const RunDev<R>* __restrict__ runs,
-                                                    const Task* __restrict__ tasks,
-                                                    const Cx<R>* __restrict__ tw, int istep,
-                                                    int flags, double* __restrict__ part) {
+// shared memory of the row kernel ahead of the grain staging area: twiddles
+// and the two FFT buffers sized for RPB rows
+template <typename R>
+MRM_HD int row_fft_smem(int lgpx, int rpb) {
+  const int M = 1 << (lgpx - 1);
+  return (row_tw_count(lgpx) + 2 * rpb * 3 * seq_stride(M)) * (int)sizeof(Cx<R>);
+}
+
+// Row kernel: one task = up to RPB grid rows of one layer of one run.
+//   kInit: forward row FFT of Ms*m (spectrum of the current state)
+//   kPred / kCorr: inverse row FFT of H^ -> H_demag, field assembly, Heun
+//                  stage, forward row FFT of Ms*m* / Ms*m_{n+1}
+//   kEval: inverse row FFT and field assembly only (H_demag and h stored)
+// stage_cap: bytes of dynamic shared memory available for grain staging.
+template <typename R, int STAGE, bool STATS, int RPB, int BLOCK, int MINB, int LGMAX>
+__global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __restrict__ runs,
+                                                          const Task* __restrict__ tasks,
+                                                          const Cx<R>* __restrict__ twg, int istep,
+                                                          int flags, double* __restrict__ part,
+                                                          int* __restrict__ err, int stage_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t bars[3];
+  __shared__ double sred[stats_slots<STAGE, STATS>()];
   pdl_launch_dependents();
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
   if (!rd.active) return;  // host-set, constant within a captured graph
+  if (rd.lgpx > LGMAX || tk.w > RPB) {  // shape not compiled into this variant (the host never picks it)
+    if (threadIdx.x == 0) atomicOr(err, kErrShape);
+    return;
+  }
 
   const int l = tk.y, row0 = tk.z, nrows = tk.w;
   const int nx = rd.nx, ny = rd.ny;
   const int lgpx = rd.lgpx, lgM = lgpx - 1, M = 1 << lgM, ph = M + 1;
-  const int cs = fft_stride(M);  // complex stride of one sequence in shared memory
+  const int cs = seq_stride(M);  // complex stride of one sequence in shared memory
   const int nseq = nrows * 3;
   const int ngr = nrows * nx;
   const LayerDev<R>& L = rd.L[l];
   const bool demag = rd.demag != 0;
   constexpr bool stats = (STAGE == kCorr) && STATS;
+  constexpr int NBMAX = 3 * RPB;
 
-  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // e^{-2 pi i k/px}, k < px
-  Cx<R>* bufA = tws + (1 << lgpx);
-  Cx<R>* bufB = bufA + nseq * cs;
-  __shared__ double sred[stats_slots<STAGE, STATS>()];
+  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // post twiddles | pass tables
+  const int ntw = row_tw_count(lgpx);
+  Cx<R>* bufA = tws + ntw;
+  Cx<R>* bufB = bufA + RPB * 3 * cs;
+  unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs);
+  const Cx<R>* twpost = tws;
+  const Cx<R>* twpass = tws + row_tw_post(lgpx);
 
-  // ---------------- static inputs (not written by the previous kernel) ----------------
-  if (demag) stage_twiddles(tws, tw, lgpx);
-  const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
   const LayerDev<R>* Lu = (l > 0) ? &rd.L[l - 1] : nullptr;
   const LayerDev<R>* Ll = (l + 1 < rd.nl) ? &rd.L[l + 1] : nullptr;
   const bool stencil = L.xst != nullptr;
   const bool ucol = L.ucol && Lu, lcol = L.lcol && Ll;
   const bool thermal = (STAGE == kPred || STAGE == kCorr) && L.thermal;
+  const V4<R>* __restrict__ mfield = (STAGE == kCorr) ? L.mp : L.m;
   const V4<R>* __restrict__ mother_u = Lu ? ((STAGE == kCorr) ? Lu->mp : Lu->m) : nullptr;
   const V4<R>* __restrict__ mother_l = Ll ? ((STAGE == kCorr) ? Ll->mp : Ll->m) : nullptr;
-  // inputs that the previous kernel does not write
-  auto load_static = [&](GrainIn<R>& G, int n) {
-    G.pb = L.pb[n];
-    if (STAGE == kInit) return;
-    G.pa = L.pa[n];
-    if (stencil) G.cst = L.xst[n];
-    if (ucol) G.cu = L.ucol[n];
-    if (lcol) G.cl = L.lcol[n];
-  };
-  // inputs written by the previous kernels of this step
-  auto load_dynamic = [&](GrainIn<R>& G, int n, int i, int j) {
-    if (STAGE == kInit) {
-      G.mf = L.m[n];
-      return;
-    }
-    G.mf = mfield[n];
-    if (stencil) {
-      const int jm = (j == 0 ? ny - 1 : j - 1), jp = (j == ny - 1 ? 0 : j + 1);
-      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
-      G.nb[0] = mfield[jm * nx + i];
-      G.nb[1] = mfield[j * nx + im];
-      G.nb[2] = mfield[j * nx + ip];
-      G.nb[3] = mfield[jp * nx + i];
-    }
-    if (STAGE == kCorr) {
-      G.dm = L.dm[n];
-      G.m0 = L.m[n];
-      if (thermal) G.ht = L.ht[n];
-    }
-    if (ucol) G.vu = mother_u[n];
-    if (lcol) G.vl = mother_l[n];
-  };
-  GrainIn<R> g[PREF ? GPT : 1];
-  if constexpr (PREF) {
-#pragma unroll
-    for (int q = 0; q < GPT; ++q) {
-      const int idx = threadIdx.x + q * BLOCK;
-      if (idx >= ngr) continue;
-      const int row = idx / nx, i = idx - row * nx;
-      load_static(g[q], (row0 + row) * nx + i);
-    }
-  }
+  const RowStage sp = row_stage_plan<R>(STAGE, nx, nrows, stencil, ucol, lcol, thermal);
+  // staged when the plan fits both the launch's staging capacity and the
+  // shared memory actually allocated behind the FFT buffers
+  const bool staged = sp.bytes <= stage_cap &&
+                      (long long)(stg - smem_raw) + sp.bytes <= (long long)dynamic_smem_bytes();
+  const int base = row0 * nx;
+  const int v4row = nx * (int)sizeof(V4<R>);
+  const int rrow = nx * (int)sizeof(R);
+  const bool inverse = (STAGE != kInit) && demag;
 
-  // predictor: Philox thermal normals (llg.f90:1083 h = H + hthm/sqrt(dt); the
-  // corrector reuses them, :1262-1266), drawn for the step counter read before
-  // the wait and redrawn only if the previous kernel advanced it meanwhile
-  const long long step_guess = rd.step + istep;
-  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
-  auto draw_one = [&](GrainIn<R>& G, int n, long long st) {
-    R gn[3];
-    thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)st, (unsigned long long)n, gn);
-    const R s = G.pb.w * tfac;
-    G.ht = V4<R>{s * gn[0], s * gn[1], s * gn[2], (R)0};
+  // bulk copy with the self-checks of the MRM_CHECKS build (source offset
+  // within its array, destination within the dynamic shared memory, 16-byte
+  // alignment)
+  auto copy = [&](uint64_t* bar, void* dst, const void* src, long long src_off_bytes, long long src_len_bytes,
+                  int bytes, int code) {
+#ifdef MRM_CHECKS
+    uint32_t dyn;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    const long long doff = (long long)smem_u32(dst) - (long long)smem_u32(smem_raw);
+    if (!MRM_CHECK(src_off_bytes >= 0 && src_off_bytes + bytes <= src_len_bytes, code, src_off_bytes)) return;
+    if (!MRM_CHECK(doff >= 0 && doff + bytes <= (long long)dyn, code + 1, doff)) return;
+    if (!MRM_CHECK(((((uintptr_t)src) | (uintptr_t)doff | (uintptr_t)bytes) & 15) == 0, code + 2,
+                   (long long)(uintptr_t)src))
+      return;
+#endif
+    bulk_copy(bar, dst, src, (uint32_t)bytes);
   };
-  auto draw = [&](long long st) {
-#pragma unroll
-    for (int q = 0; q < GPT; ++q) {
-      const int idx = threadIdx.x + q * BLOCK;
-      if (idx >= ngr) continue;
-      const int row = idx / nx, i = idx - row * nx;
-      draw_one(g[q], (row0 + row) * nx + i, st);
+  const long long nlay = (long long)nx * ny;  // grains per layer
+  const long long v4b = (long long)sizeof(V4<R>), rb = (long long)sizeof(R), cb = (long long)sizeof(Cx<R>);
+  MRM_CHECK(l >= 0 && l < rd.nl && row0 >= 0 && nrows >= 1 && row0 + nrows <= ny, 900, row0);
+
+  // ---------------- static inputs: twiddles, parameter rows ----------------
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (demag)
+      copy(&bars[0], tws, twg + rd.tw_row, rd.tw_row * cb, (long long)tw_table_size() * cb, ntw * (int)cb, 100);
+    if (staged) {
+      copy(&bars[0], stg + sp.pb, L.pb + base, base * v4b, nlay * v4b, nrows * v4row, 110);
+      if (sp.pa >= 0) copy(&bars[0], stg + sp.pa, L.pa + base, base * v4b, nlay * v4b, nrows * v4row, 120);
+      if (sp.xst >= 0) copy(&bars[0], stg + sp.xst, L.xst + base, base * v4b, nlay * v4b, nrows * v4row, 130);
+      if (sp.ucol >= 0) copy(&bars[0], stg + sp.ucol, L.ucol + base, base * rb, nlay * rb, nrows * rrow, 140);
+      if (sp.lcol >= 0) copy(&bars[0], stg + sp.lcol, L.lcol + base, base * rb, nlay * rb, nrows * rrow, 150);
     }
-  };
-  if constexpr (PREF) {
-    if (STAGE == kPred && thermal) draw(step_guess);
+    mbar_arrive(&bars[0]);
   }
 
   // ---------------- wait for the previous kernel's results ----------------
   pdl_wait();
   const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
-  if (!(flags & kFlagForce) && step >= rd.step_end) return;
-  if constexpr (PREF) {
-    if (STAGE == kPred && thermal && step != step_guess) draw(step);
-  }
-
-  // ---------------- dynamic per-grain inputs ----------------
-  if constexpr (PREF) {
-#pragma unroll
-    for (int q = 0; q < GPT; ++q) {
-      const int idx = threadIdx.x + q * BLOCK;
-      if (idx >= ngr) continue;
-      const int row = idx / nx, i = idx - row * nx, j = row0 + row;
-      load_dynamic(g[q], j * nx + i, i, j);
+  const bool run_it = (flags & kFlagForce) || step < rd.step_end;
+  if (threadIdx.x == 0) {
+    if (run_it && inverse)
+      for (int s = 0; s < nseq; ++s) {
+        const int row = s / 3, comp = s - 3 * row;
+        const long long off = ((long long)(l * 3 + comp) * ny + row0 + row) * rd.phs;
+        copy(&bars[1], bufB + s * cs, rd.spech + off, off * cb, (long long)rd.nl * 3 * ny * rd.phs * cb,
+             rd.phs * (int)cb, 200);
+      }
+    mbar_arrive(&bars[1]);
+    if (run_it && staged) {
+      if (sp.halo) {
+        const int jm = row0 == 0 ? ny - 1 : row0 - 1, jp = row0 + nrows == ny ? 0 : row0 + nrows;
+        copy(&bars[2], stg + sp.mf, mfield + (size_t)jm * nx, (long long)jm * nx * v4b, nlay * v4b, v4row, 210);
+        copy(&bars[2], stg + sp.mf + v4row, mfield + base, base * v4b, nlay * v4b, nrows * v4row, 220);
+        copy(&bars[2], stg + sp.mf + (nrows + 1) * v4row, mfield + (size_t)jp * nx, (long long)jp * nx * v4b,
+             nlay * v4b, v4row, 230);
+      } else {
+        copy(&bars[2], stg + sp.mf, mfield + base, base * v4b, nlay * v4b, nrows * v4row, 240);
+      }
+      if (sp.m0 >= 0) copy(&bars[2], stg + sp.m0, L.m + base, base * v4b, nlay * v4b, nrows * v4row, 250);
+      if (sp.dm >= 0) copy(&bars[2], stg + sp.dm, L.dm + base, base * v4b, nlay * v4b, nrows * v4row, 260);
+      if (sp.ht >= 0) copy(&bars[2], stg + sp.ht, L.ht + base, base * v4b, nlay * v4b, nrows * v4row, 270);
+      if (sp.vu >= 0) copy(&bars[2], stg + sp.vu, mother_u + base, base * v4b, nlay * v4b, nrows * v4row, 280);
+      if (sp.vl >= 0) copy(&bars[2], stg + sp.vl, mother_l + base, base * v4b, nlay * v4b, nrows * v4row, 290);
     }
+    mbar_arrive(&bars[2]);
+  }
+  // every barrier completes (an unused one on the arrive alone); a block whose
+  // copies do not land in time raises the error flag and leaves
+  auto leave_on_timeout = [&](bool ok) -> bool {
+    if (!__syncthreads_or(!ok)) return false;
+    if (threadIdx.x == 0) atomicOr(err, kErrBarrierTimeout);
+    for (int b = 0; b < 3; ++b) mbar_wait(&bars[b], 0);
+    return true;
+  };
+  if (!run_it) {
+    // nothing to do at this step: let the static copies land before leaving
+    leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0) & mbar_wait(&bars[2], 0));
+    return;
   }
 
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
   Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
-  if (STAGE != kInit && demag) {
-    __syncthreads();  // staged twiddles visible to every thread
+  if (inverse) {
+    if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0))) return;
     const int tot = nseq * M;
-    for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
-      Cx<R> xk[4], xm[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int idx = base + u * BLOCK;
-        if (idx < tot) {
-          const int s = idx >> lgM, k = idx & (M - 1);
-          const int row = s / 3, comp = s - 3 * row;
-          const Cx<R>* X = rd.spech + ((size_t)(l * 3 + comp) * ny + row0 + row) * ph;
-          xk[u] = X[k];
-          xm[u] = X[M - k];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int idx = base + u * BLOCK;
-        if (idx < tot) {
-          const int s = idx >> lgM, k = idx & (M - 1);
-          Cx<R> a = xk[u], b = xm[u];
-          if (k == 0) { a.y = 0; b.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
-          const Cx<R> e = cadd(a, cconj(b));
-          const Cx<R> o = csub(a, cconj(b));
-          const Cx<R> w = cconj(tws[k]);  // e^{+2 pi i k / px}
-          bufA[s * cs + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
-        }
-      }
+    for (int idx = threadIdx.x; idx < tot; idx += BLOCK) {
+      const int s = idx >> lgM, k = idx & (M - 1);
+      const Cx<R>* X = bufB + s * cs;
+      Cx<R> a = X[k], b = X[M - k];
+      if (k == 0) { a.y = 0; b.y = 0; }  // self-conjugate bins: imaginary parts ignored (c2r)
+      const Cx<R> e = cadd(a, cconj(b));
+      const Cx<R> o = csub(a, cconj(b));
+      const Cx<R> w = cconj(twpost[k]);  // e^{+2 pi i k / px}
+      bufA[s * cs + k] = cadd(e, cmul_i(cmul(o, w), (R)1));
     }
     __syncthreads();
-    Z = block_fft_c<R, +1, 1>(bufA, bufB, lgM, nseq, tws);
+    Z = block_fft_c<R, +1, NBMAX, BLOCK, LGMAX - 1>(bufA, bufB, lgM, nseq, twpass);
   }
   Cx<R>* W = (Z == bufA) ? bufB : bufA;  // real outputs of this stage (forward input)
   const R* hdr = reinterpret_cast<const R*>(Z);
   R* outr = reinterpret_cast<R*>(W);
   const int rs = 2 * cs;  // real stride of one sequence
+  if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[2], 0))) return;
 
   // ---------------- per-grain field + integrator stage ----------------
+  // row views: staged rows in shared memory, or the global arrays
+  const V4<R>* PB = staged ? reinterpret_cast<const V4<R>*>(stg + sp.pb) : L.pb + base;
+  const V4<R>* PA = (staged && sp.pa >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.pa) : L.pa + base;
+  const V4<R>* XS = (staged && sp.xst >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.xst) : L.xst + base;
+  const R* UC = (staged && sp.ucol >= 0) ? reinterpret_cast<const R*>(stg + sp.ucol) : (ucol ? L.ucol + base : nullptr);
+  const R* LC = (staged && sp.lcol >= 0) ? reinterpret_cast<const R*>(stg + sp.lcol) : (lcol ? L.lcol + base : nullptr);
+  const V4<R>* MF = staged ? reinterpret_cast<const V4<R>*>(stg + sp.mf) + sp.halo * nx : mfield + base;
+  const V4<R>* M0 = (staged && sp.m0 >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.m0) : L.m + base;
+  const V4<R>* DM = (staged && sp.dm >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.dm) : L.dm + base;
+  const V4<R>* HT = (staged && sp.ht >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.ht) : L.ht + base;
+  const V4<R>* VU = (staged && sp.vu >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.vu) : (ucol ? mother_u + base : nullptr);
+  const V4<R>* VL = (staged && sp.vl >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.vl) : (lcol ? mother_l + base : nullptr);
+  // field row rr in [-1, nrows] (lattice neighbours wrap periodically)
+  auto mf_row = [&](int rr) -> const V4<R>* {
+    if (staged) return MF + rr * nx;
+    int j = row0 + rr;
+    j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
+    return mfield + (size_t)j * nx;
+  };
+
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
   const double t_stage = (STAGE == kCorr) ? t_now + rd.dt : t_now;
   const double sc = ramp(L, t_stage);
   const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
+  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
   const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
+  const bool pow2x = (nx & (nx - 1)) == 0;
+  const int lgnx = __ffs(nx) - 1;
 
   double rec[stats ? kNPart : 1];
 #pragma unroll
   for (int s = 0; s < (stats ? kNPart : 1); ++s) rec[s] = 0.0;
 
-#pragma unroll
-  for (int q = 0; q < GPT; ++q) {
-    const int idx = threadIdx.x + q * BLOCK;
-    if (idx >= ngr) continue;
-    const int row = idx / nx, i = idx - row * nx;
-    const int n = (row0 + row) * nx + i;
-    GrainIn<R>& G = g[PREF ? q : 0];
-    if constexpr (!PREF) {
-      load_static(G, n);
-      load_dynamic(G, n, i, row0 + row);
-      if (STAGE == kPred && thermal) draw_one(G, n, step);
-    }
-    const R mse = G.pb.x;  // Ms * ms_scale
+  for (int idx = threadIdx.x; idx < ngr; idx += BLOCK) {
+    const int rr = pow2x ? (idx >> lgnx) : idx / nx;
+    const int i = idx - rr * nx;
+    const int q = idx;                // index within the task's rows
+    const int n = base + idx;         // grain index within the layer
+    const V4<R> pb = PB[q];
+    const R mse = pb.x;  // Ms * ms_scale
     if (STAGE == kInit) {
-      outr[(row * 3 + 0) * rs + i] = mse * G.mf.x;
-      outr[(row * 3 + 1) * rs + i] = mse * G.mf.y;
-      outr[(row * 3 + 2) * rs + i] = mse * G.mf.z;
+      const V4<R> mf = MF[q];
+      outr[(rr * 3 + 0) * rs + i] = mse * mf.x;
+      outr[(rr * 3 + 1) * rs + i] = mse * mf.y;
+      outr[(rr * 3 + 2) * rs + i] = mse * mf.z;
       continue;
     }
-    const V4<R> mf = G.mf;
+    const V4<R> mf = MF[q];
+    const V4<R> pa = PA[q];
     R hdx = 0, hdy = 0, hdz = 0;
     if (demag) {
-      hdx = hdr[(row * 3 + 0) * rs + i];
-      hdy = hdr[(row * 3 + 1) * rs + i];
-      hdz = hdr[(row * 3 + 2) * rs + i];
+      hdx = hdr[(rr * 3 + 0) * rs + i];
+      hdy = hdr[(rr * 3 + 1) * rs + i];
+      hdz = hdr[(rr * 3 + 2) * rs + i];
     }
     // h = h_app + h_demag + H_uni + H_ex (+ interlayer)   (field.f90:201,211-220)
     R hx = hax + hdx, hy = hay + hdy, hz = haz + hdz;
-    const V4<R> pa = G.pa, pb = G.pb;
     R e_k;
     {
       // get_uni_hk (field.f90:366-375); pa.w = Hk1*hk_scale, pb.y = Hk2*hk_scale
@@ -363,22 +430,30 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
     }
     R ex = 0, ey = 0, ez = 0;
     if (stencil) {
-      ex = G.cst.x * G.nb[0].x + G.cst.y * G.nb[1].x + G.cst.z * G.nb[2].x + G.cst.w * G.nb[3].x;
-      ey = G.cst.x * G.nb[0].y + G.cst.y * G.nb[1].y + G.cst.z * G.nb[2].y + G.cst.w * G.nb[3].y;
-      ez = G.cst.x * G.nb[0].z + G.cst.y * G.nb[1].z + G.cst.z * G.nb[2].z + G.cst.w * G.nb[3].z;
+      const V4<R> c = XS[q];
+      const V4<R>* rowc = mf_row(rr);
+      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
+      const V4<R> n0 = mf_row(rr - 1)[i], n1 = rowc[im], n2 = rowc[ip], n3 = mf_row(rr + 1)[i];
+      ex = c.x * n0.x + c.y * n1.x + c.z * n2.x + c.w * n3.x;
+      ey = c.x * n0.y + c.y * n1.y + c.z * n2.y + c.w * n3.y;
+      ez = c.x * n0.z + c.y * n1.z + c.z * n2.z + c.w * n3.z;
     } else if (L.xidx) {
       csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
     }
     R vx = 0, vy = 0, vz = 0;
     if (ucol) {
-      vx += G.cu * G.vu.x; vy += G.cu * G.vu.y; vz += G.cu * G.vu.z;
+      const R cu = UC[q];
+      const V4<R> vu = VU[q];
+      vx += cu * vu.x; vy += cu * vu.y; vz += cu * vu.z;
     } else if (L.uidx && Lu) {
-      csr_sum<R>(L.uidx, L.unbr, L.ucoef, (STAGE == kCorr) ? Lu->mp : Lu->m, n, vx, vy, vz);
+      csr_sum<R>(L.uidx, L.unbr, L.ucoef, mother_u, n, vx, vy, vz);
     }
     if (lcol) {
-      vx += G.cl * G.vl.x; vy += G.cl * G.vl.y; vz += G.cl * G.vl.z;
+      const R cl = LC[q];
+      const V4<R> vl = VL[q];
+      vx += cl * vl.x; vy += cl * vl.y; vz += cl * vl.z;
     } else if (L.lidx && Ll) {
-      csr_sum<R>(L.lidx, L.lnbr, L.lcoef, (STAGE == kCorr) ? Ll->mp : Ll->m, n, vx, vy, vz);
+      csr_sum<R>(L.lidx, L.lnbr, L.lcoef, mother_l, n, vx, vy, vz);
     }
     hx += ex + vx;
     hy += ey + vy;
@@ -389,13 +464,24 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
       continue;
     }
 
-    // thermal field / sqrt(dt) (llg.f90:1083): drawn by the predictor, reused by the corrector
+    // thermal field / sqrt(dt) (llg.f90:1083): drawn by the predictor from the
+    // step counter, reused by the corrector (:1262-1266)
     R htx = 0, hty = 0, htz = 0;
     if (thermal) {
-      htx = G.ht.x;
-      hty = G.ht.y;
-      htz = G.ht.z;
-      if (STAGE == kPred) L.ht[n] = G.ht;
+      if (STAGE == kPred) {
+        R gn[3];
+        thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)n, gn);
+        const R s = pb.w * tfac;
+        htx = s * gn[0];
+        hty = s * gn[1];
+        htz = s * gn[2];
+        L.ht[n] = V4<R>{htx, hty, htz, (R)0};
+      } else {
+        const V4<R> ht = HT[q];
+        htx = ht.x;
+        hty = ht.y;
+        htz = ht.z;
+      }
     }
     const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
     V4<R> mn;
@@ -415,10 +501,11 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
         L.dm[n] = V4<R>{dx, dy, dz, (R)0};
         m0 = mf;
       } else {
-        dx = (R)0.5 * (dx + G.dm.x);
-        dy = (R)0.5 * (dy + G.dm.y);
-        dz = (R)0.5 * (dz + G.dm.z);
-        m0 = G.m0;
+        const V4<R> d1 = DM[q];
+        dx = (R)0.5 * (dx + d1.x);
+        dy = (R)0.5 * (dy + d1.y);
+        dz = (R)0.5 * (dz + d1.z);
+        m0 = M0[q];
       }
       mn.x = m0.x + dx;
       mn.y = m0.y + dy;
@@ -436,15 +523,15 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
       if (y > (R)0) {
         mn.x = hx / y; mn.y = hy / y; mn.z = hz / y;
       } else {
-        mn = (STAGE == kCorr) ? G.m0 : mf;
+        mn = (STAGE == kCorr) ? M0[q] : mf;
       }
     }
     mn.w = (R)0;
     if (STAGE == kPred) L.mp[n] = mn;
     else L.m[n] = mn;
-    outr[(row * 3 + 0) * rs + i] = mse * mn.x;
-    outr[(row * 3 + 1) * rs + i] = mse * mn.y;
-    outr[(row * 3 + 2) * rs + i] = mse * mn.z;
+    outr[(rr * 3 + 0) * rs + i] = mse * mn.x;
+    outr[(rr * 3 + 1) * rs + i] = mse * mn.y;
+    outr[(rr * 3 + 2) * rs + i] = mse * mn.z;
 
     if constexpr (stats) {
       const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 0}
@@ -481,7 +568,7 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
   }
   if (STAGE == kEval || !demag) return;
 
-  // ---------------- forward row transform of Ms*m -> spectrum rows ----------------
+  // ---------------- forward row transform of Ms*m -> spectrum columns ----------------
   const int two_m = 2 * M;
   if (nx < two_m) {
     const int pad = two_m - nx;
@@ -492,89 +579,145 @@ __global__ void __launch_bounds__(BLOCK, row_min_blocks<R, PREF>()) row_kernel(c
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
-  Cx<R>* Y = block_fft_c<R, -1, 1>(W, scratch, lgM, nseq, tws);
-  for (int idx = threadIdx.x; idx < nseq * ph; idx += BLOCK) {
-    const int s = idx / ph, k = idx - s * ph;
-    const int row = s / 3, comp = s - 3 * row;
-    const Cx<R> yk = Y[s * cs + (k & (M - 1))];
-    const Cx<R> ymk = cconj(Y[s * cs + ((M - k) & (M - 1))]);
-    const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
-    const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
-    // X[k] = e - i w^k o,  w = e^{-2 pi i / px}
-    const Cx<R> wo = cmul(tws[k & (two_m - 1)], o);
-    rd.specx[((size_t)(l * 3 + comp) * ph + k) * ny + row0 + row] = csub(e, cmul_i(wo, (R)1));
+  Cx<R>* Y = block_fft_c<R, -1, NBMAX, BLOCK, LGMAX - 1>(W, scratch, lgM, nseq, twpass);
+  // X[k] = e - i w^k o (w = e^{-2 pi i / px}); a task's rows are adjacent in
+  // the column-major spectrum, so consecutive threads take consecutive rows
+  const int lgr = nrows > 1 ? 32 - __clz(nrows - 1) : 0;
+  const int rmask = (1 << lgr) - 1;
+  const int nys = rd.nys;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    Cx<R>* dst = rd.specx + (size_t)(l * 3 + comp) * ph * nys + row0;
+    for (int t = threadIdx.x; t < (ph << lgr); t += BLOCK) {
+      const int row = t & rmask, k = t >> lgr;
+      if (row >= nrows) continue;
+      const Cx<R>* Ys = Y + (row * 3 + comp) * cs;
+      const Cx<R> yk = Ys[k & (M - 1)];
+      const Cx<R> ymk = cconj(Ys[(M - k) & (M - 1)]);
+      const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
+      const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
+      const Cx<R> wo = cmul(twpost[k], o);
+      if (!MRM_CHECK((long long)(l * 3 + comp) * ph * nys + (long long)k * nys + row0 + row <
+                         (long long)rd.nl * 3 * ph * nys, 300, k))
+        continue;
+      dst[(size_t)k * nys + row] = csub(e, cmul_i(wo, (R)1));
+    }
   }
 }
 
 // Column kernel: per spectral column k, forward FFT along y of the 3*nl
-// half-spectra, H^_a = sum_b N^_ab M^_b, inverse FFT, written back in place.
+// half-spectra, H^_a = sum_b N^_ab M^_b, inverse FFT, written back row-major.
 // PACKED: tensor stored as one real per (k, 0<=ky<=py/2) and component (the
 // parity of each component restores the rest); otherwise the full complex
-// tensor spectrum [k][pair][9][py] is used (FP64 runs).
-// packed tensor slice of a column task staged in shared memory up to this size
+// tensor spectrum [k][pair][9][py] is used (FP64 runs).  The columns and the
+// task's packed tensor slice arrive by bulk copies.
 constexpr int kTensSliceBytes = 48 * 1024;
 template <typename R>
 MRM_HD bool tens_slice_fits(int reals) { return (size_t)reals * sizeof(R) <= (size_t)kTensSliceBytes; }
 
-template <typename R, bool PACKED, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, PACKED ? 3 : 1) col_kernel(const RunDev<R>* __restrict__ runs,
-                                                    const Task* __restrict__ tasks,
-                                                    const Cx<R>* __restrict__ tw, int istep,
-                                                    int flags) {
+template <typename R>
+MRM_HD int col_fft_smem(int lgpy, int nseq) {
+  return (col_tw_count(lgpy) + 2 * nseq * seq_stride(1 << lgpy)) * (int)sizeof(Cx<R>);
+}
+
+template <typename R, bool PACKED, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __restrict__ runs,
+                                                          const Task* __restrict__ tasks,
+                                                          const Cx<R>* __restrict__ twg, int istep,
+                                                          int flags, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t bars[2];
   pdl_launch_dependents();
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
   if (!rd.active || !rd.demag) return;
   const int k0 = tk.y, nc = tk.z;
   const int nl = rd.nl, ny = rd.ny, py = rd.py, lgpy = rd.lgpy;
-  const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1;
-  const int cs = fft_stride(py);
+  const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1, pyhs = rd.pyhs, nys = rd.nys, phs = rd.phs;
+  const int cs = seq_stride(py);
   const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
-  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // e^{-2 pi i k/py}, k < py
-  Cx<R>* A = tws + py;
+  Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);
+  const int ntw = col_tw_count(lgpy);
+  Cx<R>* A = tws + ntw;
   Cx<R>* B = A + nseq * cs;
-
-  // static inputs: twiddles and this task's packed tensor slice (when it fits)
-  stage_twiddles(tws, tw, lgpy);
   const int npair = nl * nl;
-  const int tslice = nc * npair * 9 * pyh;  // reals
-  const bool tsm = PACKED && tens_slice_fits<R>(tslice);
+  const int tslice = nc * npair * 9 * pyhs;  // reals
   R* Ts = reinterpret_cast<R*>(B + nseq * cs);
-  if (tsm) {
-    const R* src = rd.tens + (size_t)k0 * npair * 9 * pyh;  // columns k0.. are contiguous
-    for (int q = threadIdx.x; q < tslice; q += BLOCK) Ts[q] = __ldg(src + q);
+  // the slice is staged only where the launch's shared memory holds it (the
+  // host sizes it for the largest task, which may not fit when a smaller last
+  // task would)
+  const bool tsm = PACKED && tens_slice_fits<R>(tslice) &&
+                   (long long)(reinterpret_cast<unsigned char*>(Ts) - smem_raw) + (long long)tslice * sizeof(R) <=
+                       (long long)dynamic_smem_bytes();
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // static inputs: twiddles and this task's packed tensor slice (columns k0.. are contiguous)
+  auto copy = [&](uint64_t* bar, void* dst, const void* src, long long src_off_bytes, long long src_len_bytes,
+                  int bytes, int code) {
+#ifdef MRM_CHECKS
+    uint32_t dyn;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    const long long doff = (long long)smem_u32(dst) - (long long)smem_u32(smem_raw);
+    if (!MRM_CHECK(src_off_bytes >= 0 && src_off_bytes + bytes <= src_len_bytes, code, src_off_bytes)) return;
+    if (!MRM_CHECK(doff >= 0 && doff + bytes <= (long long)dyn, code + 1, doff)) return;
+    if (!MRM_CHECK(((((uintptr_t)src) | (uintptr_t)doff | (uintptr_t)bytes) & 15) == 0, code + 2,
+                   (long long)(uintptr_t)src))
+      return;
+#endif
+    bulk_copy(bar, dst, src, (uint32_t)bytes);
+  };
+  const long long cb = (long long)sizeof(Cx<R>);
+  const long long tens_len = PACKED ? (long long)ph * npair * 9 * pyhs * (long long)sizeof(R)
+                                    : (long long)ph * npair * 9 * py * cb;
+  MRM_CHECK(k0 >= 0 && nc >= 1 && k0 + nc <= ph, 500, k0);
+  if (threadIdx.x == 0) {
+    copy(&bars[0], tws, twg + rd.tw_col, rd.tw_col * cb, (long long)tw_table_size() * cb, ntw * (int)cb, 400);
+    if (tsm) {
+      const long long off = (long long)k0 * npair * 9 * pyhs;
+      copy(&bars[0], Ts, rd.tens + off, off * (long long)sizeof(R), tens_len, tslice * (int)sizeof(R), 410);
+    }
+    mbar_arrive(&bars[0]);
   }
   pdl_wait();
-  if (!(flags & kFlagForce) && rd.step + istep >= rd.step_end) return;
-
-  // batched, coalesced loads of the columns (column-major M^; rows >= ny are the zero padding)
-  const int tot = nseq * py;
-  for (int base = threadIdx.x; base < tot; base += 4 * BLOCK) {
-    Cx<R> v[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int idx = base + u * BLOCK;
-      v[u] = Cx<R>{(R)0, (R)0};
-      if (idx < tot) {
-        const int j = idx & (py - 1), s = idx >> lgpy;  // s = c*nl*3 + lc
+  const bool run_it = (flags & kFlagForce) || rd.step + istep < rd.step_end;
+  if (threadIdx.x == 0) {
+    if (run_it)
+      for (int s = 0; s < nseq; ++s) {
         const int c = s / (nl * 3), lc = s - c * nl * 3;
-        if (j < ny) v[u] = rd.specx[((size_t)lc * ph + k0 + c) * ny + j];
+        const long long off = ((long long)lc * ph + k0 + c) * nys;
+        copy(&bars[1], A + s * cs, rd.specx + off, off * cb, (long long)nl * 3 * ph * nys * cb, nys * (int)cb, 420);
       }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int idx = base + u * BLOCK;
-      if (idx < tot) A[(idx >> lgpy) * cs + (idx & (py - 1))] = v[u];
+    mbar_arrive(&bars[1]);
+  }
+  const bool ok = mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicOr(err, kErrBarrierTimeout);
+    mbar_wait(&bars[0], 0);
+    mbar_wait(&bars[1], 0);
+    return;
+  }
+  if (!run_it) return;
+
+  // rows >= ny of the columns are the zero padding
+  if (ny < py) {
+    const int pad = py - ny;
+    for (int idx = threadIdx.x; idx < nseq * pad; idx += BLOCK) {
+      const int s = idx / pad, j = ny + (idx - s * pad);
+      A[s * cs + j] = Cx<R>{(R)0, (R)0};
     }
   }
   __syncthreads();
-  Cx<R>* F = block_fft_c<R, -1, 0>(A, B, lgpy, nseq, tws);
+  Cx<R>* F = block_fft_c<R, -1, 0, BLOCK>(A, B, lgpy, nseq, tws);
   Cx<R>* G = (F == A) ? B : A;
 
   // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
   for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK) {
-    const int c = idx / py, ky = idx - c * py;
+    const int c = idx >> lgpy, ky = idx & (py - 1);
     for (int ko = 0; ko < nl; ++ko) {
       Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
       for (int ks = 0; ks < nl; ++ks) {
@@ -584,11 +727,15 @@ __global__ void __launch_bounds__(BLOCK, PACKED ? 3 : 1) col_kernel(const RunDev
         if constexpr (PACKED) {
           const bool upper = ky > (py >> 1);
           const int kyh = upper ? py - ky : ky;
-          const size_t off = ((size_t)c * npair + ks * nl + ko) * 9 * pyh;
-          const R* Tp = tsm ? Ts + off : rd.tens + (size_t)k0 * npair * 9 * pyh + off;
+          const size_t off = ((size_t)c * npair + ks * nl + ko) * 9 * pyhs;
+          const R* Tp = tsm ? Ts + off : rd.tens + (size_t)k0 * npair * 9 * pyhs + off;
           R tv[9];
+          const bool tok = MRM_CHECK(
+              tsm || ((long long)k0 * npair * 9 * pyhs + (long long)off + 8 * pyhs + kyh) * (long long)sizeof(R) <
+                         tens_len,
+              430, kyh);
 #pragma unroll
-          for (int cc = 0; cc < 9; ++cc) tv[cc] = Tp[cc * pyh + kyh];
+          for (int cc = 0; cc < 9; ++cc) tv[cc] = tok ? Tp[cc * pyhs + kyh] : (R)0;
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -616,13 +763,15 @@ __global__ void __launch_bounds__(BLOCK, PACKED ? 3 : 1) col_kernel(const RunDev
     }
   }
   __syncthreads();
-  Cx<R>* Hs = block_fft_c<R, +1, 0>(G, F, lgpy, nseq, tws);
+  Cx<R>* Hs = block_fft_c<R, +1, 0, BLOCK>(G, F, lgpy, nseq, tws);
 
+  (void)pyh;
   const int tot2 = nseq * ny;
   for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
     const int c = idx % nc, rest = idx / nc;
     const int j = rest % ny, lc = rest / ny;
-    rd.spech[((size_t)lc * ny + j) * ph + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
+    if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nl * 3 * ny * phs, 440, idx)) continue;
+    rd.spech[((size_t)lc * ny + j) * phs + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
   }
 }
 

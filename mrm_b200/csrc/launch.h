@@ -1,0 +1,122 @@
+// launch.h -- host-side interface between the engine (mrm_gpu.cu) and the
+// translation units that compile the row and column kernels (k_row_f32.cu,
+// k_row_f64.cu, k_col.cu), so that the heavy kernel instantiations build in
+// parallel.  Kernel shapes are compiled variants; the engine picks one per
+// launch (default heuristic or the autotuner).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mrm {
+
+// Row kernel shapes: at most `rpb` grid rows per block, `block` threads,
+// `minb` resident blocks per SM requested from the register allocator, FFT
+// grids of at most 2^lgmax columns (row transforms of 2^(lgmax-1) points).
+struct RowVariant {
+  int rpb, block, minb, lgmax;
+};
+constexpr int kRowVariantsF32 = 5;
+constexpr RowVariant kRowF32[kRowVariantsF32] = {
+    {1, 256, 4, 12}, {1, 128, 8, 12}, {2, 256, 3, 11}, {4, 256, 2, 10}, {8, 256, 2, 8}};
+constexpr int kRowVariantsF64 = 3;
+constexpr RowVariant kRowF64[kRowVariantsF64] = {{1, 256, 2, 12}, {2, 256, 2, 11}, {8, 256, 1, 8}};
+template <typename R>
+constexpr int row_variant_count() { return sizeof(R) == sizeof(float) ? kRowVariantsF32 : kRowVariantsF64; }
+template <typename R>
+constexpr RowVariant row_variant(int v) { return sizeof(R) == sizeof(float) ? kRowF32[v] : kRowF64[v]; }
+
+// Column kernel shapes (the columns per task are chosen at run time).
+struct ColVariant {
+  int block, minb;
+};
+constexpr int kColVariantsF32 = 3;
+constexpr ColVariant kColF32[kColVariantsF32] = {{256, 3}, {128, 6}, {256, 2}};
+constexpr int kColVariantsF64 = 2;
+constexpr ColVariant kColF64[kColVariantsF64] = {{256, 1}, {128, 2}};
+template <typename R>
+constexpr int col_variant_count() { return sizeof(R) == sizeof(float) ? kColVariantsF32 : kColVariantsF64; }
+template <typename R>
+constexpr ColVariant col_variant(int v) { return sizeof(R) == sizeof(float) ? kColF32[v] : kColF64[v]; }
+
+struct RowLaunch;
+// entry points of one compiled row shape (defined in its own translation unit)
+struct RowOps {
+  cudaError_t (*launch)(int stage, bool stats, const RowLaunch& a, int istep, int flags);
+  const void* fn[5];  // kInit, kPred, kCorr, kCorr with reductions, kEval
+};
+template <typename R, int V>
+const RowOps& row_ops();
+
+struct RowLaunch {
+  cudaStream_t st;
+  const void* runs;  // RunDev<R>[]
+  const Task* tasks;
+  const void* tw;    // Cx<R> global twiddle table
+  double* part;
+  int* err;
+  int ntasks;
+  size_t smem;
+  int stage_cap;
+  bool pdl;          // programmatic stream serialization with the previous kernel
+};
+
+struct ColLaunch {
+  cudaStream_t st;
+  const void* runs;
+  const Task* tasks;
+  const void* tw;
+  int* err;
+  int ntasks;
+  size_t smem;
+  bool pdl;
+};
+
+// stage: kInit, kPred, kCorr, kEval; stats selects the corrector with reductions
+template <typename R>
+cudaError_t launch_row(int variant, int stage, bool stats, const RowLaunch& a, int istep, int flags);
+// lets each stage kernel of a variant use smem5[slot] bytes of dynamic shared
+// memory on the current device (slots: kInit, kPred, kCorr, kCorr with
+// reductions, kEval; the limit only grows)
+template <typename R>
+cudaError_t row_allow_smem(int variant, const size_t* smem5);
+template <typename R>
+cudaError_t row_occupancy(int variant, int stage, size_t smem, int* blocks_per_sm);
+// loads every stage's code (CUDA lazy loading would load it at first launch)
+template <typename R>
+cudaError_t row_load(int variant);
+// static shared memory of a stage (bytes)
+template <typename R>
+cudaError_t row_static_smem(int variant, int stage, bool stats, size_t* bytes);
+
+template <typename R>
+cudaError_t launch_col(int variant, const ColLaunch& a, int istep, int flags);
+template <typename R>
+cudaError_t col_allow_smem(int variant, size_t smem);
+template <typename R>
+cudaError_t col_occupancy(int variant, size_t smem, int* blocks_per_sm);
+template <typename R>
+cudaError_t col_load(int variant);
+
+// launches with or without programmatic stream serialization
+template <typename... KArgs, typename... Args>
+cudaError_t launch_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                          Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+// raises a kernel's dynamic shared-memory limit on the current device; the
+// limit only grows, so engines sharing a kernel never lower it for each other
+cudaError_t allow_smem(const void* kern, size_t bytes);
+
+}  // namespace mrm

@@ -20,13 +20,13 @@
 #include "../../include/mrm_gpu.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "launch.h"
 #include "tensor.cuh"
 
 using namespace mrm;
 
 namespace {
 
-constexpr int kBlock = 256;
 constexpr int kGraphSteps = 16;
 constexpr size_t kMaxSmem = 227 * 1024;
 
@@ -98,15 +98,26 @@ struct Engine {
   Task* d_rtasks = nullptr;
   Task* d_ctasks = nullptr;
   int nrt = 0, nct = 0, rt_cap = 0, ct_cap = 0;
-  size_t smem_row = 0, smem_col = 0;
-  int rowcfg = 0;
-  bool pref = true;  // row kernel gathers grain inputs up front (few blocks per SM)
+  int rowv = 0, colv = 0, cpt = 0;  // row / column shapes (launch.h), columns per task (0: default)
+  bool shape_forced = false;         // shapes set by the caller instead of tuned
+  int force_rowv = 0, force_colv = 0, force_cpt = 0;
+  bool autotune = true;
+  size_t smem_row[5] = {0, 0, 0, 0, 0};  // per launch slot: init, pred, corr, corr+stats, eval
+  int stage_cap[5] = {0, 0, 0, 0, 0};
+  size_t smem_col = 0;
+  // the corrector with reductions always runs row shape 0 over one-row tasks,
+  // so that the FP64 reductions do not depend on the tuned shapes
+  Task* d_stasks = nullptr;
+  int nst = 0, st_cap = 0;
+  size_t smem_stats = 0;
+  int cap_stats = 0;
+  int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
   StatsDev* h_stats = nullptr;  // pinned
   int stats_cap = 0;
-  void* d_tw = nullptr;  // Cx<R>[kTwN]
+  void* d_tw = nullptr;  // Cx<R>[tw_table_size()] (fft.cuh layout)
   bool tables_dirty = true;
   bool desc_dirty = true;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (steps, with stats)
@@ -166,23 +177,45 @@ int engine_init(Engine* e, int prec, int dev) {
   if (dev < 0 || dev >= ndev) return set_err(errp, MRM_ERR_ARG, "device %d out of range (%d)", dev, ndev);
   CK(cudaSetDevice(dev));
   CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
-  // twiddles e^{-2 pi i k / 4096}, computed in FP64
-  std::vector<double> tw(2 * kTwN);
-  for (int k = 0; k < kTwN; ++k) {
-    double a = -2.0 * M_PI * (double)k / (double)kTwN;
-    tw[2 * k] = std::cos(a);
-    tw[2 * k + 1] = std::sin(a);
+  // twiddle table of every row / column FFT length (fft.cuh layout), in FP64
+  std::vector<double> tw(2 * (size_t)tw_table_size(), 0.0);
+  auto put = [&](int at, double num, double den) {
+    const double a = -2.0 * M_PI * num / den;
+    tw[2 * (size_t)at] = std::cos(a);
+    tw[2 * (size_t)at + 1] = std::sin(a);
+  };
+  auto pass_tables = [&](int at, int lgn) {
+    for (int lgns = 0; lgns < lgn;) {
+      const int lgr = pass_lgr(lgn, lgns), R = 1 << lgr, NS = 1 << lgns;
+      if (lgns > 0) {
+        for (int r = 1; r < R; ++r)
+          for (int k = 0; k < NS; ++k) put(at + (r - 1) * NS + k, (double)k * r, (double)NS * R);
+        at += (R - 1) * NS;
+      }
+      lgns += lgr;
+    }
+  };
+  for (int lg = 1; lg <= kTwLog; ++lg) {
+    const int o = row_tw_off(lg), M = 1 << (lg - 1);
+    for (int k = 0; k <= M; ++k) put(o + k, (double)k, (double)(2 * M));
+    pass_tables(o + row_tw_post(lg), lg - 1);
+    pass_tables(col_tw_off(lg), lg);
   }
+  const size_t ntw = (size_t)tw_table_size();
   if (prec == MRM_FP64) {
-    int rc = dmalloc(errp, &e->d_tw, sizeof(double) * 2 * kTwN);
+    int rc = dmalloc(errp, &e->d_tw, sizeof(double) * 2 * ntw);
     if (rc) return rc;
-    CK(cudaMemcpy(e->d_tw, tw.data(), sizeof(double) * 2 * kTwN, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_tw, tw.data(), sizeof(double) * 2 * ntw, cudaMemcpyHostToDevice));
   } else {
-    std::vector<float> twf(2 * kTwN);
-    for (int k = 0; k < 2 * kTwN; ++k) twf[k] = (float)tw[k];
-    int rc = dmalloc(errp, &e->d_tw, sizeof(float) * 2 * kTwN);
+    std::vector<float> twf(2 * ntw);
+    for (size_t k = 0; k < 2 * ntw; ++k) twf[k] = (float)tw[k];
+    int rc = dmalloc(errp, &e->d_tw, sizeof(float) * 2 * ntw);
     if (rc) return rc;
-    CK(cudaMemcpy(e->d_tw, twf.data(), sizeof(float) * 2 * kTwN, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_tw, twf.data(), sizeof(float) * 2 * ntw, cudaMemcpyHostToDevice));
+  }
+  {
+    int rc = dmalloc(errp, (void**)&e->d_err, 4 * sizeof(int));  // flags, first check code, its value
+    if (rc) return rc;
   }
   e->init_done = true;
   return MRM_OK;
@@ -195,11 +228,13 @@ void engine_free(Engine* e) {
   dfree(e->d_runs);
   dfree(e->d_rtasks);
   dfree(e->d_ctasks);
+  dfree(e->d_stasks);
   dfree(e->d_part);
   dfree(e->d_stats);
   if (e->h_stats) cudaFreeHost(e->h_stats);
   e->h_stats = nullptr;
   dfree(e->d_tw);
+  dfree(e->d_err);
   if (e->st) cudaStreamDestroy(e->st);
   e->st = nullptr;
 }
@@ -215,40 +250,64 @@ void fft_grid(const mrm_geom& g, int* px, int* py) {
   }
 }
 
-int rows_per_task(const mrm_gpu* r) {
-  if (r->g.nx >= kBlock) return 1;
-  return std::max(1, std::min(r->g.ny, kBlock / std::max(1, r->g.nx)));
+// padded strides (16-byte aligned rows for the bulk copies of the kernels)
+int spec_row_stride(int px) { return even_up(px / 2 + 1); }  // complex per spectrum row
+int spec_col_stride(int ny) { return even_up(ny); }          // complex per spectrum column
+int tens_row_stride(int py) { return (py / 2 + 1 + 3) & ~3; } // reals per packed tensor row
+
+// default columns per column task: about 16 complex values per thread of a 256-thread block
+int default_cols(const mrm_gpu* r) {
+  const int ph = r->px / 2 + 1;
+  return std::max(1, std::min(ph, 256 * 16 / (3 * r->nl * r->py)));
 }
-// columns per column task: enough sequences for one radix-16 butterfly per thread
-int cols_per_task(const mrm_gpu* r) {
-  int ph = r->px / 2 + 1;
-  return std::max(1, std::min(ph, kBlock * 16 / (3 * r->nl * r->py)));
+int cols_per_task(const Engine* e, const mrm_gpu* r) {
+  const int ph = r->px / 2 + 1;
+  return std::max(1, std::min(ph, e->cpt > 0 ? e->cpt : default_cols(r)));
 }
-size_t cx_bytes(int prec) { return 2 * relem(prec); }
-// shared memory: twiddle table of the transform length + two padded ping-pong buffers
-size_t row_smem(const mrm_gpu* r, int prec) {
-  return ((size_t)r->px + 2ull * rows_per_task(r) * 3 * fft_stride(r->px / 2)) * cx_bytes(prec);
-}
-size_t col_smem(const mrm_gpu* r, int prec) {
-  size_t b = ((size_t)r->py + 2ull * cols_per_task(r) * r->nl * 3 * fft_stride(r->py)) * cx_bytes(prec);
-  if (prec == MRM_FP32) {  // packed tensor slice (kernels.cuh: tens_slice_fits)
-    const int reals = cols_per_task(r) * r->nl * r->nl * 9 * (r->py / 2 + 1);
-    if (tens_slice_fits<float>(reals)) b += (size_t)reals * sizeof(float);
-  }
-  return b;
-}
-// row-kernel shape: grains per thread x block size
-int row_config(int max_grains) {
-  if (max_grains <= 256) return 0;   // GPT 1, 256 threads
-  if (max_grains <= 512) return 1;   // GPT 2, 256 threads
-  return 2;                          // GPT 2, 512 threads (<= 1024 grains)
-}
+int rows_per_task(const mrm_gpu* r, int rpb) { return std::max(1, std::min(rpb, r->g.ny)); }
+
 size_t tensor_bytes(const mrm_gpu* r) {
   const size_t ph = r->px / 2 + 1, npair = (size_t)r->nl * r->nl;
   if (r->g.precision == MRM_FP64) return ph * npair * 9 * r->py * 2 * sizeof(double);
-  return ph * npair * 9 * (r->py / 2 + 1) * sizeof(float);
+  return ph * npair * 9 * tens_row_stride(r->py) * sizeof(float);
 }
 
+// row-kernel launch slots: kInit, kPred, kCorr, kCorr with reductions, kEval
+constexpr int kSlots = 5;
+constexpr int kSlotStage[kSlots] = {kInit, kPred, kCorr, kCorr, kEval};
+int slot_of(int stage, bool stats) {
+  return stage == kInit ? 0 : stage == kPred ? 1 : stage == kCorr ? (stats ? 3 : 2) : 4;
+}
+// static shared memory of a row stage (mbarriers, reduction scratch) with margin
+size_t row_static_bytes(int slot) { return (slot == 3 ? 32 * kNPart * sizeof(double) : sizeof(double)) + 64; }
+constexpr size_t kSmemPerSM = 228 * 1024;
+constexpr size_t kSmemReserved = 1024;  // per block
+
+// staging bytes a run needs at a stage (largest over its layers)
+template <typename R>
+int run_stage_bytes(const mrm_gpu* r, int stage, int rows) {
+  int need = 0;
+  for (int l = 0; l < r->nl; ++l) {
+    const LayerBufs& b = r->L[l];
+    const bool ucol = b.ucol && l > 0, lcol = b.lcol && l + 1 < r->nl;
+    const RowStage p = row_stage_plan<R>(stage, r->g.nx, rows, b.xst != nullptr, ucol, lcol, b.thermal != 0);
+    need = std::max(need, p.bytes);
+  }
+  return need;
+}
+
+template <typename R>
+size_t col_smem_of(const mrm_gpu* r, int nc) {
+  size_t b = col_fft_smem<R>(r->lgpy, nc * r->nl * 3);
+  if (sizeof(R) == sizeof(float)) {
+    const int reals = nc * r->nl * r->nl * 9 * tens_row_stride(r->py);
+    if (tens_slice_fits<R>(reals)) b += (size_t)reals * sizeof(R);
+  }
+  return b;
+}
+
+// The geometry must run with the most economical shapes (one row per row
+// task, one column per column task, no staging).
 int validate_geom(const mrm_geom* g, std::string* errp) {
   if (!g) return set_err(errp, MRM_ERR_ARG, "geometry is NULL");
   if (g->nx < 2 || g->ny < 2) return set_err(errp, MRM_ERR_ARG, "nx, ny must be >= 2");
@@ -261,8 +320,6 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
   if (!(g->dx > 0 && g->dy > 0)) return set_err(errp, MRM_ERR_ARG, "dx, dy must be > 0");
   for (int l = 0; l < g->n_lay; ++l)
     if (!(g->dz[l] > 0)) return set_err(errp, MRM_ERR_ARG, "dz[%d] must be > 0", l);
-  if (g->nx > 1024)
-    return set_err(errp, MRM_ERR_UNSUPPORTED, "rows of more than 1024 grains are not supported (nx=%d)", g->nx);
   if (g->boundary == MRM_PERIODIC && (!is_pow2(g->nx) || !is_pow2(g->ny)))
     return set_err(errp, MRM_ERR_UNSUPPORTED,
                    "periodic demag needs power-of-two nx, ny on this path (got %d x %d)", g->nx, g->ny);
@@ -274,8 +331,13 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
   tmp.g = *g;
   tmp.px = px;
   tmp.py = py;
+  tmp.lgpx = ilog2(px);
+  tmp.lgpy = ilog2(py);
   tmp.nl = g->n_lay;
-  if (row_smem(&tmp, g->precision) > kMaxSmem || col_smem(&tmp, g->precision) > kMaxSmem)
+  const bool f64 = g->precision == MRM_FP64;
+  const size_t rs = f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1);
+  const size_t cs = f64 ? col_smem_of<double>(&tmp, 1) : col_smem_of<float>(&tmp, 1);
+  if (rs + row_static_bytes(3) > kMaxSmem || cs + 64 > kMaxSmem)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d x %d layers exceeds shared memory", px,
                    py, g->n_lay);
   return MRM_OK;
@@ -304,6 +366,11 @@ RunDev<R> make_desc(const mrm_gpu* r) {
   d.active = r->active ? 1 : 0;
   d.row_task0 = r->row_task0;
   d.nrow_tasks = r->nrow_tasks;
+  d.phs = spec_row_stride(r->px);
+  d.nys = spec_col_stride(r->g.ny);
+  d.pyhs = tens_row_stride(r->py);
+  d.tw_row = row_tw_off(r->lgpx);
+  d.tw_col = col_tw_off(r->lgpy);
   d.spech = static_cast<Cx<R>*>(r->spech);
   d.specx = static_cast<Cx<R>*>(r->specx);
   d.tens = static_cast<const R*>(r->tens);
@@ -379,33 +446,93 @@ int push_descs(Engine* e) {
     }
   }
   if (n) CK(cudaMemcpyAsync(e->d_runs, host.data(), ds * n, cudaMemcpyHostToDevice, e->st));
+  CK(cudaStreamSynchronize(e->st));  // the host buffer is released on return
   e->desc_dirty = false;
   return MRM_OK;
 }
 
+// Shared memory of every row stage and of the column kernel for the engine's
+// current shapes: FFT part for the largest grid, plus grain staging up to what
+// keeps the shape's intended blocks per SM resident.
+template <typename R>
+int plan_smem(Engine* e) {
+  std::string* errp = &e->err;
+  const RowVariant rv = row_variant<R>(e->rowv);
+  size_t fft = 16;
+  int need[kSlots] = {0, 0, 0, 0, 0};
+  size_t scol = 16;
+  for (auto* r : e->runs) {
+    if (r->lgpx > rv.lgmax)
+      return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d does not cover %d-column FFT grids", e->rowv, r->px);
+    const int rows = rows_per_task(r, rv.rpb);
+    fft = std::max(fft, (size_t)row_fft_smem<R>(r->lgpx, rv.rpb));
+    for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
+    if (r->demag && r->tensor_ready) scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r)));
+  }
+  for (int q = 0; q < kSlots; ++q) {
+    const long long per_block = (long long)(kSmemPerSM / rv.minb) - (long long)kSmemReserved -
+                                (long long)row_static_bytes(q) - (long long)fft;
+    const long long hard = (long long)kMaxSmem - (long long)row_static_bytes(q) - (long long)fft;
+    if (hard < 0) return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d exceeds shared memory", e->rowv);
+    const long long cap = std::min<long long>(need[q], std::max(0LL, std::min(per_block, hard)));
+    e->stage_cap[q] = (int)(cap & ~15LL);
+    e->smem_row[q] = fft + (size_t)e->stage_cap[q];
+  }
+  if (scol + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
+  e->smem_col = scol;
+  CK(row_allow_smem<R>(e->rowv, e->smem_row));
+  // the reductions launch: row shape 0, one row per task
+  {
+    const RowVariant r0 = row_variant<R>(0);
+    size_t f0 = 16;
+    int n0 = 0;
+    for (auto* r : e->runs) {
+      f0 = std::max(f0, (size_t)row_fft_smem<R>(r->lgpx, 1));
+      n0 = std::max(n0, run_stage_bytes<R>(r, kCorr, 1));
+    }
+    const long long per_block = (long long)(kSmemPerSM / r0.minb) - (long long)kSmemReserved -
+                                (long long)row_static_bytes(3) - (long long)f0;
+    const long long hard = (long long)kMaxSmem - (long long)row_static_bytes(3) - (long long)f0;
+    if (hard < 0) return set_err(errp, MRM_ERR_UNSUPPORTED, "grid exceeds shared memory");
+    e->cap_stats = (int)(std::min<long long>(n0, std::max(0LL, std::min(per_block, hard))) & ~15LL);
+    e->smem_stats = f0 + (size_t)e->cap_stats;
+    size_t lim[kSlots] = {0, 0, 0, e->smem_stats, 0};
+    CK(row_allow_smem<R>(0, lim));
+  }
+  CK(col_allow_smem<R>(e->colv, e->smem_col));
+  return MRM_OK;
+}
+
+template <typename R>
 int build_tables(Engine* e) {
   std::string* errp = &e->err;
-  std::vector<Task> rt, ct;
-  size_t srow = 0, scol = 0;
-  int maxg = 1;
+  const RowVariant rv = row_variant<R>(e->rowv);
+  std::vector<Task> rt, ct, stt;
   for (size_t i = 0; i < e->runs.size(); ++i) {
     mrm_gpu* r = e->runs[i];
     r->slot = (int)i;
-    r->row_task0 = (int)rt.size();
-    const int rpt = rows_per_task(r);
+    const int rpt = rows_per_task(r, rv.rpb);
     for (int l = 0; l < r->nl; ++l)
       for (int j = 0; j < r->g.ny; j += rpt) rt.push_back(make_int4((int)i, l, j, std::min(rpt, r->g.ny - j)));
-    r->nrow_tasks = (int)rt.size() - r->row_task0;
-    maxg = std::max(maxg, rpt * r->g.nx);
-    srow = std::max(srow, row_smem(r, e->prec));
+    // one-row tasks of the reductions launch; the run's partial records
+    r->row_task0 = (int)stt.size();
+    for (int l = 0; l < r->nl; ++l)
+      for (int j = 0; j < r->g.ny; ++j) stt.push_back(make_int4((int)i, l, j, 1));
+    r->nrow_tasks = (int)stt.size() - r->row_task0;
     if (r->demag && r->tensor_ready) {
-      const int cpt = cols_per_task(r), ph = r->px / 2 + 1;
+      const int cpt = cols_per_task(e, r), ph = r->px / 2 + 1;
       for (int k = 0; k < ph; k += cpt) ct.push_back(make_int4((int)i, k, std::min(cpt, ph - k), 0));
-      scol = std::max(scol, col_smem(r, e->prec));
     }
   }
   e->nrt = (int)rt.size();
   e->nct = (int)ct.size();
+  e->nst = (int)stt.size();
+  if (e->nst > e->st_cap) {
+    dfree(e->d_stasks);
+    e->st_cap = std::max(e->nst, 2 * e->st_cap);
+    int rc = dmalloc(errp, (void**)&e->d_stasks, sizeof(Task) * e->st_cap);
+    if (rc) return rc;
+  }
   if (e->nrt > e->rt_cap) {
     dfree(e->d_rtasks);
     e->rt_cap = std::max(e->nrt, 2 * e->rt_cap);
@@ -418,9 +545,9 @@ int build_tables(Engine* e) {
     int rc = dmalloc(errp, (void**)&e->d_ctasks, sizeof(Task) * e->ct_cap);
     if (rc) return rc;
   }
-  if (e->nrt > e->part_cap) {
+  if (e->nst > e->part_cap) {
     dfree(e->d_part);
-    e->part_cap = std::max(e->nrt, 2 * e->part_cap);
+    e->part_cap = std::max(e->nst, 2 * e->part_cap);
     int rc = dmalloc(errp, (void**)&e->d_part, sizeof(double) * kNPart * e->part_cap);
     if (rc) return rc;
   }
@@ -437,143 +564,237 @@ int build_tables(Engine* e) {
   }
   if (e->nrt) CK(cudaMemcpyAsync(e->d_rtasks, rt.data(), sizeof(Task) * e->nrt, cudaMemcpyHostToDevice, e->st));
   if (e->nct) CK(cudaMemcpyAsync(e->d_ctasks, ct.data(), sizeof(Task) * e->nct, cudaMemcpyHostToDevice, e->st));
-  e->smem_row = srow;
-  e->smem_col = scol;
-  e->rowcfg = row_config(maxg);
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->dev);
-  // enough row blocks to fill four per SM: the throughput variant wins
-  e->pref = !(e->prec == MRM_FP32 && e->rowcfg <= 1 && e->nrt >= 4 * nsm);
+  if (e->nst) CK(cudaMemcpyAsync(e->d_stasks, stt.data(), sizeof(Task) * e->nst, cudaMemcpyHostToDevice, e->st));
+  CK(cudaStreamSynchronize(e->st));  // the host vectors are released on return
+  int rc = plan_smem<R>(e);
+  if (rc) return rc;
   clear_graphs(e);
   e->tables_dirty = false;
   e->desc_dirty = true;
   return MRM_OK;
 }
 
-// The dynamic shared-memory limit is a per-function attribute shared by every
-// engine in the process, so it only ever grows.
-template <typename K>
-int raise_smem(K* kern, size_t bytes, std::string* errp) {
-  static std::map<const void*, size_t> set;
-  size_t& cur = set[(const void*)kern];
-  if (bytes <= cur) return MRM_OK;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  cur = bytes;
+template <typename R>
+cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
+  if (!e->nrt) return cudaSuccess;
+  if (stats) {
+    RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats,
+                e->cap_stats, pdl};
+    return launch_row<R>(0, stage, true, a, istep, flags);
+  }
+  const int q = slot_of(stage, false);
+  RowLaunch a{e->st, e->d_runs, e->d_rtasks, e->d_tw, e->d_part, e->d_err, e->nrt, e->smem_row[q],
+              e->stage_cap[q], pdl};
+  return launch_row<R>(e->rowv, stage, false, a, istep, flags);
+}
+
+template <typename R>
+cudaError_t launch_col_e(Engine* e, int istep, int flags, bool pdl = true) {
+  if (!e->nct) return cudaSuccess;
+  ColLaunch a{e->st, e->d_runs, e->d_ctasks, e->d_tw, e->d_err, e->nct, e->smem_col, pdl};
+  return launch_col<R>(e->colv, a, istep, flags);
+}
+
+template <typename R>
+cudaError_t enqueue_steps(Engine* e, int k, bool stats) {
+  cudaError_t ce = cudaSuccess;
+  auto acc = [&](cudaError_t x) { if (ce == cudaSuccess) ce = x; };
+  for (int i = 0; i < k; ++i) {
+    const bool last = stats && i == k - 1;
+    acc(launch_row_e<R>(e, kPred, false, i, 0));
+    acc(launch_col_e<R>(e, i, 0));
+    acc(launch_row_e<R>(e, kCorr, last, i, last ? (kFlagStats | kFlagStoreField) : 0));
+    acc(launch_col_e<R>(e, i, 0));
+  }
+  const int nr = (int)e->runs.size();
+  acc(launch_kernel(advance_kernel<R>, dim3((nr + 127) / 128), dim3(128), 0, e->st, true,
+                    static_cast<RunDev<R>*>(e->d_runs), nr, k));
+  if (stats)
+    acc(launch_kernel(finalize_stats_kernel<R>, dim3(nr), dim3(256), 0, e->st, true,
+                      static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_stasks,
+                      (const double*)e->d_part, e->d_stats, nr));
+  return ce;
+}
+
+// spectrum = H^(m) for active runs whose state or tensor changed
+template <typename R>
+int establish_spectra(Engine* e) {
+  std::string* errp = &e->err;
+  bool need = false;
+  for (auto* r : e->runs)
+    if (r->active && !r->spec_valid) need = true;
+  if (!need) return MRM_OK;
+  CK(launch_row_e<R>(e, kInit, false, 0, kFlagForce));
+  CK(launch_col_e<R>(e, 0, kFlagForce));
+  CK(cudaGetLastError());
+  for (auto* r : e->runs)
+    if (r->active) r->spec_valid = true;
   return MRM_OK;
 }
 
-// Launch with programmatic stream serialization: the kernel may start while its
-// predecessor drains; it runs its independent prologue and then waits
-// (griddepcontrol.wait) for the predecessor's results.
-template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
-
-template <typename R, int GPT, int BLK, bool PREF>
-int set_row_attrs(size_t rs, std::string* errp) {
-  int rc = 0;
-  rc |= raise_smem(row_kernel<R, kInit, false, GPT, BLK, PREF>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kPred, false, GPT, BLK, PREF>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, false, GPT, BLK, PREF>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kCorr, true, GPT, BLK, PREF>, rs, errp);
-  rc |= raise_smem(row_kernel<R, kEval, false, GPT, BLK, PREF>, rs, errp);
-  return rc;
-}
-
+// ---------------- shapes: default heuristic and autotuner ----------------
 template <typename R>
-int set_smem_attrs(Engine* e) {
+void default_shapes(Engine* e) {
+  int maxnx = 1, maxlg = 1;
+  for (auto* r : e->runs) {
+    maxnx = std::max(maxnx, r->g.nx);
+    maxlg = std::max(maxlg, r->lgpx);
+  }
+  // rows per block so that a block holds about 256 grains
+  const int want = std::max(1, 256 / maxnx);
+  int best = 0;
+  for (int v = 0; v < row_variant_count<R>(); ++v) {
+    const RowVariant rv = row_variant<R>(v);
+    if (rv.lgmax < maxlg || rv.block != 256) continue;
+    const RowVariant bv = row_variant<R>(best);
+    if (std::abs(rv.rpb - want) < std::abs(bv.rpb - want)) best = v;
+  }
+  e->rowv = best;
+  e->colv = 0;
+  e->cpt = 0;
+}
+
+// signature of a batch for the tuner's cache: precision, largest grid, layers,
+// order of magnitude of the grain count
+std::string shape_key(const Engine* e) {
+  int lgx = 0, lgy = 0, nl = 0;
+  long long grains = 0;
+  for (auto* r : e->runs) {
+    if (!r->active) continue;
+    lgx = std::max(lgx, r->lgpx);
+    lgy = std::max(lgy, r->lgpy);
+    nl = std::max(nl, r->nl);
+    grains += (long long)r->g.nx * r->g.ny * r->nl;
+  }
+  char buf[96];
+  std::snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d", e->dev, e->prec, lgx, lgy, nl, grains > 0 ? ilog2((int)std::min<long long>(grains, 1LL << 30)) : 0);
+  return buf;
+}
+
+struct Shape {
+  int rowv, colv, cpt;
+};
+std::mutex g_tune_mu;
+std::map<std::string, Shape>& tune_cache() {
+  static std::map<std::string, Shape> c;
+  return c;
+}
+
+// Times each row shape (predictor + corrector launches) and each column
+// shape x columns per task on the batch itself and keeps the fastest.  The
+// kernels run on the real state, which is saved before and restored after
+// (m and the stored field per layer; the spectra are re-established).
+template <typename R>
+int autotune(Engine* e) {
   std::string* errp = &e->err;
-  const size_t rs = std::max<size_t>(e->smem_row, 16), cs = std::max<size_t>(e->smem_col, 16);
-  int rc = 0;
-  if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256, true>(rs, errp);
-  else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256, true>(rs, errp);
-  else rc |= set_row_attrs<R, 2, 512, true>(rs, errp);
-  if constexpr (sizeof(R) == sizeof(float)) {
-    if (e->rowcfg == 0) rc |= set_row_attrs<R, 1, 256, false>(rs, errp);
-    else if (e->rowcfg == 1) rc |= set_row_attrs<R, 2, 256, false>(rs, errp);
-  }
-  rc |= raise_smem(col_kernel<R, true, kBlock>, cs, errp);
-  rc |= raise_smem(col_kernel<R, false, kBlock>, cs, errp);
-  return rc ? MRM_ERR_CUDA : MRM_OK;
-}
-
-template <typename R, int GPT, int BLK, bool PREF>
-void launch_row_cfg(Engine* e, int stage, int istep, int flags) {
-  const RunDev<R>* runs = static_cast<const RunDev<R>*>(e->d_runs);
-  const Cx<R>* tw = static_cast<const Cx<R>*>(e->d_tw);
-  const dim3 g(e->nrt), b(BLK);
-  const size_t sm = e->smem_row;
-  switch (stage) {
-    case kInit:
-      launch_pdl(row_kernel<R, kInit, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
-      break;
-    case kPred:
-      launch_pdl(row_kernel<R, kPred, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
-      break;
-    case kCorr:
-      if (flags & kFlagStats)
-        launch_pdl(row_kernel<R, kCorr, true, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
-      else
-        launch_pdl(row_kernel<R, kCorr, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
-      break;
-    default:
-      launch_pdl(row_kernel<R, kEval, false, GPT, BLK, PREF>, g, b, sm, e->st, runs, e->d_rtasks, tw, istep, flags, e->d_part);
-      break;
-  }
-}
-
-template <typename R>
-void launch_row(Engine* e, int stage, int istep, int flags) {
-  if (!e->nrt) return;
-  if constexpr (sizeof(R) == sizeof(float)) {
-    if (!e->pref) {
-      if (e->rowcfg == 0) launch_row_cfg<R, 1, 256, false>(e, stage, istep, flags);
-      else launch_row_cfg<R, 2, 256, false>(e, stage, istep, flags);
-      return;
+  const std::string key = shape_key(e);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+      e->rowv = it->second.rowv;
+      e->colv = it->second.colv;
+      e->cpt = it->second.cpt;
+      return MRM_OK;
     }
   }
-  if (e->rowcfg == 0) launch_row_cfg<R, 1, 256, true>(e, stage, istep, flags);
-  else if (e->rowcfg == 1) launch_row_cfg<R, 2, 256, true>(e, stage, istep, flags);
-  else launch_row_cfg<R, 2, 512, true>(e, stage, istep, flags);
-}
-
-template <typename R>
-void launch_col(Engine* e, int istep, int flags) {
-  if (!e->nct) return;
-  constexpr bool packed = sizeof(R) == sizeof(float);
-  launch_pdl(col_kernel<R, packed, kBlock>, dim3(e->nct), dim3(kBlock), e->smem_col, e->st,
-             static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_ctasks,
-             static_cast<const Cx<R>*>(e->d_tw), istep, flags);
-}
-
-template <typename R>
-void enqueue_steps(Engine* e, int k, bool stats) {
-  for (int i = 0; i < k; ++i) {
-    const int last = (stats && i == k - 1) ? (kFlagStats | kFlagStoreField) : 0;
-    launch_row<R>(e, kPred, i, 0);
-    launch_col<R>(e, i, 0);
-    launch_row<R>(e, kCorr, i, last);
-    launch_col<R>(e, i, 0);
+  default_shapes<R>(e);
+  bool any = false;
+  for (auto* r : e->runs) any = any || r->active;
+  if (!any) return MRM_OK;
+  // save the state
+  std::vector<std::pair<void*, void*>> saved;  // (device buffer, copy)
+  for (auto* r : e->runs)
+    for (int l = 0; l < r->nl; ++l)
+      for (void* p : {r->L[l].m, r->L[l].hf}) {
+        void* c = nullptr;
+        const size_t bytes = (size_t)r->L[l].n * sizeof(V4<R>);
+        int rc = dmalloc(errp, &c, bytes);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(c, p, bytes, cudaMemcpyDeviceToDevice, e->st));
+        saved.push_back({p, c});
+      }
+  cudaEvent_t ev[2];
+  CK(cudaEventCreate(&ev[0]));
+  CK(cudaEventCreate(&ev[1]));
+  auto time_it = [&](auto&& body, int reps, float* ms) -> int {
+    for (int w = 0; w < 2; ++w) CK(body());
+    CK(cudaEventRecord(ev[0], e->st));
+    for (int s = 0; s < reps; ++s) CK(body());
+    CK(cudaEventRecord(ev[1], e->st));
+    CK(cudaEventSynchronize(ev[1]));
+    CK(cudaEventElapsedTime(ms, ev[0], ev[1]));
+    return MRM_OK;
+  };
+  auto prepare = [&]() -> int {
+    int rc = build_tables<R>(e);
+    if (rc) return rc;
+    rc = push_descs(e);
+    if (rc) return rc;
+    for (auto* r : e->runs) r->spec_valid = false;
+    return establish_spectra<R>(e);
+  };
+  const int reps = 4;
+  // column shapes with the default row shape
+  Shape best = {e->rowv, e->colv, e->cpt};
+  float best_ms = 1e30f;
+  for (int cv = 0; cv < col_variant_count<R>(); ++cv)
+    for (int nc : {1, 2, 4, 8}) {
+      e->colv = cv;
+      e->cpt = nc;
+      e->err.clear();
+      if (prepare() != MRM_OK) continue;
+      float ms = 0;
+      int rc = time_it([&]() { return launch_col_e<R>(e, 0, kFlagForce, false); }, reps, &ms);
+      if (rc) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best.colv = cv;
+        best.cpt = nc;
+      }
+    }
+  e->colv = best.colv;
+  e->cpt = best.cpt;
+  // row shapes with the chosen column shape
+  best_ms = 1e30f;
+  for (int v = 0; v < row_variant_count<R>(); ++v) {
+    e->rowv = v;
+    e->err.clear();
+    if (prepare() != MRM_OK) continue;
+    float ms = 0;
+    int rc = time_it(
+        [&]() {
+          cudaError_t a = launch_row_e<R>(e, kPred, false, 0, kFlagForce, false);
+          cudaError_t b = launch_col_e<R>(e, 0, kFlagForce, false);
+          cudaError_t c = launch_row_e<R>(e, kCorr, false, 0, kFlagForce, false);
+          cudaError_t d = launch_col_e<R>(e, 0, kFlagForce, false);
+          return a != cudaSuccess ? a : b != cudaSuccess ? b : c != cudaSuccess ? c : d;
+        },
+        reps, &ms);
+    if (rc) return rc;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best.rowv = v;
+    }
   }
-  const int nr = (int)e->runs.size();
-  launch_pdl(advance_kernel<R>, dim3((nr + 127) / 128), dim3(128), 0, e->st,
-             static_cast<RunDev<R>*>(e->d_runs), nr, k);
-  if (stats)
-    launch_pdl(finalize_stats_kernel<R>, dim3(nr), dim3(256), 0, e->st,
-               static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_rtasks,
-               (const double*)e->d_part, e->d_stats, nr);
+  e->rowv = best.rowv;
+  e->err.clear();
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  // restore the state
+  for (auto& s : saved) {
+    for (auto* r : e->runs)
+      for (int l = 0; l < r->nl; ++l)
+        if (s.first == r->L[l].m || s.first == r->L[l].hf)
+          CK(cudaMemcpyAsync(s.first, s.second, (size_t)r->L[l].n * sizeof(V4<R>), cudaMemcpyDeviceToDevice, e->st));
+  }
+  CK(cudaStreamSynchronize(e->st));
+  for (auto& s : saved) dfree(s.second);
+  for (auto* r : e->runs) r->spec_valid = false;
+  e->tables_dirty = true;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_cache()[key] = best;
+  return MRM_OK;
 }
 
 template <typename R>
@@ -581,27 +802,29 @@ int ensure_ready(Engine* e) {
   std::string* errp = &e->err;
   CK(cudaSetDevice(e->dev));
   if (e->tables_dirty) {
-    int rc = build_tables(e);
-    if (rc) return rc;
-    rc = set_smem_attrs<R>(e);
+    if (e->shape_forced) {
+      e->rowv = e->force_rowv;
+      e->colv = e->force_colv;
+      e->cpt = e->force_cpt;
+    } else if (e->autotune) {
+      // tuning needs every active run uploaded with its tensor
+      bool ready = true;
+      for (auto* r : e->runs)
+        if (r->active && r->demag && !r->tensor_ready) ready = false;
+      int rc = ready ? autotune<R>(e) : MRM_OK;
+      if (!ready) default_shapes<R>(e);
+      if (rc) return rc;
+    } else {
+      default_shapes<R>(e);
+    }
+    int rc = build_tables<R>(e);
     if (rc) return rc;
   }
   if (e->desc_dirty) {
     int rc = push_descs(e);
     if (rc) return rc;
   }
-  // establish spec = H^(m) for runs whose state or tensor changed
-  bool need = false;
-  for (auto* r : e->runs)
-    if (r->active && !r->spec_valid) need = true;
-  if (need) {
-    launch_row<R>(e, kInit, 0, kFlagForce);
-    launch_col<R>(e, 0, kFlagForce);
-    CK(cudaGetLastError());
-    for (auto* r : e->runs)
-      if (r->active) r->spec_valid = true;
-  }
-  return MRM_OK;
+  return establish_spectra<R>(e);
 }
 
 template <typename R>
@@ -618,8 +841,9 @@ int run_steps(Engine* e, int nsteps) {
     if (it == e->graphs.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-      enqueue_steps<R>(e, k, stats);
+      cudaError_t le = enqueue_steps<R>(e, k, stats);
       cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+      if (le != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "launch in capture: %s", cudaGetErrorString(le));
       if (ce != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
       cudaGraphExec_t ge;
       ce = cudaGraphInstantiate(&ge, g, 0);
@@ -650,21 +874,37 @@ int engine_eval(Engine* e) {
   std::string* errp = &e->err;
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
-  launch_row<R>(e, kEval, 0, kFlagForce | kFlagStoreField);
+  CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField));
   CK(cudaGetLastError());
   return MRM_OK;
+}
+
+// device-side error flag (bulk-copy waits that ran out, shapes not compiled):
+// read and cleared at the host's synchronisation points
+int check_device_error(Engine* e) {
+  std::string* errp = &e->err;
+  int v[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(v, e->d_err, sizeof(v), cudaMemcpyDeviceToHost, e->st));
+  CK(cudaStreamSynchronize(e->st));
+  if (v[0] == 0) return MRM_OK;
+  CK(cudaMemsetAsync(e->d_err, 0, sizeof(v), e->st));
+  const long long val = (long long)(unsigned)v[2] | ((long long)v[3] << 32);
+  return set_err(errp, MRM_ERR_DEVICE, "device error flag 0x%x (%s; check %d, value %lld)", v[0],
+                 (v[0] & kErrBarrierTimeout) ? "a bulk-copy wait ran out"
+                 : (v[0] & kErrShape)        ? "kernel shape mismatch"
+                                             : "self-check failed",
+                 v[1], val);
 }
 
 // ---------------- run buffers ----------------
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
-  const int ph = r->px / 2 + 1, pyh = r->py / 2 + 1;
-  int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
+  const int ph = r->px / 2 + 1;
+  int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * 2 * re);
   if (rc) return rc;
-  rc = dmalloc(errp, &r->specx, (size_t)r->nl * 3 * r->g.ny * ph * 2 * re);
+  rc = dmalloc(errp, &r->specx, (size_t)r->nl * 3 * ph * spec_col_stride(r->g.ny) * 2 * re);
   if (rc) return rc;
-  (void)pyh;
   rc = dmalloc(errp, &r->tens, tensor_bytes(r));
   if (rc) return rc;
   const size_t n = (size_t)r->g.nx * r->g.ny;
@@ -701,9 +941,9 @@ int64_t footprint(const mrm_geom& g) {
   fft_grid(g, &px, &py);
   const size_t re = g.precision == MRM_FP64 ? 8 : 4;
   const int64_t n = (int64_t)g.nx * g.ny, nl = g.n_lay;
-  const int64_t ph = px / 2 + 1, pyh = py / 2 + 1;
-  int64_t b = 2 * nl * 3 * g.ny * ph * 2 * re;
-  b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * pyh * 4;
+  const int64_t ph = px / 2 + 1;
+  int64_t b = nl * 3 * g.ny * spec_row_stride(px) * 2 * re + nl * 3 * ph * spec_col_stride(g.ny) * 2 * re;
+  b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * tens_row_stride(py) * 4;
   b += nl * n * (8 * 4 * re + 4 * 8);
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
   if (nl > 1) b += 2 * nl * ((n + 1) * 4 + n * (4 + re));
@@ -940,8 +1180,9 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   const Cx<double>* tw64 = static_cast<const Cx<double>*>(d_tw64);
   const int M = r->px / 2;
   // two shared buffers of one padded-stride sequence each (fft.cuh)
-  size_t s1 = 2 * (size_t)fft_stride(M) * sizeof(Cx<double>), s2 = 2 * (size_t)fft_stride(r->py) * sizeof(Cx<double>);
-  if (raise_smem(r2c_rows_f64, s1, errp) || raise_smem(c2c_cols_f64, s2, errp)) return MRM_ERR_CUDA;
+  size_t s1 = 2 * (size_t)pad_stride(M) * sizeof(Cx<double>), s2 = 2 * (size_t)pad_stride(r->py) * sizeof(Cx<double>);
+  CK(allow_smem((const void*)r2c_rows_f64, s1));
+  CK(allow_smem((const void*)c2c_cols_f64, s2));
   r2c_rows_f64<<<planes * r->py, 256, s1, e->st>>>(d_n2d, static_cast<Cx<double>*>(d_spec), r->lgpx, r->py, tw64);
   CK(cudaGetLastError());
   c2c_cols_f64<<<planes * ph, 256, s2, e->st>>>(static_cast<Cx<double>*>(d_spec), r->lgpy, ph, tw64);
@@ -956,7 +1197,8 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   } else {
     const long long total = (long long)ph * npair * 9 * pyh;
     pack_tensor_kernel<float><<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
-        static_cast<const Cx<double>*>(d_spec), static_cast<float*>(r->tens), npair, r->py, ph, d_mx, d_mx + 1);
+        static_cast<const Cx<double>*>(d_spec), static_cast<float*>(r->tens), npair, r->py, ph,
+        tens_row_stride(r->py), d_mx, d_mx + 1);
   }
   CK(cudaGetLastError());
   unsigned long long hm[2];
@@ -1405,6 +1647,10 @@ int mrm_gpu_read_stats(mrm_gpu* h, mrm_gpu_stats* out) {
   CK(cudaSetDevice(e->dev));
   CK(cudaMemcpyAsync(e->h_stats + h->slot, e->d_stats + h->slot, sizeof(StatsDev), cudaMemcpyDeviceToHost, e->st));
   CK(cudaStreamSynchronize(e->st));
+  if (check_device_error(e)) {
+    h->err = e->err;
+    return MRM_ERR_DEVICE;
+  }
   static_assert(sizeof(StatsDev) == sizeof(mrm_gpu_stats), "stats layout");
   std::memcpy(out, e->h_stats + h->slot, sizeof(StatsDev));
   return MRM_OK;
@@ -1420,6 +1666,53 @@ int mrm_gpu_step(mrm_gpu* h, int nsteps, double dt, int llg_type, mrm_gpu_stats*
     return mrm_gpu_read_stats(h, out);
   }
   CK(cudaStreamSynchronize(h->eng->st));
+  if (check_device_error(h->eng)) {
+    h->err = h->eng->err;
+    return MRM_ERR_DEVICE;
+  }
+  return MRM_OK;
+}
+
+int mrm_gpu_set_shape(mrm_gpu* h, int row_shape, int col_shape, int cols_per_task) {
+  if (!h) return MRM_ERR_ARG;
+  Engine* e = h->eng;
+  const bool f64 = e->prec == MRM_FP64;
+  const int nrv = f64 ? row_variant_count<double>() : row_variant_count<float>();
+  const int ncv = f64 ? col_variant_count<double>() : col_variant_count<float>();
+  if (row_shape < 0 || col_shape < 0) {
+    e->shape_forced = false;
+  } else {
+    if (row_shape >= nrv || col_shape >= ncv)
+      return set_err(&h->err, MRM_ERR_ARG, "shape (%d, %d) outside %d row / %d column shapes", row_shape,
+                     col_shape, nrv, ncv);
+    e->shape_forced = true;
+    e->force_rowv = row_shape;
+    e->force_colv = col_shape;
+    e->force_cpt = std::max(0, cols_per_task);
+  }
+  e->tables_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_gpu_set_autotune(mrm_gpu* h, int on) {
+  if (!h) return MRM_ERR_ARG;
+  h->eng->autotune = on != 0;
+  h->eng->tables_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_gpu_check_device(mrm_gpu* h) {
+  if (!h) return MRM_ERR_ARG;
+  int rc = check_device_error(h->eng);
+  if (rc) h->err = h->eng->err;
+  return rc;
+}
+
+int mrm_gpu_get_shape(const mrm_gpu* h, int* out3) {
+  if (!h || !out3) return MRM_ERR_ARG;
+  out3[0] = h->eng->rowv;
+  out3[1] = h->eng->colv;
+  out3[2] = h->eng->cpt;
   return MRM_OK;
 }
 
@@ -1441,13 +1734,13 @@ static int profile_t(Engine* e, int reps, double* ms_out) {
   const int nr = (int)e->runs.size();
   for (int s = 0; s < reps; ++s) {
     CK(cudaEventRecord(ev[5 * s + 0], e->st));
-    launch_row<R>(e, kPred, 0, 0);
+    CK(launch_row_e<R>(e, kPred, false, 0, 0));
     CK(cudaEventRecord(ev[5 * s + 1], e->st));
-    launch_col<R>(e, 0, 0);
+    CK(launch_col_e<R>(e, 0, 0));
     CK(cudaEventRecord(ev[5 * s + 2], e->st));
-    launch_row<R>(e, kCorr, 0, 0);
+    CK(launch_row_e<R>(e, kCorr, false, 0, 0));
     CK(cudaEventRecord(ev[5 * s + 3], e->st));
-    launch_col<R>(e, 0, 0);
+    CK(launch_col_e<R>(e, 0, 0));
     CK(cudaEventRecord(ev[5 * s + 4], e->st));
     advance_kernel<R><<<(nr + 127) / 128, 128, 0, e->st>>>(static_cast<RunDev<R>*>(e->d_runs), nr, 1);
   }
@@ -1598,6 +1891,7 @@ int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats
   CK(cudaSetDevice(e->dev));
   CK(cudaMemcpyAsync(e->h_stats, e->d_stats, sizeof(StatsDev) * nr, cudaMemcpyDeviceToHost, e->st));
   CK(cudaStreamSynchronize(e->st));
+  if (check_device_error(e)) return MRM_ERR_DEVICE;
   for (int i = 0; i < nruns; ++i) {
     if (!runs[i] || runs[i]->eng != e || runs[i]->slot < 0 || runs[i]->slot >= nr)
       return set_err(errp, MRM_ERR_ARG, "run %d is not in this batch", i);
@@ -1612,15 +1906,10 @@ template <typename R>
 static int occ_t(Engine* e, int* out2) {
   std::string* errp = &e->err;
   int a = 0, b = 0;
-  if (e->rowcfg == 0 && !e->pref && sizeof(R) == sizeof(float))
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256, false>, 256, e->smem_row));
-  else if (e->rowcfg == 0)
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 1, 256, true>, 256, e->smem_row));
-  else if (e->rowcfg == 1)
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 256, true>, 256, e->smem_row));
-  else
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, row_kernel<R, kPred, false, 2, 512, true>, 512, e->smem_row));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, col_kernel<R, sizeof(R) == 4, kBlock>, kBlock, e->smem_col));
+  if (!e->tables_dirty) {
+    CK(row_occupancy<R>(e->rowv, kPred, e->smem_row[1], &a));
+    CK(col_occupancy<R>(e->colv, e->smem_col, &b));
+  }
   out2[0] = a;
   out2[1] = b;
   return MRM_OK;
@@ -1694,15 +1983,14 @@ NoAllocLayout noalloc_layout(const mrm_gpu* r, int nrt, int nct) {
   };
   const size_t n = (size_t)r->g.nx * r->g.ny, ph = r->px / 2 + 1;
   const size_t grains = (size_t)r->nl * n * sizeof(V4<float>);
-  const size_t spec = (size_t)r->nl * 3 * r->g.ny * ph * sizeof(Cx<float>);
   o.desc = take(sizeof(RunDev<float>));
   o.rtask = take(sizeof(Task) * nrt);
   o.ctask = take(sizeof(Task) * nct);
   o.m = take(grains);
   o.hd = take(grains);
   o.hf = take(grains);
-  o.specx = take(spec);
-  o.spech = take(spec);
+  o.specx = take((size_t)r->nl * 3 * ph * spec_col_stride(r->g.ny) * sizeof(Cx<float>));
+  o.spech = take((size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * sizeof(Cx<float>));
   o.total = off;
   return o;
 }
@@ -1737,29 +2025,11 @@ __global__ void noalloc_unpack_kernel(const V4<float>* __restrict__ hd, float* _
   out[3 * i + 2] = v.z;
 }
 
-// Loads a kernel (CUDA lazy loading would otherwise load it, and allocate its
-// code, at its first launch) and lets it use all opt-in shared memory.  The
-// raise_smem record is lifted to the same value so that no engine lowers it.
-template <typename K>
-int noalloc_prepare(K* kern, int optin, std::string* errp) {
-  cudaFuncAttributes fa;
-  CK(cudaFuncGetAttributes(&fa, kern));
-  const size_t dyn = (size_t)optin - fa.sharedSizeBytes;
-  int rc = raise_smem(kern, dyn, errp);
-  if (rc) return rc;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  return MRM_OK;
-}
-
-template <int GPT, int BLK>
-int noalloc_prepare_rows(int optin, std::string* errp) {
-  int rc = noalloc_prepare(row_kernel<float, kInit, false, GPT, BLK, true>, optin, errp);
-  if (!rc) rc = noalloc_prepare(row_kernel<float, kEval, false, GPT, BLK, true>, optin, errp);
-  return rc;
-}
-
-// Once per device, with that device current: the scratch address and the
-// kernels' attributes.  Runs inside the first call on the device.
+// Once per device, with that device current: the scratch address, and the
+// kernels of the call loaded (CUDA lazy loading would otherwise load them,
+// and allocate their code, at their first launch) with their shared-memory
+// limits raised to the device's maximum.  Runs inside the first call on the
+// device.
 int noalloc_setup(int dev, std::string* errp, unsigned char** base) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   NoAllocDev& s = g_noalloc_dev[dev];
@@ -1771,11 +2041,12 @@ int noalloc_setup(int dev, std::string* errp, unsigned char** base) {
   CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  int rc = noalloc_prepare_rows<1, 256>(optin, errp);
-  if (!rc) rc = noalloc_prepare_rows<2, 256>(optin, errp);
-  if (!rc) rc = noalloc_prepare_rows<2, 512>(optin, errp);
-  if (!rc) rc = noalloc_prepare(col_kernel<float, true, kBlock>, optin, errp);
-  if (rc) return rc;
+  CK(row_load<float>(0));
+  CK(col_load<float>(0));
+  size_t lim[kSlots];
+  for (int q = 0; q < kSlots; ++q) lim[q] = (size_t)optin - row_static_bytes(q);
+  CK(row_allow_smem<float>(0, lim));
+  CK(col_allow_smem<float>(0, (size_t)optin - 64));
   cudaFuncAttributes fa;
   CK(cudaFuncGetAttributes(&fa, noalloc_pack_kernel));
   CK(cudaFuncGetAttributes(&fa, noalloc_unpack_kernel));
@@ -1783,27 +2054,6 @@ int noalloc_setup(int dev, std::string* errp, unsigned char** base) {
   s.ready = true;
   *base = s.base;
   return MRM_OK;
-}
-
-// kInit follows the pack kernel with a plain launch: it reads the descriptor
-// and tasks before its dependency wait, so it must not overlap their writer.
-// kEval follows the column kernel with programmatic serialization, as in the
-// engine.
-template <int GPT, int BLK>
-void noalloc_rows(int stage, int nrt, size_t smem, cudaStream_t st, const RunDev<float>* runs,
-                  const Task* tasks, const Cx<float>* tw) {
-  if (stage == kInit)
-    row_kernel<float, kInit, false, GPT, BLK, true><<<nrt, BLK, smem, st>>>(runs, tasks, tw, 0, kFlagForce, nullptr);
-  else
-    launch_pdl(row_kernel<float, kEval, false, GPT, BLK, true>, dim3(nrt), dim3(BLK), smem, st, runs, tasks, tw, 0,
-               kFlagForce | kFlagStoreField, (double*)nullptr);
-}
-
-void noalloc_rows_cfg(int cfg, int stage, int nrt, size_t smem, cudaStream_t st, const RunDev<float>* runs,
-                      const Task* tasks, const Cx<float>* tw) {
-  if (cfg == 0) noalloc_rows<1, 256>(stage, nrt, smem, st, runs, tasks, tw);
-  else if (cfg == 1) noalloc_rows<2, 256>(stage, nrt, smem, st, runs, tasks, tw);
-  else noalloc_rows<2, 512>(stage, nrt, smem, st, runs, tasks, tw);
 }
 
 }  // namespace
@@ -1817,8 +2067,8 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   if (h->g.precision != MRM_FP32)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
   const int nl = h->nl, ny = h->g.ny, ph = h->px / 2 + 1;
-  const int rpt = rows_per_task(h), nrt = nl * ((ny + rpt - 1) / rpt);
-  const int cpt = cols_per_task(h), nct = (ph + cpt - 1) / cpt;
+  const int rpt = 1, nrt = nl * ny;  // one row per task (row shape 0)
+  const int cpt = std::max(1, std::min(ph, default_cols(h))), nct = (ph + cpt - 1) / cpt;
   const NoAllocLayout lay = noalloc_layout(h, nrt, nct);
   if (lay.total > kNoAllocBytes)
     return set_err(errp, MRM_ERR_UNSUPPORTED,
@@ -1855,17 +2105,27 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   RunDev<float>* desc = reinterpret_cast<RunDev<float>*>(base + lay.desc);
   Task* rt = reinterpret_cast<Task*>(base + lay.rtask);
   Task* ct = reinterpret_cast<Task*>(base + lay.ctask);
-  const Cx<float>* tw = static_cast<const Cx<float>*>(e->d_tw);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e->st;
   const long long work = std::max<long long>(ntot, std::max(nrt, nct));
-  const int cfg = row_config(rpt * h->g.nx);
+  // shared memory: FFT part plus grain staging where it fits
+  const size_t fft = (size_t)row_fft_smem<float>(h->lgpx, 1);
+  auto stage_cap = [&](int stage, int slot) {
+    const long long hard = (long long)kMaxSmem - (long long)row_static_bytes(slot) - (long long)fft;
+    return (int)(std::min<long long>(run_stage_bytes<float>(h, stage, rpt), std::max(0LL, hard)) & ~15LL);
+  };
+  const int cap_init = stage_cap(kInit, 0), cap_eval = stage_cap(kEval, 4);
 
   noalloc_pack_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(d, desc, rt, nrt, rpt, ct, nct, cpt, m, sm,
                                                                       ntot);
-  noalloc_rows_cfg(cfg, kInit, nrt, row_smem(h, MRM_FP32), st, desc, rt, tw);
-  launch_pdl(col_kernel<float, true, kBlock>, dim3(nct), dim3(kBlock), col_smem(h, MRM_FP32), st,
-             (const RunDev<float>*)desc, (const Task*)ct, tw, 0, (int)kFlagForce);
-  noalloc_rows_cfg(cfg, kEval, nrt, row_smem(h, MRM_FP32), st, desc, rt, tw);
+  // kInit reads the descriptor and tasks before its dependency wait: a plain
+  // launch, so it cannot overlap their writer; the rest chain with
+  // programmatic serialization as in the engine
+  CK(launch_row<float>(0, kInit, false, RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false},
+                       0, kFlagForce));
+  CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt), true}, 0,
+                       kFlagForce));
+  CK(launch_row<float>(0, kEval, false, RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_eval, cap_eval, true},
+                       0, kFlagForce | kFlagStoreField));
   noalloc_unpack_kernel<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(shd, hdemag, ntot);
   CK(cudaGetLastError());
   return MRM_OK;

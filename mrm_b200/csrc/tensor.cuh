@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256) r2c_rows_f64(const double* __restrict__ i
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lgM = lgpx - 1, M = 1 << lgM, ph = M + 1, px = 2 * M;
   const long long row = blockIdx.x;  // p*py + j
-  const int cs = fft_stride(M);
+  const int cs = pad_stride(M);
   Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
   Cx<double>* B = A + cs;
   const double* src = in + row * px;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(256) c2c_cols_f64(Cx<double>* __restrict__ dat
   const int py = 1 << lgpy;
   const long long p = blockIdx.x / ph;
   const int k = blockIdx.x - (int)(p * ph);
-  const int cs = fft_stride(py);
+  const int cs = pad_stride(py);
   Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
   Cx<double>* B = A + cs;
   Cx<double>* base = data + p * (long long)py * ph + k;
@@ -221,11 +221,12 @@ __device__ __forceinline__ void parity_parts(const Cx<double>* S, int c, int kyh
   *disc = d;
 }
 
-// spectrum [pair][9][py][ph] (FP64) -> tens[k][pair][c][kyh] (R): one real per
-// component and 0 <= ky <= py/2 (FP32 runs); tracks the dropped residue.
+// spectrum [pair][9][py][ph] (FP64) -> tens[k][pair][c][kyh] (R, rows of pyhs
+// reals): one real per component and 0 <= ky <= py/2 (FP32 runs); tracks the
+// dropped residue.
 template <typename R>
 __global__ void pack_tensor_kernel(const Cx<double>* __restrict__ spec, R* __restrict__ tens,
-                                   int npair, int py, int ph, unsigned long long* resid,
+                                   int npair, int py, int ph, int pyhs, unsigned long long* resid,
                                    unsigned long long* kept) {
   const int pyh = py / 2 + 1;
   const long long total = (long long)ph * npair * 9 * pyh;
@@ -239,7 +240,7 @@ __global__ void pack_tensor_kernel(const Cx<double>* __restrict__ spec, R* __res
     const int pair = (int)(r % npair);
     const int k = (int)(r / npair);
     parity_parts(spec + ((long long)pair * 9 + c) * py * ph, c, kyh, k, py, ph, &keep, &disc);
-    tens[gid] = (R)keep;
+    tens[(gid / pyh) * pyhs + kyh] = (R)keep;
   }
   block_max2(disc, fabs(keep), resid, kept);
 }

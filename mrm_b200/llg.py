@@ -138,6 +138,18 @@ class _RunMixin:
         self._check(_lib.load().mrm_gpu_get_time(self.h, C.byref(t), C.byref(s)))
         return t.value, s.value
 
+    def set_shape(self, row_shape: int, col_shape: int, cols_per_task: int = 0):
+        """Forces compiled kernel shapes (negative: automatic)."""
+        self._check(_lib.load().mrm_gpu_set_shape(self.h, int(row_shape), int(col_shape), int(cols_per_task)))
+
+    def set_autotune(self, on: bool):
+        self._check(_lib.load().mrm_gpu_set_autotune(self.h, 1 if on else 0))
+
+    def get_shape(self):
+        out = (C.c_int * 3)()
+        self._check(_lib.load().mrm_gpu_get_shape(self.h, out))
+        return int(out[0]), int(out[1]), int(out[2])
+
     def eval_field(self, t: float, layer: int = 0) -> np.ndarray:
         """get_field(t) on the current state; returns H_demag of `layer`."""
         out = np.zeros((self.medium.layers[layer].N, 3))
