@@ -235,6 +235,8 @@ def batched_leg(args, torch, local, rank, dist):
     for i, med in enumerate(meds):
         runs.append(b.add(med, dt=DT, thermal_seed=1 + rank * args.batch + i,
                           tensor_from=runs[0] if runs else None))
+    if args.shape:
+        runs[0].set_shape(*[int(x) for x in args.shape.split(",")])
     n = meds[0].n_grains
     ext = torch.cuda.ExternalStream(b.stream(), device=local)
     hdirs = [np.array(m.layers[0].hdir) for m in meds]
@@ -403,6 +405,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50, help="bench steps of the end-to-end leg")
     ap.add_argument("--served", type=int, default=48, help="requests of the served sample (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="",
+                    help="row,column,columns-per-task kernel shapes of the batch (default: autotuned)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the headline batch (profiling runs)")
     args = ap.parse_args()

@@ -169,10 +169,13 @@ int mrm_gpu_get_time(const mrm_gpu* h, double* t, int64_t* step);
  * `layer` is returned if hdemag != NULL, the total field via get_field. */
 int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag);
 
-/* Advances nsteps fixed-dt steps of llg_type (-3 Heun; src/llg.f90:1122-1139,
- * :1195-1271).  Replaces nsteps iterations of the llg() loop body for a
- * fixed-step run (fixed_dt_p, conv_torque = conv_angle = 0).  `out` (may be
- * NULL) receives the reductions of the last step. */
+/* Advances nsteps fixed-dt steps of llg_type (src/llg.f90:1195-1271):
+ * -3 Heun (:1122-1139, two field evaluations per step), 2 semi-implicit push
+ * (:1109-1118, one field evaluation), -2 semi-implicit midpoint (predictor over
+ * dt/2, field at t+dt/2 on it, push of m_n over dt).  Replaces nsteps
+ * iterations of the llg() loop body for a fixed-step run (fixed_dt_p,
+ * conv_torque = conv_angle = 0); other types return MRM_ERR_UNSUPPORTED.
+ * `out` (may be NULL) receives the reductions of the last step. */
 int mrm_gpu_step(mrm_gpu* h, int nsteps, double dt, int llg_type, mrm_gpu_stats* out);
 
 /* Enqueues nsteps like mrm_gpu_step without waiting for them; the stats of
@@ -222,7 +225,7 @@ int mrm_batch_add(mrm_batch* b, const mrm_geom* geom, mrm_gpu** run);
 int mrm_batch_remove(mrm_batch* b, mrm_gpu* run);
 /* per-run time step and step budget: the run advances while step < step_end */
 int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active);
-/* Advances every active run by up to nsteps Heun steps (llg_type -3). */
+/* Advances every active run by up to nsteps steps of llg_type (-3, 2 or -2). */
 int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type);
 /* Stats of each listed run at its last executed step that ended an
  * mrm_batch_step / mrm_batch_enqueue call (a run whose budget ends inside a

@@ -79,9 +79,6 @@ static const RowOps* row_ops_of(int v) {
     }
   }
 }
-static int stage_slot(int stage, bool stats) {
-  return stage == kInit ? 0 : stage == kPred ? 1 : stage == kCorr ? (stats ? 3 : 2) : 4;
-}
 
 template <typename R>
 static cudaError_t launch_row_any(int v, int stage, bool stats, const RowLaunch& a, int istep, int flags) {
@@ -89,11 +86,11 @@ static cudaError_t launch_row_any(int v, int stage, bool stats, const RowLaunch&
   return o ? o->launch(stage, stats, a, istep, flags) : cudaErrorInvalidValue;
 }
 template <typename R>
-static cudaError_t row_allow_any(int v, const size_t* smem5) {
+static cudaError_t row_allow_any(int v, const size_t* smem6) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int q = 0; q < 5; ++q) {
-    cudaError_t e = allow_smem(o->fn[q], smem5[q]);
+  for (int q = 0; q < kRowSlots; ++q) {
+    cudaError_t e = allow_smem(o->fn[q], smem6[q]);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -102,14 +99,14 @@ template <typename R>
 static cudaError_t row_occ_any(int v, int stage, size_t smem, int* blocks) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn[stage_slot(stage, false)],
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn[row_slot(stage, false)],
                                                        row_variant<R>(v).block, smem);
 }
 template <typename R>
 static cudaError_t row_load_any(int v) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int q = 0; q < 5; ++q) {
+  for (int q = 0; q < kRowSlots; ++q) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[q]);
     if (e != cudaSuccess) return e;
@@ -121,7 +118,7 @@ static cudaError_t row_static_any(int v, int stage, bool stats, size_t* bytes) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[stage_slot(stage, stats)]);
+  cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[row_slot(stage, stats)]);
   if (e == cudaSuccess) *bytes = fa.sharedSizeBytes;
   return e;
 }
@@ -135,9 +132,9 @@ cudaError_t launch_row<double>(int v, int stage, bool stats, const RowLaunch& a,
   return launch_row_any<double>(v, stage, stats, a, istep, flags);
 }
 template <>
-cudaError_t row_allow_smem<float>(int v, const size_t* smem5) { return row_allow_any<float>(v, smem5); }
+cudaError_t row_allow_smem<float>(int v, const size_t* smem6) { return row_allow_any<float>(v, smem6); }
 template <>
-cudaError_t row_allow_smem<double>(int v, const size_t* smem5) { return row_allow_any<double>(v, smem5); }
+cudaError_t row_allow_smem<double>(int v, const size_t* smem6) { return row_allow_any<double>(v, smem6); }
 template <>
 cudaError_t row_occupancy<float>(int v, int stage, size_t smem, int* b) { return row_occ_any<float>(v, stage, smem, b); }
 template <>

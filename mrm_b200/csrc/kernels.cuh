@@ -27,7 +27,12 @@
 namespace mrm {
 
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
-enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4 };
+enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16 };
+// llg_type -3 (Heun): kPred + kCorr.  llg_type -2: kPred with kFlagBoris |
+// kFlagMid (semi-implicit push over dt/2) then kCorr with the same flags (field
+// at t+dt/2 on the predicted state, push of m_n over dt).  llg_type 2: kPred
+// with kFlagBoris alone (one push over dt into the predictor buffer; the
+// commit kernel copies it to the state).
 
 template <typename R>
 MRM_D void cross3(R ax, R ay, R az, R bx, R by, R bz, R& cx, R& cy, R& cz) {
@@ -122,7 +127,7 @@ MRM_D void block_reduce_record(double* rec, double* sred /* [32][kNPart] */, dou
 }
 
 template <int STAGE, bool STATS>
-__host__ __device__ constexpr int stats_slots() { return (STAGE == kCorr && STATS) ? 32 * kNPart : 1; }
+__host__ __device__ constexpr int stats_slots() { return ((STAGE == kCorr || STAGE == kPred) && STATS) ? 32 * kNPart : 1; }
 
 // ---------------- grain-row staging plan ----------------
 //
@@ -217,8 +222,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const int ngr = nrows * nx;
   const LayerDev<R>& L = rd.L[l];
   const bool demag = rd.demag != 0;
-  constexpr bool stats = (STAGE == kCorr) && STATS;
+  constexpr bool stats = (STAGE == kCorr || STAGE == kPred) && STATS;
   constexpr int NBMAX = 3 * RPB;
+  const bool boris = (flags & kFlagBoris) != 0, mid = (flags & kFlagMid) != 0;
 
   Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // post twiddles | pass tables
   const int ntw = row_tw_count(lgpx);
@@ -379,7 +385,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   };
 
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
-  const double t_stage = (STAGE == kCorr) ? t_now + rd.dt : t_now;
+  const double t_stage = (STAGE == kCorr) ? t_now + (mid ? 0.5 * rd.dt : rd.dt) : t_now;
   const double sc = ramp(L, t_stage);
   const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
@@ -486,7 +492,31 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
     V4<R> mn;
     R dx = 0, dy = 0, dz = 0, tq2 = 0;
-    if (mse > (R)0) {
+    if (mse > (R)0 && boris) {
+      // semi-implicit push (llg.f90:1109-1118): o = -g dt/2 h - alpha m,
+      // d = 2/(1+|o|^2) (m + m x o) x o, m' = m + d (norm preserved, no renormalisation);
+      // m is m_n in both stages, h the field of this stage
+      const V4<R> m0 = (STAGE == kCorr) ? M0[q] : mf;
+      const R a = pb.z;  // alpha * alpha_scale
+      const R s1 = (R)(-0.5) * gamma * ((STAGE == kPred && mid) ? (R)0.5 * dt : dt);
+      R tx, ty, tz;
+      cross3(m0.x, m0.y, m0.z, fx, fy, fz, tx, ty, tz);
+      tq2 = tx * tx + ty * ty + tz * tz;
+      const R ox = s1 * fx - a * m0.x, oy = s1 * fy - a * m0.y, oz = s1 * fz - a * m0.z;
+      R px, py, pz;
+      cross3(m0.x, m0.y, m0.z, ox, oy, oz, px, py, pz);
+      px += m0.x;
+      py += m0.y;
+      pz += m0.z;
+      const R y = (R)2 / ((R)1 + ox * ox + oy * oy + oz * oz);
+      cross3(px, py, pz, ox, oy, oz, dx, dy, dz);
+      dx *= y;
+      dy *= y;
+      dz *= y;
+      mn.x = m0.x + dx;
+      mn.y = m0.y + dy;
+      mn.z = m0.z + dz;
+    } else if (mse > (R)0) {
       const R a = pb.z;  // alpha * alpha_scale
       const R s11 = -gamma * dt / ((R)1 + a * a);
       R tx, ty, tz, ux, uy, uz;
@@ -773,6 +803,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
     if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nl * 3 * ny * phs, 440, idx)) continue;
     rd.spech[((size_t)lc * ny + j) * phs + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
   }
+}
+
+// llg_type 2: the predictor buffer holds m_{n+1} after the single push; copy
+// it to the state (one row task per block).
+template <typename R>
+__global__ void __launch_bounds__(256) commit_kernel(const RunDev<R>* __restrict__ runs,
+                                                     const Task* __restrict__ tasks, int istep, int flags) {
+  pdl_launch_dependents();
+  const Task tk = tasks[blockIdx.x];
+  const RunDev<R>& rd = runs[tk.x];
+  if (!rd.active) return;
+  pdl_wait();
+  const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
+  if (!(flags & kFlagForce) && step >= rd.step_end) return;
+  const LayerDev<R>& L = rd.L[tk.y];
+  const int n0 = tk.z * rd.nx, cnt = tk.w * rd.nx;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) L.m[n0 + i] = L.mp[n0 + i];
 }
 
 // Advances every active run's step counter after a captured chunk of k steps.

@@ -43,7 +43,7 @@ struct RowLaunch;
 // entry points of one compiled row shape (defined in its own translation unit)
 struct RowOps {
   cudaError_t (*launch)(int stage, bool stats, const RowLaunch& a, int istep, int flags);
-  const void* fn[5];  // kInit, kPred, kCorr, kCorr with reductions, kEval
+  const void* fn[6];  // kInit, kPred, kCorr, kCorr with reductions, kEval, kPred with reductions
 };
 template <typename R, int V>
 const RowOps& row_ops();
@@ -75,11 +75,16 @@ struct ColLaunch {
 // stage: kInit, kPred, kCorr, kEval; stats selects the corrector with reductions
 template <typename R>
 cudaError_t launch_row(int variant, int stage, bool stats, const RowLaunch& a, int istep, int flags);
-// lets each stage kernel of a variant use smem5[slot] bytes of dynamic shared
-// memory on the current device (slots: kInit, kPred, kCorr, kCorr with
-// reductions, kEval; the limit only grows)
+// launch slots of the row stages: kInit, kPred, kCorr, kCorr with reductions,
+// kEval, kPred with reductions (the single-stage integrator's last step)
+constexpr int kRowSlots = 6;
+inline int row_slot(int stage, bool stats) {
+  return stage == 0 ? 0 : stage == 1 ? (stats ? 5 : 1) : stage == 2 ? (stats ? 3 : 2) : 4;
+}
+// lets each stage kernel of a variant use smem6[slot] bytes of dynamic shared
+// memory on the current device (the limit only grows)
 template <typename R>
-cudaError_t row_allow_smem(int variant, const size_t* smem5);
+cudaError_t row_allow_smem(int variant, const size_t* smem6);
 template <typename R>
 cudaError_t row_occupancy(int variant, int stage, size_t smem, int* blocks_per_sm);
 // loads every stage's code (CUDA lazy loading would load it at first launch)

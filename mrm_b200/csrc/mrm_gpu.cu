@@ -102,15 +102,15 @@ struct Engine {
   bool shape_forced = false;         // shapes set by the caller instead of tuned
   int force_rowv = 0, force_colv = 0, force_cpt = 0;
   bool autotune = true;
-  size_t smem_row[5] = {0, 0, 0, 0, 0};  // per launch slot: init, pred, corr, corr+stats, eval
-  int stage_cap[5] = {0, 0, 0, 0, 0};
+  size_t smem_row[kRowSlots] = {0, 0, 0, 0, 0, 0};  // per launch slot (launch.h row_slot)
+  int stage_cap[kRowSlots] = {0, 0, 0, 0, 0, 0};
   size_t smem_col = 0;
   // the corrector with reductions always runs row shape 0 over one-row tasks,
   // so that the FP64 reductions do not depend on the tuned shapes
   Task* d_stasks = nullptr;
   int nst = 0, st_cap = 0;
-  size_t smem_stats = 0;
-  int cap_stats = 0;
+  size_t smem_stats[2] = {0, 0};  // reductions launch of kPred (single-stage integrator), kCorr
+  int cap_stats[2] = {0, 0};
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
   double* d_part = nullptr;
   int part_cap = 0;
@@ -273,13 +273,12 @@ size_t tensor_bytes(const mrm_gpu* r) {
 }
 
 // row-kernel launch slots: kInit, kPred, kCorr, kCorr with reductions, kEval
-constexpr int kSlots = 5;
-constexpr int kSlotStage[kSlots] = {kInit, kPred, kCorr, kCorr, kEval};
-int slot_of(int stage, bool stats) {
-  return stage == kInit ? 0 : stage == kPred ? 1 : stage == kCorr ? (stats ? 3 : 2) : 4;
-}
+constexpr int kSlots = kRowSlots;
+constexpr int kSlotStage[kSlots] = {kInit, kPred, kCorr, kCorr, kEval, kPred};
 // static shared memory of a row stage (mbarriers, reduction scratch) with margin
-size_t row_static_bytes(int slot) { return (slot == 3 ? 32 * kNPart * sizeof(double) : sizeof(double)) + 64; }
+size_t row_static_bytes(int slot) {
+  return ((slot == 3 || slot == 5) ? 32 * kNPart * sizeof(double) : sizeof(double)) + 64;
+}
 constexpr size_t kSmemPerSM = 228 * 1024;
 constexpr size_t kSmemReserved = 1024;  // per block
 
@@ -459,7 +458,7 @@ int plan_smem(Engine* e) {
   std::string* errp = &e->err;
   const RowVariant rv = row_variant<R>(e->rowv);
   size_t fft = 16;
-  int need[kSlots] = {0, 0, 0, 0, 0};
+  int need[kSlots] = {0, 0, 0, 0, 0, 0};
   size_t scol = 16;
   for (auto* r : e->runs) {
     if (r->lgpx > rv.lgmax)
@@ -481,22 +480,26 @@ int plan_smem(Engine* e) {
   if (scol + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
   e->smem_col = scol;
   CK(row_allow_smem<R>(e->rowv, e->smem_row));
-  // the reductions launch: row shape 0, one row per task
+  // the reductions launches (kPred of the single-stage integrator, kCorr):
+  // row shape 0, one row per task
   {
     const RowVariant r0 = row_variant<R>(0);
     size_t f0 = 16;
-    int n0 = 0;
+    int n0[2] = {0, 0};
     for (auto* r : e->runs) {
       f0 = std::max(f0, (size_t)row_fft_smem<R>(r->lgpx, 1));
-      n0 = std::max(n0, run_stage_bytes<R>(r, kCorr, 1));
+      n0[0] = std::max(n0[0], run_stage_bytes<R>(r, kPred, 1));
+      n0[1] = std::max(n0[1], run_stage_bytes<R>(r, kCorr, 1));
     }
-    const long long per_block = (long long)(kSmemPerSM / r0.minb) - (long long)kSmemReserved -
-                                (long long)row_static_bytes(3) - (long long)f0;
-    const long long hard = (long long)kMaxSmem - (long long)row_static_bytes(3) - (long long)f0;
+    const long long stat = (long long)row_static_bytes(3);
+    const long long per_block = (long long)(kSmemPerSM / r0.minb) - (long long)kSmemReserved - stat - (long long)f0;
+    const long long hard = (long long)kMaxSmem - stat - (long long)f0;
     if (hard < 0) return set_err(errp, MRM_ERR_UNSUPPORTED, "grid exceeds shared memory");
-    e->cap_stats = (int)(std::min<long long>(n0, std::max(0LL, std::min(per_block, hard))) & ~15LL);
-    e->smem_stats = f0 + (size_t)e->cap_stats;
-    size_t lim[kSlots] = {0, 0, 0, e->smem_stats, 0};
+    for (int i = 0; i < 2; ++i) {
+      e->cap_stats[i] = (int)(std::min<long long>(n0[i], std::max(0LL, std::min(per_block, hard))) & ~15LL);
+      e->smem_stats[i] = f0 + (size_t)e->cap_stats[i];
+    }
+    size_t lim[kSlots] = {0, 0, 0, e->smem_stats[1], 0, e->smem_stats[0]};
     CK(row_allow_smem<R>(0, lim));
   }
   CK(col_allow_smem<R>(e->colv, e->smem_col));
@@ -578,11 +581,12 @@ template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
   if (stats) {
-    RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats,
-                e->cap_stats, pdl};
+    const int i = stage == kPred ? 0 : 1;
+    RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
+                e->cap_stats[i], pdl};
     return launch_row<R>(0, stage, true, a, istep, flags);
   }
-  const int q = slot_of(stage, false);
+  const int q = row_slot(stage, false);
   RowLaunch a{e->st, e->d_runs, e->d_rtasks, e->d_tw, e->d_part, e->d_err, e->nrt, e->smem_row[q],
               e->stage_cap[q], pdl};
   return launch_row<R>(e->rowv, stage, false, a, istep, flags);
@@ -595,15 +599,26 @@ cudaError_t launch_col_e(Engine* e, int istep, int flags, bool pdl = true) {
   return launch_col<R>(e->colv, a, istep, flags);
 }
 
+// llg_type -3 (Heun) and -2 (semi-implicit midpoint): two field evaluations
+// per step; llg_type 2 (semi-implicit): one, then the commit of the new state
 template <typename R>
-cudaError_t enqueue_steps(Engine* e, int k, bool stats) {
+cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type) {
   cudaError_t ce = cudaSuccess;
   auto acc = [&](cudaError_t x) { if (ce == cudaSuccess) ce = x; };
+  const int f = llg_type == 2 ? kFlagBoris : llg_type == -2 ? (kFlagBoris | kFlagMid) : 0;
   for (int i = 0; i < k; ++i) {
     const bool last = stats && i == k - 1;
-    acc(launch_row_e<R>(e, kPred, false, i, 0));
+    const int lf = last ? (kFlagStats | kFlagStoreField) : 0;
+    if (llg_type == 2) {
+      acc(launch_row_e<R>(e, kPred, last, i, f | lf));
+      acc(launch_col_e<R>(e, i, 0));
+      acc(launch_kernel(commit_kernel<R>, dim3(e->nst), dim3(256), 0, e->st, true,
+                        static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_stasks, i, 0));
+      continue;
+    }
+    acc(launch_row_e<R>(e, kPred, false, i, f));
     acc(launch_col_e<R>(e, i, 0));
-    acc(launch_row_e<R>(e, kCorr, last, i, last ? (kFlagStats | kFlagStoreField) : 0));
+    acc(launch_row_e<R>(e, kCorr, last, i, f | lf));
     acc(launch_col_e<R>(e, i, 0));
   }
   const int nr = (int)e->runs.size();
@@ -828,7 +843,7 @@ int ensure_ready(Engine* e) {
 }
 
 template <typename R>
-int run_steps(Engine* e, int nsteps) {
+int run_steps(Engine* e, int nsteps, int llg_type) {
   std::string* errp = &e->err;
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
@@ -836,12 +851,12 @@ int run_steps(Engine* e, int nsteps) {
   while (left > 0) {
     const int k = std::min(left, kGraphSteps);
     const bool stats = (left == k);  // reductions only on the call's last step
-    auto key = std::make_pair(k, stats ? 1 : 0);
+    auto key = std::make_pair(k, (stats ? 1 : 0) + 2 * (llg_type + 3));
     auto it = e->graphs.find(key);
     if (it == e->graphs.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-      cudaError_t le = enqueue_steps<R>(e, k, stats);
+      cudaError_t le = enqueue_steps<R>(e, k, stats, llg_type);
       cudaError_t ce = cudaStreamEndCapture(e->st, &g);
       if (le != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "launch in capture: %s", cudaGetErrorString(le));
       if (ce != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
@@ -864,10 +879,12 @@ int run_steps(Engine* e, int nsteps) {
   return MRM_OK;
 }
 
-int engine_step(Engine* e, int nsteps) {
-  if (e->prec == MRM_FP64) return run_steps<double>(e, nsteps);
-  return run_steps<float>(e, nsteps);
+int engine_step(Engine* e, int nsteps, int llg_type) {
+  if (e->prec == MRM_FP64) return run_steps<double>(e, nsteps, llg_type);
+  return run_steps<float>(e, nsteps, llg_type);
 }
+
+bool llg_type_ok(int t) { return t == -3 || t == -2 || t == 2; }
 
 template <typename R>
 int engine_eval(Engine* e) {
@@ -1604,7 +1621,9 @@ static int plain_prepare(mrm_gpu* h, int nsteps, double dt, int llg_type) {
   std::string* errp = &h->err;
   if (nsteps < 0) return set_err(errp, MRM_ERR_ARG, "nsteps must be >= 0");
   if (!(dt > 0)) return set_err(errp, MRM_ERR_ARG, "dt must be > 0");
-  if (llg_type != -3) return set_err(errp, MRM_ERR_UNSUPPORTED, "llg_type %d: only Heun (-3) is on this path", llg_type);
+  if (!llg_type_ok(llg_type))
+    return set_err(errp, MRM_ERR_UNSUPPORTED,
+                   "llg_type %d: this path has Heun (-3) and the semi-implicit pushes (2, -2)", llg_type);
   for (int l = 0; l < h->nl; ++l)
     if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
   if (h->demag && !h->tensor_ready) return set_err(errp, MRM_ERR_STATE, "build or upload the tensor first (or disable demag)");
@@ -1629,7 +1648,7 @@ int mrm_gpu_enqueue_steps(mrm_gpu* h, int nsteps, double dt, int llg_type) {
   int rc = plain_prepare(h, nsteps, dt, llg_type);
   if (rc) return rc;
   if (nsteps > 0) {
-    rc = engine_step(h->eng, nsteps);
+    rc = engine_step(h->eng, nsteps, llg_type);
     if (rc) {
       h->err = h->eng->err;
       return rc;
@@ -1851,7 +1870,8 @@ int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type) {
   if (!b) return MRM_ERR_ARG;
   Engine* e = &b->eng;
   std::string* errp = &e->err;
-  if (llg_type != -3) return set_err(errp, MRM_ERR_UNSUPPORTED, "llg_type %d: only Heun (-3)", llg_type);
+  if (!llg_type_ok(llg_type))
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "llg_type %d: this path has -3, -2 and 2", llg_type);
   for (auto* r : e->runs) {
     if (!r->active) continue;
     for (int l = 0; l < r->nl; ++l)
@@ -1859,7 +1879,7 @@ int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type) {
     if (r->demag && !r->tensor_ready) return set_err(errp, MRM_ERR_STATE, "a run has no tensor");
   }
   if (nsteps <= 0) return MRM_OK;
-  return engine_step(e, nsteps);
+  return engine_step(e, nsteps, llg_type);
 }
 
 int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type) {

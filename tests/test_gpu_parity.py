@@ -124,3 +124,37 @@ def test_two_layer_trajectory_fp64(oracle, gpulib):
     for l in range(2):
         assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-9
     assert np.allclose(sg["mave_l"][:2], so["mave_l"][:2], atol=1e-10)
+
+
+# The semi-implicit push keeps |m| without renormalising it, so FP32 rounding
+# of |m| accumulates over the steps (about 1e-7 per step, a random walk): the
+# FP32 tolerance after 2,000 steps through switching is 5e-4 per component.
+@pytest.mark.parametrize("llg_type", [2, -2])
+@pytest.mark.parametrize("precision,tol", [(FP64, 1e-9), (FP32, 5e-4)])
+def test_semi_implicit_t0_trajectory(oracle, gpulib, llg_type, precision, tol):
+    """Semi-implicit pushes (llg.f90:1109-1118): one field evaluation per step
+    (type 2) or the midpoint form (type -2), against the oracle through switching."""
+    med = small_medium(16, boundary=1)
+    med.layers[0].t_end = 2e-10
+    orc, gpu = _pair(oracle, med, precision)
+    dt = 1e-13
+    for chunk in range(4):
+        so = orc.step(500, dt, llg_type=llg_type)
+        sg = gpu.step(500, dt, llg_type=llg_type)
+        assert np.abs(gpu.get_state(0) - orc.get_state(0)).max() < tol, chunk
+    assert so["mave"][2] < 0.5
+    for key in ("errmx", "errmx1", "mmag"):
+        assert sg[key] == pytest.approx(so[key], rel=max(tol, 1e-9) * 50, abs=1e-30), key
+    assert sg["step"] == so["step"] == 2000
+
+
+@pytest.mark.parametrize("llg_type", [2, -2])
+def test_semi_implicit_thermal_two_layers_fp64(oracle, gpulib, llg_type):
+    med = two_layer(16, 8, temperature=300.0)
+    orc, gpu = _pair(oracle, med, FP64, seed=4)
+    so = orc.step(150, 1e-13, llg_type=llg_type)
+    gpu.step(150, 1e-13, llg_type=llg_type)
+    for l in range(2):
+        assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-8
+    # the push preserves |m| without renormalisation (to rounding)
+    assert np.abs(np.linalg.norm(gpu.get_state(0), axis=1) - 1.0).max() < 1e-12

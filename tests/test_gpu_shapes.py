@@ -64,3 +64,28 @@ def test_autotune_restores_state(gpulib):
     m, used, _ = _run(med, FP32, autotune=True, steps=64)
     assert 0 <= used[0] < 5 and 0 <= used[1] < 3
     assert np.array_equal(m[0], ref[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("llg_type", [2, -2])
+def test_semi_implicit_shapes_and_batch(gpulib, llg_type):
+    """The semi-implicit integrators are shape-independent and batch == alone."""
+    from mrm_b200 import FP32, GpuSim
+    from mrm_b200.batch import Batch
+    med = small_medium(64, boundary=1, seed=12, temperature=300.0)
+    outs = []
+    for shape in [(0, 0, 0), (1, 1, 2), (3, 2, 4)]:
+        sim = GpuSim(med, precision=FP32, thermal_seed=2)
+        sim.set_shape(*shape)
+        st = sim.step(48, DT, llg_type=llg_type)
+        outs.append((sim.get_state(0), st["mave"].copy()))
+        sim.close()
+    for m, mv in outs[1:]:
+        assert np.array_equal(m, outs[0][0]) and np.array_equal(mv, outs[0][1])
+    b = Batch(FP32)
+    r = b.add(med, dt=DT, steps=48, thermal_seed=2)
+    b.add(small_medium(32, boundary=1, seed=13, temperature=300.0), dt=DT, steps=48, thermal_seed=3)
+    b.step(48, llg_type=llg_type)
+    assert np.array_equal(r.get_state(0), outs[0][0])
+    assert np.array_equal(b.stats([r])[0]["mave"], outs[0][1])
+    b.close()
