@@ -18,6 +18,8 @@ Beside the headline (sub-objects of the same JSON line):
            same medium and seed;
   mix      64 realisations with grain counts log-uniform in [1,024, 65,536],
            Hk sigma in [3 %, 10 %], 5,000 Heun steps each, one batch;
+  write    the two-layer 1,024 x 256 recording write by the moving Karlqvist
+           head (PRBS pattern), a bounded 2,000-step sample;
   served   a bounded sample of the Poisson request stream (200 req/s, M(H)
            and write requests of 1,024..262,144 grains, 2,000..20,000 steps):
            aggregate grain-steps/s and p50/p99 latency.
@@ -349,6 +351,32 @@ def plain_leg(torch, local, precision, heun_chunk=100, total=RAMP_STEPS, flush_l
             1e3 * dev_ms / (nchunks * heun_chunk), "hc_oe": hc, "mr": mr, "prof": prof}
 
 
+def write_leg(torch, local, steps=2000):
+    """The two-layer recording write (1,024 x 256 grains per layer, 7 nm pitch,
+    Karlqvist head at 20 m/s writing a 64-bit PRBS at 15 nm bits, T = 300 K,
+    FP32, Heun) as one plain run: a bounded sample of the 480,000-step write."""
+    from mrm_b200 import FP32, GpuSim, media
+    med = media.head_write_medium(1024, 256, seed=1, prbs_seed=1, temperature=300.0)
+    sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.step(48, DT, stats=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.enqueue(steps, DT)
+    e1.record(ext)
+    st = sim.stats()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    px, py = sim.fft_grid()
+    sim.close()
+    grains = 2 * 1024 * 256
+    return {"workload": f"two-layer 1024x256x2 head write (gap 25 nm, fly 6 nm, 12 kOe, 20 m/s, 64-bit PRBS "
+                        f"at 15 nm), T=300 K, FP32, {px}x{py} padded FFT, {steps} Heun steps of the 480,000",
+            "grains": grains, "value": grains * steps / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
+            "us_per_heun_step": 1e3 * ms / steps, "mave_top": np.asarray(st["mave_l"][0]).tolist()}
+
+
 def mix_leg(torch, local, steps=5000, nreal=64):
     from mrm_b200 import FP32
     from mrm_b200.batch import Batch
@@ -491,6 +519,7 @@ def main():
                                 "mr_fp32": p32["mr"], "mr_fp64": p64["mr"],
                                 "fp64_us_per_heun_step": p64["us_per_heun_step"]})
         line["mix"] = mix_leg(torch, local)
+        line["write"] = write_leg(torch, local)
         if args.served > 0:
             line["served"] = served_leg(local, args.served)
         if world == 1 and not args.no_cpu_baseline:

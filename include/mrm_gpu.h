@@ -150,6 +150,20 @@ int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int 
                                double gamma, double phase, double param, double duty,
                                double moddepth, double dc, double scale);
 
+/* Moving write head on `layer` (applied-field form 6; the reference has no
+ * analytic head and drives writes with a tabulated moving field,
+ * applied.f90:711-813,1471-1520): the 2-D Karlqvist field of a ring head with
+ * gap `gap` (cm) whose gap centre sits at x0 + velocity*(t - t0) down-track
+ * (+x, cm), at distance z (cm) from the layer's mid-plane, deep-gap field hg
+ * (Oe):
+ *   h_x = P hg/pi (atan((u + gap/2)/z) - atan((u - gap/2)/z)),
+ *   h_z = P hg/(2 pi) ln(((u - gap/2)^2 + z^2) / ((u + gap/2)^2 + z^2)),
+ * u = (i + 1/2) dx - gap centre for grain column i; write polarity P = +1 if
+ * bit floor((t - t0)/bit_time) mod nbits of `pattern` is set (bit 0 first),
+ * else -1.  Replaces the layer's uniform field. */
+int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double hg, double velocity, double x0,
+                           double t0, double bit_time, uint64_t pattern, int nbits);
+
 /* Thermal (Brown) field of `layer` at `temperature` K (get_thermal,
  * field.f90:397-436).  The normals come from a counter-based Philox4x64-10
  * stream keyed by `seed` (statistical, not bitwise, equivalence with the

@@ -33,7 +33,7 @@ EXPORTS = [
     "mrm_batch_enqueue", "mrm_batch_stream", "mrm_batch_create", "mrm_batch_destroy", "mrm_batch_last_error",
     "mrm_batch_add", "mrm_batch_remove", "mrm_batch_set_run", "mrm_batch_step", "mrm_batch_stats",
     "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
-    "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile",
+    "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile", "mrm_gpu_set_head_field",
     "mrm_gpu_set_shape", "mrm_gpu_set_autotune", "mrm_gpu_get_shape", "mrm_gpu_check_device",
 ]
 
@@ -122,6 +122,7 @@ def load(path: str = LIB_PATH):
         "mrm_device_memory": ([i, P(i64), P(i64)], i),
         "mrm_gpu_demag_noalloc": ([vp, vp, vp, vp], i),
         "mrm_batch_profile": ([vp, i, pd], i),
+        "mrm_gpu_set_head_field": ([vp, i, d, d, d, d, d, d, d, u64, i], i),
         "mrm_gpu_set_shape": ([vp, i, i, i], i),
         "mrm_gpu_set_autotune": ([vp, i], i),
         "mrm_gpu_get_shape": ([vp, P(i)], i),

@@ -66,8 +66,15 @@ struct LayerDev {
   const R* lcol;
   double hdir[3];
   double t_start, t_end, s_start, s_end, scale;
-  int func;  // 0 linear ramp; 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW (applied.f90:328-377)
+  int func;  // 0 linear ramp; 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW (applied.f90:328-377); 6 head
   double amp, fgamma, phase, param, duty, moddepth, dc;
+  // moving write head (func 6): Karlqvist field of a ring head, gap hd_gap, at
+  // distance hd_z above the layer's mid-plane, deep-gap field hd_hg, gap centre
+  // at hd_x0 + hd_v (t - hd_t0) down-track; write polarity from bit
+  // floor((t - hd_t0)/hd_tbit) mod hd_nbits of hd_bits; grain column i at (i + 1/2) hd_dx
+  double hd_gap, hd_z, hd_hg, hd_v, hd_x0, hd_t0, hd_tbit, hd_dx;
+  unsigned long long hd_bits;
+  int hd_nbits;
   double temperature;
   double gamma;
   int thermal;
@@ -99,6 +106,8 @@ struct RunDev {
                            // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];
 };
+
+constexpr int kFuncHead = 6;
 
 // Tensor component parity (c = 3*field + source): the spectrum is purely
 // imaginary for xz, yz, zx, zy and odd in ky for xy, yx, yz, zy.

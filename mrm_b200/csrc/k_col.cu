@@ -89,28 +89,30 @@ template <typename R>
 static cudaError_t row_allow_any(int v, const size_t* smem6) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int q = 0; q < kRowSlots; ++q) {
-    cudaError_t e = allow_smem(o->fn[q], smem6[q]);
-    if (e != cudaSuccess) return e;
-  }
+  for (int g = 0; g < 2; ++g)
+    for (int q = 0; q < kRowSlots; ++q) {
+      cudaError_t e = allow_smem(o->fn[g][q], smem6[q]);
+      if (e != cudaSuccess) return e;
+    }
   return cudaSuccess;
 }
 template <typename R>
 static cudaError_t row_occ_any(int v, int stage, size_t smem, int* blocks) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn[row_slot(stage, false)],
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn[0][row_slot(stage, false)],
                                                        row_variant<R>(v).block, smem);
 }
 template <typename R>
 static cudaError_t row_load_any(int v) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int q = 0; q < kRowSlots; ++q) {
-    cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[q]);
-    if (e != cudaSuccess) return e;
-  }
+  for (int g = 0; g < 2; ++g)
+    for (int q = 0; q < kRowSlots; ++q) {
+      cudaFuncAttributes fa;
+      cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[g][q]);
+      if (e != cudaSuccess) return e;
+    }
   return cudaSuccess;
 }
 template <typename R>
@@ -118,7 +120,7 @@ static cudaError_t row_static_any(int v, int stage, bool stats, size_t* bytes) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[row_slot(stage, stats)]);
+  cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[1][row_slot(stage, stats)]);
   if (e == cudaSuccess) *bytes = fa.sharedSizeBytes;
   return e;
 }

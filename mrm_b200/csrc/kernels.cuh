@@ -84,6 +84,34 @@ MRM_D double ramp(const LayerDev<R>& L, double t) {
   return ((L.s_end - L.s_start) * u + L.s_start) * L.scale;
 }
 
+// Write head (func 6): gap-centre position and write polarity at time t
+template <typename R>
+MRM_D void head_state(const LayerDev<R>& L, double t, double* xh, double* pol) {
+  *xh = L.hd_x0 + L.hd_v * (t - L.hd_t0);
+  long long k = (long long)floor((t - L.hd_t0) / L.hd_tbit);
+  const long long nb = L.hd_nbits > 0 ? L.hd_nbits : 1;
+  k %= nb;
+  if (k < 0) k += nb;
+  *pol = ((L.hd_bits >> k) & 1ull) ? 1.0 : -1.0;
+}
+
+// Karlqvist field at down-track offset u from the gap centre:
+//   h_x = Hg/pi (atan((u + g/2)/z) - atan((u - g/2)/z))
+//   h_z = Hg/(2 pi) ln(((u - g/2)^2 + z^2) / ((u + g/2)^2 + z^2))
+template <typename R>
+MRM_D void karlqvist(R u, R g, R z, R hg, R& hx, R& hz) {
+  const R a = u + (R)0.5 * g, b = u - (R)0.5 * g;
+  const R pi = (R)3.14159265358979323846;
+  hx = hg / pi * (atan(a / z) - atan(b / z));
+  hz = hg / ((R)2 * pi) * log((b * b + z * z) / (a * a + z * z));
+}
+
+// shared memory of a row block's head-field table (one (h_x, h_z) per grid column)
+template <typename R>
+MRM_HD int head_table_bytes(int nx) {
+  return (nx * (int)sizeof(Cx<R>) + 15) & ~15;
+}
+
 // CSR neighbour sum  sum_j c_j m_j  (field.f90:350-363 / :326-348)
 template <typename R>
 MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
@@ -196,7 +224,9 @@ MRM_HD int row_fft_smem(int lgpx, int rpb) {
 //                  stage, forward row FFT of Ms*m* / Ms*m_{n+1}
 //   kEval: inverse row FFT and field assembly only (H_demag and h stored)
 // stage_cap: bytes of dynamic shared memory available for grain staging.
-template <typename R, int STAGE, bool STATS, int RPB, int BLOCK, int MINB, int LGMAX>
+// GEN: the general instantiation (semi-implicit pushes, write head); the other
+// one is Heun without a head, with those paths compiled out.
+template <typename R, int STAGE, bool STATS, int RPB, int BLOCK, int MINB, int LGMAX, bool GEN>
 __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __restrict__ runs,
                                                           const Task* __restrict__ tasks,
                                                           const Cx<R>* __restrict__ twg, int istep,
@@ -224,13 +254,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const bool demag = rd.demag != 0;
   constexpr bool stats = (STAGE == kCorr || STAGE == kPred) && STATS;
   constexpr int NBMAX = 3 * RPB;
-  const bool boris = (flags & kFlagBoris) != 0, mid = (flags & kFlagMid) != 0;
+  const bool boris = GEN && (flags & kFlagBoris) != 0, mid = GEN && (flags & kFlagMid) != 0;
 
   Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // post twiddles | pass tables
   const int ntw = row_tw_count(lgpx);
   Cx<R>* bufA = tws + ntw;
   Cx<R>* bufB = bufA + RPB * 3 * cs;
-  unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs);
+  // a layer under the moving write head gets its head field per grid column in
+  // a table after the FFT buffers (the host reserves it), then the staging area
+  // (its byte offset; 0: no head)
+  const int htab_off = GEN && rd.L[tk.y].func == kFuncHead
+                           ? (int)(reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) - smem_raw)
+                           : 0;
+  unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) +
+                       (htab_off ? head_table_bytes<R>(rd.nx) : 0);
+  if (htab_off && (long long)(stg - smem_raw) > (long long)dynamic_smem_bytes()) {  // host bug: no room reserved
+    if (threadIdx.x == 0) atomicOr(err, kErrShape);
+    return;
+  }
   const Cx<R>* twpost = tws;
   const Cx<R>* twpass = tws + row_tw_post(lgpx);
 
@@ -392,6 +433,37 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const R gamma = (R)L.gamma;
   const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
   const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
+  // Write head: its field depends on the column and the time only.  The
+  // stepping stages add it to the block's demag values in shared memory (zero
+  // when demag is off), so their per-grain loop is the same with or without a
+  // head; the evaluation stage keeps demag apart and reads a per-column table.
+  const bool fold_head = (STAGE == kPred || STAGE == kCorr) && htab_off;
+  const bool use_hdr = demag || fold_head;
+  if (STAGE != kInit && htab_off) {
+    double xh, pol;
+    head_state(L, t_stage, &xh, &pol);
+    R* hw = reinterpret_cast<R*>(Z);
+    for (int c = threadIdx.x; c < nx; c += BLOCK) {
+      R khx, khz;
+      karlqvist<R>((R)(((double)c + 0.5) * L.hd_dx - xh), (R)L.hd_gap, (R)L.hd_z, (R)(pol * L.hd_hg), khx, khz);
+      if (STAGE == kEval) {
+        reinterpret_cast<Cx<R>*>(smem_raw + htab_off)[c] = Cx<R>{khx, khz};
+      } else {
+        for (int r = 0; r < nrows; ++r) {
+          R* w = hw + (size_t)(r * 3) * rs + c;
+          if (demag) {
+            w[0] += khx;
+            w[2 * rs] += khz;
+          } else {
+            w[0] = khx;
+            w[rs] = (R)0;
+            w[2 * rs] = khz;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
   const bool pow2x = (nx & (nx - 1)) == 0;
   const int lgnx = __ffs(nx) - 1;
 
@@ -416,13 +488,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const V4<R> mf = MF[q];
     const V4<R> pa = PA[q];
     R hdx = 0, hdy = 0, hdz = 0;
-    if (demag) {
+    if (use_hdr) {
       hdx = hdr[(rr * 3 + 0) * rs + i];
       hdy = hdr[(rr * 3 + 1) * rs + i];
       hdz = hdr[(rr * 3 + 2) * rs + i];
     }
+    // applied field of this grain: the uniform part (plus the write head's in
+    // the evaluation stage; the stepping stages carry it in hdx, hdz)
+    R apx = hax, apy = hay, apz = haz;
+    if constexpr (STAGE == kEval) {
+      if (htab_off) {
+        const Cx<R> kh = reinterpret_cast<const Cx<R>*>(smem_raw + htab_off)[i];
+        apx += kh.x;
+        apz += kh.y;
+      }
+    }
     // h = h_app + h_demag + H_uni + H_ex (+ interlayer)   (field.f90:201,211-220)
-    R hx = hax + hdx, hy = hay + hdy, hz = haz + hdz;
+    R hx = apx + hdx, hy = apy + hdy, hz = apz + hdz;
     R e_k;
     {
       // get_uni_hk (field.f90:366-375); pa.w = Hk1*hk_scale, pb.y = Hk2*hk_scale
@@ -586,8 +668,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
       rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
       // energy at the evaluated state (field.f90:200, :360, :374, :339)
-      const double e_d = -((double)mf.x * ((double)hdx + hax) + (double)mf.y * ((double)hdy + hay) +
-                           (double)mf.z * ((double)hdz + haz)) * (double)mse;
+      const double e_d = -((double)mf.x * ((double)hdx + apx) + (double)mf.y * ((double)hdy + apy) +
+                           (double)mf.z * ((double)hdz + apz)) * (double)mse;
       const double e_x = -((double)(ex + vx) * mf.x + (double)(ey + vy) * mf.y +
                            (double)(ez + vz) * mf.z) * (double)mse;
       rec[kSlotE] += (e_d + (double)e_k + e_x) * v;
@@ -596,7 +678,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   if constexpr (stats) {
     block_reduce_record(rec, sred, part + (size_t)blockIdx.x * kNPart);
   }
-  if (STAGE == kEval || !demag) return;
+  if (STAGE == kEval || rd.demag == 0) return;  // (reloaded: one register less across the loop)
 
   // ---------------- forward row transform of Ms*m -> spectrum columns ----------------
   const int two_m = 2 * M;

@@ -43,7 +43,9 @@ struct RowLaunch;
 // entry points of one compiled row shape (defined in its own translation unit)
 struct RowOps {
   cudaError_t (*launch)(int stage, bool stats, const RowLaunch& a, int istep, int flags);
-  const void* fn[6];  // kInit, kPred, kCorr, kCorr with reductions, kEval, kPred with reductions
+  // [general][slot]: slots kInit, kPred, kCorr, kCorr with reductions, kEval,
+  // kPred with reductions; general: semi-implicit pushes and the write head
+  const void* fn[2][6];
 };
 template <typename R, int V>
 const RowOps& row_ops();
@@ -59,6 +61,7 @@ struct RowLaunch {
   size_t smem;
   int stage_cap;
   bool pdl;          // programmatic stream serialization with the previous kernel
+  bool gen;          // the general instantiation (needed for llg_type 2/-2 and write heads)
 };
 
 struct ColLaunch {

@@ -57,6 +57,9 @@ struct LayerBufs {
   double amp = 0, fgamma = 0, phase = 0, param = 0, duty = 0, moddepth = 0, dc = 0;
   double temperature = 0.0, gamma = 1.76e7;
   int thermal = 0;
+  double hd_gap = 0, hd_z = 1, hd_hg = 0, hd_v = 0, hd_x0 = 0, hd_t0 = 0, hd_tbit = 1;
+  unsigned long long hd_bits = 0;
+  int hd_nbits = 1;
 };
 
 struct Engine;
@@ -112,6 +115,7 @@ struct Engine {
   size_t smem_stats[2] = {0, 0};  // reductions launch of kPred (single-stage integrator), kCorr
   int cap_stats[2] = {0, 0};
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
+  bool has_head = false;             // a run has a layer under the write head (general kernels)
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -295,6 +299,16 @@ int run_stage_bytes(const mrm_gpu* r, int stage, int rows) {
   return need;
 }
 
+// row-kernel shared memory before the staging area: twiddles, FFT buffers and,
+// for a run with a layer under the write head, the head-field table
+template <typename R>
+size_t row_fixed_smem(const mrm_gpu* r, int rpb) {
+  size_t b = (size_t)row_fft_smem<R>(r->lgpx, rpb);
+  for (int l = 0; l < r->nl; ++l)
+    if (r->L[l].func == kFuncHead) return b + (size_t)head_table_bytes<R>(r->g.nx);
+  return b;
+}
+
 template <typename R>
 size_t col_smem_of(const mrm_gpu* r, int nc) {
   size_t b = col_fft_smem<R>(r->lgpy, nc * r->nl * 3);
@@ -334,7 +348,8 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
   tmp.lgpy = ilog2(py);
   tmp.nl = g->n_lay;
   const bool f64 = g->precision == MRM_FP64;
-  const size_t rs = f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1);
+  const size_t rs = (f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1)) +
+                    (size_t)(f64 ? head_table_bytes<double>(g->nx) : head_table_bytes<float>(g->nx));
   const size_t cs = f64 ? col_smem_of<double>(&tmp, 1) : col_smem_of<float>(&tmp, 1);
   if (rs + row_static_bytes(3) > kMaxSmem || cs + 64 > kMaxSmem)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d x %d layers exceeds shared memory", px,
@@ -415,6 +430,16 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.gamma = b.gamma;
     o.thermal = b.thermal;
     o.n = b.n;
+    o.hd_gap = b.hd_gap;
+    o.hd_z = b.hd_z;
+    o.hd_hg = b.hd_hg;
+    o.hd_v = b.hd_v;
+    o.hd_x0 = b.hd_x0;
+    o.hd_t0 = b.hd_t0;
+    o.hd_tbit = b.hd_tbit;
+    o.hd_dx = r->g.dx;
+    o.hd_bits = b.hd_bits;
+    o.hd_nbits = b.hd_nbits;
   }
   return d;
 }
@@ -464,7 +489,7 @@ int plan_smem(Engine* e) {
     if (r->lgpx > rv.lgmax)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d does not cover %d-column FFT grids", e->rowv, r->px);
     const int rows = rows_per_task(r, rv.rpb);
-    fft = std::max(fft, (size_t)row_fft_smem<R>(r->lgpx, rv.rpb));
+    fft = std::max(fft, row_fixed_smem<R>(r, rv.rpb));
     for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
     if (r->demag && r->tensor_ready) scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r)));
   }
@@ -487,7 +512,7 @@ int plan_smem(Engine* e) {
     size_t f0 = 16;
     int n0[2] = {0, 0};
     for (auto* r : e->runs) {
-      f0 = std::max(f0, (size_t)row_fft_smem<R>(r->lgpx, 1));
+      f0 = std::max(f0, row_fixed_smem<R>(r, 1));
       n0[0] = std::max(n0[0], run_stage_bytes<R>(r, kPred, 1));
       n0[1] = std::max(n0[1], run_stage_bytes<R>(r, kCorr, 1));
     }
@@ -529,6 +554,9 @@ int build_tables(Engine* e) {
   }
   e->nrt = (int)rt.size();
   e->nct = (int)ct.size();
+  e->has_head = false;
+  for (auto* r : e->runs)
+    for (int l = 0; l < r->nl; ++l) e->has_head = e->has_head || r->L[l].func == kFuncHead;
   e->nst = (int)stt.size();
   if (e->nst > e->st_cap) {
     dfree(e->d_stasks);
@@ -580,15 +608,17 @@ int build_tables(Engine* e) {
 template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
+  // the general kernels for the semi-implicit pushes and write heads
+  const bool gen = (flags & kFlagBoris) || e->has_head;
   if (stats) {
     const int i = stage == kPred ? 0 : 1;
     RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
-                e->cap_stats[i], pdl};
+                e->cap_stats[i], pdl, gen};
     return launch_row<R>(0, stage, true, a, istep, flags);
   }
   const int q = row_slot(stage, false);
   RowLaunch a{e->st, e->d_runs, e->d_rtasks, e->d_tw, e->d_part, e->d_err, e->nrt, e->smem_row[q],
-              e->stage_cap[q], pdl};
+              e->stage_cap[q], pdl, gen};
   return launch_row<R>(e->rowv, stage, false, a, istep, flags);
 }
 
@@ -1500,6 +1530,31 @@ int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int 
   return MRM_OK;
 }
 
+int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double hg, double velocity, double x0,
+                           double t0, double bit_time, uint64_t pattern, int nbits) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  if (!(gap > 0 && z > 0 && bit_time > 0) || nbits < 1 || nbits > 64)
+    return set_err(&h->err, MRM_ERR_ARG, "head field needs gap, z, bit_time > 0 and 1 <= nbits <= 64");
+  LayerBufs& b = h->L[layer];
+  b.func = kFuncHead;
+  b.amp = 0.0;
+  b.dc = 0.0;
+  b.scale = 1.0;
+  b.hd_gap = gap;
+  b.hd_z = z;
+  b.hd_hg = hg;
+  b.hd_v = velocity;
+  b.hd_x0 = x0;
+  b.hd_t0 = t0;
+  b.hd_tbit = bit_time;
+  b.hd_bits = pattern;
+  b.hd_nbits = nbits;
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the row kernel's shared memory grows by the head table
+  return MRM_OK;
+}
+
 int mrm_gpu_set_thermal(mrm_gpu* h, int layer, int on, double temperature, uint64_t seed) {
   if (!h) return MRM_ERR_ARG;
   if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
@@ -2128,7 +2183,7 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e->st;
   const long long work = std::max<long long>(ntot, std::max(nrt, nct));
   // shared memory: FFT part plus grain staging where it fits
-  const size_t fft = (size_t)row_fft_smem<float>(h->lgpx, 1);
+  const size_t fft = row_fixed_smem<float>(h, 1);
   auto stage_cap = [&](int stage, int slot) {
     const long long hard = (long long)kMaxSmem - (long long)row_static_bytes(slot) - (long long)fft;
     return (int)(std::min<long long>(run_stage_bytes<float>(h, stage, rpt), std::max(0LL, hard)) & ~15LL);
@@ -2140,11 +2195,15 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   // kInit reads the descriptor and tasks before its dependency wait: a plain
   // launch, so it cannot overlap their writer; the rest chain with
   // programmatic serialization as in the engine
-  CK(launch_row<float>(0, kInit, false, RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false},
+  bool head = false;
+  for (int l = 0; l < nl; ++l) head = head || h->L[l].func == kFuncHead;
+  CK(launch_row<float>(0, kInit, false,
+                       RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false, head},
                        0, kFlagForce));
   CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt), true}, 0,
                        kFlagForce));
-  CK(launch_row<float>(0, kEval, false, RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_eval, cap_eval, true},
+  CK(launch_row<float>(0, kEval, false,
+                       RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_eval, cap_eval, true, head},
                        0, kFlagForce | kFlagStoreField));
   noalloc_unpack_kernel<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(shd, hdemag, ntot);
   CK(cudaGetLastError());

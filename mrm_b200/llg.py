@@ -67,6 +67,8 @@ class _RunMixin:
             else:
                 self.set_uniform_field(l, lay.hdir, lay.t_start, lay.t_end, lay.s_start, lay.s_end,
                                        lay.scale)
+            if getattr(lay, "head", None):
+                self.set_head_field(l, **lay.head)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
         if medium.m0 is not None:
             for l, m in enumerate(medium.m0):
@@ -111,6 +113,10 @@ class _RunMixin:
         self._check(_lib.load().mrm_gpu_set_field_function(self.h, layer, fptr(d), int(func), amp,
                                                            gamma, phase, param, duty, moddepth,
                                                            dc, scale))
+
+    def set_head_field(self, layer, gap, z, hg, velocity, x0, t0, bit_time, pattern, nbits):
+        self._check(_lib.load().mrm_gpu_set_head_field(self.h, layer, gap, z, hg, velocity, x0, t0,
+                                                       bit_time, int(pattern), int(nbits)))
 
     def set_thermal(self, layer, on, temperature, seed):
         self._check(_lib.load().mrm_gpu_set_thermal(self.h, layer, 1 if on else 0,

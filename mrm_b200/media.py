@@ -74,6 +74,10 @@ class Layer:
     duty: float = 0.0
     moddepth: float = 0.0
     dc: float = 0.0
+    # moving write head replacing the uniform field: dict(gap, z, hg, velocity,
+    # x0, t0, bit_time, pattern, nbits) in cm, Oe, s (include/mrm_gpu.h
+    # mrm_gpu_set_head_field)
+    head: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -251,3 +255,45 @@ def two_layer_medium(nx: int = 1024, ny: int = 256, *, pitch_nm: float = 7.0, se
     m0 = [np.tile([0.0, 0.0, 1.0], (n, 1)), np.tile([0.0, 0.0, 1.0], (n, 1))]
     return Medium(nx=nx, ny=ny, dx=dx, dy=dy, dz=[8e-7, 4e-7], il_space=[0.0, 0.0],
                   layers=[hard, soft], boundary=boundary, m0=m0)
+
+
+def prbs_pattern(nbits: int = 64, seed: int = 1) -> int:
+    """Seeded pseudo-random bit pattern: the PRBS7 sequence (x^7 + x^6 + 1
+    linear-feedback shift register) started from a seed-dependent non-zero
+    state; bit k of the result is the k-th bit written."""
+    state = (seed * 0x5B + 0x2D) & 0x7F or 1
+    out = 0
+    for k in range(nbits):
+        bit = ((state >> 6) ^ (state >> 5)) & 1
+        state = ((state << 1) | bit) & 0x7F
+        out |= (state & 1) << k
+    return out
+
+
+def karlqvist_deep_gap(peak_oe: float, gap_cm: float, z_cm: float) -> float:
+    """Deep-gap field whose Karlqvist h_x peak (under the gap centre) at
+    distance z equals peak_oe: h_x(0, z) = 2 Hg/pi atan(gap / (2 z))."""
+    return peak_oe * math.pi / (2.0 * math.atan(gap_cm / (2.0 * z_cm)))
+
+
+def head_write_medium(nx: int = 1024, ny: int = 256, *, seed: int = 1, prbs_seed: int = 1,
+                      temperature: float = 300.0, gap_nm: float = 25.0, fly_nm: float = 6.0,
+                      peak_oe: float = 12000.0, velocity_cm_s: float = 2000.0, bit_nm: float = 15.0,
+                      nbits: int = 64, boundary: int = 1) -> Medium:
+    """Two-layer recording write (the 1,024 x 256 x 2-layer workload): the
+    hard/soft bilayer of two_layer_medium written by a Karlqvist ring head
+    (gap 25 nm, 6 nm above the top layer, 12 kOe peak at the top surface)
+    moving down-track at 20 m/s, polarity from a seeded 64-bit PRBS at 15 nm
+    bit length (bit time = bit length / velocity).  The head enters at the
+    left edge of the grid at t = 0.  Layer 0 is the top layer."""
+    med = two_layer_medium(nx, ny, seed=seed, temperature=temperature, boundary=boundary)
+    gap, fly = gap_nm * 1e-7, fly_nm * 1e-7
+    hg = karlqvist_deep_gap(peak_oe, gap, fly)
+    pattern = prbs_pattern(nbits, prbs_seed)
+    depth = 0.0
+    for l, lay in enumerate(med.layers):
+        z = fly + depth + 0.5 * med.dz[l]
+        depth += med.dz[l] + med.il_space[l]
+        lay.head = dict(gap=gap, z=z, hg=hg, velocity=velocity_cm_s, x0=0.0, t0=0.0,
+                        bit_time=bit_nm * 1e-7 / velocity_cm_s, pattern=pattern, nbits=nbits)
+    return med

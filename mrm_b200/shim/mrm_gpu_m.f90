@@ -13,7 +13,8 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_thermal, gpu_set_state, gpu_get_state, gpu_get_field, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
   integer(C_INT), parameter, public :: MRM_PERIODIC = 0, MRM_OPEN = 1, MRM_FP32 = 0, MRM_FP64 = 1
@@ -92,6 +93,14 @@ module mrm_gpu_m
       integer(C_INT), value :: layer, func
       real(C_DOUBLE), intent(in) :: hdir(3)
       real(C_DOUBLE), value :: amp, gamma, phase, param, duty, moddepth, dc, scale
+    end function
+    integer(C_INT) function c_set_head_field(h, layer, gap, z, hg, velocity, x0, t0, bit_time, pattern, &
+        nbits) bind(C, name="mrm_gpu_set_head_field")
+      import :: C_INT, C_PTR, C_DOUBLE, C_INT64_T
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, nbits
+      real(C_DOUBLE), value :: gap, z, hg, velocity, x0, t0, bit_time
+      integer(C_INT64_T), value :: pattern
     end function
     integer(C_INT) function c_set_thermal(h, layer, on, temperature, seed) bind(C, name="mrm_gpu_set_thermal")
       import :: C_INT, C_PTR, C_DOUBLE, C_INT64_T
@@ -219,6 +228,17 @@ contains
     real(C_DOUBLE), intent(in) :: hdir(3), amp, gamma, phase, param, duty, moddepth, dc, scale
     ok_p = ok(c_set_field_function(h, int(layer - 1, C_INT), hdir, int(func, C_INT), amp, gamma, &
                                   phase, param, duty, moddepth, dc, scale))
+  end function
+
+  ! moving Karlqvist write head on `layer` (include/mrm_gpu.h mrm_gpu_set_head_field)
+  logical function gpu_set_head_field(h, layer, gap, z, hg, velocity, x0, t0, bit_time, pattern, nbits) &
+      result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer, nbits
+    real(C_DOUBLE), intent(in) :: gap, z, hg, velocity, x0, t0, bit_time
+    integer(C_INT64_T), intent(in) :: pattern
+    ok_p = ok(c_set_head_field(h, int(layer - 1, C_INT), gap, z, hg, velocity, x0, t0, bit_time, pattern, &
+                               int(nbits, C_INT)))
   end function
 
   logical function gpu_set_thermal(h, layer, on, temperature, seed) result(ok_p)

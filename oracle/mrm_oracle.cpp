@@ -459,6 +459,12 @@ struct Layer {
   double amp = 0, fgamma = 0, phase = 0, param = 0, duty = 0, moddepth = 0, dc = 0;
   double temperature = 0.0;
   bool thermal = false;
+  // moving write head (form 6; the config's head model, no reference counterpart):
+  // Karlqvist field, gap centre at hd_x0 + hd_v (t - hd_t0), polarity from hd_bits
+  bool head = false;
+  double hd_gap = 0, hd_z = 1, hd_hg = 0, hd_v = 0, hd_x0 = 0, hd_t0 = 0, hd_tbit = 1;
+  uint64_t hd_bits = 0;
+  int hd_nbits = 1;
   MT rng;
 };
 
@@ -608,18 +614,44 @@ static double ramp_scale(const Layer& Ly, double t) {
   return ((Ly.s_end - Ly.s_start) * u + Ly.s_start) * Ly.scale;
 }
 
+// Karlqvist field of a ring head at down-track offset u from the gap centre,
+// distance z below it, deep-gap field hg (polarity included)
+static void karlqvist(double u, double g, double z, double hg, double* hx, double* hz) {
+  const double a = u + 0.5 * g, b = u - 0.5 * g;
+  *hx = hg / M_PI * (std::atan(a / z) - std::atan(b / z));
+  *hz = hg / (2.0 * M_PI) * std::log((b * b + z * z) / (a * a + z * z));
+}
+
+static double head_polarity(const Layer& Ly, double t) {
+  long long k = (long long)std::floor((t - Ly.hd_t0) / Ly.hd_tbit);
+  const long long nb = Ly.hd_nbits > 0 ? Ly.hd_nbits : 1;
+  k %= nb;
+  if (k < 0) k += nb;
+  return ((Ly.hd_bits >> k) & 1ull) ? 1.0 : -1.0;
+}
+
 // get_field (field.f90:160-273) for the LLG path; energy per grain summed into *energy
 static void get_field(Sim* s, double t, int buf, double* energy) {
   compute_demag(s, buf);
   double e_tot = 0.0;
   for (int l = 0; l < s->nl; ++l) {
     Layer& Ly = s->L[l];
-    double sc = ramp_scale(Ly, t);
+    double sc = Ly.head ? 0.0 : ramp_scale(Ly, t);
     const double* m = Ly.m[buf].data();
+    const double pol = Ly.head ? head_polarity(Ly, t) : 0.0;
+    const double xh = Ly.hd_x0 + Ly.hd_v * (t - Ly.hd_t0);
     double el = 0.0;
 #pragma omp parallel for reduction(+ : el)
     for (int n = 0; n < Ly.N; ++n) {
       double ha[3] = {sc * Ly.hdir[0], sc * Ly.hdir[1], sc * Ly.hdir[2]};
+      if (Ly.head) {
+        // the grain's down-track position: centre of its (first) cell column
+        const double x = ((double)Ly.g2c_i[Ly.g2c_idx[n]] + 0.5) * s->dx;
+        double hx, hz;
+        karlqvist(x - xh, Ly.hd_gap, Ly.hd_z, pol * Ly.hd_hg, &hx, &hz);
+        ha[0] += hx;
+        ha[2] += hz;
+      }
       for (int a = 0; a < 3; ++a) Ly.happ[3 * n + a] = ha[a];
       const double* mn = m + 3 * n;
       const double* hd = &Ly.hdemag[3 * n];
@@ -1113,6 +1145,17 @@ int orc_set_field_function(void* h, int l, const double* dir, int func, double a
   Ly.func = func; Ly.amp = amp; Ly.fgamma = g; Ly.phase = phase; Ly.param = param;
   Ly.duty = std::max(0.0, std::min(1.0, duty)); Ly.moddepth = std::max(0.0, std::min(1.0, moddepth));
   Ly.dc = dc; Ly.scale = scale;
+  return 0;
+}
+
+int orc_set_head_field(void* h, int l, double gap, double z, double hg, double v, double x0, double t0,
+                       double tbit, uint64_t bits, int nbits) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl || !(gap > 0 && z > 0 && tbit > 0) || nbits < 1 || nbits > 64) return 1;
+  Layer& Ly = s->L[l];
+  Ly.head = true;
+  Ly.hd_gap = gap; Ly.hd_z = z; Ly.hd_hg = hg; Ly.hd_v = v; Ly.hd_x0 = x0; Ly.hd_t0 = t0;
+  Ly.hd_tbit = tbit; Ly.hd_bits = bits; Ly.hd_nbits = nbits;
   return 0;
 }
 

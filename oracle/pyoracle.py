@@ -52,6 +52,7 @@ def lib():
         L.orc_set_uniform_field.argtypes = [vp, i, P(d), d, d, d, d, d]
         L.orc_set_thermal.argtypes = [vp, i, i, d, i, C.c_longlong]
         L.orc_set_field_function.argtypes = [vp, i, P(d), i, d, d, d, d, d, d, d, d]
+        L.orc_set_head_field.argtypes = [vp, i, d, d, d, d, d, d, d, u64, i]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
         L.orc_get_field.argtypes = [vp, i, P(d)]
@@ -206,6 +207,11 @@ class OracleSim:
             else:
                 L.orc_set_uniform_field(self.h, l, _p(d), lay.t_start, lay.t_end, lay.s_start,
                                         lay.s_end, lay.scale)
+            hd = getattr(lay, "head", None)
+            if hd:
+                rc = L.orc_set_head_field(self.h, l, hd["gap"], hd["z"], hd["hg"], hd["velocity"], hd["x0"],
+                                          hd["t0"], hd["bit_time"], int(hd["pattern"]), int(hd["nbits"]))
+                assert rc == 0
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
         for l, lay in enumerate(medium.layers):
             for side, cpl in ((0, lay.uhx), (1, lay.lhx)):

@@ -158,3 +158,47 @@ def test_semi_implicit_thermal_two_layers_fp64(oracle, gpulib, llg_type):
         assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-8
     # the push preserves |m| without renormalisation (to rounding)
     assert np.abs(np.linalg.norm(gpu.get_state(0), axis=1) - 1.0).max() < 1e-12
+
+
+def _fast_head(med, velocity=4e5, bit_time=7e-11):
+    for lay in med.layers:
+        lay.head["velocity"] = velocity
+        lay.head["bit_time"] = bit_time
+    return med
+
+
+# FP32: grains switching under the moving head amplify rounding near their
+# switching field, so the per-component tolerance after 1,000 steps is 1e-3;
+# the written pattern (which grains reversed) must agree within 1 % of the grains.
+@pytest.mark.parametrize("precision,tol", [(FP64, 1e-9), (FP32, 1e-3)])
+def test_head_write_t0_trajectory(oracle, gpulib, precision, tol):
+    """Two-layer write by the moving Karlqvist head (PRBS polarity): the head
+    sweeps the 64-column grid and reverses grains under it; GPU against the
+    oracle, Heun, T = 0."""
+    med = _fast_head(media.head_write_medium(64, 16, temperature=0.0))
+    orc, gpu = _pair(oracle, med, precision)
+    for chunk in range(4):
+        so = orc.step(250, 1e-13)
+        sg = gpu.step(250, 1e-13)
+        for l in range(2):
+            assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < tol, (chunk, l)
+    assert np.allclose(sg["have_l"][:2], so["have_l"][:2], rtol=max(tol, 1e-9) * 50, atol=1e-6)
+    # the head wrote: part of the top layer was reversed, the same grains on both sides
+    assert (orc.get_state(0)[:, 2] < 0).mean() > 0.05
+    for l in range(2):
+        assert np.mean((gpu.get_state(l)[:, 2] < 0) != (orc.get_state(l)[:, 2] < 0)) <= 0.01
+
+
+@pytest.mark.parametrize("demag", [True, False])
+def test_head_write_thermal_fp64_same_stream(oracle, gpulib, demag):
+    med = _fast_head(media.head_write_medium(64, 16, temperature=300.0))
+    orc, gpu = _pair(oracle, med, FP64, seed=3, demag=demag)
+    orc.step(200, 1e-13)
+    gpu.step(200, 1e-13)
+    for l in range(2):
+        assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-8
+    # the evaluation stage reports the demag field alone and the total field with the head
+    orc.eval_field(2.1e-11)
+    for l in range(2):
+        assert np.abs(gpu.eval_field(2.1e-11, l) - orc.get_demag(l)).max() < 1e-6
+        assert np.abs(gpu.get_field(l) - orc.get_field(l)).max() < 1e-6
