@@ -220,6 +220,23 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """Largest value over the ranks (a timed region's duration: the job ends
+    with its slowest replica); the value itself on a single process."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, world: int, seconds: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank within `seconds` (the max over ranks)."""
+    return world * units_per_rank / seconds
+
+
 def launches_per_bench_step(heun: int, stats: bool = True) -> int:
     """Kernels per call of `heun` Heun steps: 4 per step, one advance per graph of
     <= 16 steps, one stats finalisation per call."""
@@ -270,10 +287,7 @@ def batched_leg(args, torch, local, rank, dist):
     torch.cuda.synchronize()
     clk = clocks.stop()
     dev_ms = sum(a.elapsed_time(c) for a, c in ev)
-    if dist:
-        tt = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms = float(tt.item())
+    dev_ms = max_over_ranks(dev_ms, dist, f"cuda:{local}")
     mh = np.array(mhs)
     hcs = [coercivity(hs, mh[:, i])[0] for i in range(len(runs))]
     hcs = [h for h in hcs if h is not None]
@@ -296,10 +310,7 @@ def batched_leg(args, torch, local, rank, dist):
             m_host[i][:] = r.get_state(0)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local}")
     h2d = sum(m.nbytes for m in m_host)
     d2h = sum(m.nbytes for m in m_host) + len(runs) * STATS_DTYPE.itemsize
 
@@ -464,8 +475,8 @@ def main():
     if rank != 0:
         return
     n, nb = B["n"], B["runs"]
-    value = world * nb * n * args.heun * args.steps / (B["dev_ms"] * 1e-3)
-    e2e_value = world * nb * n * args.heun * B["k_e2e"] / B["e2e_s"]
+    value = job_throughput(nb * n * args.heun * args.steps, world, B["dev_ms"] * 1e-3)
+    e2e_value = job_throughput(nb * n * args.heun * B["k_e2e"], world, B["e2e_s"])
     px, py = B["fft"]
     ab = {k: v * nb for k, v in algorithmic_bytes(SIDE, SIDE, px, py).items()}
     prof = B["prof"]
