@@ -57,10 +57,10 @@ RAMP_STEPS = 20000  # 2 ns at 0.1 ps
 WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
             "512x512 zero-padded FFT demag, Heun 0.1 ps")
 
-# DRAM traffic per launch of the dominant kernel (bytes per grain of the
-# launch, from the ncu capture summarised in profiles/; None: no capture of the
-# current kernel version)
-NCU_TRAFFIC_BYTES_PER_GRAIN = None
+# DRAM traffic per launch of each kernel in bytes per grain of the launch, for
+# the headline batch with its tuned shapes (ncu capture summarised in
+# profiles/batched_32x65536_launch_list.md)
+NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 139.07, "col": 69.20, "row_corr": 166.26}
 
 
 def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4) -> dict:
@@ -503,8 +503,10 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes": ab[dom], "avg_launch_ms": per_kernel[dom],
-                     "traffic": (NCU_TRAFFIC_BYTES_PER_GRAIN * nb * n
-                                 if NCU_TRAFFIC_BYTES_PER_GRAIN is not None else None),
+                     "traffic": (NCU_TRAFFIC_BYTES_PER_GRAIN[dom] * nb * n
+                                 if dom in NCU_TRAFFIC_BYTES_PER_GRAIN else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 32 x 65,536 "
+                                       "grains, row/column shapes 1/1, 2 columns per task",
                      "per_kernel_ms": per_kernel, "launches_per_heun_step": launches_per_heun,
                      "per_kernel_frac": {k: ab[k] / (v * 1e-3) / 1e9 / peak for k, v in per_kernel.items()},
                      "occupancy_blocks_per_sm": {"row": B["occupancy"][0], "col": B["occupancy"][1]},
