@@ -165,9 +165,10 @@ int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double h
                            double t0, double bit_time, uint64_t pattern, int nbits);
 
 /* Thermal (Brown) field of `layer` at `temperature` K (get_thermal,
- * field.f90:397-436).  The normals come from a counter-based Philox4x64-10
- * stream keyed by `seed` (statistical, not bitwise, equivalence with the
- * reference's MT19937 stream, random.f90:231-249). */
+ * field.f90:397-436).  The normals come from a counter-based Philox stream
+ * keyed by `seed` (Philox4x64-10 for MRM_FP64 handles, Philox4x32-10 for
+ * MRM_FP32; statistical, not bitwise, equivalence with the reference's
+ * MT19937 stream, random.f90:231-249). */
 int mrm_gpu_set_thermal(mrm_gpu* h, int layer, int on, double temperature, uint64_t seed);
 
 /* m(3,N) of `layer` (the active half m(1+in:3+in,:)) */
@@ -203,7 +204,8 @@ int mrm_gpu_stream(const mrm_gpu* h, void** stream);
  * row_shape / col_shape index the compiled row / column kernel shapes
  * (rows per block, threads, resident blocks; threads and resident blocks of
  * the column kernel) and cols_per_task > 0 fixes the spectral columns per
- * column task; a negative shape returns to the automatic choice.  Results do
+ * column task (rounded down to a power of two, at most 8: the width of the
+ * column tiles the row kernel writes the M spectrum in); a negative shape returns to the automatic choice.  Results do
  * not depend on the shape.  Automatic: with autotuning on (the default), the
  * first step after the set of runs changes times every compiled shape on the
  * runs themselves (their state is restored) and keeps the fastest, cached per

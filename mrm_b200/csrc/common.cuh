@@ -101,7 +101,9 @@ struct RunDev {
                            // (ny -> even), packed tensor row (py/2+1 -> multiple of 4)
   int tw_row, tw_col;      // offsets of this grid's twiddle blocks in the global table (fft.cuh)
   Cx<R>* spech;            // H^ half spectra, row-major [nl][3][ny][phs] (column kernel -> row kernel)
-  Cx<R>* specx;            // M^ half spectra, column-major [nl][3][px/2+1][nys] (row kernel -> column kernel)
+  int lgct;                // log2 of the column-tile width T (= columns per column task)
+  Cx<R>* specx;            // M^ half spectra in column tiles [nl*3][ntile][nys][T], ntile = ceil((px/2+1)/T)
+                           // (row kernel -> column kernel)
   const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][pyhs] reals,
                            // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];

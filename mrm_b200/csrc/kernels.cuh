@@ -692,27 +692,30 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
   Cx<R>* Y = block_fft_c<R, -1, NBMAX, BLOCK, LGMAX - 1>(W, scratch, lgM, nseq, twpass);
-  // X[k] = e - i w^k o (w = e^{-2 pi i / px}); a task's rows are adjacent in
-  // the column-major spectrum, so consecutive threads take consecutive rows
+  // X[k] = e - i w^k o (w = e^{-2 pi i / px}), stored in column tiles of T =
+  // 2^lgct columns (one column task), each tile row by row: consecutive threads
+  // take the T columns of a row, then the task's next rows, then the next tile
   const int lgr = nrows > 1 ? 32 - __clz(nrows - 1) : 0;
   const int rmask = (1 << lgr) - 1;
-  const int nys = rd.nys;
+  const int nys = rd.nys, lgct = rd.lgct, T = 1 << lgct, ntile = (ph + T - 1) >> lgct;
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) {
-    Cx<R>* dst = rd.specx + (size_t)(l * 3 + comp) * ph * nys + row0;
-    for (int t = threadIdx.x; t < (ph << lgr); t += BLOCK) {
-      const int row = t & rmask, k = t >> lgr;
-      if (row >= nrows) continue;
+    Cx<R>* dst = rd.specx + (size_t)(l * 3 + comp) * ntile * nys * T;
+    for (int t = threadIdx.x; t < (ntile << (lgct + lgr)); t += BLOCK) {
+      const int c = t & (T - 1), row = (t >> lgct) & rmask, tile = t >> (lgct + lgr);
+      const int k = (tile << lgct) + c;
+      if (row >= nrows || k >= ph) continue;
       const Cx<R>* Ys = Y + (row * 3 + comp) * cs;
       const Cx<R> yk = Ys[k & (M - 1)];
       const Cx<R> ymk = cconj(Ys[(M - k) & (M - 1)]);
       const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
       const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
       const Cx<R> wo = cmul(twpost[k], o);
-      if (!MRM_CHECK((long long)(l * 3 + comp) * ph * nys + (long long)k * nys + row0 + row <
-                         (long long)rd.nl * 3 * ph * nys, 300, k))
+      const long long at = (((long long)tile * nys + row0 + row) << lgct) + c;
+      if (!MRM_CHECK((long long)(l * 3 + comp) * ntile * nys * T + at < (long long)rd.nl * 3 * ntile * nys * T, 300,
+                     k))
         continue;
-      dst[(size_t)k * nys + row] = csub(e, cmul_i(wo, (R)1));
+      dst[at] = csub(e, cmul_i(wo, (R)1));
     }
   }
 }
@@ -727,6 +730,7 @@ constexpr int kTensSliceBytes = 48 * 1024;
 template <typename R>
 MRM_HD bool tens_slice_fits(int reals) { return (size_t)reals * sizeof(R) <= (size_t)kTensSliceBytes; }
 
+// nseq: sequences of a whole column tile (tile width x layers x 3)
 template <typename R>
 MRM_HD int col_fft_smem(int lgpy, int nseq) {
   return (col_tw_count(lgpy) + 2 * nseq * seq_stride(1 << lgpy)) * (int)sizeof(Cx<R>);
@@ -750,11 +754,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
   const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
   Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);
   const int ntw = col_tw_count(lgpy);
+  // buffers sized for a whole column tile (T = 2^lgct columns; a short last
+  // task still receives whole tiles)
+  const int lgct = rd.lgct, T = 1 << lgct, ntile = (ph + T - 1) >> lgct;
   Cx<R>* A = tws + ntw;
-  Cx<R>* B = A + nseq * cs;
+  Cx<R>* B = A + T * nl * 3 * cs;
   const int npair = nl * nl;
   const int tslice = nc * npair * 9 * pyhs;  // reals
-  R* Ts = reinterpret_cast<R*>(B + nseq * cs);
+  R* Ts = reinterpret_cast<R*>(B + T * nl * 3 * cs);
   // the slice is staged only where the launch's shared memory holds it (the
   // host sizes it for the largest task, which may not fit when a smaller last
   // task would)
@@ -798,11 +805,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
   pdl_wait();
   const bool run_it = (flags & kFlagForce) || rd.step + istep < rd.step_end;
   if (threadIdx.x == 0) {
+    // the task's tile of each of the 3 nl component planes: nys rows of T columns
     if (run_it)
-      for (int s = 0; s < nseq; ++s) {
-        const int c = s / (nl * 3), lc = s - c * nl * 3;
-        const long long off = ((long long)lc * ph + k0 + c) * nys;
-        copy(&bars[1], A + s * cs, rd.specx + off, off * cb, (long long)nl * 3 * ph * nys * cb, nys * (int)cb, 420);
+      for (int lc = 0; lc < nl * 3; ++lc) {
+        const long long off = ((long long)lc * ntile + (k0 >> lgct)) * nys * T;
+        copy(&bars[1], B + (size_t)lc * nys * T, rd.specx + off, off * cb, (long long)nl * 3 * ntile * nys * T * cb,
+             nys * T * (int)cb, 420);
       }
     mbar_arrive(&bars[1]);
   }
@@ -815,13 +823,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
   }
   if (!run_it) return;
 
-  // rows >= ny of the columns are the zero padding
-  if (ny < py) {
-    const int pad = py - ny;
-    for (int idx = threadIdx.x; idx < nseq * pad; idx += BLOCK) {
-      const int s = idx / pad, j = ny + (idx - s * pad);
-      A[s * cs + j] = Cx<R>{(R)0, (R)0};
-    }
+  // tiles -> one sequence per (column, layer, component); rows >= ny are the
+  // zero padding of the FFT grid
+  // (consecutive threads read consecutive tile entries)
+  for (int idx = threadIdx.x; idx < (nl * 3 * py) << lgct; idx += BLOCK) {
+    const int c = idx & (T - 1), j = (idx >> lgct) & (py - 1), lc = idx >> (lgct + lgpy);
+    if (c >= nc) continue;
+    A[(c * nl * 3 + lc) * cs + j] = j < ny ? B[((size_t)lc * nys + j) * T + c] : Cx<R>{(R)0, (R)0};
   }
   __syncthreads();
   Cx<R>* F = block_fft_c<R, -1, 0, BLOCK>(A, B, lgpy, nseq, tws);

@@ -85,6 +85,7 @@ struct mrm_gpu {
   bool spec_valid = false;
   bool has_stats = false;
   int slot = -1;
+  int lgct = 0;  // log2 of the column-tile width (= columns per column task)
   int row_task0 = 0, nrow_tasks = 0;
   std::string err;
 };
@@ -264,9 +265,19 @@ int default_cols(const mrm_gpu* r) {
   const int ph = r->px / 2 + 1;
   return std::max(1, std::min(ph, 256 * 16 / (3 * r->nl * r->py)));
 }
-int cols_per_task(const Engine* e, const mrm_gpu* r) {
+// columns per column task: also the width of the column tiles of the M^
+// spectrum, so a power of two up to kMaxColTile
+constexpr int kMaxColTile = 8;
+int col_tile(int want) {
+  int t = 1;
+  while (2 * t <= std::min(want, kMaxColTile)) t *= 2;
+  return t;
+}
+int cols_per_task(const Engine* e, const mrm_gpu* r) { return col_tile(e->cpt > 0 ? e->cpt : default_cols(r)); }
+// complex values of the M^ spectrum of a run (column tiles of any width up to kMaxColTile)
+size_t specx_count(const mrm_gpu* r) {
   const int ph = r->px / 2 + 1;
-  return std::max(1, std::min(ph, e->cpt > 0 ? e->cpt : default_cols(r)));
+  return (size_t)r->nl * 3 * ((ph + kMaxColTile - 1) / kMaxColTile * kMaxColTile) * spec_col_stride(r->g.ny);
 }
 int rows_per_task(const mrm_gpu* r, int rpb) { return std::max(1, std::min(rpb, r->g.ny)); }
 
@@ -382,6 +393,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
   d.nrow_tasks = r->nrow_tasks;
   d.phs = spec_row_stride(r->px);
   d.nys = spec_col_stride(r->g.ny);
+  d.lgct = r->lgct;
   d.pyhs = tens_row_stride(r->py);
   d.tw_row = row_tw_off(r->lgpx);
   d.tw_col = col_tw_off(r->lgpy);
@@ -549,6 +561,7 @@ int build_tables(Engine* e) {
     r->nrow_tasks = (int)stt.size() - r->row_task0;
     if (r->demag && r->tensor_ready) {
       const int cpt = cols_per_task(e, r), ph = r->px / 2 + 1;
+      r->lgct = ilog2(cpt);
       for (int k = 0; k < ph; k += cpt) ct.push_back(make_int4((int)i, k, std::min(cpt, ph - k), 0));
     }
   }
@@ -947,10 +960,9 @@ int check_device_error(Engine* e) {
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
-  const int ph = r->px / 2 + 1;
   int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * 2 * re);
   if (rc) return rc;
-  rc = dmalloc(errp, &r->specx, (size_t)r->nl * 3 * ph * spec_col_stride(r->g.ny) * 2 * re);
+  rc = dmalloc(errp, &r->specx, specx_count(r) * 2 * re);
   if (rc) return rc;
   rc = dmalloc(errp, &r->tens, tensor_bytes(r));
   if (rc) return rc;
@@ -989,7 +1001,8 @@ int64_t footprint(const mrm_geom& g) {
   const size_t re = g.precision == MRM_FP64 ? 8 : 4;
   const int64_t n = (int64_t)g.nx * g.ny, nl = g.n_lay;
   const int64_t ph = px / 2 + 1;
-  int64_t b = nl * 3 * g.ny * spec_row_stride(px) * 2 * re + nl * 3 * ph * spec_col_stride(g.ny) * 2 * re;
+  const int64_t ph8 = (ph + kMaxColTile - 1) / kMaxColTile * kMaxColTile;  // whole column tiles
+  int64_t b = nl * 3 * g.ny * spec_row_stride(px) * 2 * re + nl * 3 * ph8 * spec_col_stride(g.ny) * 2 * re;
   b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * tens_row_stride(py) * 4;
   b += nl * n * (8 * 4 * re + 4 * 8);
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
@@ -2056,7 +2069,7 @@ NoAllocLayout noalloc_layout(const mrm_gpu* r, int nrt, int nct) {
     off += align256(bytes);
     return at;
   };
-  const size_t n = (size_t)r->g.nx * r->g.ny, ph = r->px / 2 + 1;
+  const size_t n = (size_t)r->g.nx * r->g.ny;
   const size_t grains = (size_t)r->nl * n * sizeof(V4<float>);
   o.desc = take(sizeof(RunDev<float>));
   o.rtask = take(sizeof(Task) * nrt);
@@ -2064,7 +2077,7 @@ NoAllocLayout noalloc_layout(const mrm_gpu* r, int nrt, int nct) {
   o.m = take(grains);
   o.hd = take(grains);
   o.hf = take(grains);
-  o.specx = take((size_t)r->nl * 3 * ph * spec_col_stride(r->g.ny) * sizeof(Cx<float>));
+  o.specx = take(specx_count(r) * sizeof(Cx<float>));
   o.spech = take((size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * sizeof(Cx<float>));
   o.total = off;
   return o;
@@ -2143,7 +2156,7 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
   const int nl = h->nl, ny = h->g.ny, ph = h->px / 2 + 1;
   const int rpt = 1, nrt = nl * ny;  // one row per task (row shape 0)
-  const int cpt = std::max(1, std::min(ph, default_cols(h))), nct = (ph + cpt - 1) / cpt;
+  const int cpt = col_tile(default_cols(h)), nct = (ph + cpt - 1) / cpt;
   const NoAllocLayout lay = noalloc_layout(h, nrt, nct);
   if (lay.total > kNoAllocBytes)
     return set_err(errp, MRM_ERR_UNSUPPORTED,
@@ -2167,6 +2180,7 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   d.demag = 1;
   d.row_task0 = 0;
   d.nrow_tasks = nrt;
+  d.lgct = ilog2(cpt);
   d.specx = reinterpret_cast<Cx<float>*>(base + lay.specx);
   d.spech = reinterpret_cast<Cx<float>*>(base + lay.spech);
   V4<float>* sm = reinterpret_cast<V4<float>*>(base + lay.m);

@@ -1,10 +1,14 @@
 // philox.cuh -- counter-based thermal-noise stream.
 //
-// Philox4x64-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
-// easy as 1, 2, 3", SC'11) with the Box-Muller transform.  Counter =
-// (grain, step, layer, 0), key = (seed, 0x6d726d): the predictor and the
-// corrector of one Heun step regenerate the same three normals instead of
-// storing them (the reference reuses hthm, src/llg.f90:1262-1266).
+// Philox (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1,
+// 2, 3", SC'11) with the Box-Muller transform, one draw of three normals per
+// grain, step and layer (the predictor stores them for the corrector, as the
+// reference reuses hthm, src/llg.f90:1262-1266).
+//  * FP64 runs: Philox4x64-10, counter (grain, step, layer, 0), key
+//    (seed, 0x6d726d), 53-bit uniforms;
+//  * FP32 runs: Philox4x32-10, counter (grain, step low, step high, layer),
+//    key (seed low, seed high ^ 0x6d726d), 24-bit uniforms (the 64-bit
+//    multiplies of the 4x64 form were a sixth of the predictor's time).
 #pragma once
 #include "common.cuh"
 
@@ -19,6 +23,24 @@ MRM_D void philox4x64_10(unsigned long long c[4], unsigned long long k0, unsigne
     unsigned long long hi1 = __umul64hi(M1, c[2]), lo1 = M1 * c[2];
     unsigned long long n0 = hi1 ^ c[1] ^ k0;
     unsigned long long n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += W0;
+    k1 += W1;
+  }
+}
+
+MRM_D void philox4x32_10(unsigned int c[4], unsigned int k0, unsigned int k1) {
+  const unsigned int M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const unsigned int W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned int hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    const unsigned int hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    const unsigned int n0 = hi1 ^ c[1] ^ k0;
+    const unsigned int n2 = hi0 ^ c[3] ^ k1;
     c[0] = n0;
     c[1] = lo1;
     c[2] = n2;
@@ -49,13 +71,13 @@ MRM_D void thermal_normals(unsigned long long seed, unsigned long long layer,
 
 MRM_D void thermal_normals(unsigned long long seed, unsigned long long layer,
                            unsigned long long step, unsigned long long grain, float n[3]) {
-  unsigned long long c[4] = {grain, step, layer, 0ull};
-  philox4x64_10(c, seed, 0x6d726dull);
+  unsigned int c[4] = {(unsigned int)grain, (unsigned int)step, (unsigned int)(step >> 32), (unsigned int)layer};
+  philox4x32_10(c, (unsigned int)seed, (unsigned int)(seed >> 32) ^ 0x6d726du);
   const float s24 = 1.0f / 16777216.0f;
-  float u0 = ((float)(unsigned)(c[0] >> 40) + 0.5f) * s24;
-  float u1 = ((float)(unsigned)(c[1] >> 40) + 0.5f) * s24;
-  float u2 = ((float)(unsigned)(c[2] >> 40) + 0.5f) * s24;
-  float u3 = ((float)(unsigned)(c[3] >> 40) + 0.5f) * s24;
+  float u0 = ((float)(c[0] >> 8) + 0.5f) * s24;
+  float u1 = ((float)(c[1] >> 8) + 0.5f) * s24;
+  float u2 = ((float)(c[2] >> 8) + 0.5f) * s24;
+  float u3 = ((float)(c[3] >> 8) + 0.5f) * s24;
   float ra = sqrtf(-2.0f * logf(u0));
   float rb = sqrtf(-2.0f * logf(u2));
   float s, co;
