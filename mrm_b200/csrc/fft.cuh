@@ -199,6 +199,124 @@ MRM_D Cx<R>* block_fft_c(Cx<R>* a, Cx<R>* b, int lgn, int nb, const Cx<R>* __res
   }
 }
 
+// ---------------- in-place form (column kernel) ----------------
+//
+// Cooley-Tukey passes that overwrite their own inputs, so one buffer holds a
+// transform.  The forward transform decimates in frequency (butterfly, then
+// twiddles) from natural order to the mixed-radix digit-reversed order of
+// ip_freq(); the inverse decimates in time (twiddles, then butterfly) from that
+// order back to natural order, so a pointwise product between the two needs no
+// reordering.  The passes are the Stockham plan's (same radices, same tables):
+// pass (LGNS, LGR) combines the elements blk*L + j0 + m*S (S = 2^LGNS,
+// L = S*2^LGR, j0 < S, m < 2^LGR) with the twiddles e^{-2 pi i j0 m / L}, table
+// entry (m-1)*S + j0; the forward transform runs the passes from the largest S
+// down, the inverse from S = 1 up.  Elements are read and written through the
+// caller's functors ld(h, c, j) / st(h, c, j, v) (h: sequence group, c: column
+// within a tile of 2^lgT columns, j: element), so the first forward pass can
+// read global memory and the last inverse pass write it.  Consecutive threads
+// take consecutive columns c, then consecutive butterflies.
+
+// S of the pass the forward transform of length 2^lgn starts with (its radix takes the remaining bits)
+MRM_HD constexpr int ip_top(int lgn) { return 3 * ((lgn - 1) / 3); }
+
+// frequency held at position p after the in-place forward transform of length 2^lgn
+MRM_HD constexpr int ip_freq(int p, int lgn) {
+  int k = 0, shift = 0, lgns = ip_top(lgn), lgr = lgn - lgns;
+  while (true) {
+    k |= ((p >> lgns) & ((1 << lgr) - 1)) << shift;
+    shift += lgr;
+    if (lgns == 0) break;
+    lgns -= 3;
+    lgr = 3;
+  }
+  return k;
+}
+
+// offset of the pass with sub-length 2^lgns_at in the pass tables of length 2^lgn
+MRM_HD constexpr int pass_tw_off(int lgn, int lgns_at) {
+  int total = 0, lgns = 0;
+  while (lgns < lgns_at) {
+    const int lgr = pass_lgr(lgn, lgns);
+    if (lgns > 0) total += ((1 << lgr) - 1) << lgns;
+    lgns += lgr;
+  }
+  return total;
+}
+
+template <typename R, int S, int RADIX>
+MRM_D void dft_r(Cx<R>* v) {
+  if constexpr (RADIX == 8) dft8<R, S>(v);
+  else if constexpr (RADIX == 4) dft4<R, S>(v[0], v[1], v[2], v[3]);
+  else dft2<R, S>(v);
+}
+
+// One in-place pass over nh sequence groups of 2^lgT columns (columns c >= nc skipped).
+template <typename R, int LGN, int LGNS, bool INV, int BLOCK, class LD, class ST>
+MRM_D void ip_pass(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
+  constexpr int LGR = pass_lgr(LGN, LGNS);
+  constexpr int RADIX = 1 << LGR, NS = 1 << LGNS, LGB = LGN - LGR;
+  constexpr int OFF = pass_tw_off(LGN, LGNS);
+  const int total = nh << (LGB + lgT);
+  const int tmask = (1 << lgT) - 1;
+  for (int q = threadIdx.x; q < total; q += BLOCK) {
+    const int c = q & tmask;
+    if (c >= nc) continue;
+    const int bf = (q >> lgT) & ((1 << LGB) - 1), h = q >> (LGB + lgT);
+    const int j0 = bf & (NS - 1), base = ((bf >> LGNS) << (LGNS + LGR)) + j0;
+    Cx<R> v[RADIX];
+#pragma unroll
+    for (int m = 0; m < RADIX; ++m) v[m] = ld(h, c, base + m * NS);
+    if constexpr (INV && LGNS > 0) {
+#pragma unroll
+      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], cconj(twp[OFF + (m - 1) * NS + j0]));
+    }
+    dft_r<R, INV ? 1 : -1, RADIX>(v);
+    if constexpr (!INV && LGNS > 0) {
+#pragma unroll
+      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], twp[OFF + (m - 1) * NS + j0]);
+    }
+#pragma unroll
+    for (int m = 0; m < RADIX; ++m) st(h, c, base + m * NS, v[m]);
+  }
+}
+
+// forward passes LGNS, LGNS-3, ..., 0 through ld/st, each followed by __syncthreads
+template <typename R, int LGN, int LGNS, int BLOCK, class LD, class ST>
+MRM_D void ip_fwd_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
+  ip_pass<R, LGN, LGNS, false, BLOCK>(lgT, nc, nh, twp, ld, st);
+  __syncthreads();
+  if constexpr (LGNS >= 3) ip_fwd_from<R, LGN, LGNS - 3, BLOCK>(lgT, nc, nh, twp, ld, st);
+}
+// inverse passes LGNS, LGNS+3, ..., top; the top one stores through st_last (no barrier after it)
+template <typename R, int LGN, int LGNS, int BLOCK, class LD, class ST, class STL>
+MRM_D void ip_inv_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
+  if constexpr (LGNS == ip_top(LGN)) {
+    ip_pass<R, LGN, LGNS, true, BLOCK>(lgT, nc, nh, twp, ld, st_last);
+  } else {
+    ip_pass<R, LGN, LGNS, true, BLOCK>(lgT, nc, nh, twp, ld, st);
+    __syncthreads();
+    ip_inv_from<R, LGN, LGNS + 3, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+  }
+}
+
+// Forward transform of length 2^LGN: the first pass reads through ld0, the
+// rest through ld; every pass writes through st; ends with __syncthreads.
+// The caller must __syncthreads() before the call if ld0 reads shared memory.
+template <typename R, int LGN, int BLOCK, class LD0, class LD, class ST>
+MRM_D void ip_fft_fwd(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD0& ld0, LD& ld, ST& st) {
+  constexpr int TOP = ip_top(LGN);
+  ip_pass<R, LGN, TOP, false, BLOCK>(lgT, nc, nh, twp, ld0, st);
+  __syncthreads();
+  if constexpr (TOP >= 3) ip_fwd_from<R, LGN, TOP - 3, BLOCK>(lgT, nc, nh, twp, ld, st);
+}
+// Inverse transform of length 2^LGN (unnormalised) from digit-reversed order:
+// every pass reads through ld, the last writes through st_last and the others
+// through st.  The caller must __syncthreads() before the call.
+template <typename R, int LGN, int BLOCK, class LD, class ST, class STL>
+MRM_D void ip_fft_inv(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
+  ip_inv_from<R, LGN, 0, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+}
+
 // ---------------- run-time form (tensor FFT) ----------------
 
 MRM_HD int pad_stride(int n) { return n + (n >> 4) + 1; }

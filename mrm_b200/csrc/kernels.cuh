@@ -724,16 +724,153 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 // half-spectra, H^_a = sum_b N^_ab M^_b, inverse FFT, written back row-major.
 // PACKED: tensor stored as one real per (k, 0<=ky<=py/2) and component (the
 // parity of each component restores the rest); otherwise the full complex
-// tensor spectrum [k][pair][9][py] is used (FP64 runs).  The columns and the
-// task's packed tensor slice arrive by bulk copies.
+// tensor spectrum [k][pair][9][py] is used (FP64 runs).
+//
+// A task is one column tile (T = 2^lgct columns; a short last tile has fewer).
+// Its 3*nl planes live in one shared buffer, transformed in place: the forward
+// pass reads the M^ tile straight from global memory (rows >= ny are the zero
+// padding, never loaded), the product runs in the transforms' digit-reversed
+// order, and the last inverse pass writes rows < ny straight to H^.  Element j
+// of column c in plane p sits at p*col_plane(py, lgct) + ((j + j/8) << lgct) + c:
+// one pad row every 8 rows keeps the 8-element butterflies of the last forward
+// (and first inverse) pass on distinct banks.
 constexpr int kTensSliceBytes = 48 * 1024;
 template <typename R>
 MRM_HD bool tens_slice_fits(int reals) { return (size_t)reals * sizeof(R) <= (size_t)kTensSliceBytes; }
 
-// nseq: sequences of a whole column tile (tile width x layers x 3)
+MRM_HD constexpr int col_plane(int py, int lgct) { return (py + (py >> 3)) << lgct; }
+// complex values of one column buffer (even: what follows stays 16-byte aligned)
+MRM_HD constexpr int col_buf_count(int py, int lgct, int nplane) { return even_up(nplane * col_plane(py, lgct)); }
+// twiddles and buffers: one buffer up to two layers (6 planes), two beyond
 template <typename R>
-MRM_HD int col_fft_smem(int lgpy, int nseq) {
-  return (col_tw_count(lgpy) + 2 * nseq * seq_stride(1 << lgpy)) * (int)sizeof(Cx<R>);
+MRM_HD int col_fft_smem(int lgpy, int lgct, int nplane) {
+  return (col_tw_count(lgpy) + (nplane > 6 ? 2 : 1) * col_buf_count(1 << lgpy, lgct, nplane)) * (int)sizeof(Cx<R>);
+}
+
+// H^ = N^ M^ at every position of the digit-reversed column buffer: in place
+// for NLC = 1, 2 layers (a thread holds a position's 3*NLC inputs), otherwise
+// (NLC = 0, nl layers) from A into the second buffer O.
+template <typename R, bool PACKED, int NLC, int BLOCK>
+MRM_D void col_product(const RunDev<R>& rd, Cx<R>* A, Cx<R>* O, const R* Ts, bool tsm, int k0, int nc, int* err) {
+  const int nl = NLC > 0 ? NLC : rd.nl;
+  const int py = rd.py, lgpy = rd.lgpy, pyhs = rd.pyhs, lgct = rd.lgct, T = 1 << lgct;
+  const int plane = col_plane(py, lgct), npair = nl * nl;
+  const int ph = (rd.px >> 1) + 1;
+  const long long tens_len = PACKED ? (long long)ph * npair * 9 * pyhs * (long long)sizeof(R)
+                                    : (long long)ph * npair * 9 * py * (long long)sizeof(Cx<R>);
+  (void)tens_len;
+  (void)err;
+  // 3 outputs of layer ko at one position from the inputs of every layer
+  auto mac = [&](int c, int ky, int ko, const Cx<R>* x, int xstride, Cx<R> h[3]) {
+    h[0] = h[1] = h[2] = Cx<R>{(R)0, (R)0};
+    for (int ks = 0; ks < nl; ++ks) {
+      Cx<R> xm[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) xm[b] = x[(size_t)(ks * 3 + b) * xstride];
+      if constexpr (PACKED) {
+        const bool upper = ky > (py >> 1);
+        const int kyh = upper ? py - ky : ky;
+        const size_t off = ((size_t)c * npair + ks * nl + ko) * 9 * pyhs;
+        const R* Tp = tsm ? Ts + off : rd.tens + (size_t)k0 * npair * 9 * pyhs + off;
+        const bool tok = MRM_CHECK(
+            tsm || ((long long)k0 * npair * 9 * pyhs + (long long)off + 8 * pyhs + kyh) * (long long)sizeof(R) <
+                       tens_len,
+            430, kyh);
+        R tv[9];
+#pragma unroll
+        for (int cc = 0; cc < 9; ++cc) tv[cc] = tok ? Tp[cc * pyhs + kyh] : (R)0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const int cc = 3 * a + b;
+            R v = tv[cc];
+            if (((kOddMask >> cc) & 1) && upper) v = -v;
+            if ((kImagMask >> cc) & 1) h[a] = cadd(h[a], cmul_i(cscale(xm[b], v), (R)1));
+            else h[a] = cadd(h[a], cscale(xm[b], v));
+          }
+      } else {
+        const Cx<R>* Tc = reinterpret_cast<const Cx<R>*>(rd.tens) + ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * py;
+        Cx<R> tv[9];
+#pragma unroll
+        for (int cc = 0; cc < 9; ++cc) tv[cc] = Tc[cc * py + ky];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) h[a] = cadd(h[a], cmul(tv[3 * a + b], xm[b]));
+      }
+    }
+  };
+  if constexpr (NLC > 0) {
+    for (int idx = threadIdx.x; idx < (py << lgct); idx += BLOCK) {
+      const int c = idx & (T - 1), p = idx >> lgct;
+      if (c >= nc) continue;
+      const int ky = ip_freq(p, lgpy);
+      const int at = ((p + (p >> 3)) << lgct) + c;
+      Cx<R> xin[3 * NLC];
+#pragma unroll
+      for (int i = 0; i < 3 * NLC; ++i) xin[i] = A[(size_t)i * plane + at];
+      Cx<R> h[NLC][3];
+#pragma unroll
+      for (int ko = 0; ko < NLC; ++ko) mac(c, ky, ko, xin, 1, h[ko]);
+#pragma unroll
+      for (int ko = 0; ko < NLC; ++ko)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) A[(size_t)(ko * 3 + a) * plane + at] = h[ko][a];
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < (nl * py) << lgct; idx += BLOCK) {
+      const int c = idx & (T - 1), p = (idx >> lgct) & (py - 1), ko = idx >> (lgct + lgpy);
+      if (c >= nc) continue;
+      const int ky = ip_freq(p, lgpy);
+      const int at = ((p + (p >> 3)) << lgct) + c;
+      Cx<R> h[3];
+      mac(c, ky, ko, A + at, plane, h);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) O[(size_t)(ko * 3 + a) * plane + at] = h[a];
+    }
+  }
+}
+
+template <typename R, int LGN, bool PACKED, int BLOCK>
+MRM_D void col_transform(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const R* Ts, bool tsm, int k0, int nc,
+                         int* err) {
+  const int nl = rd.nl, ny = rd.ny, nys = rd.nys, phs = rd.phs, lgct = rd.lgct;
+  const int ph = (rd.px >> 1) + 1, ntile = (ph + (1 << lgct) - 1) >> lgct;
+  const int plane = col_plane(1 << LGN, lgct), nplane = nl * 3;
+  (void)err;
+  // the task's tile of M^: plane lc at ((lc*ntile + tile)*nys + j)*T + c
+  const Cx<R>* src = rd.specx + ((size_t)(k0 >> lgct) * nys << lgct);
+  const size_t src_plane = (size_t)ntile * nys << lgct;
+  auto ld_g = [&](int lc, int c, int j) -> Cx<R> {
+    if (j >= ny) return Cx<R>{(R)0, (R)0};
+    MRM_CHECK((long long)(k0 >> lgct) * nys * (1 << lgct) + (long long)lc * src_plane + ((long long)j << lgct) + c <
+                  (long long)nplane * src_plane,
+              420, j);
+    return src[lc * src_plane + ((size_t)j << lgct) + c];
+  };
+  auto ld_s = [&](int lc, int c, int j) -> Cx<R> { return A[lc * plane + ((j + (j >> 3)) << lgct) + c]; };
+  auto st_s = [&](int lc, int c, int j, Cx<R> v) { A[lc * plane + ((j + (j >> 3)) << lgct) + c] = v; };
+  auto st_g = [&](int lc, int c, int j, Cx<R> v) {
+    if (j >= ny) return;
+    if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nplane * ny * phs, 440, j)) return;
+    rd.spech[((size_t)lc * ny + j) * phs + k0 + c] = v;
+  };
+  ip_fft_fwd<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_g, ld_s, st_s);
+  if (nl <= 2) {
+    if (nl == 1) col_product<R, PACKED, 1, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
+    else col_product<R, PACKED, 2, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
+    __syncthreads();
+    ip_fft_inv<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_s, st_s, st_g);
+  } else {
+    // three or more layers: the product goes to the second buffer
+    Cx<R>* O = A + col_buf_count(1 << LGN, lgct, nplane);
+    col_product<R, PACKED, 0, BLOCK>(rd, A, O, Ts, tsm, k0, nc, err);
+    __syncthreads();
+    auto ld_o = [&](int lc, int c, int j) -> Cx<R> { return O[lc * plane + ((j + (j >> 3)) << lgct) + c]; };
+    auto st_o = [&](int lc, int c, int j, Cx<R> v) { O[lc * plane + ((j + (j >> 3)) << lgct) + c] = v; };
+    ip_fft_inv<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_o, st_o, st_g);
+  }
 }
 
 template <typename R, bool PACKED, int BLOCK, int MINB>
@@ -742,36 +879,31 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
                                                           const Cx<R>* __restrict__ twg, int istep,
                                                           int flags, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint64_t bars[2];
+  __shared__ uint64_t bars[1];
   pdl_launch_dependents();
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
   if (!rd.active || !rd.demag) return;
   const int k0 = tk.y, nc = tk.z;
-  const int nl = rd.nl, ny = rd.ny, py = rd.py, lgpy = rd.lgpy;
-  const int ph = (rd.px >> 1) + 1, pyh = (py >> 1) + 1, pyhs = rd.pyhs, nys = rd.nys, phs = rd.phs;
-  const int cs = seq_stride(py);
-  const int nseq = nc * nl * 3;  // s = (c*nl + layer)*3 + comp
+  const int nl = rd.nl, py = rd.py, lgpy = rd.lgpy, lgct = rd.lgct;
+  const int ph = (rd.px >> 1) + 1, pyhs = rd.pyhs;
   Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);
   const int ntw = col_tw_count(lgpy);
-  // buffers sized for a whole column tile (T = 2^lgct columns; a short last
-  // task still receives whole tiles)
-  const int lgct = rd.lgct, T = 1 << lgct, ntile = (ph + T - 1) >> lgct;
   Cx<R>* A = tws + ntw;
-  Cx<R>* B = A + T * nl * 3 * cs;
   const int npair = nl * nl;
   const int tslice = nc * npair * 9 * pyhs;  // reals
-  R* Ts = reinterpret_cast<R*>(B + T * nl * 3 * cs);
+  R* Ts = reinterpret_cast<R*>(A + (nl > 2 ? 2 : 1) * col_buf_count(py, lgct, nl * 3));
   // the slice is staged only where the launch's shared memory holds it (the
-  // host sizes it for the largest task, which may not fit when a smaller last
-  // task would)
+  // host leaves it out where it would cost resident blocks, and a smaller last
+  // task may fit where the largest does not)
   const bool tsm = PACKED && tens_slice_fits<R>(tslice) &&
                    (long long)(reinterpret_cast<unsigned char*>(Ts) - smem_raw) + (long long)tslice * sizeof(R) <=
                        (long long)dynamic_smem_bytes();
+  MRM_CHECK(k0 >= 0 && nc >= 1 && k0 + nc <= ph && (k0 & ((1 << lgct) - 1)) == 0 && nc <= (1 << lgct), 500, k0);
+  MRM_CHECK((long long)col_fft_smem<R>(lgpy, lgct, nl * 3) <= (long long)dynamic_smem_bytes(), 501, lgpy);
 
   if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -791,107 +923,38 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
     bulk_copy(bar, dst, src, (uint32_t)bytes);
   };
   const long long cb = (long long)sizeof(Cx<R>);
-  const long long tens_len = PACKED ? (long long)ph * npair * 9 * pyhs * (long long)sizeof(R)
-                                    : (long long)ph * npair * 9 * py * cb;
-  MRM_CHECK(k0 >= 0 && nc >= 1 && k0 + nc <= ph, 500, k0);
   if (threadIdx.x == 0) {
     copy(&bars[0], tws, twg + rd.tw_col, rd.tw_col * cb, (long long)tw_table_size() * cb, ntw * (int)cb, 400);
     if (tsm) {
       const long long off = (long long)k0 * npair * 9 * pyhs;
-      copy(&bars[0], Ts, rd.tens + off, off * (long long)sizeof(R), tens_len, tslice * (int)sizeof(R), 410);
+      copy(&bars[0], Ts, rd.tens + off, off * (long long)sizeof(R), (long long)ph * npair * 9 * pyhs * sizeof(R),
+           tslice * (int)sizeof(R), 410);
     }
     mbar_arrive(&bars[0]);
   }
   pdl_wait();
   const bool run_it = (flags & kFlagForce) || rd.step + istep < rd.step_end;
-  if (threadIdx.x == 0) {
-    // the task's tile of each of the 3 nl component planes: nys rows of T columns
-    if (run_it)
-      for (int lc = 0; lc < nl * 3; ++lc) {
-        const long long off = ((long long)lc * ntile + (k0 >> lgct)) * nys * T;
-        copy(&bars[1], B + (size_t)lc * nys * T, rd.specx + off, off * cb, (long long)nl * 3 * ntile * nys * T * cb,
-             nys * T * (int)cb, 420);
-      }
-    mbar_arrive(&bars[1]);
-  }
-  const bool ok = mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0);
+  const bool ok = mbar_wait(&bars[0], 0);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) atomicOr(err, kErrBarrierTimeout);
     mbar_wait(&bars[0], 0);
-    mbar_wait(&bars[1], 0);
     return;
   }
   if (!run_it) return;
 
-  // tiles -> one sequence per (column, layer, component); rows >= ny are the
-  // zero padding of the FFT grid
-  // (consecutive threads read consecutive tile entries)
-  for (int idx = threadIdx.x; idx < (nl * 3 * py) << lgct; idx += BLOCK) {
-    const int c = idx & (T - 1), j = (idx >> lgct) & (py - 1), lc = idx >> (lgct + lgpy);
-    if (c >= nc) continue;
-    A[(c * nl * 3 + lc) * cs + j] = j < ny ? B[((size_t)lc * nys + j) * T + c] : Cx<R>{(R)0, (R)0};
-  }
-  __syncthreads();
-  Cx<R>* F = block_fft_c<R, -1, 0, BLOCK>(A, B, lgpy, nseq, tws);
-  Cx<R>* G = (F == A) ? B : A;
-
-  // H^_a(k, ky) = sum_ks sum_b N^_ab(ko,ks)(k, ky) M^_b(ks)(k, ky)
-  for (int idx = threadIdx.x; idx < nc * py; idx += BLOCK) {
-    const int c = idx >> lgpy, ky = idx & (py - 1);
-    for (int ko = 0; ko < nl; ++ko) {
-      Cx<R> h[3] = {{0, 0}, {0, 0}, {0, 0}};
-      for (int ks = 0; ks < nl; ++ks) {
-        Cx<R> xm[3];
-#pragma unroll
-        for (int b = 0; b < 3; ++b) xm[b] = F[((c * nl + ks) * 3 + b) * cs + ky];
-        if constexpr (PACKED) {
-          const bool upper = ky > (py >> 1);
-          const int kyh = upper ? py - ky : ky;
-          const size_t off = ((size_t)c * npair + ks * nl + ko) * 9 * pyhs;
-          const R* Tp = tsm ? Ts + off : rd.tens + (size_t)k0 * npair * 9 * pyhs + off;
-          R tv[9];
-          const bool tok = MRM_CHECK(
-              tsm || ((long long)k0 * npair * 9 * pyhs + (long long)off + 8 * pyhs + kyh) * (long long)sizeof(R) <
-                         tens_len,
-              430, kyh);
-#pragma unroll
-          for (int cc = 0; cc < 9; ++cc) tv[cc] = tok ? Tp[cc * pyhs + kyh] : (R)0;
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const int cc = 3 * a + b;
-              R v = tv[cc];
-              if (((kOddMask >> cc) & 1) && upper) v = -v;
-              if ((kImagMask >> cc) & 1) h[a] = cadd(h[a], cmul_i(cscale(xm[b], v), (R)1));
-              else h[a] = cadd(h[a], cscale(xm[b], v));
-            }
-        } else {
-          const Cx<R>* Tc = reinterpret_cast<const Cx<R>*>(rd.tens) +
-                            ((size_t)(k0 + c) * npair + ks * nl + ko) * 9 * py;
-          Cx<R> tv[9];
-#pragma unroll
-          for (int cc = 0; cc < 9; ++cc) tv[cc] = Tc[cc * py + ky];
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) h[a] = cadd(h[a], cmul(tv[3 * a + b], xm[b]));
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) G[((c * nl + ko) * 3 + a) * cs + ky] = h[a];
-    }
-  }
-  __syncthreads();
-  Cx<R>* Hs = block_fft_c<R, +1, 0, BLOCK>(G, F, lgpy, nseq, tws);
-
-  (void)pyh;
-  const int tot2 = nseq * ny;
-  for (int idx = threadIdx.x; idx < tot2; idx += BLOCK) {
-    const int c = idx % nc, rest = idx / nc;
-    const int j = rest % ny, lc = rest / ny;
-    if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nl * 3 * ny * phs, 440, idx)) continue;
-    rd.spech[((size_t)lc * ny + j) * phs + k0 + c] = Hs[(c * nl * 3 + lc) * cs + j];
+  switch (lgpy) {
+    case 1: col_transform<R, 1, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 2: col_transform<R, 2, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 3: col_transform<R, 3, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 4: col_transform<R, 4, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 5: col_transform<R, 5, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 6: col_transform<R, 6, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 7: col_transform<R, 7, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 8: col_transform<R, 8, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 9: col_transform<R, 9, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 10: col_transform<R, 10, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 11: col_transform<R, 11, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    default: col_transform<R, 12, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
   }
 }
 

@@ -320,14 +320,18 @@ size_t row_fixed_smem(const mrm_gpu* r, int rpb) {
   return b;
 }
 
+// Column-kernel shared memory for tasks of nc columns (a power of two).  The
+// task's packed tensor slice is staged too where that keeps as many blocks per
+// SM resident as without it (up to minb; minb = 0: never staged).
 template <typename R>
-size_t col_smem_of(const mrm_gpu* r, int nc) {
-  size_t b = col_fft_smem<R>(r->lgpy, nc * r->nl * 3);
-  if (sizeof(R) == sizeof(float)) {
-    const int reals = nc * r->nl * r->nl * 9 * tens_row_stride(r->py);
-    if (tens_slice_fits<R>(reals)) b += (size_t)reals * sizeof(R);
-  }
-  return b;
+size_t col_smem_of(const mrm_gpu* r, int nc, int minb) {
+  const size_t b = col_fft_smem<R>(r->lgpy, ilog2(nc), r->nl * 3);
+  if (sizeof(R) != sizeof(float) || minb <= 0) return b;
+  const int reals = nc * r->nl * r->nl * 9 * tens_row_stride(r->py);
+  if (!tens_slice_fits<R>(reals)) return b;
+  const size_t with = b + (size_t)reals * sizeof(R);
+  auto resident = [](size_t bytes) { return (int)(kSmemPerSM / (bytes + kSmemReserved)); };
+  return resident(with) >= std::min(minb, resident(b)) ? with : b;
 }
 
 // The geometry must run with the most economical shapes (one row per row
@@ -361,7 +365,7 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
   const bool f64 = g->precision == MRM_FP64;
   const size_t rs = (f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1)) +
                     (size_t)(f64 ? head_table_bytes<double>(g->nx) : head_table_bytes<float>(g->nx));
-  const size_t cs = f64 ? col_smem_of<double>(&tmp, 1) : col_smem_of<float>(&tmp, 1);
+  const size_t cs = f64 ? col_smem_of<double>(&tmp, 1, 0) : col_smem_of<float>(&tmp, 1, 0);
   if (rs + row_static_bytes(3) > kMaxSmem || cs + 64 > kMaxSmem)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d x %d layers exceeds shared memory", px,
                    py, g->n_lay);
@@ -503,7 +507,7 @@ int plan_smem(Engine* e) {
     const int rows = rows_per_task(r, rv.rpb);
     fft = std::max(fft, row_fixed_smem<R>(r, rv.rpb));
     for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
-    if (r->demag && r->tensor_ready) scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r)));
+    if (r->demag && r->tensor_ready) scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r), col_variant<R>(e->colv).minb));
   }
   for (int q = 0; q < kSlots; ++q) {
     const long long per_block = (long long)(kSmemPerSM / rv.minb) - (long long)kSmemReserved -
@@ -2214,7 +2218,7 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   CK(launch_row<float>(0, kInit, false,
                        RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false, head},
                        0, kFlagForce));
-  CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt), true}, 0,
+  CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt, col_variant<float>(0).minb), true}, 0,
                        kFlagForce));
   CK(launch_row<float>(0, kEval, false,
                        RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_eval, cap_eval, true, head},
