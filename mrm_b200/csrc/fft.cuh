@@ -250,71 +250,107 @@ MRM_D void dft_r(Cx<R>* v) {
   else dft2<R, S>(v);
 }
 
-// One in-place pass over nh sequence groups of 2^lgT columns (columns c >= nc skipped).
-template <typename R, int LGN, int LGNS, bool INV, int BLOCK, class LD, class ST>
+// One in-place pass over nh sequence groups of 2^lgT columns.  A thread takes
+// CP (1 or 2) adjacent columns of one butterfly, through ld(h, c, j, v) /
+// st(h, c, j, v) with v the CP values of columns c, c+1; column groups at or
+// past nc are skipped.  HALF: the upper half of the elements (m >= RADIX/2 of
+// this pass) is zero on input (forward) or not wanted on output (inverse); set
+// only on the pass that spans the whole length, where m alone decides
+// j >= 2^LGN / 2.
+template <typename R, int LGN, int LGNS, bool INV, int CP, bool HALF, int BLOCK, class LD, class ST>
 MRM_D void ip_pass(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
   constexpr int LGR = pass_lgr(LGN, LGNS);
   constexpr int RADIX = 1 << LGR, NS = 1 << LGNS, LGB = LGN - LGR;
   constexpr int OFF = pass_tw_off(LGN, LGNS);
-  const int total = nh << (LGB + lgT);
-  const int tmask = (1 << lgT) - 1;
+  constexpr int LGCP = CP == 2 ? 1 : 0;
+  constexpr int MIN = HALF && !INV ? RADIX / 2 : RADIX;  // inputs that can be non-zero
+  constexpr int MOUT = HALF && INV ? RADIX / 2 : RADIX;  // outputs that are stored
+  static_assert(!HALF || LGNS + LGR == LGN, "HALF applies to the pass spanning the whole length");
+  const int lgq = lgT - LGCP;
+  const int total = nh << (LGB + lgq);
+  const int gmask = (1 << lgq) - 1;
   for (int q = threadIdx.x; q < total; q += BLOCK) {
-    const int c = q & tmask;
+    const int c = (q & gmask) << LGCP;
     if (c >= nc) continue;
-    const int bf = (q >> lgT) & ((1 << LGB) - 1), h = q >> (LGB + lgT);
+    const int bf = (q >> lgq) & ((1 << LGB) - 1), h = q >> (LGB + lgq);
     const int j0 = bf & (NS - 1), base = ((bf >> LGNS) << (LGNS + LGR)) + j0;
-    Cx<R> v[RADIX];
+    Cx<R> v[RADIX][CP];
 #pragma unroll
-    for (int m = 0; m < RADIX; ++m) v[m] = ld(h, c, base + m * NS);
+    for (int m = 0; m < RADIX; ++m) {
+      if (m < MIN) {
+        ld(h, c, base + m * NS, v[m]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < CP; ++k) v[m][k] = Cx<R>{(R)0, (R)0};
+      }
+    }
     if constexpr (INV && LGNS > 0) {
 #pragma unroll
-      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], cconj(twp[OFF + (m - 1) * NS + j0]));
+      for (int m = 1; m < RADIX; ++m) {
+        const Cx<R> w = cconj(twp[OFF + (m - 1) * NS + j0]);
+#pragma unroll
+        for (int k = 0; k < CP; ++k) v[m][k] = cmul(v[m][k], w);
+      }
     }
-    dft_r<R, INV ? 1 : -1, RADIX>(v);
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      Cx<R> t[RADIX];
+#pragma unroll
+      for (int m = 0; m < RADIX; ++m) t[m] = v[m][k];
+      dft_r<R, INV ? 1 : -1, RADIX>(t);
+#pragma unroll
+      for (int m = 0; m < RADIX; ++m) v[m][k] = t[m];
+    }
     if constexpr (!INV && LGNS > 0) {
 #pragma unroll
-      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], twp[OFF + (m - 1) * NS + j0]);
+      for (int m = 1; m < RADIX; ++m) {
+        const Cx<R> w = twp[OFF + (m - 1) * NS + j0];
+#pragma unroll
+        for (int k = 0; k < CP; ++k) v[m][k] = cmul(v[m][k], w);
+      }
     }
 #pragma unroll
-    for (int m = 0; m < RADIX; ++m) st(h, c, base + m * NS, v[m]);
+    for (int m = 0; m < MOUT; ++m) st(h, c, base + m * NS, v[m]);
   }
 }
 
 // forward passes LGNS, LGNS-3, ..., 0 through ld/st, each followed by __syncthreads
-template <typename R, int LGN, int LGNS, int BLOCK, class LD, class ST>
+template <typename R, int LGN, int LGNS, int CP, int BLOCK, class LD, class ST>
 MRM_D void ip_fwd_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
-  ip_pass<R, LGN, LGNS, false, BLOCK>(lgT, nc, nh, twp, ld, st);
+  ip_pass<R, LGN, LGNS, false, CP, false, BLOCK>(lgT, nc, nh, twp, ld, st);
   __syncthreads();
-  if constexpr (LGNS >= 3) ip_fwd_from<R, LGN, LGNS - 3, BLOCK>(lgT, nc, nh, twp, ld, st);
+  if constexpr (LGNS >= 3) ip_fwd_from<R, LGN, LGNS - 3, CP, BLOCK>(lgT, nc, nh, twp, ld, st);
 }
 // inverse passes LGNS, LGNS+3, ..., top; the top one stores through st_last (no barrier after it)
-template <typename R, int LGN, int LGNS, int BLOCK, class LD, class ST, class STL>
+template <typename R, int LGN, int LGNS, int CP, bool HALF, int BLOCK, class LD, class ST, class STL>
 MRM_D void ip_inv_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
   if constexpr (LGNS == ip_top(LGN)) {
-    ip_pass<R, LGN, LGNS, true, BLOCK>(lgT, nc, nh, twp, ld, st_last);
+    ip_pass<R, LGN, LGNS, true, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st_last);
   } else {
-    ip_pass<R, LGN, LGNS, true, BLOCK>(lgT, nc, nh, twp, ld, st);
+    ip_pass<R, LGN, LGNS, true, CP, false, BLOCK>(lgT, nc, nh, twp, ld, st);
     __syncthreads();
-    ip_inv_from<R, LGN, LGNS + 3, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+    ip_inv_from<R, LGN, LGNS + 3, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
   }
 }
 
 // Forward transform of length 2^LGN: the first pass reads through ld0, the
 // rest through ld; every pass writes through st; ends with __syncthreads.
-// The caller must __syncthreads() before the call if ld0 reads shared memory.
-template <typename R, int LGN, int BLOCK, class LD0, class LD, class ST>
+// HALF: elements j >= 2^LGN / 2 are zero (ld0 is not called for them).  The
+// caller must __syncthreads() before the call if ld0 reads shared memory.
+template <typename R, int LGN, int CP, bool HALF, int BLOCK, class LD0, class LD, class ST>
 MRM_D void ip_fft_fwd(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD0& ld0, LD& ld, ST& st) {
   constexpr int TOP = ip_top(LGN);
-  ip_pass<R, LGN, TOP, false, BLOCK>(lgT, nc, nh, twp, ld0, st);
+  ip_pass<R, LGN, TOP, false, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld0, st);
   __syncthreads();
-  if constexpr (TOP >= 3) ip_fwd_from<R, LGN, TOP - 3, BLOCK>(lgT, nc, nh, twp, ld, st);
+  if constexpr (TOP >= 3) ip_fwd_from<R, LGN, TOP - 3, CP, BLOCK>(lgT, nc, nh, twp, ld, st);
 }
 // Inverse transform of length 2^LGN (unnormalised) from digit-reversed order:
 // every pass reads through ld, the last writes through st_last and the others
-// through st.  The caller must __syncthreads() before the call.
-template <typename R, int LGN, int BLOCK, class LD, class ST, class STL>
+// through st.  HALF: only elements j < 2^LGN / 2 are stored by the last pass.
+// The caller must __syncthreads() before the call.
+template <typename R, int LGN, int CP, bool HALF, int BLOCK, class LD, class ST, class STL>
 MRM_D void ip_fft_inv(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
-  ip_inv_from<R, LGN, 0, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+  ip_inv_from<R, LGN, 0, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
 }
 
 // ---------------- run-time form (tensor FFT) ----------------

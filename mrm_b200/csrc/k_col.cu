@@ -1,5 +1,5 @@
-// k_col.cu -- column kernels (FP32 packed tensor, FP64 complex tensor), their
-// launch wrappers, and the dispatch over the row shapes compiled in k_row_*.cu.
+// k_col.cu -- dispatch over the compiled column shapes (k_col_*.cu) and row
+// shapes (k_row_*.cu), and the shared-memory limits of their kernels.
 #include <map>
 #include <mutex>
 #include <utility>
@@ -10,37 +10,33 @@
 namespace mrm {
 namespace {
 
-template <typename R, int V>
-struct ColV {
-  static constexpr ColVariant s = col_variant<R>(V);
-  static constexpr bool packed = sizeof(R) == sizeof(float);
-  static constexpr auto fn() { return col_kernel<R, packed, s.block, s.minb>; }
-};
-
 template <typename R>
-const void* col_fn_any(int v) {
-  switch (v) {
-    case 0: return (const void*)ColV<R, 0>::fn();
-    case 1: return (const void*)ColV<R, 1 < col_variant_count<R>() ? 1 : 0>::fn();
-    default: return (const void*)ColV<R, 2 < col_variant_count<R>() ? 2 : 0>::fn();
+const ColOps* col_ops_of(int v) {
+  if (v < 0 || v >= col_variant_count<R>()) return nullptr;
+  if constexpr (sizeof(R) == sizeof(float)) {
+    switch (v) {
+      case 0: return &col_ops<float, 0>();
+      case 1: return &col_ops<float, 1>();
+      default: return &col_ops<float, 2>();
+    }
+  } else {
+    switch (v) {
+      case 0: return &col_ops<double, 0>();
+      default: return &col_ops<double, 1>();
+    }
   }
 }
 
-template <typename R, int V>
-cudaError_t col_launch_v(const ColLaunch& a, int istep, int flags) {
-  return launch_kernel(ColV<R, V>::fn(), dim3(a.ntasks), dim3(ColV<R, V>::s.block), a.smem, a.st, a.pdl,
-                       static_cast<const RunDev<R>*>(a.runs), a.tasks, static_cast<const Cx<R>*>(a.tw), istep,
-                       flags, a.err);
+template <typename R>
+const void* col_fn_any(int v) {
+  const ColOps* o = col_ops_of<R>(v);
+  return o ? o->fn : nullptr;
 }
 
 template <typename R>
 cudaError_t col_launch_any(int v, const ColLaunch& a, int istep, int flags) {
-  if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;
-  switch (v) {
-    case 0: return col_launch_v<R, 0>(a, istep, flags);
-    case 1: return col_launch_v<R, 1 < col_variant_count<R>() ? 1 : 0>(a, istep, flags);
-    default: return col_launch_v<R, 2 < col_variant_count<R>() ? 2 : 0>(a, istep, flags);
-  }
+  const ColOps* o = col_ops_of<R>(v);
+  return o ? o->launch(a, istep, flags) : cudaErrorInvalidValue;
 }
 
 }  // namespace

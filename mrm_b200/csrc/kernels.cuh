@@ -832,7 +832,33 @@ MRM_D void col_product(const RunDev<R>& rd, Cx<R>* A, Cx<R>* O, const R* Ts, boo
   }
 }
 
-template <typename R, int LGN, bool PACKED, int BLOCK>
+// CP adjacent complex values (CP = 2: one 16-byte access in FP32)
+template <typename R, int CP>
+MRM_D void ld_cp(const Cx<R>* p, Cx<R>* v) {
+  if constexpr (CP == 2 && sizeof(R) == sizeof(float)) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = Cx<R>{t.x, t.y};
+    v[1] = Cx<R>{t.z, t.w};
+  } else {
+#pragma unroll
+    for (int k = 0; k < CP; ++k) v[k] = p[k];
+  }
+}
+template <typename R, int CP>
+MRM_D void st_cp(Cx<R>* p, const Cx<R>* v) {
+  if constexpr (CP == 2 && sizeof(R) == sizeof(float)) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+  } else {
+#pragma unroll
+    for (int k = 0; k < CP; ++k) p[k] = v[k];
+  }
+}
+
+// The column transform of one task: CP columns per thread (2 when the tile
+// has at least two), HALF when rows >= py/2 are the zero padding (open
+// boundary: py >= 2 ny), so the first forward pass skips them and the last
+// inverse pass does not produce them.
+template <typename R, int LGN, bool PACKED, int CP, bool HALF, int BLOCK>
 MRM_D void col_transform(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const R* Ts, bool tsm, int k0, int nc,
                          int* err) {
   const int nl = rd.nl, ny = rd.ny, nys = rd.nys, phs = rd.phs, lgct = rd.lgct;
@@ -842,35 +868,55 @@ MRM_D void col_transform(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const 
   // the task's tile of M^: plane lc at ((lc*ntile + tile)*nys + j)*T + c
   const Cx<R>* src = rd.specx + ((size_t)(k0 >> lgct) * nys << lgct);
   const size_t src_plane = (size_t)ntile * nys << lgct;
-  auto ld_g = [&](int lc, int c, int j) -> Cx<R> {
-    if (j >= ny) return Cx<R>{(R)0, (R)0};
-    MRM_CHECK((long long)(k0 >> lgct) * nys * (1 << lgct) + (long long)lc * src_plane + ((long long)j << lgct) + c <
+  auto ld_g = [&](int lc, int c, int j, Cx<R>* v) {
+    if (j >= ny) {
+#pragma unroll
+      for (int k = 0; k < CP; ++k) v[k] = Cx<R>{(R)0, (R)0};
+      return;
+    }
+    MRM_CHECK((long long)(k0 >> lgct) * nys * (1 << lgct) + (long long)lc * src_plane + ((long long)j << lgct) + c +
+                      CP <=
                   (long long)nplane * src_plane,
               420, j);
-    return src[lc * src_plane + ((size_t)j << lgct) + c];
+    ld_cp<R, CP>(src + lc * src_plane + ((size_t)j << lgct) + c, v);
   };
-  auto ld_s = [&](int lc, int c, int j) -> Cx<R> { return A[lc * plane + ((j + (j >> 3)) << lgct) + c]; };
-  auto st_s = [&](int lc, int c, int j, Cx<R> v) { A[lc * plane + ((j + (j >> 3)) << lgct) + c] = v; };
-  auto st_g = [&](int lc, int c, int j, Cx<R> v) {
+  auto ld_s = [&](int lc, int c, int j, Cx<R>* v) { ld_cp<R, CP>(A + lc * plane + ((j + (j >> 3)) << lgct) + c, v); };
+  auto st_s = [&](int lc, int c, int j, const Cx<R>* v) {
+    st_cp<R, CP>(A + lc * plane + ((j + (j >> 3)) << lgct) + c, v);
+  };
+  auto st_g = [&](int lc, int c, int j, const Cx<R>* v) {
     if (j >= ny) return;
+    Cx<R>* d = rd.spech + ((size_t)lc * ny + j) * phs + k0 + c;
     if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nplane * ny * phs, 440, j)) return;
-    rd.spech[((size_t)lc * ny + j) * phs + k0 + c] = v;
+    if (CP == 1 || c + 1 < nc) st_cp<R, CP>(d, v);
+    else d[0] = v[0];  // the last column of a short tile
   };
-  ip_fft_fwd<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_g, ld_s, st_s);
+  ip_fft_fwd<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_g, ld_s, st_s);
   if (nl <= 2) {
     if (nl == 1) col_product<R, PACKED, 1, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
     else col_product<R, PACKED, 2, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
     __syncthreads();
-    ip_fft_inv<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_s, st_s, st_g);
+    ip_fft_inv<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_s, st_s, st_g);
   } else {
     // three or more layers: the product goes to the second buffer
     Cx<R>* O = A + col_buf_count(1 << LGN, lgct, nplane);
     col_product<R, PACKED, 0, BLOCK>(rd, A, O, Ts, tsm, k0, nc, err);
     __syncthreads();
-    auto ld_o = [&](int lc, int c, int j) -> Cx<R> { return O[lc * plane + ((j + (j >> 3)) << lgct) + c]; };
-    auto st_o = [&](int lc, int c, int j, Cx<R> v) { O[lc * plane + ((j + (j >> 3)) << lgct) + c] = v; };
-    ip_fft_inv<R, LGN, BLOCK>(lgct, nc, nplane, tws, ld_o, st_o, st_g);
+    auto ld_o = [&](int lc, int c, int j, Cx<R>* v) { ld_cp<R, CP>(O + lc * plane + ((j + (j >> 3)) << lgct) + c, v); };
+    auto st_o = [&](int lc, int c, int j, const Cx<R>* v) {
+      st_cp<R, CP>(O + lc * plane + ((j + (j >> 3)) << lgct) + c, v);
+    };
+    ip_fft_inv<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_o, st_o, st_g);
   }
+}
+
+template <typename R, int LGN, bool PACKED, int BLOCK>
+MRM_D void col_transform_any(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const R* Ts, bool tsm, int k0, int nc,
+                             int* err) {
+  // (two columns per thread measured slower at the tuned shapes: fewer,
+  // unevenly shared butterflies per pass)
+  if (rd.py >= 2 * rd.ny) col_transform<R, LGN, PACKED, 1, true, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
+  else col_transform<R, LGN, PACKED, 1, false, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
 }
 
 template <typename R, bool PACKED, int BLOCK, int MINB>
@@ -943,18 +989,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
   if (!run_it) return;
 
   switch (lgpy) {
-    case 1: col_transform<R, 1, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 2: col_transform<R, 2, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 3: col_transform<R, 3, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 4: col_transform<R, 4, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 5: col_transform<R, 5, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 6: col_transform<R, 6, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 7: col_transform<R, 7, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 8: col_transform<R, 8, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 9: col_transform<R, 9, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 10: col_transform<R, 10, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    case 11: col_transform<R, 11, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
-    default: col_transform<R, 12, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 1: col_transform_any<R, 1, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 2: col_transform_any<R, 2, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 3: col_transform_any<R, 3, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 4: col_transform_any<R, 4, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 5: col_transform_any<R, 5, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 6: col_transform_any<R, 6, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 7: col_transform_any<R, 7, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 8: col_transform_any<R, 8, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 9: col_transform_any<R, 9, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 10: col_transform_any<R, 10, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    case 11: col_transform_any<R, 11, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
+    default: col_transform_any<R, 12, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
   }
 }
 

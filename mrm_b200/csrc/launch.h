@@ -75,6 +75,14 @@ struct ColLaunch {
   bool pdl;
 };
 
+// entry points of one compiled column shape (defined in its own translation unit)
+struct ColOps {
+  cudaError_t (*launch)(const ColLaunch& a, int istep, int flags);
+  const void* fn;
+};
+template <typename R, int V>
+const ColOps& col_ops();
+
 // stage: kInit, kPred, kCorr, kEval; stats selects the corrector with reductions
 template <typename R>
 cudaError_t launch_row(int variant, int stage, bool stats, const RowLaunch& a, int istep, int flags);
