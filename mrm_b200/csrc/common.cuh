@@ -76,6 +76,7 @@ struct LayerDev {
   unsigned long long hd_bits;
   int hd_nbits;
   double temperature;
+  double tfac;  // sqrt(temperature / dt), set with the run's dt
   double gamma;
   int thermal;
   int n;

@@ -113,6 +113,13 @@ MRM_HD int head_table_bytes(int nx) {
 }
 
 // CSR neighbour sum  sum_j c_j m_j  (field.f90:350-363 / :326-348)
+// The FP32 stepping arithmetic uses the hardware reciprocal and reciprocal
+// square root (a couple of ulp) where FP64 runs keep the correctly rounded forms.
+MRM_D float fast_div(float a, float b) { return __fdividef(a, b); }
+MRM_D double fast_div(double a, double b) { return a / b; }
+MRM_D float fast_rsqrt(float x) { return rsqrtf(x); }
+MRM_D double fast_rsqrt(double x) { return 1.0 / sqrt(x); }
+
 template <typename R>
 MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
                    const R* __restrict__ cf, const V4<R>* __restrict__ mb, int n, R& hx, R& hy,
@@ -431,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
-  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;
+  const R tfac = thermal ? (R)L.tfac : (R)0;
   const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
   // Write head: its field depends on the column and the time only.  The
   // stepping stages add it to the block's demag values in shared memory (zero
@@ -600,7 +607,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       mn.z = m0.z + dz;
     } else if (mse > (R)0) {
       const R a = pb.z;  // alpha * alpha_scale
-      const R s11 = -gamma * dt / ((R)1 + a * a);
+      const R s11 = fast_div(-gamma * dt, (R)1 + a * a);
       R tx, ty, tz, ux, uy, uz;
       cross3(mf.x, mf.y, mf.z, fx, fy, fz, tx, ty, tz);
       cross3(mf.x, mf.y, mf.z, tx, ty, tz, ux, uy, uz);
@@ -624,7 +631,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       mn.z = m0.z + dz;
       const R y = mn.x * mn.x + mn.y * mn.y + mn.z * mn.z;
       if (y > (R)0) {
-        const R r = (R)1 / sqrt(y);
+        const R r = fast_rsqrt(y);
         mn.x *= r;
         mn.y *= r;
         mn.z *= r;
@@ -683,11 +690,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // ---------------- forward row transform of Ms*m -> spectrum columns ----------------
   const int two_m = 2 * M;
   if (nx < two_m) {
-    const int pad = two_m - nx;
-    for (int idx = threadIdx.x; idx < nseq * pad; idx += BLOCK) {
-      const int s = idx / pad, i = nx + (idx - s * pad);
-      outr[s * rs + i] = (R)0;
-    }
+    for (int s = 0; s < nseq; ++s)
+      for (int i = nx + threadIdx.x; i < two_m; i += BLOCK) outr[s * rs + i] = (R)0;
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;

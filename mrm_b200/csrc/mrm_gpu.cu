@@ -443,6 +443,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.moddepth = b.moddepth;
     o.dc = b.dc;
     o.temperature = b.temperature;
+    o.tfac = std::sqrt(b.temperature / r->dt);
     o.gamma = b.gamma;
     o.thermal = b.thermal;
     o.n = b.n;

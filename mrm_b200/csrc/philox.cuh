@@ -7,8 +7,9 @@
 //  * FP64 runs: Philox4x64-10, counter (grain, step, layer, 0), key
 //    (seed, 0x6d726d), 53-bit uniforms;
 //  * FP32 runs: Philox4x32-10, counter (grain, step low, step high, layer),
-//    key (seed low, seed high ^ 0x6d726d), 24-bit uniforms (the 64-bit
-//    multiplies of the 4x64 form were a sixth of the predictor's time).
+//    key (seed low, seed high ^ 0x6d726d), 24-bit uniforms and the hardware
+//    approximations of log, sqrt and sin/cos (the 64-bit multiplies of the
+//    4x64 form were a sixth of the predictor's time).
 #pragma once
 #include "common.cuh"
 
@@ -78,13 +79,18 @@ MRM_D void thermal_normals(unsigned long long seed, unsigned long long layer,
   float u1 = ((float)(c[1] >> 8) + 0.5f) * s24;
   float u2 = ((float)(c[2] >> 8) + 0.5f) * s24;
   float u3 = ((float)(c[3] >> 8) + 0.5f) * s24;
-  float ra = sqrtf(-2.0f * logf(u0));
-  float rb = sqrtf(-2.0f * logf(u2));
+  // Box-Muller on the hardware approximations (__logf, rsqrtf, __sincosf with
+  // the angle in (-pi, pi), where they are accurate to about 1e-6 absolute).
+  // The floor keeps the radius finite when __logf of a u just below 1 rounds
+  // to a non-negative value (the radius there is below 1e-3 either way).
+  const float la = fmaxf(-2.0f * __logf(u0), 1e-30f), lb = fmaxf(-2.0f * __logf(u2), 1e-30f);
+  const float ra = la * rsqrtf(la), rb = lb * rsqrtf(lb);
+  const float kPi = 3.14159265358979f;
   float s, co;
-  sincospif(2.0f * u1, &s, &co);
+  __sincosf(kPi * (2.0f * u1 - 1.0f), &s, &co);
   n[0] = ra * co;
   n[1] = ra * s;
-  n[2] = rb * cospif(2.0f * u3);
+  n[2] = rb * __cosf(kPi * (2.0f * u3 - 1.0f));
 }
 
 }  // namespace mrm
