@@ -307,7 +307,7 @@ def batched_leg(args, torch, local, rank, dist):
         b.step(args.heun)
         st = b.stats(runs)
         for i, r in enumerate(runs):
-            m_host[i][:] = r.get_state(0)
+            r.get_state(0, out=m_host[i])
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local}")

@@ -74,6 +74,7 @@ struct mrm_gpu {
   LayerBufs L[MRM_MAX_LAYERS];
   void* spech = nullptr;
   void* specx = nullptr;
+  void* xfer = nullptr;  // 3 x N doubles: host <-> device transfers of one layer's state
   void* tens = nullptr;
   bool tensor_ready = false;
   bool demag = true;
@@ -961,6 +962,26 @@ int check_device_error(Engine* e) {
                  v[1], val);
 }
 
+// ---------------- state transfers ----------------
+// (x, y, z) doubles of the host layout <-> the float4 / double4 grain records
+template <typename R>
+__global__ void state_in_kernel(const double* __restrict__ in, V4<R>* __restrict__ m, V4<R>* __restrict__ mp, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V4<R> v{(R)in[3 * i], (R)in[3 * i + 1], (R)in[3 * i + 2], (R)0};
+  m[i] = v;
+  mp[i] = v;
+}
+template <typename R>
+__global__ void state_out_kernel(const V4<R>* __restrict__ src, double* __restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V4<R> v = src[i];
+  out[3 * i] = (double)v.x;
+  out[3 * i + 1] = (double)v.y;
+  out[3 * i + 2] = (double)v.z;
+}
+
 // ---------------- run buffers ----------------
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
@@ -968,6 +989,8 @@ int run_alloc(mrm_gpu* r) {
   int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * 2 * re);
   if (rc) return rc;
   rc = dmalloc(errp, &r->specx, specx_count(r) * 2 * re);
+  if (rc) return rc;
+  rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
   if (rc) return rc;
   rc = dmalloc(errp, &r->tens, tensor_bytes(r));
   if (rc) return rc;
@@ -989,6 +1012,7 @@ int run_alloc(mrm_gpu* r) {
 void run_free(mrm_gpu* r) {
   dfree(r->spech);
   dfree(r->specx);
+  dfree(r->xfer);
   dfree(r->tens);
   for (int l = 0; l < MRM_MAX_LAYERS; ++l) {
     LayerBufs& b = r->L[l];
@@ -1010,6 +1034,7 @@ int64_t footprint(const mrm_geom& g) {
   int64_t b = nl * 3 * g.ny * spec_row_stride(px) * 2 * re + nl * 3 * ph8 * spec_col_stride(g.ny) * 2 * re;
   b += g.precision == MRM_FP64 ? ph * nl * nl * 9 * py * 16 : ph * nl * nl * 9 * tens_row_stride(py) * 4;
   b += nl * n * (8 * 4 * re + 4 * 8);
+  b += n * 3 * 8;  // host transfer buffer of one layer's state
   b += nl * (n + 1) * 4 + nl * n * 4 * (4 + re);  // exchange CSR (4 neighbours)
   if (nl > 1) b += 2 * nl * ((n + 1) * 4 + n * (4 + re));
   return b;
@@ -1590,23 +1615,22 @@ int mrm_gpu_set_state(mrm_gpu* h, int layer, const double* m) {
   if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
   if (!h->L[layer].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", layer);
   const int n = h->L[layer].n;
+  cudaStream_t st = h->eng->st;
   CK(cudaSetDevice(h->eng->dev));
-  CK(cudaStreamSynchronize(h->eng->st));
-  if (h->g.precision == MRM_FP64) {
-    std::vector<double> v(4 * n);
-    for (int g = 0; g < n; ++g) {
-      v[4 * g] = m[3 * g]; v[4 * g + 1] = m[3 * g + 1]; v[4 * g + 2] = m[3 * g + 2]; v[4 * g + 3] = 0;
-    }
-    CK(cudaMemcpy(h->L[layer].m, v.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->L[layer].mp, v.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float> v(4 * n);
-    for (int g = 0; g < n; ++g) {
-      v[4 * g] = (float)m[3 * g]; v[4 * g + 1] = (float)m[3 * g + 1]; v[4 * g + 2] = (float)m[3 * g + 2]; v[4 * g + 3] = 0;
-    }
-    CK(cudaMemcpy(h->L[layer].m, v.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->L[layer].mp, v.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice));
-  }
+  // the caller's array as it is, then widened on the device into m and m*,
+  // in stream order after the work already queued
+  CK(cudaMemcpyAsync(h->xfer, m, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (h->g.precision == MRM_FP64)
+    state_in_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer),
+                                                     static_cast<V4<double>*>(h->L[layer].m),
+                                                     static_cast<V4<double>*>(h->L[layer].mp), n);
+  else
+    state_in_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer),
+                                                    static_cast<V4<float>*>(h->L[layer].m),
+                                                    static_cast<V4<float>*>(h->L[layer].mp), n);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));  // the caller may reuse its array on return
   h->spec_valid = false;
   return MRM_OK;
 }
@@ -1615,17 +1639,18 @@ static int get_v4(mrm_gpu* h, int layer, void* src, double* out) {
   std::string* errp = &h->err;
   if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
   const int n = h->L[layer].n;
+  cudaStream_t st = h->eng->st;
   CK(cudaSetDevice(h->eng->dev));
-  CK(cudaStreamSynchronize(h->eng->st));
-  if (h->g.precision == MRM_FP64) {
-    std::vector<double> v(4 * n);
-    CK(cudaMemcpy(v.data(), src, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
-    for (int g = 0; g < n; ++g) { out[3 * g] = v[4 * g]; out[3 * g + 1] = v[4 * g + 1]; out[3 * g + 2] = v[4 * g + 2]; }
-  } else {
-    std::vector<float> v(4 * n);
-    CK(cudaMemcpy(v.data(), src, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
-    for (int g = 0; g < n; ++g) { out[3 * g] = v[4 * g]; out[3 * g + 1] = v[4 * g + 1]; out[3 * g + 2] = v[4 * g + 2]; }
-  }
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (h->g.precision == MRM_FP64)
+    state_out_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const V4<double>*>(src),
+                                                      static_cast<double*>(h->xfer), n);
+  else
+    state_out_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const V4<float>*>(src),
+                                                     static_cast<double*>(h->xfer), n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, h->xfer, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return MRM_OK;
 }
 

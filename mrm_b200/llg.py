@@ -126,8 +126,14 @@ class _RunMixin:
         mm = f64(m)
         self._check(_lib.load().mrm_gpu_set_state(self.h, layer, fptr(mm)))
 
-    def get_state(self, layer: int) -> np.ndarray:
-        out = np.zeros((self.medium.layers[layer].N, 3))
+    def get_state(self, layer: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """m of `layer` as (N, 3) float64; `out`: a C-contiguous (N, 3) float64
+        array to fill instead of a new one (pinned host memory copies fastest)."""
+        n = self.medium.layers[layer].N
+        if out is None:
+            out = np.zeros((n, 3))
+        elif out.shape != (n, 3) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous ({n}, 3) float64 array")
         self._check(_lib.load().mrm_gpu_get_state(self.h, layer, fptr(out)))
         return out
 
