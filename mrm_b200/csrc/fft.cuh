@@ -250,107 +250,92 @@ MRM_D void dft_r(Cx<R>* v) {
   else dft2<R, S>(v);
 }
 
-// One in-place pass over nh sequence groups of 2^lgT columns.  A thread takes
-// CP (1 or 2) adjacent columns of one butterfly, through ld(h, c, j, v) /
-// st(h, c, j, v) with v the CP values of columns c, c+1; column groups at or
-// past nc are skipped.  HALF: the upper half of the elements (m >= RADIX/2 of
-// this pass) is zero on input (forward) or not wanted on output (inverse); set
-// only on the pass that spans the whole length, where m alone decides
-// j >= 2^LGN / 2.
-template <typename R, int LGN, int LGNS, bool INV, int CP, bool HALF, int BLOCK, class LD, class ST>
-MRM_D void ip_pass(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
+// Element access of the in-place passes.  An accessor maps the butterfly
+// start (h: sequence group, c: column within a tile of 2^lgT columns, base:
+// element index) to a pointer and gives the element stride of a pass of span
+// NS, so the 2^LGR elements base + m*NS of a butterfly sit at ptr + m*stride:
+//   ptr(h, c, base), stride(NS), valid(j) (false: the element is outside the
+//   data: read as zero, not written).
+// One in-place pass over nh sequence groups (columns c >= nc skipped).  HALF:
+// the upper half of the elements (m >= RADIX/2) is zero on input (forward) or
+// not wanted on output (inverse); set only on the pass that spans the whole
+// length, where m alone decides j >= 2^LGN / 2.
+template <typename R, int LGN, int LGNS, bool INV, bool HALF, int BLOCK, class IN, class OUT>
+MRM_D void ip_pass(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, const IN& in, const OUT& out) {
   constexpr int LGR = pass_lgr(LGN, LGNS);
   constexpr int RADIX = 1 << LGR, NS = 1 << LGNS, LGB = LGN - LGR;
   constexpr int OFF = pass_tw_off(LGN, LGNS);
-  constexpr int LGCP = CP == 2 ? 1 : 0;
   constexpr int MIN = HALF && !INV ? RADIX / 2 : RADIX;  // inputs that can be non-zero
   constexpr int MOUT = HALF && INV ? RADIX / 2 : RADIX;  // outputs that are stored
   static_assert(!HALF || LGNS + LGR == LGN, "HALF applies to the pass spanning the whole length");
-  const int lgq = lgT - LGCP;
-  const int total = nh << (LGB + lgq);
-  const int gmask = (1 << lgq) - 1;
+  const int total = nh << (LGB + lgT);
+  const int tmask = (1 << lgT) - 1;
+  const int es_in = in.stride(NS), es_out = out.stride(NS);
   for (int q = threadIdx.x; q < total; q += BLOCK) {
-    const int c = (q & gmask) << LGCP;
+    const int c = q & tmask;
     if (c >= nc) continue;
-    const int bf = (q >> lgq) & ((1 << LGB) - 1), h = q >> (LGB + lgq);
+    const int bf = (q >> lgT) & ((1 << LGB) - 1), h = q >> (LGB + lgT);
     const int j0 = bf & (NS - 1), base = ((bf >> LGNS) << (LGNS + LGR)) + j0;
-    Cx<R> v[RADIX][CP];
+    Cx<R> v[RADIX];
+    {
+      const Cx<R>* pi = in.ptr(h, c, base);
 #pragma unroll
-    for (int m = 0; m < RADIX; ++m) {
-      if (m < MIN) {
-        ld(h, c, base + m * NS, v[m]);
-      } else {
-#pragma unroll
-        for (int k = 0; k < CP; ++k) v[m][k] = Cx<R>{(R)0, (R)0};
-      }
+      for (int m = 0; m < RADIX; ++m)
+        v[m] = (m < MIN && in.valid(base + m * NS)) ? pi[m * es_in] : Cx<R>{(R)0, (R)0};
     }
     if constexpr (INV && LGNS > 0) {
 #pragma unroll
-      for (int m = 1; m < RADIX; ++m) {
-        const Cx<R> w = cconj(twp[OFF + (m - 1) * NS + j0]);
-#pragma unroll
-        for (int k = 0; k < CP; ++k) v[m][k] = cmul(v[m][k], w);
-      }
+      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], cconj(twp[OFF + (m - 1) * NS + j0]));
     }
-#pragma unroll
-    for (int k = 0; k < CP; ++k) {
-      Cx<R> t[RADIX];
-#pragma unroll
-      for (int m = 0; m < RADIX; ++m) t[m] = v[m][k];
-      dft_r<R, INV ? 1 : -1, RADIX>(t);
-#pragma unroll
-      for (int m = 0; m < RADIX; ++m) v[m][k] = t[m];
-    }
+    dft_r<R, INV ? 1 : -1, RADIX>(v);
     if constexpr (!INV && LGNS > 0) {
 #pragma unroll
-      for (int m = 1; m < RADIX; ++m) {
-        const Cx<R> w = twp[OFF + (m - 1) * NS + j0];
-#pragma unroll
-        for (int k = 0; k < CP; ++k) v[m][k] = cmul(v[m][k], w);
-      }
+      for (int m = 1; m < RADIX; ++m) v[m] = cmul(v[m], twp[OFF + (m - 1) * NS + j0]);
     }
+    Cx<R>* po = out.ptr(h, c, base);
 #pragma unroll
-    for (int m = 0; m < MOUT; ++m) st(h, c, base + m * NS, v[m]);
+    for (int m = 0; m < MOUT; ++m)
+      if (out.valid(base + m * NS)) po[m * es_out] = v[m];
   }
 }
 
-// forward passes LGNS, LGNS-3, ..., 0 through ld/st, each followed by __syncthreads
-template <typename R, int LGN, int LGNS, int CP, int BLOCK, class LD, class ST>
-MRM_D void ip_fwd_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st) {
-  ip_pass<R, LGN, LGNS, false, CP, false, BLOCK>(lgT, nc, nh, twp, ld, st);
+// forward passes LGNS, LGNS-3, ..., 0 through acc, each followed by __syncthreads
+template <typename R, int LGN, int LGNS, int BLOCK, class ACC>
+MRM_D void ip_fwd_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, const ACC& acc) {
+  ip_pass<R, LGN, LGNS, false, false, BLOCK>(lgT, nc, nh, twp, acc, acc);
   __syncthreads();
-  if constexpr (LGNS >= 3) ip_fwd_from<R, LGN, LGNS - 3, CP, BLOCK>(lgT, nc, nh, twp, ld, st);
+  if constexpr (LGNS >= 3) ip_fwd_from<R, LGN, LGNS - 3, BLOCK>(lgT, nc, nh, twp, acc);
 }
-// inverse passes LGNS, LGNS+3, ..., top; the top one stores through st_last (no barrier after it)
-template <typename R, int LGN, int LGNS, int CP, bool HALF, int BLOCK, class LD, class ST, class STL>
-MRM_D void ip_inv_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
+// inverse passes LGNS, LGNS+3, ..., top; the top one writes through last (no barrier after it)
+template <typename R, int LGN, int LGNS, bool HALF, int BLOCK, class ACC, class LAST>
+MRM_D void ip_inv_from(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, const ACC& acc, const LAST& last) {
   if constexpr (LGNS == ip_top(LGN)) {
-    ip_pass<R, LGN, LGNS, true, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st_last);
+    ip_pass<R, LGN, LGNS, true, HALF, BLOCK>(lgT, nc, nh, twp, acc, last);
   } else {
-    ip_pass<R, LGN, LGNS, true, CP, false, BLOCK>(lgT, nc, nh, twp, ld, st);
+    ip_pass<R, LGN, LGNS, true, false, BLOCK>(lgT, nc, nh, twp, acc, acc);
     __syncthreads();
-    ip_inv_from<R, LGN, LGNS + 3, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+    ip_inv_from<R, LGN, LGNS + 3, HALF, BLOCK>(lgT, nc, nh, twp, acc, last);
   }
 }
 
-// Forward transform of length 2^LGN: the first pass reads through ld0, the
-// rest through ld; every pass writes through st; ends with __syncthreads.
-// HALF: elements j >= 2^LGN / 2 are zero (ld0 is not called for them).  The
-// caller must __syncthreads() before the call if ld0 reads shared memory.
-template <typename R, int LGN, int CP, bool HALF, int BLOCK, class LD0, class LD, class ST>
-MRM_D void ip_fft_fwd(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD0& ld0, LD& ld, ST& st) {
+// Forward transform of length 2^LGN: the first pass reads through first, the
+// rest through acc; every pass writes through acc; ends with __syncthreads.
+// HALF: elements j >= 2^LGN / 2 are zero (not read).  The caller must
+// __syncthreads() before the call if first reads shared memory.
+template <typename R, int LGN, bool HALF, int BLOCK, class FIRST, class ACC>
+MRM_D void ip_fft_fwd(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, const FIRST& first, const ACC& acc) {
   constexpr int TOP = ip_top(LGN);
-  ip_pass<R, LGN, TOP, false, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld0, st);
+  ip_pass<R, LGN, TOP, false, HALF, BLOCK>(lgT, nc, nh, twp, first, acc);
   __syncthreads();
-  if constexpr (TOP >= 3) ip_fwd_from<R, LGN, TOP - 3, CP, BLOCK>(lgT, nc, nh, twp, ld, st);
+  if constexpr (TOP >= 3) ip_fwd_from<R, LGN, TOP - 3, BLOCK>(lgT, nc, nh, twp, acc);
 }
 // Inverse transform of length 2^LGN (unnormalised) from digit-reversed order:
-// every pass reads through ld, the last writes through st_last and the others
-// through st.  HALF: only elements j < 2^LGN / 2 are stored by the last pass.
+// every pass reads through acc, the last writes through last and the others
+// through acc.  HALF: only elements j < 2^LGN / 2 are written by the last pass.
 // The caller must __syncthreads() before the call.
-template <typename R, int LGN, int CP, bool HALF, int BLOCK, class LD, class ST, class STL>
-MRM_D void ip_fft_inv(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, LD& ld, ST& st, STL& st_last) {
-  ip_inv_from<R, LGN, 0, CP, HALF, BLOCK>(lgT, nc, nh, twp, ld, st, st_last);
+template <typename R, int LGN, bool HALF, int BLOCK, class ACC, class LAST>
+MRM_D void ip_fft_inv(int lgT, int nc, int nh, const Cx<R>* __restrict__ twp, const ACC& acc, const LAST& last) {
+  ip_inv_from<R, LGN, 0, HALF, BLOCK>(lgT, nc, nh, twp, acc, last);
 }
 
 // ---------------- run-time form (tensor FFT) ----------------

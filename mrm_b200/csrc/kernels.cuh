@@ -836,91 +836,75 @@ MRM_D void col_product(const RunDev<R>& rd, Cx<R>* A, Cx<R>* O, const R* Ts, boo
   }
 }
 
-// CP adjacent complex values (CP = 2: one 16-byte access in FP32)
-template <typename R, int CP>
-MRM_D void ld_cp(const Cx<R>* p, Cx<R>* v) {
-  if constexpr (CP == 2 && sizeof(R) == sizeof(float)) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    v[0] = Cx<R>{t.x, t.y};
-    v[1] = Cx<R>{t.z, t.w};
-  } else {
-#pragma unroll
-    for (int k = 0; k < CP; ++k) v[k] = p[k];
+// Accessors of the column transform (see ip_pass).  Shared buffer: element j
+// of column c in plane h at h*plane + ((j + j/8) << lgT) + c; a butterfly's
+// elements base + m*NS are affine in m there (NS = 1: base a multiple of 8;
+// NS >= 8: a multiple of 8 apart).
+template <typename R>
+struct ColSmem {
+  Cx<R>* A;
+  int plane, lgT;
+  MRM_D Cx<R>* ptr(int h, int c, int base) const { return A + h * plane + ((base + (base >> 3)) << lgT) + c; }
+  MRM_D int stride(int ns) const { return (ns == 1 ? 1 : ns + (ns >> 3)) << lgT; }
+  MRM_D bool valid(int) const { return true; }
+};
+// the task's tile of M^ in global memory: plane h at ((h*ntile + tile)*nys + j)*T + c;
+// rows >= ny are the zero padding of the grid
+template <typename R>
+struct ColTileIn {
+  const Cx<R>* src;  // the tile of plane 0
+  size_t plane;
+  int lgT, ny;
+  MRM_D Cx<R>* ptr(int h, int c, int base) const {
+    return const_cast<Cx<R>*>(src) + h * plane + ((size_t)base << lgT) + c;
   }
-}
-template <typename R, int CP>
-MRM_D void st_cp(Cx<R>* p, const Cx<R>* v) {
-  if constexpr (CP == 2 && sizeof(R) == sizeof(float)) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-  } else {
-#pragma unroll
-    for (int k = 0; k < CP; ++k) p[k] = v[k];
-  }
-}
+  MRM_D int stride(int ns) const { return ns << lgT; }
+  MRM_D bool valid(int j) const { return j < ny; }
+};
+// H^ rows in global memory: plane h, row j at (h*ny + j)*phs + k0 + c; rows >= ny not stored
+template <typename R>
+struct ColRowsOut {
+  Cx<R>* dst;  // column k0 of row 0, plane 0
+  int ny, phs;
+  MRM_D Cx<R>* ptr(int h, int c, int base) const { return dst + ((size_t)h * ny + base) * phs + c; }
+  MRM_D int stride(int ns) const { return ns * phs; }
+  MRM_D bool valid(int j) const { return j < ny; }
+};
 
-// The column transform of one task: CP columns per thread (2 when the tile
-// has at least two), HALF when rows >= py/2 are the zero padding (open
-// boundary: py >= 2 ny), so the first forward pass skips them and the last
-// inverse pass does not produce them.
-template <typename R, int LGN, bool PACKED, int CP, bool HALF, int BLOCK>
+// The column transform of one task.  HALF when rows >= py/2 are the zero
+// padding (open boundary: py >= 2 ny), so the first forward pass skips them and
+// the last inverse pass does not produce them.
+template <typename R, int LGN, bool PACKED, bool HALF, int BLOCK>
 MRM_D void col_transform(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const R* Ts, bool tsm, int k0, int nc,
                          int* err) {
-  const int nl = rd.nl, ny = rd.ny, nys = rd.nys, phs = rd.phs, lgct = rd.lgct;
+  const int nl = rd.nl, ny = rd.ny, nys = rd.nys, lgct = rd.lgct;
   const int ph = (rd.px >> 1) + 1, ntile = (ph + (1 << lgct) - 1) >> lgct;
   const int plane = col_plane(1 << LGN, lgct), nplane = nl * 3;
-  (void)err;
-  // the task's tile of M^: plane lc at ((lc*ntile + tile)*nys + j)*T + c
-  const Cx<R>* src = rd.specx + ((size_t)(k0 >> lgct) * nys << lgct);
-  const size_t src_plane = (size_t)ntile * nys << lgct;
-  auto ld_g = [&](int lc, int c, int j, Cx<R>* v) {
-    if (j >= ny) {
-#pragma unroll
-      for (int k = 0; k < CP; ++k) v[k] = Cx<R>{(R)0, (R)0};
-      return;
-    }
-    MRM_CHECK((long long)(k0 >> lgct) * nys * (1 << lgct) + (long long)lc * src_plane + ((long long)j << lgct) + c +
-                      CP <=
-                  (long long)nplane * src_plane,
-              420, j);
-    ld_cp<R, CP>(src + lc * src_plane + ((size_t)j << lgct) + c, v);
-  };
-  auto ld_s = [&](int lc, int c, int j, Cx<R>* v) { ld_cp<R, CP>(A + lc * plane + ((j + (j >> 3)) << lgct) + c, v); };
-  auto st_s = [&](int lc, int c, int j, const Cx<R>* v) {
-    st_cp<R, CP>(A + lc * plane + ((j + (j >> 3)) << lgct) + c, v);
-  };
-  auto st_g = [&](int lc, int c, int j, const Cx<R>* v) {
-    if (j >= ny) return;
-    Cx<R>* d = rd.spech + ((size_t)lc * ny + j) * phs + k0 + c;
-    if (!MRM_CHECK(((long long)lc * ny + j) * phs + k0 + c < (long long)nplane * ny * phs, 440, j)) return;
-    if (CP == 1 || c + 1 < nc) st_cp<R, CP>(d, v);
-    else d[0] = v[0];  // the last column of a short tile
-  };
-  ip_fft_fwd<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_g, ld_s, st_s);
+  const ColTileIn<R> tile{rd.specx + ((size_t)(k0 >> lgct) * nys << lgct), (size_t)ntile * nys << lgct, lgct, ny};
+  const ColSmem<R> sm{A, plane, lgct};
+  const ColRowsOut<R> rows{rd.spech + k0, ny, rd.phs};
+  MRM_CHECK((long long)(k0 + nc) <= ph && nys >= ny, 420, k0);
+  ip_fft_fwd<R, LGN, HALF, BLOCK>(lgct, nc, nplane, tws, tile, sm);
   if (nl <= 2) {
     if (nl == 1) col_product<R, PACKED, 1, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
     else col_product<R, PACKED, 2, BLOCK>(rd, A, A, Ts, tsm, k0, nc, err);
     __syncthreads();
-    ip_fft_inv<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_s, st_s, st_g);
+    ip_fft_inv<R, LGN, HALF, BLOCK>(lgct, nc, nplane, tws, sm, rows);
   } else {
     // three or more layers: the product goes to the second buffer
     Cx<R>* O = A + col_buf_count(1 << LGN, lgct, nplane);
     col_product<R, PACKED, 0, BLOCK>(rd, A, O, Ts, tsm, k0, nc, err);
     __syncthreads();
-    auto ld_o = [&](int lc, int c, int j, Cx<R>* v) { ld_cp<R, CP>(O + lc * plane + ((j + (j >> 3)) << lgct) + c, v); };
-    auto st_o = [&](int lc, int c, int j, const Cx<R>* v) {
-      st_cp<R, CP>(O + lc * plane + ((j + (j >> 3)) << lgct) + c, v);
-    };
-    ip_fft_inv<R, LGN, CP, HALF, BLOCK>(lgct, nc, nplane, tws, ld_o, st_o, st_g);
+    const ColSmem<R> so{O, plane, lgct};
+    ip_fft_inv<R, LGN, HALF, BLOCK>(lgct, nc, nplane, tws, so, rows);
   }
 }
 
 template <typename R, int LGN, bool PACKED, int BLOCK>
 MRM_D void col_transform_any(const RunDev<R>& rd, Cx<R>* A, const Cx<R>* tws, const R* Ts, bool tsm, int k0, int nc,
                              int* err) {
-  // (two columns per thread measured slower at the tuned shapes: fewer,
-  // unevenly shared butterflies per pass)
-  if (rd.py >= 2 * rd.ny) col_transform<R, LGN, PACKED, 1, true, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
-  else col_transform<R, LGN, PACKED, 1, false, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
+  if (rd.py >= 2 * rd.ny) col_transform<R, LGN, PACKED, true, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
+  else col_transform<R, LGN, PACKED, false, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err);
 }
 
 template <typename R, bool PACKED, int BLOCK, int MINB>
