@@ -164,6 +164,16 @@ int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int 
 int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double hg, double velocity, double x0,
                            double t0, double bit_time, uint64_t pattern, int nbits);
 
+/* Cubic magnetocrystalline anisotropy on `layer` (get_cubic_hk,
+ * field.f90:377-395; set up by construct_hk_direction with k_cubic,
+ * construct_grain.f90:1620-1625, which then drops the uniaxial axis):
+ * cubic_axis is the reference's cubic_axis(3,3,N) (column-major: lab
+ * component k of crystal axis i of grain n at cubic_axis[k + 3*i + 9*n]); the
+ * layer's hk(1), hk(2) of mrm_gpu_upload_layer act as K1, K2 (Oe) and its
+ * uniaxial axes are ignored.  NULL returns the layer to uniaxial anisotropy.
+ * Call after mrm_gpu_upload_layer (and again after a re-upload). */
+int mrm_gpu_set_cubic_axes(mrm_gpu* h, int layer, const double* cubic_axis);
+
 /* Thermal (Brown) field of `layer` at `temperature` K (get_thermal,
  * field.f90:397-436).  The normals come from a counter-based Philox stream
  * keyed by `seed` (Philox4x64-10 for MRM_FP64 handles, Philox4x32-10 for

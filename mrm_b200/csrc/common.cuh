@@ -62,6 +62,9 @@ struct LayerDev {
   const int* lnbr;
   const R* lcoef;
   const V4<R>* xst;  // lattice form of the intralayer exchange: coef of (j-1, i-1, i+1, j+1)
+  // cubic anisotropy (null: uniaxial): per grain the crystal axes a1, a2, a3 in
+  // lab coordinates as 3 records, a1's w = hk_scale * Ms (energy term)
+  const V4<R>* cax;
   const R* ucol;     // columnar form of the interlayer coupling (grain n <-> grain n)
   const R* lcol;
   double hdir[3];

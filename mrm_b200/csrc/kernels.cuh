@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   }
   const bool pow2x = (nx & (nx - 1)) == 0;
   const int lgnx = __ffs(nx) - 1;
+  const bool cubic = GEN && L.cax != nullptr;
 
   double rec[stats ? kNPart : 1];
 #pragma unroll
@@ -513,7 +514,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     // h = h_app + h_demag + H_uni + H_ex (+ interlayer)   (field.f90:201,211-220)
     R hx = apx + hdx, hy = apy + hdy, hz = apz + hdz;
     R e_k;
-    {
+    if (GEN && cubic) {
+      // get_cubic_hk (field.f90:377-395): a_i = m . e_i,
+      // h = -sum_i e_i a_i (K1 (a_j^2 + a_k^2) + K2 a_j^2 a_k^2) with K = pa.w, pb.y
+      // (hk_scale folded in); the energy keeps the reference's factors (:392-394)
+      const V4<R> c1 = L.cax[3 * n], c2 = L.cax[3 * n + 1], c3 = L.cax[3 * n + 2];
+      const R a1 = c1.x * mf.x + c1.y * mf.y + c1.z * mf.z;
+      const R a2 = c2.x * mf.x + c2.y * mf.y + c2.z * mf.z;
+      const R a3 = c3.x * mf.x + c3.y * mf.y + c3.z * mf.z;
+      const R s1 = a1 * a1, s2 = a2 * a2, s3 = a3 * a3;
+      const R k1 = pa.w, k2 = pb.y;
+      const R d1 = a1 * (k1 * (s2 + s3) + k2 * s2 * s3);
+      const R d2 = a2 * (k1 * (s1 + s3) + k2 * s1 * s3);
+      const R d3 = a3 * (k1 * (s1 + s2) + k2 * s1 * s2);
+      hx -= c1.x * d1 + c2.x * d2 + c3.x * d3;
+      hy -= c1.y * d1 + c2.y * d2 + c3.y * d3;
+      hz -= c1.z * d1 + c2.z * d2 + c3.z * d3;
+      e_k = (R)0.5 * (k1 * (s1 * s2 + s1 * s3 + s2 * s3) + k2 * s1 * s2 * s3) * c1.w * mse;
+    } else {
       // get_uni_hk (field.f90:366-375); pa.w = Hk1*hk_scale, pb.y = Hk2*hk_scale
       const R hks = mf.x * pa.x + mf.y * pa.y + mf.z * pa.z;
       const R yy = (R)1 - hks * hks;

@@ -49,6 +49,7 @@ struct LayerBufs {
   int *lidx = nullptr, *lnbr = nullptr;
   void* lcoef = nullptr;
   void* xst = nullptr;   // V4<R> lattice exchange coefficients (null: CSR form)
+  void* cax = nullptr;   // V4<R> x 3 per grain: cubic crystal axes (null: uniaxial)
   void* ucol = nullptr;  // R columnar interlayer coefficients (null: CSR form)
   void* lcol = nullptr;
   double hdir[3] = {0, 0, 0};
@@ -118,6 +119,7 @@ struct Engine {
   int cap_stats[2] = {0, 0};
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
   bool has_head = false;             // a run has a layer under the write head (general kernels)
+  bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -427,6 +429,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.lnbr = b.lnbr;
     o.lcoef = static_cast<const R*>(b.lcoef);
     o.xst = static_cast<const V4<R>*>(b.xst);
+    o.cax = static_cast<const V4<R>*>(b.cax);
     o.ucol = static_cast<const R*>(b.ucol);
     o.lcol = static_cast<const R*>(b.lcol);
     for (int a = 0; a < 3; ++a) o.hdir[a] = b.hdir[a];
@@ -574,8 +577,12 @@ int build_tables(Engine* e) {
   e->nrt = (int)rt.size();
   e->nct = (int)ct.size();
   e->has_head = false;
+  e->has_cubic = false;
   for (auto* r : e->runs)
-    for (int l = 0; l < r->nl; ++l) e->has_head = e->has_head || r->L[l].func == kFuncHead;
+    for (int l = 0; l < r->nl; ++l) {
+      e->has_head = e->has_head || r->L[l].func == kFuncHead;
+      e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
+    }
   e->nst = (int)stt.size();
   if (e->nst > e->st_cap) {
     dfree(e->d_stasks);
@@ -628,7 +635,7 @@ template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
   // the general kernels for the semi-implicit pushes and write heads
-  const bool gen = (flags & kFlagBoris) || e->has_head;
+  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic;
   if (stats) {
     const int i = stage == kPred ? 0 : 1;
     RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
@@ -1020,7 +1027,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
-    dfree(b.xst); dfree(b.ucol); dfree(b.lcol);
+    dfree(b.xst); dfree(b.ucol); dfree(b.lcol); dfree(b.cax);
   }
 }
 
@@ -1102,7 +1109,7 @@ int upload_csr(mrm_gpu* r, int n, const int32_t* index, const int32_t* grain, co
 
 // host copies of ms_scale per layer (neighbour scaling of exchange coefficients)
 struct HostLayerCache {
-  std::vector<double> ms_scale;
+  std::vector<double> ms_scale, ms, hk_scale;
 };
 std::map<const mrm_gpu*, std::vector<HostLayerCache>>& host_cache() {
   static std::map<const mrm_gpu*, std::vector<HostLayerCache>> m;
@@ -1156,6 +1163,8 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
   auto& hc = host_cache()[r];
   hc.resize(MRM_MAX_LAYERS);
   hc[l].ms_scale.assign(ms_scale, ms_scale + n);
+  hc[l].ms.assign(ms, ms + n);
+  hc[l].hk_scale.assign(hk_scale, hk_scale + n);
   dfree(b.xst);
   if (hxi && hxg && hx) {
     int rc = upload_csr<R>(r, n, hxi, hxg, hx, ms_scale, n, &b.xidx, &b.xnbr, &b.xcoef);
@@ -1310,6 +1319,28 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
 }
 
 thread_local std::string g_create_err;
+
+template <typename R>
+int set_cubic_t(mrm_gpu* h, int layer, const double* cubic_axis) {
+  std::string* errp = &h->err;
+  LayerBufs& b = h->L[layer];
+  const int n = b.n;
+  const HostLayerCache& hc = host_cache()[h][layer];
+  std::vector<R> v(12 * (size_t)n);
+  for (int g = 0; g < n; ++g) {
+    const double hs = hc.hk_scale[g] > 0.0 ? hc.hk_scale[g] : 0.0;  // get_cubic_hk returns 0 for hk_scale <= 0
+    for (int i = 0; i < 3; ++i) {
+      for (int k = 0; k < 3; ++k) v[12 * (size_t)g + 4 * i + k] = (R)cubic_axis[9 * (size_t)g + 3 * i + k];
+      v[12 * (size_t)g + 4 * i + 3] = (R)(i == 0 ? hs * hc.ms[g] : 0.0);
+    }
+  }
+  if (!b.cax) {
+    int rc = dmalloc(errp, &b.cax, sizeof(R) * 12 * (size_t)n);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpy(b.cax, v.data(), sizeof(R) * 12 * (size_t)n, cudaMemcpyHostToDevice));
+  return MRM_OK;
+}
 
 }  // namespace
 
@@ -1595,6 +1626,25 @@ int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double h
   b.hd_nbits = nbits;
   h->eng->desc_dirty = true;
   h->eng->tables_dirty = true;  // the row kernel's shared memory grows by the head table
+  return MRM_OK;
+}
+
+int mrm_gpu_set_cubic_axes(mrm_gpu* h, int layer, const double* cubic_axis) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  if (!h->L[layer].uploaded) return set_err(&h->err, MRM_ERR_STATE, "upload layer %d first", layer);
+  std::string* errp = &h->err;
+  CK(cudaSetDevice(h->eng->dev));
+  if (!cubic_axis) {
+    dfree(h->L[layer].cax);
+  } else {
+    int rc = h->g.precision == MRM_FP64 ? set_cubic_t<double>(h, layer, cubic_axis)
+                                        : set_cubic_t<float>(h, layer, cubic_axis);
+    if (rc) return rc;
+  }
+  h->spec_valid = false;
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the general kernels take the cubic layers
   return MRM_OK;
 }
 

@@ -69,6 +69,8 @@ class _RunMixin:
                                        lay.scale)
             if getattr(lay, "head", None):
                 self.set_head_field(l, **lay.head)
+            if getattr(lay, "cubic_axis", None) is not None:
+                self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
         if medium.m0 is not None:
             for l, m in enumerate(medium.m0):
@@ -117,6 +119,17 @@ class _RunMixin:
     def set_head_field(self, layer, gap, z, hg, velocity, x0, t0, bit_time, pattern, nbits):
         self._check(_lib.load().mrm_gpu_set_head_field(self.h, layer, gap, z, hg, velocity, x0, t0,
                                                        bit_time, int(pattern), int(nbits)))
+
+    def set_cubic_axes(self, layer, cubic_axis):
+        """Cubic anisotropy on `layer`: cubic_axis (N,3,3), row i = crystal axis i in
+        lab coordinates (None: back to uniaxial)."""
+        if cubic_axis is None:
+            self._check(_lib.load().mrm_gpu_set_cubic_axes(self.h, layer, None))
+            return
+        a = f64(cubic_axis)
+        if a.shape != (self.medium.layers[layer].N, 3, 3):
+            raise ValueError("cubic_axis must be (N, 3, 3)")
+        self._check(_lib.load().mrm_gpu_set_cubic_axes(self.h, layer, fptr(a)))
 
     def set_thermal(self, layer, on, temperature, seed):
         self._check(_lib.load().mrm_gpu_set_thermal(self.h, layer, 1 if on else 0,

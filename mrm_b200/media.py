@@ -78,6 +78,9 @@ class Layer:
     # x0, t0, bit_time, pattern, nbits) in cm, Oe, s (include/mrm_gpu.h
     # mrm_gpu_set_head_field)
     head: Optional[dict] = None
+    # cubic anisotropy instead of uniaxial (field.f90:377-395): (N,3,3), row i
+    # = crystal axis i of the grain in lab coordinates; hk holds K1, K2 as fields
+    cubic_axis: Optional[np.ndarray] = None
 
     @property
     def N(self) -> int:
@@ -202,6 +205,25 @@ def make_layer(rng, nx, ny, dx, dy, dz, ms, hk, k_sigma, k_ang_deg, hex_oe, alph
         g2c_index=g2c_index, g2c=g2c,
         hx_index=hx_index, hx_grain=hx_grain, hx=hx,
     )
+
+
+def cubic_frames(rng: np.random.Generator, n: int) -> np.ndarray:
+    """(n,3,3) uniformly random orthonormal crystal frames (rows = axes)."""
+    q, r = np.linalg.qr(rng.standard_normal((n, 3, 3)))
+    q *= np.sign(np.diagonal(r, axis1=1, axis2=2))[:, None, :]
+    return np.ascontiguousarray(np.transpose(q, (0, 2, 1)))
+
+
+def cubic_medium(side: int, *, k1_oe: float = 4000.0, k2_oe: float = 1000.0, seed: int = 1,
+                 temperature: float = 0.0, boundary: int = 1, hex_oe: float = 500.0) -> Medium:
+    """M(H) medium of the 4,096/65,536-grain kind with cubic anisotropy:
+    random crystal frames per grain, K1 and K2 as fields (hk(1), hk(2))."""
+    med = mh_medium(side, temperature=temperature, boundary=boundary, seed=seed, hex_oe=hex_oe)
+    lay = med.layers[0]
+    rng = np.random.default_rng(seed + 1000)
+    lay.cubic_axis = cubic_frames(rng, lay.N)
+    lay.hk = np.stack([np.full(lay.N, k1_oe), np.full(lay.N, k2_oe)], axis=1)
+    return med
 
 
 def columnar_coupling(n: int, coef_oe: float):

@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -101,6 +101,12 @@ module mrm_gpu_m
       integer(C_INT), value :: layer, nbits
       real(C_DOUBLE), value :: gap, z, hg, velocity, x0, t0, bit_time
       integer(C_INT64_T), value :: pattern
+    end function
+    integer(C_INT) function c_set_cubic_axes(h, layer, cubic_axis) bind(C, name="mrm_gpu_set_cubic_axes")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer
+      real(C_DOUBLE), intent(in) :: cubic_axis(3, 3, *)
     end function
     integer(C_INT) function c_set_thermal(h, layer, on, temperature, seed) bind(C, name="mrm_gpu_set_thermal")
       import :: C_INT, C_PTR, C_DOUBLE, C_INT64_T
@@ -239,6 +245,14 @@ contains
     integer(C_INT64_T), intent(in) :: pattern
     ok_p = ok(c_set_head_field(h, int(layer - 1, C_INT), gap, z, hg, velocity, x0, t0, bit_time, pattern, &
                                int(nbits, C_INT)))
+  end function
+
+  ! cubic anisotropy on `layer` from field(il)%cubic_axis (include/mrm_gpu.h mrm_gpu_set_cubic_axes)
+  logical function gpu_set_cubic_axes(h, layer, cubic_axis) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: cubic_axis(:, :, :)
+    ok_p = ok(c_set_cubic_axes(h, int(layer - 1, C_INT), cubic_axis))
   end function
 
   logical function gpu_set_thermal(h, layer, on, temperature, seed) result(ok_p)

@@ -444,6 +444,10 @@ struct FFT2 {
 struct Layer {
   int N = 0;
   std::vector<double> ms, vol, axis, hk, hk_scale, ms_scale, alpha_scale;
+  // cubic anisotropy (field.f90:377-395): cubic_axis(3,3,N), lab component k of
+  // crystal axis i of grain n at cax[k + 3 i + 9 n]; empty: uniaxial layer
+  // (construct_grain.f90:1620-1625 keeps one of the two per layer)
+  std::vector<double> cax;
   double alpha = 1.0, gamma = 1.76e7, floor_ms = 0.01;
   std::vector<int> hx_idx, hx_nbr;  // CSR: hx_idx[N+1] cumulative, hx_nbr 0-based
   std::vector<double> hx;
@@ -658,8 +662,27 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
       double en = -(mn[0] * (hd[0] + ha[0]) + mn[1] * (hd[1] + ha[1]) + mn[2] * (hd[2] + ha[2])) *
                   Ly.ms[n] * Ly.ms_scale[n];
       double h[3] = {ha[0] + hd[0], ha[1] + hd[1], ha[2] + hd[2]};
-      // get_uni_hk field.f90:366-375
-      if (Ly.hk_scale[n] > 0.0) {
+      // get_cubic_hk field.f90:377-395: direction cosines d1 in the crystal
+      // frame, h = -hk_scale * A d3, d3_i = d1_i (K1 (d1_j^2 + d1_k^2) + K2 d1_j^2 d1_k^2);
+      // the energy term keeps the reference's factors as written (:392-394)
+      if (!Ly.cax.empty() && Ly.hk_scale[n] > 0.0) {
+        const double* A = &Ly.cax[9 * n];
+        double d1[3], d2[3], d3[3];
+        for (int i = 0; i < 3; ++i) {
+          d1[i] = A[3 * i] * mn[0] + A[3 * i + 1] * mn[1] + A[3 * i + 2] * mn[2];
+          d2[i] = d1[i] * d1[i];
+        }
+        const double K1 = Ly.hk[2 * n], K2 = Ly.hk[2 * n + 1], hs = Ly.hk_scale[n];
+        d3[0] = d1[0] * (K1 * (d2[1] + d2[2]) + K2 * d2[1] * d2[2]);
+        d3[1] = d1[1] * (K1 * (d2[0] + d2[2]) + K2 * d2[0] * d2[2]);
+        d3[2] = d1[2] * (K1 * (d2[0] + d2[1]) + K2 * d2[0] * d2[1]);
+        for (int k = 0; k < 3; ++k) h[k] -= (A[k] * d3[0] + A[k + 3] * d3[1] + A[k + 6] * d3[2]) * hs;
+        en += 0.5 * hs * Ly.ms[n] *
+              (K1 * (d2[0] * d2[1] + d2[0] * d2[2] + d2[1] * d2[2]) + K2 * d2[0] * d2[1] * d2[2]) * hs * Ly.ms[n] *
+              Ly.ms_scale[n];
+      }
+      // get_uni_hk field.f90:366-375 (no uniaxial axis on a cubic layer)
+      if (Ly.cax.empty() && Ly.hk_scale[n] > 0.0) {
         const double* k = &Ly.axis[3 * n];
         double hks = mn[0] * k[0] + mn[1] * k[1] + mn[2] * k[2];
         double yy = 1.0 - hks * hks;
@@ -1145,6 +1168,16 @@ int orc_set_field_function(void* h, int l, const double* dir, int func, double a
   Ly.func = func; Ly.amp = amp; Ly.fgamma = g; Ly.phase = phase; Ly.param = param;
   Ly.duty = std::max(0.0, std::min(1.0, duty)); Ly.moddepth = std::max(0.0, std::min(1.0, moddepth));
   Ly.dc = dc; Ly.scale = scale;
+  return 0;
+}
+
+// cubic axes of layer l (NULL: back to uniaxial); layout of Layer::cax
+int orc_set_cubic_axes(void* h, int l, const double* cax) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  if (!cax) Ly.cax.clear();
+  else Ly.cax.assign(cax, cax + 9 * (size_t)Ly.N);
   return 0;
 }
 

@@ -53,6 +53,7 @@ def lib():
         L.orc_set_thermal.argtypes = [vp, i, i, d, i, C.c_longlong]
         L.orc_set_field_function.argtypes = [vp, i, P(d), i, d, d, d, d, d, d, d, d]
         L.orc_set_head_field.argtypes = [vp, i, d, d, d, d, d, d, d, u64, i]
+        L.orc_set_cubic_axes.argtypes = [vp, i, P(d)]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
         L.orc_get_field.argtypes = [vp, i, P(d)]
@@ -213,6 +214,11 @@ class OracleSim:
                                           hd["t0"], hd["bit_time"], int(hd["pattern"]), int(hd["nbits"]))
                 assert rc == 0
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
+            cub = getattr(lay, "cubic_axis", None)
+            if cub is not None:
+                ca = f64(cub)
+                assert ca.shape == (lay.N, 3, 3)
+                assert L.orc_set_cubic_axes(self.h, l, _p(ca)) == 0
         for l, lay in enumerate(medium.layers):
             for side, cpl in ((0, lay.uhx), (1, lay.lhx)):
                 if cpl is not None:
