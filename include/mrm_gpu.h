@@ -82,6 +82,7 @@ typedef struct mrm_gpu_stats {
   double have_l[MRM_MAX_LAYERS][3], mms_l[MRM_MAX_LAYERS][3];
   double vol_l[MRM_MAX_LAYERS], msvol_l[MRM_MAX_LAYERS];
   int64_t nup_l[MRM_MAX_LAYERS];
+  double errmx1_l[MRM_MAX_LAYERS]; /* max |dm|^2 of the last stage per layer */
 } mrm_gpu_stats;
 
 typedef struct mrm_gpu mrm_gpu;     /* one medium realisation (a "run") */
@@ -209,6 +210,20 @@ int mrm_gpu_enqueue_steps(mrm_gpu* h, int nsteps, double dt, int llg_type);
 int mrm_gpu_read_stats(mrm_gpu* h, mrm_gpu_stats* out);
 /* The cudaStream_t (as void*) the handle launches on, for event timing. */
 int mrm_gpu_stream(const mrm_gpu* h, void** stream);
+
+/* nsteps iterations of llg()'s loop with the adaptive time step (dt_frac != 0;
+ * llg.f90:240-269, get_fields :363-388, push_m :1195-1271, set_llg :1452-1486):
+ * each step evaluates the field at t, sets dt = min(dt_max, min over layers
+ * (1+alpha^2)/((1+alpha) gamma) dt_frac / max(1, max |h + hthm/sqrt(dt*max_dmdt)|)),
+ * takes the step at dt*max_dmdt and, while the first layer (in order) whose
+ * rotation acos(1 - max|dm|^2/2) exceeds max_dm[layer] (radians) says so,
+ * retries it from the saved state with max_dmdt *= 0.9/ratio; then
+ * dt = dt*max_dmdt, the next max_dmdt follows push_m, t advances by dt.
+ * *dt and *max_dmdt are llgp%dt and llgp%max_dmdt, carried from call to call
+ * (start: the run's dt, 1).  Host-driven, a few synchronisations per step; a
+ * handle of its own (not in a batch).  out: the stats of the last step. */
+int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, double dt_max,
+                          const double* max_dm, double* dt, double* max_dmdt, mrm_gpu_stats* out);
 
 /* Kernel shapes of the engine a handle runs in (a batch run: the batch's).
  * row_shape / col_shape index the compiled row / column kernel shapes

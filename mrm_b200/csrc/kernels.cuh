@@ -27,7 +27,10 @@
 namespace mrm {
 
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
-enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16 };
+enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32 };
+// kFlagStoredField (kPred): the push uses the stored field L.hf instead of the
+// field of m_n -- push_m's retry after a rejected adaptive step, whose field
+// is still the one of the rejected predicted state (llg.f90:1205-1266)
 // llg_type -3 (Heun): kPred + kCorr.  llg_type -2: kPred with kFlagBoris |
 // kFlagMid (semi-implicit push over dt/2) then kCorr with the same flags (field
 // at t+dt/2 on the predicted state, push of m_n over dt).  llg_type 2: kPred
@@ -571,6 +574,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     hx += ex + vx;
     hy += ey + vy;
     hz += ez + vz;
+    if (STAGE == kPred && (flags & kFlagStoredField)) {
+      const V4<R> hs = L.hf[n];
+      hx = hs.x;
+      hy = hs.y;
+      hz = hs.z;
+    }
     if (store_field) L.hf[n] = V4<R>{hx, hy, hz, (R)0};
     if (STAGE == kEval) {
       L.hd[n] = V4<R>{hdx, hdy, hdz, (R)0};
@@ -1051,6 +1060,7 @@ struct StatsDev {
   double mave_l[kMaxLayers][3], mvar_l[kMaxLayers][3], have_l[kMaxLayers][3], mms_l[kMaxLayers][3];
   double vol_l[kMaxLayers], msvol_l[kMaxLayers];
   long long nup_l[kMaxLayers];
+  double errmx1_l[kMaxLayers];
 };
 
 // FP64 reduction of each run's per-task stats records into StatsDev; one
@@ -1102,6 +1112,7 @@ __global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __
     st.vol_l[l] = V;
     st.msvol_l[l] = on ? acc[l][kSlotW] : 0.0;
     st.nup_l[l] = on ? (long long)acc[l][kSlotNup] : 0;
+    st.errmx1_l[l] = on ? acc[l][kSlotMaxD2] : 0.0;
     if (on && V > 0) {
       for (int a = 0; a < 3; ++a) {
         st.mave[a] += V * st.mave_l[l][a] / vt;

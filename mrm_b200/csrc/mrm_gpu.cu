@@ -56,7 +56,7 @@ struct LayerBufs {
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
   int func = 0;
   double amp = 0, fgamma = 0, phase = 0, param = 0, duty = 0, moddepth = 0, dc = 0;
-  double temperature = 0.0, gamma = 1.76e7;
+  double temperature = 0.0, gamma = 1.76e7, alpha = 0.1;
   int thermal = 0;
   double hd_gap = 0, hd_z = 1, hd_hg = 0, hd_v = 0, hd_x0 = 0, hd_t0 = 0, hd_tbit = 1;
   unsigned long long hd_bits = 0;
@@ -120,6 +120,7 @@ struct Engine {
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
   bool has_head = false;             // a run has a layer under the write head (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
+  bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -658,7 +659,7 @@ cudaError_t launch_col_e(Engine* e, int istep, int flags, bool pdl = true) {
 // llg_type -3 (Heun) and -2 (semi-implicit midpoint): two field evaluations
 // per step; llg_type 2 (semi-implicit): one, then the commit of the new state
 template <typename R>
-cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type) {
+cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type, bool stored = false) {
   cudaError_t ce = cudaSuccess;
   auto acc = [&](cudaError_t x) { if (ce == cudaSuccess) ce = x; };
   const int f = llg_type == 2 ? kFlagBoris : llg_type == -2 ? (kFlagBoris | kFlagMid) : 0;
@@ -672,7 +673,7 @@ cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type) {
                         static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_stasks, i, 0));
       continue;
     }
-    acc(launch_row_e<R>(e, kPred, false, i, f));
+    acc(launch_row_e<R>(e, kPred, false, i, f | ((stored && i == 0) ? kFlagStoredField : 0)));
     acc(launch_col_e<R>(e, i, 0));
     acc(launch_row_e<R>(e, kCorr, last, i, f | lf));
     acc(launch_col_e<R>(e, i, 0));
@@ -907,12 +908,13 @@ int run_steps(Engine* e, int nsteps, int llg_type) {
   while (left > 0) {
     const int k = std::min(left, kGraphSteps);
     const bool stats = (left == k);  // reductions only on the call's last step
-    auto key = std::make_pair(k, (stats ? 1 : 0) + 2 * (llg_type + 3));
+    const bool stored = e->pred_stored && left == nsteps;
+    auto key = std::make_pair(k, (stats ? 1 : 0) + 2 * (llg_type + 3) + (stored ? 64 : 0));
     auto it = e->graphs.find(key);
     if (it == e->graphs.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-      cudaError_t le = enqueue_steps<R>(e, k, stats, llg_type);
+      cudaError_t le = enqueue_steps<R>(e, k, stats, llg_type, stored);
       cudaError_t ce = cudaStreamEndCapture(e->st, &g);
       if (le != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "launch in capture: %s", cudaGetErrorString(le));
       if (ce != cudaSuccess) return set_err(errp, MRM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
@@ -925,6 +927,7 @@ int run_steps(Engine* e, int nsteps, int llg_type) {
     CK(cudaGraphLaunch(it->second, e->st));
     left -= k;
   }
+  e->pred_stored = false;
   CK(cudaGetLastError());
   // mirror the device-side step counters
   for (auto* r : e->runs) {
@@ -987,6 +990,35 @@ __global__ void state_out_kernel(const V4<R>* __restrict__ src, double* __restri
   out[3 * i] = (double)v.x;
   out[3 * i + 1] = (double)v.y;
   out[3 * i + 2] = (double)v.z;
+}
+
+// ---------------- adaptive time step ----------------
+// max over a layer's grains of |h + hthm * dti|^2 (get_fields, llg.f90:375-382):
+// h the stored field of the last evaluation, hthm = sigma sqrt(T) N(0,1)^3 the
+// thermal draw of step `step` (the one the predictor takes); the maximum goes
+// to *out as the bits of a non-negative double (ordered like the values)
+template <typename R>
+__global__ void hmag_kernel(const RunDev<R>* __restrict__ runs, int slot, int layer, double dti, long long step,
+                            unsigned long long* __restrict__ out) {
+  const RunDev<R>& rd = runs[slot];
+  const LayerDev<R>& L = rd.L[layer];
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  double v2 = 0.0;
+  if (n < L.n) {
+    const V4<R> h = L.hf[n];
+    double x = h.x, y = h.y, z = h.z;
+    if (L.thermal) {
+      R gn[3];
+      thermal_normals(rd.seed, (unsigned long long)layer, (unsigned long long)step, (unsigned long long)n, gn);
+      const double s = (double)L.pb[n].w * sqrt(L.temperature) * dti;
+      x += s * (double)gn[0];
+      y += s * (double)gn[1];
+      z += s * (double)gn[2];
+    }
+    v2 = x * x + y * y + z * z;
+  }
+  for (int o = 16; o > 0; o >>= 1) v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v2));
 }
 
 // ---------------- run buffers ----------------
@@ -1197,6 +1229,7 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
   }
   b.gamma = gamma;
+  b.alpha = alpha;
   b.uploaded = true;
   r->spec_valid = false;
   r->eng->desc_dirty = true;
@@ -1838,6 +1871,112 @@ int mrm_gpu_step(mrm_gpu* h, int nsteps, double dt, int llg_type, mrm_gpu_stats*
     return MRM_ERR_DEVICE;
   }
   return MRM_OK;
+}
+
+// The reference's adaptive-dt loop (llg.f90:240-269 with get_fields :363-388 and
+// push_m :1203-1270), driven from the host one step at a time: field at t,
+// dt from the largest |h + hthm/sqrt(dt_prev)|, then the step at
+// dt*max_dmdt, retried from the saved state with a smaller max_dmdt while a
+// layer rotates further than max_dm.
+int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, double dt_max,
+                          const double* max_dm, double* dt, double* max_dmdt, mrm_gpu_stats* out) {
+  if (!h || !max_dm || !dt || !max_dmdt) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  if (nsteps < 1) return set_err(errp, MRM_ERR_ARG, "nsteps must be >= 1");
+  if (!(dt_frac > 0) || !(dt_max > 0) || !(*dt > 0) || !(*max_dmdt > 0))
+    return set_err(errp, MRM_ERR_ARG, "adaptive steps need dt_frac, dt_max, dt and max_dmdt > 0");
+  for (int l = 0; l < h->nl; ++l)
+    if (!(max_dm[l] > 0)) return set_err(errp, MRM_ERR_ARG, "max_dm[%d] must be > 0", l);
+  Engine* e = h->eng;
+  if (e->runs.size() != 1)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps run on a handle of its own, not in a batch");
+  int rc = plain_prepare(h, 0, h->dt, llg_type);
+  if (rc) return rc;
+  const size_t re = relem(h->g.precision), n = (size_t)h->g.nx * h->g.ny;
+  void* save = nullptr;
+  unsigned long long* d_hm = nullptr;
+  rc = dmalloc(errp, &save, (size_t)h->nl * n * 4 * re);
+  if (!rc) rc = dmalloc(errp, (void**)&d_hm, sizeof(unsigned long long) * MRM_MAX_LAYERS);
+  auto finish = [&](int code) {
+    dfree(save);
+    dfree(d_hm);
+    return code;
+  };
+  if (rc) return finish(rc);
+  mrm_gpu_stats st;
+  for (int it = 0; it < nsteps; ++it) {
+    const double t0 = h->t_base + (double)(h->step - h->step_base) * h->dt;
+    const long long s0 = h->step;
+    // get_fields: h at t, then dt from the largest |h + hthm*dti| (llg.f90:369-387)
+    rc = mrm_gpu_eval_field(h, t0, 0, nullptr);
+    if (rc) return finish(rc);
+    const double dti = 1.0 / std::sqrt(*dt * *max_dmdt);
+    unsigned long long hm[MRM_MAX_LAYERS];
+    if (cudaMemsetAsync(d_hm, 0, sizeof(hm), e->st) != cudaSuccess) return finish(set_err(errp, MRM_ERR_CUDA, "memset"));
+    for (int l = 0; l < h->nl; ++l) {
+      const unsigned blocks = (unsigned)((n + 255) / 256);
+      if (e->prec == MRM_FP64)
+        hmag_kernel<double><<<blocks, 256, 0, e->st>>>(static_cast<const RunDev<double>*>(e->d_runs), h->slot, l, dti,
+                                                       s0, d_hm + l);
+      else
+        hmag_kernel<float><<<blocks, 256, 0, e->st>>>(static_cast<const RunDev<float>*>(e->d_runs), h->slot, l, dti,
+                                                      s0, d_hm + l);
+    }
+    if (cudaMemcpyAsync(hm, d_hm, sizeof(hm), cudaMemcpyDeviceToHost, e->st) != cudaSuccess ||
+        cudaStreamSynchronize(e->st) != cudaSuccess)
+      return finish(set_err(errp, MRM_ERR_CUDA, "field magnitude: %s", cudaGetErrorString(cudaGetLastError())));
+    double ndt = 1e22;
+    for (int l = 0; l < h->nl; ++l) {
+      long long bits = (long long)hm[l];
+      double hmag = 0.0;
+      std::memcpy(&hmag, &bits, sizeof(hmag));
+      hmag = std::sqrt(hmag);
+      const LayerBufs& b = h->L[l];
+      const double fact1 = (1.0 + b.alpha * b.alpha) / ((1.0 + b.alpha) * b.gamma) * dt_frac;
+      ndt = std::min(ndt, std::min(dt_max, fact1 / std::max(1.0, hmag)));
+    }
+    *dt = ndt;
+    // push_m: the step at dt*max_dmdt, retried from the saved state (llg.f90:1205-1238)
+    for (int l = 0; l < h->nl; ++l)
+      if (cudaMemcpyAsync(static_cast<char*>(save) + l * n * 4 * re, h->L[l].m, n * 4 * re, cudaMemcpyDeviceToDevice,
+                          e->st) != cudaSuccess)
+        return finish(set_err(errp, MRM_ERR_CUDA, "state copy"));
+    double next = 1e22;
+    for (int attempt = 0;; ++attempt) {
+      if (attempt > 200) return finish(set_err(errp, MRM_ERR_DEVICE, "adaptive step: no accepted step after 200 retries"));
+      const double dts = *dt * *max_dmdt;
+      rc = mrm_gpu_step(h, 1, dts, llg_type, &st);
+      if (rc) return finish(rc);
+      bool too_far = false;
+      next = 1e22;
+      for (int l = 0; l < h->nl; ++l) {
+        const double r = std::acos(1.0 - 0.5 * st.errmx1_l[l]) / max_dm[l];
+        if (r > 1.0) {
+          *max_dmdt = 0.9 * *max_dmdt / r;
+          too_far = true;
+          break;
+        }
+        next = std::min(next, r < 2.0 / 3.0 ? std::min(2.0, *max_dmdt / (r + 1e-200)) : *max_dmdt);
+      }
+      if (!too_far) break;
+      // back to the state and time before the attempt
+      for (int l = 0; l < h->nl; ++l)
+        if (cudaMemcpyAsync(h->L[l].m, static_cast<char*>(save) + l * n * 4 * re, n * 4 * re,
+                            cudaMemcpyDeviceToDevice, e->st) != cudaSuccess)
+          return finish(set_err(errp, MRM_ERR_CUDA, "state copy"));
+      h->t_base = t0;
+      h->step_base = s0;
+      h->step = s0;
+      h->spec_valid = false;
+      e->desc_dirty = true;
+      e->pred_stored = true;  // the retry's predictor takes the rejected attempt's corrector field
+    }
+    if (next > 1e20) next = *max_dmdt;
+    *dt = *dt * *max_dmdt;  // llg.f90:268
+    *max_dmdt = next;
+  }
+  if (out) *out = st;
+  return finish(MRM_OK);
 }
 
 int mrm_gpu_set_shape(mrm_gpu* h, int row_shape, int col_shape, int cols_per_task) {

@@ -234,6 +234,18 @@ class GpuSim(_RunMixin):
         self._check(_lib.load().mrm_gpu_profile(self.h, int(reps), float(dt), fptr(out)))
         return out
 
+    def step_adaptive(self, nsteps: int, dt: float, max_dmdt: float = 1.0, llg_type: int = -3,
+                      dt_frac: float = 0.2, dt_max: float = 1e-8, max_dm=None):
+        """nsteps steps with the reference's adaptive dt (include/mrm_gpu.h
+        mrm_gpu_step_adaptive); returns (stats, dt, max_dmdt) for the next call."""
+        st = np.zeros(1, _lib.STATS_DTYPE)
+        md = f64(max_dm if max_dm is not None else [3.1415925] * self.medium.n_lay)
+        a, b = C.c_double(dt), C.c_double(max_dmdt)
+        self._check(_lib.load().mrm_gpu_step_adaptive(self.h, int(nsteps), int(llg_type), float(dt_frac),
+                                                      float(dt_max), fptr(md), C.byref(a), C.byref(b),
+                                                      st.ctypes.data))
+        return st[0], a.value, b.value
+
     def step(self, nsteps: int, dt: float, llg_type: int = -3, stats: bool = True):
         st = np.zeros(1, _lib.STATS_DTYPE) if stats else None
         self._check(_lib.load().mrm_gpu_step(self.h, int(nsteps), float(dt), int(llg_type),

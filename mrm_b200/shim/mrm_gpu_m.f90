@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -33,6 +33,7 @@ module mrm_gpu_m
     real(C_DOUBLE) :: mave_l(3, MAXL), mvar_l(3, MAXL), have_l(3, MAXL), mms_l(3, MAXL)
     real(C_DOUBLE) :: vol_l(MAXL), msvol_l(MAXL)
     integer(C_INT64_T) :: nup_l(MAXL)
+    real(C_DOUBLE) :: errmx1_l(MAXL)
   end type
 
   interface
@@ -107,6 +108,16 @@ module mrm_gpu_m
       type(C_PTR), value :: h
       integer(C_INT), value :: layer
       real(C_DOUBLE), intent(in) :: cubic_axis(3, 3, *)
+    end function
+    integer(C_INT) function c_step_adaptive(h, nsteps, llg_type, dt_frac, dt_max, max_dm, dt, max_dmdt, stats) &
+        bind(C, name="mrm_gpu_step_adaptive")
+      import :: C_INT, C_PTR, C_DOUBLE, mrm_stats_t
+      type(C_PTR), value :: h
+      integer(C_INT), value :: nsteps, llg_type
+      real(C_DOUBLE), value :: dt_frac, dt_max
+      real(C_DOUBLE), intent(in) :: max_dm(*)
+      real(C_DOUBLE), intent(inout) :: dt, max_dmdt
+      type(mrm_stats_t), intent(out) :: stats
     end function
     integer(C_INT) function c_set_thermal(h, layer, on, temperature, seed) bind(C, name="mrm_gpu_set_thermal")
       import :: C_INT, C_PTR, C_DOUBLE, C_INT64_T
@@ -253,6 +264,18 @@ contains
     integer, intent(in) :: layer
     real(C_DOUBLE), intent(in) :: cubic_axis(:, :, :)
     ok_p = ok(c_set_cubic_axes(h, int(layer - 1, C_INT), cubic_axis))
+  end function
+
+  ! iter steps of llg()'s adaptive loop (dt_frac /= 0): llgp%dt and llgp%max_dmdt
+  ! in and out, llgl(:)%max_dm in radians (include/mrm_gpu.h mrm_gpu_step_adaptive)
+  logical function gpu_step_adaptive(h, iter, llg_type, dt_frac, dt_max, max_dm, dt, max_dmdt, stats) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: iter, llg_type
+    real(C_DOUBLE), intent(in) :: dt_frac, dt_max, max_dm(:)
+    real(C_DOUBLE), intent(inout) :: dt, max_dmdt
+    type(mrm_stats_t), intent(out) :: stats
+    ok_p = ok(c_step_adaptive(h, int(iter, C_INT), int(llg_type, C_INT), dt_frac, dt_max, max_dm, dt, max_dmdt, &
+                              stats))
   end function
 
   logical function gpu_set_thermal(h, layer, on, temperature, seed) result(ok_p)

@@ -480,6 +480,7 @@ struct Stats {
   double mave_l[8][3], mvar_l[8][3], have_l[8][3], mms_l[8][3];
   double vol_l[8], msvol_l[8];
   long long nup_l[8];
+  double errmx1_l[8];
 };
 
 struct Sim {
@@ -839,9 +840,11 @@ static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, d
   *mmag1 = mm;
 }
 
-static void compute_stats(Sim* s, double errmx, double errmx1, double mmag, double energy) {
+static void compute_stats(Sim* s, double errmx, double errmx1, double mmag, double energy,
+                          const double* errmx1_l) {
   Stats& st = s->last;
   std::memset(&st, 0, sizeof(st));
+  for (int l = 0; l < s->nl; ++l) st.errmx1_l[l] = errmx1_l[l];
   st.t = s->t;
   st.step = s->step;
   double vtot = 0.0;
@@ -892,45 +895,109 @@ static void compute_stats(Sim* s, double errmx, double errmx1, double mmag, doub
   st.energy = energy;
 }
 
-// One pass of the llg() loop body (llg.f90:240-269) with push_m (llg.f90:1195-1271)
-// at fixed dt (fixed_dt_p: max_dmdt = 1, no retries).
-static void heun_or_boris_step(Sim* s, double dt, int type) {
+// push_m's passes (llg.f90:1207-1266) at step dt with the field and thermal
+// draw at t already in place: the new state is left in the other buffer (the
+// caller toggles `in`, llg.f90:1269); per-layer max |dm|^2 of the last pass in e1l.
+static void push_passes(Sim* s, double dt, int type, double* errmx, double* errmx1, double* mmag, double* e1l,
+                        double* energy) {
   const int nl = s->nl;
-  double energy = 0.0;
-  // get_fields(t): field + thermal at the current state (llg.f90:363-365)
-  get_field(s, s->t, s->in, &energy);
-  get_thermal(s);
   double dt_s = 1.0;
   int iter = 1;
   if (type < 0) {
     iter = 2;
     if (type > -3) dt_s = 0.5;
   }
-  double errmx = 0, errmx1 = 0, mmag = 0;
   while (iter > 0) {
-    errmx = 0; errmx1 = 0; mmag = 0;
+    *errmx = 0; *errmx1 = 0; *mmag = 0;
     for (int l = 0; l < nl; ++l) {
       double e0, e1, m1;
       push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
       double vs = 0;
       for (int n = 0; n < s->L[l].N; ++n) vs += s->L[l].vol[n];
-      mmag += m1 / vs;
-      errmx = std::max(errmx, std::sqrt(e0));
-      errmx1 = std::max(errmx1, e1);
+      *mmag += m1 / vs;
+      *errmx = std::max(*errmx, std::sqrt(e0));
+      *errmx1 = std::max(*errmx1, e1);
+      e1l[l] = e1;
     }
     iter -= 1;
     if (iter > 0) {
       // llg.f90:1262-1266: field at t+dt*dt_s on the predicted state, thermal reused
       s->in = 1 - s->in;
-      get_field(s, s->t + dt * dt_s, s->in, &energy);
+      get_field(s, s->t + dt * dt_s, s->in, energy);
       s->in = 1 - s->in;
       dt_s = 1.0;
     }
   }
+}
+
+// One pass of the llg() loop body (llg.f90:240-269) with push_m (llg.f90:1195-1271)
+// at fixed dt (fixed_dt_p: max_dmdt = 1, no retries).
+static void heun_or_boris_step(Sim* s, double dt, int type) {
+  double energy = 0.0;
+  // get_fields(t): field + thermal at the current state (llg.f90:363-365)
+  get_field(s, s->t, s->in, &energy);
+  get_thermal(s);
+  double errmx = 0, errmx1 = 0, mmag = 0, e1l[8] = {0};
+  push_passes(s, dt, type, &errmx, &errmx1, &mmag, e1l, &energy);
   s->in = 1 - s->in;  // llg.f90:1269
   s->t += dt;
   s->step += 1;
-  compute_stats(s, errmx, errmx1, mmag, energy);
+  compute_stats(s, errmx, errmx1, mmag, energy, e1l);
+}
+
+// The same with the adaptive time step (dt_frac != 0): get_fields picks dt from
+// the largest |h + hthm/sqrt(dt*max_dmdt)| (llg.f90:369-387); push_m retries
+// from the unchanged state with max_dmdt *= 0.9/rot_ratio while the first layer
+// (in order) whose rot_ratio = acos(1 - |dm|^2/2)/max_dm exceeds 1 says so, and
+// sets the next max_dmdt (llg.f90:1225-1253,1270); dt becomes the step taken
+// and t advances by it (llg.f90:268-269).
+static void adaptive_step(Sim* s, int type, double dt_frac, double dt_max, const double* max_dm, double* dt,
+                          double* max_dmdt) {
+  double energy = 0.0;
+  get_field(s, s->t, s->in, &energy);
+  get_thermal(s);
+  const double dti = 1.0 / std::sqrt(*dt * *max_dmdt);
+  double ndt = 1e22;
+  for (int l = 0; l < s->nl; ++l) {
+    const Layer& Ly = s->L[l];
+    double hmag = 0.0;
+    for (int n = 0; n < Ly.N; ++n) {
+      double v2 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double v = Ly.h[3 * n + a] + Ly.hthm[3 * n + a] * dti;
+        v2 += v * v;
+      }
+      hmag = std::max(hmag, v2);
+    }
+    hmag = std::sqrt(hmag);
+    const double fact1 = (1.0 + Ly.alpha * Ly.alpha) / ((1.0 + Ly.alpha) * Ly.gamma) * dt_frac;
+    const double fact0 = fact1 != 0.0 ? 0.0 : 1.0;
+    ndt = std::min(std::min(ndt, dt_max), fact1 / std::max(1.0, hmag) + fact0 * ndt);
+  }
+  *dt = ndt;
+  double errmx = 0, errmx1 = 0, mmag = 0, e1l[8] = {0}, next = 1e22;
+  while (true) {
+    push_passes(s, *dt * *max_dmdt, type, &errmx, &errmx1, &mmag, e1l, &energy);
+    bool too_far = false;
+    next = 1e22;
+    for (int l = 0; l < s->nl; ++l) {
+      const double r = std::acos(1.0 - 0.5 * e1l[l]) / max_dm[l];
+      if (r > 1.0) {
+        *max_dmdt = 0.9 * *max_dmdt / r;
+        too_far = true;
+        break;
+      }
+      next = std::min(next, r < 2.0 / 3.0 ? std::min(2.0, *max_dmdt / (r + 1e-200)) : *max_dmdt);
+    }
+    if (!too_far) break;
+  }
+  if (next > 1e20) next = *max_dmdt;
+  s->in = 1 - s->in;
+  *dt = *dt * *max_dmdt;
+  *max_dmdt = next;
+  s->t += *dt;
+  s->step += 1;
+  compute_stats(s, errmx, errmx1, mmag, energy, e1l);
 }
 
 }  // namespace orc
@@ -1261,6 +1328,17 @@ int orc_step(void* h, int nsteps, double dt, int type, double* stats_out, double
       for (int l = 0; l < s->nl; ++l)
         for (int a = 0; a < 3; ++a) traj[((size_t)k * s->nl + l) * 3 + a] = s->last.mave_l[l][a];
   }
+  if (stats_out) std::memcpy(stats_out, &s->last, sizeof(Stats));
+  return 0;
+}
+
+// nsteps adaptive steps (see adaptive_step); dt and max_dmdt carry llgp%dt and
+// llgp%max_dmdt from call to call; max_dm per layer in radians.
+int orc_step_adaptive(void* h, int nsteps, int type, double dt_frac, double dt_max, const double* max_dm, double* dt,
+                      double* max_dmdt, double* stats_out) {
+  Sim* s = static_cast<Sim*>(h);
+  if (!(type == -3 || type == 2 || type == -2)) return 2;
+  for (int k = 0; k < nsteps; ++k) adaptive_step(s, type, dt_frac, dt_max, max_dm, dt, max_dmdt);
   if (stats_out) std::memcpy(stats_out, &s->last, sizeof(Stats));
   return 0;
 }

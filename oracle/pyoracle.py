@@ -24,6 +24,7 @@ STATS_DTYPE = np.dtype([
     ("mave_l", "f8", (MAX_LAYERS, 3)), ("mvar_l", "f8", (MAX_LAYERS, 3)),
     ("have_l", "f8", (MAX_LAYERS, 3)), ("mms_l", "f8", (MAX_LAYERS, 3)),
     ("vol_l", "f8", MAX_LAYERS), ("msvol_l", "f8", MAX_LAYERS), ("nup_l", "i8", MAX_LAYERS),
+    ("errmx1_l", "f8", MAX_LAYERS),
 ])
 
 
@@ -61,6 +62,7 @@ def lib():
         L.orc_set_time.argtypes = [vp, d, C.c_longlong]
         L.orc_eval_field.argtypes = [vp, d]
         L.orc_step.argtypes = [vp, i, d, i, vp, vp]
+        L.orc_step_adaptive.argtypes = [vp, i, i, d, d, P(d), P(d), P(d), vp]
         L.orc_mt_u32.argtypes = [i, i, P(C.c_uint32)]
         L.orc_mt_state.argtypes = [i, P(C.c_uint32)]
         L.orc_mt_normals.argtypes = [i, i, P(d)]
@@ -276,6 +278,18 @@ class OracleSim:
 
     def eval_field(self, t: float):
         lib().orc_eval_field(self.h, t)
+
+    def step_adaptive(self, nsteps: int, dt: float, max_dmdt: float = 1.0, llg_type: int = -3,
+                      dt_frac: float = 0.2, dt_max: float = 1e-8, max_dm=None):
+        """nsteps adaptive steps; returns (stats, dt, max_dmdt) to pass to the next call."""
+        st = np.zeros(1, STATS_DTYPE)
+        md = f64(max_dm if max_dm is not None else [3.1415925] * self.medium.n_lay)
+        a, b = C.c_double(dt), C.c_double(max_dmdt)
+        rc = lib().orc_step_adaptive(self.h, nsteps, llg_type, dt_frac, dt_max, _p(md), C.byref(a), C.byref(b),
+                                     st.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"orc_step_adaptive failed rc={rc}")
+        return st[0], a.value, b.value
 
     def step(self, nsteps: int, dt: float, llg_type: int = -3, traj: bool = False):
         st = np.zeros(1, STATS_DTYPE)

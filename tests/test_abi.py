@@ -24,4 +24,6 @@ def test_library_exports_every_symbol(gpulib):
 
 
 def test_stats_layout():
-    assert _lib.STATS_DTYPE.itemsize == 8 * (2 + 9 + 4 + 4 * 24 + 3 * 8)
+    # t, step, mave/mvar/have, errmx/errmx1/mmag/energy, 4 x [8][3] per layer,
+    # vol_l, msvol_l, nup_l, errmx1_l
+    assert _lib.STATS_DTYPE.itemsize == 8 * (2 + 9 + 4 + 4 * 24 + 4 * 8)
