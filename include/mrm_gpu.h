@@ -101,9 +101,13 @@ const char* mrm_gpu_last_error(const mrm_gpu* h);
  * hk_scale/ms_scale/alpha_scale(N); alpha, gamma, floor_ms scalars;
  * grain2gridindex(0:N), grain2grid(2,ncell) (field.f90:22-23); intralayer
  * exchange hxgrainindex(0:N), hxgrain(nnz), hx(nnz) (field.f90:28-29), or
- * NULL for none.  This path requires one cell per grain on the nx*ny grid
- * (grains are nodes, construct_grain.f90:160-189) and returns
- * MRM_ERR_UNSUPPORTED for multi-cell grains. */
+ * NULL for none.  One cell per grain in grid order (grains are nodes,
+ * construct_grain.f90:160-189) runs the fused path; any other map (grains
+ * of several cells, empty cells; each cell in at most one grain) runs the
+ * grain-averaged form of get_mag / get_magnetostatic (data.f90:322-390,
+ * field.f90:438-517): two more launches per stage (the cells' demag and its
+ * grain average).  The state, field and demag arrays of the other calls stay
+ * per grain.  A write head needs one grain per cell. */
 int mrm_gpu_upload_layer(mrm_gpu* h, int layer, int n_grains, const double* ms,
                          const double* grain_vol, const double* uni_axis, const double* hk,
                          const double* hk_scale, const double* ms_scale,

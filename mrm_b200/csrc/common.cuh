@@ -65,6 +65,13 @@ struct LayerDev {
   // cubic anisotropy (null: uniaxial): per grain the crystal axes a1, a2, a3 in
   // lab coordinates as 3 records, a1's w = hk_scale * Ms (energy term)
   const V4<R>* cax;
+  // grains of several cells (null cgrain: one grain per cell in grid order):
+  // the cell's grain (-1: empty cell), each grain's cells (gcs[gci[g]..gci[g+1]),
+  // the first one is the grain's own), the grain-averaged demag per cell
+  const int* cgrain;
+  const int* gci;
+  const int* gcs;
+  V4<R>* hdm;
   const R* ucol;     // columnar form of the interlayer coupling (grain n <-> grain n)
   const R* lcol;
   double hdir[3];

@@ -27,7 +27,14 @@
 namespace mrm {
 
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
-enum Flags { kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32 };
+enum Flags {
+  kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32,
+  kFlagMapped = 64, kFlagDemagOnly = 128
+};
+// kFlagMapped (kPred, kCorr, kEval): the demag field comes from an earlier
+// evaluation's per-cell values averaged over each grain's cells (L.hdm; L.hd
+// with one grain per cell), not from this launch's inverse row transform.
+// kFlagDemagOnly (kEval): the inverse transforms' demag per cell (L.hd) only.
 // kFlagStoredField (kPred): the push uses the stored field L.hf instead of the
 // field of m_n -- push_m's retry after a rejected adaptive step, whose field
 // is still the one of the rejected predicted state (llg.f90:1205-1266)
@@ -301,7 +308,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const int base = row0 * nx;
   const int v4row = nx * (int)sizeof(V4<R>);
   const int rrow = nx * (int)sizeof(R);
-  const bool inverse = (STAGE != kInit) && demag;
+  const bool mapped = (STAGE != kInit) && (flags & kFlagMapped);
+  const bool inverse = (STAGE != kInit) && demag && !mapped;
 
   // bulk copy with the self-checks of the MRM_CHECKS build (source offset
   // within its array, destination within the dynamic shared memory, 16-byte
@@ -442,13 +450,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
   const R tfac = thermal ? (R)L.tfac : (R)0;
-  const bool store_field = (flags & kFlagStoreField) || STAGE == kEval;
+  // (a demag-only evaluation leaves L.hf alone: it holds the last stepping
+  // stage's field, which a retried adaptive step reads)
+  const bool store_field = (flags & kFlagStoreField) || (STAGE == kEval && !(flags & kFlagDemagOnly));
   // Write head: its field depends on the column and the time only.  The
   // stepping stages add it to the block's demag values in shared memory (zero
   // when demag is off), so their per-grain loop is the same with or without a
   // head; the evaluation stage keeps demag apart and reads a per-column table.
   const bool fold_head = (STAGE == kPred || STAGE == kCorr) && htab_off;
-  const bool use_hdr = demag || fold_head;
+  const bool use_hdr = !mapped && (demag || fold_head);
   if (STAGE != kInit && htab_off) {
     double xh, pol;
     head_state(L, t_stage, &xh, &pol);
@@ -499,7 +509,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const V4<R> mf = MF[q];
     const V4<R> pa = PA[q];
     R hdx = 0, hdy = 0, hdz = 0;
-    if (use_hdr) {
+    if (mapped) {
+      const V4<R> g = L.cgrain ? L.hdm[n] : L.hd[n];
+      hdx = g.x;
+      hdy = g.y;
+      hdz = g.z;
+    } else if (use_hdr) {
       hdx = hdr[(rr * 3 + 0) * rs + i];
       hdy = hdr[(rr * 3 + 1) * rs + i];
       hdz = hdr[(rr * 3 + 2) * rs + i];
@@ -592,7 +607,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     if (thermal) {
       if (STAGE == kPred) {
         R gn[3];
-        thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)n, gn);
+        // the grain's stream (one per grain, shared by its cells)
+        const int nt = L.cgrain ? max(0, L.cgrain[n]) : n;
+        thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)nt, gn);
         const R s = pb.w * tfac;
         htx = s * gn[0];
         hty = s * gn[1];
@@ -680,7 +697,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     outr[(rr * 3 + 2) * rs + i] = mse * mn.z;
 
     if constexpr (stats) {
-      const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 0}
+      const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 1}; (0, .., 0) on the extra cells of a grain
       const double v = pv.x, w = pv.z * pv.y * v;
       const double mx = mn.x, my = mn.y, mz = mn.z;
       rec[kSlotV] += v;
@@ -697,7 +714,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       rec[kSlotWM + 1] += w * my;
       rec[kSlotWM + 2] += w * mz;
       rec[kSlotW] += w;
-      if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += 1.0;
+      if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += pv.w;  // 1: counted grain record
       rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / (pv.z * pv.z));
       rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
       rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
@@ -1017,6 +1034,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
     case 11: col_transform_any<R, 11, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
     default: col_transform_any<R, 12, PACKED, BLOCK>(rd, A, tws, Ts, tsm, k0, nc, err); break;
   }
+}
+
+// Grain average of the evaluation stage's demag over each grain's cells,
+// written to every cell of the grain (get_magnetostatic, field.f90:449-470:
+// FP64 sum over the cells, divided by their count).  Block row y: run y /
+// kMaxLayers, layer y % kMaxLayers; layers with one grain per cell are skipped.
+template <typename R>
+__global__ void gather_demag_kernel(const RunDev<R>* __restrict__ runs, int nruns) {
+  const int r = blockIdx.y / kMaxLayers, l = blockIdx.y % kMaxLayers;
+  if (r >= nruns) return;
+  const RunDev<R>& rd = runs[r];
+  if (!rd.active || l >= rd.nl) return;
+  const LayerDev<R>& L = rd.L[l];
+  if (!L.cgrain) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  const int g = L.cgrain[c];
+  if (g < 0) return;
+  const int q0 = L.gci[g], q1 = L.gci[g + 1];
+  double x = 0.0, y = 0.0, z = 0.0;
+  for (int q = q0; q < q1; ++q) {
+    const V4<R> h = L.hd[L.gcs[q]];
+    x += (double)h.x;
+    y += (double)h.y;
+    z += (double)h.z;
+  }
+  const double k = (double)(q1 - q0);
+  L.hdm[c] = V4<R>{(R)(x / k), (R)(y / k), (R)(z / k), (R)0};
 }
 
 // llg_type 2: the predictor buffer holds m_{n+1} after the single push; copy

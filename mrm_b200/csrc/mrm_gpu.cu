@@ -52,6 +52,11 @@ struct LayerBufs {
   void* cax = nullptr;   // V4<R> x 3 per grain: cubic crystal axes (null: uniaxial)
   void* ucol = nullptr;  // R columnar interlayer coefficients (null: CSR form)
   void* lcol = nullptr;
+  // grains of several cells (map layers): cell -> grain (-1 empty), grain -> cells
+  // CSR, grain-averaged demag per cell; null on one-grain-per-cell layers
+  int *cgrain = nullptr, *gci = nullptr, *gcs = nullptr;
+  void* hdm = nullptr;
+  int ng = 0;  // grains (n counts cells)
   double hdir[3] = {0, 0, 0};
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
   int func = 0;
@@ -121,6 +126,7 @@ struct Engine {
   bool has_head = false;             // a run has a layer under the write head (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
   bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
+  bool mapped = false;               // a run has grains of several cells (grain-averaged demag)
   double* d_part = nullptr;
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
@@ -431,6 +437,10 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.lcoef = static_cast<const R*>(b.lcoef);
     o.xst = static_cast<const V4<R>*>(b.xst);
     o.cax = static_cast<const V4<R>*>(b.cax);
+    o.cgrain = b.cgrain;
+    o.gci = b.gci;
+    o.gcs = b.gcs;
+    o.hdm = static_cast<V4<R>*>(b.hdm);
     o.ucol = static_cast<const R*>(b.ucol);
     o.lcol = static_cast<const R*>(b.lcol);
     for (int a = 0; a < 3; ++a) o.hdir[a] = b.hdir[a];
@@ -579,11 +589,15 @@ int build_tables(Engine* e) {
   e->nct = (int)ct.size();
   e->has_head = false;
   e->has_cubic = false;
+  e->mapped = false;
   for (auto* r : e->runs)
     for (int l = 0; l < r->nl; ++l) {
       e->has_head = e->has_head || r->L[l].func == kFuncHead;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
+      e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
+  if (e->mapped && e->has_head)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "the write head needs one grain per cell (no grain maps in the batch)");
   e->nst = (int)stt.size();
   if (e->nst > e->st_cap) {
     dfree(e->d_stasks);
@@ -662,23 +676,37 @@ template <typename R>
 cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type, bool stored = false) {
   cudaError_t ce = cudaSuccess;
   auto acc = [&](cudaError_t x) { if (ce == cudaSuccess) ce = x; };
-  const int f = llg_type == 2 ? kFlagBoris : llg_type == -2 ? (kFlagBoris | kFlagMid) : 0;
+  const int f0 = llg_type == 2 ? kFlagBoris : llg_type == -2 ? (kFlagBoris | kFlagMid) : 0;
+  // grains of several cells: each stage's demag comes from an evaluation stage
+  // (inverse row transforms of every cell) averaged over the grains' cells
+  const int f = f0 | (e->mapped ? kFlagMapped : 0);
+  const int nr = (int)e->runs.size();
+  auto mapped_demag = [&](int i) {
+    if (!e->mapped) return;
+    acc(launch_row_e<R>(e, kEval, false, i, f0 | kFlagDemagOnly));
+    int maxc = 1;
+    for (auto* r : e->runs) maxc = std::max(maxc, r->g.nx * r->g.ny);
+    acc(launch_kernel(gather_demag_kernel<R>, dim3((maxc + 255) / 256, nr * kMaxLayers), dim3(256), 0, e->st, false,
+                      static_cast<const RunDev<R>*>(e->d_runs), nr));
+  };
   for (int i = 0; i < k; ++i) {
     const bool last = stats && i == k - 1;
     const int lf = last ? (kFlagStats | kFlagStoreField) : 0;
     if (llg_type == 2) {
+      mapped_demag(i);
       acc(launch_row_e<R>(e, kPred, last, i, f | lf));
       acc(launch_col_e<R>(e, i, 0));
       acc(launch_kernel(commit_kernel<R>, dim3(e->nst), dim3(256), 0, e->st, true,
                         static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_stasks, i, 0));
       continue;
     }
+    mapped_demag(i);
     acc(launch_row_e<R>(e, kPred, false, i, f | ((stored && i == 0) ? kFlagStoredField : 0)));
     acc(launch_col_e<R>(e, i, 0));
+    mapped_demag(i);
     acc(launch_row_e<R>(e, kCorr, last, i, f | lf));
     acc(launch_col_e<R>(e, i, 0));
   }
-  const int nr = (int)e->runs.size();
   acc(launch_kernel(advance_kernel<R>, dim3((nr + 127) / 128), dim3(128), 0, e->st, true,
                     static_cast<RunDev<R>*>(e->d_runs), nr, k));
   if (stats)
@@ -950,7 +978,18 @@ int engine_eval(Engine* e) {
   std::string* errp = &e->err;
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
-  CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField));
+  if (e->mapped) {
+    // grains of several cells: demag per cell, its grain average, then the field
+    const int nr = (int)e->runs.size();
+    int maxc = 1;
+    for (auto* r : e->runs) maxc = std::max(maxc, r->g.nx * r->g.ny);
+    CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagDemagOnly));
+    CK(launch_kernel(gather_demag_kernel<R>, dim3((maxc + 255) / 256, nr * kMaxLayers), dim3(256), 0, e->st, false,
+                     static_cast<const RunDev<R>*>(e->d_runs), nr));
+    CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField | kFlagMapped));
+  } else {
+    CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField));
+  }
   CK(cudaGetLastError());
   return MRM_OK;
 }
@@ -974,19 +1013,24 @@ int check_device_error(Engine* e) {
 
 // ---------------- state transfers ----------------
 // (x, y, z) doubles of the host layout <-> the float4 / double4 grain records
+// (map layers: every cell takes its grain's value, empty cells zero; a grain
+// is read at its first cell)
 template <typename R>
-__global__ void state_in_kernel(const double* __restrict__ in, V4<R>* __restrict__ m, V4<R>* __restrict__ mp, int n) {
+__global__ void state_in_kernel(const double* __restrict__ in, V4<R>* __restrict__ m, V4<R>* __restrict__ mp, int n,
+                                const int* __restrict__ cgrain) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const V4<R> v{(R)in[3 * i], (R)in[3 * i + 1], (R)in[3 * i + 2], (R)0};
+  const int g = cgrain ? cgrain[i] : i;
+  const V4<R> v = g >= 0 ? V4<R>{(R)in[3 * g], (R)in[3 * g + 1], (R)in[3 * g + 2], (R)0} : V4<R>{0, 0, 0, 0};
   m[i] = v;
   mp[i] = v;
 }
 template <typename R>
-__global__ void state_out_kernel(const V4<R>* __restrict__ src, double* __restrict__ out, int n) {
+__global__ void state_out_kernel(const V4<R>* __restrict__ src, double* __restrict__ out, int n,
+                                 const int* __restrict__ gci, const int* __restrict__ gcs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const V4<R> v = src[i];
+  const V4<R> v = src[gci ? gcs[gci[i]] : i];
   out[3 * i] = (double)v.x;
   out[3 * i + 1] = (double)v.y;
   out[3 * i + 2] = (double)v.z;
@@ -1005,11 +1049,12 @@ __global__ void hmag_kernel(const RunDev<R>* __restrict__ runs, int slot, int la
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   double v2 = 0.0;
   if (n < L.n) {
-    const V4<R> h = L.hf[n];
+    const int g = L.cgrain ? L.cgrain[n] : n;  // grains only, each on its cells
+    const V4<R> h = g >= 0 ? L.hf[n] : V4<R>{0, 0, 0, 0};
     double x = h.x, y = h.y, z = h.z;
-    if (L.thermal) {
+    if (L.thermal && g >= 0) {
       R gn[3];
-      thermal_normals(rd.seed, (unsigned long long)layer, (unsigned long long)step, (unsigned long long)n, gn);
+      thermal_normals(rd.seed, (unsigned long long)layer, (unsigned long long)step, (unsigned long long)g, gn);
       const double s = (double)L.pb[n].w * sqrt(L.temperature) * dti;
       x += s * (double)gn[0];
       y += s * (double)gn[1];
@@ -1037,6 +1082,7 @@ int run_alloc(mrm_gpu* r) {
   for (int l = 0; l < r->nl; ++l) {
     LayerBufs& b = r->L[l];
     b.n = (int)n;
+    b.ng = (int)n;
     void** v4s[] = {&b.m, &b.mp, &b.dm, &b.hf, &b.hd, &b.ht, &b.pa, &b.pb};
     for (void** p : v4s) {
       rc = dmalloc(errp, p, n * 4 * re);
@@ -1060,6 +1106,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
     dfree(b.xst); dfree(b.ucol); dfree(b.lcol); dfree(b.cax);
+    dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm);
   }
 }
 
@@ -1141,7 +1188,9 @@ int upload_csr(mrm_gpu* r, int n, const int32_t* index, const int32_t* grain, co
 
 // host copies of ms_scale per layer (neighbour scaling of exchange coefficients)
 struct HostLayerCache {
-  std::vector<double> ms_scale, ms, hk_scale;
+  std::vector<double> ms_scale, ms, hk_scale;  // per grain
+  std::vector<int> cgrain, rep;                // map layers: cell -> grain (-1 empty), grain -> its first cell
+  std::vector<double> ms_scale_cell;           // map layers: the cell's grain's ms_scale (0: empty)
 };
 std::map<const mrm_gpu*, std::vector<HostLayerCache>>& host_cache() {
   static std::map<const mrm_gpu*, std::vector<HostLayerCache>> m;
@@ -1155,50 +1204,113 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
                    const int32_t* g2ci, const int32_t* g2c, const int32_t* hxi, const int32_t* hxg,
                    const double* hx) {
   std::string* errp = &r->err;
-  const int nx = r->g.nx, ny = r->g.ny;
-  if (n != nx * ny)
-    return set_err(errp, MRM_ERR_UNSUPPORTED, "layer %d: %d grains on a %dx%d grid; this path needs one grain per cell", l, n, nx, ny);
+  const int nx = r->g.nx, ny = r->g.ny, nc = nx * ny;
   if (!ms || !vol || !axis || !hk || !hk_scale || !ms_scale || !alpha_scale || !g2ci || !g2c)
     return set_err(errp, MRM_ERR_ARG, "layer %d: NULL array", l);
-  for (int g = 0; g < n; ++g) {
-    if (g2ci[g] != g || g2ci[g + 1] != g + 1)
-      return set_err(errp, MRM_ERR_UNSUPPORTED, "grain %d spans %d cells; multi-cell grains are not supported", g + 1, g2ci[g + 1] - g2ci[g]);
-    const int i = g2c[2 * g] - 1, j = g2c[2 * g + 1] - 1;
-    if (i != g % nx || j != g / nx)
-      return set_err(errp, MRM_ERR_UNSUPPORTED, "grain %d sits at cell (%d,%d), expected (%d,%d)", g + 1, i + 1, j + 1, g % nx + 1, g / nx + 1);
+  if (n < 1 || n > nc) return set_err(errp, MRM_ERR_ARG, "layer %d: %d grains on %d cells", l, n, nc);
+  // one grain per cell in grid order (the fused path), or a grain -> cells map
+  // (get_mag / get_magnetostatic, data.f90:322-390, field.f90:438-517)
+  bool identity = n == nc;
+  for (int g = 0; identity && g < n; ++g)
+    identity = g2ci[g] == g && g2ci[g + 1] == g + 1 && g2c[2 * g] - 1 == g % nx && g2c[2 * g + 1] - 1 == g / nx;
+  std::vector<int> cg, repc;
+  if (!identity) {
+    if (g2ci[0] != 0) return set_err(errp, MRM_ERR_ARG, "layer %d: grain2gridindex(0) must be 0", l);
+    cg.assign(nc, -1);
+    repc.resize(n);
+    for (int g = 0; g < n; ++g) {
+      if (g2ci[g + 1] <= g2ci[g]) return set_err(errp, MRM_ERR_ARG, "layer %d: grain %d has no cell", l, g + 1);
+      for (int q = g2ci[g]; q < g2ci[g + 1]; ++q) {
+        const int i = g2c[2 * q] - 1, j = g2c[2 * q + 1] - 1;
+        if (i < 0 || i >= nx || j < 0 || j >= ny)
+          return set_err(errp, MRM_ERR_ARG, "layer %d: grain %d cell (%d,%d) outside the grid", l, g + 1, i + 1, j + 1);
+        const int c = j * nx + i;
+        if (cg[c] >= 0) return set_err(errp, MRM_ERR_ARG, "layer %d: cell (%d,%d) in two grains", l, i + 1, j + 1);
+        cg[c] = g;
+        if (q == g2ci[g]) repc[g] = c;
+      }
+    }
   }
+  // records per cell: the cell's grain's (a grain's first cell carries its
+  // volume and counts it in the reductions; empty cells: Ms = 0, no dynamics)
   const double kB = 1.380662e-16;  // field.f90:407
   const double tsig = std::sqrt(2.0 * kB * alpha / gamma);
-  std::vector<R> pa(4 * n), pb(4 * n);
-  std::vector<double> pv(4 * n);
-  for (int g = 0; g < n; ++g) {
-    pa[4 * g + 0] = (R)axis[3 * g];
-    pa[4 * g + 1] = (R)axis[3 * g + 1];
-    pa[4 * g + 2] = (R)axis[3 * g + 2];
+  std::vector<R> pa(4 * (size_t)nc, (R)0), pb(4 * (size_t)nc, (R)0);
+  std::vector<double> pv(4 * (size_t)nc, 0.0);
+  for (int c = 0; c < nc; ++c) {
+    const int g = identity ? c : cg[c];
+    if (g < 0) {
+      pv[4 * c + 2] = 1.0;
+      continue;
+    }
+    const bool first = identity || repc[g] == c;
+    pa[4 * c + 0] = (R)axis[3 * g];
+    pa[4 * c + 1] = (R)axis[3 * g + 1];
+    pa[4 * c + 2] = (R)axis[3 * g + 2];
     const double hks = hk_scale[g] > 0.0 ? hk_scale[g] : 0.0;  // get_uni_hk returns 0 for hk_scale <= 0
-    pa[4 * g + 3] = (R)(hk[2 * g] * hks);
-    pb[4 * g + 0] = (R)(ms[g] * ms_scale[g]);
-    pb[4 * g + 1] = (R)(hk[2 * g + 1] * hks);
-    pb[4 * g + 2] = (R)(alpha * alpha_scale[g]);
+    pa[4 * c + 3] = (R)(hk[2 * g] * hks);
+    pb[4 * c + 0] = (R)(ms[g] * ms_scale[g]);
+    pb[4 * c + 1] = (R)(hk[2 * g + 1] * hks);
+    pb[4 * c + 2] = (R)(alpha * alpha_scale[g]);
     double x = 0.0;  // field.f90:418-419 without the temperature (applied per step)
     if (ms_scale[g] > 0.0) x = alpha_scale[g] / (ms[g] * vol[g] * std::max(floor_ms, ms_scale[g]));
-    pb[4 * g + 3] = (R)(std::sqrt(x) * tsig);
-    pv[4 * g + 0] = vol[g];
-    pv[4 * g + 1] = ms_scale[g];
-    pv[4 * g + 2] = ms[g];
-    pv[4 * g + 3] = 0.0;
+    pb[4 * c + 3] = (R)(std::sqrt(x) * tsig);
+    pv[4 * c + 0] = first ? vol[g] : 0.0;
+    pv[4 * c + 1] = ms_scale[g];
+    pv[4 * c + 2] = ms[g];
+    pv[4 * c + 3] = first ? 1.0 : 0.0;
   }
   LayerBufs& b = r->L[l];
-  CK(cudaMemcpy(b.pa, pa.data(), sizeof(R) * 4 * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.pb, pb.data(), sizeof(R) * 4 * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.pv, pv.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.pa, pa.data(), sizeof(R) * 4 * nc, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.pb, pb.data(), sizeof(R) * 4 * nc, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.pv, pv.data(), sizeof(double) * 4 * nc, cudaMemcpyHostToDevice));
   auto& hc = host_cache()[r];
   hc.resize(MRM_MAX_LAYERS);
   hc[l].ms_scale.assign(ms_scale, ms_scale + n);
   hc[l].ms.assign(ms, ms + n);
   hc[l].hk_scale.assign(hk_scale, hk_scale + n);
+  hc[l].cgrain = cg;
+  hc[l].rep = repc;
+  hc[l].ms_scale_cell.clear();
   dfree(b.xst);
-  if (hxi && hxg && hx) {
+  dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm);
+  b.ng = n;
+  if (!identity) {
+    hc[l].ms_scale_cell.assign(nc, 0.0);
+    for (int c = 0; c < nc; ++c)
+      if (cg[c] >= 0) hc[l].ms_scale_cell[c] = ms_scale[cg[c]];
+    std::vector<int> cells(g2ci[n]);
+    for (int q = 0; q < g2ci[n]; ++q) cells[q] = (g2c[2 * q + 1] - 1) * nx + (g2c[2 * q] - 1);
+    int rc = dmalloc(errp, (void**)&b.cgrain, sizeof(int) * nc);
+    if (!rc) rc = dmalloc(errp, (void**)&b.gci, sizeof(int) * (n + 1));
+    if (!rc) rc = dmalloc(errp, (void**)&b.gcs, sizeof(int) * cells.size());
+    if (!rc) rc = dmalloc(errp, &b.hdm, sizeof(R) * 4 * (size_t)nc);
+    if (rc) return rc;
+    CK(cudaMemcpy(b.cgrain, cg.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.gci, g2ci, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.gcs, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+  }
+  if (!identity && hxi && hxg && hx) {
+    // intralayer exchange of the grains, on every cell of each grain, with each
+    // neighbour grain read at its first cell
+    if (hxi[0] != 0) return set_err(errp, MRM_ERR_ARG, "CSR index(0) must be 0");
+    std::vector<int> ci(nc + 1, 0), cn;
+    std::vector<double> cf;
+    for (int c = 0; c < nc; ++c) {
+      const int g = cg[c];
+      if (g >= 0)
+        for (int q = hxi[g]; q < hxi[g + 1]; ++q) {
+          const int j = hxg[q] - 1;
+          if (j < 0 || j >= n) return set_err(errp, MRM_ERR_ARG, "CSR neighbour %d out of range", hxg[q]);
+          cn.push_back(repc[j] + 1);
+          cf.push_back(hx[q]);
+        }
+      ci[c + 1] = (int)cn.size();
+    }
+    int rc = upload_csr<R>(r, nc, ci.data(), cn.data(), cf.data(), hc[l].ms_scale_cell.data(), nc, &b.xidx,
+                           &b.xnbr, &b.xcoef);
+    if (rc) return rc;
+  } else if (hxi && hxg && hx) {
     int rc = upload_csr<R>(r, n, hxi, hxg, hx, ms_scale, n, &b.xidx, &b.xnbr, &b.xcoef);
     if (rc) return rc;
     // lattice form: every entry is one of the 4 periodic nearest neighbours, each
@@ -1357,14 +1469,16 @@ template <typename R>
 int set_cubic_t(mrm_gpu* h, int layer, const double* cubic_axis) {
   std::string* errp = &h->err;
   LayerBufs& b = h->L[layer];
-  const int n = b.n;
+  const int n = b.n;  // cells
   const HostLayerCache& hc = host_cache()[h][layer];
-  std::vector<R> v(12 * (size_t)n);
-  for (int g = 0; g < n; ++g) {
+  std::vector<R> v(12 * (size_t)n, (R)0);
+  for (int c = 0; c < n; ++c) {
+    const int g = hc.cgrain.empty() ? c : hc.cgrain[c];
+    if (g < 0) continue;
     const double hs = hc.hk_scale[g] > 0.0 ? hc.hk_scale[g] : 0.0;  // get_cubic_hk returns 0 for hk_scale <= 0
     for (int i = 0; i < 3; ++i) {
-      for (int k = 0; k < 3; ++k) v[12 * (size_t)g + 4 * i + k] = (R)cubic_axis[9 * (size_t)g + 3 * i + k];
-      v[12 * (size_t)g + 4 * i + 3] = (R)(i == 0 ? hs * hc.ms[g] : 0.0);
+      for (int k = 0; k < 3; ++k) v[12 * (size_t)c + 4 * i + k] = (R)cubic_axis[9 * (size_t)g + 3 * i + k];
+      v[12 * (size_t)c + 4 * i + 3] = (R)(i == 0 ? hs * hc.ms[g] : 0.0);
     }
   }
   if (!b.cax) {
@@ -1464,19 +1578,51 @@ int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* in
   cudaSetDevice(h->eng->dev);
   cudaStreamSynchronize(h->eng->st);
   LayerBufs& b = h->L[layer];
-  const int n = b.n;
+  int n = b.n;
   int rc;
+  // map layers: the coupling of each grain on every one of its cells, the other
+  // layer's grain read at its first cell
+  std::vector<int> mi, mg;
+  std::vector<double> mc;
+  const double* nbr_scale = hc[other].ms_scale.data();
+  int n_nbr = h->L[other].n;
+  const bool mapped = !hc[layer].cgrain.empty() || !hc[other].cgrain.empty();
+  if (mapped) {
+    const std::vector<int>& cg = hc[layer].cgrain;
+    const int ng = b.ng, ngo = h->L[other].ng;
+    if (index[0] != 0) return set_err(errp, MRM_ERR_ARG, "CSR index(0) must be 0");
+    mi.assign(n + 1, 0);
+    for (int c = 0; c < n; ++c) {
+      const int g = cg.empty() ? c : cg[c];
+      if (g >= 0 && g < ng)
+        for (int q = index[g]; q < index[g + 1]; ++q) {
+          const int j = grain[q] - 1;
+          if (j < 0 || j >= ngo) return set_err(errp, MRM_ERR_ARG, "interlayer neighbour %d out of range", grain[q]);
+          mg.push_back((hc[other].cgrain.empty() ? j : hc[other].rep[j]) + 1);
+          mc.push_back(coef[q]);
+        }
+      mi[c + 1] = (int)mg.size();
+    }
+    if (mg.empty()) {  // keep the arrays non-empty
+      mg.push_back(1);
+      mc.push_back(0.0);
+    }
+    index = mi.data();
+    grain = mg.data();
+    coef = mc.data();
+    if (!hc[other].cgrain.empty()) nbr_scale = hc[other].ms_scale_cell.data();
+  }
   if (h->g.precision == MRM_FP64)
-    rc = side == 0 ? upload_csr<double>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.uidx, &b.unbr, &b.ucoef)
-                   : upload_csr<double>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.lidx, &b.lnbr, &b.lcoef);
+    rc = side == 0 ? upload_csr<double>(h, n, index, grain, coef, nbr_scale, n_nbr, &b.uidx, &b.unbr, &b.ucoef)
+                   : upload_csr<double>(h, n, index, grain, coef, nbr_scale, n_nbr, &b.lidx, &b.lnbr, &b.lcoef);
   else
-    rc = side == 0 ? upload_csr<float>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.uidx, &b.unbr, &b.ucoef)
-                   : upload_csr<float>(h, n, index, grain, coef, hc[other].ms_scale.data(), h->L[other].n, &b.lidx, &b.lnbr, &b.lcoef);
+    rc = side == 0 ? upload_csr<float>(h, n, index, grain, coef, nbr_scale, n_nbr, &b.uidx, &b.unbr, &b.ucoef)
+                   : upload_csr<float>(h, n, index, grain, coef, nbr_scale, n_nbr, &b.lidx, &b.lnbr, &b.lcoef);
   if (rc) return rc;
   // columnar form: grain n couples to grain n of the other layer only
   void** col = side == 0 ? &b.ucol : &b.lcol;
   dfree(*col);
-  bool columnar = h->L[other].n == n;
+  bool columnar = !mapped && h->L[other].n == n;
   for (int g = 0; columnar && g < n; ++g)
     columnar = (index[g + 1] - index[g] == 1) && (grain[index[g]] == g + 1);
   if (columnar) {
@@ -1697,21 +1843,22 @@ int mrm_gpu_set_state(mrm_gpu* h, int layer, const double* m) {
   std::string* errp = &h->err;
   if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
   if (!h->L[layer].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", layer);
-  const int n = h->L[layer].n;
+  const LayerBufs& b = h->L[layer];
+  const int n = b.n;
   cudaStream_t st = h->eng->st;
   CK(cudaSetDevice(h->eng->dev));
-  // the caller's array as it is, then widened on the device into m and m*,
-  // in stream order after the work already queued
-  CK(cudaMemcpyAsync(h->xfer, m, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+  // the caller's array as it is (one record per grain), then widened on the
+  // device into m and m* of every cell, in stream order after the work already queued
+  CK(cudaMemcpyAsync(h->xfer, m, sizeof(double) * 3 * b.ng, cudaMemcpyHostToDevice, st));
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (h->g.precision == MRM_FP64)
     state_in_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer),
-                                                     static_cast<V4<double>*>(h->L[layer].m),
-                                                     static_cast<V4<double>*>(h->L[layer].mp), n);
+                                                     static_cast<V4<double>*>(b.m), static_cast<V4<double>*>(b.mp),
+                                                     n, b.cgrain);
   else
     state_in_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer),
-                                                    static_cast<V4<float>*>(h->L[layer].m),
-                                                    static_cast<V4<float>*>(h->L[layer].mp), n);
+                                                    static_cast<V4<float>*>(b.m), static_cast<V4<float>*>(b.mp), n,
+                                                    b.cgrain);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));  // the caller may reuse its array on return
   h->spec_valid = false;
@@ -1721,16 +1868,17 @@ int mrm_gpu_set_state(mrm_gpu* h, int layer, const double* m) {
 static int get_v4(mrm_gpu* h, int layer, void* src, double* out) {
   std::string* errp = &h->err;
   if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
-  const int n = h->L[layer].n;
+  const LayerBufs& b = h->L[layer];
+  const int n = b.ng;  // grains
   cudaStream_t st = h->eng->st;
   CK(cudaSetDevice(h->eng->dev));
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (h->g.precision == MRM_FP64)
     state_out_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const V4<double>*>(src),
-                                                      static_cast<double*>(h->xfer), n);
+                                                      static_cast<double*>(h->xfer), n, b.gci, b.gcs);
   else
     state_out_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const V4<float>*>(src),
-                                                     static_cast<double*>(h->xfer), n);
+                                                     static_cast<double*>(h->xfer), n, b.gci, b.gcs);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->xfer, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1793,7 +1941,9 @@ int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag) {
     h->err = e->err;
     return rc;
   }
-  if (hdemag) return get_v4(h, layer, h->L[layer].hd, hdemag);
+  if (hdemag) {
+    return get_v4(h, layer, h->L[layer].hd, hdemag);
+  }
   CK(cudaStreamSynchronize(e->st));
   return MRM_OK;
 }
@@ -2373,6 +2523,9 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   if (!m || !hdemag) return set_err(errp, MRM_ERR_ARG, "m and hdemag must be device pointers");
   if (h->g.precision != MRM_FP32)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
+  for (int l = 0; l < h->nl; ++l)
+    if (h->L[l].cgrain)
+      return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes one grain per cell");
   const int nl = h->nl, ny = h->g.ny, ph = h->px / 2 + 1;
   const int rpt = 1, nrt = nl * ny;  // one row per task (row shape 0)
   const int cpt = col_tile(default_cols(h)), nct = (ph + cpt - 1) / cpt;

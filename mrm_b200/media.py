@@ -226,6 +226,59 @@ def cubic_medium(side: int, *, k1_oe: float = 4000.0, k2_oe: float = 1000.0, see
     return med
 
 
+def grain_map_medium(nx: int = 16, ny: int = 16, *, seed: int = 1, temperature: float = 0.0,
+                     empty_frac: float = 0.05, hex_oe: float = 300.0, boundary: int = 1, ms: float = 700.0,
+                     hk: float = 15000.0, pitch_nm: float = 8.0, thickness_nm: float = 10.0) -> Medium:
+    """M(H) medium whose grains cover one to four cells (1x1, 2x1, 1x2, 2x2
+    blocks, clipped where cells are taken) with a few empty cells: the
+    grain <-> cell maps of get_mag / get_magnetostatic (data.f90:322-390,
+    field.f90:438-517).  Exchange between grains sharing a cell edge."""
+    rng = np.random.default_rng(seed)
+    owner = -np.ones((ny, nx), dtype=np.int64)
+    grains = []
+    shapes = [(1, 1), (2, 1), (1, 2), (2, 2)]
+    for j in range(ny):
+        for i in range(nx):
+            if owner[j, i] >= 0 or rng.random() < empty_frac:
+                continue
+            w, h = shapes[int(rng.integers(0, len(shapes)))]
+            cells = [(i + a, j + b) for b in range(h) for a in range(w)
+                     if i + a < nx and j + b < ny and owner[j + b, i + a] < 0]
+            for ci, cj in cells:
+                owner[cj, ci] = len(grains)
+            grains.append(cells)
+    n = len(grains)
+    g2c_index = np.concatenate([[0], np.cumsum([len(c) for c in grains])]).astype(np.int32)
+    g2c = np.array([(ci + 1, cj + 1) for c in grains for ci, cj in c], dtype=np.int32)
+    nbrs = []
+    for g, cells in enumerate(grains):
+        s_ = set()
+        for ci, cj in cells:
+            for di, dj in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+                a, b = ci + di, cj + dj
+                if 0 <= a < nx and 0 <= b < ny and owner[b, a] >= 0 and owner[b, a] != g:
+                    s_.add(int(owner[b, a]))
+        nbrs.append(sorted(s_))
+    hx_index = np.concatenate([[0], np.cumsum([len(x) for x in nbrs])]).astype(np.int32)
+    hx_grain = np.array([q + 1 for x in nbrs for q in x], dtype=np.int32)
+    hx = np.full(len(hx_grain), float(hex_oe))
+    dx = dy = pitch_nm * 1e-7
+    dz = thickness_nm * 1e-7
+    ncell = np.array([len(c) for c in grains], dtype=float)
+    lay = Layer(nx=nx, ny=ny, ms=np.full(n, float(ms)), vol=ncell * dx * dy * dz,
+                axis=easy_axes(rng, n, 3.0), hk=np.stack([hk_magnitudes(rng, n, hk, -0.05), np.zeros(n)], axis=1),
+                hk_scale=np.ones(n), ms_scale=np.ones(n), alpha_scale=np.ones(n), alpha=0.1, gamma=1.76e7,
+                floor_ms=0.01, g2c_index=g2c_index, g2c=g2c, hx_index=hx_index, hx_grain=hx_grain, hx=hx)
+    a = math.radians(10.0)
+    lay.hdir = (math.sin(a), 0.0, math.cos(a))
+    lay.t_start, lay.t_end, lay.s_start, lay.s_end, lay.scale = 0.0, 2e-10, 20000.0, -20000.0, 1.0
+    lay.temperature = float(temperature)
+    lay.thermal = temperature > 0.0
+    m0 = np.zeros((n, 3))
+    m0[:, 2] = 1.0
+    return Medium(nx=nx, ny=ny, dx=dx, dy=dy, dz=[dz], il_space=[0.0], layers=[lay], boundary=boundary, m0=[m0])
+
+
 def columnar_coupling(n: int, coef_oe: float):
     idx = np.arange(n + 1, dtype=np.int32)
     grain = np.arange(1, n + 1, dtype=np.int32)
