@@ -88,3 +88,22 @@ def test_grain_map_two_layers_interlayer(oracle, gpulib):
     for l in range(2):
         assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-9
     assert np.allclose(sg["mave_l"][:2], so["mave_l"][:2], atol=1e-10)
+
+
+def test_medium_from_grain_file(oracle, gpulib, tmp_path):
+    # a reference-format grain file (maps, cubic layer, interlayer coupling) on the GPU path
+    from mrm_b200 import formats
+    from tests.test_formats import _two_layer_map_medium
+    med = _two_layer_map_medium()
+    p = str(tmp_path / "grain.bin")
+    formats.write_grain_file(p, formats.grain_file_layers(med), med.nx, med.ny, med.dx, med.dy)
+    back = formats.medium_from_grain_file(p, med.dz, boundary=1)
+    for lay, orig in zip(back.layers, med.layers):
+        lay.hdir, lay.t_start, lay.t_end, lay.s_start, lay.s_end = (orig.hdir, orig.t_start, orig.t_end,
+                                                                     orig.s_start, orig.s_end)
+    orc, gpu = _pair(oracle, back, FP64)
+    so = orc.step(300, 1e-13)
+    sg = gpu.step(300, 1e-13)
+    for l in range(2):
+        assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-9
+    assert sg["energy"] == pytest.approx(so["energy"], rel=1e-8)
