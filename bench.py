@@ -182,9 +182,19 @@ def cpu_baseline_sample(threads: int, min_s: float = 10.0, chunk: int = 25, max_
             break
     el = time.perf_counter() - t0
     n = med.n_grains
+    sim.close()
+    # the write leg's readback call on the oracle (initial state of the same medium)
+    from mrm_b200 import media
+    wsim = pyoracle.OracleSim(media.head_write_medium(1024, 256, seed=1, prbs_seed=1, temperature=300.0),
+                              rng_mode=1, seed=1, demag=False)
+    t0 = time.perf_counter()
+    wsim.off_field(**READBACK)
+    off_ms = (time.perf_counter() - t0) * 1e3
+    wsim.close()
     return {"value": n * done / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{done} Heun steps of one {n}-grain realisation in {el:.1f} s (FP64 oracle, "
-                      f"OpenMP, after 2 warm-up steps; tensor build excluded)"}
+                      f"OpenMP, after 2 warm-up steps; tensor build excluded)",
+            "readback_ms_per_call": off_ms}
 
 
 def run_reference(args, rank, world):
@@ -362,6 +372,11 @@ def plain_leg(torch, local, precision, heun_chunk=100, total=RAMP_STEPS, flush_l
             1e3 * dev_ms / (nchunks * heun_chunk), "hc_oe": hc, "mr": mr, "prof": prof}
 
 
+# readback slab 1 nm above the media, 1 nm thick, no images (lengths in cm)
+READBACK = dict(zoff=1e-7, dzobs=1e-7, num_images=0)
+READBACK_TEXT = "(slab 1 nm above the media, 1 nm thick, FP64 tensor, FFTs and products on the device)"
+
+
 def write_leg(torch, local, steps=2000):
     """The two-layer recording write (1,024 x 256 grains per layer, 7 nm pitch,
     Karlqvist head at 20 m/s writing a 64-bit PRBS at 15 nm bits, T = 300 K,
@@ -380,12 +395,21 @@ def write_leg(torch, local, steps=2000):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     px, py = sim.fft_grid()
+    # readback field of the written track (plot_off_field): one synchronous call
+    # through the public API, the field copied back to host memory
+    sim.off_field(**READBACK)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        hr = sim.off_field(**READBACK)
+    off_ms = (time.perf_counter() - t0) / 3 * 1e3
     sim.close()
     grains = 2 * 1024 * 256
     return {"workload": f"two-layer 1024x256x2 head write (gap 25 nm, fly 6 nm, 12 kOe, 20 m/s, 64-bit PRBS "
                         f"at 15 nm), T=300 K, FP32, {px}x{py} padded FFT, {steps} Heun steps of the 480,000",
             "grains": grains, "value": grains * steps / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
-            "us_per_heun_step": 1e3 * ms / steps, "mave_top": np.asarray(st["mave_l"][0]).tolist()}
+            "us_per_heun_step": 1e3 * ms / steps, "mave_top": np.asarray(st["mave_l"][0]).tolist(),
+            "readback": {"call": "off_field " + READBACK_TEXT, "grid": [1024, 256], "ms_per_call": off_ms,
+                         "hz_rms_oe": float(np.sqrt(np.mean(hr[2] ** 2)))}}
 
 
 def mix_leg(torch, local, steps=5000, nreal=64):

@@ -229,6 +229,19 @@ int mrm_gpu_stream(const mrm_gpu* h, void** stream);
 int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, double dt_max,
                           const double* max_dm, double* dt, double* max_dmdt, mrm_gpu_stats* out);
 
+/* Stray field of the current state at an observation slab above the media
+ * (plot_off_field / get_off_field and calculate_off_field_tensor,
+ * off_field.f90:25-108,216-320; e.g. a readback plane): the slab's bottom
+ * is zoff (cm) above the top of the top layer, its thickness dzobs (cm); the
+ * field is averaged over the slab, on the nx x ny grid with num_images
+ * periodic images in x and y (the module's periodic_x/y), a soft underlayer
+ * image when sul_mu > 1 (space_to_sul below the bottom layer) and a head
+ * image when head_mu > 1 (fly_height above the top layer).  out[(c*ny + j)*nx + i]
+ * = H_c (Oe), c = x, y, z.  Computed in FP64 on the device (tensor, FFTs and
+ * products); nx, ny powers of two. */
+int mrm_gpu_off_field(mrm_gpu* h, double zoff, double dzobs, double head_mu, double fly_height, double sul_mu,
+                      double space_to_sul, int num_images, double* out);
+
 /* Kernel shapes of the engine a handle runs in (a batch run: the batch's).
  * row_shape / col_shape index the compiled row / column kernel shapes
  * (rows per block, threads, resident blocks; threads and resident blocks of

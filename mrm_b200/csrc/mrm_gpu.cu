@@ -1066,6 +1066,36 @@ __global__ void hmag_kernel(const RunDev<R>* __restrict__ runs, int slot, int la
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v2));
 }
 
+// ---------------- off-plane field (off_field.f90) ----------------
+// Ms ms_scale m per cell of every layer (get_mag, data.f90:322-390), FP64 planes [l*3 + a][ny][nx]
+template <typename R>
+__global__ void mgrid_kernel(const RunDev<R>* __restrict__ runs, int slot, double* __restrict__ out) {
+  const RunDev<R>& rd = runs[slot];
+  const int l = blockIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = rd.nx * rd.ny;
+  if (c >= n) return;
+  const LayerDev<R>& L = rd.L[l];
+  const V4<R> m = L.m[c];
+  const double f = (double)L.pb[c].x;  // 0 on empty cells
+  out[((size_t)l * 3 + 0) * n + c] = f * (double)m.x;
+  out[((size_t)l * 3 + 1) * n + c] = f * (double)m.y;
+  out[((size_t)l * 3 + 2) * n + c] = f * (double)m.z;
+}
+// H^_a = sum over source layers and components of N^[ks][3a + b] M^[ks][b] (off_field.f90:70-95)
+__global__ void off_mac_kernel(const Cx<double>* __restrict__ T, const Cx<double>* __restrict__ X,
+                               Cx<double>* __restrict__ H, int nl, long long hplane) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= hplane) return;
+  for (int a = 0; a < 3; ++a) {
+    Cx<double> h{0.0, 0.0};
+    for (int ks = 0; ks < nl; ++ks)
+      for (int b = 0; b < 3; ++b)
+        h = cadd(h, cmul(T[((long long)ks * 9 + 3 * a + b) * hplane + q], X[((long long)ks * 3 + b) * hplane + q]));
+    H[(long long)a * hplane + q] = h;
+  }
+}
+
 // ---------------- run buffers ----------------
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
@@ -1640,6 +1670,121 @@ int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* in
   }
   h->eng->desc_dirty = true;
   return MRM_OK;
+}
+
+// The stray field of all layers at an observation slab of thickness dzobs whose
+// bottom is zoff above the top layer, on the nx x ny grid with the periodic
+// images of the reference's off-plane tensor (off_field.f90:55-108,216-320).
+int mrm_gpu_off_field(mrm_gpu* h, double zoff, double dzobs, double head_mu, double fly_height, double sul_mu,
+                      double space_to_sul, int num_images, double* out) {
+  if (!h || !out) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  const int nx = h->g.nx, ny = h->g.ny, nl = h->nl;
+  if (!(dzobs > 0)) return set_err(errp, MRM_ERR_ARG, "dzobs must be > 0");
+  if (num_images < 0) return set_err(errp, MRM_ERR_ARG, "num_images must be >= 0");
+  if (!is_pow2(nx) || !is_pow2(ny) || nx < 4 || ny < 2 || nx > kTwN || ny > kTwN)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "the off-plane field needs power-of-two nx >= 4, ny >= 2 (got %d x %d)",
+                   nx, ny);
+  for (int l = 0; l < nl; ++l)
+    if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
+  Engine* e = h->eng;
+  CK(cudaSetDevice(e->dev));
+  int rc = e->prec == MRM_FP64 ? ensure_ready<double>(e) : ensure_ready<float>(e);
+  if (rc) {
+    h->err = e->err;
+    return rc;
+  }
+  // calculate_off_field_tensor (off_field.f90:216-320): source layer ks, slab above the media
+  const mrm_geom& g = h->g;
+  std::vector<PairGeom> pg(nl);
+  const bool sul_p = sul_mu > 1.0, head_p = head_mu > 1.0;
+  const double mus = sul_p ? std::max(0.0, (std::max(1.0, sul_mu) - 1.0) / (std::max(1.0, sul_mu) + 1.0)) : 0.0;
+  const double mush = head_p ? std::max(0.0, (std::max(1.0, head_mu) - 1.0) / (std::max(1.0, head_mu) + 1.0)) : 0.0;
+  std::vector<double> hdz(nl);
+  hdz[0] = fly_height;
+  for (int k = 1; k < nl; ++k) hdz[k] = hdz[k - 1] + g.dz[k - 1] + g.il_space[k];
+  for (int k = 0; k < nl; ++k) hdz[k] += 0.5 * g.dz[k];
+  double zob = space_to_sul + zoff;
+  for (int k = 0; k < nl; ++k) zob += g.dz[k] + (k != nl - 1 ? g.il_space[k] : 0.0);
+  const double zot = zob + dzobs;
+  double zsb = space_to_sul;
+  for (int ks = nl - 1; ks >= 0; --ks) {
+    const double zst = zsb + g.dz[ks];
+    PairGeom& p = pg[ks];
+    p.dz_s = g.dz[ks];
+    p.dz_o = dzobs;
+    p.rz = 0.5 * (zst - zot + zsb - zob);
+    p.rz_sul = 0.5 * (-zst - zot - zsb - zob);
+    p.f_sul = mus;
+    p.rz_head = hdz[ks] + fly_height - (zoff + 0.5 * dzobs);
+    p.f_head = mush;
+    p.norm = 1.0 / (g.dx * g.dy * dzobs * (double)nx * (double)ny);
+    zsb = zst + g.il_space[ks];
+  }
+  const int ph = nx / 2 + 1, lgx = ilog2(nx), lgy = ilog2(ny);
+  const size_t plane = (size_t)nx * ny, hplane = (size_t)ph * ny;
+  void *d_pg = nullptr, *d_t = nullptr, *d_ts = nullptr, *d_m = nullptr, *d_ms = nullptr, *d_h = nullptr,
+       *d_out = nullptr, *d_tw = nullptr;
+  auto finish = [&](int code) {
+    for (void* q : {d_pg, d_t, d_ts, d_m, d_ms, d_h, d_out, d_tw}) {
+      void* qq = q;
+      dfree(qq);
+    }
+    return code;
+  };
+  rc = dmalloc(errp, &d_pg, sizeof(PairGeom) * nl);
+  if (!rc) rc = dmalloc(errp, &d_t, sizeof(double) * 9 * nl * plane);
+  if (!rc) rc = dmalloc(errp, &d_ts, sizeof(double) * 2 * 9 * nl * hplane);
+  if (!rc) rc = dmalloc(errp, &d_m, sizeof(double) * 3 * nl * plane);
+  if (!rc) rc = dmalloc(errp, &d_ms, sizeof(double) * 2 * 3 * nl * hplane);
+  if (!rc) rc = dmalloc(errp, &d_h, sizeof(double) * 2 * 3 * hplane);
+  if (!rc) rc = dmalloc(errp, &d_out, sizeof(double) * 3 * plane);
+  if (!rc) rc = dmalloc(errp, &d_tw, sizeof(double) * 2 * kTwN);
+  if (rc) return finish(rc);
+  std::vector<double> tw(2 * kTwN);
+  for (int k = 0; k < kTwN; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)kTwN;
+    tw[2 * k] = std::cos(a);
+    tw[2 * k + 1] = std::sin(a);
+  }
+  const cudaStream_t st = e->st;
+  auto ok = [&](cudaError_t c) { return c == cudaSuccess; };
+  if (!ok(cudaMemcpyAsync(d_tw, tw.data(), sizeof(double) * 2 * kTwN, cudaMemcpyHostToDevice, st)) ||
+      !ok(cudaMemcpyAsync(d_pg, pg.data(), sizeof(PairGeom) * nl, cudaMemcpyHostToDevice, st)))
+    return finish(set_err(errp, MRM_ERR_CUDA, "off-plane field: copy"));
+  const Cx<double>* tw64 = static_cast<const Cx<double>*>(d_tw);
+  const long long tot = (long long)nl * plane;
+  tensor_real_kernel<<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(static_cast<double*>(d_t),
+                                                                     static_cast<const PairGeom*>(d_pg), nl, nx, ny,
+                                                                     g.dx, g.dy, num_images);
+  if (e->prec == MRM_FP64)
+    mgrid_kernel<double><<<dim3((unsigned)((plane + 255) / 256), nl), 256, 0, st>>>(
+        static_cast<const RunDev<double>*>(e->d_runs), h->slot, static_cast<double*>(d_m));
+  else
+    mgrid_kernel<float><<<dim3((unsigned)((plane + 255) / 256), nl), 256, 0, st>>>(
+        static_cast<const RunDev<float>*>(e->d_runs), h->slot, static_cast<double*>(d_m));
+  const size_t s1 = 2 * (size_t)pad_stride(nx / 2) * sizeof(Cx<double>), s2 = 2 * (size_t)pad_stride(ny) * sizeof(Cx<double>);
+  if (!ok(allow_smem((const void*)r2c_rows_f64, s1)) || !ok(allow_smem((const void*)c2c_cols_f64, s2)) ||
+      !ok(allow_smem((const void*)c2c_cols_f64_inv, s2)) || !ok(allow_smem((const void*)c2r_rows_f64, s1)))
+    return finish(set_err(errp, MRM_ERR_CUDA, "off-plane field: shared memory"));
+  // forward transforms of the tensor and of M, the products, the inverse transform
+  r2c_rows_f64<<<(unsigned)(9 * nl * ny), 256, s1, st>>>(static_cast<const double*>(d_t), static_cast<Cx<double>*>(d_ts),
+                                                           lgx, ny, tw64);
+  c2c_cols_f64<<<(unsigned)(9 * nl * ph), 256, s2, st>>>(static_cast<Cx<double>*>(d_ts), lgy, ph, tw64);
+  r2c_rows_f64<<<(unsigned)(3 * nl * ny), 256, s1, st>>>(static_cast<const double*>(d_m), static_cast<Cx<double>*>(d_ms),
+                                                           lgx, ny, tw64);
+  c2c_cols_f64<<<(unsigned)(3 * nl * ph), 256, s2, st>>>(static_cast<Cx<double>*>(d_ms), lgy, ph, tw64);
+  off_mac_kernel<<<(unsigned)((hplane + 255) / 256), 256, 0, st>>>(static_cast<const Cx<double>*>(d_ts),
+                                                                     static_cast<const Cx<double>*>(d_ms),
+                                                                     static_cast<Cx<double>*>(d_h), nl, (long long)hplane);
+  c2c_cols_f64_inv<<<(unsigned)(3 * ph), 256, s2, st>>>(static_cast<Cx<double>*>(d_h), lgy, ph, tw64);
+  c2r_rows_f64<<<(unsigned)(3 * ny), 256, s1, st>>>(static_cast<const Cx<double>*>(d_h), static_cast<double*>(d_out), lgx,
+                                                    tw64);
+  if (!ok(cudaGetLastError()) ||
+      !ok(cudaMemcpyAsync(out, d_out, sizeof(double) * 3 * plane, cudaMemcpyDeviceToHost, st)) ||
+      !ok(cudaStreamSynchronize(st)))
+    return finish(set_err(errp, MRM_ERR_CUDA, "off-plane field: %s", cudaGetErrorString(cudaGetLastError())));
+  return finish(MRM_OK);
 }
 
 int mrm_gpu_build_tensor(mrm_gpu* h) {

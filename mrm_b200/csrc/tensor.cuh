@@ -187,6 +187,54 @@ __global__ void __launch_bounds__(256) c2c_cols_f64(Cx<double>* __restrict__ dat
   for (int j = threadIdx.x; j < py; j += blockDim.x) base[(long long)j * ph] = Y[j];
 }
 
+// inverse FP64 complex FFT along y of [p][py][ph], in place (unnormalised)
+__global__ void __launch_bounds__(256) c2c_cols_f64_inv(Cx<double>* __restrict__ data, int lgpy, int ph,
+                                                        const Cx<double>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int py = 1 << lgpy;
+  const long long p = blockIdx.x / ph;
+  const int k = blockIdx.x - (int)(p * ph);
+  const int cs = pad_stride(py);
+  Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* B = A + cs;
+  Cx<double>* base = data + p * (long long)py * ph + k;
+  for (int j = threadIdx.x; j < py; j += blockDim.x) A[j] = base[(long long)j * ph];
+  __syncthreads();
+  Cx<double>* Y = block_fft<double, +1>(A, B, lgpy, 1, cs, tw, kTwLog);
+  for (int j = threadIdx.x; j < py; j += blockDim.x) base[(long long)j * ph] = Y[j];
+}
+
+// FP64 c2r along x (FFTW's unnormalised c2r): rows [p][py][px/2+1] -> real
+// [p][py][px] through the half-length complex transform (imaginary parts of
+// the k = 0 and k = px/2 bins ignored)
+__global__ void __launch_bounds__(256) c2r_rows_f64(const Cx<double>* __restrict__ in, double* __restrict__ out,
+                                                    int lgpx, const Cx<double>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lgM = lgpx - 1, M = 1 << lgM, ph = M + 1, px = 2 * M;
+  const long long row = blockIdx.x;  // p*py + j
+  const int cs = pad_stride(M);
+  Cx<double>* A = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* B = A + cs;
+  const Cx<double>* X = in + row * ph;
+  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+    Cx<double> a = X[k], b = X[M - k];
+    if (k == 0) {
+      a.y = 0.0;
+      b.y = 0.0;
+    }
+    const Cx<double> e = cadd(a, cconj(b)), o = csub(a, cconj(b));
+    const Cx<double> w = cconj(twiddle(tw, k, lgpx));  // e^{+2 pi i k / px}
+    A[k] = cadd(e, cmul_i(cmul(o, w), 1.0));
+  }
+  __syncthreads();
+  Cx<double>* Z = block_fft<double, +1>(A, B, lgM, 1, cs, tw, kTwLog);
+  double* dst = out + row * px;
+  for (int n = threadIdx.x; n < M; n += blockDim.x) {
+    dst[2 * n] = Z[n].x;
+    dst[2 * n + 1] = Z[n].y;
+  }
+}
+
 // block-wide max of two non-negative doubles, one atomicMax per block
 __device__ __forceinline__ void block_max2(double a, double b, unsigned long long* ga,
                                            unsigned long long* gb) {

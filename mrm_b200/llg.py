@@ -80,8 +80,12 @@ class _RunMixin:
         self._check(_lib.load().mrm_gpu_build_tensor(self.h))
 
     def upload_tensor(self, n2d: np.ndarray):
+        """Real-space FP64 tensor (n_lay, n_lay, 9, py, px) on this handle's FFT grid."""
         n2d = f64(n2d)
         px, py = self.fft_grid()
+        nl = self.medium.n_lay
+        if n2d.shape != (nl, nl, 9, py, px):
+            raise ValueError(f"tensor of shape {n2d.shape}; this handle's grid needs {(nl, nl, 9, py, px)}")
         self._check(_lib.load().mrm_gpu_upload_tensor(self.h, fptr(n2d), px, py))
 
     def download_tensor(self) -> np.ndarray:
@@ -232,6 +236,16 @@ class GpuSim(_RunMixin):
     def profile(self, reps: int, dt: float) -> np.ndarray:
         out = np.zeros(4)
         self._check(_lib.load().mrm_gpu_profile(self.h, int(reps), float(dt), fptr(out)))
+        return out
+
+    def off_field(self, zoff: float, dzobs: float, head_mu: float = 1.0, fly_height: float = 8e-7,
+                  sul_mu: float = 1.0, space_to_sul: float = 40e-7, num_images: int = 2) -> np.ndarray:
+        """Stray field (3, ny, nx) in Oe averaged over a slab dzobs thick whose bottom is
+        zoff above the media (include/mrm_gpu.h mrm_gpu_off_field); lengths in cm."""
+        out = np.zeros((3, self.medium.ny, self.medium.nx))
+        self._check(_lib.load().mrm_gpu_off_field(self.h, float(zoff), float(dzobs), float(head_mu),
+                                                  float(fly_height), float(sul_mu), float(space_to_sul),
+                                                  int(num_images), fptr(out)))
         return out
 
     def step_adaptive(self, nsteps: int, dt: float, max_dmdt: float = 1.0, llg_type: int = -3,

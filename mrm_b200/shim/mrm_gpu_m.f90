@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -108,6 +108,14 @@ module mrm_gpu_m
       type(C_PTR), value :: h
       integer(C_INT), value :: layer
       real(C_DOUBLE), intent(in) :: cubic_axis(3, 3, *)
+    end function
+    integer(C_INT) function c_off_field(h, zoff, dzobs, head_mu, fly_height, sul_mu, space_to_sul, num_images, out) &
+        bind(C, name="mrm_gpu_off_field")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      real(C_DOUBLE), value :: zoff, dzobs, head_mu, fly_height, sul_mu, space_to_sul
+      integer(C_INT), value :: num_images
+      real(C_DOUBLE), intent(out) :: out(*)
     end function
     integer(C_INT) function c_step_adaptive(h, nsteps, llg_type, dt_frac, dt_max, max_dm, dt, max_dmdt, stats) &
         bind(C, name="mrm_gpu_step_adaptive")
@@ -264,6 +272,18 @@ contains
     integer, intent(in) :: layer
     real(C_DOUBLE), intent(in) :: cubic_axis(:, :, :)
     ok_p = ok(c_set_cubic_axes(h, int(layer - 1, C_INT), cubic_axis))
+  end function
+
+  ! stray field of the current state on the slab zoff..zoff+dzobs (cm) above the
+  ! media, as init_demag + get_off_field of off_field.f90 compute it:
+  ! h(:,:,1:3) = hx, hy, hz on the nx x ny grid (include/mrm_gpu.h mrm_gpu_off_field)
+  logical function gpu_off_field(h, zoff, dzobs, mu_head, fly_height, sul_mu, space_to_sul, num_images, hxyz) &
+      result(ok_p)
+    type(C_PTR), intent(in) :: h
+    real(C_DOUBLE), intent(in) :: zoff, dzobs, mu_head, fly_height, sul_mu, space_to_sul
+    integer, intent(in) :: num_images
+    real(C_DOUBLE), intent(out) :: hxyz(:, :, :)
+    ok_p = ok(c_off_field(h, zoff, dzobs, mu_head, fly_height, sul_mu, space_to_sul, int(num_images, C_INT), hxyz))
   end function
 
   ! iter steps of llg()'s adaptive loop (dt_frac /= 0): llgp%dt and llgp%max_dmdt

@@ -1343,6 +1343,69 @@ int orc_step_adaptive(void* h, int nsteps, int type, double dt_frac, double dt_m
   return 0;
 }
 
+// calculate_off_field_tensor (off_field.f90:216-320) and get_off_field
+// (:55-108) on the nx x ny data grid: out[(c*ny + j)*nx + i] = H_c at the
+// observation slab (bottom zoff above the top layer, thickness dzobs)
+int orc_off_field(void* h, double zoff, double dzobs, double head_mu, double fly_height, double sul_mu,
+                  double space_to_sul, int nimg, double* out) {
+  Sim* s = static_cast<Sim*>(h);
+  const int nx = s->nx, ny = s->ny, nl = s->nl;
+  const size_t plane = (size_t)nx * ny, hplane = (size_t)(nx / 2 + 1) * ny;
+  const bool sul_p = sul_mu > 1.0, head_p = head_mu > 1.0;  // off_field.f90:191,251-256
+  const double mus = sul_p ? std::max(0.0, (std::max(1.0, sul_mu) - 1.0) / (std::max(1.0, sul_mu) + 1.0)) : 0.0;
+  const double mush = head_p ? std::max(0.0, (std::max(1.0, head_mu) - 1.0) / (std::max(1.0, head_mu) + 1.0)) : 0.0;
+  std::vector<double> hdz(nl);
+  hdz[0] = fly_height;
+  for (int k = 1; k < nl; ++k) hdz[k] = hdz[k - 1] + s->dz[k - 1] + s->il_space[k];
+  for (int k = 0; k < nl; ++k) hdz[k] += 0.5 * s->dz[k];
+  double zob = space_to_sul + zoff;
+  for (int k = 0; k < nl; ++k) {
+    zob += s->dz[k];
+    if (k != nl - 1) zob += s->il_space[k];
+  }
+  const double zot = zob + dzobs;
+  FFT2 f;
+  f.init(nx, ny);
+  std::vector<double> nn(9 * plane), t(9 * plane), grid(3 * plane);
+  std::vector<cd> T(9 * hplane), X(3 * hplane), H(3 * hplane, cd(0, 0));
+  double zsb = space_to_sul;
+  for (int ks = nl - 1; ks >= 0; --ks) {
+    const double zst = zsb + s->dz[ks];
+    std::fill(t.begin(), t.end(), 0.0);
+    auto add = [&](double rz, double fxy, double fz) {
+      plane_to_plane(nx, ny, s->dx, s->dy, s->dz[ks], dzobs, rz, nimg, nimg, nn.data());
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          for (size_t p = 0; p < plane; ++p)
+            t[(3 * b + a) * plane + p] += (a < 2 ? fxy : fz) * nn[(a * 3 + b) * plane + p];
+    };
+    add(0.5 * (zst - zot + zsb - zob), 1.0, 1.0);
+    if (sul_p) add(0.5 * (-zst - zot - zsb - zob), -mus, mus);
+    if (head_p) add(hdz[ks] + fly_height - (zoff + 0.5 * dzobs), -mush, mush);
+    const double norm = 1.0 / (s->dx * s->dy * dzobs * (double)nx * (double)ny);
+    for (auto& v : t) v *= norm;
+    // get_mag of layer ks on the data grid
+    std::fill(grid.begin(), grid.end(), 0.0);
+    const Layer& Ly = s->L[ks];
+    const double* m = Ly.m[s->in].data();
+    for (int n = 0; n < Ly.N; ++n) {
+      const double fm = Ly.ms[n] * Ly.ms_scale[n];
+      for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
+        const size_t cell = (size_t)Ly.g2c_j[q] * nx + Ly.g2c_i[q];
+        for (int a = 0; a < 3; ++a) grid[a * plane + cell] = fm * m[3 * n + a];
+      }
+    }
+    for (int c = 0; c < 9; ++c) f.r2c(&t[c * plane], &T[c * hplane]);
+    for (int b = 0; b < 3; ++b) f.r2c(&grid[b * plane], &X[b * hplane]);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        for (size_t q = 0; q < hplane; ++q) H[a * hplane + q] += T[(3 * a + b) * hplane + q] * X[b * hplane + q];
+    zsb = zst + s->il_space[ks];
+  }
+  for (int a = 0; a < 3; ++a) f.c2r(&H[a * hplane], out + a * plane);
+  return 0;
+}
+
 int orc_stats_size(void) { return (int)sizeof(Stats); }
 
 }  // extern "C"

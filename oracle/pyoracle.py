@@ -63,6 +63,7 @@ def lib():
         L.orc_eval_field.argtypes = [vp, d]
         L.orc_step.argtypes = [vp, i, d, i, vp, vp]
         L.orc_step_adaptive.argtypes = [vp, i, i, d, d, P(d), P(d), P(d), vp]
+        L.orc_off_field.argtypes = [vp, d, d, d, d, d, d, i, P(d)]
         L.orc_mt_u32.argtypes = [i, i, P(C.c_uint32)]
         L.orc_mt_state.argtypes = [i, P(C.c_uint32)]
         L.orc_mt_normals.argtypes = [i, i, P(d)]
@@ -278,6 +279,14 @@ class OracleSim:
 
     def eval_field(self, t: float):
         lib().orc_eval_field(self.h, t)
+
+    def off_field(self, zoff: float, dzobs: float, head_mu: float = 1.0, fly_height: float = 8e-7,
+                  sul_mu: float = 1.0, space_to_sul: float = 40e-7, num_images: int = 2) -> np.ndarray:
+        """Stray field (3, ny, nx) at the observation slab (off_field.f90)."""
+        out = np.zeros((3, self.medium.ny, self.medium.nx))
+        assert lib().orc_off_field(self.h, zoff, dzobs, head_mu, fly_height, sul_mu, space_to_sul, num_images,
+                                   _p(out)) == 0
+        return out
 
     def step_adaptive(self, nsteps: int, dt: float, max_dmdt: float = 1.0, llg_type: int = -3,
                       dt_frac: float = 0.2, dt_max: float = 1e-8, max_dm=None):

@@ -78,7 +78,8 @@ def test_grain_file_round_trip_and_dynamics(tmp_path):
     (s0, m0), (s1, m1) = runs
     for a, b in zip(m0, m1):
         assert np.array_equal(a, b)
-    assert s0["energy"] == s1["energy"]
+    # the energy weighs by the volumes, which the file's dz round trip returns to 1e-15
+    assert abs(s0["energy"] - s1["energy"]) <= 1e-14 * abs(s0["energy"])
 
 
 def test_tensor_cache_round_trip(tmp_path):

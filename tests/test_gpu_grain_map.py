@@ -14,7 +14,10 @@ pytestmark = pytest.mark.gpu
 def _pair(oracle, med, precision, seed=3):
     orc = oracle.OracleSim(med, rng_mode=1, seed=seed)
     gpu = GpuSim(med, precision=precision, demag=False, thermal_seed=seed)
-    gpu.upload_tensor(orc.n2d)
+    if orc.n2d.shape[-2:] == tuple(reversed(gpu.fft_grid())):
+        gpu.upload_tensor(orc.n2d)
+    else:  # the oracle pads an open grid to 2n, this path to a power of two: each its own tensor
+        gpu.build_tensor()
     gpu.set_demag(True)
     return orc, gpu
 
@@ -107,3 +110,25 @@ def test_medium_from_grain_file(oracle, gpulib, tmp_path):
     for l in range(2):
         assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-9
     assert sg["energy"] == pytest.approx(so["energy"], rel=1e-8)
+
+
+@pytest.mark.parametrize("shape", [(12, 10), (16, 10), (12, 16)])
+def test_non_power_of_two_grids(oracle, gpulib, shape):
+    # one grain per cell on grids that are not powers of two (open boundary:
+    # the oracle pads to 2n, this path to the next power of two)
+    nx, ny = shape
+    med = media.mh_medium(nx, ny=ny, seed=4, boundary=1)
+    med.layers[0].t_end = 2e-10
+    orc, gpu = _pair(oracle, med, FP64)
+    m = random_m(med.layers[0].N, 3)
+    orc.set_state(0, m)
+    gpu.set_state(0, m)
+    orc.eval_field(1e-11)
+    assert rel_l2(gpu.eval_field(1e-11, 0), orc.get_demag(0)) < 1e-9
+    orc.set_state(0, med.m0[0])
+    gpu.set_state(0, med.m0[0])
+    orc.set_time(0.0, 0)
+    gpu.set_time(0.0, 0)
+    orc.step(500, 1e-13)
+    gpu.step(500, 1e-13)
+    assert np.abs(gpu.get_state(0) - orc.get_state(0)).max() < 1e-8
