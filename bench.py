@@ -409,7 +409,32 @@ def write_leg(torch, local, steps=2000):
             "grains": grains, "value": grains * steps / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
             "us_per_heun_step": 1e3 * ms / steps, "mave_top": np.asarray(st["mave_l"][0]).tolist(),
             "readback": {"call": "off_field " + READBACK_TEXT, "grid": [1024, 256], "ms_per_call": off_ms,
-                         "hz_rms_oe": float(np.sqrt(np.mean(hr[2] ** 2)))}}
+                         "hz_rms_oe": float(np.sqrt(np.mean(hr[2] ** 2)))},
+            "tabulated": table_write_leg(torch, local, steps)}
+
+
+def table_write_leg(torch, local, steps):
+    """The same write driven by a tabulated head-field profile per layer (97 x 33
+    nodes, bilinear per cell, the way the reference drives writes) instead of
+    the analytic head: the field-table path's cost in the stepping kernels."""
+    from mrm_b200 import FP32, GpuSim, media
+    med = media.table_write_medium(1024, 256, seed=1, temperature=300.0)
+    sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.step(48, DT, stats=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.enqueue(steps, DT)
+    e1.record(ext)
+    sim.stats()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    grains = 2 * 1024 * 256
+    return {"workload": f"two-layer 1024x256x2 write, tabulated head profile (97 x 33 nodes) at 20 m/s, "
+                        f"STE polarity, T=300 K, FP32, {steps} Heun steps",
+            "value": grains * steps / (ms * 1e-3), "unit": UNIT, "us_per_heun_step": 1e3 * ms / steps}
 
 
 def mix_leg(torch, local, steps=5000, nreal=64):

@@ -169,6 +169,26 @@ int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int 
 int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double hg, double velocity, double x0,
                            double t0, double bit_time, uint64_t pattern, int nbits);
 
+/* Tabulated (moving) field profile on `layer` (file_applied + the moving
+ * branch of get_appl + get_applied, applied.f90:711-813,896-903,1471-1520,
+ * 1757-1776, field.f90:546-560): vfld(3, nfx, nfy) in Oe (Fortran order,
+ * vfld[c + 3*(i + nfx*j)]) at ascending node positions xpos(nfx), ypos(nfy)
+ * (cm, nfx, nfy >= 2).  At time t the grid cell (i, j) centre
+ * ((i+1/2) dx, (j+1/2) dy) sits at table position
+ *   x = (i+1/2) dx - (offset_x + vel_x (t - t_origin) - ref_x)   (y alike);
+ * each axis takes the interval closed by the first node above x (from the
+ * second node on, at most the last) with the lower node's weight
+ * clamp((x_hi - x)/(x_hi - x_lo), 0, 1) (set); the cell's field is the
+ * bilinear sum scaled by the layer's time scale s(t) (the linear ramp of
+ * mrm_gpu_set_uniform_field or the function of mrm_gpu_set_field_function,
+ * whose direction the profile replaces), and a grain's field the average over
+ * its cells.  offset_x/offset_y below -1e200 take file_applied's default, the
+ * grid centre (nx dx/2, ny dy/2).  nfx = nfy = 0 removes the profile.
+ * Replaces a write head on the layer. */
+int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const double* xpos, const double* ypos,
+                            const double* vfld, double vel_x, double vel_y, double offset_x, double offset_y,
+                            double ref_x, double ref_y, double t_origin);
+
 /* Cubic magnetocrystalline anisotropy on `layer` (get_cubic_hk,
  * field.f90:377-395; set up by construct_hk_direction with k_cubic,
  * construct_grain.f90:1620-1625, which then drops the uniaxial axis):

@@ -35,7 +35,7 @@ EXPORTS = [
     "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
     "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile", "mrm_gpu_set_head_field",
     "mrm_gpu_set_shape", "mrm_gpu_set_autotune", "mrm_gpu_get_shape", "mrm_gpu_check_device",
-    "mrm_gpu_set_cubic_axes", "mrm_gpu_step_adaptive", "mrm_gpu_off_field",
+    "mrm_gpu_set_cubic_axes", "mrm_gpu_step_adaptive", "mrm_gpu_off_field", "mrm_gpu_set_field_table",
 ]
 
 
@@ -128,6 +128,7 @@ def load(path: str = LIB_PATH):
         "mrm_gpu_set_cubic_axes": ([vp, i, pd], i),
         "mrm_gpu_step_adaptive": ([vp, i, i, d, d, pd, pd, pd, vp], i),
         "mrm_gpu_off_field": ([vp, d, d, d, d, d, d, i, pd], i),
+        "mrm_gpu_set_field_table": ([vp, i, i, i, pd, pd, pd, d, d, d, d, d, d, d], i),
         "mrm_gpu_set_shape": ([vp, i, i, i], i),
         "mrm_gpu_set_autotune": ([vp, i], i),
         "mrm_gpu_get_shape": ([vp, P(i)], i),

@@ -39,6 +39,18 @@ MRM_HD Cx<R> cscale(Cx<R> a, R s) { return {a.x * s, a.y * s}; }
 template <typename R>
 MRM_HD Cx<R> cmul_i(Cx<R> a, R s) { return {-s * a.y, s * a.x}; }
 
+// Tabulated (moving) field profile of a layer, in device memory: file_applied
+// + set + interpolate (applied.f90:711-813,1471-1520,1757-1776).  Values
+// v[c + 3 (i + nx j)] (Oe) at table nodes pos[i] (x), pos[nx + j] (y) (cm); the
+// profile's origin sits at ox + vx (t - t0) - rx (y alike) on the grid, whose
+// cell (i, j) centre is ((i + 1/2) dx, (j + 1/2) dy).
+struct TabDev {
+  const double* v;
+  const double* pos;
+  int nx, ny;
+  double ox, oy, vx, vy, rx, ry, t0, dx, dy;
+};
+
 // Per-layer device view of one run.  State vectors are float4/double4
 // "SoA of 4-vectors": (x,y,z,unused) per grain for one 16/32-byte load.
 template <typename R>
@@ -72,6 +84,7 @@ struct LayerDev {
   const int* gci;
   const int* gcs;
   V4<R>* hdm;
+  V4<R>* hapm;       // grain-averaged tabulated applied field per cell (map layers with a table)
   const R* ucol;     // columnar form of the interlayer coupling (grain n <-> grain n)
   const R* lcol;
   double hdir[3];
@@ -85,6 +98,7 @@ struct LayerDev {
   double hd_gap, hd_z, hd_hg, hd_v, hd_x0, hd_t0, hd_tbit, hd_dx;
   unsigned long long hd_bits;
   int hd_nbits;
+  const struct TabDev* tab;  // tabulated field profile (null: the uniform hdir applies)
   double temperature;
   double tfac;  // sqrt(temperature / dt), set with the run's dt
   double gamma;

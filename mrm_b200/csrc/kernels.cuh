@@ -29,12 +29,13 @@ namespace mrm {
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
 enum Flags {
   kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32,
-  kFlagMapped = 64, kFlagDemagOnly = 128
+  kFlagMapped = 64, kFlagDemagOnly = 128, kFlagCorrTime = 256
 };
 // kFlagMapped (kPred, kCorr, kEval): the demag field comes from an earlier
 // evaluation's per-cell values averaged over each grain's cells (L.hdm; L.hd
 // with one grain per cell), not from this launch's inverse row transform.
 // kFlagDemagOnly (kEval): the inverse transforms' demag per cell (L.hd) only.
+// kFlagCorrTime (gather_demag_kernel): the applied field at the corrector's time.
 // kFlagStoredField (kPred): the push uses the stored field L.hf instead of the
 // field of m_n -- push_m's retry after a rejected adaptive step, whose field
 // is still the one of the rejected predicted state (llg.f90:1205-1266)
@@ -115,6 +116,49 @@ MRM_D void karlqvist(R u, R g, R z, R hg, R& hx, R& hz) {
   hx = hg / pi * (atan(a / z) - atan(b / z));
   hz = hg / ((R)2 * pi) * log((b * b + z * z) / (a * a + z * z));
 }
+
+// Interpolation weights of a tabulated field profile: the table interval
+// [k, k+1] and the weight f of node k for one mesh coordinate.
+struct TabW {
+  int k, pad;
+  double f;
+};
+
+// set (applied.f90:1757-1776) for one mesh coordinate x over the n >= 2
+// ascending nodes pos[]: the first node above x, searched from the second
+// node on and capped at the last, closes the interval; the lower node's
+// weight is clamped to [0, 1].  (A bisection: the reference's sweep gives the
+// same node on ascending positions.)
+MRM_D TabW tab_weight(const double* __restrict__ pos, int n, double x) {
+  int lo = 1, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (pos[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  TabW w;
+  w.k = lo - 1;
+  w.pad = 0;
+  w.f = fmax(0.0, fmin(1.0, (pos[lo] - x) / (pos[lo] - pos[lo - 1])));
+  return w;
+}
+
+// interpolate (applied.f90:1471-1520): s-scaled bilinear value of the vector
+// profile at one cell from its column and row weights
+MRM_D void tab_value(const double* __restrict__ v, int tnx, TabW wx, TabW wy, double s, double& vx, double& vy,
+                     double& vz) {
+  const double yf = s * wy.f, yfc = s * (1.0 - wy.f);
+  const double w00 = wx.f * yf, w10 = (1.0 - wx.f) * yf, w01 = wx.f * yfc, w11 = (1.0 - wx.f) * yfc;
+  const double* __restrict__ a = v + 3 * ((size_t)wy.k * tnx + wx.k);
+  const double* __restrict__ c = a + 3 * (size_t)tnx;
+  vx = w00 * a[0] + w10 * a[3] + w01 * c[0] + w11 * c[3];
+  vy = w00 * a[1] + w10 * a[4] + w01 * c[1] + w11 * c[4];
+  vz = w00 * a[2] + w10 * a[5] + w01 * c[2] + w11 * c[5];
+}
+
+// shared memory of a row block's table weights (grid columns, then the
+// block's rows; at most 8 rows per block)
+MRM_HD int field_table_bytes(int nx) { return (nx + 8) * (int)sizeof(TabW); }
 
 // shared memory of a row block's head-field table (one (h_x, h_z) per grid column)
 template <typename R>
@@ -280,11 +324,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // a layer under the moving write head gets its head field per grid column in
   // a table after the FFT buffers (the host reserves it), then the staging area
   // (its byte offset; 0: no head)
-  const int htab_off = GEN && rd.L[tk.y].func == kFuncHead
+  // (a tabulated field profile gets its interpolation weights there instead)
+  const bool ftab = GEN && STAGE != kInit && rd.L[tk.y].tab != nullptr;
+  const int htab_off = GEN && (rd.L[tk.y].func == kFuncHead || ftab)
                            ? (int)(reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) - smem_raw)
                            : 0;
   unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) +
-                       (htab_off ? head_table_bytes<R>(rd.nx) : 0);
+                       (ftab ? field_table_bytes(rd.nx) : htab_off ? head_table_bytes<R>(rd.nx) : 0);
   if (htab_off && (long long)(stg - smem_raw) > (long long)dynamic_smem_bytes()) {  // host bug: no room reserved
     if (threadIdx.x == 0) atomicOr(err, kErrShape);
     return;
@@ -446,7 +492,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
   const double t_stage = (STAGE == kCorr) ? t_now + (mid ? 0.5 * rd.dt : rd.dt) : t_now;
   const double sc = ramp(L, t_stage);
-  const R hax = (R)(sc * L.hdir[0]), hay = (R)(sc * L.hdir[1]), haz = (R)(sc * L.hdir[2]);
+  // a layer's field is its uniform direction or its tabulated profile, scaled
+  const R hax = ftab ? (R)0 : (R)(sc * L.hdir[0]), hay = ftab ? (R)0 : (R)(sc * L.hdir[1]),
+          haz = ftab ? (R)0 : (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
   const R tfac = thermal ? (R)L.tfac : (R)0;
@@ -457,9 +505,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // stepping stages add it to the block's demag values in shared memory (zero
   // when demag is off), so their per-grain loop is the same with or without a
   // head; the evaluation stage keeps demag apart and reads a per-column table.
-  const bool fold_head = (STAGE == kPred || STAGE == kCorr) && htab_off;
+  const bool fold_head = (STAGE == kPred || STAGE == kCorr) && htab_off && !ftab;
   const bool use_hdr = !mapped && (demag || fold_head);
-  if (STAGE != kInit && htab_off) {
+  if (ftab) {
+    // set (applied.f90:896-902) for the grid columns and the block's rows
+    TabW* tw = reinterpret_cast<TabW*>(smem_raw + htab_off);
+    const TabDev& T = *L.tab;
+    const double ox = T.ox + T.vx * (t_stage - T.t0) - T.rx;
+    const double oy = T.oy + T.vy * (t_stage - T.t0) - T.ry;
+    for (int c = threadIdx.x; c < nx + nrows; c += BLOCK)
+      tw[c] = c < nx ? tab_weight(T.pos, T.nx, ((double)c + 0.5) * T.dx - ox)
+                     : tab_weight(T.pos + T.nx, T.ny, ((double)(row0 + c - nx) + 0.5) * T.dy - oy);
+    __syncthreads();
+  } else if (STAGE != kInit && htab_off) {
     double xh, pol;
     head_state(L, t_stage, &xh, &pol);
     R* hw = reinterpret_cast<R*>(Z);
@@ -522,7 +580,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     // applied field of this grain: the uniform part (plus the write head's in
     // the evaluation stage; the stepping stages carry it in hdx, hdz)
     R apx = hax, apy = hay, apz = haz;
-    if constexpr (STAGE == kEval) {
+    if (ftab) {
+      // the profile at the cell; a grain of several cells takes the average
+      // over its cells that the gather kernel formed (get_applied,
+      // field.f90:546-560)
+      if (mapped && L.cgrain) {
+        const V4<R> a = L.hapm[n];
+        apx += a.x;
+        apy += a.y;
+        apz += a.z;
+      } else if (!(STAGE == kEval && (flags & kFlagDemagOnly))) {
+        const TabW* tw = reinterpret_cast<const TabW*>(smem_raw + htab_off);
+        double vx, vy, vz;
+        tab_value(L.tab->v, L.tab->nx, tw[i], tw[nx + rr], sc, vx, vy, vz);
+        apx += (R)vx;
+        apy += (R)vy;
+        apz += (R)vz;
+      }
+    } else if (STAGE == kEval) {
       if (htab_off) {
         const Cx<R> kh = reinterpret_cast<const Cx<R>*>(smem_raw + htab_off)[i];
         apx += kh.x;
@@ -1040,8 +1115,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
 // written to every cell of the grain (get_magnetostatic, field.f90:449-470:
 // FP64 sum over the cells, divided by their count).  Block row y: run y /
 // kMaxLayers, layer y % kMaxLayers; layers with one grain per cell are skipped.
+// A tabulated applied-field profile is averaged the same way into L.hapm
+// (get_applied, field.f90:546-560), at the time of the stage that follows
+// (istep, kFlagCorrTime, kFlagMid as the row kernel reads them).
 template <typename R>
-__global__ void gather_demag_kernel(const RunDev<R>* __restrict__ runs, int nruns) {
+__global__ void gather_demag_kernel(const RunDev<R>* __restrict__ runs, int nruns, int istep, int flags) {
   const int r = blockIdx.y / kMaxLayers, l = blockIdx.y % kMaxLayers;
   if (r >= nruns) return;
   const RunDev<R>& rd = runs[r];
@@ -1062,6 +1140,26 @@ __global__ void gather_demag_kernel(const RunDev<R>* __restrict__ runs, int nrun
   }
   const double k = (double)(q1 - q0);
   L.hdm[c] = V4<R>{(R)(x / k), (R)(y / k), (R)(z / k), (R)0};
+  if (L.tab && L.hapm) {
+    const TabDev& T = *L.tab;
+    const long long step = rd.step + istep;
+    const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
+    const double t = (flags & kFlagCorrTime) ? t_now + ((flags & kFlagMid) ? 0.5 * rd.dt : rd.dt) : t_now;
+    const double s = ramp(L, t);
+    const double ox = T.ox + T.vx * (t - T.t0) - T.rx;
+    const double oy = T.oy + T.vy * (t - T.t0) - T.ry;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int q = q0; q < q1; ++q) {
+      const int cc = L.gcs[q], j = cc / rd.nx, i = cc - j * rd.nx;
+      double vx, vy, vz;
+      tab_value(T.v, T.nx, tab_weight(T.pos, T.nx, ((double)i + 0.5) * T.dx - ox),
+                tab_weight(T.pos + T.nx, T.ny, ((double)j + 0.5) * T.dy - oy), s, vx, vy, vz);
+      ax += vx;
+      ay += vy;
+      az += vz;
+    }
+    L.hapm[c] = V4<R>{(R)(ax / k), (R)(ay / k), (R)(az / k), (R)0};
+  }
 }
 
 // llg_type 2: the predictor buffer holds m_{n+1} after the single push; copy

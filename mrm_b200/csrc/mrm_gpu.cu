@@ -56,6 +56,7 @@ struct LayerBufs {
   // CSR, grain-averaged demag per cell; null on one-grain-per-cell layers
   int *cgrain = nullptr, *gci = nullptr, *gcs = nullptr;
   void* hdm = nullptr;
+  void* hapm = nullptr;  // grain-averaged tabulated applied field per cell (map layers)
   int ng = 0;  // grains (n counts cells)
   double hdir[3] = {0, 0, 0};
   double t_start = -1e22, t_end = 1e22, s_start = 1.0, s_end = 1.0, scale = 1.0;
@@ -66,6 +67,11 @@ struct LayerBufs {
   double hd_gap = 0, hd_z = 1, hd_hg = 0, hd_v = 0, hd_x0 = 0, hd_t0 = 0, hd_tbit = 1;
   unsigned long long hd_bits = 0;
   int hd_nbits = 1;
+  // tabulated field profile (null tab: none): the device TabDev, its FP64
+  // values (3, nx, ny) and node positions (x then y)
+  void* tab = nullptr;
+  void* tb_v = nullptr;
+  void* tb_pos = nullptr;
 };
 
 struct Engine;
@@ -123,7 +129,8 @@ struct Engine {
   size_t smem_stats[2] = {0, 0};  // reductions launch of kPred (single-stage integrator), kCorr
   int cap_stats[2] = {0, 0};
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
-  bool has_head = false;             // a run has a layer under the write head (general kernels)
+  bool has_head = false;             // a run has a layer under the write head or a tabulated
+                                     // field profile (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
   bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
   bool mapped = false;               // a run has grains of several cells (grain-averaged demag)
@@ -321,13 +328,16 @@ int run_stage_bytes(const mrm_gpu* r, int stage, int rows) {
 }
 
 // row-kernel shared memory before the staging area: twiddles, FFT buffers and,
-// for a run with a layer under the write head, the head-field table
+// for a run with a layer under the write head, the head-field table (with a
+// tabulated field profile, its interpolation weights)
 template <typename R>
 size_t row_fixed_smem(const mrm_gpu* r, int rpb) {
-  size_t b = (size_t)row_fft_smem<R>(r->lgpx, rpb);
-  for (int l = 0; l < r->nl; ++l)
-    if (r->L[l].func == kFuncHead) return b + (size_t)head_table_bytes<R>(r->g.nx);
-  return b;
+  size_t b = (size_t)row_fft_smem<R>(r->lgpx, rpb), t = 0;
+  for (int l = 0; l < r->nl; ++l) {
+    if (r->L[l].tab) t = std::max(t, (size_t)field_table_bytes(r->g.nx));
+    else if (r->L[l].func == kFuncHead) t = std::max(t, (size_t)head_table_bytes<R>(r->g.nx));
+  }
+  return b + t;
 }
 
 // Column-kernel shared memory for tasks of nc columns (a power of two).  The
@@ -441,6 +451,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.gci = b.gci;
     o.gcs = b.gcs;
     o.hdm = static_cast<V4<R>*>(b.hdm);
+    o.hapm = static_cast<V4<R>*>(b.hapm);
     o.ucol = static_cast<const R*>(b.ucol);
     o.lcol = static_cast<const R*>(b.lcol);
     for (int a = 0; a < 3; ++a) o.hdir[a] = b.hdir[a];
@@ -472,6 +483,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.hd_dx = r->g.dx;
     o.hd_bits = b.hd_bits;
     o.hd_nbits = b.hd_nbits;
+    o.tab = static_cast<const TabDev*>(b.tab);
   }
   return d;
 }
@@ -590,13 +602,15 @@ int build_tables(Engine* e) {
   e->has_head = false;
   e->has_cubic = false;
   e->mapped = false;
+  bool karlqvist_head = false;
   for (auto* r : e->runs)
     for (int l = 0; l < r->nl; ++l) {
-      e->has_head = e->has_head || r->L[l].func == kFuncHead;
+      karlqvist_head = karlqvist_head || r->L[l].func == kFuncHead;
+      e->has_head = e->has_head || r->L[l].func == kFuncHead || r->L[l].tab != nullptr;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
       e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
-  if (e->mapped && e->has_head)
+  if (e->mapped && karlqvist_head)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the write head needs one grain per cell (no grain maps in the batch)");
   e->nst = (int)stt.size();
   if (e->nst > e->st_cap) {
@@ -681,29 +695,29 @@ cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type, bool store
   // (inverse row transforms of every cell) averaged over the grains' cells
   const int f = f0 | (e->mapped ? kFlagMapped : 0);
   const int nr = (int)e->runs.size();
-  auto mapped_demag = [&](int i) {
+  auto mapped_demag = [&](int i, bool corr) {
     if (!e->mapped) return;
     acc(launch_row_e<R>(e, kEval, false, i, f0 | kFlagDemagOnly));
     int maxc = 1;
     for (auto* r : e->runs) maxc = std::max(maxc, r->g.nx * r->g.ny);
     acc(launch_kernel(gather_demag_kernel<R>, dim3((maxc + 255) / 256, nr * kMaxLayers), dim3(256), 0, e->st, false,
-                      static_cast<const RunDev<R>*>(e->d_runs), nr));
+                      static_cast<const RunDev<R>*>(e->d_runs), nr, i, f0 | (corr ? kFlagCorrTime : 0)));
   };
   for (int i = 0; i < k; ++i) {
     const bool last = stats && i == k - 1;
     const int lf = last ? (kFlagStats | kFlagStoreField) : 0;
     if (llg_type == 2) {
-      mapped_demag(i);
+      mapped_demag(i, false);
       acc(launch_row_e<R>(e, kPred, last, i, f | lf));
       acc(launch_col_e<R>(e, i, 0));
       acc(launch_kernel(commit_kernel<R>, dim3(e->nst), dim3(256), 0, e->st, true,
                         static_cast<const RunDev<R>*>(e->d_runs), (const Task*)e->d_stasks, i, 0));
       continue;
     }
-    mapped_demag(i);
+    mapped_demag(i, false);
     acc(launch_row_e<R>(e, kPred, false, i, f | ((stored && i == 0) ? kFlagStoredField : 0)));
     acc(launch_col_e<R>(e, i, 0));
-    mapped_demag(i);
+    mapped_demag(i, true);
     acc(launch_row_e<R>(e, kCorr, last, i, f | lf));
     acc(launch_col_e<R>(e, i, 0));
   }
@@ -985,7 +999,7 @@ int engine_eval(Engine* e) {
     for (auto* r : e->runs) maxc = std::max(maxc, r->g.nx * r->g.ny);
     CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagDemagOnly));
     CK(launch_kernel(gather_demag_kernel<R>, dim3((maxc + 255) / 256, nr * kMaxLayers), dim3(256), 0, e->st, false,
-                     static_cast<const RunDev<R>*>(e->d_runs), nr));
+                     static_cast<const RunDev<R>*>(e->d_runs), nr, 0, 0));
     CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField | kFlagMapped));
   } else {
     CK(launch_row_e<R>(e, kEval, false, 0, kFlagForce | kFlagStoreField));
@@ -1136,7 +1150,8 @@ void run_free(mrm_gpu* r) {
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
     dfree(b.xst); dfree(b.ucol); dfree(b.lcol); dfree(b.cax);
-    dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm);
+    dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm); dfree(b.hapm);
+    dfree(b.tab); dfree(b.tb_v); dfree(b.tb_pos);
   }
 }
 
@@ -1303,7 +1318,7 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
   hc[l].rep = repc;
   hc[l].ms_scale_cell.clear();
   dfree(b.xst);
-  dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm);
+  dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm); dfree(b.hapm);
   b.ng = n;
   if (!identity) {
     hc[l].ms_scale_cell.assign(nc, 0.0);
@@ -1315,6 +1330,7 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
     if (!rc) rc = dmalloc(errp, (void**)&b.gci, sizeof(int) * (n + 1));
     if (!rc) rc = dmalloc(errp, (void**)&b.gcs, sizeof(int) * cells.size());
     if (!rc) rc = dmalloc(errp, &b.hdm, sizeof(R) * 4 * (size_t)nc);
+    if (!rc) rc = dmalloc(errp, &b.hapm, sizeof(R) * 4 * (size_t)nc);
     if (rc) return rc;
     CK(cudaMemcpy(b.cgrain, cg.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b.gci, g2ci, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
@@ -1935,6 +1951,9 @@ int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double h
   if (!(gap > 0 && z > 0 && bit_time > 0) || nbits < 1 || nbits > 64)
     return set_err(&h->err, MRM_ERR_ARG, "head field needs gap, z, bit_time > 0 and 1 <= nbits <= 64");
   LayerBufs& b = h->L[layer];
+  dfree(b.tab);  // a layer has one field profile
+  dfree(b.tb_v);
+  dfree(b.tb_pos);
   b.func = kFuncHead;
   b.amp = 0.0;
   b.dc = 0.0;
@@ -1950,6 +1969,66 @@ int mrm_gpu_set_head_field(mrm_gpu* h, int layer, double gap, double z, double h
   b.hd_nbits = nbits;
   h->eng->desc_dirty = true;
   h->eng->tables_dirty = true;  // the row kernel's shared memory grows by the head table
+  return MRM_OK;
+}
+
+int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const double* xpos, const double* ypos,
+                            const double* vfld, double vel_x, double vel_y, double offset_x, double offset_y,
+                            double ref_x, double ref_y, double t_origin) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  std::string* errp = &h->err;
+  LayerBufs& b = h->L[layer];
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaStreamSynchronize(h->eng->st));  // a step in flight may read the old table
+  dfree(b.tab);
+  dfree(b.tb_v);
+  dfree(b.tb_pos);
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the row kernel's shared memory holds the interpolation weights
+  if (nfx == 0 && nfy == 0) return MRM_OK;
+  if (!xpos || !ypos || !vfld || nfx < 2 || nfy < 2)
+    return set_err(errp, MRM_ERR_ARG, "a field table needs at least 2 x 2 nodes (got %d x %d)", nfx, nfy);
+  for (int i = 0; i < nfx; ++i)
+    if (!std::isfinite(xpos[i]) || (i && !(xpos[i] > xpos[i - 1])))
+      return set_err(errp, MRM_ERR_ARG, "table x positions must be finite and ascending (node %d)", i);
+  for (int j = 0; j < nfy; ++j)
+    if (!std::isfinite(ypos[j]) || (j && !(ypos[j] > ypos[j - 1])))
+      return set_err(errp, MRM_ERR_ARG, "table y positions must be finite and ascending (node %d)", j);
+  const size_t nv = 3 * (size_t)nfx * nfy;
+  std::vector<double> pos(xpos, xpos + nfx);
+  pos.insert(pos.end(), ypos, ypos + nfy);
+  int rc = dmalloc(errp, &b.tb_v, sizeof(double) * nv);
+  if (!rc) rc = dmalloc(errp, &b.tb_pos, sizeof(double) * pos.size());
+  if (!rc) rc = dmalloc(errp, &b.tab, sizeof(TabDev));
+  if (rc) {
+    dfree(b.tb_v);
+    dfree(b.tb_pos);
+    return rc;
+  }
+  TabDev td{};
+  td.v = static_cast<const double*>(b.tb_v);
+  td.pos = static_cast<const double*>(b.tb_pos);
+  td.nx = nfx;
+  td.ny = nfy;
+  // file_applied's default offset: the centre of the grid (applied.f90:804-805)
+  td.ox = offset_x < -1e200 ? h->g.dx * h->g.nx * 0.5 : offset_x;
+  td.oy = offset_y < -1e200 ? h->g.dy * h->g.ny * 0.5 : offset_y;
+  td.vx = vel_x;
+  td.vy = vel_y;
+  td.rx = ref_x;
+  td.ry = ref_y;
+  td.t0 = t_origin;
+  td.dx = h->g.dx;
+  td.dy = h->g.dy;
+  CK(cudaMemcpy(b.tb_v, vfld, sizeof(double) * nv, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.tb_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.tab, &td, sizeof(TabDev), cudaMemcpyHostToDevice));
+  if (b.func == kFuncHead) {  // back to the default time scale (1)
+    b.func = 0;
+    b.scale = 1.0;
+    b.s_start = b.s_end = 1.0;
+  }
   return MRM_OK;
 }
 

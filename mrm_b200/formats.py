@@ -354,3 +354,102 @@ def read_mag_ascii(path: str, grid2grain_layers: Sequence[np.ndarray], n_grains:
                     m[g - 1] = v / np.sqrt(mg) if mg != 0.0 else v
         out.append(m)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Tabulated applied-field files (file_applied, applied.f90:711-813)
+# ---------------------------------------------------------------------------
+
+def _tecplot_size(line: str) -> Tuple[int, int]:
+    """I= and J= of a Tecplot zone line, as file_applied reads them (the digits
+    after 'I='/'i=' and 'J='/'j=')."""
+    def after(keys):
+        for k in keys:
+            p = line.find(k)
+            if p >= 0:
+                q = p + 2
+                while q < len(line) and line[q] == " ":
+                    q += 1
+                r = q
+                while r < len(line) and line[r].isdigit():
+                    r += 1
+                return int(line[q:r])
+        raise ValueError(f"no {keys[0]} in {line!r}")
+    return after(("I=", "i=")), after(("J=", "j="))
+
+
+def _is_data_line(line: str) -> bool:
+    """file_applied's test for the first data line: nothing but blanks, digits,
+    signs, points and exponent letters."""
+    s = line.strip()
+    return len(s) > 0 and all(c in " 0123456789+-.eEdD" for c in s)
+
+
+def read_field_file(path: str, nval: int = 3, scale: float = 1.0):
+    """A tabulated field (nval 3) or temperature (nval 1) profile as file_applied
+    reads it: the zone line with I= and J= gives the node counts, the data start
+    at the first purely numeric line, then one list-directed record per node,
+    x fastest.  Vector records are FEM coordinates `x y z Hx Hy Hz`, mapped to
+    the model's axes (x -> -x, z -> y, H_y <-> H_z, H_x -> -H_x) with the x nodes
+    reversed so they ascend; the values are multiplied by `scale`.  Returns
+    (xpos (nx,), ypos (ny,), values (ny, nx, 3) or (ny, nx))."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    p = 0
+    while p < len(lines) and not any(k in lines[p] for k in ("I=", "i=", "J=", "j=")):
+        p += 1
+    if p == len(lines):
+        raise ValueError("no Tecplot zone line (I=, J=)")
+    nx, ny = _tecplot_size(lines[p].strip())
+    p += 1
+    while p < len(lines) and not _is_data_line(lines[p]):
+        p += 1
+    tokens: List[str] = []
+
+    def record(k: int) -> List[float]:
+        # a list-directed read starts at a new record and continues onto the
+        # following ones until it has its k values; the rest of the last one is skipped
+        nonlocal p
+        vals: List[float] = []
+        while len(vals) < k:
+            if p >= len(lines):
+                raise ValueError("field file ends early")
+            vals += [float(t.replace("d", "e").replace("D", "e")) for t in lines[p].replace(",", " ").split()]
+            p += 1
+        return vals[:k]
+
+    xpos, ypos = np.zeros(nx), np.zeros(ny)
+    vals = np.zeros((ny, nx, 3)) if nval != 1 else np.zeros((ny, nx))
+    for j in range(ny):
+        for i in range(nx):
+            if nval == 1:
+                x, y, v = record(3)
+                xpos[i], ypos[j], vals[j, i] = x, y, v
+            else:
+                x, _, y, h1, h3, h2 = record(6)
+                ii = nx - 1 - i
+                xpos[ii], ypos[j] = x, y
+                vals[j, ii] = (h1, h2, h3)
+    if nval != 1:
+        xpos = -xpos
+        vals[..., 0] = -vals[..., 0]
+    if scale != 1.0:
+        vals = vals * scale
+    return xpos, ypos, vals
+
+
+def write_field_file(path: str, xpos: np.ndarray, ypos: np.ndarray, vfld: np.ndarray,
+                     title: str = "write field") -> None:
+    """Writes a vector profile (ny, nx, 3) on ascending nodes in the FEM
+    orientation that read_field_file (file_applied) maps back."""
+    xpos, ypos, vfld = np.asarray(xpos, float), np.asarray(ypos, float), np.asarray(vfld, float)
+    nx, ny = xpos.size, ypos.size
+    with open(path, "w") as f:
+        f.write(f'TITLE = "{title}"\n')
+        f.write('VARIABLES = "x" "y" "z" "Hx" "Hy" "Hz"\n')
+        f.write(f"ZONE I={nx}, J={ny}, F=POINT\n")
+        for j in range(ny):
+            for i in range(nx):
+                ii = nx - 1 - i  # the file's i-th node is the model's node nx-1-i, at -x
+                h = vfld[j, ii]
+                f.write(f"{-xpos[ii]:.17e} {0.0:.17e} {ypos[j]:.17e} {-h[0]:.17e} {h[2]:.17e} {h[1]:.17e}\n")

@@ -69,6 +69,8 @@ class _RunMixin:
                                        lay.scale)
             if getattr(lay, "head", None):
                 self.set_head_field(l, **lay.head)
+            if getattr(lay, "field_table", None):
+                self.set_field_table(l, **lay.field_table)
             if getattr(lay, "cubic_axis", None) is not None:
                 self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
@@ -123,6 +125,25 @@ class _RunMixin:
     def set_head_field(self, layer, gap, z, hg, velocity, x0, t0, bit_time, pattern, nbits):
         self._check(_lib.load().mrm_gpu_set_head_field(self.h, layer, gap, z, hg, velocity, x0, t0,
                                                        bit_time, int(pattern), int(nbits)))
+
+    def set_field_table(self, layer, xpos, ypos, vfld, vel=(0.0, 0.0), offset=(None, None), ref=(0.0, 0.0),
+                        t_origin=0.0):
+        """Tabulated (moving) field profile on `layer` (include/mrm_gpu.h
+        mrm_gpu_set_field_table): vfld (ny_tab, nx_tab, 3) in Oe at ascending
+        node positions xpos (nx_tab), ypos (ny_tab) in cm; offset None: the
+        grid centre; vfld None removes the profile."""
+        L = _lib.load()
+        if vfld is None:
+            self._check(L.mrm_gpu_set_field_table(self.h, layer, 0, 0, None, None, None, 0.0, 0.0, 0.0, 0.0,
+                                                  0.0, 0.0, 0.0))
+            return
+        xp, yp, v = f64(xpos), f64(ypos), f64(vfld)
+        if v.shape != (yp.size, xp.size, 3):
+            raise ValueError(f"vfld of shape {v.shape}; the nodes need {(yp.size, xp.size, 3)}")
+        off = [-1e300 if o is None else float(o) for o in offset]
+        self._check(L.mrm_gpu_set_field_table(self.h, layer, xp.size, yp.size, fptr(xp), fptr(yp), fptr(v),
+                                              float(vel[0]), float(vel[1]), off[0], off[1], float(ref[0]),
+                                              float(ref[1]), float(t_origin)))
 
     def set_cubic_axes(self, layer, cubic_axis):
         """Cubic anisotropy on `layer`: cubic_axis (N,3,3), row i = crystal axis i in

@@ -81,6 +81,10 @@ class Layer:
     # cubic anisotropy instead of uniaxial (field.f90:377-395): (N,3,3), row i
     # = crystal axis i of the grain in lab coordinates; hk holds K1, K2 as fields
     cubic_axis: Optional[np.ndarray] = None
+    # tabulated (moving) field profile replacing the uniform direction, scaled by
+    # the layer's time scale: dict(xpos, ypos, vfld (ny_tab, nx_tab, 3), vel,
+    # offset, ref, t_origin) (include/mrm_gpu.h mrm_gpu_set_field_table)
+    field_table: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -371,4 +375,54 @@ def head_write_medium(nx: int = 1024, ny: int = 256, *, seed: int = 1, prbs_seed
         depth += med.dz[l] + med.il_space[l]
         lay.head = dict(gap=gap, z=z, hg=hg, velocity=velocity_cm_s, x0=0.0, t0=0.0,
                         bit_time=bit_nm * 1e-7 / velocity_cm_s, pattern=pattern, nbits=nbits)
+    return med
+
+
+def tabulated_head_profile(gap: float, z: float, hg: float, track_width: float, *, nx_tab: int = 97,
+                           ny_tab: int = 33, x_half: Optional[float] = None, y_half: Optional[float] = None):
+    """A write-head field table (the stand-in for a FEM head-field file): the
+    Karlqvist field of a ring head of gap `gap` at distance z, deep-gap field hg,
+    times a cross-track envelope 0.5 (tanh((y + w/2)/e) - tanh((y - w/2)/e)),
+    e = gap/4, on nodes that crowd towards the gap (x) and the track centre (y).
+    Returns (xpos, ypos, vfld (ny_tab, nx_tab, 3)) in cm and Oe."""
+    xh = 8.0 * gap if x_half is None else x_half
+    yh = track_width if y_half is None else y_half
+    u = np.linspace(-1.0, 1.0, nx_tab)
+    xpos = xh * np.sinh(2.0 * u) / np.sinh(2.0)
+    ypos = yh * np.sinh(1.5 * np.linspace(-1.0, 1.0, ny_tab)) / np.sinh(1.5)
+    a, b = xpos + 0.5 * gap, xpos - 0.5 * gap
+    kx = hg / np.pi * (np.arctan(a / z) - np.arctan(b / z))
+    kz = hg / (2.0 * np.pi) * np.log((b * b + z * z) / (a * a + z * z))
+    e = 0.25 * gap
+    env = 0.5 * (np.tanh((ypos + 0.5 * track_width) / e) - np.tanh((ypos - 0.5 * track_width) / e))
+    vfld = np.zeros((ny_tab, nx_tab, 3))
+    vfld[..., 0] = env[:, None] * kx[None, :]
+    vfld[..., 2] = env[:, None] * kz[None, :]
+    return xpos, ypos, vfld
+
+
+def table_write_medium(nx: int = 1024, ny: int = 256, *, seed: int = 1, temperature: float = 300.0,
+                       gap_nm: float = 25.0, fly_nm: float = 6.0, peak_oe: float = 12000.0,
+                       velocity_cm_s: float = 2000.0, bit_nm: float = 15.0, track_nm: Optional[float] = None,
+                       rise_frac: float = 0.2, boundary: int = 1) -> Medium:
+    """The two-layer write of head_write_medium driven the way the reference
+    drives writes: a tabulated head-field profile per layer (tabulated_head_profile
+    at the layer's depth, track width 3/4 of the grid's width by default) moving
+    down-track at `velocity_cm_s` from the grid's left edge at t = 0, centred
+    cross-track, its polarity from the STE time function (square wave of
+    period two bit times, rise time rise_frac of a bit), i.e. alternating bits."""
+    med = two_layer_medium(nx, ny, seed=seed, temperature=temperature, boundary=boundary)
+    gap, fly = gap_nm * 1e-7, fly_nm * 1e-7
+    hg = karlqvist_deep_gap(peak_oe, gap, fly)
+    tw = 0.75 * ny * med.dy if track_nm is None else track_nm * 1e-7
+    tbit = bit_nm * 1e-7 / velocity_cm_s
+    depth = 0.0
+    for l, lay in enumerate(med.layers):
+        z = fly + depth + 0.5 * med.dz[l]
+        depth += med.dz[l] + med.il_space[l]
+        xpos, ypos, vfld = tabulated_head_profile(gap, z, hg, tw)
+        lay.field_table = dict(xpos=xpos, ypos=ypos, vfld=vfld, vel=(velocity_cm_s, 0.0), offset=(0.0, None),
+                               ref=(0.0, 0.0), t_origin=0.0)
+        lay.func, lay.amp, lay.fgamma, lay.param, lay.dc, lay.scale = 4, 1.0, 2.0 * tbit, rise_frac * tbit, 0.0, 1.0
+        lay.phase, lay.duty, lay.moddepth = 0.0, 0.0, 0.0
     return med

@@ -469,6 +469,12 @@ struct Layer {
   double hd_gap = 0, hd_z = 1, hd_hg = 0, hd_v = 0, hd_x0 = 0, hd_t0 = 0, hd_tbit = 1;
   uint64_t hd_bits = 0;
   int hd_nbits = 1;
+  // tabulated field profile (file_applied, applied.f90:711-813): tab_v(3, tnx, tny),
+  // node positions, origin offset / velocity / reference / time origin
+  bool tab = false;
+  int tnx = 0, tny = 0;
+  std::vector<double> tab_x, tab_y, tab_v;
+  double tox = 0, toy = 0, tvx = 0, tvy = 0, trx = 0, try_ = 0, tt0 = 0;
   MT rng;
 };
 
@@ -619,6 +625,46 @@ static double ramp_scale(const Layer& Ly, double t) {
   return ((Ly.s_end - Ly.s_start) * u + Ly.s_start) * Ly.scale;
 }
 
+// set (applied.f90:1757-1776), 0-based: for mesh cell i (centre (i+1/2) dd)
+// the lower table node ind[i] and its weight f[i]
+static void set_weights(double offset, int n, double dd, const std::vector<double>& pos, std::vector<int>& ind,
+                        std::vector<double>& f) {
+  const int npos = (int)pos.size();
+  ind.assign(n, 0);
+  f.assign(n, 0.0);
+  int i0 = 2;  // 1-based node index, as the reference sweeps it
+  for (int i = 1; i <= n; ++i) {
+    const double x = (i - .5) * dd - offset;
+    while (pos[i0 - 1] <= x && i0 < npos) ++i0;
+    ind[i - 1] = std::min(npos - 1, i0 - 1) - 1;
+    f[i - 1] = std::max(0.0, std::min(1.0, (pos[i0 - 1] - x) / (pos[i0 - 1] - pos[i0 - 2])));
+  }
+}
+
+// get_appl's moving-profile branch (applied.f90:896-903: set, then interpolate
+// :1471-1520 with the time scale s) and get_applied's average over each
+// grain's cells (field.f90:546-560): h_app per grain into ha[3 N]
+static void table_field(const Sim* s, const Layer& Ly, double t, double sc, std::vector<double>& ha) {
+  std::vector<int> ix, iy;
+  std::vector<double> fx, fy;
+  set_weights(Ly.tox + Ly.tvx * (t - Ly.tt0) - Ly.trx, s->nx, s->dx, Ly.tab_x, ix, fx);
+  set_weights(Ly.toy + Ly.tvy * (t - Ly.tt0) - Ly.try_, s->ny, s->dy, Ly.tab_y, iy, fy);
+  auto F = [&](int c, int i, int j) { return Ly.tab_v[c + 3 * ((size_t)i + (size_t)Ly.tnx * j)]; };
+  ha.assign(3 * (size_t)Ly.N, 0.0);
+  for (int n = 0; n < Ly.N; ++n) {
+    double y[3] = {0, 0, 0};
+    for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
+      const int i = Ly.g2c_i[q], j = Ly.g2c_j[q];
+      const double yf = sc * fy[j], yfc = sc * (1.0 - fy[j]);
+      for (int c = 0; c < 3; ++c)
+        y[c] += fx[i] * yf * F(c, ix[i], iy[j]) + (1.0 - fx[i]) * yf * F(c, ix[i] + 1, iy[j]) +
+                fx[i] * yfc * F(c, ix[i], iy[j] + 1) + (1.0 - fx[i]) * yfc * F(c, ix[i] + 1, iy[j] + 1);
+    }
+    const double k = (double)(Ly.g2c_idx[n + 1] - Ly.g2c_idx[n]);
+    for (int c = 0; c < 3; ++c) ha[3 * n + c] = y[c] / k;
+  }
+}
+
 // Karlqvist field of a ring head at down-track offset u from the gap centre,
 // distance z below it, deep-gap field hg (polarity included)
 static void karlqvist(double u, double g, double z, double hg, double* hx, double* hz) {
@@ -642,6 +688,8 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
   for (int l = 0; l < s->nl; ++l) {
     Layer& Ly = s->L[l];
     double sc = Ly.head ? 0.0 : ramp_scale(Ly, t);
+    std::vector<double> hat;
+    if (Ly.tab) table_field(s, Ly, t, sc, hat);
     const double* m = Ly.m[buf].data();
     const double pol = Ly.head ? head_polarity(Ly, t) : 0.0;
     const double xh = Ly.hd_x0 + Ly.hd_v * (t - Ly.hd_t0);
@@ -649,6 +697,8 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
 #pragma omp parallel for reduction(+ : el)
     for (int n = 0; n < Ly.N; ++n) {
       double ha[3] = {sc * Ly.hdir[0], sc * Ly.hdir[1], sc * Ly.hdir[2]};
+      if (Ly.tab)
+        for (int a = 0; a < 3; ++a) ha[a] = hat[3 * n + a];
       if (Ly.head) {
         // the grain's down-track position: centre of its (first) cell column
         const double x = ((double)Ly.g2c_i[Ly.g2c_idx[n]] + 0.5) * s->dx;
@@ -1254,8 +1304,32 @@ int orc_set_head_field(void* h, int l, double gap, double z, double hg, double v
   if (l < 0 || l >= s->nl || !(gap > 0 && z > 0 && tbit > 0) || nbits < 1 || nbits > 64) return 1;
   Layer& Ly = s->L[l];
   Ly.head = true;
+  Ly.tab = false;
   Ly.hd_gap = gap; Ly.hd_z = z; Ly.hd_hg = hg; Ly.hd_v = v; Ly.hd_x0 = x0; Ly.hd_t0 = t0;
   Ly.hd_tbit = tbit; Ly.hd_bits = bits; Ly.hd_nbits = nbits;
+  return 0;
+}
+
+// tabulated field profile (mrm_gpu_set_field_table's arguments; nfx = nfy = 0 removes it)
+int orc_set_field_table(void* h, int l, int nfx, int nfy, const double* xpos, const double* ypos,
+                        const double* vfld, double vx, double vy, double ox, double oy, double rx, double ry,
+                        double t0) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.tab = false;
+  if (nfx == 0 && nfy == 0) return 0;
+  if (nfx < 2 || nfy < 2) return 1;
+  Ly.head = false;
+  Ly.tnx = nfx;
+  Ly.tny = nfy;
+  Ly.tab_x.assign(xpos, xpos + nfx);
+  Ly.tab_y.assign(ypos, ypos + nfy);
+  Ly.tab_v.assign(vfld, vfld + 3 * (size_t)nfx * nfy);
+  Ly.tox = ox < -1e200 ? s->dx * s->nx * 0.5 : ox;  // applied.f90:804-805
+  Ly.toy = oy < -1e200 ? s->dy * s->ny * 0.5 : oy;
+  Ly.tvx = vx; Ly.tvy = vy; Ly.trx = rx; Ly.try_ = ry; Ly.tt0 = t0;
+  Ly.tab = true;
   return 0;
 }
 
@@ -1300,6 +1374,14 @@ int orc_get_demag(void* h, int l, double* out) {
   Sim* s = static_cast<Sim*>(h);
   if (l < 0 || l >= s->nl) return 1;
   std::memcpy(out, s->L[l].hdemag.data(), sizeof(double) * 3 * s->L[l].N);
+  return 0;
+}
+
+// applied field per grain of the last field evaluation (field(k)%h_app)
+int orc_get_applied(void* h, int l, double* out) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  std::memcpy(out, s->L[l].happ.data(), sizeof(double) * 3 * s->L[l].N);
   return 0;
 }
 

@@ -55,10 +55,12 @@ def lib():
         L.orc_set_field_function.argtypes = [vp, i, P(d), i, d, d, d, d, d, d, d, d]
         L.orc_set_head_field.argtypes = [vp, i, d, d, d, d, d, d, d, u64, i]
         L.orc_set_cubic_axes.argtypes = [vp, i, P(d)]
+        L.orc_set_field_table.argtypes = [vp, i, i, i, P(d), P(d), P(d), d, d, d, d, d, d, d]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
         L.orc_get_field.argtypes = [vp, i, P(d)]
         L.orc_get_demag.argtypes = [vp, i, P(d)]
+        L.orc_get_applied.argtypes = [vp, i, P(d)]
         L.orc_set_time.argtypes = [vp, d, C.c_longlong]
         L.orc_eval_field.argtypes = [vp, d]
         L.orc_step.argtypes = [vp, i, d, i, vp, vp]
@@ -216,6 +218,9 @@ class OracleSim:
                 rc = L.orc_set_head_field(self.h, l, hd["gap"], hd["z"], hd["hg"], hd["velocity"], hd["x0"],
                                           hd["t0"], hd["bit_time"], int(hd["pattern"]), int(hd["nbits"]))
                 assert rc == 0
+            tb = getattr(lay, "field_table", None)
+            if tb:
+                self.set_field_table(l, **tb)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
             cub = getattr(lay, "cubic_axis", None)
             if cub is not None:
@@ -274,11 +279,31 @@ class OracleSim:
         lib().orc_get_demag(self.h, layer, _p(out))
         return out
 
+    def get_applied(self, layer: int) -> np.ndarray:
+        """Applied field per grain of the last field evaluation."""
+        n = self.medium.layers[layer].N
+        out = np.zeros((n, 3))
+        lib().orc_get_applied(self.h, layer, _p(out))
+        return out
+
     def set_time(self, t: float, step: int = 0):
         lib().orc_set_time(self.h, t, step)
 
     def eval_field(self, t: float):
         lib().orc_eval_field(self.h, t)
+
+    def set_field_table(self, layer, xpos, ypos, vfld, vel=(0.0, 0.0), offset=(None, None), ref=(0.0, 0.0),
+                        t_origin=0.0):
+        """Tabulated field profile (GpuSim.set_field_table's arguments; vfld None removes it)."""
+        if vfld is None:
+            assert lib().orc_set_field_table(self.h, layer, 0, 0, None, None, None, 0, 0, 0, 0, 0, 0, 0) == 0
+            return
+        xp, yp, v = f64(xpos), f64(ypos), f64(vfld)
+        assert v.shape == (yp.size, xp.size, 3)
+        off = [-1e300 if o is None else float(o) for o in offset]
+        assert lib().orc_set_field_table(self.h, layer, xp.size, yp.size, _p(xp), _p(yp), _p(v), float(vel[0]),
+                                         float(vel[1]), off[0], off[1], float(ref[0]), float(ref[1]),
+                                         float(t_origin)) == 0
 
     def off_field(self, zoff: float, dzobs: float, head_mu: float = 1.0, fly_height: float = 8e-7,
                   sul_mu: float = 1.0, space_to_sul: float = 40e-7, num_images: int = 2) -> np.ndarray:
