@@ -410,7 +410,38 @@ def write_leg(torch, local, steps=2000):
             "us_per_heun_step": 1e3 * ms / steps, "mave_top": np.asarray(st["mave_l"][0]).tolist(),
             "readback": {"call": "off_field " + READBACK_TEXT, "grid": [1024, 256], "ms_per_call": off_ms,
                          "hz_rms_oe": float(np.sqrt(np.mean(hr[2] ** 2)))},
-            "tabulated": table_write_leg(torch, local, steps)}
+            "tabulated": table_write_leg(torch, local, steps),
+            "windowed": window_write_leg(torch, local, steps)}
+
+
+def window_write_leg(torch, local, steps):
+    """A longer track (2048 x 256 grains x 2 layers) written by the tabulated
+    head with a moving demag window of 512 x 256 cells centred on it (nxfft <
+    nx): only the window's grains are evaluated and pushed, the FFT covers the
+    window.  Value: grain-steps/s of the pushed (windowed) grains."""
+    from mrm_b200 import FP32, GpuSim, media
+    med = media.table_write_medium(2048, 256, seed=1, temperature=300.0)
+    med.window = dict(nx=512, ny=256, v=(2000.0, 0.0), offset=(-0.5 * 2048 * med.dx, 0.0))
+    sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.set_time(4e-8, 0)  # the head 800 nm (1,143 cells) down the track, the window centred on it
+    sim.step(48, DT, stats=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.enqueue(steps, DT)
+    e1.record(ext)
+    sim.stats()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    px, py = sim.fft_grid()
+    win = sim.get_window()
+    sim.close()
+    active = 2 * 512 * 256
+    return {"workload": f"two-layer 2048x256x2 track, tabulated head at 20 m/s, 512x256 demag window following "
+                        f"it ({px}x{py} FFT), T=300 K, FP32, {steps} Heun steps",
+            "value": active * steps / (ms * 1e-3), "unit": UNIT, "us_per_heun_step": 1e3 * ms / steps,
+            "window_origin": list(win[2:])}
 
 
 def table_write_leg(torch, local, steps):

@@ -189,6 +189,25 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
                             const double* vfld, double vel_x, double vel_y, double offset_x, double offset_y,
                             double ref_x, double ref_y, double t_origin);
 
+/* Moving demag window (nxfft/nyfft < nx/ny; window_m and update_do_grain,
+ * data.f90:1-65,120-157, get_mag / get_magnetostatic :322-390,
+ * field.f90:438-517): the demag FFT covers nx_win x ny_win cells whose origin
+ * follows off = v t + offset (window%v, window%offset: the CLI's field
+ * VELOCITY and -REF) as
+ *   i0 = clamp(nint((nx - nx_win)/2 + off_x/dx), 1, nx - nx_win + 1) - 1  (j0 alike),
+ * placed before the first step and after every step.  Grains inside the
+ * window (do_grain) are evaluated and pushed; the others keep their state and
+ * their last field; the stats reduce every grain (a frozen grain with its last
+ * field) and mmag over the grains from the window's first to its last index,
+ * normalised by the pushed grains' volume, as llg() does.  The window's FFT
+ * grid follows the boundary rule of mrm_geom on nx_win x ny_win; the tensor
+ * must be built or uploaded again for it.  nx_win = nx and ny_win = ny: no
+ * window.  One grain per cell, a handle of its own (not in a batch), fixed dt.
+ * mrm_gpu_get_window: out4 = {nx_win, ny_win, i0, j0}, the origin at the
+ * handle's current time (where the next step evaluates). */
+int mrm_gpu_set_window(mrm_gpu* h, int nx_win, int ny_win, double vx, double vy, double offset_x, double offset_y);
+int mrm_gpu_get_window(const mrm_gpu* h, int* out4);
+
 /* Cubic magnetocrystalline anisotropy on `layer` (get_cubic_hk,
  * field.f90:377-395; set up by construct_hk_direction with k_cubic,
  * construct_grain.f90:1620-1625, which then drops the uniaxial axis):

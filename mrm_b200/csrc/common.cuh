@@ -129,6 +129,10 @@ struct RunDev {
   int lgct;                // log2 of the column-tile width T (= columns per column task)
   Cx<R>* specx;            // M^ half spectra in column tiles [nl*3][ntile][nys][T], ntile = ceil((px/2+1)/T)
                            // (row kernel -> column kernel)
+  // moving demag window (gnx = 0: none): the FFT grid covers the nx x ny cells
+  // from grid column wi0, row wj0 of the full gnx x gny grid of the per-grain
+  // arrays; frz: the run's first stats record of the frozen grains (-1: none)
+  int gnx, gny, wi0, wj0, frz;
   const R* tens;           // tensor spectrum: FP32 packed [px/2+1][nl*nl][9][pyhs] reals,
                            // FP64 full [px/2+1][nl*nl][9][py] complex
   LayerDev<R> L[kMaxLayers];

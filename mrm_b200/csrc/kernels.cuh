@@ -191,7 +191,7 @@ MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
 
 // stats record slots (sums except the two maxima)
 constexpr int kSlotV = 0, kSlotM = 1, kSlotM2 = 4, kSlotH = 7, kSlotWM = 10, kSlotW = 13,
-              kSlotNup = 14, kSlotMaxTq = 15, kSlotMaxD2 = 16, kSlotMmag = 17, kSlotE = 18;
+              kSlotNup = 14, kSlotMaxTq = 15, kSlotMaxD2 = 16, kSlotMmag = 17, kSlotE = 18, kSlotVA = 19;
 MRM_HD constexpr bool slot_is_max(int s) { return s == kSlotMaxTq || s == kSlotMaxD2; }
 
 MRM_D void block_reduce_record(double* rec, double* sred /* [32][kNPart] */, double* out) {
@@ -307,6 +307,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 
   const int l = tk.y, row0 = tk.z, nrows = tk.w;
   const int nx = rd.nx, ny = rd.ny;
+  // moving demag window (general kernels, one row per task): the task's row is
+  // grid row wj0 + row0, its cells grid columns wi0 .. wi0 + nx - 1 of the full
+  // gnx x gny grid that the per-grain arrays cover
+  const bool win = GEN && rd.gnx > 0;
+  if (win && nrows != 1) {
+    if (threadIdx.x == 0) atomicOr(err, kErrShape);
+    return;
+  }
+  const int gnx = win ? rd.gnx : nx, gny = win ? rd.gny : ny, wi0 = win ? rd.wi0 : 0, wj0 = win ? rd.wj0 : 0;
   const int lgpx = rd.lgpx, lgM = lgpx - 1, M = 1 << lgM, ph = M + 1;
   const int cs = seq_stride(M);  // complex stride of one sequence in shared memory
   const int nseq = nrows * 3;
@@ -349,9 +358,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const RowStage sp = row_stage_plan<R>(STAGE, nx, nrows, stencil, ucol, lcol, thermal);
   // staged when the plan fits both the launch's staging capacity and the
   // shared memory actually allocated behind the FFT buffers
-  const bool staged = sp.bytes <= stage_cap &&
+  const bool staged = !win && sp.bytes <= stage_cap &&
                       (long long)(stg - smem_raw) + sp.bytes <= (long long)dynamic_smem_bytes();
-  const int base = row0 * nx;
+  const int base = win ? (wj0 + row0) * gnx + wi0 : row0 * nx;
   const int v4row = nx * (int)sizeof(V4<R>);
   const int rrow = nx * (int)sizeof(R);
   const bool mapped = (STAGE != kInit) && (flags & kFlagMapped);
@@ -374,7 +383,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 #endif
     bulk_copy(bar, dst, src, (uint32_t)bytes);
   };
-  const long long nlay = (long long)nx * ny;  // grains per layer
+  const long long nlay = (long long)gnx * gny;  // grains per layer
   const long long v4b = (long long)sizeof(V4<R>), rb = (long long)sizeof(R), cb = (long long)sizeof(Cx<R>);
   MRM_CHECK(l >= 0 && l < rd.nl && row0 >= 0 && nrows >= 1 && row0 + nrows <= ny, 900, row0);
 
@@ -484,6 +493,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // field row rr in [-1, nrows] (lattice neighbours wrap periodically)
   auto mf_row = [&](int rr) -> const V4<R>* {
     if (staged) return MF + rr * nx;
+    if (win) {
+      int j = wj0 + row0 + rr;
+      j = j < 0 ? j + gny : (j >= gny ? j - gny : j);
+      return mfield + (size_t)j * gnx;
+    }
     int j = row0 + rr;
     j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
     return mfield + (size_t)j * nx;
@@ -514,8 +528,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const double ox = T.ox + T.vx * (t_stage - T.t0) - T.rx;
     const double oy = T.oy + T.vy * (t_stage - T.t0) - T.ry;
     for (int c = threadIdx.x; c < nx + nrows; c += BLOCK)
-      tw[c] = c < nx ? tab_weight(T.pos, T.nx, ((double)c + 0.5) * T.dx - ox)
-                     : tab_weight(T.pos + T.nx, T.ny, ((double)(row0 + c - nx) + 0.5) * T.dy - oy);
+      tw[c] = c < nx ? tab_weight(T.pos, T.nx, ((double)(wi0 + c) + 0.5) * T.dx - ox)
+                     : tab_weight(T.pos + T.nx, T.ny, ((double)(wj0 + row0 + c - nx) + 0.5) * T.dy - oy);
     __syncthreads();
   } else if (STAGE != kInit && htab_off) {
     double xh, pol;
@@ -523,7 +537,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     R* hw = reinterpret_cast<R*>(Z);
     for (int c = threadIdx.x; c < nx; c += BLOCK) {
       R khx, khz;
-      karlqvist<R>((R)(((double)c + 0.5) * L.hd_dx - xh), (R)L.hd_gap, (R)L.hd_z, (R)(pol * L.hd_hg), khx, khz);
+      karlqvist<R>((R)(((double)(wi0 + c) + 0.5) * L.hd_dx - xh), (R)L.hd_gap, (R)L.hd_z, (R)(pol * L.hd_hg), khx,
+                   khz);
       if (STAGE == kEval) {
         reinterpret_cast<Cx<R>*>(smem_raw + htab_off)[c] = Cx<R>{khx, khz};
       } else {
@@ -638,8 +653,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     if (stencil) {
       const V4<R> c = XS[q];
       const V4<R>* rowc = mf_row(rr);
-      const int im = (i == 0 ? nx - 1 : i - 1), ip = (i == nx - 1 ? 0 : i + 1);
-      const V4<R> n0 = mf_row(rr - 1)[i], n1 = rowc[im], n2 = rowc[ip], n3 = mf_row(rr + 1)[i];
+      // (in a window the neighbours are the full grid's: row pointers at the
+      // full rows' starts, the grid column wi0 + i)
+      const int ci = wi0 + i;
+      const int im = (ci == 0 ? gnx - 1 : ci - 1), ip = (ci == gnx - 1 ? 0 : ci + 1);
+      const V4<R> n0 = mf_row(rr - 1)[ci], n1 = rowc[im], n2 = rowc[ip], n3 = mf_row(rr + 1)[ci];
       ex = c.x * n0.x + c.y * n1.x + c.z * n2.x + c.w * n3.x;
       ey = c.x * n0.y + c.y * n1.y + c.z * n2.y + c.w * n3.y;
       ez = c.x * n0.z + c.y * n1.z + c.z * n2.z + c.w * n3.z;
@@ -793,6 +811,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / (pv.z * pv.z));
       rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
       rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+      rec[kSlotVA] += v;  // volume of the grains pushed (do_grain)
       // energy at the evaluated state (field.f90:200, :360, :374, :339)
       const double e_d = -((double)mf.x * ((double)hdx + apx) + (double)mf.y * ((double)hdy + apy) +
                            (double)mf.z * ((double)hdz + apz)) * (double)mse;
@@ -1162,6 +1181,65 @@ __global__ void gather_demag_kernel(const RunDev<R>* __restrict__ runs, int nrun
   }
 }
 
+// Moving demag window (update_do_grain, data.f90:120-157): the copy of the
+// current state into the other buffer (:139), m -> mp for every grain of
+// run `slot`, so that grains outside the window read as their frozen state.
+template <typename R>
+__global__ void window_copy_kernel(const RunDev<R>* __restrict__ runs, int slot) {
+  const RunDev<R>& rd = runs[slot];
+  const int l = blockIdx.y;
+  if (l >= rd.nl) return;
+  const LayerDev<R>& L = rd.L[l];
+  const long long n = (long long)rd.gnx * rd.gny;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    L.mp[c] = L.m[c];
+}
+
+// Stats records of the grains outside the window (frozen, do_grain false), one
+// block per layer: volume, moments, the stale field of their last evaluation
+// (llg.f90:215-233 reduces every grain), and |m| ms_scale vol of those whose
+// index lies within the window's first and last grain (push_llg sums mmag1
+// over min_n..max_n, llg.f90:1081,1152); into part[rd.frz + layer].
+template <typename R>
+__global__ void __launch_bounds__(256) frozen_stats_kernel(const RunDev<R>* __restrict__ runs, int slot,
+                                                           double* __restrict__ part) {
+  __shared__ double sred[32 * kNPart];
+  const RunDev<R>& rd = runs[slot];
+  const int l = blockIdx.x;
+  if (l >= rd.nl || rd.frz < 0) return;
+  const LayerDev<R>& L = rd.L[l];
+  double rec[kNPart];
+#pragma unroll
+  for (int s = 0; s < kNPart; ++s) rec[s] = 0.0;
+  const int gnx = rd.gnx, gny = rd.gny, i0 = rd.wi0, j0 = rd.wj0;
+  const long long nmin = (long long)j0 * gnx + i0, nmax = (long long)(j0 + rd.ny - 1) * gnx + i0 + rd.nx - 1;
+  for (long long c = threadIdx.x; c < (long long)gnx * gny; c += blockDim.x) {
+    const int j = (int)(c / gnx), i = (int)(c - (long long)j * gnx);
+    if (j >= j0 && j < j0 + rd.ny && i >= i0 && i < i0 + rd.nx) continue;
+    const V4<double> pv = L.pv[c];
+    const V4<R> mr = L.m[c], hr = L.hf[c];
+    const double v = pv.x, w = pv.z * pv.y * v;
+    const double mx = mr.x, my = mr.y, mz = mr.z;
+    rec[kSlotV] += v;
+    rec[kSlotM + 0] += v * mx;
+    rec[kSlotM + 1] += v * my;
+    rec[kSlotM + 2] += v * mz;
+    rec[kSlotM2 + 0] += v * mx * mx;
+    rec[kSlotM2 + 1] += v * my * my;
+    rec[kSlotM2 + 2] += v * mz * mz;
+    rec[kSlotH + 0] += v * (double)hr.x;
+    rec[kSlotH + 1] += v * (double)hr.y;
+    rec[kSlotH + 2] += v * (double)hr.z;
+    rec[kSlotWM + 0] += w * mx;
+    rec[kSlotWM + 1] += w * my;
+    rec[kSlotWM + 2] += w * mz;
+    rec[kSlotW] += w;
+    if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += pv.w;
+    if (c >= nmin && c <= nmax) rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+  }
+  block_reduce_record(rec, sred, part + (size_t)(rd.frz + l) * kNPart);
+}
+
 // llg_type 2: the predictor buffer holds m_{n+1} after the single push; copy
 // it to the state (one row task per block).
 template <typename R>
@@ -1175,7 +1253,8 @@ __global__ void __launch_bounds__(256) commit_kernel(const RunDev<R>* __restrict
   const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
   if (!(flags & kFlagForce) && step >= rd.step_end) return;
   const LayerDev<R>& L = rd.L[tk.y];
-  const int n0 = tk.z * rd.nx, cnt = tk.w * rd.nx;
+  // (a windowed run's task row is grid row wj0 + row from column wi0)
+  const int n0 = rd.gnx ? (rd.wj0 + tk.z) * rd.gnx + rd.wi0 : tk.z * rd.nx, cnt = tk.w * rd.nx;
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) L.m[n0 + i] = L.mp[n0 + i];
 }
 
@@ -1235,6 +1314,12 @@ __global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
+  if (rd.frz >= 0)  // the frozen grains outside a moving demag window
+    for (int l = 0; l < rd.nl; ++l)
+      for (int s = 0; s < kNPart; ++s) {
+        const double f = part[(size_t)(rd.frz + l) * kNPart + s];
+        acc[l][s] = slot_is_max(s) ? fmax(acc[l][s], f) : acc[l][s] + f;
+      }
   StatsDev& st = out[r];
   st.step = rd.step;
   st.t = rd.t_base + (double)(rd.step - rd.step_base) * rd.dt;
@@ -1262,7 +1347,7 @@ __global__ void __launch_bounds__(256) finalize_stats_kernel(const RunDev<R>* __
         st.mvar[a] += V * st.mvar_l[l][a] / vt;
         st.have[a] += V * st.have_l[l][a] / vt;
       }
-      mmag += acc[l][kSlotMmag] / V;
+      mmag += acc[l][kSlotMmag] / acc[l][kSlotVA];  // over the pushed grains' volume (llg.f90:1239)
       mt = fmax(mt, acc[l][kSlotMaxTq]);
       m1 = fmax(m1, acc[l][kSlotMaxD2]);
       en += acc[l][kSlotE];

@@ -100,6 +100,15 @@ struct mrm_gpu {
   int slot = -1;
   int lgct = 0;  // log2 of the column-tile width (= columns per column task)
   int row_task0 = 0, nrow_tasks = 0;
+  // moving demag window (wnx = 0: none; window_m, data.f90:1-65): its size, its
+  // velocity and offset (window%v, window%offset), its current origin (-1: not
+  // placed yet); frz: the run's first frozen-grain stats record
+  int wnx = 0, wny = 0, wi0 = -1, wj0 = -1, frz = -1;
+  double wvx = 0, wvy = 0, wox = 0, woy = 0;
+  // the time as llg() accumulates it (t = t + dt, llg.f90:268), which places
+  // the window: t_base + k dt can differ from it in the last bit, and a window
+  // edge at an exact half cell would then move a step early or late
+  double t_acc = 0.0;
   std::string err;
 };
 
@@ -129,6 +138,7 @@ struct Engine {
   size_t smem_stats[2] = {0, 0};  // reductions launch of kPred (single-stage integrator), kCorr
   int cap_stats[2] = {0, 0};
   int* d_err = nullptr;              // device error flag (tma.cuh DeviceError bits)
+  bool has_window = false;           // a run with a moving demag window (general kernels)
   bool has_head = false;             // a run has a layer under the write head or a tabulated
                                      // field profile (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
@@ -291,12 +301,16 @@ int col_tile(int want) {
   return t;
 }
 int cols_per_task(const Engine* e, const mrm_gpu* r) { return col_tile(e->cpt > 0 ? e->cpt : default_cols(r)); }
+// cells per row and rows of the FFT source (the moving demag window, else the grid)
+int fnx(const mrm_gpu* r) { return r->wnx ? r->wnx : r->g.nx; }
+int fny(const mrm_gpu* r) { return r->wnx ? r->wny : r->g.ny; }
 // complex values of the M^ spectrum of a run (column tiles of any width up to kMaxColTile)
 size_t specx_count(const mrm_gpu* r) {
   const int ph = r->px / 2 + 1;
-  return (size_t)r->nl * 3 * ((ph + kMaxColTile - 1) / kMaxColTile * kMaxColTile) * spec_col_stride(r->g.ny);
+  return (size_t)r->nl * 3 * ((ph + kMaxColTile - 1) / kMaxColTile * kMaxColTile) * spec_col_stride(fny(r));
 }
-int rows_per_task(const mrm_gpu* r, int rpb) { return std::max(1, std::min(rpb, r->g.ny)); }
+// (a windowed run's rows are segments of the grid's rows: one per task)
+int rows_per_task(const mrm_gpu* r, int rpb) { return r->wnx ? 1 : std::max(1, std::min(rpb, r->g.ny)); }
 
 size_t tensor_bytes(const mrm_gpu* r) {
   const size_t ph = r->px / 2 + 1, npair = (size_t)r->nl * r->nl;
@@ -321,7 +335,7 @@ int run_stage_bytes(const mrm_gpu* r, int stage, int rows) {
   for (int l = 0; l < r->nl; ++l) {
     const LayerBufs& b = r->L[l];
     const bool ucol = b.ucol && l > 0, lcol = b.lcol && l + 1 < r->nl;
-    const RowStage p = row_stage_plan<R>(stage, r->g.nx, rows, b.xst != nullptr, ucol, lcol, b.thermal != 0);
+    const RowStage p = row_stage_plan<R>(stage, fnx(r), rows, b.xst != nullptr, ucol, lcol, b.thermal != 0);
     need = std::max(need, p.bytes);
   }
   return need;
@@ -334,8 +348,8 @@ template <typename R>
 size_t row_fixed_smem(const mrm_gpu* r, int rpb) {
   size_t b = (size_t)row_fft_smem<R>(r->lgpx, rpb), t = 0;
   for (int l = 0; l < r->nl; ++l) {
-    if (r->L[l].tab) t = std::max(t, (size_t)field_table_bytes(r->g.nx));
-    else if (r->L[l].func == kFuncHead) t = std::max(t, (size_t)head_table_bytes<R>(r->g.nx));
+    if (r->L[l].tab) t = std::max(t, (size_t)field_table_bytes(fnx(r)));
+    else if (r->L[l].func == kFuncHead) t = std::max(t, (size_t)head_table_bytes<R>(fnx(r)));
   }
   return b + t;
 }
@@ -397,8 +411,13 @@ template <typename R>
 RunDev<R> make_desc(const mrm_gpu* r) {
   RunDev<R> d;
   std::memset(&d, 0, sizeof(d));
-  d.nx = r->g.nx;
-  d.ny = r->g.ny;
+  d.nx = fnx(r);
+  d.ny = fny(r);
+  d.gnx = r->wnx ? r->g.nx : 0;
+  d.gny = r->wnx ? r->g.ny : 0;
+  d.wi0 = std::max(0, r->wi0);
+  d.wj0 = std::max(0, r->wj0);
+  d.frz = r->wnx ? r->frz : -1;
   d.nl = r->nl;
   d.px = r->px;
   d.py = r->py;
@@ -416,7 +435,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
   d.row_task0 = r->row_task0;
   d.nrow_tasks = r->nrow_tasks;
   d.phs = spec_row_stride(r->px);
-  d.nys = spec_col_stride(r->g.ny);
+  d.nys = spec_col_stride(fny(r));
   d.lgct = r->lgct;
   d.pyhs = tens_row_stride(r->py);
   d.tw_row = row_tw_off(r->lgpx);
@@ -584,12 +603,13 @@ int build_tables(Engine* e) {
     mrm_gpu* r = e->runs[i];
     r->slot = (int)i;
     const int rpt = rows_per_task(r, rv.rpb);
+    const int ny = fny(r);
     for (int l = 0; l < r->nl; ++l)
-      for (int j = 0; j < r->g.ny; j += rpt) rt.push_back(make_int4((int)i, l, j, std::min(rpt, r->g.ny - j)));
+      for (int j = 0; j < ny; j += rpt) rt.push_back(make_int4((int)i, l, j, std::min(rpt, ny - j)));
     // one-row tasks of the reductions launch; the run's partial records
     r->row_task0 = (int)stt.size();
     for (int l = 0; l < r->nl; ++l)
-      for (int j = 0; j < r->g.ny; ++j) stt.push_back(make_int4((int)i, l, j, 1));
+      for (int j = 0; j < ny; ++j) stt.push_back(make_int4((int)i, l, j, 1));
     r->nrow_tasks = (int)stt.size() - r->row_task0;
     if (r->demag && r->tensor_ready) {
       const int cpt = cols_per_task(e, r), ph = r->px / 2 + 1;
@@ -612,6 +632,11 @@ int build_tables(Engine* e) {
     }
   if (e->mapped && karlqvist_head)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the write head needs one grain per cell (no grain maps in the batch)");
+  e->has_window = false;
+  for (auto* r : e->runs) e->has_window = e->has_window || r->wnx > 0;
+  if (e->has_window && (e->runs.size() > 1 || e->mapped))
+    return set_err(errp, MRM_ERR_UNSUPPORTED,
+                   "a moving demag window runs on a handle of its own with one grain per cell");
   e->nst = (int)stt.size();
   if (e->nst > e->st_cap) {
     dfree(e->d_stasks);
@@ -631,13 +656,16 @@ int build_tables(Engine* e) {
     int rc = dmalloc(errp, (void**)&e->d_ctasks, sizeof(Task) * e->ct_cap);
     if (rc) return rc;
   }
-  if (e->nst > e->part_cap) {
+  // the row tasks' records, then kMaxLayers frozen-grain records per run
+  const int nr = (int)e->runs.size();
+  const int npart = e->nst + nr * kMaxLayers;
+  for (int i = 0; i < nr; ++i) e->runs[i]->frz = e->nst + i * kMaxLayers;
+  if (npart > e->part_cap) {
     dfree(e->d_part);
-    e->part_cap = std::max(e->nst, 2 * e->part_cap);
+    e->part_cap = std::max(npart, 2 * e->part_cap);
     int rc = dmalloc(errp, (void**)&e->d_part, sizeof(double) * kNPart * e->part_cap);
     if (rc) return rc;
   }
-  const int nr = (int)e->runs.size();
   if (nr > e->stats_cap) {
     dfree(e->d_stats);
     if (e->h_stats) cudaFreeHost(e->h_stats);
@@ -664,7 +692,7 @@ template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
   // the general kernels for the semi-implicit pushes and write heads
-  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic;
+  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic || e->has_window;
   if (stats) {
     const int i = stage == kPred ? 0 : 1;
     RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
@@ -751,7 +779,7 @@ template <typename R>
 void default_shapes(Engine* e) {
   int maxnx = 1, maxlg = 1;
   for (auto* r : e->runs) {
-    maxnx = std::max(maxnx, r->g.nx);
+    maxnx = std::max(maxnx, fnx(r));
     maxlg = std::max(maxlg, r->lgpx);
   }
   // rows per block so that a block holds about 256 grains
@@ -1087,9 +1115,9 @@ __global__ void mgrid_kernel(const RunDev<R>* __restrict__ runs, int slot, doubl
   const RunDev<R>& rd = runs[slot];
   const int l = blockIdx.y;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = rd.nx * rd.ny;
-  if (c >= n) return;
   const LayerDev<R>& L = rd.L[l];
+  const int n = L.n;  // cells of the grid
+  if (c >= n) return;
   const V4<R> m = L.m[c];
   const double f = (double)L.pb[c].x;  // 0 on empty cells
   out[((size_t)l * 3 + 0) * n + c] = f * (double)m.x;
@@ -1111,12 +1139,19 @@ __global__ void off_mac_kernel(const Cx<double>* __restrict__ T, const Cx<double
 }
 
 // ---------------- run buffers ----------------
+// spectra and tensor of the run's FFT grid
+int spectra_alloc(mrm_gpu* r) {
+  std::string* errp = &r->err;
+  const size_t re = relem(r->g.precision);
+  int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * fny(r) * spec_row_stride(r->px) * 2 * re);
+  if (!rc) rc = dmalloc(errp, &r->specx, specx_count(r) * 2 * re);
+  return rc;
+}
+
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
-  int rc = dmalloc(errp, &r->spech, (size_t)r->nl * 3 * r->g.ny * spec_row_stride(r->px) * 2 * re);
-  if (rc) return rc;
-  rc = dmalloc(errp, &r->specx, specx_count(r) * 2 * re);
+  int rc = spectra_alloc(r);
   if (rc) return rc;
   rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
   if (rc) return rc;
@@ -2126,6 +2161,7 @@ int mrm_gpu_set_time(mrm_gpu* h, double t, int64_t step) {
   h->t_base = t;
   h->step_base = step;
   h->step = step;
+  h->t_acc = t;
   h->eng->desc_dirty = true;
   return MRM_OK;
 }
@@ -2137,6 +2173,9 @@ int mrm_gpu_get_time(const mrm_gpu* h, double* t, int64_t* step) {
   return MRM_OK;
 }
 
+static void window_origin(const mrm_gpu* h, double t, int* i0, int* j0);
+static int place_window(mrm_gpu* h, int i0, int j0);
+
 int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag) {
   if (!h) return MRM_ERR_ARG;
   std::string* errp = &h->err;
@@ -2145,6 +2184,12 @@ int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag) {
     if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
   if (h->demag && !h->tensor_ready) return set_err(errp, MRM_ERR_STATE, "build or upload the tensor first (or disable demag)");
   Engine* e = h->eng;
+  if (h->wnx) {  // the window where update_do_grain puts it at t
+    int i0, j0;
+    window_origin(h, t, &i0, &j0);
+    int rc = place_window(h, i0, j0);
+    if (rc) return rc;
+  }
   // evaluate this run alone at time t: move its time origin and park the others
   const double tb = h->t_base;
   const long long sb = h->step_base;
@@ -2169,6 +2214,52 @@ int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag) {
     return get_v4(h, layer, h->L[layer].hd, hdemag);
   }
   CK(cudaStreamSynchronize(e->st));
+  return MRM_OK;
+}
+
+// update_do_grain (data.f90:120-135) with get_window (:52-64): the window
+// origin (0-based cell offsets) at time t
+static void window_origin(const mrm_gpu* h, double t, int* i0, int* j0) {
+  // off = v t + offset rounded as two operations (no fused multiply-add), so
+  // that a half-cell tie in nint falls the same way on every build
+  volatile double vtx = h->wvx * t, vty = h->wvy * t;
+  const double offx = vtx + h->wox, offy = vty + h->woy;
+  const int nx = h->g.nx, ny = h->g.ny;
+  *i0 = std::max(1, std::min(nx - h->wnx + 1, (int)std::lround((nx - h->wnx) * 0.5 + offx / h->g.dx))) - 1;
+  *j0 = std::max(1, std::min(ny - h->wny + 1, (int)std::lround((ny - h->wny) * 0.5 + offy / h->g.dy))) - 1;
+}
+
+// Moves the window to (i0, j0): the grains now inside are the do_grain ones;
+// every grain's other buffer takes its current state (data.f90:139), the
+// spectrum is re-formed over the new window, and the frozen grains' stats
+// records are taken (they stay fixed until the window moves again).
+static int place_window(mrm_gpu* h, int i0, int j0) {
+  std::string* errp = &h->err;
+  Engine* e = h->eng;
+  if (i0 == h->wi0 && j0 == h->wj0 && h->spec_valid) return MRM_OK;
+  h->wi0 = i0;
+  h->wj0 = j0;
+  h->spec_valid = false;
+  e->desc_dirty = true;
+  int rc = e->prec == MRM_FP64 ? ensure_ready<double>(e) : ensure_ready<float>(e);
+  if (rc) {
+    h->err = e->err;
+    return rc;
+  }
+  const long long n = (long long)h->g.nx * h->g.ny;
+  const unsigned gx = (unsigned)std::min<long long>((n + 255) / 256, 4096);
+  if (e->prec == MRM_FP64) {
+    window_copy_kernel<double><<<dim3(gx, h->nl), 256, 0, e->st>>>(static_cast<const RunDev<double>*>(e->d_runs),
+                                                                   h->slot);
+    frozen_stats_kernel<double><<<h->nl, 256, 0, e->st>>>(static_cast<const RunDev<double>*>(e->d_runs), h->slot,
+                                                          e->d_part);
+  } else {
+    window_copy_kernel<float><<<dim3(gx, h->nl), 256, 0, e->st>>>(static_cast<const RunDev<float>*>(e->d_runs),
+                                                                  h->slot);
+    frozen_stats_kernel<float><<<h->nl, 256, 0, e->st>>>(static_cast<const RunDev<float>*>(e->d_runs), h->slot,
+                                                         e->d_part);
+  }
+  CK(cudaGetLastError());
   return MRM_OK;
 }
 
@@ -2202,14 +2293,96 @@ int mrm_gpu_enqueue_steps(mrm_gpu* h, int nsteps, double dt, int llg_type) {
   if (!h) return MRM_ERR_ARG;
   int rc = plain_prepare(h, nsteps, dt, llg_type);
   if (rc) return rc;
+  if (nsteps > 0 && h->wnx) {
+    // llg() calls update_do_grain(t) before its loop and after every step
+    // (llg.f90:138,284): the steps go in runs over which the window stays put
+    int left = nsteps;
+    double t = h->t_acc;
+    while (left > 0) {
+      int i0, j0;
+      window_origin(h, t, &i0, &j0);
+      rc = place_window(h, i0, j0);
+      if (rc) return rc;
+      double tn = t + h->dt;  // the time after each further step, accumulated
+      int k = 1;
+      for (; k < left; ++k) {
+        int a, b;
+        window_origin(h, tn, &a, &b);
+        if (a != i0 || b != j0) break;
+        tn += h->dt;
+      }
+      rc = engine_step(h->eng, k, llg_type);
+      if (rc) {
+        h->err = h->eng->err;
+        return rc;
+      }
+      t = tn;
+      left -= k;
+    }
+    h->t_acc = t;
+    h->has_stats = true;
+    return MRM_OK;
+  }
   if (nsteps > 0) {
     rc = engine_step(h->eng, nsteps, llg_type);
     if (rc) {
       h->err = h->eng->err;
       return rc;
     }
+    for (int k = 0; k < nsteps; ++k) h->t_acc += h->dt;
     h->has_stats = true;
   }
+  return MRM_OK;
+}
+
+int mrm_gpu_set_window(mrm_gpu* h, int nx_win, int ny_win, double vx, double vy, double offset_x, double offset_y) {
+  if (!h) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  Engine* e = h->eng;
+  if (!h->own_engine || e->runs.size() != 1)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "a moving demag window runs on a handle of its own, not in a batch");
+  if (nx_win < 2 || ny_win < 2 || nx_win > h->g.nx || ny_win > h->g.ny)
+    return set_err(errp, MRM_ERR_ARG, "window %d x %d outside 2 .. %d x %d", nx_win, ny_win, h->g.nx, h->g.ny);
+  const bool none = nx_win == h->g.nx && ny_win == h->g.ny;  // update_do_grain: the whole grid (data.f90:127)
+  mrm_geom gw = h->g;
+  gw.nx = nx_win;
+  gw.ny = ny_win;
+  int rc = validate_geom(&gw, errp);
+  if (rc) return rc;
+  for (int l = 0; l < h->nl; ++l)
+    if (h->L[l].cgrain) return set_err(errp, MRM_ERR_UNSUPPORTED, "a moving demag window needs one grain per cell");
+  CK(cudaSetDevice(e->dev));
+  CK(cudaStreamSynchronize(e->st));
+  dfree(h->spech);
+  dfree(h->specx);
+  dfree(h->tens);
+  h->wnx = none ? 0 : nx_win;
+  h->wny = none ? 0 : ny_win;
+  h->wvx = vx;
+  h->wvy = vy;
+  h->wox = offset_x;
+  h->woy = offset_y;
+  h->wi0 = h->wj0 = -1;
+  fft_grid(none ? h->g : gw, &h->px, &h->py);
+  h->lgpx = ilog2(h->px);
+  h->lgpy = ilog2(h->py);
+  rc = spectra_alloc(h);
+  if (!rc) rc = dmalloc(errp, &h->tens, tensor_bytes(h));
+  if (rc) return rc;
+  h->tensor_ready = false;  // the window's tensor: build or upload it again
+  h->spec_valid = false;
+  e->tables_dirty = true;
+  e->desc_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_gpu_get_window(const mrm_gpu* h, int* out4) {
+  if (!h || !out4) return MRM_ERR_ARG;
+  out4[0] = h->wnx ? h->wnx : h->g.nx;
+  out4[1] = h->wnx ? h->wny : h->g.ny;
+  out4[2] = out4[3] = 0;
+  // where update_do_grain puts it at the handle's time (after the last step)
+  if (h->wnx) window_origin(h, h->t_acc, &out4[2], &out4[3]);
   return MRM_OK;
 }
 
@@ -2264,6 +2437,7 @@ int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, 
   Engine* e = h->eng;
   if (e->runs.size() != 1)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps run on a handle of its own, not in a batch");
+  if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps with a moving demag window");
   int rc = plain_prepare(h, 0, h->dt, llg_type);
   if (rc) return rc;
   const size_t re = relem(h->g.precision), n = (size_t)h->g.nx * h->g.ny;
@@ -2349,6 +2523,7 @@ int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, 
     *dt = *dt * *max_dmdt;  // llg.f90:268
     *max_dmdt = next;
   }
+  h->t_acc = h->t_base + (double)(h->step - h->step_base) * h->dt;  // (no window here)
   if (out) *out = st;
   return finish(MRM_OK);
 }
@@ -2747,6 +2922,7 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   if (!m || !hdemag) return set_err(errp, MRM_ERR_ARG, "m and hdemag must be device pointers");
   if (h->g.precision != MRM_FP32)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
+  if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation has no moving window");
   for (int l = 0; l < h->nl; ++l)
     if (h->L[l].cgrain)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes one grain per cell");

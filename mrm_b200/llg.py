@@ -145,6 +145,18 @@ class _RunMixin:
                                               float(vel[0]), float(vel[1]), off[0], off[1], float(ref[0]),
                                               float(ref[1]), float(t_origin)))
 
+    def set_window(self, nx_win: int, ny_win: int, v=(0.0, 0.0), offset=(0.0, 0.0)):
+        """Moving demag window (include/mrm_gpu.h mrm_gpu_set_window); the tensor
+        must be built or uploaded again afterwards."""
+        self._check(_lib.load().mrm_gpu_set_window(self.h, int(nx_win), int(ny_win), float(v[0]), float(v[1]),
+                                                   float(offset[0]), float(offset[1])))
+
+    def get_window(self):
+        """(nx_win, ny_win, i0, j0): the window's size and current origin."""
+        out = (C.c_int * 4)()
+        self._check(_lib.load().mrm_gpu_get_window(self.h, out))
+        return tuple(out)
+
     def set_cubic_axes(self, layer, cubic_axis):
         """Cubic anisotropy on `layer`: cubic_axis (N,3,3), row i = crystal axis i in
         lab coordinates (None: back to uniaxial)."""
@@ -221,6 +233,9 @@ class GpuSim(_RunMixin):
         if rc != 0:
             raise MrmError(rc, (L.mrm_gpu_last_error(None) or b"").decode())
         self.h = h
+        win = getattr(medium, "window", None)
+        if win:
+            self.set_window(win["nx"], win["ny"], win.get("v", (0.0, 0.0)), win.get("offset", (0.0, 0.0)))
         self.upload_medium(medium, thermal_seed)
         if demag:
             if tensor is None:

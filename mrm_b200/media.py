@@ -102,6 +102,9 @@ class Medium:
     layers: List[Layer]
     boundary: int = 1          # 0 periodic (reference), 1 open / zero-padded 2x
     images: int = 2
+    # moving demag window: dict(nx, ny, v=(vx, vy), offset=(ox, oy)) (include/mrm_gpu.h
+    # mrm_gpu_set_window); None: the demag covers the whole grid
+    window: Optional[dict] = None
     space_to_sul: float = 0.0
     sul_mu: float = 1.0
     head_mu: float = 1.0

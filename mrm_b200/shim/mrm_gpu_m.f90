@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -108,6 +108,20 @@ module mrm_gpu_m
       type(C_PTR), value :: h
       integer(C_INT), value :: layer
       real(C_DOUBLE), intent(in) :: cubic_axis(3, 3, *)
+    end function
+    integer(C_INT) function c_set_window(h, nxw, nyw, vx, vy, ox, oy) bind(C, name="mrm_gpu_set_window")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: nxw, nyw
+      real(C_DOUBLE), value :: vx, vy, ox, oy
+    end function
+    integer(C_INT) function c_set_field_table(h, layer, nfx, nfy, xpos, ypos, vfld, vx, vy, ox, oy, rx, ry, t0) &
+        bind(C, name="mrm_gpu_set_field_table")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, nfx, nfy
+      real(C_DOUBLE), intent(in) :: xpos(*), ypos(*), vfld(*)
+      real(C_DOUBLE), value :: vx, vy, ox, oy, rx, ry, t0
     end function
     integer(C_INT) function c_off_field(h, zoff, dzobs, head_mu, fly_height, sul_mu, space_to_sul, num_images, out) &
         bind(C, name="mrm_gpu_off_field")
@@ -272,6 +286,27 @@ contains
     integer, intent(in) :: layer
     real(C_DOUBLE), intent(in) :: cubic_axis(:, :, :)
     ok_p = ok(c_set_cubic_axes(h, int(layer - 1, C_INT), cubic_axis))
+  end function
+
+  ! moving demag window nxfft x nyfft following window%v, window%offset
+  ! (include/mrm_gpu.h mrm_gpu_set_window); build or upload its tensor afterwards
+  logical function gpu_set_window(h, nxfft, nyfft, v, offset) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: nxfft, nyfft
+    real(C_DOUBLE), intent(in) :: v(2), offset(2)
+    ok_p = ok(c_set_window(h, int(nxfft, C_INT), int(nyfft, C_INT), v(1), v(2), offset(1), offset(2)))
+  end function
+
+  ! a file_applied field table on `layer`: vfld(3, nx, ny) at xpos(nx), ypos(ny)
+  ! (include/mrm_gpu.h mrm_gpu_set_field_table)
+  logical function gpu_set_field_table(h, layer, xpos, ypos, vfld, vel_x, vel_y, offset_x, offset_y, ref_x, ref_y, &
+                                       t_origin) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: xpos(:), ypos(:), vfld(:, :, :)
+    real(C_DOUBLE), intent(in) :: vel_x, vel_y, offset_x, offset_y, ref_x, ref_y, t_origin
+    ok_p = ok(c_set_field_table(h, int(layer - 1, C_INT), int(size(xpos), C_INT), int(size(ypos), C_INT), xpos, ypos, &
+                                vfld, vel_x, vel_y, offset_x, offset_y, ref_x, ref_y, t_origin))
   end function
 
   ! stray field of the current state on the slab zoff..zoff+dzobs (cm) above the

@@ -454,6 +454,11 @@ struct Layer {
   std::vector<int> uhx_idx, uhx_nbr, lhx_idx, lhx_nbr;  // interlayer (upper = layer-1)
   std::vector<double> uhx, lhx;
   std::vector<int> g2c_idx, g2c_i, g2c_j;  // grain -> cells (0-based i,j)
+  std::vector<int> c2g;                    // cell -> grain (-1: empty), grid2grain
+  // moving demag window (update_do_grain, data.f90:120-157): grains with a cell
+  // in the window, and the first and last of them (min_n, max_n, 0-based)
+  std::vector<char> do_grain;
+  int min_n = 0, max_n = -1;
   std::vector<double> m[2], dm, h, hthm, hdemag, happ;
   // schedule: uniform field x linear ramp (applied.f90:863-883)
   double hdir[3] = {0, 0, 0};
@@ -502,6 +507,10 @@ struct Sim {
   bool demag_on = true;
   std::vector<Layer> L;
   int in = 0;          // which m buffer is current (llg.f90 `in` toggle, 0 or 1)
+  // moving demag window (window_m, data.f90:1-65): size (0: none), window%v,
+  // window%offset, current origin
+  int wnx = 0, wny = 0, wi0 = 0, wj0 = 0;
+  double wvx = 0, wvy = 0, wox = 0, woy = 0;
   double t = 0.0;
   long long step = 0;
   int rng_mode = 0;  // 0: MT per layer (reference), 1: Philox (GPU stream)
@@ -528,9 +537,13 @@ static void scatter_m(Sim* s, int buf, std::vector<double>& grid) {
     Layer& Ly = s->L[l];
     const double* m = Ly.m[buf].data();
     for (int n = 0; n < Ly.N; ++n) {
+      if (!Ly.do_grain[n]) continue;
       double f = Ly.ms[n] * Ly.ms_scale[n];
       for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
-        size_t cell = (size_t)Ly.g2c_j[q] * s->px + Ly.g2c_i[q];
+        // get_mag with a window (data.f90:357-385): the cells inside it, shifted
+        const int i = Ly.g2c_i[q] - s->wi0, j = Ly.g2c_j[q] - s->wj0;
+        if (s->wnx && (i < 0 || j < 0 || i >= s->wnx || j >= s->wny)) continue;
+        size_t cell = (size_t)j * s->px + i;
         for (int a = 0; a < 3; ++a) grid[((size_t)l * 3 + a) * plane + cell] = f * m[3 * n + a];
       }
     }
@@ -563,9 +576,14 @@ static void gather_demag(Sim* s, const std::vector<double>& grid) {
   for (int l = 0; l < s->nl; ++l) {
     Layer& Ly = s->L[l];
     for (int n = 0; n < Ly.N; ++n) {
+      if (!Ly.do_grain[n]) continue;
       double y[3] = {0, 0, 0};
       for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) {
-        size_t cell = (size_t)Ly.g2c_j[q] * s->px + Ly.g2c_i[q];
+        // get_magnetostatic with a window (field.f90:472-495): the cells inside
+        // it, over all of the grain's cells
+        const int i = Ly.g2c_i[q] - s->wi0, j = Ly.g2c_j[q] - s->wj0;
+        if (s->wnx && (i < 0 || j < 0 || i >= s->wnx || j >= s->wny)) continue;
+        size_t cell = (size_t)j * s->px + i;
         for (int a = 0; a < 3; ++a) y[a] += grid[((size_t)l * 3 + a) * plane + cell];
       }
       double cnt = (double)(Ly.g2c_idx[n + 1] - Ly.g2c_idx[n]);
@@ -696,6 +714,7 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
     double el = 0.0;
 #pragma omp parallel for reduction(+ : el)
     for (int n = 0; n < Ly.N; ++n) {
+      if (!Ly.do_grain[n]) continue;  // field.f90:199-233 (a frozen grain keeps its last field)
       double ha[3] = {sc * Ly.hdir[0], sc * Ly.hdir[1], sc * Ly.hdir[2]};
       if (Ly.tab)
         for (int a = 0; a < 3; ++a) ha[a] = hat[3 * n + a];
@@ -789,6 +808,7 @@ static void get_thermal(Sim* s) {
     }
     double tsigma = std::sqrt(2.0 * kB * Ly.alpha / Ly.gamma);
     for (int n = 0; n < Ly.N; ++n) {
+      if (!Ly.do_grain[n]) continue;
       double x = 0.0;
       if (Ly.ms_scale[n] > 0.0)
         x = Ly.alpha_scale[n] * Ly.temperature /
@@ -824,11 +844,18 @@ static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, d
   const double sdt0 = std::sqrt(dt0);
 #pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
   for (int n = 0; n < Ly.N; ++n) {
+    if (n < Ly.min_n || n > Ly.max_n) continue;  // llg.f90:1081
     double h[3];
     for (int a = 0; a < 3; ++a) h[a] = Ly.hthm[3 * n + a] / sdt0 + Ly.h[3 * n + a];
     double* mnext = &Ly.m[1 - id][3 * n];
     const double* mcur = &Ly.m[id][3 * n];
-    if (Ly.ms_scale[n] > 0.0) {
+    if (!Ly.do_grain[n]) {
+      // a frozen grain keeps its state (llg.f90:1149-1152)
+      for (int a = 0; a < 3; ++a) {
+        mnext[a] = mcur[a];
+        Ly.dm[3 * n + a] = 0.0;
+      }
+    } else if (Ly.ms_scale[n] > 0.0) {
       double m[3] = {mcur[0], mcur[1], mcur[2]};
       double t[3], d[3], y;
       const double ms2 = Ly.ms[n] * Ly.ms[n];
@@ -962,8 +989,9 @@ static void push_passes(Sim* s, double dt, int type, double* errmx, double* errm
     for (int l = 0; l < nl; ++l) {
       double e0, e1, m1;
       push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
-      double vs = 0;
-      for (int n = 0; n < s->L[l].N; ++n) vs += s->L[l].vol[n];
+      double vs = 0;  // sum(grain_vol, mask=do_grain), llg.f90:1239
+      for (int n = 0; n < s->L[l].N; ++n)
+        if (s->L[l].do_grain[n]) vs += s->L[l].vol[n];
       *mmag += m1 / vs;
       *errmx = std::max(*errmx, std::sqrt(e0));
       *errmx1 = std::max(*errmx1, e1);
@@ -980,6 +1008,42 @@ static void push_passes(Sim* s, double dt, int type, double* errmx, double* errm
   }
 }
 
+// update_do_grain (data.f90:120-157) with get_window (:52-64): the window
+// origin at time t, the grains with a cell inside it and their index range,
+// and the copy of every grain's state into the other buffer (:139).
+// Without a window every grain is pushed.
+static void update_do_grain(Sim* s, double t) {
+  for (auto& Ly : s->L) {
+    if (s->wnx == 0) {
+      Ly.do_grain.assign(Ly.N, 1);
+      Ly.min_n = 0;
+      Ly.max_n = Ly.N - 1;
+      continue;
+    }
+  }
+  if (s->wnx == 0) return;
+  // off = v t + offset rounded as two operations (no fused multiply-add), so
+  // that a half-cell tie in nint falls the same way on every build
+  volatile double vtx = s->wvx * t, vty = s->wvy * t;
+  const double offx = vtx + s->wox, offy = vty + s->woy;
+  s->wi0 = std::max(1, std::min(s->nx - s->wnx + 1, (int)std::lround((s->nx - s->wnx) * 0.5 + offx / s->dx))) - 1;
+  s->wj0 = std::max(1, std::min(s->ny - s->wny + 1, (int)std::lround((s->ny - s->wny) * 0.5 + offy / s->dy))) - 1;
+  for (auto& Ly : s->L) {
+    Ly.do_grain.assign(Ly.N, 0);
+    Ly.min_n = Ly.N;
+    Ly.max_n = -1;
+    Ly.m[1 - s->in] = Ly.m[s->in];
+    for (int j = s->wj0; j < s->wj0 + s->wny; ++j)
+      for (int i = s->wi0; i < s->wi0 + s->wnx; ++i) {
+        const int g = Ly.c2g[(size_t)j * s->nx + i];
+        if (g < 0) continue;
+        Ly.do_grain[g] = 1;
+        Ly.min_n = std::min(Ly.min_n, g);
+        Ly.max_n = std::max(Ly.max_n, g);
+      }
+  }
+}
+
 // One pass of the llg() loop body (llg.f90:240-269) with push_m (llg.f90:1195-1271)
 // at fixed dt (fixed_dt_p: max_dmdt = 1, no retries).
 static void heun_or_boris_step(Sim* s, double dt, int type) {
@@ -993,6 +1057,7 @@ static void heun_or_boris_step(Sim* s, double dt, int type) {
   s->t += dt;
   s->step += 1;
   compute_stats(s, errmx, errmx1, mmag, energy, e1l);
+  update_do_grain(s, s->t);  // llg.f90:284
 }
 
 // The same with the adaptive time step (dt_frac != 0): get_fields picks dt from
@@ -1180,6 +1245,34 @@ void* orc_create(int nx, int ny, int nl, int boundary, int images, double dx, do
 
 void orc_destroy(void* h) { delete static_cast<Sim*>(h); }
 
+// {window nx, ny, origin i0, j0} (the whole grid and 0, 0 without a window)
+void orc_get_window(void* h, int* out4) {
+  Sim* s = static_cast<Sim*>(h);
+  out4[0] = s->wnx ? s->wnx : s->nx;
+  out4[1] = s->wnx ? s->wny : s->ny;
+  out4[2] = s->wi0;
+  out4[3] = s->wj0;
+}
+
+// moving demag window (mrm_gpu_set_window's arguments): the FFT grid becomes
+// the window's; the tensor must be built or set again
+int orc_set_window(void* h, int nxw, int nyw, double vx, double vy, double ox, double oy) {
+  Sim* s = static_cast<Sim*>(h);
+  if (nxw < 2 || nyw < 2 || nxw > s->nx || nyw > s->ny) return 1;
+  const bool none = nxw == s->nx && nyw == s->ny;
+  s->wnx = none ? 0 : nxw;
+  s->wny = none ? 0 : nyw;
+  s->wvx = vx; s->wvy = vy; s->wox = ox; s->woy = oy;
+  s->wi0 = s->wj0 = 0;
+  const int fx = none ? s->nx : nxw, fy = none ? s->ny : nyw;
+  s->px = s->boundary == 1 ? 2 * fx : fx;
+  s->py = s->boundary == 1 ? 2 * fy : fy;
+  s->ph = s->px / 2 + 1;
+  s->fft.init(s->px, s->py);
+  s->nhat.clear();
+  return 0;
+}
+
 // Real-space tensor of the FFT grid (reference layout, with normalisation), FP64.
 // Periodic: calculate_tensor on (nx,ny) with the handle's images; open: on the
 // padded grid (2nx,2ny) with no images.
@@ -1238,6 +1331,12 @@ int orc_upload_layer(void* h, int l, int N, const double* ms, const double* vol,
   Ly.hthm.assign(3 * N, 0.0);
   Ly.hdemag.assign(3 * N, 0.0);
   Ly.happ.assign(3 * N, 0.0);
+  Ly.c2g.assign((size_t)s->nx * s->ny, -1);
+  for (int n = 0; n < N; ++n)
+    for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) Ly.c2g[(size_t)Ly.g2c_j[q] * s->nx + Ly.g2c_i[q]] = n;
+  Ly.do_grain.assign(N, 1);
+  Ly.min_n = 0;
+  Ly.max_n = N - 1;
   return 0;
 }
 
@@ -1395,6 +1494,7 @@ void orc_set_time(void* h, double t, long long step) {
 void orc_eval_field(void* h, double t) {
   Sim* s = static_cast<Sim*>(h);
   double e;
+  update_do_grain(s, t);
   get_field(s, t, s->in, &e);
 }
 
@@ -1404,6 +1504,7 @@ void orc_eval_field(void* h, double t) {
 int orc_step(void* h, int nsteps, double dt, int type, double* stats_out, double* traj) {
   Sim* s = static_cast<Sim*>(h);
   if (!(type == -3 || type == 2 || type == -2)) return 2;
+  update_do_grain(s, s->t);  // llg.f90:138
   for (int k = 0; k < nsteps; ++k) {
     heun_or_boris_step(s, dt, type);
     if (traj)
@@ -1420,6 +1521,7 @@ int orc_step_adaptive(void* h, int nsteps, int type, double dt_frac, double dt_m
                       double* max_dmdt, double* stats_out) {
   Sim* s = static_cast<Sim*>(h);
   if (!(type == -3 || type == 2 || type == -2)) return 2;
+  if (s->wnx) return 3;  // fixed dt only with a moving window
   for (int k = 0; k < nsteps; ++k) adaptive_step(s, type, dt_frac, dt_max, max_dm, dt, max_dmdt);
   if (stats_out) std::memcpy(stats_out, &s->last, sizeof(Stats));
   return 0;

@@ -56,6 +56,8 @@ def lib():
         L.orc_set_head_field.argtypes = [vp, i, d, d, d, d, d, d, d, u64, i]
         L.orc_set_cubic_axes.argtypes = [vp, i, P(d)]
         L.orc_set_field_table.argtypes = [vp, i, i, i, P(d), P(d), P(d), d, d, d, d, d, d, d]
+        L.orc_set_window.argtypes = [vp, i, i, d, d, d, d]
+        L.orc_get_window.argtypes = [vp, P(i)]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
         L.orc_get_field.argtypes = [vp, i, P(d)]
@@ -232,8 +234,14 @@ class OracleSim:
                 if cpl is not None:
                     idx, gr, cf = i32(cpl[0]), i32(cpl[1]), f64(cpl[2])
                     L.orc_upload_interlayer(self.h, l, side, _p(idx, C.c_int), _p(gr, C.c_int), _p(cf))
-        px = medium.nx * (2 if medium.boundary == 1 else 1)
-        py = medium.ny * (2 if medium.boundary == 1 else 1)
+        fx, fy = medium.nx, medium.ny
+        win = getattr(medium, "window", None)
+        if win:
+            assert L.orc_set_window(self.h, win["nx"], win["ny"], *win.get("v", (0.0, 0.0)),
+                                    *win.get("offset", (0.0, 0.0))) == 0
+            fx, fy = win["nx"], win["ny"]
+        px = fx * (2 if medium.boundary == 1 else 1)
+        py = fy * (2 if medium.boundary == 1 else 1)
         self.px, self.py = px, py
         if demag:
             if tensor is None:
@@ -278,6 +286,12 @@ class OracleSim:
         out = np.zeros((n, 3))
         lib().orc_get_demag(self.h, layer, _p(out))
         return out
+
+    def get_window(self):
+        """(nx_win, ny_win, i0, j0) of the moving demag window."""
+        out = (C.c_int * 4)()
+        lib().orc_get_window(self.h, out)
+        return tuple(out)
 
     def get_applied(self, layer: int) -> np.ndarray:
         """Applied field per grain of the last field evaluation."""
