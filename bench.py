@@ -424,7 +424,7 @@ def window_write_leg(torch, local, steps):
     med.window = dict(nx=512, ny=256, v=(2000.0, 0.0), offset=(-0.5 * 2048 * med.dx, 0.0))
     sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1)
     ext = torch.cuda.ExternalStream(sim.stream(), device=local)
-    sim.set_time(4e-8, 0)  # the head 800 nm (1,143 cells) down the track, the window centred on it
+    sim.set_time(3.6e-7, 0)  # the head 7.2 um (1,029 cells) down the track, the window centred on it
     sim.step(48, DT, stats=False)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
