@@ -468,6 +468,33 @@ def table_write_leg(torch, local, steps):
             "value": grains * steps / (ms * 1e-3), "unit": UNIT, "us_per_heun_step": 1e3 * ms / steps}
 
 
+def llb_leg(torch, local, steps=2000):
+    """The heat-assisted LLB workload (f3): a 256 x 256-grain FePt-like layer at
+    T = 600 K below a distributed Tc ~ 700 K with thermal noise and a reversing
+    field, push_llb's Heun branch with |m| per grain, FP32 state (the push in
+    FP64 arithmetic), one plain run."""
+    from mrm_b200 import FP32, GpuSim, media
+    med = media.llb_medium(256, seed=1)
+    sim = GpuSim(med, precision=FP32, device=local, thermal_seed=1)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.step(48, 1e-14, stats=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.enqueue(steps, 1e-14)
+    e1.record(ext)
+    st = sim.stats()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    mag = float(np.mean(sim.get_mag(0)))
+    sim.close()
+    n = med.n_grains
+    return {"workload": f"LLB heat-assisted layer 256x256 (T 600 K, Tc ~ 700 K +- 3 %, S = 1/2, 8 kOe reversing), "
+                        f"FP32, {steps} Heun steps of 10 fs",
+            "value": n * steps / (ms * 1e-3), "unit": UNIT, "us_per_heun_step": 1e3 * ms / steps,
+            "mean_abs_m": mag, "mave_z": float(st["mave"][2])}
+
+
 def mix_leg(torch, local, steps=5000, nreal=64):
     from mrm_b200 import FP32
     from mrm_b200.batch import Batch
@@ -613,6 +640,7 @@ def main():
                                 "fp64_us_per_heun_step": p64["us_per_heun_step"]})
         line["mix"] = mix_leg(torch, local)
         line["write"] = write_leg(torch, local)
+        line["llb"] = llb_leg(torch, local)
         if args.served > 0:
             line["served"] = served_leg(local, args.served)
         if world == 1 and not args.no_cpu_baseline:

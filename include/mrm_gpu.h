@@ -189,6 +189,21 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
                             const double* vfld, double vel_x, double vel_y, double offset_x, double offset_y,
                             double ref_x, double ref_y, double t_origin);
 
+/* LLB integrator (llgp%llb; push_llb, llg.f90:916-1064, Heun branch
+ * :1000-1047 and the |m| = 0 branch :1048-1060) on `layer`: spin S, per grain
+ * Curie temperature tc (K, > 0) and lambdaMs (Oe; lambda_m = lambdaMs (S+1)/S);
+ * the layer's temperature (mrm_gpu_set_thermal, > 0), damping and gamma.  Each
+ * grain carries a magnitude |m| (mag, 1 after mrm_gpu_set_state) beside its
+ * direction; the thermal variance divides by max(floor_ms, |m|) once |m| != 1
+ * (get_thermal, field.f90:416-417); the stats' mmag is sum |m| vol over the
+ * pushed grains' volume.  llgp%llb is one switch for all layers: every layer of
+ * the run must have it; llg_type -3 only.  tc = NULL turns it off.  Set it after
+ * the layer's upload (an upload clears it).  mrm_gpu_set_mag / _get_mag: |m|
+ * per grain (layer%mag(in, :)). */
+int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms);
+int mrm_gpu_set_mag(mrm_gpu* h, int layer, const double* mag);
+int mrm_gpu_get_mag(mrm_gpu* h, int layer, double* mag);
+
 /* Moving demag window (nxfft/nyfft < nx/ny; window_m and update_do_grain,
  * data.f90:1-65,120-157, get_mag / get_magnetostatic :322-390,
  * field.f90:438-517): the demag FFT covers nx_win x ny_win cells whose origin

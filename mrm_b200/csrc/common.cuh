@@ -51,8 +51,20 @@ struct TabDev {
   double ox, oy, vx, vy, rx, ry, t0, dx, dy;
 };
 
+// LLB integrator of a layer (llgp%llb: push_llb, llg.f90:916-1064), in device
+// memory: per grain {Tc, lambda_m = lambdaMs (spin + 1)/spin,
+// 2 k_B alpha alpha_scale / (gamma Ms V) (get_thermal's variance without
+// T/|m|), 0}; the layer's spin, damping alpha and floor_ms (get_thermal's
+// |m| floor); the temperature is the layer's (LayerDev::temperature).  The
+// grain's magnitude |m| (mag) rides in the w lane of m and mp.
+struct LlbDev {
+  const V4<double>* p;
+  double spin, alpha, floor_ms;
+};
+
 // Per-layer device view of one run.  State vectors are float4/double4
-// "SoA of 4-vectors": (x,y,z,unused) per grain for one 16/32-byte load.
+// "SoA of 4-vectors": (x,y,z,w) per grain for one 16/32-byte load (w of m and
+// mp: the magnitude |m| of the LLB integrator; unused otherwise).
 template <typename R>
 struct LayerDev {
   V4<R>* m;         // m_n (state at step boundaries)
@@ -99,6 +111,7 @@ struct LayerDev {
   unsigned long long hd_bits;
   int hd_nbits;
   const struct TabDev* tab;  // tabulated field profile (null: the uniform hdir applies)
+  const LlbDev* llb;         // LLB integrator (null: LLG)
   double temperature;
   double tfac;  // sqrt(temperature / dt), set with the run's dt
   double gamma;

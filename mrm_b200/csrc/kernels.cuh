@@ -156,6 +156,194 @@ MRM_D void tab_value(const double* __restrict__ v, int tnx, TabW wx, TabW wy, do
   vz = w00 * a[2] + w10 * a[5] + w01 * c[2] + w11 * c[5];
 }
 
+// ---------------- LLB integrator (llgp%llb) ----------------
+constexpr double kGmubKb = 1.343427768e-4;  // g mu_B / k_B (llg.f90:924)
+constexpr double kBoltz = 1.380662e-16;     // field.f90:407
+
+// lv(x) = coth x - 1/x and dlv = d lv/dx = 1/x^2 - csch^2 x with the
+// reference's small-argument forms (llg.f90:704-710,727-733)
+MRM_D double llb_lv(double x) { return fabs(x) > 1e-2 ? 1.0 / tanh(x) - 1.0 / x : x / 3.0; }
+MRM_D double llb_dlv(double x) {
+  if (fabs(x) > 4e-3) {
+    const double s = sinh(x);
+    return 1.0 / (x * x) - 1.0 / (s * s);
+  }
+  return 1.0 / 3.0;
+}
+
+// One grain of push_llb (llg.f90:916-1064), Heun (llg_type -3):
+//   mc, magc: the current state and magnitude; mpr, magp: the predicted ones
+//   (second pass); h: the field without thermal; ht: thermal field / sqrt(dt);
+//   d1: the first pass's increment (second pass); ab = alpha alpha_scale;
+//   tc, lam = Tc and lambdaMs (spin + 1)/spin; T the temperature; dt the step.
+// Out: the new direction and magnitude, the increment d (the first pass
+// stores it), |d|^2 (errmx1: the squared magnitude change on the |m| = 0
+// branch) and |m x (h + h_perp)|^2 (errmx).
+struct LlbStep {
+  double m[3], mag, d[3], d2, tq2;
+};
+MRM_D LlbStep llb_heun(bool corr, const double* mc, double magc, const double* mpr, double magp, const double* h,
+                       const double* ht, const double* d1, double ab, double tc, double lam, const LlbDev& P,
+                       double T, double gamma, double dt) {
+  LlbStep o;
+  const double scale1 = -0.5 * gamma * dt;
+  o.tq2 = 0.0;
+  if (!(magc > 0.0)) {
+    // |m| = 0 (llg.f90:1048-1060): m along h, |m| relaxed towards its equilibrium
+    const double y = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    if (y > 0.0) {
+      for (int a = 0; a < 3; ++a) o.m[a] = h[a] / y;
+      const double meq = kGmubKb * P.spin * y / T;
+      const double scale2 = lam * T / (3.0 * llb_dlv(meq) * tc);
+      o.mag = (y / scale2 + llb_lv(meq)) * (1.0 - exp(2.0 * scale1 * scale2 * 2.0 * T * P.alpha / (3.0 * tc)));
+    } else {
+      for (int a = 0; a < 3; ++a) o.m[a] = mc[a];
+      o.mag = magc;
+    }
+    for (int a = 0; a < 3; ++a) o.d[a] = 0.0;
+    o.d2 = (o.mag - magc) * (o.mag - magc);
+    return o;
+  }
+  double m[3], mag;
+  if (corr) {  // llg.f90:1002-1004
+    for (int a = 0; a < 3; ++a) m[a] = mpr[a];
+    mag = magp;
+    if (mag <= 0.0) {
+      mag = 0.0;
+      const double y = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+      if (y != 0.0)
+        for (int a = 0; a < 3; ++a) m[a] = h[a] / y;
+    }
+  } else {
+    for (int a = 0; a < 3; ++a) m[a] = mc[a];
+    mag = magc;
+  }
+  double ht3[3];
+  for (int a = 0; a < 3; ++a) ht3[a] = h[a] + lam * mag * m[a];
+  const double mh = sqrt(ht3[0] * ht3[0] + ht3[1] * ht3[1] + ht3[2] * ht3[2]);
+  if (mh != 0.0)
+    for (int a = 0; a < 3; ++a) ht3[a] /= mh;
+  const double meq = kGmubKb * P.spin * mh / T;
+  const double lvm = llb_lv(meq);
+  const double aperp = P.alpha * (1.0 - lam * lvm * T / (3.0 * mh * tc));
+  const double apar = P.alpha * 2.0 * T / (3.0 * tc);
+  // thermal field hthm / sqrt(alpha alpha_scale dt0), split along m (llg.f90:1016-1026)
+  const double rs = 1.0 / sqrt(ab);
+  double th[3], hpar[3], hperp[3];
+  for (int a = 0; a < 3; ++a) th[a] = ht[a] * rs;
+  const double tp = th[0] * m[0] + th[1] * m[1] + th[2] * m[2];
+  const double fpar = sqrt(apar), fperp = sqrt(fmax(0.0, aperp - apar) / (aperp * aperp));
+  for (int a = 0; a < 3; ++a) {
+    hpar[a] = tp * m[a];
+    hperp[a] = (th[a] - hpar[a]) * fperp;
+    hpar[a] *= fpar;
+  }
+  const double scale11 = 2.0 * scale1;
+  const double mht = m[0] * ht3[0] + m[1] * ht3[1] + m[2] * ht3[2];
+  const double mq = apar * (lam / mh) * lam * 2.0 * scale1 * T * lvm / (3.0 * llb_dlv(meq) * tc) * (mag - lvm * mht);
+  double hh[3] = {h[0] + hperp[0], h[1] + hperp[1], h[2] + hperp[2]}, t[3], mxh[3], mxt[3];
+  cross3(m[0], m[1], m[2], hh[0], hh[1], hh[2], t[0], t[1], t[2]);
+  cross3(m[0], m[1], m[2], h[0], h[1], h[2], mxh[0], mxh[1], mxh[2]);
+  cross3(m[0], m[1], m[2], t[0], t[1], t[2], mxt[0], mxt[1], mxt[2]);
+  const double sm = copysign(fmin(0.5, fabs(mq)), mq);
+  for (int a = 0; a < 3; ++a) o.d[a] = scale11 * (mag * mxh[a] + aperp * mxt[a] + hpar[a]) + sm * m[a];
+  if (corr)
+    for (int a = 0; a < 3; ++a) o.d[a] = 0.5 * (o.d[a] + d1[a]);
+  o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+  o.d2 = o.d[0] * o.d[0] + o.d[1] * o.d[1] + o.d[2] * o.d[2];
+  // m(t+dt) = m |m| + d (llg.f90:1039-1047)
+  double w[3];
+  for (int a = 0; a < 3; ++a) w[a] = mc[a] * magc + o.d[a];
+  const double y = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (y > 0.0) {
+    for (int a = 0; a < 3; ++a) o.m[a] = w[a] / y;
+    o.mag = y;
+  } else {
+    for (int a = 0; a < 3; ++a) o.m[a] = -mc[a];
+    o.mag = 0.0;
+  }
+  return o;
+}
+
+// One grain of push_llb's semi-implicit branch (llg.f90:935-999), |type| = 2:
+// first = the first or only pass (llg_type 2, or the first pass of -2, which
+// relaxes |m| from the current state), else the second pass of -2 (from the
+// predicted state mpr, magp).  dt is the pass's step (dt/2 for the first pass
+// of -2).  Out: the new direction and magnitude, |dm|^2 as errmx1 forms it,
+// |m x h|^2.  (|m| = 0: llb_heun's branch, the same for both pushes.)
+MRM_D LlbStep llb_boris(bool first, const double* mc, double magc, const double* mpr, double magp, const double* h,
+                        const double* ht, double ab, double tc, double lam, const LlbDev& P, double T, double gamma,
+                        double dt) {
+  LlbStep o;
+  const double scale1 = -0.5 * gamma * dt, scale11 = scale1;
+  const double a = P.alpha;
+  double m[3], mag, ht3[3], mh, meq;
+  auto field_tot = [&](const double* mm, double mg) {
+    for (int c = 0; c < 3; ++c) ht3[c] = h[c] + lam * mg * mm[c];
+    mh = sqrt(ht3[0] * ht3[0] + ht3[1] * ht3[1] + ht3[2] * ht3[2]);
+    if (mh != 0.0)
+      for (int c = 0; c < 3; ++c) ht3[c] /= mh;
+    meq = kGmubKb * P.spin * mh / T;
+  };
+  if (first) {  // :940-947
+    for (int c = 0; c < 3; ++c) m[c] = mc[c];
+    field_tot(m, magc);
+    const double lvm = llb_lv(meq);
+    mag = lvm * (m[0] * ht3[0] + m[1] * ht3[1] + m[2] * ht3[2]);
+    mag = mag + (magc - mag) * exp(scale1 * 2.0 * a * lam * lam * T * T * lvm /
+                                   (3.0 * tc * tc * llb_dlv(meq) * (mh + 1e-20)));
+  } else {
+    for (int c = 0; c < 3; ++c) m[c] = mpr[c];
+    mag = magp;
+  }
+  field_tot(m, mag);  // :952-954
+  const double aperp = a * (1.0 - lam * llb_lv(meq) * T / (3.0 * mh * tc));
+  const double apar = a * 2.0 * T / (3.0 * tc);
+  const double scale2 = -aperp / (fabs(mag) + 1e-20);
+  // h + hthm sqrt(|scale2 / (alpha alpha_scale dt0 (|mag| + 1e-20))|), hthm / sqrt(dt0) = ht
+  const double fth = sqrt(fabs(scale2 / (ab * (fabs(mag) + 1e-20))));
+  double hb[3], t[3], om[3], tt[3], d[3];
+  for (int c = 0; c < 3; ++c) hb[c] = h[c] + ht[c] * fth;
+  cross3(mc[0], mc[1], mc[2], hb[0], hb[1], hb[2], t[0], t[1], t[2]);
+  o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+  for (int c = 0; c < 3; ++c) om[c] = scale11 * hb[c] + scale2 * mc[c];  // |type| = 2 (:971)
+  cross3(mc[0], mc[1], mc[2], om[0], om[1], om[2], tt[0], tt[1], tt[2]);
+  for (int c = 0; c < 3; ++c) tt[c] += mc[c];
+  const double y = 2.0 / (1.0 + om[0] * om[0] + om[1] * om[1] + om[2] * om[2]);
+  cross3(tt[0], tt[1], tt[2], om[0], om[1], om[2], d[0], d[1], d[2]);
+  for (int c = 0; c < 3; ++c) {
+    d[c] *= y;
+    o.m[c] = mc[c] + d[c];
+  }
+  // the magnitude at the midpoint direction (:978-986)
+  double mid[3];
+  for (int c = 0; c < 3; ++c) mid[c] = mc[c] + 0.5 * d[c];
+  field_tot(mid, mag);
+  const double lvm = llb_lv(meq);
+  const double sg = copysign(1.0, mag);
+  double mg2 = lvm * sg * (mid[0] * ht3[0] + mid[1] * ht3[1] + mid[2] * ht3[2]);
+  double q = mg2 + (magc - mg2) * exp(scale1 * 4.0 * a * lam * lam * T * T * lvm /
+                                      (3.0 * tc * tc * llb_dlv(meq) * (mh + 1e-20)));
+  const double fpar = sqrt(fabs(apar / ab));
+  q = q - 2.0 * scale11 * (ht[0] * fpar * mid[0] + ht[1] * fpar * mid[1] + ht[2] * fpar * mid[2]);
+  o.mag = fabs(q);
+  if (q < 0.0) {  // :988-991
+    const double r = sqrt(mid[0] * mid[0] + mid[1] * mid[1] + mid[2] * mid[2]);
+    for (int c = 0; c < 3; ++c) {
+      o.m[c] = -mid[c] / r;
+      d[c] = o.m[c] - mc[c];
+    }
+  }
+  const double ya = 0.5 * (o.mag + magc);
+  double e[3];
+  for (int c = 0; c < 3; ++c) {
+    o.d[c] = d[c];
+    e[c] = d[c] * ya + mc[c] * (o.mag - magc);
+  }
+  o.d2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+  return o;
+}
+
 // shared memory of a row block's table weights (grid columns, then the
 // block's rows; at most 8 rows per block)
 MRM_HD int field_table_bytes(int nx) { return (nx + 8) * (int)sizeof(TabW); }
@@ -703,7 +891,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         // the grain's stream (one per grain, shared by its cells)
         const int nt = L.cgrain ? max(0, L.cgrain[n]) : n;
         thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)nt, gn);
-        const R s = pb.w * tfac;
+        R s = pb.w * tfac;
+        if (GEN && L.llb && (double)mf.w != 1.0) {
+          // get_thermal with |m| != 1 (field.f90:416-417): the variance over
+          // max(floor_ms, |m|) instead of max(floor_ms, ms_scale)
+          const LlbDev& P = *L.llb;
+          s = (R)sqrt(P.p[n].z * L.temperature / (fmax(P.floor_ms, fabs((double)mf.w)) * rd.dt));
+        }
         htx = s * gn[0];
         hty = s * gn[1];
         htz = s * gn[2];
@@ -718,7 +912,35 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const R fx = hx + htx, fy = hy + hty, fz = hz + htz;
     V4<R> mn;
     R dx = 0, dy = 0, dz = 0, tq2 = 0;
-    if (mse > (R)0 && boris) {
+    double d2x = -1.0;  // errmx1's |dm|^2 where it is not |d|^2 (LLB)
+    const bool llb = GEN && L.llb != nullptr;
+    if (llb) {
+      // push_llb (llg.f90:916-1064), Heun, in FP64; |m| in the w lane
+      const LlbDev& P = *L.llb;
+      const V4<double> gp = P.p[n];
+      const V4<R> m0 = (STAGE == kCorr) ? M0[q] : mf;
+      const double mc[3] = {(double)m0.x, (double)m0.y, (double)m0.z};
+      const double mpr[3] = {(double)mf.x, (double)mf.y, (double)mf.z};
+      const double hh[3] = {(double)hx, (double)hy, (double)hz}, th[3] = {(double)htx, (double)hty, (double)htz};
+      double d1[3] = {0.0, 0.0, 0.0};
+      if (STAGE == kCorr) {
+        const V4<R> dd = DM[q];
+        d1[0] = dd.x;
+        d1[1] = dd.y;
+        d1[2] = dd.z;
+      }
+      // (semi-implicit: push_llb's |type| = 2 branch, its first pass over dt/2 for -2)
+      const LlbStep st =
+          (boris && (double)m0.w > 0.0)
+              ? llb_boris(STAGE == kPred, mc, (double)m0.w, mpr, (double)mf.w, hh, th, (double)pb.z, gp.x, gp.y, P,
+                          L.temperature, L.gamma, (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt)
+              : llb_heun(STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1, (double)pb.z, gp.x, gp.y, P,
+                         L.temperature, L.gamma, (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt);
+      if (STAGE == kPred && !boris) L.dm[n] = V4<R>{(R)st.d[0], (R)st.d[1], (R)st.d[2], (R)0};
+      mn = V4<R>{(R)st.m[0], (R)st.m[1], (R)st.m[2], (R)st.mag};
+      tq2 = (R)st.tq2;
+      d2x = st.d2;
+    } else if (mse > (R)0 && boris) {
       // semi-implicit push (llg.f90:1109-1118): o = -g dt/2 h - alpha m,
       // d = 2/(1+|o|^2) (m + m x o) x o, m' = m + d (norm preserved, no renormalisation);
       // m is m_n in both stages, h the field of this stage
@@ -782,7 +1004,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         mn = (STAGE == kCorr) ? M0[q] : mf;
       }
     }
-    mn.w = (R)0;
+    if (!llb) mn.w = (R)0;
     if (STAGE == kPred) L.mp[n] = mn;
     else L.m[n] = mn;
     outr[(rr * 3 + 0) * rs + i] = mse * mn.x;
@@ -809,8 +1031,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       rec[kSlotW] += w;
       if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += pv.w;  // 1: counted grain record
       rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / (pv.z * pv.z));
-      rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], (double)(dx * dx + dy * dy + dz * dz));
-      rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+      rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], d2x >= 0.0 ? d2x : (double)(dx * dx + dy * dy + dz * dz));
+      // mmag1: |m| ms_scale vol (push_llg, llg.f90:1152), |m| vol (push_llb, :1062)
+      rec[kSlotMmag] += llb ? (double)mn.w * v : sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
       rec[kSlotVA] += v;  // volume of the grains pushed (do_grain)
       // energy at the evaluated state (field.f90:200, :360, :374, :339)
       const double e_d = -((double)mf.x * ((double)hdx + apx) + (double)mf.y * ((double)hdy + apy) +
@@ -1235,7 +1458,7 @@ __global__ void __launch_bounds__(256) frozen_stats_kernel(const RunDev<R>* __re
     rec[kSlotWM + 2] += w * mz;
     rec[kSlotW] += w;
     if (mx * L.hdir[0] + my * L.hdir[1] + mz * L.hdir[2] > 0.0) rec[kSlotNup] += pv.w;
-    if (c >= nmin && c <= nmax) rec[kSlotMmag] += sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+    if (c >= nmin && c <= nmax) rec[kSlotMmag] += L.llb ? (double)mr.w * v : sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
   }
   block_reduce_record(rec, sred, part + (size_t)(rd.frz + l) * kNPart);
 }

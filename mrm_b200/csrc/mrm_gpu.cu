@@ -72,6 +72,10 @@ struct LayerBufs {
   void* tab = nullptr;
   void* tb_v = nullptr;
   void* tb_pos = nullptr;
+  // LLB integrator (null llb: LLG): the device LlbDev and its per-cell records
+  void* llb = nullptr;
+  void* llbp = nullptr;
+  double floor_ms = 0.01;
 };
 
 struct Engine;
@@ -142,6 +146,7 @@ struct Engine {
   bool has_head = false;             // a run has a layer under the write head or a tabulated
                                      // field profile (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
+  bool has_llb = false;              // a run integrates with LLB (general kernels)
   bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
   bool mapped = false;               // a run has grains of several cells (grain-averaged demag)
   double* d_part = nullptr;
@@ -503,6 +508,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.hd_bits = b.hd_bits;
     o.hd_nbits = b.hd_nbits;
     o.tab = static_cast<const TabDev*>(b.tab);
+    o.llb = static_cast<const LlbDev*>(b.llb);
   }
   return d;
 }
@@ -621,6 +627,7 @@ int build_tables(Engine* e) {
   e->nct = (int)ct.size();
   e->has_head = false;
   e->has_cubic = false;
+  e->has_llb = false;
   e->mapped = false;
   bool karlqvist_head = false;
   for (auto* r : e->runs)
@@ -628,6 +635,7 @@ int build_tables(Engine* e) {
       karlqvist_head = karlqvist_head || r->L[l].func == kFuncHead;
       e->has_head = e->has_head || r->L[l].func == kFuncHead || r->L[l].tab != nullptr;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
+      e->has_llb = e->has_llb || r->L[l].llb != nullptr;
       e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
   if (e->mapped && karlqvist_head)
@@ -692,7 +700,7 @@ template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
   // the general kernels for the semi-implicit pushes and write heads
-  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic || e->has_window;
+  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic || e->has_window || e->has_llb;
   if (stats) {
     const int i = stage == kPred ? 0 : 1;
     RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
@@ -972,6 +980,21 @@ int ensure_ready(Engine* e) {
 template <typename R>
 int run_steps(Engine* e, int nsteps, int llg_type) {
   std::string* errp = &e->err;
+  // llgp%llb is one switch for all layers (push_m, llg.f90:1218); this path has
+  // its Heun branch, and its formulas divide by the temperature
+  for (auto* r : e->runs) {
+    int nllb = 0;
+    for (int l = 0; l < r->nl; ++l) nllb += r->L[l].llb != nullptr;
+    if (!nllb) continue;
+    if (nllb != r->nl) return set_err(errp, MRM_ERR_UNSUPPORTED, "LLB on some layers of a run but not all");
+    if (llg_type != -3 && llg_type != 2 && llg_type != -2)
+      return set_err(errp, MRM_ERR_UNSUPPORTED, "LLB runs with llg_type -3, 2 or -2 on this path");
+    // update_do_grain refreshes the other buffer of m but not of |m|
+    // (data.f90:139): a frozen grain's |m| would depend on its history
+    if (r->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "LLB with a moving demag window");
+    for (int l = 0; l < r->nl; ++l)
+      if (!(r->L[l].temperature > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs a temperature > 0 (layer %d)", l);
+  }
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
   int left = nsteps;
@@ -1063,7 +1086,8 @@ __global__ void state_in_kernel(const double* __restrict__ in, V4<R>* __restrict
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int g = cgrain ? cgrain[i] : i;
-  const V4<R> v = g >= 0 ? V4<R>{(R)in[3 * g], (R)in[3 * g + 1], (R)in[3 * g + 2], (R)0} : V4<R>{0, 0, 0, 0};
+  // (w: |m| = 1, the magnitude the LLB integrator starts from, data.f90:202)
+  const V4<R> v = g >= 0 ? V4<R>{(R)in[3 * g], (R)in[3 * g + 1], (R)in[3 * g + 2], (R)1} : V4<R>{0, 0, 0, 0};
   m[i] = v;
   mp[i] = v;
 }
@@ -1076,6 +1100,25 @@ __global__ void state_out_kernel(const V4<R>* __restrict__ src, double* __restri
   out[3 * i] = (double)v.x;
   out[3 * i + 1] = (double)v.y;
   out[3 * i + 2] = (double)v.z;
+}
+
+// the LLB magnitude |m| (w lane of m): per grain in, per grain out
+template <typename R>
+__global__ void mag_in_kernel(const double* __restrict__ in, V4<R>* __restrict__ m, V4<R>* __restrict__ mp, int n,
+                              const int* __restrict__ cgrain) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int g = cgrain ? cgrain[i] : i;
+  if (g < 0) return;
+  m[i].w = (R)in[g];
+  mp[i].w = (R)in[g];
+}
+template <typename R>
+__global__ void mag_out_kernel(const V4<R>* __restrict__ src, double* __restrict__ out, int n,
+                               const int* __restrict__ gci, const int* __restrict__ gcs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = (double)src[gci ? gcs[gci[i]] : i].w;
 }
 
 // ---------------- adaptive time step ----------------
@@ -1187,6 +1230,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.xst); dfree(b.ucol); dfree(b.lcol); dfree(b.cax);
     dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm); dfree(b.hapm);
     dfree(b.tab); dfree(b.tb_v); dfree(b.tb_pos);
+    dfree(b.llb); dfree(b.llbp);
   }
 }
 
@@ -1268,7 +1312,7 @@ int upload_csr(mrm_gpu* r, int n, const int32_t* index, const int32_t* grain, co
 
 // host copies of ms_scale per layer (neighbour scaling of exchange coefficients)
 struct HostLayerCache {
-  std::vector<double> ms_scale, ms, hk_scale;  // per grain
+  std::vector<double> ms_scale, ms, hk_scale, vol, alpha_scale;  // per grain
   std::vector<int> cgrain, rep;                // map layers: cell -> grain (-1 empty), grain -> its first cell
   std::vector<double> ms_scale_cell;           // map layers: the cell's grain's ms_scale (0: empty)
 };
@@ -1349,6 +1393,8 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
   hc[l].ms_scale.assign(ms_scale, ms_scale + n);
   hc[l].ms.assign(ms, ms + n);
   hc[l].hk_scale.assign(hk_scale, hk_scale + n);
+  hc[l].vol.assign(vol, vol + n);
+  hc[l].alpha_scale.assign(alpha_scale, alpha_scale + n);
   hc[l].cgrain = cg;
   hc[l].rep = repc;
   hc[l].ms_scale_cell.clear();
@@ -1423,6 +1469,9 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
   }
   b.gamma = gamma;
   b.alpha = alpha;
+  b.floor_ms = floor_ms;
+  dfree(b.llb);  // LLB records hold the old grains' parameters: set again after an upload
+  dfree(b.llbp);
   b.uploaded = true;
   r->spec_valid = false;
   r->eng->desc_dirty = true;
@@ -2067,6 +2116,51 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
   return MRM_OK;
 }
 
+int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  std::string* errp = &h->err;
+  LayerBufs& b = h->L[layer];
+  if (!b.uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", layer);
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaStreamSynchronize(h->eng->st));
+  dfree(b.llb);
+  dfree(b.llbp);
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the general kernels
+  if (!tc) return MRM_OK;
+  if (!lambda_ms || !(spin > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs spin > 0, Tc and lambdaMs");
+  const HostLayerCache& hc = host_cache()[h][layer];
+  const int ng = b.ng, nc = b.n;
+  for (int g = 0; g < ng; ++g)
+    if (!(tc[g] > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs Tc > 0 (grain %d)", g);
+  // per cell: Tc, lambda_m = lambdaMs (spin+1)/spin (llg.f90:931), and
+  // get_thermal's 2 k_B alpha alpha_scale / (gamma Ms V) (field.f90:407,417)
+  std::vector<V4<double>> rec(nc, V4<double>{1.0, 0.0, 0.0, 0.0});
+  for (int c = 0; c < nc; ++c) {
+    const int g = hc.cgrain.empty() ? c : hc.cgrain[c];
+    if (g < 0) continue;
+    const double msv = hc.ms[g] * hc.vol[g];
+    rec[c].x = tc[g];
+    rec[c].y = lambda_ms[g] * (spin + 1.0) / spin;
+    rec[c].z = msv > 0 ? 2.0 * kBoltz * b.alpha * hc.alpha_scale[g] / (b.gamma * msv) : 0.0;
+  }
+  LlbDev d{};
+  int rc = dmalloc(errp, &b.llbp, sizeof(V4<double>) * (size_t)nc);
+  if (!rc) rc = dmalloc(errp, &b.llb, sizeof(LlbDev));
+  if (rc) {
+    dfree(b.llbp);
+    return rc;
+  }
+  d.p = static_cast<const V4<double>*>(b.llbp);
+  d.spin = spin;
+  d.alpha = b.alpha;
+  d.floor_ms = b.floor_ms;
+  CK(cudaMemcpy(b.llbp, rec.data(), sizeof(V4<double>) * (size_t)nc, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.llb, &d, sizeof(LlbDev), cudaMemcpyHostToDevice));
+  return MRM_OK;
+}
+
 int mrm_gpu_set_cubic_axes(mrm_gpu* h, int layer, const double* cubic_axis) {
   if (!h) return MRM_ERR_ARG;
   if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
@@ -2140,6 +2234,47 @@ static int get_v4(mrm_gpu* h, int layer, void* src, double* out) {
                                                      static_cast<double*>(h->xfer), n, b.gci, b.gcs);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->xfer, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MRM_OK;
+}
+
+int mrm_gpu_set_mag(mrm_gpu* h, int layer, const double* mag) {
+  if (!h || !mag) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
+  const LayerBufs& b = h->L[layer];
+  if (!b.uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", layer);
+  cudaStream_t st = h->eng->st;
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaMemcpyAsync(h->xfer, mag, sizeof(double) * b.ng, cudaMemcpyHostToDevice, st));
+  const unsigned blocks = (unsigned)((b.n + 255) / 256);
+  if (h->g.precision == MRM_FP64)
+    mag_in_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer), static_cast<V4<double>*>(b.m),
+                                                  static_cast<V4<double>*>(b.mp), b.n, b.cgrain);
+  else
+    mag_in_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const double*>(h->xfer), static_cast<V4<float>*>(b.m),
+                                                 static_cast<V4<float>*>(b.mp), b.n, b.cgrain);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return MRM_OK;
+}
+
+int mrm_gpu_get_mag(mrm_gpu* h, int layer, double* mag) {
+  if (!h || !mag) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
+  const LayerBufs& b = h->L[layer];
+  cudaStream_t st = h->eng->st;
+  CK(cudaSetDevice(h->eng->dev));
+  const unsigned blocks = (unsigned)((b.ng + 255) / 256);
+  if (h->g.precision == MRM_FP64)
+    mag_out_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const V4<double>*>(b.m),
+                                                   static_cast<double*>(h->xfer), b.ng, b.gci, b.gcs);
+  else
+    mag_out_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const V4<float>*>(b.m), static_cast<double*>(h->xfer),
+                                                  b.ng, b.gci, b.gcs);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(mag, h->xfer, sizeof(double) * b.ng, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return MRM_OK;
 }
@@ -2438,6 +2573,8 @@ int mrm_gpu_step_adaptive(mrm_gpu* h, int nsteps, int llg_type, double dt_frac, 
   if (e->runs.size() != 1)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps run on a handle of its own, not in a batch");
   if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps with a moving demag window");
+  for (int l = 0; l < h->nl; ++l)
+    if (h->L[l].llb) return set_err(errp, MRM_ERR_UNSUPPORTED, "adaptive steps with the LLB integrator");
   int rc = plain_prepare(h, 0, h->dt, llg_type);
   if (rc) return rc;
   const size_t re = relem(h->g.precision), n = (size_t)h->g.nx * h->g.ny;

@@ -71,6 +71,8 @@ class _RunMixin:
                 self.set_head_field(l, **lay.head)
             if getattr(lay, "field_table", None):
                 self.set_field_table(l, **lay.field_table)
+            if getattr(lay, "llb", None):
+                self.set_llb(l, **lay.llb)
             if getattr(lay, "cubic_axis", None) is not None:
                 self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
@@ -144,6 +146,26 @@ class _RunMixin:
         self._check(L.mrm_gpu_set_field_table(self.h, layer, xp.size, yp.size, fptr(xp), fptr(yp), fptr(v),
                                               float(vel[0]), float(vel[1]), off[0], off[1], float(ref[0]),
                                               float(ref[1]), float(t_origin)))
+
+    def set_llb(self, layer, spin, tc, lambda_ms):
+        """LLB integrator on `layer` (include/mrm_gpu.h mrm_gpu_set_llb): spin,
+        per-grain Curie temperature (K) and lambdaMs (Oe); tc None turns it off."""
+        L = _lib.load()
+        if tc is None:
+            self._check(L.mrm_gpu_set_llb(self.h, layer, 0.0, None, None))
+            return
+        t, lm = f64(tc), f64(lambda_ms)
+        self._check(L.mrm_gpu_set_llb(self.h, layer, float(spin), fptr(t), fptr(lm)))
+
+    def set_mag(self, layer: int, mag):
+        """The LLB magnitude |m| per grain."""
+        a = f64(mag)
+        self._check(_lib.load().mrm_gpu_set_mag(self.h, layer, fptr(a)))
+
+    def get_mag(self, layer: int) -> np.ndarray:
+        out = np.zeros(self.medium.layers[layer].N)
+        self._check(_lib.load().mrm_gpu_get_mag(self.h, layer, fptr(out)))
+        return out
 
     def set_window(self, nx_win: int, ny_win: int, v=(0.0, 0.0), offset=(0.0, 0.0)):
         """Moving demag window (include/mrm_gpu.h mrm_gpu_set_window); the tensor

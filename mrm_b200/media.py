@@ -85,6 +85,9 @@ class Layer:
     # the layer's time scale: dict(xpos, ypos, vfld (ny_tab, nx_tab, 3), vel,
     # offset, ref, t_origin) (include/mrm_gpu.h mrm_gpu_set_field_table)
     field_table: Optional[dict] = None
+    # LLB integrator (llgp%llb): dict(spin, tc (N,) K, lambda_ms (N,) Oe)
+    # (include/mrm_gpu.h mrm_gpu_set_llb)
+    llb: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -428,4 +431,27 @@ def table_write_medium(nx: int = 1024, ny: int = 256, *, seed: int = 1, temperat
                                ref=(0.0, 0.0), t_origin=0.0)
         lay.func, lay.amp, lay.fgamma, lay.param, lay.dc, lay.scale = 4, 1.0, 2.0 * tbit, rise_frac * tbit, 0.0, 1.0
         lay.phase, lay.duty, lay.moddepth = 0.0, 0.0, 0.0
+    return med
+
+
+def llb_medium(side: int = 32, *, temperature: float = 600.0, tc: float = 700.0, tc_sigma: float = 0.03,
+               spin: float = 0.5, seed: int = 1, boundary: int = 1, h_oe: float = 8000.0) -> Medium:
+    """A heat-assisted write of a single FePt-like layer with the LLB integrator:
+    the M(H) medium of mh_medium at a uniform temperature below a grain-to-grain
+    distributed Curie temperature (Tc ~ N(tc, tc_sigma tc)), spin S, and the
+    mean-field coupling of each grain's Tc, lambdaMs = 3 Tc / ((g mu_B/k_B)
+    (S + 1)) (the mean-field Tc of push_llb's Langevin form, lambda_m =
+    lambdaMs (S+1)/S, is (g mu_B/k_B) S lambda_m / 3), under a constant
+    reversing field of h_oe along the medium's field direction; the anisotropy
+    and Ms scales stay the inputs (Tc-free scaling)."""
+    med = mh_medium(side, seed=seed, boundary=boundary, temperature=temperature)
+    rng = np.random.default_rng(seed + 1000)
+    for lay in med.layers:
+        lay.thermal = True
+        lay.temperature = temperature
+        lay.t_start, lay.t_end = -1e22, 1e22
+        lay.s_start = lay.s_end = 1.0
+        lay.scale = -h_oe
+        tcs = np.clip(rng.normal(tc, tc_sigma * tc, lay.N), temperature * 1.02, None)
+        lay.llb = dict(spin=spin, tc=tcs, lambda_ms=3.0 * tcs / (1.343427768e-4 * (spin + 1.0)))
     return med

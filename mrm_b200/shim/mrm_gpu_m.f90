@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -108,6 +108,25 @@ module mrm_gpu_m
       type(C_PTR), value :: h
       integer(C_INT), value :: layer
       real(C_DOUBLE), intent(in) :: cubic_axis(3, 3, *)
+    end function
+    integer(C_INT) function c_set_llb(h, layer, spin, tc, lambda_ms) bind(C, name="mrm_gpu_set_llb")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer
+      real(C_DOUBLE), value :: spin
+      real(C_DOUBLE), intent(in) :: tc(*), lambda_ms(*)
+    end function
+    integer(C_INT) function c_set_mag(h, layer, mag) bind(C, name="mrm_gpu_set_mag")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer
+      real(C_DOUBLE), intent(in) :: mag(*)
+    end function
+    integer(C_INT) function c_get_mag(h, layer, mag) bind(C, name="mrm_gpu_get_mag")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer
+      real(C_DOUBLE), intent(out) :: mag(*)
     end function
     integer(C_INT) function c_set_window(h, nxw, nyw, vx, vy, ox, oy) bind(C, name="mrm_gpu_set_window")
       import :: C_INT, C_PTR, C_DOUBLE
@@ -286,6 +305,27 @@ contains
     integer, intent(in) :: layer
     real(C_DOUBLE), intent(in) :: cubic_axis(:, :, :)
     ok_p = ok(c_set_cubic_axes(h, int(layer - 1, C_INT), cubic_axis))
+  end function
+
+  ! llgp%llb on `layer`: layer(il)%spin, %tc(:), %lambdaMs(:) (include/mrm_gpu.h
+  ! mrm_gpu_set_llb); gpu_set_mag / gpu_get_mag carry layer(il)%mag(in/3+1,:)
+  logical function gpu_set_llb(h, layer, spin, tc, lambda_ms) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: spin, tc(:), lambda_ms(:)
+    ok_p = ok(c_set_llb(h, int(layer - 1, C_INT), spin, tc, lambda_ms))
+  end function
+  logical function gpu_set_mag(h, layer, mag) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: mag(:)
+    ok_p = ok(c_set_mag(h, int(layer - 1, C_INT), mag))
+  end function
+  logical function gpu_get_mag(h, layer, mag) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(out) :: mag(:)
+    ok_p = ok(c_get_mag(h, int(layer - 1, C_INT), mag))
   end function
 
   ! moving demag window nxfft x nyfft following window%v, window%offset

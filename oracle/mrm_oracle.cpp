@@ -459,6 +459,11 @@ struct Layer {
   // in the window, and the first and last of them (min_n, max_n, 0-based)
   std::vector<char> do_grain;
   int min_n = 0, max_n = -1;
+  // LLB integrator (llgp%llb, push_llb llg.f90:916-1064): spin, Tc and
+  // lambdaMs per grain, the magnitude |m| per buffer (data.f90:202: 1)
+  bool llb = false;
+  double spin = 1.0;
+  std::vector<double> tc, lam_ms, mag[2];
   std::vector<double> m[2], dm, h, hthm, hdemag, happ;
   // schedule: uniform field x linear ramp (applied.f90:863-883)
   double hdir[3] = {0, 0, 0};
@@ -810,7 +815,10 @@ static void get_thermal(Sim* s) {
     for (int n = 0; n < Ly.N; ++n) {
       if (!Ly.do_grain[n]) continue;
       double x = 0.0;
-      if (Ly.ms_scale[n] > 0.0)
+      if (Ly.mag[s->in][n] != 1.0)  // field.f90:416-417
+        x = Ly.alpha_scale[n] * Ly.temperature /
+            (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, std::abs(Ly.mag[s->in][n])));
+      else if (Ly.ms_scale[n] > 0.0)
         x = Ly.alpha_scale[n] * Ly.temperature /
             (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, Ly.ms_scale[n]));
       x = std::sqrt(x) * tsigma;
@@ -831,6 +839,197 @@ static inline void cross(const double* a, const double* b, double* c) {
   c[0] = a[1] * b[2] - a[2] * b[1];
   c[1] = a[2] * b[0] - a[0] * b[2];
   c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// lv(x) = coth(x) - 1/x and its derivative (llg.f90:704-710,727-733)
+static double lv(double x) { return std::abs(x) > 1e-2 ? 1.0 / std::tanh(x) - 1.0 / x : x / 3.0; }
+static double dlv(double x) {
+  if (std::abs(x) > 4e-3) {
+    const double b = std::sinh(x);
+    return 1.0 / (x * x) - 1.0 / (b * b);
+  }
+  return 1.0 / 3.0;
+}
+
+// push_llb (llg.f90:916-1064): the semi-implicit (|type| = 2, :935-999) and
+// Heun (:1000-1047) branches and the |m| = 0 branch (:1048-1060), for one
+// layer; iter 2: the first pass of a two-pass push, 1: the last (or only).
+static void push_llb(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l, double* errmx1_l,
+                     double* mmag1) {
+  Layer& Ly = s->L[l];
+  const int id = s->in;
+  const double gmub_kb = 1.343427768e-4;  // llg.f90:924
+  const double scale1 = -0.5 * Ly.gamma * dt;
+  const double T = Ly.temperature;
+  double em = 0.0, em1 = 0.0, mm = 0.0;
+#pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
+  for (int n = 0; n < Ly.N; ++n) {
+    if (n < Ly.min_n || n > Ly.max_n) continue;
+    double* mnext = &Ly.m[1 - id][3 * n];
+    const double* mcur = &Ly.m[id][3 * n];
+    double& magn = Ly.mag[1 - id][n];
+    const double magc = Ly.mag[id][n];
+    const double* hn = &Ly.h[3 * n];
+    if (!Ly.do_grain[n]) {  // llg.f90:1061-1064 (the magnitude kept too)
+      for (int a = 0; a < 3; ++a) {
+        mnext[a] = mcur[a];
+        Ly.dm[3 * n + a] = 0.0;
+      }
+      magn = magc;
+      mm += magn * Ly.vol[n];
+      continue;
+    }
+    const double lambdam = Ly.lam_ms[n] * (Ly.spin + 1.0) / Ly.spin;  // :931
+    const double tc = Ly.tc[n];
+    if (magc > 0.0 && std::abs(type) < 3) {
+      // semi-implicit push of direction and magnitude (:935-999)
+      const double scale11 = scale1;
+      double m[3], mag, htot[3], mhtot, meq;
+      auto tot = [&](const double* mm, double mg) {
+        for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mg * mm[a];
+        mhtot = std::sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+        if (mhtot != 0.0)
+          for (int a = 0; a < 3; ++a) htot[a] /= mhtot;
+        meq = gmub_kb * Ly.spin * mhtot / T;
+      };
+      if (iter == 2 || type > 0) {
+        for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+        mag = magc;
+        tot(m, mag);
+        mag = lv(meq) * (m[0] * htot[0] + m[1] * htot[1] + m[2] * htot[2]);
+        mag = mag + (magc - mag) * std::exp(scale1 * 2.0 * Ly.alpha * lambdam * lambdam * T * T * lv(meq) /
+                                            (3.0 * tc * tc * dlv(meq) * (mhtot + 1e-20)));
+      } else {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+      }
+      tot(m, mag);
+      const double aperp = Ly.alpha * (1.0 - lambdam * lv(meq) * T / (3.0 * mhtot * tc));
+      const double apar = Ly.alpha * 2.0 * T / (3.0 * tc);
+      const double scale2 = -aperp / (std::abs(mag) + 1e-20);
+      double h[3], t[3], o[3], mo[3], tt[3], d[3];
+      const double fh = std::sqrt(std::abs(scale2 / (Ly.alpha * Ly.alpha_scale[n] * dt0 * (std::abs(mag) + 1e-20))));
+      for (int a = 0; a < 3; ++a) h[a] = hn[a] + Ly.hthm[3 * n + a] * fh;
+      for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+      cross(m, h, t);
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      const double ms2 = Ly.ms[n] * Ly.ms[n];
+      if (y2 > em * ms2) em = y2 / ms2;
+      for (int a = 0; a < 3; ++a) o[a] = scale11 * h[a] + scale2 * m[a];
+      cross(m, o, mo);
+      for (int a = 0; a < 3; ++a) tt[a] = m[a] + mo[a];
+      const double yy = 2.0 / (1.0 + o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+      cross(tt, o, d);
+      for (int a = 0; a < 3; ++a) {
+        d[a] *= yy;
+        mnext[a] = m[a] + d[a];
+      }
+      double mm2[3];
+      for (int a = 0; a < 3; ++a) mm2[a] = m[a] + 0.5 * d[a];
+      tot(mm2, mag);
+      const double sg = std::copysign(1.0, mag);
+      mag = lv(meq) * (sg * mm2[0] * htot[0] + sg * mm2[1] * htot[1] + sg * mm2[2] * htot[2]);
+      double q = mag + (magc - mag) * std::exp(scale1 * 4.0 * Ly.alpha * lambdam * lambdam * T * T * lv(meq) /
+                                               (3.0 * tc * tc * dlv(meq) * (mhtot + 1e-20)));
+      const double fp = std::sqrt(std::abs(apar / (Ly.alpha * Ly.alpha_scale[n] * dt0)));
+      q = q - 2.0 * scale11 * (Ly.hthm[3 * n] * fp * mm2[0] + Ly.hthm[3 * n + 1] * fp * mm2[1] +
+                               Ly.hthm[3 * n + 2] * fp * mm2[2]);
+      magn = std::abs(q);
+      if (q < 0.0) {
+        const double r = std::sqrt(mm2[0] * mm2[0] + mm2[1] * mm2[1] + mm2[2] * mm2[2]);
+        for (int a = 0; a < 3; ++a) {
+          mnext[a] = -mm2[a] / r;
+          d[a] = mnext[a] - m[a];
+        }
+      }
+      const double ya = 0.5 * (magn + magc);
+      double e[3];
+      for (int a = 0; a < 3; ++a) e[a] = d[a] * ya + m[a] * (magn - magc);
+      em1 = std::max(em1, e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+    } else if (magc > 0.0) {
+      double m[3], mag;
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+        if (mag <= 0.0) {
+          mag = 0.0;
+          const double y = std::sqrt(hn[0] * hn[0] + hn[1] * hn[1] + hn[2] * hn[2]);
+          if (y != 0.0)
+            for (int a = 0; a < 3; ++a) m[a] = hn[a] / y;
+        }
+      } else {
+        for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+        mag = magc;
+      }
+      double htot[3];
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mag * m[a];
+      const double mhtot = std::sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+      if (mhtot != 0.0)
+        for (int a = 0; a < 3; ++a) htot[a] /= mhtot;
+      double meq = gmub_kb * Ly.spin * mhtot / T;
+      const double aperp = Ly.alpha * (1.0 - lambdam * lv(meq) * T / (3.0 * mhtot * tc));
+      const double apar = Ly.alpha * 2.0 * T / (3.0 * tc);
+      double h[3], hpar[3], hperp[3];
+      const double rt = std::sqrt(Ly.alpha * Ly.alpha_scale[n] * dt0);
+      for (int a = 0; a < 3; ++a) h[a] = Ly.hthm[3 * n + a] / rt;
+      const double hm = h[0] * m[0] + h[1] * m[1] + h[2] * m[2];
+      for (int a = 0; a < 3; ++a) {
+        hpar[a] = hm * m[a];
+        hperp[a] = h[a] - hpar[a];
+      }
+      const double fpar = std::sqrt(apar), fperp = std::sqrt(std::max(0.0, aperp - apar) / (aperp * aperp));
+      for (int a = 0; a < 3; ++a) {
+        hpar[a] *= fpar;
+        hperp[a] *= fperp;
+      }
+      const double scale11 = 2.0 * scale1;  // (type -3: no rescaling, :1029)
+      const double mht = m[0] * htot[0] + m[1] * htot[1] + m[2] * htot[2];
+      meq = apar * (lambdam / mhtot) * lambdam * 2.0 * scale1 * T * lv(meq) / (3.0 * dlv(meq) * tc) *
+            (mag - lv(meq) * mht);
+      double hh[3] = {hn[0] + hperp[0], hn[1] + hperp[1], hn[2] + hperp[2]}, t[3], mh[3], mt[3], d[3];
+      cross(m, hh, t);
+      cross(m, hn, mh);
+      cross(m, t, mt);
+      const double sg = std::copysign(std::min(0.5, std::abs(meq)), meq);
+      for (int a = 0; a < 3; ++a) d[a] = scale11 * (mag * mh[a] + aperp * mt[a] + hpar[a]) + sg * m[a];
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) d[a] = 0.5 * (d[a] + Ly.dm[3 * n + a]);
+      } else {
+        for (int a = 0; a < 3; ++a) Ly.dm[3 * n + a] = d[a];
+      }
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      const double ms2 = Ly.ms[n] * Ly.ms[n];
+      if (y2 > em * ms2) em = y2 / ms2;
+      em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      double o[3];
+      for (int a = 0; a < 3; ++a) o[a] = mcur[a] * magc + d[a];
+      double y = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+      if (y > 0.0) {
+        for (int a = 0; a < 3; ++a) mnext[a] = o[a] / y;
+      } else {
+        y = 0.0;
+        for (int a = 0; a < 3; ++a) mnext[a] = -mcur[a];
+      }
+      magn = y;
+    } else {
+      const double y = std::sqrt(hn[0] * hn[0] + hn[1] * hn[1] + hn[2] * hn[2]);
+      if (y > 0.0) {
+        for (int a = 0; a < 3; ++a) mnext[a] = hn[a] / y;
+        const double scale11 = 2.0 * scale1;
+        const double meq = gmub_kb * Ly.spin * y / T;
+        const double scale2 = lambdam * T / (3.0 * dlv(meq) * tc);
+        magn = (y / scale2 + lv(meq)) * (1.0 - std::exp(scale11 * scale2 * 2.0 * T * Ly.alpha / (3.0 * tc)));
+      } else {
+        for (int a = 0; a < 3; ++a) mnext[a] = mcur[a];
+        magn = magc;
+      }
+      em1 = std::max(em1, (magn - magc) * (magn - magc));
+    }
+    mm += magn * Ly.vol[n];
+  }
+  *errmx_l = em;
+  *errmx1_l = em1;
+  *mmag1 = mm;
 }
 
 // push_llg (llg.f90:1066-1155): one stage for one layer.
@@ -988,7 +1187,10 @@ static void push_passes(Sim* s, double dt, int type, double* errmx, double* errm
     *errmx = 0; *errmx1 = 0; *mmag = 0;
     for (int l = 0; l < nl; ++l) {
       double e0, e1, m1;
-      push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
+      if (s->L[l].llb)
+        push_llb(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
+      else
+        push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
       double vs = 0;  // sum(grain_vol, mask=do_grain), llg.f90:1239
       for (int n = 0; n < s->L[l].N; ++n)
         if (s->L[l].do_grain[n]) vs += s->L[l].vol[n];
@@ -1337,6 +1539,9 @@ int orc_upload_layer(void* h, int l, int N, const double* ms, const double* vol,
   Ly.do_grain.assign(N, 1);
   Ly.min_n = 0;
   Ly.max_n = N - 1;
+  Ly.mag[0].assign(N, 1.0);
+  Ly.mag[1].assign(N, 1.0);
+  Ly.llb = false;
   return 0;
 }
 
@@ -1452,6 +1657,37 @@ int orc_set_state(void* h, int l, const double* m) {
   Layer& Ly = s->L[l];
   std::memcpy(Ly.m[s->in].data(), m, sizeof(double) * 3 * Ly.N);
   std::memcpy(Ly.m[1 - s->in].data(), m, sizeof(double) * 3 * Ly.N);
+  Ly.mag[0].assign(Ly.N, 1.0);  // a new state starts at |m| = 1 (data.f90:202)
+  Ly.mag[1].assign(Ly.N, 1.0);
+  return 0;
+}
+
+// LLB on layer l (mrm_gpu_set_llb's arguments; tc NULL: off)
+int orc_set_llb(void* h, int l, double spin, const double* tc, const double* lam_ms) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.llb = tc != nullptr;
+  if (!tc) return 0;
+  Ly.spin = spin;
+  Ly.tc.assign(tc, tc + Ly.N);
+  Ly.lam_ms.assign(lam_ms, lam_ms + Ly.N);
+  return 0;
+}
+
+int orc_set_mag(void* h, int l, const double* mag) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.mag[s->in].assign(mag, mag + Ly.N);
+  Ly.mag[1 - s->in].assign(mag, mag + Ly.N);
+  return 0;
+}
+
+int orc_get_mag(void* h, int l, double* mag) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  std::memcpy(mag, s->L[l].mag[s->in].data(), sizeof(double) * s->L[l].N);
   return 0;
 }
 

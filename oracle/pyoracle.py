@@ -57,6 +57,9 @@ def lib():
         L.orc_set_cubic_axes.argtypes = [vp, i, P(d)]
         L.orc_set_field_table.argtypes = [vp, i, i, i, P(d), P(d), P(d), d, d, d, d, d, d, d]
         L.orc_set_window.argtypes = [vp, i, i, d, d, d, d]
+        L.orc_set_llb.argtypes = [vp, i, d, P(d), P(d)]
+        L.orc_set_mag.argtypes = [vp, i, P(d)]
+        L.orc_get_mag.argtypes = [vp, i, P(d)]
         L.orc_get_window.argtypes = [vp, P(i)]
         L.orc_set_state.argtypes = [vp, i, P(d)]
         L.orc_get_state.argtypes = [vp, i, P(d)]
@@ -223,6 +226,9 @@ class OracleSim:
             tb = getattr(lay, "field_table", None)
             if tb:
                 self.set_field_table(l, **tb)
+            lb = getattr(lay, "llb", None)
+            if lb:
+                self.set_llb(l, **lb)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
             cub = getattr(lay, "cubic_axis", None)
             if cub is not None:
@@ -285,6 +291,24 @@ class OracleSim:
         n = self.medium.layers[layer].N
         out = np.zeros((n, 3))
         lib().orc_get_demag(self.h, layer, _p(out))
+        return out
+
+    def set_llb(self, layer, spin, tc, lambda_ms):
+        """LLB integrator on `layer` (GpuSim.set_llb's arguments; tc None: off)."""
+        if tc is None:
+            assert lib().orc_set_llb(self.h, layer, 0.0, None, None) == 0
+            return
+        t, lm = f64(tc), f64(lambda_ms)
+        self._keep += [t, lm]
+        assert lib().orc_set_llb(self.h, layer, float(spin), _p(t), _p(lm)) == 0
+
+    def set_mag(self, layer, mag):
+        a = f64(mag)
+        assert lib().orc_set_mag(self.h, layer, _p(a)) == 0
+
+    def get_mag(self, layer):
+        out = np.zeros(self.medium.layers[layer].N)
+        lib().orc_get_mag(self.h, layer, _p(out))
         return out
 
     def get_window(self):
