@@ -49,9 +49,11 @@ def test_llb_semi_implicit_fp64(oracle, gpulib, llg_type):
 
 
 def test_llb_trajectory_fp32(oracle, gpulib):
-    # the LLB push runs in FP64 arithmetic on FP32 state: the state's rounding
-    # (1e-7) grows through the thermal trajectory
+    # the LLB push runs in FP64 arithmetic on FP32 state; FP32 runs draw their
+    # noise from the 32-bit Philox stream, so the comparison runs without noise
+    # (T = 600 K still sets the longitudinal physics)
     med = media.llb_medium(16, seed=4)
+    med.layers[0].thermal = False
     orc, gpu = _pair(oracle, med, FP32)
     orc.step(500, 1e-14)
     gpu.step(500, 1e-14)
