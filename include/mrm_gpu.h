@@ -201,6 +201,14 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
  * the layer's upload (an upload clears it).  mrm_gpu_set_mag / _get_mag: |m|
  * per grain (layer%mag(in, :)). */
 int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms);
+/* MT integrator (llgp%mt: push_mt, llg.f90:735-915, dm/dt = -gamma m x H -
+ * (m - m_eq)/tau + eta, with |m| per grain as for LLB): spin S, per grain
+ * lambdaMs (Oe), the equilibrium from the Brillouin function B_S (meq_bs = 1,
+ * the mean field lambdaMs) or the Langevin function (meq_bs = 0, lambdaMs
+ * (S+1)/S), tau from Xu & Zhang (garanin_tau = 0) or Garanin (1); Heun and the
+ * semi-implicit |type| = 2 branch (llg_type -3, 2, -2); the same switch, checks
+ * and magnitude accessors as the LLB integrator.  lambda_ms = NULL: off. */
+int mrm_gpu_set_mt(mrm_gpu* h, int layer, double spin, const double* lambda_ms, int meq_bs, int garanin_tau);
 int mrm_gpu_set_mag(mrm_gpu* h, int layer, const double* mag);
 int mrm_gpu_get_mag(mrm_gpu* h, int layer, double* mag);
 

@@ -344,6 +344,137 @@ MRM_D LlbStep llb_boris(bool first, const double* mc, double magc, const double*
   return o;
 }
 
+// Brillouin function B_S and its derivative as bs / dbs write them (llg.f90:390-408)
+MRM_D double mt_bs(double x, double sp) {
+  double b = x / (2.0 * sp);
+  if (b != 0.0) b = ((2.0 * sp + 1.0) / tanh((2.0 * sp + 1.0) * b) - 1.0 / tanh(b)) / (2.0 * sp);
+  return b;
+}
+MRM_D double mt_dbs(double x, double sp) {
+  double b = (1.0 + sp) / (3.0 * sp);
+  if (x != 0.0) {
+    b = x / (2.0 * sp);
+    const double b1 = sinh(b);
+    b = sinh(x + b);
+    b = (1.0 / (b1 * b1) - (1.0 + 2.0 * sp) * (1.0 + 2.0 * sp) / (b * b)) / (4.0 * sp * sp);
+  }
+  return b;
+}
+
+// One grain of push_mt (llg.f90:735-915), dm/dt = -gamma m x H - (m - meq)/tau + eta:
+// the Heun branch (:843-906; corr: the second pass) or the semi-implicit
+// |type| = 2 branch (:757-842; first: the first or only pass).  mc, magc: the
+// current state; mpr, magp: the predicted (second pass); h the field without
+// thermal; ht the thermal field / sqrt(dt); d1 the first pass's increment
+// (Heun); ab = alpha alpha_scale; lam = lambdaMs; T the temperature; dt the
+// pass's step.  Out as llb_heun.
+MRM_D LlbStep mt_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr, double magp,
+                      const double* h, const double* ht, const double* d1, double ab, double lam0, const LlbDev& P,
+                      double T, double gamma, double dt, double dt0) {
+  LlbStep o;
+  const double sp = P.spin;
+  const double lam = P.meq_bs ? lam0 : lam0 * (sp + 1.0) / sp;
+  const double y0 = kGmubKb * sp / T;
+  const double scale1 = -0.5 * gamma * dt, scale11 = 2.0 * scale1;
+  const double hth[3] = {ht[0] * sqrt(dt0), ht[1] * sqrt(dt0), ht[2] * sqrt(dt0)};  // hthm
+  double m[3], mag, htot[3], mhtot;
+  auto tot = [&](const double* v, double mg) {  // htot = h + lam mg v, normalised
+    for (int c = 0; c < 3; ++c) htot[c] = h[c] + lam * mg * v[c];
+    mhtot = sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+    if (mhtot != 0.0)
+      for (int c = 0; c < 3; ++c) htot[c] /= mhtot;
+  };
+  // eta, the stochastic increment with its parallel part scaled (:820-826, :874-884)
+  auto noise = [&](double meq, double sig_p, double sig_l, double* eta) {
+    double e[3];
+    for (int c = 0; c < 3; ++c)
+      e[c] = P.garanin_tau ? dt * hth[c] * gamma * sig_p * sqrt(2.0 / ((sig_l + (boris ? 1e-80 : 1e-22)) * dt0))
+                           : dt * hth[c] * gamma * sqrt(lam * meq / ((mhtot + (boris ? 1e-80 : 1e-22)) * dt0));
+    const double pe = htot[0] * e[0] + htot[1] * e[1] + htot[2] * e[2], r = sqrt(sig_l / sig_p);
+    double x1[3], x2[3];
+    cross3(htot[0], htot[1], htot[2], e[0], e[1], e[2], x1[0], x1[1], x1[2]);
+    cross3(htot[0], htot[1], htot[2], x1[0], x1[1], x1[2], x2[0], x2[1], x2[2]);
+    for (int c = 0; c < 3; ++c) eta[c] = r * pe * htot[c] - x2[c];
+  };
+  double d[3], t[3], eta[3];
+  if (boris) {
+    for (int c = 0; c < 3; ++c) m[c] = first ? mc[c] : mpr[c];
+    mag = first ? magc : magp;
+    tot(m, mag);
+    const double yh = y0 * mhtot;
+    double meq = P.meq_bs ? mt_bs(yh, sp) : llb_lv(yh);
+    double scale2;
+    if (P.garanin_tau) {
+      const double sg = meq / (yh * (P.meq_bs ? mt_dbs(yh, sp) : llb_dlv(yh)) + 1e-80);
+      scale2 = 2.0 * ab * sg / y0;
+    } else {
+      scale2 = ab * lam;
+    }
+    for (int c = 0; c < 3; ++c) m[c] = mc[c];
+    mag = magc;
+    cross3(m[0], m[1], m[2], h[0], h[1], h[2], t[0], t[1], t[2]);
+    o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+    const double dec = 1.0 - exp(scale1 * scale2);
+    double w[3], x[3];
+    for (int c = 0; c < 3; ++c) d[c] = (meq * htot[c] - mag * m[c]) * dec;  // half decay (:802)
+    for (int c = 0; c < 3; ++c) w[c] = mag * m[c] + d[c];
+    cross3(w[0], w[1], w[2], h[0], h[1], h[2], x[0], x[1], x[2]);
+    for (int c = 0; c < 3; ++c) d[c] += scale11 * x[c];  // full rotation (:803)
+    for (int c = 0; c < 3; ++c) w[c] = mag * m[c] + d[c];
+    for (int c = 0; c < 3; ++c) htot[c] = h[c] + lam * w[c];
+    mhtot = sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+    if (mhtot != 0.0)
+      for (int c = 0; c < 3; ++c) htot[c] /= mhtot;
+    const double y2 = y0 * mhtot;
+    meq = P.meq_bs ? mt_bs(y2, sp) : llb_lv(y2);
+    const double sig_p = meq / (y2 + 1e-80), sig_l = P.meq_bs ? mt_dbs(y2, sp) : llb_dlv(y2);
+    if (P.garanin_tau) scale2 = 2.0 * ab * sig_p / (y0 * (sig_l + 1e-80));
+    noise(meq, sig_p, sig_l, eta);
+    const double dec2 = 1.0 - exp(scale1 * scale2);
+    for (int c = 0; c < 3; ++c) d[c] = d[c] + (meq * htot[c] - w[c]) * dec2 + eta[c];  // :833
+  } else {
+    for (int c = 0; c < 3; ++c) m[c] = mc[c];
+    mag = magc;
+    if (corr) {  // :844-847
+      for (int c = 0; c < 3; ++c) m[c] = mpr[c];
+      mag = magp;
+      if (mag <= 0.0) {
+        mag = 0.0;
+        const double e = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+        if (e != 0.0)
+          for (int c = 0; c < 3; ++c) m[c] = h[c] / e;
+      }
+    }
+    tot(m, mag);
+    const double y = y0 * mhtot;
+    const double meq = P.meq_bs ? mt_bs(y, sp) : llb_lv(y);
+    const double sig_l = P.meq_bs ? mt_dbs(y, sp) : llb_dlv(y), sig_p = meq / (y + 1e-22);
+    noise(meq, sig_p, sig_l, eta);
+    const double scale2 = P.garanin_tau ? 2.0 * T * sig_p / (kGmubKb * sp * (sig_l + 1e-22)) : lam;
+    double mm[3], x[3];
+    for (int c = 0; c < 3; ++c) mm[c] = m[c] * mag;
+    cross3(mm[0], mm[1], mm[2], h[0], h[1], h[2], x[0], x[1], x[2]);
+    for (int c = 0; c < 3; ++c) d[c] = scale11 * (x[c] + (mm[c] - meq * htot[c]) * scale2 * ab) + eta[c];
+    if (corr)
+      for (int c = 0; c < 3; ++c) d[c] = 0.5 * (d[c] + d1[c]);
+    cross3(m[0], m[1], m[2], h[0], h[1], h[2], t[0], t[1], t[2]);
+    o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+  }
+  for (int c = 0; c < 3; ++c) o.d[c] = d[c];
+  o.d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  double w[3];
+  for (int c = 0; c < 3; ++c) w[c] = mc[c] * magc + d[c];
+  const double e = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (e > 0.0) {
+    for (int c = 0; c < 3; ++c) o.m[c] = w[c] / e;
+    o.mag = e;
+  } else {
+    for (int c = 0; c < 3; ++c) o.m[c] = -mc[c];
+    o.mag = 0.0;
+  }
+  return o;
+}
+
 // shared memory of a row block's table weights (grid columns, then the
 // block's rows; at most 8 rows per block)
 MRM_HD int field_table_bytes(int nx) { return (nx + 8) * (int)sizeof(TabW); }
@@ -929,9 +1060,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         d1[1] = dd.y;
         d1[2] = dd.z;
       }
-      // (semi-implicit: push_llb's |type| = 2 branch, its first pass over dt/2 for -2)
+      // (semi-implicit: push_llb's |type| = 2 branch, its first pass over dt/2 for -2;
+      // mode 1: push_mt)
+      const double pdt = (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt;
       const LlbStep st =
-          (boris && (double)m0.w > 0.0)
+          P.mode == 1
+              ? mt_step(boris, STAGE == kPred, STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1,
+                        (double)pb.z, gp.y, P, L.temperature, L.gamma, pdt, rd.dt)
+          : (boris && (double)m0.w > 0.0)
               ? llb_boris(STAGE == kPred, mc, (double)m0.w, mpr, (double)mf.w, hh, th, (double)pb.z, gp.x, gp.y, P,
                           L.temperature, L.gamma, (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt)
               : llb_heun(STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1, (double)pb.z, gp.x, gp.y, P,

@@ -2116,7 +2116,19 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
   return MRM_OK;
 }
 
+static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms, int mode,
+                        int meq_bs, int garanin_tau);
+
 int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms) {
+  return set_llb_mode(h, layer, spin, tc, lambda_ms, 0, 0, 0);
+}
+
+int mrm_gpu_set_mt(mrm_gpu* h, int layer, double spin, const double* lambda_ms, int meq_bs, int garanin_tau) {
+  return set_llb_mode(h, layer, spin, lambda_ms, lambda_ms, 1, meq_bs, garanin_tau);
+}
+
+static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms, int mode,
+                        int meq_bs, int garanin_tau) {
   if (!h) return MRM_ERR_ARG;
   if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
   std::string* errp = &h->err;
@@ -2132,8 +2144,9 @@ int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const 
   if (!lambda_ms || !(spin > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs spin > 0, Tc and lambdaMs");
   const HostLayerCache& hc = host_cache()[h][layer];
   const int ng = b.ng, nc = b.n;
-  for (int g = 0; g < ng; ++g)
-    if (!(tc[g] > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs Tc > 0 (grain %d)", g);
+  if (mode == 0)
+    for (int g = 0; g < ng; ++g)
+      if (!(tc[g] > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs Tc > 0 (grain %d)", g);
   // per cell: Tc, lambda_m = lambdaMs (spin+1)/spin (llg.f90:931), and
   // get_thermal's 2 k_B alpha alpha_scale / (gamma Ms V) (field.f90:407,417)
   std::vector<V4<double>> rec(nc, V4<double>{1.0, 0.0, 0.0, 0.0});
@@ -2141,8 +2154,9 @@ int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const 
     const int g = hc.cgrain.empty() ? c : hc.cgrain[c];
     if (g < 0) continue;
     const double msv = hc.ms[g] * hc.vol[g];
-    rec[c].x = tc[g];
-    rec[c].y = lambda_ms[g] * (spin + 1.0) / spin;
+    rec[c].x = mode == 0 ? tc[g] : 0.0;
+    // LLB: lambda_m = lambdaMs (S+1)/S; MT: lambdaMs (push_mt scales it by meq_bs)
+    rec[c].y = mode == 0 ? lambda_ms[g] * (spin + 1.0) / spin : lambda_ms[g];
     rec[c].z = msv > 0 ? 2.0 * kBoltz * b.alpha * hc.alpha_scale[g] / (b.gamma * msv) : 0.0;
   }
   LlbDev d{};
@@ -2156,6 +2170,9 @@ int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const 
   d.spin = spin;
   d.alpha = b.alpha;
   d.floor_ms = b.floor_ms;
+  d.mode = mode;
+  d.meq_bs = meq_bs ? 1 : 0;
+  d.garanin_tau = garanin_tau ? 1 : 0;
   CK(cudaMemcpy(b.llbp, rec.data(), sizeof(V4<double>) * (size_t)nc, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b.llb, &d, sizeof(LlbDev), cudaMemcpyHostToDevice));
   return MRM_OK;

@@ -73,6 +73,8 @@ class _RunMixin:
                 self.set_field_table(l, **lay.field_table)
             if getattr(lay, "llb", None):
                 self.set_llb(l, **lay.llb)
+            if getattr(lay, "mt", None):
+                self.set_mt(l, **lay.mt)
             if getattr(lay, "cubic_axis", None) is not None:
                 self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
@@ -156,6 +158,17 @@ class _RunMixin:
             return
         t, lm = f64(tc), f64(lambda_ms)
         self._check(L.mrm_gpu_set_llb(self.h, layer, float(spin), fptr(t), fptr(lm)))
+
+    def set_mt(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False):
+        """MT integrator on `layer` (include/mrm_gpu.h mrm_gpu_set_mt); lambda_ms
+        None turns it off."""
+        L = _lib.load()
+        if lambda_ms is None:
+            self._check(L.mrm_gpu_set_mt(self.h, layer, 0.0, None, 0, 0))
+            return
+        lm = f64(lambda_ms)
+        self._check(L.mrm_gpu_set_mt(self.h, layer, float(spin), fptr(lm), int(bool(meq_bs)),
+                                     int(bool(garanin_tau))))
 
     def set_mag(self, layer: int, mag):
         """The LLB magnitude |m| per grain."""

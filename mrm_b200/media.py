@@ -88,6 +88,9 @@ class Layer:
     # LLB integrator (llgp%llb): dict(spin, tc (N,) K, lambda_ms (N,) Oe)
     # (include/mrm_gpu.h mrm_gpu_set_llb)
     llb: Optional[dict] = None
+    # MT integrator (llgp%mt): dict(spin, lambda_ms (N,) Oe, meq_bs, garanin_tau)
+    # (include/mrm_gpu.h mrm_gpu_set_mt)
+    mt: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -454,4 +457,19 @@ def llb_medium(side: int = 32, *, temperature: float = 600.0, tc: float = 700.0,
         lay.scale = -h_oe
         tcs = np.clip(rng.normal(tc, tc_sigma * tc, lay.N), temperature * 1.02, None)
         lay.llb = dict(spin=spin, tc=tcs, lambda_ms=3.0 * tcs / (1.343427768e-4 * (spin + 1.0)))
+    return med
+
+
+def mt_medium(side: int = 32, *, meq_bs: bool = False, garanin_tau: bool = False, **kw) -> Medium:
+    """llb_medium's heat-assisted layer driven by the MT integrator instead:
+    the same spin and mean-field coupling (lambdaMs from each grain's Tc, as
+    the Brillouin (meq_bs) or Langevin mean field of push_mt fixes Tc)."""
+    med = llb_medium(side, **kw)
+    for lay in med.layers:
+        lb = lay.llb
+        sp = lb["spin"]
+        # mean-field Tc: B_S'(0) = (S+1)/(3S), so lambdaMs = 3 Tc/((g mu_B/k_B)(S+1))
+        # for B_S; the Langevin form takes the same lambdaMs through lambda_m (S+1)/S
+        lay.mt = dict(spin=sp, lambda_ms=lb["lambda_ms"], meq_bs=meq_bs, garanin_tau=garanin_tau)
+        lay.llb = None
     return med

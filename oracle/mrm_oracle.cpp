@@ -462,6 +462,7 @@ struct Layer {
   // LLB integrator (llgp%llb, push_llb llg.f90:916-1064): spin, Tc and
   // lambdaMs per grain, the magnitude |m| per buffer (data.f90:202: 1)
   bool llb = false;
+  int mode = 0, meq_bs = 0, garanin_tau = 0;  // mode 1: push_mt (llgp%mt)
   double spin = 1.0;
   std::vector<double> tc, lam_ms, mag[2];
   std::vector<double> m[2], dm, h, hthm, hdemag, happ;
@@ -1032,6 +1033,182 @@ static void push_llb(Sim* s, int l, int type, int iter, double dt, double dt0, d
   *mmag1 = mm;
 }
 
+// bs / dbs (llg.f90:390-408): Brillouin function and its derivative
+static double bs(double x, double sp) {
+  double b = x / (2.0 * sp);
+  if (b != 0.0) b = ((2.0 * sp + 1.0) / std::tanh((2.0 * sp + 1.0) * b) - 1.0 / std::tanh(b)) / (2.0 * sp);
+  return b;
+}
+static double dbs(double x, double sp) {
+  double b = (1.0 + sp) / (3.0 * sp);
+  if (x != 0.0) {
+    b = x / (2.0 * sp);
+    const double b1 = std::sinh(b);
+    b = std::sinh(x + b);
+    b = (1.0 / (b1 * b1) - (1.0 + 2.0 * sp) * (1.0 + 2.0 * sp) / (b * b)) / (4.0 * sp * sp);
+  }
+  return b;
+}
+
+// push_mt (llg.f90:735-915): the |type| = 2 explicit-rotation branch
+// (:757-842) and the Heun branch (:843-906), for one layer.
+static void push_mt(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l, double* errmx1_l,
+                    double* mmag1) {
+  Layer& Ly = s->L[l];
+  const int id = s->in;
+  const double gmub_kb = 1.343427768e-4;
+  const double scale1 = -0.5 * Ly.gamma * dt, scale11 = 2.0 * scale1;
+  const double T = Ly.temperature, sp = Ly.spin;
+  double em = 0.0, em1 = 0.0, mm = 0.0;
+#pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
+  for (int n = 0; n < Ly.N; ++n) {
+    if (n < Ly.min_n || n > Ly.max_n) continue;
+    double* mnext = &Ly.m[1 - id][3 * n];
+    const double* mcur = &Ly.m[id][3 * n];
+    double& magn = Ly.mag[1 - id][n];
+    double m[3] = {mcur[0], mcur[1], mcur[2]}, mag = Ly.mag[id][n];
+    if (!Ly.do_grain[n]) {
+      for (int a = 0; a < 3; ++a) {
+        mnext[a] = m[a];
+        Ly.dm[3 * n + a] = 0.0;
+      }
+      magn = mag;
+      mm += magn * Ly.vol[n];
+      continue;
+    }
+    double lambdam = Ly.lam_ms[n];
+    if (!Ly.meq_bs) lambdam = lambdam * (sp + 1.0) / sp;
+    double y = gmub_kb * sp / T;
+    const double* hn = &Ly.h[3 * n];
+    const double* th = &Ly.hthm[3 * n];
+    const double ab = Ly.alpha_scale[n] * Ly.alpha;
+    double htot[3], mhtot, meq, sig_p, sig_l, scale2, d[3], t[3], eta[3], o[3];
+    auto norm_tot = [&]() {
+      mhtot = std::sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+      if (mhtot != 0.0)
+        for (int a = 0; a < 3; ++a) htot[a] /= mhtot;
+    };
+    auto shape_eta = [&]() {  // eta = sqrt(sig_l/sig_p) (htot.eta) htot - htot x (htot x eta)
+      double x1[3], x2[3];
+      cross(htot, eta, x1);
+      cross(htot, x1, x2);
+      const double pe = htot[0] * eta[0] + htot[1] * eta[1] + htot[2] * eta[2];
+      for (int a = 0; a < 3; ++a) eta[a] = std::sqrt(sig_l / sig_p) * pe * htot[a] - x2[a];
+    };
+    if (std::abs(type) < 3) {
+      if (iter == 1 && type < 0) {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+      }
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mag * m[a];
+      norm_tot();
+      meq = Ly.meq_bs ? bs(y * mhtot, sp) : lv(y * mhtot);
+      if (Ly.garanin_tau) {
+        sig_p = Ly.meq_bs ? meq / (y * mhtot * dbs(y * mhtot, sp) + 1e-80) : meq / (y * mhtot * dlv(y * mhtot) + 1e-80);
+        scale2 = 2.0 * ab * sig_p / y;
+      } else {
+        scale2 = ab * lambdam;
+      }
+      if (iter == 1 && type < 0) {
+        for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+        mag = Ly.mag[id][n];
+      }
+      cross(m, hn, t);
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      if (y2 > em * Ly.ms[n] * Ly.ms[n]) em = y2 / (Ly.ms[n] * Ly.ms[n]);
+      // |type| = 2: explicit gyro-rotation and analytic decay (:801-803)
+      for (int a = 0; a < 3; ++a) d[a] = (meq * htot[a] - mag * m[a]) * (1.0 - std::exp(scale1 * scale2));
+      double w[3], r[3];
+      for (int a = 0; a < 3; ++a) w[a] = mag * m[a] + d[a];
+      cross(w, hn, r);
+      for (int a = 0; a < 3; ++a) d[a] = d[a] + scale11 * r[a];
+      for (int a = 0; a < 3; ++a) o[a] = mag * m[a] + d[a];
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * o[a];
+      norm_tot();
+      if (Ly.meq_bs) {
+        meq = bs(y * mhtot, sp);
+        sig_p = meq / (y * mhtot + 1e-80);
+        sig_l = dbs(y * mhtot, sp);
+      } else {
+        meq = lv(y * mhtot);
+        sig_p = meq / (y * mhtot + 1e-80);
+        sig_l = dlv(y * mhtot);
+      }
+      if (Ly.garanin_tau) {
+        for (int a = 0; a < 3; ++a)
+          eta[a] = dt * th[a] * Ly.gamma * sig_p * std::sqrt(2.0 / ((sig_l + 1e-80) * dt0));
+        scale2 = 2.0 * ab * sig_p / (y * (sig_l + 1e-80));
+      } else {
+        for (int a = 0; a < 3; ++a) eta[a] = dt * th[a] * Ly.gamma * std::sqrt(lambdam * meq / ((mhtot + 1e-80) * dt0));
+      }
+      shape_eta();
+      for (int a = 0; a < 3; ++a) d[a] = d[a] + (meq * htot[a] - o[a]) * (1.0 - std::exp(scale1 * scale2)) + eta[a];
+      em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    } else {
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+        if (mag <= 0.0) {
+          mag = 0.0;
+          const double e = std::sqrt(hn[0] * hn[0] + hn[1] * hn[1] + hn[2] * hn[2]);
+          if (e != 0.0)
+            for (int a = 0; a < 3; ++a) m[a] = hn[a] / e;
+        }
+      }
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mag * m[a];
+      norm_tot();
+      y = y * mhtot;
+      if (Ly.meq_bs) {
+        meq = bs(y, sp);
+        sig_l = dbs(y, sp);
+        sig_p = meq / (y + 1e-22);
+      } else {
+        meq = lv(y);
+        sig_l = dlv(y);
+        sig_p = meq / (y + 1e-22);
+      }
+      if (Ly.garanin_tau) {
+        for (int a = 0; a < 3; ++a)
+          eta[a] = dt * th[a] * Ly.gamma * sig_p * std::sqrt(2.0 / ((sig_l + 1e-22) * dt0));
+        shape_eta();
+        scale2 = 2.0 * T * sig_p / (gmub_kb * sp * (sig_l + 1e-22));
+      } else {
+        for (int a = 0; a < 3; ++a) eta[a] = dt * th[a] * Ly.gamma * std::sqrt(lambdam * meq / ((mhtot + 1e-22) * dt0));
+        shape_eta();
+        scale2 = lambdam;
+      }
+      double mmg[3], r[3];
+      for (int a = 0; a < 3; ++a) mmg[a] = m[a] * mag;
+      cross(mmg, hn, r);
+      for (int a = 0; a < 3; ++a) d[a] = scale11 * (r[a] + (mmg[a] - meq * htot[a]) * scale2 * ab) + eta[a];
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) d[a] = 0.5 * (d[a] + Ly.dm[3 * n + a]);
+      } else {
+        for (int a = 0; a < 3; ++a) Ly.dm[3 * n + a] = d[a];
+      }
+      cross(m, hn, t);
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      if (y2 > em * Ly.ms[n] * Ly.ms[n]) em = y2 / (Ly.ms[n] * Ly.ms[n]);
+      em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+      mag = Ly.mag[id][n];
+    }
+    for (int a = 0; a < 3; ++a) o[a] = m[a] * mag + d[a];
+    double e = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    if (e > 0.0) {
+      for (int a = 0; a < 3; ++a) mnext[a] = o[a] / e;
+    } else {
+      e = 0.0;
+      for (int a = 0; a < 3; ++a) mnext[a] = -m[a];
+    }
+    magn = e;
+    mm += magn * Ly.vol[n];
+  }
+  *errmx_l = em;
+  *errmx1_l = em1;
+  *mmag1 = mm;
+}
+
 // push_llg (llg.f90:1066-1155): one stage for one layer.
 // Heun (type -3) branch :1122-1139, Boris/semi-implicit (|type|=2) :1109-1118.
 static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l,
@@ -1187,7 +1364,9 @@ static void push_passes(Sim* s, double dt, int type, double* errmx, double* errm
     *errmx = 0; *errmx1 = 0; *mmag = 0;
     for (int l = 0; l < nl; ++l) {
       double e0, e1, m1;
-      if (s->L[l].llb)
+      if (s->L[l].llb && s->L[l].mode == 1)
+        push_mt(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
+      else if (s->L[l].llb)
         push_llb(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
       else
         push_llg(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
@@ -1662,12 +1841,29 @@ int orc_set_state(void* h, int l, const double* m) {
   return 0;
 }
 
+// MT on layer l (mrm_gpu_set_mt's arguments; lam_ms NULL: off)
+int orc_set_mt(void* h, int l, double spin, const double* lam_ms, int meq_bs, int garanin_tau) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.llb = lam_ms != nullptr;
+  Ly.mode = 1;
+  if (!lam_ms) return 0;
+  Ly.spin = spin;
+  Ly.meq_bs = meq_bs;
+  Ly.garanin_tau = garanin_tau;
+  Ly.tc.assign(Ly.N, 0.0);
+  Ly.lam_ms.assign(lam_ms, lam_ms + Ly.N);
+  return 0;
+}
+
 // LLB on layer l (mrm_gpu_set_llb's arguments; tc NULL: off)
 int orc_set_llb(void* h, int l, double spin, const double* tc, const double* lam_ms) {
   Sim* s = static_cast<Sim*>(h);
   if (l < 0 || l >= s->nl) return 1;
   Layer& Ly = s->L[l];
   Ly.llb = tc != nullptr;
+  Ly.mode = 0;
   if (!tc) return 0;
   Ly.spin = spin;
   Ly.tc.assign(tc, tc + Ly.N);

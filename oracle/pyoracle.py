@@ -58,6 +58,7 @@ def lib():
         L.orc_set_field_table.argtypes = [vp, i, i, i, P(d), P(d), P(d), d, d, d, d, d, d, d]
         L.orc_set_window.argtypes = [vp, i, i, d, d, d, d]
         L.orc_set_llb.argtypes = [vp, i, d, P(d), P(d)]
+        L.orc_set_mt.argtypes = [vp, i, d, P(d), i, i]
         L.orc_set_mag.argtypes = [vp, i, P(d)]
         L.orc_get_mag.argtypes = [vp, i, P(d)]
         L.orc_get_window.argtypes = [vp, P(i)]
@@ -229,6 +230,9 @@ class OracleSim:
             lb = getattr(lay, "llb", None)
             if lb:
                 self.set_llb(l, **lb)
+            mt = getattr(lay, "mt", None)
+            if mt:
+                self.set_mt(l, **mt)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
             cub = getattr(lay, "cubic_axis", None)
             if cub is not None:
@@ -301,6 +305,14 @@ class OracleSim:
         t, lm = f64(tc), f64(lambda_ms)
         self._keep += [t, lm]
         assert lib().orc_set_llb(self.h, layer, float(spin), _p(t), _p(lm)) == 0
+
+    def set_mt(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False):
+        """MT integrator on `layer` (GpuSim.set_mt's arguments)."""
+        if lambda_ms is None:
+            assert lib().orc_set_mt(self.h, layer, 0.0, None, 0, 0) == 0
+            return
+        lm = f64(lambda_ms)
+        assert lib().orc_set_mt(self.h, layer, float(spin), _p(lm), int(bool(meq_bs)), int(bool(garanin_tau))) == 0
 
     def set_mag(self, layer, mag):
         a = f64(mag)

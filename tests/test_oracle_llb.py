@@ -106,3 +106,37 @@ def test_semi_implicit_relaxes_to_equilibrium(oracle, llg_type):
     lam = med.layers[0].llb["lambda_ms"][0] * 3.0
     np.testing.assert_allclose(orc.get_mag(0), _find_meq(0.0, GMUB_KB * 0.5 * lam / 560.0), rtol=2e-5)
     orc.close()
+
+
+def _bs(x, s):
+    b = x / (2.0 * s)
+    if b != 0.0:
+        b = ((2.0 * s + 1.0) / math.tanh((2.0 * s + 1.0) * b) - 1.0 / math.tanh(b)) / (2.0 * s)
+    return b
+
+
+@pytest.mark.parametrize("meq_bs", [False, True])
+@pytest.mark.parametrize("llg_type", [-3, 2, -2])
+def test_mt_relaxes_to_mean_field(oracle, meq_bs, llg_type):
+    # push_mt (llg.f90:735-915) without field or noise: |m| decays to the
+    # equilibrium m = L(y lambda_m m) (Langevin) or B_S(y lambdaMs m) (Brillouin)
+    med = media.mt_medium(8, tc=700.0, tc_sigma=0.0, temperature=560.0, meq_bs=meq_bs)
+    for lay in med.layers:
+        lay.scale = 0.0
+        lay.hk[:] = 0.0
+        lay.hx = np.zeros_like(lay.hx)
+        lay.thermal = False
+    orc = oracle.OracleSim(med, demag=False)
+    orc.step(4000, 1e-14, llg_type=llg_type)
+    lms = med.layers[0].mt["lambda_ms"][0]
+    y = GMUB_KB * 0.5 / 560.0
+    if meq_bs:
+        b0, b1 = 0.0, 1.0
+        while b1 - b0 > 1e-13:
+            b = 0.5 * (b0 + b1)
+            b0, b1 = (b0, b) if b > _bs(y * lms * b, 0.5) else (b, b1)
+        want = 0.5 * (b0 + b1)
+    else:
+        want = _find_meq(0.0, y * lms * 3.0)
+    np.testing.assert_allclose(orc.get_mag(0), want, rtol=1e-4)
+    orc.close()
