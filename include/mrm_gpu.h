@@ -189,6 +189,26 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
                             const double* vfld, double vel_x, double vel_y, double offset_x, double offset_y,
                             double ref_x, double ref_y, double t_origin);
 
+/* Moving super-Gaussian temperature profile on `layer` (HAMR: suprgaus_temp
+ * and ref_temp, set_sg / get_sg, applied.f90:446-483,889-896,1778-1809; the
+ * grain's temperature, field.f90:546-560):
+ *   T(cell i, j; t) = background + s(t) dtemp fx(i) fy(j),
+ *   fx(i) = exp(-(((i + 1/2) dx + ref_x - vel_x (t - t_origin) - offset_x)/sigma_x)^(2 expn))
+ * (y alike; sigma 0: flat; offsets below -1e200: the grid centre), s(t) the
+ * profile's time scale (mrm_gpu_set_temp_function; default 1).  The grain's
+ * temperature replaces the layer's in the thermal variance and in the LLB / MT
+ * pushes (the temperature-scaling tables are not part of this path: Ms, Hk and
+ * alpha scales stay inputs).  One grain per cell.  expn < 0 removes it.
+ * mrm_gpu_set_temp_function: s(t) = ((s_end - s_start) clamp((t - t_start) /
+ * (t_end - t_start), 0, 1) + s_start) scale (func 0) or (amp f(t) + dc) scale
+ * with f as in mrm_gpu_set_field_function (func 1..5). */
+int mrm_gpu_set_temp_profile(mrm_gpu* h, int layer, double background, double dtemp, double sigma_x, double sigma_y,
+                             int expn, double vel_x, double vel_y, double offset_x, double offset_y, double ref_x,
+                             double ref_y, double t_origin);
+int mrm_gpu_set_temp_function(mrm_gpu* h, int layer, int func, double t_start, double t_end, double s_start,
+                              double s_end, double amp, double gamma, double phase, double param, double duty,
+                              double moddepth, double dc, double scale);
+
 /* LLB integrator (llgp%llb; push_llb, llg.f90:916-1064, Heun branch
  * :1000-1047 and the |m| = 0 branch :1048-1060) on `layer`: spin S, per grain
  * Curie temperature tc (K, > 0) and lambdaMs (Oe; lambda_m = lambdaMs (S+1)/S);

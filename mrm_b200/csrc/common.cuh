@@ -66,6 +66,20 @@ struct LlbDev {
   int mode, meq_bs, garanin_tau;
 };
 
+// Moving super-Gaussian temperature profile of a layer (HAMR: suprgaus_temp,
+// set_sg / get_sg and the temperature branch of get_appl / get_applied,
+// applied.f90:446-483,889-896,1778-1809, field.f90:546-560), in device
+// memory: T(cell (i, j), t) = bg + s(t) dtemp fx(i) fy(j),
+// fx(i) = exp(-(((i + 1/2) dx + rx - vx (t - t0) - ox) isx)^expn) (y alike,
+// isx = 1/sigma_x, 0: flat), s(t) the profile's own time scale (linear ramp
+// or funct, as a field's).
+struct TempDev {
+  double bg, dtemp, isx, isy, vx, vy, ox, oy, rx, ry, t0, dx, dy;
+  int expn;
+  int func;
+  double t_start, t_end, s_start, s_end, scale, amp, fgamma, phase, param, duty, moddepth, dc;
+};
+
 // Per-layer device view of one run.  State vectors are float4/double4
 // "SoA of 4-vectors": (x,y,z,w) per grain for one 16/32-byte load (w of m and
 // mp: the magnitude |m| of the LLB integrator; unused otherwise).
@@ -116,8 +130,8 @@ struct LayerDev {
   int hd_nbits;
   const struct TabDev* tab;  // tabulated field profile (null: the uniform hdir applies)
   const LlbDev* llb;         // LLB integrator (null: LLG)
+  const TempDev* tprof;      // temperature profile (null: the uniform temperature)
   double temperature;
-  double tfac;  // sqrt(temperature / dt), set with the run's dt
   double gamma;
   int thermal;
   int n;

@@ -95,6 +95,32 @@ MRM_D double ramp(const LayerDev<R>& L, double t) {
   return ((L.s_end - L.s_start) * u + L.s_start) * L.scale;
 }
 
+// Temperature profile (TempDev): x**n for an integer n >= 0 by squaring (the
+// reference's real**integer), the profile's time scale and a cell's temperature
+MRM_HD double powi(double x, int n) {
+  double r = 1.0;
+  while (n > 0) {
+    if (n & 1) r *= x;
+    x *= x;
+    n >>= 1;
+  }
+  return r;
+}
+MRM_D double temp_scale(const TempDev& P, double t) {
+  if (P.func != 0) return (P.amp * funct(P.func, t, P.fgamma, P.phase, P.param, P.duty, P.moddepth) + P.dc) * P.scale;
+  double u = (t - P.t_start) / (P.t_end - P.t_start);
+  u = fmax(0.0, fmin(1.0, u));
+  return ((P.s_end - P.s_start) * u + P.s_start) * P.scale;
+}
+// set_sg (applied.f90:1778-1790) and get_sg (:1792-1809) at grid cell (i, j);
+// s = dtemp times the time scale
+MRM_D double temp_cell(const TempDev& P, double s, double t, int i, int j) {
+  const double delx = P.rx - P.vx * (t - P.t0) - P.ox, dely = P.ry - P.vy * (t - P.t0) - P.oy;
+  const double fx = exp(-powi((P.dx * ((double)i + 0.5) + delx) * P.isx, P.expn));
+  const double fy = exp(-powi((P.dy * ((double)j + 0.5) + dely) * P.isy, P.expn));
+  return P.bg + s * fy * fx;
+}
+
 // Write head (func 6): gap-centre position and write polarity at time t
 template <typename R>
 MRM_D void head_state(const LayerDev<R>& L, double t, double* xh, double* pol) {
@@ -825,12 +851,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
   const double t_stage = (STAGE == kCorr) ? t_now + (mid ? 0.5 * rd.dt : rd.dt) : t_now;
   const double sc = ramp(L, t_stage);
+  const double tps = (GEN && L.tprof) ? L.tprof->dtemp * temp_scale(*L.tprof, t_stage) : 0.0;
   // a layer's field is its uniform direction or its tabulated profile, scaled
   const R hax = ftab ? (R)0 : (R)(sc * L.hdir[0]), hay = ftab ? (R)0 : (R)(sc * L.hdir[1]),
           haz = ftab ? (R)0 : (R)(sc * L.hdir[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
-  const R tfac = thermal ? (R)L.tfac : (R)0;
+  const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;  // sqrt(T/dt)
   // (a demag-only evaluation leaves L.hf alone: it holds the last stepping
   // stage's field, which a retried adaptive step reads)
   const bool store_field = (flags & kFlagStoreField) || (STAGE == kEval && !(flags & kFlagDemagOnly));
@@ -1013,6 +1040,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       continue;
     }
 
+    // the grain's temperature: the layer's, or its profile's at the stage's time
+    const double Tg = (GEN && L.tprof) ? temp_cell(*L.tprof, tps, t_stage, wi0 + i, wj0 + row0 + rr) : L.temperature;
     // thermal field / sqrt(dt) (llg.f90:1083): drawn by the predictor from the
     // step counter, reused by the corrector (:1262-1266)
     R htx = 0, hty = 0, htz = 0;
@@ -1022,12 +1051,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         // the grain's stream (one per grain, shared by its cells)
         const int nt = L.cgrain ? max(0, L.cgrain[n]) : n;
         thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)nt, gn);
-        R s = pb.w * tfac;
+        R s = (GEN && L.tprof) ? (R)((double)pb.w * sqrt(Tg / rd.dt)) : pb.w * tfac;
         if (GEN && L.llb && (double)mf.w != 1.0) {
           // get_thermal with |m| != 1 (field.f90:416-417): the variance over
           // max(floor_ms, |m|) instead of max(floor_ms, ms_scale)
           const LlbDev& P = *L.llb;
-          s = (R)sqrt(P.p[n].z * L.temperature / (fmax(P.floor_ms, fabs((double)mf.w)) * rd.dt));
+          s = (R)sqrt(P.p[n].z * Tg / (fmax(P.floor_ms, fabs((double)mf.w)) * rd.dt));
         }
         htx = s * gn[0];
         hty = s * gn[1];
@@ -1066,12 +1095,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       const LlbStep st =
           P.mode == 1
               ? mt_step(boris, STAGE == kPred, STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1,
-                        (double)pb.z, gp.y, P, L.temperature, L.gamma, pdt, rd.dt)
+                        (double)pb.z, gp.y, P, Tg, L.gamma, pdt, rd.dt)
           : (boris && (double)m0.w > 0.0)
               ? llb_boris(STAGE == kPred, mc, (double)m0.w, mpr, (double)mf.w, hh, th, (double)pb.z, gp.x, gp.y, P,
-                          L.temperature, L.gamma, (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt)
+                          Tg, L.gamma, pdt)
               : llb_heun(STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1, (double)pb.z, gp.x, gp.y, P,
-                         L.temperature, L.gamma, (STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt);
+                         Tg, L.gamma, pdt);
       if (STAGE == kPred && !boris) L.dm[n] = V4<R>{(R)st.d[0], (R)st.d[1], (R)st.d[2], (R)0};
       mn = V4<R>{(R)st.m[0], (R)st.m[1], (R)st.m[2], (R)st.mag};
       tq2 = (R)st.tq2;

@@ -76,6 +76,9 @@ struct LayerBufs {
   void* llb = nullptr;
   void* llbp = nullptr;
   double floor_ms = 0.01;
+  // temperature profile (null tprof: the uniform temperature): device TempDev and its host copy
+  void* tprof = nullptr;
+  TempDev tp{};
 };
 
 struct Engine;
@@ -146,7 +149,8 @@ struct Engine {
   bool has_head = false;             // a run has a layer under the write head or a tabulated
                                      // field profile (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
-  bool has_llb = false;              // a run integrates with LLB (general kernels)
+  bool has_llb = false;              // a run integrates with LLB / MT or has a temperature profile
+                                     // (general kernels)
   bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
   bool mapped = false;               // a run has grains of several cells (grain-averaged demag)
   double* d_part = nullptr;
@@ -493,7 +497,6 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.moddepth = b.moddepth;
     o.dc = b.dc;
     o.temperature = b.temperature;
-    o.tfac = std::sqrt(b.temperature / r->dt);
     o.gamma = b.gamma;
     o.thermal = b.thermal;
     o.n = b.n;
@@ -509,6 +512,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.hd_nbits = b.hd_nbits;
     o.tab = static_cast<const TabDev*>(b.tab);
     o.llb = static_cast<const LlbDev*>(b.llb);
+    o.tprof = static_cast<const TempDev*>(b.tprof);
   }
   return d;
 }
@@ -635,7 +639,7 @@ int build_tables(Engine* e) {
       karlqvist_head = karlqvist_head || r->L[l].func == kFuncHead;
       e->has_head = e->has_head || r->L[l].func == kFuncHead || r->L[l].tab != nullptr;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
-      e->has_llb = e->has_llb || r->L[l].llb != nullptr;
+      e->has_llb = e->has_llb || r->L[l].llb != nullptr || r->L[l].tprof != nullptr;
       e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
   if (e->mapped && karlqvist_head)
@@ -993,7 +997,8 @@ int run_steps(Engine* e, int nsteps, int llg_type) {
     // (data.f90:139): a frozen grain's |m| would depend on its history
     if (r->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "LLB with a moving demag window");
     for (int l = 0; l < r->nl; ++l)
-      if (!(r->L[l].temperature > 0)) return set_err(errp, MRM_ERR_ARG, "LLB needs a temperature > 0 (layer %d)", l);
+      if (!((r->L[l].tprof ? r->L[l].tp.bg : r->L[l].temperature) > 0))
+        return set_err(errp, MRM_ERR_ARG, "LLB needs a temperature > 0 (layer %d)", l);
   }
   int rc = ensure_ready<R>(e);
   if (rc) return rc;
@@ -1230,7 +1235,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.xst); dfree(b.ucol); dfree(b.lcol); dfree(b.cax);
     dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm); dfree(b.hapm);
     dfree(b.tab); dfree(b.tb_v); dfree(b.tb_pos);
-    dfree(b.llb); dfree(b.llbp);
+    dfree(b.llb); dfree(b.llbp); dfree(b.tprof);
   }
 }
 
@@ -2176,6 +2181,88 @@ static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, co
   CK(cudaMemcpy(b.llbp, rec.data(), sizeof(V4<double>) * (size_t)nc, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b.llb, &d, sizeof(LlbDev), cudaMemcpyHostToDevice));
   return MRM_OK;
+}
+
+static int push_temp_profile(mrm_gpu* h, LayerBufs& b) {
+  std::string* errp = &h->err;
+  if (!b.tprof) {
+    int rc = dmalloc(errp, &b.tprof, sizeof(TempDev));
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaStreamSynchronize(h->eng->st));
+  CK(cudaMemcpy(b.tprof, &b.tp, sizeof(TempDev), cudaMemcpyHostToDevice));
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the general kernels
+  return MRM_OK;
+}
+
+int mrm_gpu_set_temp_profile(mrm_gpu* h, int layer, double background, double dtemp, double sigma_x, double sigma_y,
+                             int expn, double vel_x, double vel_y, double offset_x, double offset_y, double ref_x,
+                             double ref_y, double t_origin) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  std::string* errp = &h->err;
+  LayerBufs& b = h->L[layer];
+  if (expn < 0) {  // off
+    CK(cudaSetDevice(h->eng->dev));
+    CK(cudaStreamSynchronize(h->eng->st));
+    dfree(b.tprof);
+    h->eng->desc_dirty = true;
+    h->eng->tables_dirty = true;
+    return MRM_OK;
+  }
+  if (b.cgrain) return set_err(errp, MRM_ERR_UNSUPPORTED, "a temperature profile needs one grain per cell");
+  if (expn < 1) return set_err(errp, MRM_ERR_ARG, "super-Gaussian exponent must be >= 1");
+  const bool fresh = !b.tprof;
+  TempDev& p = b.tp;
+  if (fresh) {  // the time scale starts constant 1
+    p.func = 0;
+    p.t_start = -1e22;
+    p.t_end = 1e22;
+    p.s_start = p.s_end = 1.0;
+    p.scale = 1.0;
+  }
+  p.bg = background;
+  p.dtemp = dtemp;
+  p.isx = sigma_x != 0.0 ? 1.0 / sigma_x : 0.0;  // suprgaus_temp (applied.f90:476-477)
+  p.isy = sigma_y != 0.0 ? 1.0 / sigma_y : 0.0;
+  p.expn = 2 * expn;
+  p.vx = vel_x;
+  p.vy = vel_y;
+  p.ox = offset_x < -1e200 ? h->g.dx * h->g.nx * 0.5 : offset_x;  // the grid centre (:459-460)
+  p.oy = offset_y < -1e200 ? h->g.dy * h->g.ny * 0.5 : offset_y;
+  p.rx = ref_x;
+  p.ry = ref_y;
+  p.t0 = t_origin;
+  p.dx = h->g.dx;
+  p.dy = h->g.dy;
+  return push_temp_profile(h, b);
+}
+
+int mrm_gpu_set_temp_function(mrm_gpu* h, int layer, int func, double t_start, double t_end, double s_start,
+                              double s_end, double amp, double gamma, double phase, double param, double duty,
+                              double moddepth, double dc, double scale) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  LayerBufs& b = h->L[layer];
+  if (!b.tprof) return set_err(&h->err, MRM_ERR_STATE, "set the temperature profile of layer %d first", layer);
+  if (func < 0 || func > 5) return set_err(&h->err, MRM_ERR_ARG, "unknown time function %d", func);
+  TempDev& p = b.tp;
+  p.func = func;
+  p.t_start = t_start;
+  p.t_end = t_end;
+  p.s_start = s_start;
+  p.s_end = s_end;
+  p.amp = amp;
+  p.fgamma = gamma;
+  p.phase = phase;
+  p.param = param;
+  p.duty = std::max(0.0, std::min(1.0, duty));
+  p.moddepth = std::max(0.0, std::min(1.0, moddepth));
+  p.dc = dc;
+  p.scale = scale;
+  return push_temp_profile(h, b);
 }
 
 int mrm_gpu_set_cubic_axes(mrm_gpu* h, int layer, const double* cubic_axis) {

@@ -75,6 +75,8 @@ class _RunMixin:
                 self.set_llb(l, **lay.llb)
             if getattr(lay, "mt", None):
                 self.set_mt(l, **lay.mt)
+            if getattr(lay, "temp_profile", None):
+                self.set_temp_profile(l, **lay.temp_profile)
             if getattr(lay, "cubic_axis", None) is not None:
                 self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
@@ -169,6 +171,26 @@ class _RunMixin:
         lm = f64(lambda_ms)
         self._check(L.mrm_gpu_set_mt(self.h, layer, float(spin), fptr(lm), int(bool(meq_bs)),
                                      int(bool(garanin_tau))))
+
+    def set_temp_profile(self, layer, background, dtemp, sigma=(0.0, 0.0), expn=1, vel=(0.0, 0.0),
+                         offset=(None, None), ref=(0.0, 0.0), t_origin=0.0, time=None):
+        """Moving super-Gaussian temperature profile (include/mrm_gpu.h
+        mrm_gpu_set_temp_profile); `time`: dict of mrm_gpu_set_temp_function's
+        arguments (func, t_start, t_end, s_start, s_end, amp, gamma, phase, param,
+        duty, moddepth, dc, scale); None: constant 1."""
+        L = _lib.load()
+        off = [-1e300 if o is None else float(o) for o in offset]
+        self._check(L.mrm_gpu_set_temp_profile(self.h, layer, float(background), float(dtemp), float(sigma[0]),
+                                               float(sigma[1]), int(expn), float(vel[0]), float(vel[1]), off[0],
+                                               off[1], float(ref[0]), float(ref[1]), float(t_origin)))
+        if time:
+            tf = time
+            self._check(L.mrm_gpu_set_temp_function(
+                self.h, layer, int(tf.get("func", 0)), float(tf.get("t_start", -1e22)), float(tf.get("t_end", 1e22)),
+                float(tf.get("s_start", 1.0)), float(tf.get("s_end", 1.0)), float(tf.get("amp", 0.0)),
+                float(tf.get("gamma", 0.0)), float(tf.get("phase", 0.0)), float(tf.get("param", 0.0)),
+                float(tf.get("duty", 0.0)), float(tf.get("moddepth", 0.0)), float(tf.get("dc", 0.0)),
+                float(tf.get("scale", 1.0))))
 
     def set_mag(self, layer: int, mag):
         """The LLB magnitude |m| per grain."""

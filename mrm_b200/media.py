@@ -91,6 +91,9 @@ class Layer:
     # MT integrator (llgp%mt): dict(spin, lambda_ms (N,) Oe, meq_bs, garanin_tau)
     # (include/mrm_gpu.h mrm_gpu_set_mt)
     mt: Optional[dict] = None
+    # moving super-Gaussian temperature profile: dict of GpuSim.set_temp_profile's
+    # arguments (include/mrm_gpu.h mrm_gpu_set_temp_profile)
+    temp_profile: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -472,4 +475,18 @@ def mt_medium(side: int = 32, *, meq_bs: bool = False, garanin_tau: bool = False
         # for B_S; the Langevin form takes the same lambdaMs through lambda_m (S+1)/S
         lay.mt = dict(spin=sp, lambda_ms=lb["lambda_ms"], meq_bs=meq_bs, garanin_tau=garanin_tau)
         lay.llb = None
+    return med
+
+
+def hamr_medium(side: int = 64, *, seed: int = 1, background: float = 300.0, peak: float = 450.0,
+                sigma_nm: float = 60.0, velocity_cm_s: float = 2000.0, **kw) -> Medium:
+    """A heat-assisted write: llb_medium's layer at a background temperature with
+    a laser spot (second-order super-Gaussian, 1/e half width sigma_nm, peak
+    rise `peak` above the background) moving down-track from the grid's left
+    edge at `velocity_cm_s`, under the medium's reversing field."""
+    med = llb_medium(side, seed=seed, temperature=background, **kw)
+    for lay in med.layers:
+        lay.temperature = background
+        lay.temp_profile = dict(background=background, dtemp=peak, sigma=(sigma_nm * 1e-7, sigma_nm * 1e-7), expn=1,
+                                vel=(velocity_cm_s, 0.0), offset=(0.0, None), ref=(0.0, 0.0), t_origin=0.0)
     return med

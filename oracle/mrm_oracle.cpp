@@ -465,6 +465,15 @@ struct Layer {
   int mode = 0, meq_bs = 0, garanin_tau = 0;  // mode 1: push_mt (llgp%mt)
   double spin = 1.0;
   std::vector<double> tc, lam_ms, mag[2];
+  // super-Gaussian temperature profile (suprgaus_temp / ref_temp / set_temp):
+  // the grain temperatures of the last field evaluation (get_applied)
+  bool tprof = false;
+  double tp_bg = 0, tp_dtemp = 0, tp_isx = 0, tp_isy = 0, tp_vx = 0, tp_vy = 0, tp_ox = 0, tp_oy = 0, tp_rx = 0,
+         tp_ry = 0, tp_t0 = 0;
+  int tp_expn = 2, tp_func = 0;
+  double tp_t_start = -1e22, tp_t_end = 1e22, tp_s_start = 1, tp_s_end = 1, tp_scale = 1, tp_amp = 0, tp_fgamma = 0,
+         tp_phase = 0, tp_param = 0, tp_duty = 0, tp_moddepth = 0, tp_dc = 0;
+  std::vector<double> temp;
   std::vector<double> m[2], dm, h, hthm, hdemag, happ;
   // schedule: uniform field x linear ramp (applied.f90:863-883)
   double hdir[3] = {0, 0, 0};
@@ -705,6 +714,43 @@ static double head_polarity(const Layer& Ly, double t) {
   return ((Ly.hd_bits >> k) & 1ull) ? 1.0 : -1.0;
 }
 
+// x**n, n a non-negative integer (real**integer by squaring)
+static double ipow(double x, int n) {
+  double r = 1.0;
+  while (n > 0) {
+    if (n & 1) r *= x;
+    x *= x;
+    n >>= 1;
+  }
+  return r;
+}
+
+// the grains' temperatures at t (get_appl's temperature branch, applied.f90:
+// 889-896 with set_sg / get_sg :1778-1809, then get_applied's average over a
+// grain's cells plus the background, field.f90:546-560)
+static void grain_temps(const Sim* s, Layer& Ly, double t) {
+  Ly.temp.assign(Ly.N, Ly.temperature);
+  if (!Ly.tprof) return;
+  double sc;
+  if (Ly.tp_func != 0) {
+    sc = (Ly.tp_amp * funct(Ly.tp_func, t, Ly.tp_fgamma, Ly.tp_phase, Ly.tp_param, Ly.tp_duty, Ly.tp_moddepth) +
+          Ly.tp_dc) * Ly.tp_scale;
+  } else {
+    const double u = std::max(0.0, std::min(1.0, (t - Ly.tp_t_start) / (Ly.tp_t_end - Ly.tp_t_start)));
+    sc = ((Ly.tp_s_end - Ly.tp_s_start) * u + Ly.tp_s_start) * Ly.tp_scale;
+  }
+  const double sdt = Ly.tp_dtemp * sc;
+  std::vector<double> fx(s->nx), fy(s->ny);
+  const double delx = Ly.tp_rx - Ly.tp_vx * (t - Ly.tp_t0) - Ly.tp_ox, dely = Ly.tp_ry - Ly.tp_vy * (t - Ly.tp_t0) - Ly.tp_oy;
+  for (int i = 1; i <= s->nx; ++i) fx[i - 1] = std::exp(-ipow((s->dx * (i - 0.5) + delx) * Ly.tp_isx, Ly.tp_expn));
+  for (int j = 1; j <= s->ny; ++j) fy[j - 1] = std::exp(-ipow((s->dy * (j - 0.5) + dely) * Ly.tp_isy, Ly.tp_expn));
+  for (int n = 0; n < Ly.N; ++n) {
+    double x = 0.0;
+    for (int q = Ly.g2c_idx[n]; q < Ly.g2c_idx[n + 1]; ++q) x += sdt * fy[Ly.g2c_j[q]] * fx[Ly.g2c_i[q]];
+    Ly.temp[n] = x / (double)(Ly.g2c_idx[n + 1] - Ly.g2c_idx[n]) + Ly.tp_bg;
+  }
+}
+
 // get_field (field.f90:160-273) for the LLG path; energy per grain summed into *energy
 static void get_field(Sim* s, double t, int buf, double* energy) {
   compute_demag(s, buf);
@@ -712,6 +758,7 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
   for (int l = 0; l < s->nl; ++l) {
     Layer& Ly = s->L[l];
     double sc = Ly.head ? 0.0 : ramp_scale(Ly, t);
+    grain_temps(s, Ly, t);
     std::vector<double> hat;
     if (Ly.tab) table_field(s, Ly, t, sc, hat);
     const double* m = Ly.m[buf].data();
@@ -816,12 +863,11 @@ static void get_thermal(Sim* s) {
     for (int n = 0; n < Ly.N; ++n) {
       if (!Ly.do_grain[n]) continue;
       double x = 0.0;
+      const double Tn = Ly.temp.empty() ? Ly.temperature : Ly.temp[n];  // field(i)%temp(n)
       if (Ly.mag[s->in][n] != 1.0)  // field.f90:416-417
-        x = Ly.alpha_scale[n] * Ly.temperature /
-            (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, std::abs(Ly.mag[s->in][n])));
+        x = Ly.alpha_scale[n] * Tn / (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, std::abs(Ly.mag[s->in][n])));
       else if (Ly.ms_scale[n] > 0.0)
-        x = Ly.alpha_scale[n] * Ly.temperature /
-            (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, Ly.ms_scale[n]));
+        x = Ly.alpha_scale[n] * Tn / (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, Ly.ms_scale[n]));
       x = std::sqrt(x) * tsigma;
       double r[3];
       if (s->rng_mode == 0) {
@@ -861,11 +907,11 @@ static void push_llb(Sim* s, int l, int type, int iter, double dt, double dt0, d
   const int id = s->in;
   const double gmub_kb = 1.343427768e-4;  // llg.f90:924
   const double scale1 = -0.5 * Ly.gamma * dt;
-  const double T = Ly.temperature;
   double em = 0.0, em1 = 0.0, mm = 0.0;
 #pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
   for (int n = 0; n < Ly.N; ++n) {
     if (n < Ly.min_n || n > Ly.max_n) continue;
+    const double T = Ly.temp[n];  // p%temp(n) of the last field evaluation
     double* mnext = &Ly.m[1 - id][3 * n];
     const double* mcur = &Ly.m[id][3 * n];
     double& magn = Ly.mag[1 - id][n];
@@ -1058,7 +1104,7 @@ static void push_mt(Sim* s, int l, int type, int iter, double dt, double dt0, do
   const int id = s->in;
   const double gmub_kb = 1.343427768e-4;
   const double scale1 = -0.5 * Ly.gamma * dt, scale11 = 2.0 * scale1;
-  const double T = Ly.temperature, sp = Ly.spin;
+  const double sp = Ly.spin;
   double em = 0.0, em1 = 0.0, mm = 0.0;
 #pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
   for (int n = 0; n < Ly.N; ++n) {
@@ -1076,6 +1122,7 @@ static void push_mt(Sim* s, int l, int type, int iter, double dt, double dt0, do
       mm += magn * Ly.vol[n];
       continue;
     }
+    const double T = Ly.temp[n];  // p%temp(n) of the last field evaluation
     double lambdam = Ly.lam_ms[n];
     if (!Ly.meq_bs) lambdam = lambdam * (sp + 1.0) / sp;
     double y = gmub_kb * sp / T;
@@ -1838,6 +1885,52 @@ int orc_set_state(void* h, int l, const double* m) {
   std::memcpy(Ly.m[1 - s->in].data(), m, sizeof(double) * 3 * Ly.N);
   Ly.mag[0].assign(Ly.N, 1.0);  // a new state starts at |m| = 1 (data.f90:202)
   Ly.mag[1].assign(Ly.N, 1.0);
+  return 0;
+}
+
+// grain temperatures of the last field evaluation (field(k)%temp)
+int orc_get_temp(void* h, int l, double* out) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl || (int)s->L[l].temp.size() != s->L[l].N) return 1;
+  std::memcpy(out, s->L[l].temp.data(), sizeof(double) * s->L[l].N);
+  return 0;
+}
+
+// temperature profile (mrm_gpu_set_temp_profile's arguments; expn < 0: off)
+int orc_set_temp_profile(void* h, int l, double bg, double dtemp, double sx, double sy, int expn, double vx,
+                         double vy, double ox, double oy, double rx, double ry, double t0) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  if (expn < 0) {
+    Ly.tprof = false;
+    return 0;
+  }
+  if (!Ly.tprof) {
+    Ly.tp_func = 0; Ly.tp_t_start = -1e22; Ly.tp_t_end = 1e22; Ly.tp_s_start = Ly.tp_s_end = 1.0; Ly.tp_scale = 1.0;
+  }
+  Ly.tprof = true;
+  Ly.tp_bg = bg; Ly.tp_dtemp = dtemp;
+  Ly.tp_isx = sx != 0.0 ? 1.0 / sx : 0.0;  // applied.f90:476-477
+  Ly.tp_isy = sy != 0.0 ? 1.0 / sy : 0.0;
+  Ly.tp_expn = 2 * expn;
+  Ly.tp_vx = vx; Ly.tp_vy = vy;
+  Ly.tp_ox = ox < -1e200 ? s->dx * s->nx * 0.5 : ox;
+  Ly.tp_oy = oy < -1e200 ? s->dy * s->ny * 0.5 : oy;
+  Ly.tp_rx = rx; Ly.tp_ry = ry; Ly.tp_t0 = t0;
+  return 0;
+}
+
+int orc_set_temp_function(void* h, int l, int func, double t_start, double t_end, double s_start, double s_end,
+                          double amp, double g, double phase, double param, double duty, double moddepth, double dc,
+                          double scale) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl || !s->L[l].tprof) return 1;
+  Layer& Ly = s->L[l];
+  Ly.tp_func = func; Ly.tp_t_start = t_start; Ly.tp_t_end = t_end; Ly.tp_s_start = s_start; Ly.tp_s_end = s_end;
+  Ly.tp_amp = amp; Ly.tp_fgamma = g; Ly.tp_phase = phase; Ly.tp_param = param;
+  Ly.tp_duty = std::max(0.0, std::min(1.0, duty)); Ly.tp_moddepth = std::max(0.0, std::min(1.0, moddepth));
+  Ly.tp_dc = dc; Ly.tp_scale = scale;
   return 0;
 }
 

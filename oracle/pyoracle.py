@@ -59,6 +59,9 @@ def lib():
         L.orc_set_window.argtypes = [vp, i, i, d, d, d, d]
         L.orc_set_llb.argtypes = [vp, i, d, P(d), P(d)]
         L.orc_set_mt.argtypes = [vp, i, d, P(d), i, i]
+        L.orc_set_temp_profile.argtypes = [vp, i, d, d, d, d, i, d, d, d, d, d, d, d]
+        L.orc_set_temp_function.argtypes = [vp, i, i] + [d] * 12
+        L.orc_get_temp.argtypes = [vp, i, P(d)]
         L.orc_set_mag.argtypes = [vp, i, P(d)]
         L.orc_get_mag.argtypes = [vp, i, P(d)]
         L.orc_get_window.argtypes = [vp, P(i)]
@@ -92,6 +95,15 @@ def lib():
 
 def _p(a, ct=C.c_double):
     return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _temp_function_args(tf):
+    """(func, t_start, t_end, s_start, s_end, amp, gamma, phase, param, duty, moddepth, dc, scale)"""
+    return (int(tf.get("func", 0)), float(tf.get("t_start", -1e22)), float(tf.get("t_end", 1e22)),
+            float(tf.get("s_start", 1.0)), float(tf.get("s_end", 1.0)), float(tf.get("amp", 0.0)),
+            float(tf.get("gamma", 0.0)), float(tf.get("phase", 0.0)), float(tf.get("param", 0.0)),
+            float(tf.get("duty", 0.0)), float(tf.get("moddepth", 0.0)), float(tf.get("dc", 0.0)),
+            float(tf.get("scale", 1.0)))
 
 
 def f64(a):
@@ -233,6 +245,9 @@ class OracleSim:
             mt = getattr(lay, "mt", None)
             if mt:
                 self.set_mt(l, **mt)
+            tp = getattr(lay, "temp_profile", None)
+            if tp:
+                self.set_temp_profile(l, **tp)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
             cub = getattr(lay, "cubic_axis", None)
             if cub is not None:
@@ -313,6 +328,23 @@ class OracleSim:
             return
         lm = f64(lambda_ms)
         assert lib().orc_set_mt(self.h, layer, float(spin), _p(lm), int(bool(meq_bs)), int(bool(garanin_tau))) == 0
+
+    def set_temp_profile(self, layer, background, dtemp, sigma=(0.0, 0.0), expn=1, vel=(0.0, 0.0),
+                         offset=(None, None), ref=(0.0, 0.0), t_origin=0.0, time=None):
+        """Temperature profile (GpuSim.set_temp_profile's arguments)."""
+        off = [-1e300 if o is None else float(o) for o in offset]
+        assert lib().orc_set_temp_profile(self.h, layer, float(background), float(dtemp), float(sigma[0]),
+                                          float(sigma[1]), int(expn), float(vel[0]), float(vel[1]), off[0], off[1],
+                                          float(ref[0]), float(ref[1]), float(t_origin)) == 0
+        if time:
+            a = _temp_function_args(time)
+            assert lib().orc_set_temp_function(self.h, layer, *a) == 0
+
+    def get_temp(self, layer):
+        """Grain temperatures of the last field evaluation."""
+        out = np.zeros(self.medium.layers[layer].N)
+        assert lib().orc_get_temp(self.h, layer, _p(out)) == 0
+        return out
 
     def set_mag(self, layer, mag):
         a = f64(mag)
