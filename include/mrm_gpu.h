@@ -229,6 +229,11 @@ int mrm_gpu_set_llb(mrm_gpu* h, int layer, double spin, const double* tc, const 
  * semi-implicit |type| = 2 branch (llg_type -3, 2, -2); the same switch, checks
  * and magnitude accessors as the LLB integrator.  lambda_ms = NULL: off. */
 int mrm_gpu_set_mt(mrm_gpu* h, int layer, double spin, const double* lambda_ms, int meq_bs, int garanin_tau);
+/* Zhang integrator (llgp%zhang: push_zhang, llg.f90:410-703; the thermal field
+ * joins the precession with variance lambda meq/(|H| |m|)): arguments as
+ * mrm_gpu_set_mt (the reference sets meq_bs = !zhang_l); Heun and the
+ * |type| = 2 branch. */
+int mrm_gpu_set_zhang(mrm_gpu* h, int layer, double spin, const double* lambda_ms, int meq_bs, int garanin_tau);
 int mrm_gpu_set_mag(mrm_gpu* h, int layer, const double* mag);
 int mrm_gpu_get_mag(mrm_gpu* h, int layer, double* mag);
 

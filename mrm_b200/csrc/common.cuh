@@ -57,9 +57,10 @@ struct TabDev {
 // T/|m|), 0}; the layer's spin, damping alpha and floor_ms (get_thermal's
 // |m| floor); the temperature is the layer's (LayerDev::temperature).  The
 // grain's magnitude |m| (mag) rides in the w lane of m and mp.
-// mode 1 is the MT integrator (llgp%mt: push_mt, llg.f90:735-915) on the same
-// records (Tc unused), with the Brillouin equilibrium (meq_bs) and Garanin's
-// tau (garanin_tau) as options.
+// mode 1 is the MT integrator (llgp%mt: push_mt, llg.f90:735-915), mode 2 the
+// Zhang integrator (llgp%zhang: push_zhang, :410-703), on the same records (Tc
+// unused, lambdaMs raw), with the Brillouin equilibrium (meq_bs) and
+// Garanin's tau (garanin_tau) as options.
 struct LlbDev {
   const V4<double>* p;
   double spin, alpha, floor_ms;

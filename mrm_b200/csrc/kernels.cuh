@@ -501,6 +501,105 @@ MRM_D LlbStep mt_step(bool boris, bool first, bool corr, const double* mc, doubl
   return o;
 }
 
+// One grain of push_zhang (llg.f90:410-703): the Heun branch (:633-700) or
+// the semi-implicit |type| = 2 branch (:428-510), arguments as mt_step.  The
+// thermal field joins the precession with the variance scale2 meq/(|H| |m|)
+// (no separate eta).
+MRM_D LlbStep zhang_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr,
+                         double magp, const double* h, const double* ht, const double* d1, double ab, double lam0,
+                         const LlbDev& P, double T, double gamma, double dt, double dt0) {
+  LlbStep o;
+  const double sp = P.spin;
+  const double lam = P.meq_bs ? lam0 : lam0 * (sp + 1.0) / sp;
+  double y = kGmubKb * sp / T;
+  const double scale1 = -0.5 * gamma * dt;
+  const double sq = sqrt(dt0);
+  double m[3], mag, htot[3], mhtot, d[3], t[3];
+  auto tot = [&](const double* v, double mg) {
+    for (int c = 0; c < 3; ++c) htot[c] = h[c] + lam * mg * v[c];
+    mhtot = sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+    if (mhtot != 0.0)
+      for (int c = 0; c < 3; ++c) htot[c] /= mhtot;
+  };
+  auto meq_of = [&](double x) { return P.meq_bs ? mt_bs(x, sp) : llb_lv(x); };
+  auto dmeq_of = [&](double x) { return P.meq_bs ? mt_dbs(x, sp) : llb_dlv(x); };
+  if (boris) {
+    for (int c = 0; c < 3; ++c) m[c] = first ? mc[c] : mpr[c];
+    mag = first ? magc : magp;
+    tot(m, mag);
+    double meq = meq_of(y * mhtot);
+    double scale2 = P.garanin_tau ? 2.0 * (meq / (y * mhtot * dmeq_of(y * mhtot) + 1e-80)) / y : lam;
+    // hthm sqrt(|scale2 meq / (|H| |m| dt0)|), hthm = ht sqrt(dt0)
+    const double fth = sqrt(fabs(scale2 * meq / (mhtot * mag * dt0 + 1e-80))) * sq;
+    scale2 = ab * scale2;
+    for (int c = 0; c < 3; ++c) m[c] = mc[c];
+    mag = magc;
+    double hb[3], w[3], x[3];
+    for (int c = 0; c < 3; ++c) hb[c] = h[c] + ht[c] * fth;
+    cross3(m[0], m[1], m[2], hb[0], hb[1], hb[2], t[0], t[1], t[2]);
+    o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+    const double dec = 1.0 - exp(scale1 * scale2);
+    for (int c = 0; c < 3; ++c) d[c] = (meq * htot[c] - mag * m[c]) * dec;
+    for (int c = 0; c < 3; ++c) w[c] = mag * m[c] + d[c];
+    cross3(w[0], w[1], w[2], hb[0], hb[1], hb[2], x[0], x[1], x[2]);
+    for (int c = 0; c < 3; ++c) d[c] += 2.0 * scale1 * x[c];  // :472
+    for (int c = 0; c < 3; ++c) w[c] = mag * m[c] + d[c];
+    tot(w, 1.0);
+    meq = meq_of(y * mhtot);
+    scale2 = ab * (P.garanin_tau ? 2.0 * (meq / (y * mhtot * dmeq_of(y * mhtot) + 1e-80)) / y : lam);
+    const double dec2 = 1.0 - exp(scale1 * scale2);
+    for (int c = 0; c < 3; ++c) d[c] = d[c] + (meq * htot[c] - w[c]) * dec2;  // :500
+  } else {
+    const double scale11 = 2.0 * scale1;
+    for (int c = 0; c < 3; ++c) m[c] = mc[c];
+    mag = magc;
+    if (corr) {  // :635-638 (y becomes |h| when |m| <= 0, as there)
+      for (int c = 0; c < 3; ++c) m[c] = mpr[c];
+      mag = magp;
+      if (mag <= 0.0) {
+        mag = 0.0;
+        y = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+        if (y != 0.0)
+          for (int c = 0; c < 3; ++c) m[c] = h[c] / y;
+      }
+    }
+    tot(m, mag);
+    y = y * mhtot;
+    const double meq = meq_of(y);
+    double scale2;
+    if (P.garanin_tau) {
+      y = meq / (y * dmeq_of(y) + 1e-66);
+      scale2 = 2.0 * T * y / (kGmubKb * sp);
+    } else {
+      scale2 = lam;
+    }
+    y = fabs(scale2 * meq / (mhtot * mag + 1e-66));
+    double hb[3], mm[3], x[3];
+    for (int c = 0; c < 3; ++c) hb[c] = h[c] + ht[c] * sq * sqrt(fabs(y / dt0));
+    scale2 = scale2 * ab;
+    for (int c = 0; c < 3; ++c) mm[c] = m[c] * mag;
+    cross3(mm[0], mm[1], mm[2], hb[0], hb[1], hb[2], x[0], x[1], x[2]);
+    for (int c = 0; c < 3; ++c) d[c] = scale11 * (x[c] + (mm[c] - meq * htot[c]) * scale2);
+    if (corr)
+      for (int c = 0; c < 3; ++c) d[c] = 0.5 * (d[c] + d1[c]);
+    cross3(m[0], m[1], m[2], hb[0], hb[1], hb[2], t[0], t[1], t[2]);
+    o.tq2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+  }
+  for (int c = 0; c < 3; ++c) o.d[c] = d[c];
+  o.d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  double w[3];
+  for (int c = 0; c < 3; ++c) w[c] = mc[c] * magc + d[c];
+  const double e = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (e > 0.0) {
+    for (int c = 0; c < 3; ++c) o.m[c] = w[c] / e;
+    o.mag = e;
+  } else {
+    for (int c = 0; c < 3; ++c) o.m[c] = -mc[c];
+    o.mag = 0.0;
+  }
+  return o;
+}
+
 // shared memory of a row block's table weights (grid columns, then the
 // block's rows; at most 8 rows per block)
 MRM_HD int field_table_bytes(int nx) { return (nx + 8) * (int)sizeof(TabW); }
@@ -1096,6 +1195,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
           P.mode == 1
               ? mt_step(boris, STAGE == kPred, STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1,
                         (double)pb.z, gp.y, P, Tg, L.gamma, pdt, rd.dt)
+          : P.mode == 2
+              ? zhang_step(boris, STAGE == kPred, STAGE == kCorr, mc, (double)m0.w, mpr, (double)mf.w, hh, th, d1,
+                           (double)pb.z, gp.y, P, Tg, L.gamma, pdt, rd.dt)
           : (boris && (double)m0.w > 0.0)
               ? llb_boris(STAGE == kPred, mc, (double)m0.w, mpr, (double)mf.w, hh, th, (double)pb.z, gp.x, gp.y, P,
                           Tg, L.gamma, pdt)

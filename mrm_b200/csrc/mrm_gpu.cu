@@ -2132,6 +2132,10 @@ int mrm_gpu_set_mt(mrm_gpu* h, int layer, double spin, const double* lambda_ms, 
   return set_llb_mode(h, layer, spin, lambda_ms, lambda_ms, 1, meq_bs, garanin_tau);
 }
 
+int mrm_gpu_set_zhang(mrm_gpu* h, int layer, double spin, const double* lambda_ms, int meq_bs, int garanin_tau) {
+  return set_llb_mode(h, layer, spin, lambda_ms, lambda_ms, 2, meq_bs, garanin_tau);
+}
+
 static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, const double* lambda_ms, int mode,
                         int meq_bs, int garanin_tau) {
   if (!h) return MRM_ERR_ARG;
@@ -2161,7 +2165,7 @@ static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, co
     const double msv = hc.ms[g] * hc.vol[g];
     rec[c].x = mode == 0 ? tc[g] : 0.0;
     // LLB: lambda_m = lambdaMs (S+1)/S; MT: lambdaMs (push_mt scales it by meq_bs)
-    rec[c].y = mode == 0 ? lambda_ms[g] * (spin + 1.0) / spin : lambda_ms[g];
+    rec[c].y = mode == 0 ? lambda_ms[g] * (spin + 1.0) / spin : lambda_ms[g];  // (MT / Zhang: raw)
     rec[c].z = msv > 0 ? 2.0 * kBoltz * b.alpha * hc.alpha_scale[g] / (b.gamma * msv) : 0.0;
   }
   LlbDev d{};

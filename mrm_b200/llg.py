@@ -75,6 +75,8 @@ class _RunMixin:
                 self.set_llb(l, **lay.llb)
             if getattr(lay, "mt", None):
                 self.set_mt(l, **lay.mt)
+            if getattr(lay, "zhang", None):
+                self.set_zhang(l, **lay.zhang)
             if getattr(lay, "temp_profile", None):
                 self.set_temp_profile(l, **lay.temp_profile)
             if getattr(lay, "cubic_axis", None) is not None:
@@ -191,6 +193,16 @@ class _RunMixin:
                 float(tf.get("gamma", 0.0)), float(tf.get("phase", 0.0)), float(tf.get("param", 0.0)),
                 float(tf.get("duty", 0.0)), float(tf.get("moddepth", 0.0)), float(tf.get("dc", 0.0)),
                 float(tf.get("scale", 1.0))))
+
+    def set_zhang(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False):
+        """Zhang integrator on `layer` (include/mrm_gpu.h mrm_gpu_set_zhang)."""
+        L = _lib.load()
+        if lambda_ms is None:
+            self._check(L.mrm_gpu_set_zhang(self.h, layer, 0.0, None, 0, 0))
+            return
+        lm = f64(lambda_ms)
+        self._check(L.mrm_gpu_set_zhang(self.h, layer, float(spin), fptr(lm), int(bool(meq_bs)),
+                                        int(bool(garanin_tau))))
 
     def set_mag(self, layer: int, mag):
         """The LLB magnitude |m| per grain."""

@@ -94,6 +94,8 @@ class Layer:
     # moving super-Gaussian temperature profile: dict of GpuSim.set_temp_profile's
     # arguments (include/mrm_gpu.h mrm_gpu_set_temp_profile)
     temp_profile: Optional[dict] = None
+    # Zhang integrator (llgp%zhang): dict(spin, lambda_ms, meq_bs, garanin_tau)
+    zhang: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -489,4 +491,12 @@ def hamr_medium(side: int = 64, *, seed: int = 1, background: float = 300.0, pea
         lay.temperature = background
         lay.temp_profile = dict(background=background, dtemp=peak, sigma=(sigma_nm * 1e-7, sigma_nm * 1e-7), expn=1,
                                 vel=(velocity_cm_s, 0.0), offset=(0.0, None), ref=(0.0, 0.0), t_origin=0.0)
+    return med
+
+
+def zhang_medium(side: int = 32, *, meq_bs: bool = False, garanin_tau: bool = False, **kw) -> Medium:
+    """mt_medium's heat-assisted layer driven by the Zhang integrator."""
+    med = mt_medium(side, meq_bs=meq_bs, garanin_tau=garanin_tau, **kw)
+    for lay in med.layers:
+        lay.zhang, lay.mt = lay.mt, None
     return med

@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_zhang, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -117,6 +117,14 @@ module mrm_gpu_m
       real(C_DOUBLE), intent(in) :: tc(*), lambda_ms(*)
     end function
     integer(C_INT) function c_set_mt(h, layer, spin, lambda_ms, meq_bs, garanin_tau) bind(C, name="mrm_gpu_set_mt")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, meq_bs, garanin_tau
+      real(C_DOUBLE), value :: spin
+      real(C_DOUBLE), intent(in) :: lambda_ms(*)
+    end function
+    integer(C_INT) function c_set_zhang(h, layer, spin, lambda_ms, meq_bs, garanin_tau) &
+        bind(C, name="mrm_gpu_set_zhang")
       import :: C_INT, C_PTR, C_DOUBLE
       type(C_PTR), value :: h
       integer(C_INT), value :: layer, meq_bs, garanin_tau
@@ -330,6 +338,15 @@ contains
     logical, intent(in) :: meq_bs, garanin_tau
     ok_p = ok(c_set_mt(h, int(layer - 1, C_INT), spin, lambda_ms, merge(1_C_INT, 0_C_INT, meq_bs), &
                        merge(1_C_INT, 0_C_INT, garanin_tau)))
+  end function
+  ! llgp%zhang on `layer` (include/mrm_gpu.h mrm_gpu_set_zhang)
+  logical function gpu_set_zhang(h, layer, spin, lambda_ms, meq_bs, garanin_tau) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: spin, lambda_ms(:)
+    logical, intent(in) :: meq_bs, garanin_tau
+    ok_p = ok(c_set_zhang(h, int(layer - 1, C_INT), spin, lambda_ms, merge(1_C_INT, 0_C_INT, meq_bs), &
+                          merge(1_C_INT, 0_C_INT, garanin_tau)))
   end function
   logical function gpu_set_mag(h, layer, mag) result(ok_p)
     type(C_PTR), intent(in) :: h

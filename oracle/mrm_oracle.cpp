@@ -1256,6 +1256,146 @@ static void push_mt(Sim* s, int l, int type, int iter, double dt, double dt0, do
   *mmag1 = mm;
 }
 
+// push_zhang (llg.f90:410-703): the |type| = 2 explicit-rotation branch
+// (:428-510) and the Heun branch (:633-700), for one layer.
+static void push_zhang(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l, double* errmx1_l,
+                       double* mmag1) {
+  Layer& Ly = s->L[l];
+  const int id = s->in;
+  const double gmub_kb = 1.343427768e-4;
+  const double scale1 = -0.5 * Ly.gamma * dt;
+  const double sp = Ly.spin;
+  double em = 0.0, em1 = 0.0, mm = 0.0;
+#pragma omp parallel for reduction(max : em, em1) reduction(+ : mm)
+  for (int n = 0; n < Ly.N; ++n) {
+    if (n < Ly.min_n || n > Ly.max_n) continue;
+    double* mnext = &Ly.m[1 - id][3 * n];
+    const double* mcur = &Ly.m[id][3 * n];
+    double& magn = Ly.mag[1 - id][n];
+    double m[3] = {mcur[0], mcur[1], mcur[2]}, mag = Ly.mag[id][n];
+    if (!Ly.do_grain[n]) {
+      for (int a = 0; a < 3; ++a) {
+        mnext[a] = m[a];
+        Ly.dm[3 * n + a] = 0.0;
+      }
+      magn = mag;
+      mm += magn * Ly.vol[n];
+      continue;
+    }
+    const double T = Ly.temp[n];
+    double lambdam = Ly.lam_ms[n];
+    if (!Ly.meq_bs) lambdam = lambdam * (sp + 1.0) / sp;
+    double y = gmub_kb * sp / T;
+    const double* hn = &Ly.h[3 * n];
+    const double* th = &Ly.hthm[3 * n];
+    double htot[3], mhtot, meq, scale2, d[3], t[3], o[3], h[3];
+    auto norm_tot = [&]() {
+      mhtot = std::sqrt(htot[0] * htot[0] + htot[1] * htot[1] + htot[2] * htot[2]);
+      if (mhtot != 0.0)
+        for (int a = 0; a < 3; ++a) htot[a] /= mhtot;
+    };
+    auto bsl = [&](double x) { return Ly.meq_bs ? bs(x, sp) : lv(x); };
+    auto dbsl = [&](double x) { return Ly.meq_bs ? dbs(x, sp) : dlv(x); };
+    if (std::abs(type) < 3) {
+      if (iter == 1 && type < 0) {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+      }
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mag * m[a];
+      norm_tot();
+      meq = bsl(y * mhtot);
+      if (Ly.garanin_tau) {
+        const double sig_p = meq / (y * mhtot * dbsl(y * mhtot) + 1e-80);
+        scale2 = 2.0 * sig_p / y;
+      } else {
+        scale2 = lambdam;
+      }
+      double hthm[3];
+      for (int a = 0; a < 3; ++a) hthm[a] = th[a] * std::sqrt(std::abs(scale2 * meq / (mhtot * mag * dt0 + 1e-80)));
+      scale2 = Ly.alpha * Ly.alpha_scale[n] * scale2;
+      if (iter == 1 && type < 0) {
+        for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+        mag = Ly.mag[id][n];
+      }
+      for (int a = 0; a < 3; ++a) h[a] = hn[a] + hthm[a];
+      cross(m, h, t);
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      if (y2 > em * Ly.ms[n] * Ly.ms[n]) em = y2 / (Ly.ms[n] * Ly.ms[n]);
+      for (int a = 0; a < 3; ++a) d[a] = (meq * htot[a] - mag * m[a]) * (1.0 - std::exp(scale1 * scale2));
+      double w[3], r[3];
+      for (int a = 0; a < 3; ++a) w[a] = mag * m[a] + d[a];
+      cross(w, h, r);
+      for (int a = 0; a < 3; ++a) d[a] = d[a] + 2.0 * scale1 * r[a];
+      for (int a = 0; a < 3; ++a) o[a] = mag * m[a] + d[a];
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * o[a];
+      norm_tot();
+      meq = bsl(y * mhtot);
+      if (Ly.garanin_tau) {
+        const double sig_p = meq / (y * mhtot * dbsl(y * mhtot) + 1e-80);
+        scale2 = 2.0 * sig_p / y;
+      } else {
+        scale2 = lambdam;
+      }
+      scale2 = Ly.alpha * Ly.alpha_scale[n] * scale2;
+      for (int a = 0; a < 3; ++a) d[a] = d[a] + (meq * htot[a] - o[a]) * (1.0 - std::exp(scale1 * scale2));
+      em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    } else {
+      const double scale11 = 2.0 * scale1;
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) m[a] = mnext[a];
+        mag = magn;
+        if (mag <= 0.0) {
+          mag = 0.0;
+          y = std::sqrt(hn[0] * hn[0] + hn[1] * hn[1] + hn[2] * hn[2]);
+          if (y != 0.0)
+            for (int a = 0; a < 3; ++a) m[a] = hn[a] / y;
+        }
+      }
+      for (int a = 0; a < 3; ++a) htot[a] = hn[a] + lambdam * mag * m[a];
+      norm_tot();
+      y = y * mhtot;
+      meq = bsl(y);
+      if (Ly.garanin_tau) {
+        y = meq / (y * dbsl(y) + 1e-66);
+        scale2 = 2.0 * T * y / (gmub_kb * sp);
+      } else {
+        scale2 = lambdam;
+      }
+      y = std::abs(scale2 * meq / (mhtot * mag + 1e-66));
+      for (int a = 0; a < 3; ++a) h[a] = hn[a] + th[a] * std::sqrt(std::abs(y / dt0));
+      scale2 = scale2 * Ly.alpha * Ly.alpha_scale[n];
+      double mmg[3], r[3];
+      for (int a = 0; a < 3; ++a) mmg[a] = m[a] * mag;
+      cross(mmg, h, r);
+      for (int a = 0; a < 3; ++a) d[a] = scale11 * (r[a] + (mmg[a] - meq * htot[a]) * scale2);
+      if (iter == 1) {
+        for (int a = 0; a < 3; ++a) d[a] = 0.5 * (d[a] + Ly.dm[3 * n + a]);
+      } else {
+        for (int a = 0; a < 3; ++a) Ly.dm[3 * n + a] = d[a];
+      }
+      cross(m, h, t);
+      const double y2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+      if (y2 > em * Ly.ms[n] * Ly.ms[n]) em = y2 / (Ly.ms[n] * Ly.ms[n]);
+      em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      for (int a = 0; a < 3; ++a) m[a] = mcur[a];
+      mag = Ly.mag[id][n];
+    }
+    for (int a = 0; a < 3; ++a) o[a] = m[a] * mag + d[a];
+    double e = std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    if (e > 0.0) {
+      for (int a = 0; a < 3; ++a) mnext[a] = o[a] / e;
+    } else {
+      e = 0.0;
+      for (int a = 0; a < 3; ++a) mnext[a] = -m[a];
+    }
+    magn = e;
+    mm += magn * Ly.vol[n];
+  }
+  *errmx_l = em;
+  *errmx1_l = em1;
+  *mmag1 = mm;
+}
+
 // push_llg (llg.f90:1066-1155): one stage for one layer.
 // Heun (type -3) branch :1122-1139, Boris/semi-implicit (|type|=2) :1109-1118.
 static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l,
@@ -1413,6 +1553,8 @@ static void push_passes(Sim* s, double dt, int type, double* errmx, double* errm
       double e0, e1, m1;
       if (s->L[l].llb && s->L[l].mode == 1)
         push_mt(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
+      else if (s->L[l].llb && s->L[l].mode == 2)
+        push_zhang(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
       else if (s->L[l].llb)
         push_llb(s, l, type, iter, dt * dt_s, dt, &e0, &e1, &m1);
       else
@@ -1934,13 +2076,13 @@ int orc_set_temp_function(void* h, int l, int func, double t_start, double t_end
   return 0;
 }
 
-// MT on layer l (mrm_gpu_set_mt's arguments; lam_ms NULL: off)
-int orc_set_mt(void* h, int l, double spin, const double* lam_ms, int meq_bs, int garanin_tau) {
+// MT (mode 1) or Zhang (mode 2) on layer l (mrm_gpu_set_mt's arguments; lam_ms NULL: off)
+int orc_set_mt(void* h, int l, double spin, const double* lam_ms, int meq_bs, int garanin_tau, int mode) {
   Sim* s = static_cast<Sim*>(h);
   if (l < 0 || l >= s->nl) return 1;
   Layer& Ly = s->L[l];
   Ly.llb = lam_ms != nullptr;
-  Ly.mode = 1;
+  Ly.mode = mode;
   if (!lam_ms) return 0;
   Ly.spin = spin;
   Ly.meq_bs = meq_bs;

@@ -58,7 +58,7 @@ def lib():
         L.orc_set_field_table.argtypes = [vp, i, i, i, P(d), P(d), P(d), d, d, d, d, d, d, d]
         L.orc_set_window.argtypes = [vp, i, i, d, d, d, d]
         L.orc_set_llb.argtypes = [vp, i, d, P(d), P(d)]
-        L.orc_set_mt.argtypes = [vp, i, d, P(d), i, i]
+        L.orc_set_mt.argtypes = [vp, i, d, P(d), i, i, i]
         L.orc_set_temp_profile.argtypes = [vp, i, d, d, d, d, i, d, d, d, d, d, d, d]
         L.orc_set_temp_function.argtypes = [vp, i, i] + [d] * 12
         L.orc_get_temp.argtypes = [vp, i, P(d)]
@@ -245,6 +245,9 @@ class OracleSim:
             mt = getattr(lay, "mt", None)
             if mt:
                 self.set_mt(l, **mt)
+            zh = getattr(lay, "zhang", None)
+            if zh:
+                self.set_mt(l, **zh, mode=2)
             tp = getattr(lay, "temp_profile", None)
             if tp:
                 self.set_temp_profile(l, **tp)
@@ -321,13 +324,14 @@ class OracleSim:
         self._keep += [t, lm]
         assert lib().orc_set_llb(self.h, layer, float(spin), _p(t), _p(lm)) == 0
 
-    def set_mt(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False):
-        """MT integrator on `layer` (GpuSim.set_mt's arguments)."""
+    def set_mt(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False, mode=1):
+        """MT (mode 1) or Zhang (mode 2) integrator on `layer` (GpuSim.set_mt's arguments)."""
         if lambda_ms is None:
-            assert lib().orc_set_mt(self.h, layer, 0.0, None, 0, 0) == 0
+            assert lib().orc_set_mt(self.h, layer, 0.0, None, 0, 0, mode) == 0
             return
         lm = f64(lambda_ms)
-        assert lib().orc_set_mt(self.h, layer, float(spin), _p(lm), int(bool(meq_bs)), int(bool(garanin_tau))) == 0
+        assert lib().orc_set_mt(self.h, layer, float(spin), _p(lm), int(bool(meq_bs)), int(bool(garanin_tau)),
+                                mode) == 0
 
     def set_temp_profile(self, layer, background, dtemp, sigma=(0.0, 0.0), expn=1, vel=(0.0, 0.0),
                          offset=(None, None), ref=(0.0, 0.0), t_origin=0.0, time=None):

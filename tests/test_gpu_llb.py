@@ -61,6 +61,19 @@ def test_mt_fp64(oracle, gpulib, meq_bs, garanin_tau, llg_type):
     orc.close()
 
 
+@pytest.mark.parametrize("meq_bs,garanin_tau", [(False, False), (True, True)])
+@pytest.mark.parametrize("llg_type", [-3, 2, -2])
+def test_zhang_fp64(oracle, gpulib, meq_bs, garanin_tau, llg_type):
+    med = media.zhang_medium(16, seed=8, meq_bs=meq_bs, garanin_tau=garanin_tau)
+    orc, gpu = _pair(oracle, med, FP64)
+    orc.step(500, 1e-14, llg_type=llg_type)
+    gpu.step(500, 1e-14, llg_type=llg_type)
+    assert np.abs(gpu.get_state(0) - orc.get_state(0)).max() < 1e-9
+    assert np.abs(gpu.get_mag(0) - orc.get_mag(0)).max() < 1e-9
+    gpu.close()
+    orc.close()
+
+
 def test_llb_trajectory_fp32(oracle, gpulib):
     # the LLB push runs in FP64 arithmetic on FP32 state; FP32 runs draw their
     # noise from the 32-bit Philox stream, so the comparison runs without noise

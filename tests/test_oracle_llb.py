@@ -115,12 +115,15 @@ def _bs(x, s):
     return b
 
 
+@pytest.mark.parametrize("kind", ["mt", "zhang"])
 @pytest.mark.parametrize("meq_bs", [False, True])
 @pytest.mark.parametrize("llg_type", [-3, 2, -2])
-def test_mt_relaxes_to_mean_field(oracle, meq_bs, llg_type):
-    # push_mt (llg.f90:735-915) without field or noise: |m| decays to the
-    # equilibrium m = L(y lambda_m m) (Langevin) or B_S(y lambdaMs m) (Brillouin)
-    med = media.mt_medium(8, tc=700.0, tc_sigma=0.0, temperature=560.0, meq_bs=meq_bs)
+def test_mt_relaxes_to_mean_field(oracle, kind, meq_bs, llg_type):
+    # push_mt (llg.f90:735-915) and push_zhang (:410-703) without field or
+    # noise: |m| decays to the equilibrium m = L(y lambda_m m) (Langevin) or
+    # B_S(y lambdaMs m) (Brillouin)
+    make = media.mt_medium if kind == "mt" else media.zhang_medium
+    med = make(8, tc=700.0, tc_sigma=0.0, temperature=560.0, meq_bs=meq_bs)
     for lay in med.layers:
         lay.scale = 0.0
         lay.hk[:] = 0.0
@@ -128,7 +131,7 @@ def test_mt_relaxes_to_mean_field(oracle, meq_bs, llg_type):
         lay.thermal = False
     orc = oracle.OracleSim(med, demag=False)
     orc.step(4000, 1e-14, llg_type=llg_type)
-    lms = med.layers[0].mt["lambda_ms"][0]
+    lms = (med.layers[0].mt or med.layers[0].zhang)["lambda_ms"][0]
     y = GMUB_KB * 0.5 / 560.0
     if meq_bs:
         b0, b1 = 0.0, 1.0
