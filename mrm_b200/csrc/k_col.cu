@@ -85,7 +85,7 @@ template <typename R>
 static cudaError_t row_allow_any(int v, const size_t* smem6) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int g = 0; g < 2; ++g)
+  for (int g = 0; g < 3; ++g)
     for (int q = 0; q < kRowSlots; ++q) {
       cudaError_t e = allow_smem(o->fn[g][q], smem6[q]);
       if (e != cudaSuccess) return e;
@@ -103,7 +103,7 @@ template <typename R>
 static cudaError_t row_load_any(int v) {
   const RowOps* o = row_ops_of<R>(v);
   if (!o) return cudaErrorInvalidValue;
-  for (int g = 0; g < 2; ++g)
+  for (int g = 0; g < 3; ++g)
     for (int q = 0; q < kRowSlots; ++q) {
       cudaFuncAttributes fa;
       cudaError_t e = cudaFuncGetAttributes(&fa, o->fn[g][q]);

@@ -183,6 +183,9 @@ MRM_D void tab_value(const double* __restrict__ v, int tnx, TabW wx, TabW wy, do
 }
 
 // ---------------- LLB integrator (llgp%llb) ----------------
+// (The integrators below are calls, not inlined: their FP64 state would
+// otherwise share the general row kernel's register budget and spill on its
+// common paths.)
 constexpr double kGmubKb = 1.343427768e-4;  // g mu_B / k_B (llg.f90:924)
 constexpr double kBoltz = 1.380662e-16;     // field.f90:407
 
@@ -208,7 +211,7 @@ MRM_D double llb_dlv(double x) {
 struct LlbStep {
   double m[3], mag, d[3], d2, tq2;
 };
-MRM_D LlbStep llb_heun(bool corr, const double* mc, double magc, const double* mpr, double magp, const double* h,
+static __device__ __noinline__ LlbStep llb_heun(bool corr, const double* mc, double magc, const double* mpr, double magp, const double* h,
                        const double* ht, const double* d1, double ab, double tc, double lam, const LlbDev& P,
                        double T, double gamma, double dt) {
   LlbStep o;
@@ -297,7 +300,7 @@ MRM_D LlbStep llb_heun(bool corr, const double* mc, double magc, const double* m
 // predicted state mpr, magp).  dt is the pass's step (dt/2 for the first pass
 // of -2).  Out: the new direction and magnitude, |dm|^2 as errmx1 forms it,
 // |m x h|^2.  (|m| = 0: llb_heun's branch, the same for both pushes.)
-MRM_D LlbStep llb_boris(bool first, const double* mc, double magc, const double* mpr, double magp, const double* h,
+static __device__ __noinline__ LlbStep llb_boris(bool first, const double* mc, double magc, const double* mpr, double magp, const double* h,
                         const double* ht, double ab, double tc, double lam, const LlbDev& P, double T, double gamma,
                         double dt) {
   LlbStep o;
@@ -394,7 +397,7 @@ MRM_D double mt_dbs(double x, double sp) {
 // thermal; ht the thermal field / sqrt(dt); d1 the first pass's increment
 // (Heun); ab = alpha alpha_scale; lam = lambdaMs; T the temperature; dt the
 // pass's step.  Out as llb_heun.
-MRM_D LlbStep mt_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr, double magp,
+static __device__ __noinline__ LlbStep mt_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr, double magp,
                       const double* h, const double* ht, const double* d1, double ab, double lam0, const LlbDev& P,
                       double T, double gamma, double dt, double dt0) {
   LlbStep o;
@@ -505,7 +508,7 @@ MRM_D LlbStep mt_step(bool boris, bool first, bool corr, const double* mc, doubl
 // the semi-implicit |type| = 2 branch (:428-510), arguments as mt_step.  The
 // thermal field joins the precession with the variance scale2 meq/(|H| |m|)
 // (no separate eta).
-MRM_D LlbStep zhang_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr,
+static __device__ __noinline__ LlbStep zhang_step(bool boris, bool first, bool corr, const double* mc, double magc, const double* mpr,
                          double magp, const double* h, const double* ht, const double* d1, double ab, double lam0,
                          const LlbDev& P, double T, double gamma, double dt, double dt0) {
   LlbStep o;
@@ -729,9 +732,12 @@ MRM_HD int row_fft_smem(int lgpx, int rpb) {
 //                  stage, forward row FFT of Ms*m* / Ms*m_{n+1}
 //   kEval: inverse row FFT and field assembly only (H_demag and h stored)
 // stage_cap: bytes of dynamic shared memory available for grain staging.
-// GEN: the general instantiation (semi-implicit pushes, write head); the other
-// one is Heun without a head, with those paths compiled out.
-template <typename R, int STAGE, bool STATS, int RPB, int BLOCK, int MINB, int LGMAX, bool GEN>
+// GEN: 0 Heun without a head (the general paths compiled out); 1 the general
+// instantiation (semi-implicit pushes, write heads, field tables, cubic
+// anisotropy, windows); 2 the general one with the LLB / MT / Zhang
+// integrators and temperature profiles as well (kept apart: their FP64 code
+// would share level 1's register budget and spill on its paths).
+template <typename R, int STAGE, bool STATS, int RPB, int BLOCK, int MINB, int LGMAX, int GEN>
 __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __restrict__ runs,
                                                           const Task* __restrict__ tasks,
                                                           const Cx<R>* __restrict__ twg, int istep,
@@ -950,7 +956,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
   const double t_stage = (STAGE == kCorr) ? t_now + (mid ? 0.5 * rd.dt : rd.dt) : t_now;
   const double sc = ramp(L, t_stage);
-  const double tps = (GEN && L.tprof) ? L.tprof->dtemp * temp_scale(*L.tprof, t_stage) : 0.0;
+  const double tps = (GEN == 2 && L.tprof) ? L.tprof->dtemp * temp_scale(*L.tprof, t_stage) : 0.0;
   // a layer's field is its uniform direction or its tabulated profile, scaled
   const R hax = ftab ? (R)0 : (R)(sc * L.hdir[0]), hay = ftab ? (R)0 : (R)(sc * L.hdir[1]),
           haz = ftab ? (R)0 : (R)(sc * L.hdir[2]);
@@ -1140,7 +1146,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     }
 
     // the grain's temperature: the layer's, or its profile's at the stage's time
-    const double Tg = (GEN && L.tprof) ? temp_cell(*L.tprof, tps, t_stage, wi0 + i, wj0 + row0 + rr) : L.temperature;
+    const double Tg = (GEN == 2 && L.tprof) ? temp_cell(*L.tprof, tps, t_stage, wi0 + i, wj0 + row0 + rr) : L.temperature;
     // thermal field / sqrt(dt) (llg.f90:1083): drawn by the predictor from the
     // step counter, reused by the corrector (:1262-1266)
     R htx = 0, hty = 0, htz = 0;
@@ -1150,8 +1156,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         // the grain's stream (one per grain, shared by its cells)
         const int nt = L.cgrain ? max(0, L.cgrain[n]) : n;
         thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)nt, gn);
-        R s = (GEN && L.tprof) ? (R)((double)pb.w * sqrt(Tg / rd.dt)) : pb.w * tfac;
-        if (GEN && L.llb && (double)mf.w != 1.0) {
+        R s = (GEN == 2 && L.tprof) ? (R)((double)pb.w * sqrt(Tg / rd.dt)) : pb.w * tfac;
+        if (GEN == 2 && L.llb && (double)mf.w != 1.0) {
           // get_thermal with |m| != 1 (field.f90:416-417): the variance over
           // max(floor_ms, |m|) instead of max(floor_ms, ms_scale)
           const LlbDev& P = *L.llb;
@@ -1172,7 +1178,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     V4<R> mn;
     R dx = 0, dy = 0, dz = 0, tq2 = 0;
     double d2x = -1.0;  // errmx1's |dm|^2 where it is not |d|^2 (LLB)
-    const bool llb = GEN && L.llb != nullptr;
+    const bool llb = GEN == 2 && L.llb != nullptr;
     if (llb) {
       // push_llb (llg.f90:916-1064), Heun, in FP64; |m| in the w lane
       const LlbDev& P = *L.llb;

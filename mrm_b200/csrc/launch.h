@@ -43,9 +43,10 @@ struct RowLaunch;
 // entry points of one compiled row shape (defined in its own translation unit)
 struct RowOps {
   cudaError_t (*launch)(int stage, bool stats, const RowLaunch& a, int istep, int flags);
-  // [general][slot]: slots kInit, kPred, kCorr, kCorr with reductions, kEval,
-  // kPred with reductions; general: semi-implicit pushes and the write head
-  const void* fn[2][6];
+  // [level][slot]: slots kInit, kPred, kCorr, kCorr with reductions, kEval,
+  // kPred with reductions; level 0 fast, 1 general, 2 general with the
+  // LLB / MT / Zhang integrators (row_kernel's GEN)
+  const void* fn[3][6];
 };
 template <typename R, int V>
 const RowOps& row_ops();
@@ -61,7 +62,8 @@ struct RowLaunch {
   size_t smem;
   int stage_cap;
   bool pdl;          // programmatic stream serialization with the previous kernel
-  bool gen;          // the general instantiation (needed for llg_type 2/-2 and write heads)
+  int gen;           // the instantiation level (row_kernel's GEN: 1 for llg_type 2/-2, write heads ...,
+                     // 2 with the LLB / MT / Zhang integrators)
 };
 
 struct ColLaunch {

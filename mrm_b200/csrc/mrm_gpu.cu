@@ -149,8 +149,8 @@ struct Engine {
   bool has_head = false;             // a run has a layer under the write head or a tabulated
                                      // field profile (general kernels)
   bool has_cubic = false;            // a run has a cubic-anisotropy layer (general kernels)
-  bool has_llb = false;              // a run integrates with LLB / MT or has a temperature profile
-                                     // (general kernels)
+  bool has_llb = false;              // a run integrates with LLB / MT / Zhang (the level-2 kernels)
+  bool has_tprof = false;            // a run has a temperature profile (the level-2 kernels)
   bool pred_stored = false;          // next chunk's first predictor pushes with the stored field
   bool mapped = false;               // a run has grains of several cells (grain-averaged demag)
   double* d_part = nullptr;
@@ -632,6 +632,7 @@ int build_tables(Engine* e) {
   e->has_head = false;
   e->has_cubic = false;
   e->has_llb = false;
+  e->has_tprof = false;
   e->mapped = false;
   bool karlqvist_head = false;
   for (auto* r : e->runs)
@@ -639,7 +640,8 @@ int build_tables(Engine* e) {
       karlqvist_head = karlqvist_head || r->L[l].func == kFuncHead;
       e->has_head = e->has_head || r->L[l].func == kFuncHead || r->L[l].tab != nullptr;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
-      e->has_llb = e->has_llb || r->L[l].llb != nullptr || r->L[l].tprof != nullptr;
+      e->has_llb = e->has_llb || r->L[l].llb != nullptr;
+      e->has_tprof = e->has_tprof || r->L[l].tprof != nullptr;
       e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
   if (e->mapped && karlqvist_head)
@@ -704,7 +706,7 @@ template <typename R>
 cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags, bool pdl = true) {
   if (!e->nrt) return cudaSuccess;
   // the general kernels for the semi-implicit pushes and write heads
-  const bool gen = (flags & kFlagBoris) || e->has_head || e->has_cubic || e->has_window || e->has_llb;
+  const int gen = (e->has_llb || e->has_tprof) ? 2 : ((flags & kFlagBoris) || e->has_head || e->has_cubic || e->has_window);
   if (stats) {
     const int i = stage == kPred ? 0 : 1;
     RowLaunch a{e->st, e->d_runs, e->d_stasks, e->d_tw, e->d_part, e->d_err, e->nst, e->smem_stats[i],
