@@ -60,7 +60,7 @@ WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
 # DRAM traffic per launch of each kernel in bytes per grain of the launch, for
 # the headline batch with its tuned shapes (ncu capture summarised in
 # profiles/batched_32x65536_launch_list.md)
-NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 139.2, "col": 69.3, "row_corr": 167.4}
+NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 140.6, "col": 70.2, "row_corr": 166.4}
 
 
 def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4) -> dict:
