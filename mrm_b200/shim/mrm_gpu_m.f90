@@ -13,7 +13,7 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_zhang, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_zhang, gpu_set_temp_profile, gpu_set_temp_function, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -130,6 +130,20 @@ module mrm_gpu_m
       integer(C_INT), value :: layer, meq_bs, garanin_tau
       real(C_DOUBLE), value :: spin
       real(C_DOUBLE), intent(in) :: lambda_ms(*)
+    end function
+    integer(C_INT) function c_set_temp_profile(h, layer, bg, dtemp, sx, sy, expn, vx, vy, ox, oy, rx, ry, t0) &
+        bind(C, name="mrm_gpu_set_temp_profile")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, expn
+      real(C_DOUBLE), value :: bg, dtemp, sx, sy, vx, vy, ox, oy, rx, ry, t0
+    end function
+    integer(C_INT) function c_set_temp_function(h, layer, func, t_start, t_end, s_start, s_end, amp, gamma, phase, &
+                                                param, duty, moddepth, dc, scale) bind(C, name="mrm_gpu_set_temp_function")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, func
+      real(C_DOUBLE), value :: t_start, t_end, s_start, s_end, amp, gamma, phase, param, duty, moddepth, dc, scale
     end function
     integer(C_INT) function c_set_mag(h, layer, mag) bind(C, name="mrm_gpu_set_mag")
       import :: C_INT, C_PTR, C_DOUBLE
@@ -347,6 +361,26 @@ contains
     logical, intent(in) :: meq_bs, garanin_tau
     ok_p = ok(c_set_zhang(h, int(layer - 1, C_INT), spin, lambda_ms, merge(1_C_INT, 0_C_INT, meq_bs), &
                           merge(1_C_INT, 0_C_INT, garanin_tau)))
+  end function
+  ! suprgaus_temp + ref_temp of `layer` (include/mrm_gpu.h mrm_gpu_set_temp_profile):
+  ! background_t, dtemp, sigma (cm, 0: flat), the exponent as suprgaus_temp takes
+  ! it, fld%vel_x/y, %offset_x/y, %ref_x/y, %t_origin
+  logical function gpu_set_temp_profile(h, layer, background, dtemp, sigma, expn, vel, offset, ref, t_origin) &
+      result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer, expn
+    real(C_DOUBLE), intent(in) :: background, dtemp, sigma(2), vel(2), offset(2), ref(2), t_origin
+    ok_p = ok(c_set_temp_profile(h, int(layer - 1, C_INT), background, dtemp, sigma(1), sigma(2), int(expn, C_INT), &
+                                 vel(1), vel(2), offset(1), offset(2), ref(1), ref(2), t_origin))
+  end function
+  ! set_temp's time scale of that profile (include/mrm_gpu.h mrm_gpu_set_temp_function)
+  logical function gpu_set_temp_function(h, layer, func, t_start, t_end, s_start, s_end, amp, gamma, phase, param, &
+                                         duty, moddepth, dc, scale) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer, func
+    real(C_DOUBLE), intent(in) :: t_start, t_end, s_start, s_end, amp, gamma, phase, param, duty, moddepth, dc, scale
+    ok_p = ok(c_set_temp_function(h, int(layer - 1, C_INT), int(func, C_INT), t_start, t_end, s_start, s_end, amp, &
+                                  gamma, phase, param, duty, moddepth, dc, scale))
   end function
   logical function gpu_set_mag(h, layer, mag) result(ok_p)
     type(C_PTR), intent(in) :: h
