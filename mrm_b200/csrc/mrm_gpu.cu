@@ -111,6 +111,9 @@ struct mrm_gpu {
   // velocity and offset (window%v, window%offset), its current origin (-1: not
   // placed yet); frz: the run's first frozen-grain stats record
   int wnx = 0, wny = 0, wi0 = -1, wj0 = -1, frz = -1;
+  // the grid's own FFT exceeds the path's limits: no full-grid spectra or
+  // tensor; demag only through a moving window
+  bool fft_big = false;
   double wvx = 0, wvy = 0, wox = 0, woy = 0;
   // the time as llg() accumulates it (t = t + dt, llg.f90:268), which places
   // the window: t_base + k dt can differ from it in the last bit, and a window
@@ -379,7 +382,9 @@ size_t col_smem_of(const mrm_gpu* r, int nc, int minb) {
 
 // The geometry must run with the most economical shapes (one row per row
 // task, one column per column task, no staging).
-int validate_geom(const mrm_geom* g, std::string* errp) {
+// big (optional): set instead of failing when the grid's own FFT exceeds the
+// path's limits (a handle that computes demag through a moving window only)
+int validate_geom(const mrm_geom* g, std::string* errp, bool* big = nullptr) {
   if (!g) return set_err(errp, MRM_ERR_ARG, "geometry is NULL");
   if (g->nx < 2 || g->ny < 2) return set_err(errp, MRM_ERR_ARG, "nx, ny must be >= 2");
   if (g->n_lay < 1 || g->n_lay > MRM_MAX_LAYERS)
@@ -396,6 +401,11 @@ int validate_geom(const mrm_geom* g, std::string* errp) {
                    "periodic demag needs power-of-two nx, ny on this path (got %d x %d)", g->nx, g->ny);
   int px, py;
   fft_grid(*g, &px, &py);
+  if (big) *big = false;
+  if ((px > kTwN || py > kTwN) && big && px >= 4 && py >= 2) {
+    *big = true;
+    return MRM_OK;
+  }
   if (px > kTwN || py > kTwN || px < 4 || py < 2)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d outside 4..%d", px, py, kTwN);
   mrm_gpu tmp;
@@ -1201,11 +1211,11 @@ int spectra_alloc(mrm_gpu* r) {
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
-  int rc = spectra_alloc(r);
+  int rc = r->fft_big ? MRM_OK : spectra_alloc(r);
   if (rc) return rc;
   rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
   if (rc) return rc;
-  rc = dmalloc(errp, &r->tens, tensor_bytes(r));
+  rc = r->fft_big ? MRM_OK : dmalloc(errp, &r->tens, tensor_bytes(r));
   if (rc) return rc;
   const size_t n = (size_t)r->g.nx * r->g.ny;
   for (int l = 0; l < r->nl; ++l) {
@@ -1257,8 +1267,9 @@ int64_t footprint(const mrm_geom& g) {
   return b;
 }
 
-mrm_gpu* new_run(Engine* e, const mrm_geom* g, std::string* errp, int* rc) {
-  *rc = validate_geom(g, errp);
+mrm_gpu* new_run(Engine* e, const mrm_geom* g, std::string* errp, int* rc, bool allow_big = false) {
+  bool big = false;
+  *rc = validate_geom(g, errp, allow_big ? &big : nullptr);
   if (*rc) return nullptr;
   if (g->precision != e->prec) {
     *rc = set_err(errp, MRM_ERR_ARG, "run precision differs from the batch precision");
@@ -1269,6 +1280,7 @@ mrm_gpu* new_run(Engine* e, const mrm_geom* g, std::string* errp, int* rc) {
   r->eng = e;
   r->g = *g;
   r->nl = g->n_lay;
+  r->fft_big = big;
   fft_grid(*g, &r->px, &r->py);
   r->lgpx = ilog2(r->px);
   r->lgpy = ilog2(r->py);
@@ -1636,7 +1648,8 @@ extern "C" {
 int mrm_gpu_create(const mrm_geom* geom, int device, mrm_gpu** out) {
   if (!out) return MRM_ERR_ARG;
   *out = nullptr;
-  int rc = validate_geom(geom, &g_create_err);
+  bool big = false;  // (new_run marks such a handle)
+  int rc = validate_geom(geom, &g_create_err, &big);
   if (rc) return rc;
   Engine* e = new Engine();
   rc = engine_init(e, geom->precision, device);
@@ -1646,7 +1659,7 @@ int mrm_gpu_create(const mrm_geom* geom, int device, mrm_gpu** out) {
     delete e;
     return rc;
   }
-  mrm_gpu* r = new_run(e, geom, &g_create_err, &rc);
+  mrm_gpu* r = new_run(e, geom, &g_create_err, &rc, true);  // (a long track demagnetises through a window)
   if (!r) {
     engine_free(e);
     delete e;
@@ -1894,9 +1907,12 @@ int mrm_gpu_off_field(mrm_gpu* h, double zoff, double dzobs, double head_mu, dou
   return finish(MRM_OK);
 }
 
+static int need_fft(mrm_gpu* h);
+
 int mrm_gpu_build_tensor(mrm_gpu* h) {
   if (!h) return MRM_ERR_ARG;
   std::string* errp = &h->err;
+  if (int rc = need_fft(h)) return rc;
   CK(cudaSetDevice(h->eng->dev));
   void* d_n2d = nullptr;
   const size_t bytes = sizeof(double) * 9 * (size_t)h->nl * h->nl * h->px * h->py;
@@ -1911,6 +1927,7 @@ int mrm_gpu_build_tensor(mrm_gpu* h) {
 int mrm_gpu_upload_tensor(mrm_gpu* h, const double* n2d, int nx_fft, int ny_fft) {
   if (!h || !n2d) return MRM_ERR_ARG;
   std::string* errp = &h->err;
+  if (int rc = need_fft(h)) return rc;
   if (nx_fft != h->px || ny_fft != h->py)
     return set_err(errp, MRM_ERR_ARG, "tensor grid %dx%d differs from the FFT grid %dx%d", nx_fft, ny_fft, h->px, h->py);
   CK(cudaSetDevice(h->eng->dev));
@@ -2423,6 +2440,7 @@ static int place_window(mrm_gpu* h, int i0, int j0);
 
 int mrm_gpu_eval_field(mrm_gpu* h, double t, int layer, double* hdemag) {
   if (!h) return MRM_ERR_ARG;
+  if (int rc = need_fft(h)) return rc;
   std::string* errp = &h->err;
   if (layer < 0 || layer >= h->nl) return set_err(errp, MRM_ERR_ARG, "layer %d out of range", layer);
   for (int l = 0; l < h->nl; ++l)
@@ -2508,8 +2526,17 @@ static int place_window(mrm_gpu* h, int i0, int j0) {
   return MRM_OK;
 }
 
+// a grid whose own FFT exceeds the path's limits computes through a window only
+static int need_fft(mrm_gpu* h) {
+  if (h->fft_big && !h->wnx)
+    return set_err(&h->err, MRM_ERR_UNSUPPORTED,
+                   "the grid's FFT (%d x %d) exceeds the path's limits: set a moving demag window", h->px, h->py);
+  return MRM_OK;
+}
+
 static int plain_prepare(mrm_gpu* h, int nsteps, double dt, int llg_type) {
   std::string* errp = &h->err;
+  if (int rc = need_fft(h)) return rc;
   if (nsteps < 0) return set_err(errp, MRM_ERR_ARG, "nsteps must be >= 0");
   if (!(dt > 0)) return set_err(errp, MRM_ERR_ARG, "dt must be > 0");
   if (!llg_type_ok(llg_type))
@@ -2589,6 +2616,8 @@ int mrm_gpu_set_window(mrm_gpu* h, int nx_win, int ny_win, double vx, double vy,
   if (nx_win < 2 || ny_win < 2 || nx_win > h->g.nx || ny_win > h->g.ny)
     return set_err(errp, MRM_ERR_ARG, "window %d x %d outside 2 .. %d x %d", nx_win, ny_win, h->g.nx, h->g.ny);
   const bool none = nx_win == h->g.nx && ny_win == h->g.ny;  // update_do_grain: the whole grid (data.f90:127)
+  if (none && h->fft_big)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "the grid's own FFT exceeds the path's limits: keep a window");
   mrm_geom gw = h->g;
   gw.nx = nx_win;
   gw.ny = ny_win;
@@ -3169,7 +3198,8 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   if (!m || !hdemag) return set_err(errp, MRM_ERR_ARG, "m and hdemag must be device pointers");
   if (h->g.precision != MRM_FP32)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes MRM_FP32 handles");
-  if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation has no moving window");
+  if (h->wnx || h->fft_big)
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation has no moving window");
   for (int l = 0; l < h->nl; ++l)
     if (h->L[l].cgrain)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes one grain per cell");

@@ -102,3 +102,27 @@ def test_window_refusals(gpulib):
     with pytest.raises(MrmError):
         r.set_window(8, 8)
     b.close()
+
+
+def test_window_long_track(oracle, gpulib):
+    # a 4096-column track, whose own FFT (8192 wide) exceeds the path's limits,
+    # computes through a 64-column window that follows the tabulated head
+    # (the head starts 100 cells in, the window centred on it: origin 67 at
+    # t = 0, about 29 cells further after the 500 steps)
+    med = media.table_write_medium(4096, 8, seed=4, temperature=0.0, velocity_cm_s=4e5, bit_nm=280.0)
+    for lay in med.layers:
+        lay.field_table["offset"] = (100 * med.dx, None)
+    med.window = dict(nx=64, ny=8, v=(4e5, 0.0), offset=(-1948 * med.dx, 0.0))
+    orc, gpu = _pair(oracle, med, FP64)
+    assert gpu.get_window()[2] == 67
+    for chunk in range(2):
+        orc.step(250, 1e-13)
+        gpu.step(250, 1e-13)
+        assert gpu.get_window() == orc.get_window(), chunk
+        for l in range(2):
+            assert np.abs(gpu.get_state(l) - orc.get_state(l)).max() < 1e-9, (chunk, l)
+    assert orc.get_window()[2] >= 90
+    _close(orc, gpu)
+    med.window = None
+    with pytest.raises(MrmError):  # no window: no demag on this grid
+        GpuSim(med, precision=FP64)
