@@ -156,3 +156,16 @@ def test_table_write_medium_runs(oracle):
     ha = orc.get_applied(0)
     assert np.abs(ha).max() > 1000.0
     orc.close()
+
+
+def test_scalar_field_file(tmp_path):
+    # file_applied with nval = 1 (a temperature table): records `x y value`,
+    # x fastest, no axis mapping, scaled
+    p = tmp_path / "temp.dat"
+    p.write_text('TITLE = "T"\nZONE I=3, J=2\n'
+                 "-1e-6 0 10\n0 0 20\n1e-6 0 30\n"
+                 "-1e-6 2e-6 40\n0 2e-6 50\n1e-6 2e-6 60\n")
+    xp, yp, v = formats.read_field_file(str(p), nval=1, scale=0.5)
+    np.testing.assert_array_equal(xp, [-1e-6, 0.0, 1e-6])
+    np.testing.assert_array_equal(yp, [0.0, 2e-6])
+    np.testing.assert_array_equal(v, [[5, 10, 15], [20, 25, 30]])
