@@ -397,8 +397,12 @@ int mrm_device_memory(int device, int64_t* free_bytes, int64_t* total_bytes);
  * init_demag); it exists for hosts that must not allocate device memory
  * while they run, e.g. under a stream-ordered pool or a caching allocator.
  *   h       an MRM_FP32 handle with every layer uploaded and a tensor built or
- *           uploaded (its tensor, parameters and twiddles are read, nothing of
- *           the handle is written);
+ *           uploaded (its tensor, parameters and twiddles are read; the one
+ *           thing of the handle that is written is its device error word: a
+ *           kernel of the call that fails -- a bulk-copy wait that ran out --
+ *           records it there, and the handle's next synchronising call,
+ *           mrm_gpu_check_device for one, reports it after the caller's
+ *           stream has finished the work);
  *   m       device pointer, n_lay x n_grains x 3 floats (each layer's m(3,n));
  *   hdemag  device pointer, same shape: the demagnetising field (Oe);
  *   stream  cudaStream_t to enqueue on (NULL: the handle's stream); the call

@@ -1,0 +1,402 @@
+// colreg.cuh -- register-resident column transform with the tensor product
+// (FP32 runs of one layer, FFT columns of 256..1024 points), sm_100a.
+//
+// The column half of get_demag (src/demag.f90:113-127): for one k_x column
+// of the three M^ half spectra, the forward FFT along y, H^ = N^ M^ with the
+// FP64-built tensor spectrum, and the inverse FFT along y.  One column is
+// transformed by NT = N/8 threads; every thread keeps eight elements of each
+// of the three components in registers through the whole transform:
+//
+//   stage 0 (global -> registers): thread t loads rows t + k NT, k < 8 (the
+//       zero padding of an open boundary, rows >= N/2, is neither loaded nor
+//       transformed), radix-2^R0 butterflies over the top position bits;
+//   stages 1..S-1: radix-8 butterflies, each preceded by an exchange of the
+//       elements through shared memory (one barrier of the column's threads);
+//   after the last forward stage thread t holds positions 8t..8t+7 of the
+//       mixed-radix digit-reversed order (fft.cuh ip_freq) and multiplies them
+//       by the tensor in registers (the tensor is stored in that order);
+//   the inverse stages run in the reverse order (decimation in time) and the
+//       last one writes rows < ny of H^ straight to global memory.
+//
+// Positions, radices and twiddle tables are those of the in-place passes of
+// fft.cuh (the same Cooley-Tukey plan, the same tables), so both column
+// kernels compute the same transform.  Exchange buffer: the three components
+// of a column, N elements each, at swizzled offsets xswz(p).
+#pragma once
+#include "kernels.cuh"
+
+namespace mrm {
+
+constexpr int kCregMinLg = 8, kCregMaxLg = 10;
+
+// Exchange-buffer swizzle in 8-byte elements: bits 0..3 xored with bits 3..6.
+// It is linear over xor, and for every stage's access pattern of a half warp
+// (16 consecutive threads, one register slot) it puts the 16 elements on
+// distinct bank pairs for N = 256 .. 2048 (checked by enumeration).
+MRM_HD constexpr int xswz(int p) { return p ^ ((p >> 3) & 15); }
+
+// Stage plan of an N = 2^LGN point column: S stages; stage 0 has radix
+// 2^R0 over the top R0 position bits, the others radix 8.  In stage s a
+// thread's eight elements differ in the three position bits from dbit(s)
+// (its register digit); the other bits are the thread index.
+template <int LGN>
+struct CregPlan {
+  static constexpr int N = 1 << LGN, NT = N / 8, S = (LGN + 2) / 3, R0 = LGN - 3 * (S - 1);
+  MRM_HD static constexpr int dbit(int s) { return s == 0 ? LGN - 3 : LGN - R0 - 3 * s; }
+  // log2 of the butterfly stride of stage s (the LGNS of its pass table)
+  MRM_HD static constexpr int lgd(int s) { return s == 0 ? LGN - R0 : dbit(s); }
+};
+
+// position of a thread's element 0 in a stage whose register digit starts at bit B
+template <int B>
+MRM_D int creg_base(int t) {
+  return (t & ((1 << B) - 1)) | ((t >> B) << (B + 3));
+}
+
+// forward radix-8 DFT of four inputs (inputs 4..7 are zero)
+MRM_D void dft8_half_in(Cx<float>* v) {
+  const float h = 0.70710678118654752440f;
+  Cx<float> e0 = v[0], e1 = v[1], e2 = v[2], e3 = v[3];
+  Cx<float> o0 = e0, o1 = cmul(e1, Cx<float>{h, -h}), o2 = cmul_i(e2, -1.f), o3 = cmul(e3, Cx<float>{-h, -h});
+  dft4<float, -1>(e0, e1, e2, e3);
+  dft4<float, -1>(o0, o1, o2, o3);
+  v[0] = e0;
+  v[2] = e1;
+  v[4] = e2;
+  v[6] = e3;
+  v[1] = o0;
+  v[3] = o1;
+  v[5] = o2;
+  v[7] = o3;
+}
+
+// The twiddles of a thread's butterflies in stage STAGE (shared by the three
+// components): w[jl * R + m] = e^{-2 pi i j0 m / L} for the radix-R
+// butterfly jl of the thread (one for radix 8; 8/R for a stage 0 of radix 2
+// or 4), m >= 1; none when the stage's stride is 1.
+template <int LGN, int STAGE>
+MRM_D void creg_twiddles(Cx<float> (&w)[8], int t, const Cx<float>* __restrict__ tw) {
+  using P = CregPlan<LGN>;
+  constexpr int LGD = P::lgd(STAGE), D = 1 << LGD, OFF = pass_tw_off(LGN, LGD);
+  constexpr int R = STAGE == 0 ? (1 << P::R0) : 8, NB = 8 / R;
+  if constexpr (D > 1) {
+#pragma unroll
+    for (int jl = 0; jl < NB; ++jl) {
+      const int j0 = STAGE == 0 ? t + (jl << (LGN - 3)) : (t & (D - 1));
+#pragma unroll
+      for (int m = 1; m < R; ++m) w[jl * R + m] = tw[OFF + (m - 1) * D + j0];
+    }
+  }
+}
+
+// Forward stage STAGE (decimation in frequency: butterfly, then twiddles) on
+// one component's eight elements; element k of the register digit is v[k].
+// HALF: positions >= N/2 are zero on input (stage 0).
+template <int LGN, int STAGE, bool HALF>
+MRM_D void creg_fwd(Cx<float> (&v)[8], const Cx<float> (&w)[8]) {
+  using P = CregPlan<LGN>;
+  constexpr int D = 1 << P::lgd(STAGE);
+  if constexpr (STAGE == 0 && P::R0 < 3) {
+    constexpr int R = 1 << P::R0, NB = 8 / R;
+#pragma unroll
+    for (int jl = 0; jl < NB; ++jl) {
+      Cx<float> u[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m) u[m] = v[jl + NB * m];
+      if constexpr (HALF) {
+        if constexpr (R == 4) {
+          const Cx<float> a0 = u[0], a1 = u[1];
+          u[0] = cadd(a0, a1);
+          u[1] = cadd(a0, cmul_i(a1, -1.f));
+          u[2] = csub(a0, a1);
+          u[3] = cadd(a0, cmul_i(a1, 1.f));
+        } else {
+          u[1] = u[0];
+        }
+      } else {
+        if constexpr (R == 4) dft4<float, -1>(u[0], u[1], u[2], u[3]);
+        else dft2<float, -1>(u);
+      }
+#pragma unroll
+      for (int m = 1; m < R; ++m) u[m] = cmul(u[m], w[jl * R + m]);
+#pragma unroll
+      for (int m = 0; m < R; ++m) v[jl + NB * m] = u[m];
+    }
+  } else {
+    if constexpr (STAGE == 0 && HALF) dft8_half_in(v);
+    else dft8<float, -1>(v);
+    if constexpr (D > 1) {
+#pragma unroll
+      for (int m = 1; m < 8; ++m) v[m] = cmul(v[m], w[m]);
+    }
+  }
+}
+
+// Inverse stage STAGE (decimation in time: conjugate twiddles, then the
+// butterfly with the + sign), unnormalised, on one component.
+template <int LGN, int STAGE>
+MRM_D void creg_inv(Cx<float> (&v)[8], const Cx<float> (&w)[8]) {
+  using P = CregPlan<LGN>;
+  constexpr int D = 1 << P::lgd(STAGE);
+  if constexpr (STAGE == 0 && P::R0 < 3) {
+    constexpr int R = 1 << P::R0, NB = 8 / R;
+#pragma unroll
+    for (int jl = 0; jl < NB; ++jl) {
+      Cx<float> u[R];
+      u[0] = v[jl];
+#pragma unroll
+      for (int m = 1; m < R; ++m) u[m] = cmul(v[jl + NB * m], cconj(w[jl * R + m]));
+      if constexpr (R == 4) dft4<float, 1>(u[0], u[1], u[2], u[3]);
+      else dft2<float, 1>(u);
+#pragma unroll
+      for (int m = 0; m < R; ++m) v[jl + NB * m] = u[m];
+    }
+  } else {
+    if constexpr (D > 1) {
+#pragma unroll
+      for (int m = 1; m < 8; ++m) v[m] = cmul(v[m], cconj(w[m]));
+    }
+    dft8<float, 1>(v);
+  }
+}
+
+// barrier of one column's NT threads: the warp itself, or named barrier 1 + c
+template <int NT>
+MRM_D void creg_sync(int c) {
+  if constexpr (NT <= 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(c + 1), "n"(NT) : "memory");
+  }
+}
+
+// A stage over the three components in the column's buffer: each component's
+// eight elements at the thread's positions of the stage are read, transformed
+// and written back in place (no other thread touches them in this stage).
+template <int LGN, int STAGE, bool INV>
+MRM_D void creg_stage(Cx<float>* __restrict__ buf, int t, const Cx<float>* __restrict__ tw) {
+  using P = CregPlan<LGN>;
+  constexpr int B = P::dbit(STAGE);
+  Cx<float> w[8];
+  creg_twiddles<LGN, STAGE>(w, t, tw);
+  const int a = xswz(creg_base<B>(t));
+#pragma unroll 1
+  for (int q = 0; q < 3; ++q) {
+    Cx<float>* b = buf + q * P::N;
+    Cx<float> v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = b[a ^ xswz(k << B)];
+    if constexpr (INV) creg_inv<LGN, STAGE>(v, w);
+    else creg_fwd<LGN, STAGE, false>(v, w);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) b[a ^ xswz(k << B)] = v[k];
+  }
+}
+
+// H^ = N^ M^ at the thread's positions 8t..8t+7 (the last stage's positions)
+// of the column's buffer.  tk: the column's tensor, six components (xx, yy,
+// zz, xy, xz, yz) of N reals in position order; the xz and yz spectra are
+// imaginary (the stored real times i) and the sign of the odd components in
+// the upper half of k_y is folded in.
+template <int LGN>
+MRM_D void creg_product(Cx<float>* __restrict__ buf, const float* __restrict__ tk, int t) {
+  constexpr int N = 1 << LGN;
+  const int a = xswz(t << 3);
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    float4 T[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) T[c] = reinterpret_cast<const float4*>(tk + c * N + 8 * t)[half];  // shared or global
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = 4 * half + i, at = a ^ k;  // xswz(k) = k for k < 8
+      auto comp = [&](int c) { return i == 0 ? T[c].x : i == 1 ? T[c].y : i == 2 ? T[c].z : T[c].w; };
+      const float xx = comp(0), yy = comp(1), zz = comp(2), xy = comp(3), xz = comp(4), yz = comp(5);
+      const Cx<float> mx = buf[at], my = buf[N + at], mz = buf[2 * N + at];
+      buf[at] = Cx<float>{fmaf(xx, mx.x, fmaf(xy, my.x, -xz * mz.y)), fmaf(xx, mx.y, fmaf(xy, my.y, xz * mz.x))};
+      buf[N + at] = Cx<float>{fmaf(xy, mx.x, fmaf(yy, my.x, -yz * mz.y)), fmaf(xy, mx.y, fmaf(yy, my.y, yz * mz.x))};
+      buf[2 * N + at] =
+          Cx<float>{fmaf(zz, mz.x, -fmaf(xz, mx.y, yz * my.y)), fmaf(zz, mz.y, fmaf(xz, mx.x, yz * my.x))};
+    }
+  }
+}
+
+// Shared memory of a block of BLOCK threads for 2^lgpy-point columns: the
+// column pass tables, one exchange buffer of three components per column
+// (which first holds the block's staged M^ tile), the columns' tensor slices.
+MRM_HD constexpr int creg_cols(int lgpy, int block) { return block >> (lgpy - 3); }
+MRM_HD constexpr int creg_xb_count(int lgpy, int block) { return creg_cols(lgpy, block) * 3 * (1 << lgpy); }
+MRM_HD constexpr int creg_smem(int lgpy, int block, bool tsm) {
+  return (col_tw_count(lgpy) + creg_xb_count(lgpy, block)) * (int)sizeof(Cx<float>) +
+         (tsm ? creg_cols(lgpy, block) * 6 * (1 << lgpy) * (int)sizeof(float) : 0);
+}
+
+// The column c of a task (global column k): forward transform, product,
+// inverse transform.  stg: the block's M^ tile staged in shared memory
+// ([plane][nys][T]), in the same space as the exchange buffers; live: c is
+// one of the task's columns (the others take part in the barriers only).
+template <int LGN, bool HALF>
+MRM_D void creg_body(const RunDev<float>& rd, int k, int t, int c, bool live, const Cx<float>* __restrict__ tw,
+                     const Cx<float>* __restrict__ stg, Cx<float>* __restrict__ buf, const float* __restrict__ tk) {
+  using P = CregPlan<LGN>;
+  constexpr int N = P::N, NT = P::NT, KIN = HALF ? 4 : 8;
+  constexpr int B0 = P::dbit(0);
+  const int ny = rd.ny, lgct = rd.lgct, cs = k & ((1 << lgct) - 1);
+  const int pstride = rd.nys << lgct;
+  Cx<float>* const spech = rd.spech;
+  const int phs = rd.phs;
+  // stage 0 from the staged tile: rows t + kk NT of every component
+  Cx<float> v0[3][KIN];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int kk = 0; kk < KIN; ++kk) {
+      const int j = t + kk * NT;
+      v0[q][kk] = j < ny ? stg[q * pstride + (j << lgct) + cs] : Cx<float>{0.f, 0.f};
+    }
+  // every thread's tile elements are in registers before the buffers are reused
+  __syncthreads();
+  {
+    Cx<float> w[8];
+    creg_twiddles<LGN, 0>(w, t, tw);
+    const int a = xswz(creg_base<B0>(t));
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      Cx<float> v[8];
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk) v[kk] = kk < KIN ? v0[q][kk] : Cx<float>{0.f, 0.f};
+      creg_fwd<LGN, 0, HALF>(v, w);
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk) buf[q * N + (a ^ xswz(kk << B0))] = v[kk];
+    }
+  }
+  creg_sync<NT>(c);
+  creg_stage<LGN, 1, false>(buf, t, tw);
+  creg_sync<NT>(c);
+  creg_stage<LGN, 2, false>(buf, t, tw);
+  if constexpr (P::S == 4) {
+    creg_sync<NT>(c);
+    creg_stage<LGN, 3, false>(buf, t, tw);
+  }
+  // the last stage's positions are the thread's own: no barrier before the product
+  if (live) creg_product<LGN>(buf, tk, t);
+  if constexpr (P::S == 4) {
+    creg_stage<LGN, 3, true>(buf, t, tw);
+    creg_sync<NT>(c);
+  }
+  creg_stage<LGN, 2, true>(buf, t, tw);
+  creg_sync<NT>(c);
+  creg_stage<LGN, 1, true>(buf, t, tw);
+  creg_sync<NT>(c);
+  if (!live) return;
+  // inverse stage 0 and the H^ rows, row-major [plane][ny][phs]
+  Cx<float> w[8];
+  creg_twiddles<LGN, 0>(w, t, tw);
+  const int a = xswz(creg_base<B0>(t));
+  Cx<float>* dst = spech + k;
+#pragma unroll 1
+  for (int q = 0; q < 3; ++q) {
+    Cx<float> v[8];
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) v[kk] = buf[q * N + (a ^ xswz(kk << B0))];
+    creg_inv<LGN, 0>(v, w);
+#pragma unroll
+    for (int kk = 0; kk < KIN; ++kk) {
+      const int j = t + kk * NT;
+      if (j < ny) dst[((size_t)q * ny + j) * phs] = v[kk];
+    }
+  }
+}
+
+template <int LGN, int BLOCK, bool TSM>
+MRM_D void creg_column(const RunDev<float>& rd, int k0, int nc, const Cx<float>* tw, Cx<float>* xb,
+                       const float* ts) {
+  using P = CregPlan<LGN>;
+  static_assert(P::NT <= BLOCK && BLOCK % P::NT == 0, "a block holds whole columns");
+  static_assert(P::NT >= 32, "a column is one or more whole warps");
+  const int c = threadIdx.x / P::NT, t = threadIdx.x % P::NT;
+  const bool live = c < nc;
+  Cx<float>* buf = xb + c * 3 * P::N;
+  // the column's tensor slice: staged in shared memory, or in global memory
+  const float* tk = TSM ? ts + c * 6 * P::N : rd.tens + (size_t)(k0 + c) * 6 * P::N;
+  if (rd.py >= 2 * rd.ny) creg_body<LGN, true>(rd, k0 + c, t, c, live, tw, xb, buf, tk);
+  else creg_body<LGN, false>(rd, k0 + c, t, c, live, tw, xb, buf, tk);
+}
+
+// One task (run, first column k0, columns nc <= BLOCK / (py/8), all in one
+// M^ tile) per block.  Bulk copies bring the twiddles and, with TSM, the
+// columns' tensor slices (static: before the dependency wait) and the M^ tile
+// (after it) into shared memory.
+template <int BLOCK, int MINB, bool TSM>
+__global__ void __launch_bounds__(BLOCK, MINB) creg_kernel(const RunDev<float>* __restrict__ runs,
+                                                           const Task* __restrict__ tasks,
+                                                           const Cx<float>* __restrict__ twg, int istep, int flags,
+                                                           int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t bars[2];
+  pdl_launch_dependents();
+  const Task tk = tasks[blockIdx.x];
+  const RunDev<float>& rd = runs[tk.x];
+  // blocks that leave early still wait for the previous kernel, so that this
+  // launch never completes before it (a column launch of the other column
+  // kernel may precede this one in the stream)
+  if (!rd.active || !rd.demag) {
+    pdl_wait();
+    return;
+  }
+  const int k0 = tk.y, nc = tk.z, lgpy = rd.lgpy, lgct = rd.lgct;
+  const int ph = (rd.px >> 1) + 1, T = 1 << lgct;
+  Cx<float>* tws = reinterpret_cast<Cx<float>*>(smem_raw);
+  const int ntw = col_tw_count(lgpy);
+  Cx<float>* xb = tws + ntw;
+  float* ts = reinterpret_cast<float*>(xb + creg_xb_count(lgpy, BLOCK));
+  const int tile_bytes = (rd.nys << lgct) * (int)sizeof(Cx<float>);  // one plane of the tile
+  const bool shape_ok = lgpy >= kCregMinLg && lgpy <= kCregMaxLg && rd.nl == 1 && nc >= 1 && k0 >= 0 &&
+                        k0 + nc <= ph && nc <= creg_cols(lgpy, BLOCK) && (k0 & (T - 1)) == 0 && nc <= T &&
+                        3 * tile_bytes <= creg_xb_count(lgpy, BLOCK) * (int)sizeof(Cx<float>) &&
+                        creg_smem(lgpy, BLOCK, TSM) <= (int)dynamic_smem_bytes();
+  if (!shape_ok) {
+    if (threadIdx.x == 0) atomicOr(err, kErrShape);
+    pdl_wait();
+    return;
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int n = 1 << lgpy;
+  if (threadIdx.x == 0) {
+    bulk_copy(&bars[0], tws, twg + rd.tw_col, (uint32_t)(ntw * sizeof(Cx<float>)));
+    if (TSM) bulk_copy(&bars[0], ts, rd.tens + (size_t)k0 * 6 * n, (uint32_t)(nc * 6 * n * sizeof(float)));
+    mbar_arrive(&bars[0]);
+  }
+  pdl_wait();
+  const bool run_it = (flags & kFlagForce) || rd.step + istep < rd.step_end;
+  if (threadIdx.x == 0) {
+    if (run_it) {
+      const int ntile = (ph + T - 1) >> lgct;
+      const Cx<float>* src = rd.specx + (((size_t)(k0 >> lgct) * rd.nys) << lgct);
+      const size_t pstride = ((size_t)ntile * rd.nys) << lgct;
+      for (int q = 0; q < 3; ++q)
+        bulk_copy(&bars[1], xb + q * (rd.nys << lgct), src + q * pstride, (uint32_t)tile_bytes);
+    }
+    mbar_arrive(&bars[1]);
+  }
+  const bool ok = mbar_wait(&bars[0], 0) && mbar_wait(&bars[1], 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicOr(err, kErrBarrierTimeout);
+    mbar_wait(&bars[0], 0);
+    mbar_wait(&bars[1], 0);
+    return;
+  }
+  if (!run_it) return;
+  switch (lgpy) {
+    case 8: creg_column<8, BLOCK, TSM>(rd, k0, nc, tws, xb, ts); break;
+    case 9: creg_column<9, BLOCK, TSM>(rd, k0, nc, tws, xb, ts); break;
+    default: creg_column<10, BLOCK, TSM>(rd, k0, nc, tws, xb, ts); break;
+  }
+}
+
+}  // namespace mrm

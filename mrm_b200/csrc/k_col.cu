@@ -176,6 +176,35 @@ cudaError_t col_occupancy<float>(int v, size_t smem, int* blocks) { return col_o
 template <>
 cudaError_t col_occupancy<double>(int v, size_t smem, int* blocks) { return col_occ_any<double>(v, smem, blocks); }
 
+// ---------------- register column kernel shapes (k_creg_*.cu) ----------------
+static const ColOps* creg_ops_of(int v) {
+  switch (v) {
+    case 0: return &creg_ops<0>();
+    case 1: return &creg_ops<1>();
+    case 2: return &creg_ops<2>();
+    default: return nullptr;
+  }
+}
+cudaError_t launch_creg(int v, const ColLaunch& a, int istep, int flags) {
+  const ColOps* o = creg_ops_of(v);
+  return o ? o->launch(a, istep, flags) : cudaErrorInvalidValue;
+}
+cudaError_t creg_allow_smem(int v, size_t smem) {
+  const ColOps* o = creg_ops_of(v);
+  return o ? allow_smem(o->fn, smem) : cudaErrorInvalidValue;
+}
+cudaError_t creg_occupancy(int v, size_t smem, int* blocks) {
+  const ColOps* o = creg_ops_of(v);
+  return o ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, o->fn, kCreg[v].block, smem)
+           : cudaErrorInvalidValue;
+}
+cudaError_t creg_load(int v) {
+  const ColOps* o = creg_ops_of(v);
+  if (!o) return cudaErrorInvalidValue;
+  cudaFuncAttributes fa;
+  return cudaFuncGetAttributes(&fa, o->fn);
+}
+
 template <typename R>
 static cudaError_t col_load_any(int v) {
   if (v < 0 || v >= col_variant_count<R>()) return cudaErrorInvalidValue;

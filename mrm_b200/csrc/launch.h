@@ -39,6 +39,17 @@ constexpr int col_variant_count() { return sizeof(R) == sizeof(float) ? kColVari
 template <typename R>
 constexpr ColVariant col_variant(int v) { return sizeof(R) == sizeof(float) ? kColF32[v] : kColF64[v]; }
 
+// Register column kernel shapes (colreg.cuh: FP32 runs of one layer with
+// 256..1024-point columns); the column shape index selects one of these for
+// those runs and one of kColF32 for the others.  tsm: the columns' tensor
+// slices are staged in shared memory (otherwise read from global memory).
+struct CregVariant {
+  int block, minb;
+  bool tsm;
+};
+constexpr int kCregVariants = 3;
+constexpr CregVariant kCreg[kCregVariants] = {{128, 4, true}, {256, 2, true}, {128, 6, false}};
+
 struct RowLaunch;
 // entry points of one compiled row shape (defined in its own translation unit)
 struct RowOps {
@@ -84,6 +95,9 @@ struct ColOps {
 };
 template <typename R, int V>
 const ColOps& col_ops();
+// entry points of one register column kernel shape (k_creg_*.cu)
+template <int V>
+const ColOps& creg_ops();
 
 // stage: kInit, kPred, kCorr, kEval; stats selects the corrector with reductions
 template <typename R>
@@ -115,6 +129,11 @@ template <typename R>
 cudaError_t col_occupancy(int variant, size_t smem, int* blocks_per_sm);
 template <typename R>
 cudaError_t col_load(int variant);
+// the register column kernel (FP32)
+cudaError_t launch_creg(int variant, const ColLaunch& a, int istep, int flags);
+cudaError_t creg_allow_smem(int variant, size_t smem);
+cudaError_t creg_occupancy(int variant, size_t smem, int* blocks_per_sm);
+cudaError_t creg_load(int variant);
 
 // launches with or without programmatic stream serialization
 template <typename... KArgs, typename... Args>

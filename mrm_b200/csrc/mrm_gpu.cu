@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "launch.h"
 #include "tensor.cuh"
+#include "colreg.cuh"
 
 using namespace mrm;
 
@@ -134,6 +135,8 @@ struct Engine {
   Task* d_rtasks = nullptr;
   Task* d_ctasks = nullptr;
   int nrt = 0, nct = 0, rt_cap = 0, ct_cap = 0;
+  Task* d_ctasks2 = nullptr;  // column tasks of the register column kernel's runs (colreg.cuh)
+  int nct2 = 0, ct2_cap = 0;
   int rowv = 0, colv = 0, cpt = 0;  // row / column shapes (launch.h), columns per task (0: default)
   bool shape_forced = false;         // shapes set by the caller instead of tuned
   int force_rowv = 0, force_colv = 0, force_cpt = 0;
@@ -141,6 +144,7 @@ struct Engine {
   size_t smem_row[kRowSlots] = {0, 0, 0, 0, 0, 0};  // per launch slot (launch.h row_slot)
   int stage_cap[kRowSlots] = {0, 0, 0, 0, 0, 0};
   size_t smem_col = 0;
+  size_t smem_creg = 0;
   // the corrector with reductions always runs row shape 0 over one-row tasks,
   // so that the FP64 reductions do not depend on the tuned shapes
   Task* d_stasks = nullptr;
@@ -272,6 +276,7 @@ void engine_free(Engine* e) {
   dfree(e->d_runs);
   dfree(e->d_rtasks);
   dfree(e->d_ctasks);
+  dfree(e->d_ctasks2);
   dfree(e->d_stasks);
   dfree(e->d_part);
   dfree(e->d_stats);
@@ -313,6 +318,8 @@ int col_tile(int want) {
   return t;
 }
 int cols_per_task(const Engine* e, const mrm_gpu* r) { return col_tile(e->cpt > 0 ? e->cpt : default_cols(r)); }
+// shape of the register column kernel: the column shape index
+int creg_v(const Engine* e) { return std::min(std::max(e->colv, 0), kCregVariants - 1); }
 // cells per row and rows of the FFT source (the moving demag window, else the grid)
 int fnx(const mrm_gpu* r) { return r->wnx ? r->wnx : r->g.nx; }
 int fny(const mrm_gpu* r) { return r->wnx ? r->wny : r->g.ny; }
@@ -324,9 +331,18 @@ size_t specx_count(const mrm_gpu* r) {
 // (a windowed run's rows are segments of the grid's rows: one per task)
 int rows_per_task(const mrm_gpu* r, int rpb) { return r->wnx ? 1 : std::max(1, std::min(rpb, r->g.ny)); }
 
+// Runs whose column step is the register column kernel (colreg.cuh): FP32,
+// one layer, 256..1024-point columns.  Their tensor is stored in that
+// kernel's layout (tensor.cuh pack_tensor_creg_kernel).
+bool creg_run(const mrm_gpu* r) {
+  return r->g.precision == MRM_FP32 && r->nl == 1 && r->lgpy >= kCregMinLg && r->lgpy <= kCregMaxLg &&
+         !r->fft_big;
+}
+
 size_t tensor_bytes(const mrm_gpu* r) {
   const size_t ph = r->px / 2 + 1, npair = (size_t)r->nl * r->nl;
   if (r->g.precision == MRM_FP64) return ph * npair * 9 * r->py * 2 * sizeof(double);
+  if (creg_run(r)) return ph * 6 * r->py * sizeof(float);
   return ph * npair * 9 * tens_row_stride(r->py) * sizeof(float);
 }
 
@@ -418,7 +434,8 @@ int validate_geom(const mrm_geom* g, std::string* errp, bool* big = nullptr) {
   const bool f64 = g->precision == MRM_FP64;
   const size_t rs = (f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1)) +
                     (size_t)(f64 ? head_table_bytes<double>(g->nx) : head_table_bytes<float>(g->nx));
-  const size_t cs = f64 ? col_smem_of<double>(&tmp, 1, 0) : col_smem_of<float>(&tmp, 1, 0);
+  const size_t cs = f64 ? col_smem_of<double>(&tmp, 1, 0)
+                       : creg_run(&tmp) ? (size_t)creg_smem(tmp.lgpy, kCreg[1].block, kCreg[1].tsm) : col_smem_of<float>(&tmp, 1, 0);
   if (rs + row_static_bytes(3) > kMaxSmem || cs + 64 > kMaxSmem)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d x %d layers exceeds shared memory", px,
                    py, g->n_lay);
@@ -567,14 +584,17 @@ int plan_smem(Engine* e) {
   const RowVariant rv = row_variant<R>(e->rowv);
   size_t fft = 16;
   int need[kSlots] = {0, 0, 0, 0, 0, 0};
-  size_t scol = 16;
+  size_t scol = 16, screg = 16;
   for (auto* r : e->runs) {
     if (r->lgpx > rv.lgmax)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d does not cover %d-column FFT grids", e->rowv, r->px);
     const int rows = rows_per_task(r, rv.rpb);
     fft = std::max(fft, row_fixed_smem<R>(r, rv.rpb));
     for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
-    if (r->demag && r->tensor_ready) scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r), col_variant<R>(e->colv).minb));
+    if (r->demag && r->tensor_ready) {
+      if (creg_run(r)) screg = std::max(screg, (size_t)creg_smem(r->lgpy, kCreg[creg_v(e)].block, kCreg[creg_v(e)].tsm));
+      else scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r), col_variant<R>(e->colv).minb));
+    }
   }
   for (int q = 0; q < kSlots; ++q) {
     const long long per_block = (long long)(kSmemPerSM / rv.minb) - (long long)kSmemReserved -
@@ -587,6 +607,8 @@ int plan_smem(Engine* e) {
   }
   if (scol + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
   e->smem_col = scol;
+  if (screg + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
+  e->smem_creg = screg;
   CK(row_allow_smem<R>(e->rowv, e->smem_row));
   // the reductions launches (kPred of the single-stage integrator, kCorr):
   // row shape 0, one row per task
@@ -611,6 +633,7 @@ int plan_smem(Engine* e) {
     CK(row_allow_smem<R>(0, lim));
   }
   CK(col_allow_smem<R>(e->colv, e->smem_col));
+  if (sizeof(R) == sizeof(float)) CK(creg_allow_smem(creg_v(e), e->smem_creg));
   return MRM_OK;
 }
 
@@ -618,7 +641,7 @@ template <typename R>
 int build_tables(Engine* e) {
   std::string* errp = &e->err;
   const RowVariant rv = row_variant<R>(e->rowv);
-  std::vector<Task> rt, ct, stt;
+  std::vector<Task> rt, ct, ct2, stt;
   for (size_t i = 0; i < e->runs.size(); ++i) {
     mrm_gpu* r = e->runs[i];
     r->slot = (int)i;
@@ -632,13 +655,22 @@ int build_tables(Engine* e) {
       for (int j = 0; j < ny; ++j) stt.push_back(make_int4((int)i, l, j, 1));
     r->nrow_tasks = (int)stt.size() - r->row_task0;
     if (r->demag && r->tensor_ready) {
-      const int cpt = cols_per_task(e, r), ph = r->px / 2 + 1;
-      r->lgct = ilog2(cpt);
-      for (int k = 0; k < ph; k += cpt) ct.push_back(make_int4((int)i, k, std::min(cpt, ph - k), 0));
+      const int ph = r->px / 2 + 1;
+      if (creg_run(r)) {
+        // a task per block of the register column kernel: block / (py/8) columns
+        const int cpt = creg_cols(r->lgpy, kCreg[creg_v(e)].block);
+        r->lgct = ilog2(col_tile(cpt));
+        for (int k = 0; k < ph; k += cpt) ct2.push_back(make_int4((int)i, k, std::min(cpt, ph - k), 0));
+      } else {
+        const int cpt = cols_per_task(e, r);
+        r->lgct = ilog2(cpt);
+        for (int k = 0; k < ph; k += cpt) ct.push_back(make_int4((int)i, k, std::min(cpt, ph - k), 0));
+      }
     }
   }
   e->nrt = (int)rt.size();
   e->nct = (int)ct.size();
+  e->nct2 = (int)ct2.size();
   e->has_head = false;
   e->has_cubic = false;
   e->has_llb = false;
@@ -680,6 +712,12 @@ int build_tables(Engine* e) {
     int rc = dmalloc(errp, (void**)&e->d_ctasks, sizeof(Task) * e->ct_cap);
     if (rc) return rc;
   }
+  if (e->nct2 > e->ct2_cap) {
+    dfree(e->d_ctasks2);
+    e->ct2_cap = std::max(e->nct2, 2 * e->ct2_cap);
+    int rc = dmalloc(errp, (void**)&e->d_ctasks2, sizeof(Task) * e->ct2_cap);
+    if (rc) return rc;
+  }
   // the row tasks' records, then kMaxLayers frozen-grain records per run
   const int nr = (int)e->runs.size();
   const int npart = e->nst + nr * kMaxLayers;
@@ -702,6 +740,7 @@ int build_tables(Engine* e) {
   }
   if (e->nrt) CK(cudaMemcpyAsync(e->d_rtasks, rt.data(), sizeof(Task) * e->nrt, cudaMemcpyHostToDevice, e->st));
   if (e->nct) CK(cudaMemcpyAsync(e->d_ctasks, ct.data(), sizeof(Task) * e->nct, cudaMemcpyHostToDevice, e->st));
+  if (e->nct2) CK(cudaMemcpyAsync(e->d_ctasks2, ct2.data(), sizeof(Task) * e->nct2, cudaMemcpyHostToDevice, e->st));
   if (e->nst) CK(cudaMemcpyAsync(e->d_stasks, stt.data(), sizeof(Task) * e->nst, cudaMemcpyHostToDevice, e->st));
   CK(cudaStreamSynchronize(e->st));  // the host vectors are released on return
   int rc = plan_smem<R>(e);
@@ -729,11 +768,20 @@ cudaError_t launch_row_e(Engine* e, int stage, bool stats, int istep, int flags,
   return launch_row<R>(e->rowv, stage, false, a, istep, flags);
 }
 
+// the column step: the in-place column kernel over its runs' tasks, then the
+// register column kernel over its runs' tasks (either may be absent)
 template <typename R>
 cudaError_t launch_col_e(Engine* e, int istep, int flags, bool pdl = true) {
-  if (!e->nct) return cudaSuccess;
-  ColLaunch a{e->st, e->d_runs, e->d_ctasks, e->d_tw, e->d_err, e->nct, e->smem_col, pdl};
-  return launch_col<R>(e->colv, a, istep, flags);
+  if (e->nct) {
+    ColLaunch a{e->st, e->d_runs, e->d_ctasks, e->d_tw, e->d_err, e->nct, e->smem_col, pdl};
+    cudaError_t ce = launch_col<R>(e->colv, a, istep, flags);
+    if (ce != cudaSuccess) return ce;
+  }
+  if (e->nct2) {
+    ColLaunch a{e->st, e->d_runs, e->d_ctasks2, e->d_tw, e->d_err, e->nct2, e->smem_creg, pdl};
+    return launch_creg(creg_v(e), a, istep, flags);
+  }
+  return cudaSuccess;
 }
 
 // llg_type -3 (Heun) and -2 (semi-implicit midpoint): two field evaluations
@@ -904,8 +952,12 @@ int autotune(Engine* e) {
   // column shapes with the default row shape
   Shape best = {e->rowv, e->colv, e->cpt};
   float best_ms = 1e30f;
+  // columns per task only matter for the in-place column kernel's runs
+  bool any_inplace = false;
+  for (auto* r : e->runs) any_inplace = any_inplace || (r->demag && r->tensor_ready && !creg_run(r));
   for (int cv = 0; cv < col_variant_count<R>(); ++cv)
     for (int nc : {1, 2, 4, 8}) {
+      if (!any_inplace && nc > 1) continue;
       e->colv = cv;
       e->cpt = nc;
       e->err.clear();
@@ -1587,6 +1639,10 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
     const long long total = (long long)ph * npair * 9 * r->py;
     pack_tensor_full_kernel<<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
         static_cast<const Cx<double>*>(d_spec), static_cast<Cx<double>*>(r->tens), npair, r->py, ph, d_mx, d_mx + 1);
+  } else if (creg_run(r)) {
+    const long long total = (long long)ph * 6 * r->py;
+    pack_tensor_creg_kernel<<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
+        static_cast<const Cx<double>*>(d_spec), static_cast<float*>(r->tens), r->lgpy, ph, d_mx, d_mx + 1);
   } else {
     const long long total = (long long)ph * npair * 9 * pyh;
     pack_tensor_kernel<float><<<(unsigned)((total + 255) / 256), 256, 0, e->st>>>(
@@ -3040,7 +3096,9 @@ static int occ_t(Engine* e, int* out2) {
   int a = 0, b = 0;
   if (!e->tables_dirty) {
     CK(row_occupancy<R>(e->rowv, kPred, e->smem_row[1], &a));
-    CK(col_occupancy<R>(e->colv, e->smem_col, &b));
+    // the column kernel of most of the batch's column tasks
+    if (e->nct2 > e->nct) CK(creg_occupancy(creg_v(e), e->smem_creg, &b));
+    else CK(col_occupancy<R>(e->colv, e->smem_col, &b));
   }
   out2[0] = a;
   out2[1] = b;
@@ -3175,10 +3233,12 @@ int noalloc_setup(int dev, std::string* errp, unsigned char** base) {
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   CK(row_load<float>(0));
   CK(col_load<float>(0));
+  CK(creg_load(0));
   size_t lim[kSlots];
   for (int q = 0; q < kSlots; ++q) lim[q] = (size_t)optin - row_static_bytes(q);
   CK(row_allow_smem<float>(0, lim));
   CK(col_allow_smem<float>(0, (size_t)optin - 64));
+  CK(creg_allow_smem(0, (size_t)optin - 64));
   cudaFuncAttributes fa;
   CK(cudaFuncGetAttributes(&fa, noalloc_pack_kernel));
   CK(cudaFuncGetAttributes(&fa, noalloc_unpack_kernel));
@@ -3205,7 +3265,8 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
       return set_err(errp, MRM_ERR_UNSUPPORTED, "the allocation-free demag evaluation takes one grain per cell");
   const int nl = h->nl, ny = h->g.ny, ph = h->px / 2 + 1;
   const int rpt = 1, nrt = nl * ny;  // one row per task (row shape 0)
-  const int cpt = col_tile(default_cols(h)), nct = (ph + cpt - 1) / cpt;
+  const bool creg = creg_run(h);
+  const int cpt = creg ? creg_cols(h->lgpy, kCreg[0].block) : col_tile(default_cols(h)), nct = (ph + cpt - 1) / cpt;
   const NoAllocLayout lay = noalloc_layout(h, nrt, nct);
   if (lay.total > kNoAllocBytes)
     return set_err(errp, MRM_ERR_UNSUPPORTED,
@@ -3263,8 +3324,12 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   CK(launch_row<float>(0, kInit, false,
                        RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false, head},
                        0, kFlagForce));
-  CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt, col_variant<float>(0).minb), true}, 0,
-                       kFlagForce));
+  if (creg)
+    CK(launch_creg(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, (size_t)creg_smem(h->lgpy, kCreg[0].block, kCreg[0].tsm), true},
+                   0, kFlagForce));
+  else
+    CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt, col_variant<float>(0).minb), true}, 0,
+                         kFlagForce));
   CK(launch_row<float>(0, kEval, false,
                        RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_eval, cap_eval, true, head},
                        0, kFlagForce | kFlagStoreField));

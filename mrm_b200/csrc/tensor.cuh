@@ -11,6 +11,7 @@
 // per (kx, 0 <= ky <= py/2) is kept.
 #pragma once
 #include "common.cuh"
+#include "dd.cuh"
 #include "fft.cuh"
 
 namespace mrm {
@@ -23,64 +24,110 @@ struct PairGeom {
   double norm;        // 1/(dx dy dz_o px py), tensor.f90:183
 };
 
-__device__ __forceinline__ double fsign_d(double a, double b) { return copysign(fabs(a), b); }
+// One corner combination of volume_averaged_n (tensor_element.f90:39-72) in
+// double-double: the corner offsets (x, y, z), d = |(x, y, z)|, the three
+// arctangents and six logarithms that g1 and g2 (:78-100) share, and the
+// six distinct elements.  g1(x,y,z,d) and g2(z,x,y,d) are the reference's
+// closed forms with their max(1e-300, .) guards and Fortran sign(); the
+// arctangent arguments y z / sign(max(1e-300, |x| d), x) and their
+// permutations are A_x, A_y, A_z.
+struct TensCorner {
+  dd t00, t11, t22, t12, t02, t01;  // g1(x,y,z), g1(y,z,x), g1(z,x,y), g2(x,y,z), g2(y,z,x), g2(z,x,y)
+};
 
-__device__ __forceinline__ double tg1(double x, double y, double z, double d) {
-  double r = x * y * z * atan(y * z / fsign_d(fmax(1.0e-300, fabs(x) * d), x));
-  r += 0.5 * y * (z * z - x * x) * log(fmax(1.0e-300, d - y));
-  r += 0.5 * z * (y * y - x * x) * log(fmax(1.0e-300, d - z));
-  r += (y * y + z * z - 2.0 * x * x) * d / 6.0;
-  return r;
+__device__ __forceinline__ dd tens_den(dd v, dd d) {
+  // sign(max(1e-300, |v| d), v)
+  const dd a = dd_max_d(dd_mul(dd_abs(v), d), 1.0e-300);
+  return signbit(v.hi) ? dd_neg(a) : a;
+}
+__device__ __forceinline__ dd tens_log(dd v) { return dd_log(dd_max_d(v, 1.0e-300)); }
+
+__device__ __noinline__ TensCorner tens_corner(dd x, dd y, dd z) {
+  const dd x2 = dd_mul(x, x), y2 = dd_mul(y, y), z2 = dd_mul(z, z);
+  const dd d = dd_sqrt(dd_add(dd_add(x2, y2), z2));
+  const dd xyz = dd_mul(dd_mul(x, y), z);
+  const dd ax = dd_atan(dd_div(dd_mul(y, z), tens_den(x, d)));
+  const dd ay = dd_atan(dd_div(dd_mul(z, x), tens_den(y, d)));
+  const dd az = dd_atan(dd_div(dd_mul(x, y), tens_den(z, d)));
+  const dd lmx = tens_log(dd_sub(d, x)), lmy = tens_log(dd_sub(d, y)), lmz = tens_log(dd_sub(d, z));
+  const dd lpx = tens_log(dd_add(d, x)), lpy = tens_log(dd_add(d, y)), lpz = tens_log(dd_add(d, z));
+  const dd sixth = dd_recip_int(6), third = dd_recip_int(3);
+  auto half = [](dd v) { return dd_ldexp(v, -1); };
+  TensCorner c;
+  // g1(x, y, z, d)
+  c.t00 = dd_add(dd_add(dd_mul(xyz, ax), half(dd_mul(dd_mul(y, dd_sub(z2, x2)), lmy))),
+                 dd_add(half(dd_mul(dd_mul(z, dd_sub(y2, x2)), lmz)),
+                        dd_mul(dd_mul(dd_sub(dd_add(y2, z2), dd_ldexp(x2, 1)), d), sixth)));
+  // g1(y, z, x, d)
+  c.t11 = dd_add(dd_add(dd_mul(xyz, ay), half(dd_mul(dd_mul(z, dd_sub(x2, y2)), lmz))),
+                 dd_add(half(dd_mul(dd_mul(x, dd_sub(z2, y2)), lmx)),
+                        dd_mul(dd_mul(dd_sub(dd_add(z2, x2), dd_ldexp(y2, 1)), d), sixth)));
+  // g1(z, x, y, d)
+  c.t22 = dd_add(dd_add(dd_mul(xyz, az), half(dd_mul(dd_mul(x, dd_sub(y2, z2)), lmx))),
+                 dd_add(half(dd_mul(dd_mul(y, dd_sub(x2, z2)), lmy)),
+                        dd_mul(dd_mul(dd_sub(dd_add(x2, y2), dd_ldexp(z2, 1)), d), sixth)));
+  // g2(x, y, z, d): -x y z log(d+x) + z (z^2 - 3x^2) log(d+y)/6 + y (y^2 - 3x^2) log(d+z)/6
+  //   + y^2 x A_y / 2 + z^2 x A_z / 2 + x^3 A_x / 6 + y z d / 3
+  c.t12 = dd_add(dd_add(dd_neg(dd_mul(xyz, lpx)),
+                        dd_mul(dd_add(dd_mul(dd_mul(z, dd_sub(z2, dd_mul_d(x2, 3.0))), lpy),
+                                      dd_mul(dd_mul(y, dd_sub(y2, dd_mul_d(x2, 3.0))), lpz)),
+                               sixth)),
+                 dd_add(dd_add(half(dd_mul(dd_mul(y2, x), ay)), half(dd_mul(dd_mul(z2, x), az))),
+                        dd_add(dd_mul(dd_mul(dd_mul(x2, x), ax), sixth), dd_mul(dd_mul(dd_mul(y, z), d), third))));
+  // g2(y, z, x, d)
+  c.t02 = dd_add(dd_add(dd_neg(dd_mul(xyz, lpy)),
+                        dd_mul(dd_add(dd_mul(dd_mul(x, dd_sub(x2, dd_mul_d(y2, 3.0))), lpz),
+                                      dd_mul(dd_mul(z, dd_sub(z2, dd_mul_d(y2, 3.0))), lpx)),
+                               sixth)),
+                 dd_add(dd_add(half(dd_mul(dd_mul(z2, y), az)), half(dd_mul(dd_mul(x2, y), ax))),
+                        dd_add(dd_mul(dd_mul(dd_mul(y2, y), ay), sixth), dd_mul(dd_mul(dd_mul(z, x), d), third))));
+  // g2(z, x, y, d)
+  c.t01 = dd_add(dd_add(dd_neg(dd_mul(xyz, lpz)),
+                        dd_mul(dd_add(dd_mul(dd_mul(y, dd_sub(y2, dd_mul_d(z2, 3.0))), lpx),
+                                      dd_mul(dd_mul(x, dd_sub(x2, dd_mul_d(z2, 3.0))), lpy)),
+                               sixth)),
+                 dd_add(dd_add(half(dd_mul(dd_mul(x2, z), ax)), half(dd_mul(dd_mul(y2, z), ay))),
+                        dd_add(dd_mul(dd_mul(dd_mul(z2, z), az), sixth), dd_mul(dd_mul(dd_mul(x, y), d), third))));
+  return c;
 }
 
-__device__ __forceinline__ double tg2(double z, double x, double y, double d) {
-  double r = -x * y * z * log(fmax(1.0e-300, d + z));
-  r += y * (y * y - 3.0 * z * z) * log(fmax(1.0e-300, d + x)) / 6.0;
-  r += x * (x * x - 3.0 * z * z) * log(fmax(1.0e-300, d + y)) / 6.0;
-  r += 0.5 * x * x * z * atan(y * z / fsign_d(fmax(1.0e-300, fabs(x) * d), x));
-  r += 0.5 * y * y * z * atan(x * z / fsign_d(fmax(1.0e-300, fabs(y) * d), y));
-  r += z * z * z * atan(x * y / fsign_d(fmax(1.0e-300, fabs(z) * d), z)) / 6.0;
-  r += x * y * d / 3.0;
-  return r;
-}
-
-// n -= t over the 64 corner combinations; n[a*3+b] = reference n(a,b)
-__device__ void vol_avg_n(double rx, double ry, double rz, double xs, double ys, double zs,
-                          double xo, double zo, double* n) {
-  const double dxo[2] = {-0.5 * xo, 0.5 * xo}, dyo[2] = {-0.5 * xo, 0.5 * xo},
-               dzo[2] = {-0.5 * zo, 0.5 * zo};
-  const double dxs[2] = {-0.5 * xs, 0.5 * xs}, dys[2] = {-0.5 * ys, 0.5 * ys},
-               dzs[2] = {-0.5 * zs, 0.5 * zs};
-  double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int i6 = 1; i6 <= 2; ++i6)
-    for (int i5 = 1; i5 <= 2; ++i5)
-      for (int i4 = 1; i4 <= 2; ++i4)
-        for (int i3 = 1; i3 <= 2; ++i3) {
-          const double dx = -rx + dxo[i3 - 1] - dxs[i6 - 1];
-          for (int i2 = 1; i2 <= 2; ++i2) {
-            const double dy = -ry + dyo[i2 - 1] - dys[i5 - 1];
-            for (int i1 = 1; i1 <= 2; ++i1) {
-              const double dz = -rz + dzo[i1 - 1] - dzs[i4 - 1];
-              const double d = sqrt(dx * dx + dy * dy + dz * dz);
-              if (d != 0.0) {
-                const double sg = ((i1 + i2 + i3 + i4 + i5 + i6 - 1) & 1) ? -1.0 : 1.0;
-                t[0] += sg * tg1(dx, dy, dz, d);
-                t[4] += sg * tg1(dy, dz, dx, d);
-                t[8] += sg * tg1(dz, dx, dy, d);
-                double x = sg * tg2(dx, dy, dz, d);
-                t[7] += x;
-                t[5] += x;
-                x = sg * tg2(dy, dz, dx, d);
-                t[6] += x;
-                t[2] += x;
-                x = sg * tg2(dz, dx, dy, d);
-                t[3] += x;
-                t[1] += x;
-              }
-            }
-          }
-        }
-  for (int k = 0; k < 9; ++k) n[k] -= t[k];
+// volume_averaged_n (tensor_element.f90:13-102) in double-double: t over the
+// 64 corner combinations with the reference's signs; the source offset
+// (rx, ry) is (ix dx, iy dy) for integers ix, iy, exactly; rz as given.
+// n[a*3+b] -= t(a,b).  The reference's quirk dyo = xo (:31) is kept.
+__device__ void vol_avg_n(double ix, double iy, double dxc, double dyc, double rz, double xs, double ys,
+                          double zs, double xo, double zo, dd* n) {
+  const dd rx = two_prod(ix, dxc), ry = two_prod(iy, dyc);
+  dd t00 = dd_from(0), t11 = dd_from(0), t22 = dd_from(0), t12 = dd_from(0), t02 = dd_from(0), t01 = dd_from(0);
+#pragma unroll 1
+  for (int c = 0; c < 64; ++c) {
+    const int i1 = 1 + (c & 1), i2 = 1 + ((c >> 1) & 1), i3 = 1 + ((c >> 2) & 1);
+    const int i4 = 1 + ((c >> 3) & 1), i5 = 1 + ((c >> 4) & 1), i6 = 1 + ((c >> 5) & 1);
+    // dx = -rx + dxo(i3) - dxs(i6), dxo = xo (-1/2, 1/2), dxs = xs (-1/2, 1/2)
+    const dd dx = dd_add_d(dd_add_d(dd_neg(rx), (i3 == 1 ? -0.5 : 0.5) * xo), -((i6 == 1 ? -0.5 : 0.5) * xs));
+    const dd dy = dd_add_d(dd_add_d(dd_neg(ry), (i2 == 1 ? -0.5 : 0.5) * xo), -((i5 == 1 ? -0.5 : 0.5) * ys));
+    const dd dz = dd_add_d(dd_add_d(dd_from(-rz), (i1 == 1 ? -0.5 : 0.5) * zo), -((i4 == 1 ? -0.5 : 0.5) * zs));
+    if (dx.hi == 0.0 && dy.hi == 0.0 && dz.hi == 0.0) continue;  // d = 0
+    const TensCorner k = tens_corner(dx, dy, dz);
+    const bool minus = ((i1 + i2 + i3 + i4 + i5 + i6 - 1) & 1) != 0;
+    auto acc = [&](dd& a, dd v) { a = minus ? dd_sub(a, v) : dd_add(a, v); };
+    acc(t00, k.t00);
+    acc(t11, k.t11);
+    acc(t22, k.t22);
+    acc(t12, k.t12);
+    acc(t02, k.t02);
+    acc(t01, k.t01);
+  }
+  // t(1,1), t(2,2), t(3,3); t(2,3) = t(3,2) = g2(x,y,z); t(1,3) = t(3,1) = g2(y,z,x); t(1,2) = t(2,1) = g2(z,x,y)
+  n[0] = dd_sub(n[0], t00);
+  n[4] = dd_sub(n[4], t11);
+  n[8] = dd_sub(n[8], t22);
+  n[5] = dd_sub(n[5], t12);
+  n[7] = dd_sub(n[7], t12);
+  n[2] = dd_sub(n[2], t02);
+  n[6] = dd_sub(n[6], t02);
+  n[1] = dd_sub(n[1], t01);
+  n[3] = dd_sub(n[3], t01);
 }
 
 // offsets i in [-n/2, n/2] with (n - i) mod n == f, ascending
@@ -96,10 +143,10 @@ __device__ __forceinline__ int slot_offsets(int f, int n, int* out) {
 
 // plane_to_plane for one slot (tensor_element.f90:233-257); acc[a*3+b]
 __device__ void slot_plane(int fi, int fj, int nx, int ny, double dx, double dy, double dz,
-                           double dzo, double rz, int nimg, double* acc) {
+                           double dzo, double rz, int nimg, dd* acc) {
   int il[2], jl[2];
   const int ni = slot_offsets(fi, nx, il), nj = slot_offsets(fj, ny, jl);
-  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  for (int k = 0; k < 9; ++k) acc[k] = dd_from(0.0);
   for (int qj = 0; qj < nj; ++qj) {
     const int j = jl[qj];
     const int yp0 = -nimg * (1 - max(0, j / ((ny + 1) / 2)));
@@ -108,14 +155,13 @@ __device__ void slot_plane(int fi, int fj, int nx, int ny, double dx, double dy,
       const int i = il[qi];
       const int xp0 = -nimg * (1 - max(0, i / ((nx + 1) / 2)));
       const int xp1 = nimg * (1 + min(0, i / ((nx + 1) / 2)));
-      double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      dd t[9];
+      for (int k = 0; k < 9; ++k) t[k] = dd_from(0.0);
       for (int iy = yp0; iy <= yp1; ++iy)
-        for (int ix = xp0; ix <= xp1; ++ix) {
-          const double rx = (double)i * dx + (double)ix * dx * (double)nx;
-          const double ry = (double)j * dy + (double)iy * dy * (double)ny;
-          vol_avg_n(rx, ry, rz, dx, dy, dz, dx, dzo, t);
-        }
-      for (int k = 0; k < 9; ++k) acc[k] += t[k];
+        for (int ix = xp0; ix <= xp1; ++ix)
+          vol_avg_n((double)i + (double)ix * (double)nx, (double)j + (double)iy * (double)ny, dx, dy, rz, dx, dy,
+                    dz, dx, dzo, t);
+      for (int k = 0; k < 9; ++k) acc[k] = dd_add(acc[k], t[k]);
     }
   }
 }
@@ -130,22 +176,23 @@ __global__ void tensor_real_kernel(double* __restrict__ n2d, const PairGeom* __r
   const int rem = (int)(gid - (long long)pair * plane);
   const int fj = rem / px, fi = rem - fj * px;
   const PairGeom g = pg[pair];
-  double acc[9], tot[9];
+  dd acc[9], tot[9];
   slot_plane(fi, fj, px, py, dx, dy, g.dz_s, g.dz_o, g.rz, nimg, acc);
   for (int k = 0; k < 9; ++k) tot[k] = acc[k];
   if (g.f_sul != 0.0) {
     slot_plane(fi, fj, px, py, dx, dy, g.dz_s, g.dz_o, g.rz_sul, nimg, acc);
     for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) tot[a * 3 + b] += (a < 2 ? -g.f_sul : g.f_sul) * acc[a * 3 + b];
+      for (int b = 0; b < 3; ++b) tot[a * 3 + b] = dd_add(tot[a * 3 + b], dd_mul_d(acc[a * 3 + b], a < 2 ? -g.f_sul : g.f_sul));
   }
   if (g.f_head != 0.0) {
     slot_plane(fi, fj, px, py, dx, dy, g.dz_s, g.dz_o, g.rz_head, nimg, acc);
     for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) tot[a * 3 + b] += (a < 2 ? -g.f_head : g.f_head) * acc[a * 3 + b];
+      for (int b = 0; b < 3; ++b)
+        tot[a * 3 + b] = dd_add(tot[a * 3 + b], dd_mul_d(acc[a * 3 + b], a < 2 ? -g.f_head : g.f_head));
   }
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b)
-      n2d[(((long long)pair * 9 + 3 * b + a) * py + fj) * px + fi] = tot[a * 3 + b] * g.norm;
+      n2d[(((long long)pair * 9 + 3 * b + a) * py + fj) * px + fi] = dd_mul_d(tot[a * 3 + b], g.norm).hi;
 }
 
 // FP64 r2c along x of `planes` real planes [p][py][px] -> [p][py][px/2+1]
@@ -289,6 +336,40 @@ __global__ void pack_tensor_kernel(const Cx<double>* __restrict__ spec, R* __res
     const int k = (int)(r / npair);
     parity_parts(spec + ((long long)pair * 9 + c) * py * ph, c, kyh, k, py, ph, &keep, &disc);
     tens[(gid / pyh) * pyhs + kyh] = (R)keep;
+  }
+  block_max2(disc, fabs(keep), resid, kept);
+}
+
+// spectrum [0][9][py][ph] (FP64, one layer) -> tens[k][6][py] floats for the
+// register column kernel (colreg.cuh): components xx, yy, zz, xy, xz, yz (the
+// tensor is symmetric: yx, zx, zy are xy, xz, yz) at the positions of the
+// column transform's digit-reversed order (element p holds k_y = ip_freq(p)),
+// the sign of the odd components for k_y > py/2 folded in.  The residue adds
+// any difference between a component and its transpose.
+__global__ void pack_tensor_creg_kernel(const Cx<double>* __restrict__ spec, float* __restrict__ tens, int lgpy,
+                                        int ph, unsigned long long* resid, unsigned long long* kept) {
+  const int py = 1 << lgpy;
+  const long long total = (long long)ph * 6 * py;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double keep = 0.0, disc = 0.0;
+  if (gid < total) {
+    const int p = (int)(gid % py);
+    const int c6 = (int)((gid / py) % 6);
+    const int k = (int)(gid / ((long long)6 * py));
+    const int ky = ip_freq(p, lgpy);
+    const bool upper = ky > py / 2;
+    const int kyh = upper ? py - ky : ky;
+    constexpr int kComp[6] = {0, 4, 8, 1, 2, 5};   // xx yy zz xy xz yz
+    constexpr int kTrans[6] = {0, 4, 8, 3, 6, 7};  // their transposes
+    const int c = kComp[c6];
+    parity_parts(spec + (long long)c * py * ph, c, kyh, k, py, ph, &keep, &disc);
+    if (kTrans[c6] != c) {
+      double kt, dt;
+      parity_parts(spec + (long long)kTrans[c6] * py * ph, kTrans[c6], kyh, k, py, ph, &kt, &dt);
+      disc = fmax(disc, fmax(dt, fabs(kt - keep)));
+    }
+    const bool odd = (kOddMask >> c) & 1;
+    tens[gid] = (float)((odd && upper) ? -keep : keep);
   }
   block_max2(disc, fabs(keep), resid, kept);
 }

@@ -18,6 +18,7 @@
 // Each routine cites the reference file:line it restates (paths relative to the
 // reference project root).
 
+#include <quadmath.h>
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -219,6 +220,71 @@ static void volume_averaged_n(double rx, double ry, double rz, double xs, double
                 x = sgn * g2(dz, dx, dy, d);
                 t[3] += x;  // t(2,1)
                 t[1] += x;  // t(1,2)
+              }
+            }
+          }
+        }
+  for (int k = 0; k < 9; ++k) n[k] -= t[k];
+}
+
+// Quadruple-precision (binary128, libquadmath) evaluation of the same
+// closed forms, for an offset (ix dx, iy dy, rz) with integer ix, iy: the
+// exact-arithmetic value of the reference's formula to ~1e-30, against which
+// the FP64 evaluation's cancellation noise and the device's double-double
+// tensor are measured (test infrastructure).
+using q128 = __float128;
+static inline q128 q_sign(q128 a, q128 b) { return signbitq(b) ? -fabsq(a) : fabsq(a); }
+static inline q128 q_max(q128 a, q128 b) { return a < b ? b : a; }
+static inline q128 q_g1(q128 x, q128 y, q128 z, q128 d) {
+  const q128 tiny = (q128)1.0e-300;
+  q128 r = x * y * z * atanq(y * z / q_sign(q_max(tiny, fabsq(x) * d), x));
+  r += (q128)0.5 * y * (z * z - x * x) * logq(q_max(tiny, d - y));
+  r += (q128)0.5 * z * (y * y - x * x) * logq(q_max(tiny, d - z));
+  r += (y * y + z * z - (q128)2 * x * x) * d / (q128)6;
+  return r;
+}
+static inline q128 q_g2(q128 z, q128 x, q128 y, q128 d) {
+  const q128 tiny = (q128)1.0e-300;
+  q128 r = -x * y * z * logq(q_max(tiny, d + z));
+  r += y * (y * y - (q128)3 * z * z) * logq(q_max(tiny, d + x)) / (q128)6;
+  r += x * (x * x - (q128)3 * z * z) * logq(q_max(tiny, d + y)) / (q128)6;
+  r += (q128)0.5 * x * x * z * atanq(y * z / q_sign(q_max(tiny, fabsq(x) * d), x));
+  r += (q128)0.5 * y * y * z * atanq(x * z / q_sign(q_max(tiny, fabsq(y) * d), y));
+  r += z * z * z * atanq(x * y / q_sign(q_max(tiny, fabsq(z) * d), z)) / (q128)6;
+  r += x * y * d / (q128)3;
+  return r;
+}
+static void volume_averaged_n_q(int ix, int iy, double dxc, double dyc, double rzd, double xsd, double ysd,
+                                double zsd, double xod, double zod, q128 n[9]) {
+  const q128 rx = (q128)ix * (q128)dxc, ry = (q128)iy * (q128)dyc, rz = (q128)rzd;
+  const q128 xs = xsd, ys = ysd, zs = zsd, xo = xod, zo = zod, h = (q128)0.5;
+  const q128 dxo[2] = {-h * xo, h * xo}, dyo[2] = {-h * xo, h * xo}, dzo[2] = {-h * zo, h * zo};
+  const q128 dxs[2] = {-h * xs, h * xs}, dys[2] = {-h * ys, h * ys}, dzs[2] = {-h * zs, h * zs};
+  q128 t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i6 = 1; i6 <= 2; ++i6)
+    for (int i5 = 1; i5 <= 2; ++i5)
+      for (int i4 = 1; i4 <= 2; ++i4)
+        for (int i3 = 1; i3 <= 2; ++i3) {
+          const q128 dx = -rx + dxo[i3 - 1] - dxs[i6 - 1];
+          for (int i2 = 1; i2 <= 2; ++i2) {
+            const q128 dy = -ry + dyo[i2 - 1] - dys[i5 - 1];
+            for (int i1 = 1; i1 <= 2; ++i1) {
+              const q128 dz = -rz + dzo[i1 - 1] - dzs[i4 - 1];
+              const q128 d = sqrtq(dx * dx + dy * dy + dz * dz);
+              if (d != 0) {
+                const q128 sgn = ((i1 + i2 + i3 + i4 + i5 + i6 - 1) % 2 == 0) ? 1 : -1;
+                t[0] += sgn * q_g1(dx, dy, dz, d);
+                t[4] += sgn * q_g1(dy, dz, dx, d);
+                t[8] += sgn * q_g1(dz, dx, dy, d);
+                q128 x = sgn * q_g2(dx, dy, dz, d);
+                t[7] += x;
+                t[5] += x;
+                x = sgn * q_g2(dy, dz, dx, d);
+                t[6] += x;
+                t[2] += x;
+                x = sgn * q_g2(dz, dx, dy, d);
+                t[3] += x;
+                t[1] += x;
               }
             }
           }
@@ -1737,6 +1803,15 @@ void orc_philox_normal3(uint64_t seed, uint64_t stream, uint64_t step, uint64_t 
 void orc_volume_averaged_n(double rx, double ry, double rz, double xs, double ys, double zs,
                            double xo, double yo, double zo, double* n9) {
   volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo, n9);
+}
+// volume_averaged_n in quadruple precision at offsets (ix dx, iy dy, rz),
+// summed over `count` offsets (ix[k], iy[k]) and scaled by `scale`, rounded to
+// FP64: one FFT-grid slot of the tensor (several offsets where the grid wraps)
+void orc_volume_averaged_n_q(int count, const int* ix, const int* iy, double dx, double dy, double rz,
+                             double xs, double ys, double zs, double xo, double zo, double scale, double* n9) {
+  q128 n[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < count; ++k) volume_averaged_n_q(ix[k], iy[k], dx, dy, rz, xs, ys, zs, xo, zo, n);
+  for (int k = 0; k < 9; ++k) n9[k] = (double)(n[k] * (q128)scale);
 }
 void orc_calculate_tensor(int nx, int ny, int nl, double dx, double dy, const double* dz,
                           const double* il_space, int imx, int imy, double space_to_sul,

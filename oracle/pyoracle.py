@@ -81,6 +81,7 @@ def lib():
         L.orc_philox4x64.argtypes = [P(u64), P(u64), P(u64)]
         L.orc_philox_normal3.argtypes = [u64, u64, u64, u64, P(d)]
         L.orc_volume_averaged_n.argtypes = [d] * 9 + [P(d)]
+        L.orc_volume_averaged_n_q.argtypes = [i, P(i), P(i)] + [d] * 9 + [P(d)]
         L.orc_calculate_tensor.argtypes = [i, i, i, d, d, P(d), P(d), i, i, d, d, d, d, P(d)]
         L.orc_fft_r2c.argtypes = [i, i, P(d), P(d)]
         L.orc_fft_c2r.argtypes = [i, i, P(d), P(d)]
@@ -151,6 +152,24 @@ def volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo) -> np.ndarray:
     n = np.zeros(9)
     lib().orc_volume_averaged_n(rx, ry, rz, xs, ys, zs, xo, yo, zo, _p(n))
     return n.reshape(3, 3)
+
+
+def tensor_slot_q(px, py, dx, dy, dz_s, dz_o, rz, fi, fj) -> np.ndarray:
+    """One slot (fi, fj) of an open-boundary FFT grid's tensor (no images) in
+    quadruple precision: the offsets that wrap onto the slot (two on the
+    n/2 lines, src/tensor_element.f90:233-257), normalised by
+    1/(dx dy dz_o px py) (src/tensor.f90:183); returns t(a, b) as [a*3+b]."""
+    def offs(f, n):
+        if n % 2 == 0 and f == n // 2:
+            return [-n // 2, n // 2]
+        return [0 if f == 0 else (-f if f <= n // 2 else n - f)]
+    pts = [(i, j) for j in offs(fj, py) for i in offs(fi, px)]
+    ix = np.array([p[0] for p in pts], np.int32)
+    iy = np.array([p[1] for p in pts], np.int32)
+    out = np.zeros(9)
+    lib().orc_volume_averaged_n_q(len(pts), _p(ix, C.c_int), _p(iy, C.c_int), dx, dy, rz, dx, dy, dz_s, dx, dz_o,
+                                  1.0 / (dx * dy * dz_o * px * py), _p(out))
+    return out
 
 
 def calculate_tensor(nx, ny, dx, dy, dz, il_space, images, space_to_sul=0.0, sul_mu=1.0,
