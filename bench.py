@@ -63,24 +63,31 @@ WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
 NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 140.6, "col": 70.2, "row_corr": 166.4}
 
 
-def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4) -> dict:
-    """Bytes each kernel must move at minimum with this path's data layout, per run.
+def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4, runs: int = 1,
+                      tensors: int = 1) -> dict:
+    """Bytes each kernel must move at minimum with this path's data layout, for
+    `runs` runs of one geometry that read `tensors` tensor copies (runs whose
+    tensor comes from another run of the same geometry share its buffer).
 
     row predictor: H^ rows in + M^ rows out (2 * 3 ny (px/2+1) complex), per grain
       m, pa, pb (3 x 16 B), exchange CSR (4 B index + 4 x (4 B nbr + 4 B coef)),
       writes m*, d (2 x 16 B)                     -> 116 B/grain
     row corrector: same spectra, per grain m, m*, d, pa, pb (5 x 16 B),
       CSR 36 B, writes m (16 B)                    -> 132 B/grain
-    column: M^ columns in + H^ out (2 * 3 ny (px/2+1) complex) + tensor
-      (px/2+1) * 9 * (py/2+1) reals (nl^2 pairs)
+    column: M^ columns in + H^ out (2 * 3 ny (px/2+1) complex) per run, plus
+      the tensor: one layer, the symmetric tensor's six components at every
+      k_y of the (px/2+1) columns (the register column kernel's layout:
+      6 py reals per column); more layers, nine components per layer pair at
+      0 <= k_y <= py/2
     """
     c = 2 * fp
     spec = 3 * nl * ny * (px // 2 + 1) * c
     n = nx * ny * nl
     row_pred = 2 * spec + n * (3 * 16 + 36 + 2 * 16)
     row_corr = 2 * spec + n * (5 * 16 + 36 + 16)
-    col = 2 * spec + (px // 2 + 1) * nl * nl * 9 * (py // 2 + 1) * fp
-    return {"row_pred": row_pred, "col": col, "row_corr": row_corr}
+    tensor = ((px // 2 + 1) * 6 * py * fp if nl == 1 else (px // 2 + 1) * nl * nl * 9 * (py // 2 + 1) * fp)
+    col = runs * 2 * spec + tensors * tensor
+    return {"row_pred": runs * row_pred, "col": col, "row_corr": runs * row_corr}
 
 
 def measured_peaks():
@@ -585,7 +592,8 @@ def main():
     value = job_throughput(nb * n * args.heun * args.steps, world, B["dev_ms"] * 1e-3)
     e2e_value = job_throughput(nb * n * args.heun * B["k_e2e"], world, B["e2e_s"])
     px, py = B["fft"]
-    ab = {k: v * nb for k, v in algorithmic_bytes(SIDE, SIDE, px, py).items()}
+    # every run of the batch shares the first run's tensor (same geometry)
+    ab = algorithmic_bytes(SIDE, SIDE, px, py, runs=nb, tensors=1)
     prof = B["prof"]
     per_kernel = {"row_pred": prof[0], "col": 0.5 * (prof[1] + prof[3]), "row_corr": prof[2]}
     launches_per_heun = {"row_pred": 1, "col": 2, "row_corr": 1}

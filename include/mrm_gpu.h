@@ -350,6 +350,17 @@ int mrm_gpu_get_shape(const mrm_gpu* h, int* out3);
  * in mrm_gpu_last_error() if it was set.  The stepping calls do this at every
  * synchronisation. */
 int mrm_gpu_check_device(mrm_gpu* h);
+/* Device failure self-test (no counterpart in the reference: its CPU code has
+ * no device waits).  Runs one field-evaluation launch of the row kernel on
+ * the handle's stream in which every block's bounded wait for its grain rows
+ * is made to run out (the barrier expects 16 bytes that no copy sends), so
+ * each block takes the path of a bulk copy that never lands: it raises the
+ * device error flag, waits once more (bounded) and returns, writing nothing.
+ * Takes about two seconds; returns what the handle's next synchronisation
+ * reports, MRM_ERR_DEVICE with "a bulk-copy wait ran out" in
+ * mrm_gpu_last_error().  The flag is cleared on that report and the handle
+ * stays usable. */
+int mrm_gpu_selftest_timeout(mrm_gpu* h);
 /* Advances `reps` Heun steps launching each kernel bracketed by CUDA events
  * on the handle's stream; ms_out[4] = mean ms of row(predictor), column,
  * row(corrector), column launches (the demag column launches are 0 when

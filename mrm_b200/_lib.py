@@ -35,6 +35,7 @@ EXPORTS = [
     "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
     "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile", "mrm_gpu_set_head_field",
     "mrm_gpu_set_shape", "mrm_gpu_set_autotune", "mrm_gpu_get_shape", "mrm_gpu_check_device",
+    "mrm_gpu_selftest_timeout",
     "mrm_gpu_set_cubic_axes", "mrm_gpu_step_adaptive", "mrm_gpu_off_field", "mrm_gpu_set_field_table",
     "mrm_gpu_set_window", "mrm_gpu_get_window", "mrm_gpu_set_llb", "mrm_gpu_set_mag", "mrm_gpu_get_mag",
     "mrm_gpu_set_mt", "mrm_gpu_set_temp_profile", "mrm_gpu_set_temp_function",
@@ -145,6 +146,7 @@ def load(path: str = LIB_PATH):
         "mrm_gpu_set_autotune": ([vp, i], i),
         "mrm_gpu_get_shape": ([vp, P(i)], i),
         "mrm_gpu_check_device": ([vp], i),
+        "mrm_gpu_selftest_timeout": ([vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -29,8 +29,12 @@ namespace mrm {
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
 enum Flags {
   kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32,
-  kFlagMapped = 64, kFlagDemagOnly = 128, kFlagCorrTime = 256
+  kFlagMapped = 64, kFlagDemagOnly = 128, kFlagCorrTime = 256, kFlagProbeTimeout = 512
 };
+// kFlagProbeTimeout (row kernel): the grain-row barrier expects 16 bytes that
+// no copy sends, so every block's bounded wait runs out and the block takes the
+// failure path a lost bulk copy would (error flag, second bounded wait,
+// return) -- the device failure test of mrm_gpu_selftest_timeout.
 // kFlagMapped (kPred, kCorr, kEval): the demag field comes from an earlier
 // evaluation's per-cell values averaged over each grain's cells (L.hdm; L.hd
 // with one grain per cell), not from this launch's inverse row transform.
@@ -887,6 +891,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       if (sp.vu >= 0) copy(&bars[2], stg + sp.vu, mother_u + base, base * v4b, nlay * v4b, nrows * v4row, 280);
       if (sp.vl >= 0) copy(&bars[2], stg + sp.vl, mother_l + base, base * v4b, nlay * v4b, nrows * v4row, 290);
     }
+    if (flags & kFlagProbeTimeout) mbar_expect_tx(&bars[2], 16);  // bytes that never come
     mbar_arrive(&bars[2]);
   }
   // every barrier completes (an unused one on the arrive alone); a block whose

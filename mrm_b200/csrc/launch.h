@@ -41,14 +41,12 @@ constexpr ColVariant col_variant(int v) { return sizeof(R) == sizeof(float) ? kC
 
 // Register column kernel shapes (colreg.cuh: FP32 runs of one layer with
 // 256..1024-point columns); the column shape index selects one of these for
-// those runs and one of kColF32 for the others.  tsm: the columns' tensor
-// slices are staged in shared memory (otherwise read from global memory).
+// those runs and one of kColF32 for the others.
 struct CregVariant {
   int block, minb;
-  bool tsm;
 };
 constexpr int kCregVariants = 3;
-constexpr CregVariant kCreg[kCregVariants] = {{128, 4, true}, {256, 2, true}, {128, 6, false}};
+constexpr CregVariant kCreg[kCregVariants] = {{128, 4}, {256, 2}, {128, 5}};
 
 struct RowLaunch;
 // entry points of one compiled row shape (defined in its own translation unit)
@@ -86,6 +84,10 @@ struct ColLaunch {
   int ntasks;
   size_t smem;
   bool pdl;
+  // register column kernel: persistent blocks (0: one per task) and the
+  // twiddle entries its shared memory holds
+  int blocks = 0;
+  int tw_cap = 0;
 };
 
 // entry points of one compiled column shape (defined in its own translation unit)

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -95,7 +96,11 @@ struct mrm_gpu {
   void* spech = nullptr;
   void* specx = nullptr;
   void* xfer = nullptr;  // 3 x N doubles: host <-> device transfers of one layer's state
+  // tensor spectrum: runs whose tensor was copied from a run of the same
+  // geometry share that run's buffer (tens_buf owns it; tens is its address),
+  // so a batch of one geometry reads one tensor, which stays in L2
   void* tens = nullptr;
+  std::shared_ptr<void> tens_buf;
   bool tensor_ready = false;
   bool demag = true;
   double tensor_resid = 0.0, tensor_kept = 0.0;
@@ -145,6 +150,7 @@ struct Engine {
   int stage_cap[kRowSlots] = {0, 0, 0, 0, 0, 0};
   size_t smem_col = 0;
   size_t smem_creg = 0;
+  int creg_tw_cap = 0, creg_blocks = 0;  // register column kernel: twiddle room, persistent blocks
   // the corrector with reductions always runs row shape 0 over one-row tasks,
   // so that the FP64 reductions do not depend on the tuned shapes
   Task* d_stasks = nullptr;
@@ -205,6 +211,12 @@ void dfree(void*& p) {
   if (p) cudaFree(p);
   p = nullptr;
 }
+
+struct CudaFreeDeleter {
+  void operator()(void* p) const {
+    if (p) cudaFree(p);
+  }
+};
 template <typename T>
 void dfree(T*& p) {
   if (p) cudaFree(p);
@@ -435,7 +447,9 @@ int validate_geom(const mrm_geom* g, std::string* errp, bool* big = nullptr) {
   const size_t rs = (f64 ? (size_t)row_fft_smem<double>(tmp.lgpx, 1) : (size_t)row_fft_smem<float>(tmp.lgpx, 1)) +
                     (size_t)(f64 ? head_table_bytes<double>(g->nx) : head_table_bytes<float>(g->nx));
   const size_t cs = f64 ? col_smem_of<double>(&tmp, 1, 0)
-                       : creg_run(&tmp) ? (size_t)creg_smem(tmp.lgpy, kCreg[1].block, kCreg[1].tsm) : col_smem_of<float>(&tmp, 1, 0);
+                       : creg_run(&tmp) ? (size_t)creg_smem(col_tw_count(tmp.lgpy), kCreg[1].block,
+                                                            creg_stage_bytes(spec_col_stride(g->ny), 3))
+                                        : col_smem_of<float>(&tmp, 1, 0);
   if (rs + row_static_bytes(3) > kMaxSmem || cs + 64 > kMaxSmem)
     return set_err(errp, MRM_ERR_UNSUPPORTED, "FFT grid %d x %d x %d layers exceeds shared memory", px,
                    py, g->n_lay);
@@ -584,7 +598,8 @@ int plan_smem(Engine* e) {
   const RowVariant rv = row_variant<R>(e->rowv);
   size_t fft = 16;
   int need[kSlots] = {0, 0, 0, 0, 0, 0};
-  size_t scol = 16, screg = 16;
+  size_t scol = 16;
+  int tw_cap = 0, stage_bytes = 0;
   for (auto* r : e->runs) {
     if (r->lgpx > rv.lgmax)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d does not cover %d-column FFT grids", e->rowv, r->px);
@@ -592,8 +607,10 @@ int plan_smem(Engine* e) {
     fft = std::max(fft, row_fixed_smem<R>(r, rv.rpb));
     for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
     if (r->demag && r->tensor_ready) {
-      if (creg_run(r)) screg = std::max(screg, (size_t)creg_smem(r->lgpy, kCreg[creg_v(e)].block, kCreg[creg_v(e)].tsm));
-      else scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r), col_variant<R>(e->colv).minb));
+      if (creg_run(r)) {
+        tw_cap = std::max(tw_cap, col_tw_count(r->lgpy));
+        stage_bytes = std::max(stage_bytes, creg_stage_bytes(spec_col_stride(fny(r)), r->lgct));
+      } else scol = std::max(scol, col_smem_of<R>(r, cols_per_task(e, r), col_variant<R>(e->colv).minb));
     }
   }
   for (int q = 0; q < kSlots; ++q) {
@@ -607,8 +624,10 @@ int plan_smem(Engine* e) {
   }
   if (scol + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
   e->smem_col = scol;
+  const size_t screg = tw_cap ? (size_t)creg_smem(tw_cap, kCreg[creg_v(e)].block, stage_bytes) : 16;
   if (screg + 64 > kMaxSmem) return set_err(errp, MRM_ERR_UNSUPPORTED, "column shape exceeds shared memory");
   e->smem_creg = screg;
+  e->creg_tw_cap = tw_cap;
   CK(row_allow_smem<R>(e->rowv, e->smem_row));
   // the reductions launches (kPred of the single-stage integrator, kCorr):
   // row shape 0, one row per task
@@ -633,7 +652,15 @@ int plan_smem(Engine* e) {
     CK(row_allow_smem<R>(0, lim));
   }
   CK(col_allow_smem<R>(e->colv, e->smem_col));
-  if (sizeof(R) == sizeof(float)) CK(creg_allow_smem(creg_v(e), e->smem_creg));
+  e->creg_blocks = 0;
+  if (sizeof(R) == sizeof(float) && e->creg_tw_cap) {
+    CK(creg_allow_smem(creg_v(e), e->smem_creg));
+    // persistent blocks: as many as stay resident
+    int per_sm = 0, sms = 0;
+    CK(creg_occupancy(creg_v(e), e->smem_creg, &per_sm));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev));
+    e->creg_blocks = std::max(1, per_sm) * sms;
+  }
   return MRM_OK;
 }
 
@@ -779,6 +806,8 @@ cudaError_t launch_col_e(Engine* e, int istep, int flags, bool pdl = true) {
   }
   if (e->nct2) {
     ColLaunch a{e->st, e->d_runs, e->d_ctasks2, e->d_tw, e->d_err, e->nct2, e->smem_creg, pdl};
+    a.blocks = e->creg_blocks;
+    a.tw_cap = e->creg_tw_cap;
     return launch_creg(creg_v(e), a, istep, flags);
   }
   return cudaSuccess;
@@ -1260,6 +1289,21 @@ int spectra_alloc(mrm_gpu* r) {
   return rc;
 }
 
+// the run's own tensor buffer (tensor_bytes), replacing any shared one
+int tensor_alloc(mrm_gpu* r) {
+  std::string* errp = &r->err;
+  void* p = nullptr;
+  int rc = dmalloc(errp, &p, tensor_bytes(r));
+  if (rc) return rc;
+  r->tens_buf = std::shared_ptr<void>(p, CudaFreeDeleter());
+  r->tens = p;
+  return MRM_OK;
+}
+void tensor_release(mrm_gpu* r) {
+  r->tens_buf.reset();
+  r->tens = nullptr;
+}
+
 int run_alloc(mrm_gpu* r) {
   std::string* errp = &r->err;
   const size_t re = relem(r->g.precision);
@@ -1267,7 +1311,7 @@ int run_alloc(mrm_gpu* r) {
   if (rc) return rc;
   rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
   if (rc) return rc;
-  rc = r->fft_big ? MRM_OK : dmalloc(errp, &r->tens, tensor_bytes(r));
+  rc = r->fft_big ? MRM_OK : tensor_alloc(r);
   if (rc) return rc;
   const size_t n = (size_t)r->g.nx * r->g.ny;
   for (int l = 0; l < r->nl; ++l) {
@@ -1289,7 +1333,7 @@ void run_free(mrm_gpu* r) {
   dfree(r->spech);
   dfree(r->specx);
   dfree(r->xfer);
-  dfree(r->tens);
+  tensor_release(r);
   for (int l = 0; l < MRM_MAX_LAYERS; ++l) {
     LayerBufs& b = r->L[l];
     dfree(b.m); dfree(b.mp); dfree(b.dm); dfree(b.hf); dfree(b.hd); dfree(b.ht); dfree(b.pa); dfree(b.pb); dfree(b.pv);
@@ -1606,6 +1650,12 @@ int tensor_real(mrm_gpu* r, double* d_n2d) {
 int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   std::string* errp = &r->err;
   Engine* e = r->eng;
+  // a buffer shared with other runs is left to them: this run writes its own
+  if (!r->tens_buf || r->tens_buf.use_count() > 1) {
+    CK(cudaStreamSynchronize(e->st));
+    int rc0 = tensor_alloc(r);
+    if (rc0) return rc0;
+  }
   const int npair = r->nl * r->nl, ph = r->px / 2 + 1, pyh = r->py / 2 + 1;
   const int planes = npair * 9;
   void* d_spec = nullptr;
@@ -2028,9 +2078,13 @@ int mrm_gpu_copy_tensor(mrm_gpu* dst, const mrm_gpu* src) {
       dst->g.num_images != src->g.num_images)
     return set_err(errp, MRM_ERR_ARG, "cell size or boundary differs");
   CK(cudaSetDevice(dst->eng->dev));
+  // the same geometry has the same tensor: share the source's buffer (it is
+  // only read from now on; a later build or upload on either run writes a
+  // buffer of its own)
   CK(cudaStreamSynchronize(src->eng->st));
-  CK(cudaMemcpyAsync(dst->tens, src->tens, tensor_bytes(dst), cudaMemcpyDeviceToDevice, dst->eng->st));
   CK(cudaStreamSynchronize(dst->eng->st));
+  dst->tens_buf = src->tens_buf;
+  dst->tens = src->tens;
   dst->tensor_ready = true;
   dst->tensor_resid = src->tensor_resid;
   dst->tensor_kept = src->tensor_kept;
@@ -2685,7 +2739,7 @@ int mrm_gpu_set_window(mrm_gpu* h, int nx_win, int ny_win, double vx, double vy,
   CK(cudaStreamSynchronize(e->st));
   dfree(h->spech);
   dfree(h->specx);
-  dfree(h->tens);
+  tensor_release(h);
   h->wnx = none ? 0 : nx_win;
   h->wny = none ? 0 : ny_win;
   h->wvx = vx;
@@ -2697,7 +2751,7 @@ int mrm_gpu_set_window(mrm_gpu* h, int nx_win, int ny_win, double vx, double vy,
   h->lgpx = ilog2(h->px);
   h->lgpy = ilog2(h->py);
   rc = spectra_alloc(h);
-  if (!rc) rc = dmalloc(errp, &h->tens, tensor_bytes(h));
+  if (!rc) rc = tensor_alloc(h);
   if (rc) return rc;
   h->tensor_ready = false;  // the window's tensor: build or upload it again
   h->spec_valid = false;
@@ -2886,6 +2940,30 @@ int mrm_gpu_set_autotune(mrm_gpu* h, int on) {
   h->eng->autotune = on != 0;
   h->eng->tables_dirty = true;
   return MRM_OK;
+}
+
+int mrm_gpu_selftest_timeout(mrm_gpu* h) {
+  if (!h) return MRM_ERR_ARG;
+  std::string* errp = &h->err;
+  for (int l = 0; l < h->nl; ++l)
+    if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
+  if (h->demag && !h->tensor_ready) return set_err(errp, MRM_ERR_STATE, "build or upload the tensor first (or disable demag)");
+  Engine* e = h->eng;
+  CK(cudaSetDevice(e->dev));
+  int rc = check_device_error(e);  // an earlier failure is reported as such
+  if (rc) {
+    h->err = e->err;
+    return rc;
+  }
+  rc = e->prec == MRM_FP64 ? ensure_ready<double>(e) : ensure_ready<float>(e);
+  if (!rc) {
+    cudaError_t ce = e->prec == MRM_FP64 ? launch_row_e<double>(e, kEval, false, 0, kFlagForce | kFlagProbeTimeout)
+                                         : launch_row_e<float>(e, kEval, false, 0, kFlagForce | kFlagProbeTimeout);
+    if (ce != cudaSuccess) rc = set_err(&e->err, MRM_ERR_CUDA, "self-test launch: %s", cudaGetErrorString(ce));
+  }
+  if (!rc) rc = check_device_error(e);
+  if (rc) h->err = e->err;
+  return rc;
 }
 
 int mrm_gpu_check_device(mrm_gpu* h) {
@@ -3324,9 +3402,14 @@ int mrm_gpu_demag_noalloc(mrm_gpu* h, const float* m, float* hdemag, void* strea
   CK(launch_row<float>(0, kInit, false,
                        RowLaunch{st, desc, rt, e->d_tw, nullptr, e->d_err, nrt, fft + cap_init, cap_init, false, head},
                        0, kFlagForce));
-  if (creg)
-    CK(launch_creg(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, (size_t)creg_smem(h->lgpy, kCreg[0].block, kCreg[0].tsm), true},
-                   0, kFlagForce));
+  if (creg) {
+    ColLaunch a{st, desc, ct, e->d_tw, e->d_err, nct,
+                (size_t)creg_smem(col_tw_count(h->lgpy), kCreg[0].block,
+                                  creg_stage_bytes(spec_col_stride(ny), ilog2(cpt))),
+                true};
+    a.tw_cap = col_tw_count(h->lgpy);
+    CK(launch_creg(0, a, 0, kFlagForce));
+  }
   else
     CK(launch_col<float>(0, ColLaunch{st, desc, ct, e->d_tw, e->d_err, nct, col_smem_of<float>(h, cpt, col_variant<float>(0).minb), true}, 0,
                          kFlagForce));

@@ -18,11 +18,17 @@ Requests that arrive while others are on the GPU are admitted as soon as
 memory frees up and join the next launch; a run's trajectory does not depend
 on its neighbours (each run's kernels read only its own data), which the
 tests check bit for bit against the same request run alone.
+
+A request can carry a timeout (seconds after its arrival) and can be
+cancelled (Server.cancel, from any thread).  At each call boundary the loop
+retires such requests -- queued or running -- with status "timeout" or
+"cancelled" and the samples taken so far, and frees their memory; the other
+runs continue unchanged.  Finished requests have status "done".
 """
 from __future__ import annotations
 
 import collections
-import math
+import threading
 import time
 from typing import Callable, Dict, List, Optional
 
@@ -88,6 +94,19 @@ class Server:
         self.sleep = sleep
         self.used = 0
         self.templates: Dict[tuple, object] = {}
+        self._cancel_lock = threading.Lock()
+        self._cancelled: set = set()
+
+    def cancel(self, rid: int):
+        """Asks the serving loop to drop request `rid` at its next call
+        boundary (queued or running); thread-safe."""
+        with self._cancel_lock:
+            self._cancelled.add(int(rid))
+
+    def _take_cancelled(self) -> set:
+        with self._cancel_lock:
+            c, self._cancelled = self._cancelled, set()
+        return c
 
     def _admit(self, req: Request, med, fp: int, now: float):
         key = (req.side, req.side)
@@ -96,6 +115,28 @@ class Server:
         if tmpl is None:
             self.templates[key] = self.be.make_template(run)
         return _Active(req, run, fp, now)
+
+    def _retire(self, a: Optional[_Active], req: Request, status: str, now: float, s=None) -> dict:
+        """Result record of a request that leaves the server (a: its run, or
+        None when it never left the queue)."""
+        samples = a.samples if a is not None else []
+        res = {"rid": req.rid, "kind": req.kind, "grains": req.grains, "steps": req.steps,
+               "arrival": req.arrival, "admitted": a.admitted if a is not None else None,
+               "finished": now, "latency": now - req.arrival, "status": status,
+               "steps_done": req.steps - (a.remaining if a is not None else req.steps),
+               "samples": len(samples)}
+        if s is not None:
+            res["final_mave"] = np.asarray(s["mave"]).tolist()
+            res["step"] = int(s["step"])
+        if status == "done" and req.kind == "mh":
+            ts = np.array(samples)
+            res["hc"], res["mr"] = coercivity(ts[:, 1], ts[:, 2])
+        if a is not None:
+            if self.keep_state and status == "done":
+                res["m"] = self.be.get_state(a.run)
+            self.be.remove(a.run)
+            self.used -= a.fp
+        return res
 
     def run(self, requests: List[Request]) -> dict:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
@@ -108,6 +149,19 @@ class Server:
             now = self.clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
+            # cancellations and timeouts, at a call boundary: queued or running
+            cancelled = self._take_cancelled()
+            for rid in cancelled:
+                for q in [p for p in pending if p.rid == rid]:
+                    pending.remove(q)
+                    results.append(self._retire(None, q, "cancelled", now))
+            expired = lambda r: r.timeout is not None and now - r.arrival >= r.timeout  # noqa: E731
+            for q in [q for q in queue if q.rid in cancelled or expired(q)]:
+                queue.remove(q)
+                results.append(self._retire(None, q, "cancelled" if q.rid in cancelled else "timeout", now))
+            for a in [a for a in active if a.req.rid in cancelled or expired(a.req)]:
+                active.remove(a)
+                results.append(self._retire(a, a.req, "cancelled" if a.req.rid in cancelled else "timeout", now))
             # admission, first come first served, by device footprint
             while queue and len(active) < self.max_active:
                 req = queue[0]
@@ -138,28 +192,18 @@ class Server:
                 if a.remaining <= 0:
                     finished.append((a, s))
             for a, s in finished:
-                ts = np.array(a.samples)
-                res = {"rid": a.req.rid, "kind": a.req.kind, "grains": a.req.grains,
-                       "steps": a.req.steps, "arrival": a.req.arrival, "admitted": a.admitted,
-                       "finished": done_t, "latency": done_t - a.req.arrival,
-                       "final_mave": np.asarray(s["mave"]).tolist(), "step": int(s["step"]),
-                       "samples": len(a.samples)}
-                if a.req.kind == "mh":
-                    hc, mr = coercivity(ts[:, 1], ts[:, 2])
-                    res["hc"], res["mr"] = hc, mr
-                if self.keep_state:
-                    res["m"] = self.be.get_state(a.run)
-                results.append(res)
-                self.be.remove(a.run)
-                self.used -= a.fp
                 active.remove(a)
+                results.append(self._retire(a, a.req, "done", done_t, s))
         wall = self.clock() - t0
-        lat = np.array([r["latency"] for r in results]) if results else np.zeros(1)
-        gs = sum(r["grains"] * r["steps"] for r in results)
+        done = [r for r in results if r["status"] == "done"]
+        lat = np.array([r["latency"] for r in done]) if done else np.zeros(1)
+        gs = sum(r["grains"] * r["steps_done"] for r in results)
         return {"results": sorted(results, key=lambda r: r["rid"]), "wall_s": wall,
                 "grain_steps": gs, "grain_steps_per_s": gs / wall if wall > 0 else 0.0,
                 "p50_latency_s": float(np.percentile(lat, 50)),
-                "p99_latency_s": float(np.percentile(lat, 99)), "calls": calls}
+                "p99_latency_s": float(np.percentile(lat, 99)), "calls": calls,
+                "completed": len(done), "timed_out": sum(r["status"] == "timeout" for r in results),
+                "cancelled": sum(r["status"] == "cancelled" for r in results)}
 
 
 class GpuBackend:

@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import List
+from typing import List, Optional
 
 import numpy as np
 
@@ -49,6 +49,7 @@ class Request:
     temperature: float
     steps: int
     seed: int
+    timeout: Optional[float] = None  # s after arrival; the server gives up on the request then
 
     @property
     def grains(self) -> int:

@@ -67,6 +67,25 @@ def test_tensor_copy_matches_build(gpulib):
     b.close()
 
 
+def test_shared_tensor_copy_on_write(gpulib):
+    """Runs whose tensor is copied from another run of the same geometry share
+    its buffer; a later upload on the source gives the source a buffer of its
+    own and leaves the copies' tensor as it was."""
+    m = media.mh_medium(32, seed=4)
+    b = Batch(FP32)
+    r1 = b.add(m, steps=40)
+    r2 = b.add(m, steps=40, tensor_from=r1)
+    n2d = r1.download_tensor()
+    r1.upload_tensor(2.0 * n2d)  # the source's tensor changes; r2 keeps the original
+    b.step(40)
+    g = GpuSim(m, precision=FP32, tensor=n2d)
+    g.step(40, 1e-13)
+    assert np.array_equal(r2.get_state(0), g.get_state(0))
+    assert not np.array_equal(r1.get_state(0), r2.get_state(0))
+    g.close()
+    b.close()
+
+
 def test_served_results_equal_alone(gpulib):
     reqs = [Request(0, 0.0, "mh", 32, 300.0, 300, 31), Request(1, 0.0, "write", 64, 260.0, 500, 32),
             Request(2, 0.0, "mh", 32, 340.0, 700, 33), Request(3, 0.05, "mh", 64, 300.0, 200, 34),

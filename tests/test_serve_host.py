@@ -116,3 +116,54 @@ def test_coercivity_interpolation():
     hc, mr = coercivity(h, mh)
     assert abs(hc - 9000.0) < 60.0
     assert abs(mr - np.tanh(9000.0 / 1500.0)) < 1e-3
+
+
+def test_timeouts_retire_queued_and_running_requests():
+    """A request whose timeout passes is dropped at the next call boundary,
+    whether it still waits for memory or is on the device; the others finish
+    with their exact step counts and the memory of the dropped ones is freed."""
+    reqs = [Request(0, 0.0, "mh", 64, 300.0, 4000, 1, timeout=0.05),   # running when it times out
+            Request(1, 0.0, "mh", 64, 300.0, 600, 2),
+            Request(2, 0.0, "mh", 64, 300.0, 600, 3, timeout=0.01),    # still queued (no memory yet)
+            Request(3, 0.001, "write", 32, 300.0, 300, 4, timeout=10.0)]
+    be = FakeBackend(budget_bytes=10**12)
+    fp = 64 * 64 * 300
+    srv = Server(backend=be, hbm_budget=2 * fp, chunk=100, clock=be.clock, sleep=be.sleep)
+    out = srv.run(reqs)
+    res = {r["rid"]: r for r in out["results"]}
+    assert len(res) == 4
+    assert res[0]["status"] == "timeout" and 0 < res[0]["steps_done"] < 4000
+    assert res[0]["finished"] - res[0]["arrival"] >= 0.05
+    assert res[2]["status"] == "timeout" and res[2]["admitted"] is None and res[2]["steps_done"] == 0
+    for rid in (1, 3):
+        assert res[rid]["status"] == "done" and res[rid]["step"] == reqs[rid].steps
+    assert out["timed_out"] == 2 and out["completed"] == 2
+    assert be.used == 0 and not be.runs  # every run left the device
+    assert out["grain_steps"] == sum(r["grains"] * r["steps_done"] for r in out["results"])
+
+
+def test_cancellation_from_another_thread():
+    """Server.cancel from another thread (here: from inside a launch) drops the
+    request at the next call boundary; a cancelled request that has not
+    arrived yet never runs."""
+    reqs = [Request(0, 0.0, "mh", 64, 300.0, 3000, 1), Request(1, 0.0, "mh", 32, 300.0, 900, 2),
+            Request(2, 5.0, "mh", 32, 300.0, 900, 3)]
+    be = FakeBackend(budget_bytes=10**12)
+    srv = Server(backend=be, chunk=100, clock=be.clock, sleep=be.sleep)
+    step = be.step
+
+    def step_and_cancel(k):
+        step(k)
+        if len(be.calls) == 3:
+            import threading
+            t = threading.Thread(target=lambda: (srv.cancel(0), srv.cancel(2)))
+            t.start()
+            t.join()
+
+    be.step = step_and_cancel
+    out = srv.run(reqs)
+    res = {r["rid"]: r for r in out["results"]}
+    assert res[0]["status"] == "cancelled" and res[0]["steps_done"] == 300
+    assert res[2]["status"] == "cancelled" and res[2]["steps_done"] == 0 and res[2]["admitted"] is None
+    assert res[1]["status"] == "done" and res[1]["step"] == 900
+    assert out["cancelled"] == 2 and not be.runs
