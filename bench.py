@@ -20,9 +20,9 @@ Beside the headline (sub-objects of the same JSON line):
            Hk sigma in [3 %, 10 %], 5,000 Heun steps each, one batch;
   write    the two-layer 1,024 x 256 recording write by the moving Karlqvist
            head (PRBS pattern), a bounded 2,000-step sample;
-  served   a bounded sample of the Poisson request stream (200 req/s, M(H)
-           and write requests of 1,024..262,144 grains, 2,000..20,000 steps):
-           aggregate grain-steps/s and p50/p99 latency.
+  served   the first 200 requests of the Poisson request stream (200 req/s,
+           M(H) and write requests of 1,024..262,144 grains, 2,000..20,000
+           steps): aggregate grain-steps/s and p50/p99 latency.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -173,13 +173,26 @@ def coercivity(h, mh):
     return hc, mr
 
 
-def cpu_baseline_sample(threads: int, min_s: float = 10.0, chunk: int = 25, max_steps: int = 2000):
-    """Oracle port (FP64, OpenMP) timed on a bounded sample of the same workload."""
+def cpu_model() -> str:
+    try:
+        for line in subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def oracle_rate(threads: int, fft_bits: int, min_s: float, chunk: int = 10, max_steps: int = 2000) -> float:
+    """Grain-steps/s of the CPU port (oracle/) on one 65,536-grain realisation of
+    the headline medium: `threads` OpenMP threads, FP32 or FP64 FFT grids
+    (the reference's default single-precision FFTW build or its FFTD=1
+    build; state and fields FP64 in both), timed after 2 warm-up steps."""
     from oracle import pyoracle
     pyoracle.build()
     pyoracle.set_threads(threads)
     med = make_medium()
-    sim = pyoracle.OracleSim(med, rng_mode=1, seed=1)
+    sim = pyoracle.OracleSim(med, rng_mode=1, seed=1, fft_bits=fft_bits)
     sim.step(2, DT)
     done, t0 = 0, time.perf_counter()
     while done < max_steps:
@@ -188,20 +201,38 @@ def cpu_baseline_sample(threads: int, min_s: float = 10.0, chunk: int = 25, max_
         if time.perf_counter() - t0 >= min_s:
             break
     el = time.perf_counter() - t0
-    n = med.n_grains
     sim.close()
+    return med.n_grains * done / el
+
+
+def cpu_baseline_sample(threads: int, reps: int = 3, min_s: float = 3.0):
+    """The CPU port on the host cores: FP32 grids on all threads (median of
+    `reps` samples; the like-precision baseline of the FP32 GPU path), FP64 on
+    all threads, FP32 on 4 threads (the reference's own openmp setting) and on
+    1 thread.  About 20 s of CPU work."""
+    from oracle import pyoracle
+    f32 = sorted(oracle_rate(threads, 32, min_s) for _ in range(reps))
+    variants = {
+        f"fp32_{threads}t_median_of_{reps}": f32[len(f32) // 2],
+        f"fp64_{threads}t": oracle_rate(threads, 64, min_s),
+        "fp32_4t": oracle_rate(min(4, threads), 32, min_s),
+        "fp32_1t": oracle_rate(1, 32, min_s),
+    }
     # the write leg's readback call on the oracle (initial state of the same medium)
     from mrm_b200 import media
+    pyoracle.set_threads(threads)
     wsim = pyoracle.OracleSim(media.head_write_medium(1024, 256, seed=1, prbs_seed=1, temperature=300.0),
                               rng_mode=1, seed=1, demag=False)
     t0 = time.perf_counter()
     wsim.off_field(**READBACK)
     off_ms = (time.perf_counter() - t0) * 1e3
     wsim.close()
-    return {"value": n * done / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{done} Heun steps of one {n}-grain realisation in {el:.1f} s (FP64 oracle, "
-                      f"OpenMP, after 2 warm-up steps; tensor build excluded)",
-            "readback_ms_per_call": off_ms}
+    return {"value": f32[len(f32) // 2], "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu": cpu_model(), "nproc": os.cpu_count(),
+            "sample": f"Heun steps of one 65,536-grain realisation for {min_s:.0f} s per sample after 2 warm-up "
+                      f"steps (oracle port, OpenMP, FP32 FFT grids with FP64 state and fields; tensor build "
+                      f"excluded); value: median of {reps} samples on {threads} threads",
+            "variants": variants, "readback_ms_per_call": off_ms}
 
 
 def run_reference(args, rank, world):
@@ -212,7 +243,8 @@ def run_reference(args, rank, world):
     pyoracle.build()
     pyoracle.set_threads(threads)
     med = make_medium()
-    sim = pyoracle.OracleSim(med, rng_mode=1, seed=1)
+    # FP32 FFT grids, as the reference's default single-precision FFTW build
+    sim = pyoracle.OracleSim(med, rng_mode=1, seed=1, fft_bits=32)
     per = 4  # Heun steps of one realisation per bench step: a bounded sample
     for _ in range(args.warmup):
         sim.step(per, DT)
@@ -225,12 +257,13 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded media)",
         "config": {"workload": WORKLOAD.format(b=args.batch) +
                    f"; CPU sample: {per} Heun steps of one realisation per bench step",
-                   "grains": n, "heun_steps_per_bench_step": per},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                   "grains": n, "heun_steps_per_bench_step": per,
+                   "precision": "FP32 FFT grids, FP64 state and fields (the reference's default build)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
                          "sample": f"{per} Heun steps x {args.steps} bench steps of one {n}-grain realisation"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -542,8 +575,9 @@ def served_leg(local, nreq):
     be.close()
     return {"workload": f"first {nreq} requests of the seeded Poisson stream (200 req/s, M(H) and STE "
                         "write requests, 1,024..262,144 grains, T 250..350 K, 2,000..20,000 Heun steps)",
-            "requests": nreq, "value": out["grain_steps_per_s"], "unit": UNIT,
+            "requests": nreq, "completed": out["completed"], "value": out["grain_steps_per_s"], "unit": UNIT,
             "p50_latency_s": out["p50_latency_s"], "p99_latency_s": out["p99_latency_s"],
+            "latency_over": f"the {out['completed']} completed requests, arrival to result",
             "wall_s": out["wall_s"], "launch_calls": out["calls"]}
 
 
@@ -556,7 +590,7 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="realisations in the headline batch")
     ap.add_argument("--heun", type=int, default=HEUN_PER_STEP, help="Heun steps per bench step")
     ap.add_argument("--e2e-steps", type=int, default=50, help="bench steps of the end-to-end leg")
-    ap.add_argument("--served", type=int, default=48, help="requests of the served sample (0: skip)")
+    ap.add_argument("--served", type=int, default=200, help="requests of the served sample (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="",
                     help="row,column,columns-per-task kernel shapes of the batch (default: autotuned)")

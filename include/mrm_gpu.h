@@ -150,7 +150,12 @@ int mrm_gpu_set_uniform_field(mrm_gpu* h, int layer, const double hdir[3], doubl
  * applied.f90:263-297,328-377,866-869):
  * h_app(t) = (amp*f(t) + dc)*scale*hdir, f = 1 sin(t*gamma+phase),
  * 2 cos(t*gamma+phase), 3 exp(t*gamma+phase), 4 STE (trapezoidal square wave
- * of period gamma and rise time param), 5 NEW (exponential pulse train). */
+ * of period gamma and rise time param), 5 NEW (exponential pulse train),
+ * 7 ROT (applied.f90:378-392 with the rotation angles given, |gamma| != 1):
+ * f = 1 and hdir replaced by the in-plane direction
+ * (cos((2 gamma t + phase) pi), sin((2 gamma t + phase) pi), 0); hdir still
+ * defines N+ in the stats.  |gamma| = 1 (a field that follows the mean
+ * magnetisation step by step) returns MRM_ERR_UNSUPPORTED. */
 int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int func, double amp,
                                double gamma, double phase, double param, double duty,
                                double moddepth, double dc, double scale);

@@ -120,7 +120,7 @@ struct LayerDev {
   const R* lcol;
   double hdir[3];
   double t_start, t_end, s_start, s_end, scale;
-  int func;  // 0 linear ramp; 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW (applied.f90:328-377); 6 head
+  int func;  // 0 linear ramp; 1 SIN, 2 COS, 3 EXP, 4 STE, 5 NEW, 7 ROT (applied.f90:328-396); 6 head
   double amp, fgamma, phase, param, duty, moddepth, dc;
   // moving write head (func 6): Karlqvist field of a ring head, gap hd_gap, at
   // distance hd_z above the layer's mid-plane, deep-gap field hd_hg, gap centre
@@ -171,6 +171,7 @@ struct RunDev {
 };
 
 constexpr int kFuncHead = 6;
+constexpr int kFuncRot = 7;  // the ROT time function: an in-plane field rotating at rate gamma
 
 // Tensor component parity (c = 3*field + source): the spectrum is purely
 // imaginary for xz, yz, zx, zy and odd in ky for xy, yx, yz, zy.

@@ -29,8 +29,10 @@ namespace mrm {
 enum Stage { kInit = 0, kPred = 1, kCorr = 2, kEval = 3 };
 enum Flags {
   kFlagStats = 1, kFlagForce = 2, kFlagStoreField = 4, kFlagBoris = 8, kFlagMid = 16, kFlagStoredField = 32,
-  kFlagMapped = 64, kFlagDemagOnly = 128, kFlagCorrTime = 256, kFlagProbeTimeout = 512
+  kFlagMapped = 64, kFlagDemagOnly = 128, kFlagCorrTime = 256, kFlagProbeTimeout = 512, kFlagRot = 1024
 };
+// kFlagRot (with kFlagBoris): the analytic-rotation push of llg_type 1 / -1
+// in place of the semi-implicit one (push_llg, llg.f90:1093-1107).
 // kFlagProbeTimeout (row kernel): the grain-row barrier expects 16 bytes that
 // no copy sends, so every block's bounded wait runs out and the block takes the
 // failure path a lost bulk copy would (error flag, second bounded wait,
@@ -56,9 +58,76 @@ MRM_D void cross3(R ax, R ay, R az, R bx, R by, R bz, R& cx, R& cy, R& cz) {
   cz = ax * by - ay * bx;
 }
 
-// funct (applied.f90:328-377); Fortran mod(x,g) = x - int(x/g)*g = fmod
+// rotate_q (transform.f90:65-74): m -> w ** (0, m) ** w* for the quaternion w
+MRM_D void rotate_q(const double* w, const double* m, double* t) {
+  const double w1 = w[0] * w[0], w2 = w[1] * w[1], w3 = w[2] * w[2], w4 = w[3] * w[3];
+  t[0] = 2.0 * (m[2] * (w[0] * w[2] + w[1] * w[3]) + m[1] * (w[1] * w[2] - w[0] * w[3])) + m[0] * (w1 + w2 - w3 - w4);
+  t[1] = 2.0 * (m[0] * (w[0] * w[3] + w[1] * w[2]) + m[2] * (w[2] * w[3] - w[0] * w[1])) + m[1] * (w1 + w3 - w2 - w4);
+  t[2] = 2.0 * (m[1] * (w[0] * w[1] + w[2] * w[3]) + m[0] * (w[1] * w[3] - w[0] * w[2])) + m[2] * (w1 + w4 - w3 - w2);
+}
+
+// rotate_2 (transform.f90:97-115) with norm0 given and norm1 absent: m
+// rotated about u0 (normalised; (0,0,1) and no turn if it is zero) by th0,
+// then about u1 (as given) by th1
+MRM_D void rotate_2(double th0, const double* u0, double th1, const double* u1, const double* m, double* t) {
+  double st1 = 0.5 * th1, st0 = 0.5 * th0;
+  double t0[3] = {u0[0], u0[1], u0[2]};
+  const double n0 = sqrt(t0[0] * t0[0] + t0[1] * t0[1] + t0[2] * t0[2]);
+  if (n0 != 0.0) {
+    t0[0] /= n0;
+    t0[1] /= n0;
+    t0[2] /= n0;
+  } else {
+    t0[0] = 0.0;
+    t0[1] = 0.0;
+    t0[2] = 1.0;
+    st0 = 0.0;
+  }
+  if (st0 == 0.0 && st0 == st1) {
+    t[0] = m[0];
+    t[1] = m[1];
+    t[2] = m[2];
+    return;
+  }
+  const double ct1 = cos(st1);
+  st1 = sin(st1);
+  const double ct0 = cos(st0);
+  st0 = sin(st0);
+  const double* t1 = u1;
+  const double q[4] = {ct0 * ct1 - (t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2]) * st0 * st1,
+                       t0[0] * ct1 * st0 + (t1[0] * ct0 + (t1[1] * t0[2] - t0[1] * t1[2]) * st0) * st1,
+                       t0[1] * ct1 * st0 + (t1[1] * ct0 + (t1[2] * t0[0] - t0[2] * t1[0]) * st0) * st1,
+                       t0[2] * ct1 * st0 + (t1[2] * ct0 + (t1[0] * t0[1] - t0[0] * t1[1]) * st0) * st1};
+  rotate_q(q, m, t);
+}
+
+// Analytic-rotation push of llg_type 1 / -1 (llg.f90:1093-1107), FP64: the
+// precession |s11| about h and the damping turn th0 - 2 atan(e^(s11 a) tan(th0/2))
+// about m x h, s11 = 2 s1 |h| / (1 + a^2), s1 = -gamma dt / 2; d = m' - m
+MRM_D void rot_push(const double* m, const double* h, double s1, double a, double* d) {
+  double y = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+  if (!(y > 0.0)) {
+    d[0] = d[1] = d[2] = 0.0;
+    return;
+  }
+  y = sqrt(y);
+  const double s11 = 2.0 * s1 * y / (1.0 + a * a);
+  const double o[3] = {h[0] / y, h[1] / y, h[2] / y};
+  const double th0 = acos(fmin(1.0, fmax(-1.0, o[0] * m[0] + o[1] * m[1] + o[2] * m[2])));
+  const double u0[3] = {m[1] * o[2] - m[2] * o[1], m[2] * o[0] - m[0] * o[2], m[0] * o[1] - m[1] * o[0]};
+  double t[3];
+  rotate_2(th0 - 2.0 * atan(exp(s11 * a) * tan(0.5 * th0)), u0, fabs(s11), o, m, t);
+  d[0] = t[0] - m[0];
+  d[1] = t[1] - m[1];
+  d[2] = t[2] - m[2];
+}
+
+// funct (applied.f90:328-377); Fortran mod(x,g) = x - int(x/g)*g = fmod.
+// f = 7 (ROT) is its branch with the rotation angles present and |gamma| != 1:
+// magnitude 1 along the rotating direction of rot_dir
 MRM_D double funct(int f, double t, double g, double phase, double param, double duty,
                    double moddepth) {
+  if (f == 7) return 1.0;
   if (f == 1) return sin(t * g + phase);
   if (f == 2) return cos(t * g + phase);
   if (f == 3) return exp(t * g + phase);
@@ -86,6 +155,15 @@ MRM_D double funct(int f, double t, double g, double phase, double param, double
     return 2.0 * (x - g) / param;
   }
   return 0.0;
+}
+
+// direction of a ROT field at time t (applied.f90:382-383, rot_fld :398-416):
+// (cos((2 gamma t + phase) pi), sin((2 gamma t + phase) pi), 0)
+MRM_D void rot_dir(double g, double phase, double t, double* d) {
+  const double th = (2.0 * g * t + phase) * 3.14159265358979323846;
+  d[0] = cos(th);
+  d[1] = sin(th);
+  d[2] = 0.0;
 }
 
 // time scale of a layer's uniform field (applied.f90:866-883; set_fld folds
@@ -963,8 +1041,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const double sc = ramp(L, t_stage);
   const double tps = (GEN == 2 && L.tprof) ? L.tprof->dtemp * temp_scale(*L.tprof, t_stage) : 0.0;
   // a layer's field is its uniform direction or its tabulated profile, scaled
-  const R hax = ftab ? (R)0 : (R)(sc * L.hdir[0]), hay = ftab ? (R)0 : (R)(sc * L.hdir[1]),
-          haz = ftab ? (R)0 : (R)(sc * L.hdir[2]);
+  double hd3[3] = {L.hdir[0], L.hdir[1], L.hdir[2]};
+  if (L.func == kFuncRot) rot_dir(L.fgamma, L.phase, t_stage, hd3);
+  const R hax = ftab ? (R)0 : (R)(sc * hd3[0]), hay = ftab ? (R)0 : (R)(sc * hd3[1]),
+          haz = ftab ? (R)0 : (R)(sc * hd3[2]);
   const R dt = (R)rd.dt;
   const R gamma = (R)L.gamma;
   const R tfac = thermal ? (R)sqrt(L.temperature / rd.dt) : (R)0;  // sqrt(T/dt)
@@ -1218,6 +1298,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       mn = V4<R>{(R)st.m[0], (R)st.m[1], (R)st.m[2], (R)st.mag};
       tq2 = (R)st.tq2;
       d2x = st.d2;
+    } else if (mse > (R)0 && boris && (flags & kFlagRot)) {
+      // analytic rotations (llg.f90:1093-1107), m_n in both stages
+      const V4<R> m0 = (STAGE == kCorr) ? M0[q] : mf;
+      const double s1 = -0.5 * (double)gamma * ((STAGE == kPred && mid) ? 0.5 * rd.dt : rd.dt);
+      R tx, ty, tz;
+      cross3(m0.x, m0.y, m0.z, fx, fy, fz, tx, ty, tz);
+      tq2 = tx * tx + ty * ty + tz * tz;
+      const double mm[3] = {(double)m0.x, (double)m0.y, (double)m0.z}, hh[3] = {(double)fx, (double)fy, (double)fz};
+      double d[3];
+      rot_push(mm, hh, s1, (double)pb.z, d);
+      dx = (R)d[0];
+      dy = (R)d[1];
+      dz = (R)d[2];
+      mn.x = (R)(mm[0] + d[0]);
+      mn.y = (R)(mm[1] + d[1]);
+      mn.z = (R)(mm[2] + d[2]);
     } else if (mse > (R)0 && boris) {
       // semi-implicit push (llg.f90:1109-1118): o = -g dt/2 h - alpha m,
       // d = 2/(1+|o|^2) (m + m x o) x o, m' = m + d (norm preserved, no renormalisation);

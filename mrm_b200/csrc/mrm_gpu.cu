@@ -819,7 +819,11 @@ template <typename R>
 cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type, bool stored = false) {
   cudaError_t ce = cudaSuccess;
   auto acc = [&](cudaError_t x) { if (ce == cudaSuccess) ce = x; };
-  const int f0 = llg_type == 2 ? kFlagBoris : llg_type == -2 ? (kFlagBoris | kFlagMid) : 0;
+  // semi-implicit (2 / -2) and analytic-rotation (1 / -1) pushes: one push
+  // over dt (then the commit), or the midpoint form (dt/2, then dt from m_n)
+  const int f0 = (llg_type == 2 || llg_type == 1)     ? kFlagBoris | (llg_type == 1 ? kFlagRot : 0)
+                 : (llg_type == -2 || llg_type == -1) ? (kFlagBoris | kFlagMid | (llg_type == -1 ? kFlagRot : 0))
+                                                      : 0;
   // grains of several cells: each stage's demag comes from an evaluation stage
   // (inverse row transforms of every cell) averaged over the grains' cells
   const int f = f0 | (e->mapped ? kFlagMapped : 0);
@@ -835,7 +839,7 @@ cudaError_t enqueue_steps(Engine* e, int k, bool stats, int llg_type, bool store
   for (int i = 0; i < k; ++i) {
     const bool last = stats && i == k - 1;
     const int lf = last ? (kFlagStats | kFlagStoreField) : 0;
-    if (llg_type == 2) {
+    if (llg_type == 2 || llg_type == 1) {
       mapped_demag(i, false);
       acc(launch_row_e<R>(e, kPred, last, i, f | lf));
       acc(launch_col_e<R>(e, i, 0));
@@ -1134,7 +1138,7 @@ int engine_step(Engine* e, int nsteps, int llg_type) {
   return run_steps<float>(e, nsteps, llg_type);
 }
 
-bool llg_type_ok(int t) { return t == -3 || t == -2 || t == 2; }
+bool llg_type_ok(int t) { return t == -3 || t == -2 || t == 2 || t == 1 || t == -1; }
 
 template <typename R>
 int engine_eval(Engine* e) {
@@ -2144,7 +2148,11 @@ int mrm_gpu_set_field_function(mrm_gpu* h, int layer, const double hdir[3], int 
                                double moddepth, double dc, double scale) {
   if (!h || !hdir) return MRM_ERR_ARG;
   if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
-  if (func < 1 || func > 5) return set_err(&h->err, MRM_ERR_ARG, "unknown time function %d", func);
+  if (func < 1 || func > 7 || func == kFuncHead) return set_err(&h->err, MRM_ERR_ARG, "unknown time function %d", func);
+  if (func == kFuncRot && std::fabs(gamma) == 1.0)
+    return set_err(&h->err, MRM_ERR_UNSUPPORTED,
+                   "ROT with |gamma| = 1 turns the field after the mean magnetisation of every step (llg.f90:332-360): "
+                   "not on this path");
   if ((func == 4 || func == 5) && !(gamma > 0 && param > 0))
     return set_err(&h->err, MRM_ERR_ARG, "STE/NEW need a period and a time constant > 0");
   LayerBufs& b = h->L[layer];
@@ -2651,7 +2659,9 @@ static int plain_prepare(mrm_gpu* h, int nsteps, double dt, int llg_type) {
   if (!(dt > 0)) return set_err(errp, MRM_ERR_ARG, "dt must be > 0");
   if (!llg_type_ok(llg_type))
     return set_err(errp, MRM_ERR_UNSUPPORTED,
-                   "llg_type %d: this path has Heun (-3) and the semi-implicit pushes (2, -2)", llg_type);
+                   "llg_type %d: this path has Heun (-3), the semi-implicit pushes (2, -2) and the "
+                   "analytic rotations (1, -1)",
+                   llg_type);
   for (int l = 0; l < h->nl; ++l)
     if (!h->L[l].uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", l);
   if (h->demag && !h->tensor_ready) return set_err(errp, MRM_ERR_STATE, "build or upload the tensor first (or disable demag)");
@@ -3117,7 +3127,7 @@ int mrm_batch_enqueue(mrm_batch* b, int nsteps, int llg_type) {
   Engine* e = &b->eng;
   std::string* errp = &e->err;
   if (!llg_type_ok(llg_type))
-    return set_err(errp, MRM_ERR_UNSUPPORTED, "llg_type %d: this path has -3, -2 and 2", llg_type);
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "llg_type %d: this path has -3, -2, 2, -1 and 1", llg_type);
   for (auto* r : e->runs) {
     if (!r->active) continue;
     for (int l = 0; l < r->nl; ++l)

@@ -385,13 +385,26 @@ static void calculate_tensor(int nx, int ny, int nl, double dx, double dy, const
 }
 
 // ---------------------------------------------------------------------------
-// FFT with FFTW's unnormalised r2c / c2r semantics (fftw.f90:37-93).
-// Radix-2 iterative for powers of two, direct DFT otherwise (test sizes only).
+// FFT with FFTW's unnormalised r2c / c2r semantics (fftw.f90:37-93), in FP64
+// or FP32 (the reference's default build links the single-precision FFTW,
+// Makefile:171-180, and its FFTD=1 build the double one).  Real rows go
+// through a complex transform of half the length (even lengths); radix-2
+// iterative passes for powers of two with per-pass twiddle tables, a direct
+// DFT for other lengths (test sizes only).  Complex products are written out
+// so that no library call checks for infinities in the inner loops.
 // ---------------------------------------------------------------------------
+template <typename T>
+static inline std::complex<T> cmul(std::complex<T> a, std::complex<T> b) {
+  return {a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real()};
+}
+
+template <typename T>
 struct FFT1 {
+  using C = std::complex<T>;
   int n = 0;
   bool pow2 = true;
-  std::vector<cd> tw;  // e^{-2 pi i k/n}
+  std::vector<C> tw;     // e^{-2 pi i k/n}, k < n
+  std::vector<C> ptw;    // pass tables: for len = 2, 4, ..., n: e^{-2 pi i k/len}, k < len/2
   std::vector<int> rev;
   void init(int n_) {
     n = n_;
@@ -399,9 +412,16 @@ struct FFT1 {
     tw.resize(n);
     for (int k = 0; k < n; ++k) {
       double a = -2.0 * M_PI * (double)k / (double)n;
-      tw[k] = cd(std::cos(a), std::sin(a));
+      tw[k] = C((T)std::cos(a), (T)std::sin(a));
     }
+    ptw.clear();
+    rev.clear();
     if (pow2) {
+      for (int len = 2; len <= n; len <<= 1)
+        for (int k = 0; k < len / 2; ++k) {
+          double a = -2.0 * M_PI * (double)k / (double)len;
+          ptw.push_back(C((T)std::cos(a), (T)std::sin(a)));
+        }
       rev.resize(n);
       int lg = 0;
       while ((1 << lg) < n) ++lg;
@@ -414,58 +434,110 @@ struct FFT1 {
     }
   }
   // in-place, sign -1 (forward) or +1 (backward), unnormalised
-  void run(cd* a, int sign, cd* scratch) const {
+  void run(C* a, int sign, C* scratch) const {
     if (pow2) {
       for (int i = 0; i < n; ++i)
         if (i < rev[i]) std::swap(a[i], a[rev[i]]);
+      const C* w0 = ptw.data();
       for (int len = 2; len <= n; len <<= 1) {
-        int half = len >> 1, step = n / len;
+        const int half = len >> 1;
         for (int i = 0; i < n; i += len)
           for (int k = 0; k < half; ++k) {
-            cd w = tw[k * step];
-            if (sign > 0) w = std::conj(w);
-            cd u = a[i + k], v = a[i + k + half] * w;
+            const C w = sign > 0 ? std::conj(w0[k]) : w0[k];
+            const C u = a[i + k], v = cmul(a[i + k + half], w);
             a[i + k] = u + v;
             a[i + k + half] = u - v;
           }
+        w0 += half;
       }
     } else {
       for (int k = 0; k < n; ++k) {
-        cd s = 0;
+        C acc = 0;
         for (int j = 0; j < n; ++j) {
-          cd w = tw[(size_t)((long long)j * k % n)];
+          C w = tw[(size_t)((long long)j * k % n)];
           if (sign > 0) w = std::conj(w);
-          s += a[j] * w;
+          acc += cmul(a[j], w);
         }
-        scratch[k] = s;
+        scratch[k] = acc;
       }
       for (int k = 0; k < n; ++k) a[k] = scratch[k];
     }
   }
 };
 
+template <typename T>
 struct FFT2 {
+  using C = std::complex<T>;
   int nx = 0, ny = 0, nh = 0;  // nh = nx/2+1
-  FFT1 fx, fy;
+  FFT1<T> fx, fh, fy;          // fh: half length (real rows of even length)
+  std::vector<C> twx;          // e^{-2 pi i k/nx}, k <= nx/2
   void init(int nx_, int ny_) {
     nx = nx_; ny = ny_; nh = nx / 2 + 1;
     fx.init(nx); fy.init(ny);
+    if (nx % 2 == 0) fh.init(nx / 2);
+    twx.resize(nh);
+    for (int k = 0; k < nh; ++k) {
+      double a = -2.0 * M_PI * (double)k / (double)nx;
+      twx[k] = C((T)std::cos(a), (T)std::sin(a));
+    }
+  }
+  // one real row -> its nh lowest bins
+  void row_r2c(const T* r, C* out, std::vector<C>& z, std::vector<C>& scr) const {
+    if (nx % 2 != 0) {
+      for (int i = 0; i < nx; ++i) z[i] = C(r[i], 0);
+      fx.run(z.data(), -1, scr.data());
+      for (int k = 0; k < nh; ++k) out[k] = z[k];
+      return;
+    }
+    const int m = nx / 2;
+    for (int k = 0; k < m; ++k) z[k] = C(r[2 * k], r[2 * k + 1]);
+    fh.run(z.data(), -1, scr.data());
+    const C mi(0, -1);
+    for (int k = 0; k < nh; ++k) {
+      const C a = z[k % m], b = std::conj(z[(m - k) % m]);
+      const C e = (a + b) * (T)0.5, o = (a - b) * (T)0.5;
+      out[k] = e + cmul(mi, cmul(twx[k], o));
+    }
+  }
+  // nh bins (Hermitian half) -> one real row, unnormalised; imaginary parts of
+  // the self-conjugate bins ignored
+  void row_c2r(const C* in, T* r, std::vector<C>& z, std::vector<C>& scr) const {
+    if (nx % 2 != 0) {
+      for (int k = 0; k < nh; ++k) z[k] = in[k];
+      for (int k = nh; k < nx; ++k) z[k] = std::conj(in[nx - k]);
+      z[0] = C(z[0].real(), 0);
+      fx.run(z.data(), +1, scr.data());
+      for (int i = 0; i < nx; ++i) r[i] = z[i].real();
+      return;
+    }
+    const int m = nx / 2;
+    const C pi(0, 1);
+    for (int k = 0; k < m; ++k) {
+      C a = in[k], b = in[m - k];
+      if (k == 0) {
+        a = C(a.real(), 0);
+        b = C(b.real(), 0);
+      }
+      const C e = a + std::conj(b), o = a - std::conj(b);
+      z[k] = e + cmul(pi, cmul(std::conj(twx[k]), o));
+    }
+    fh.run(z.data(), +1, scr.data());
+    for (int k = 0; k < m; ++k) {
+      r[2 * k] = z[k].real();
+      r[2 * k + 1] = z[k].imag();
+    }
   }
   // r[ny][nx] -> c[ny][nh]
-  void r2c(const double* r, cd* c) const {
+  void r2c(const T* r, C* c) const {
 #pragma omp parallel
     {
-      std::vector<cd> row(nx), scr(std::max(nx, ny));
+      std::vector<C> z(nx), scr(std::max(nx, ny));
 #pragma omp for
-      for (int j = 0; j < ny; ++j) {
-        for (int i = 0; i < nx; ++i) row[i] = cd(r[(size_t)j * nx + i], 0.0);
-        fx.run(row.data(), -1, scr.data());
-        for (int k = 0; k < nh; ++k) c[(size_t)j * nh + k] = row[k];
-      }
+      for (int j = 0; j < ny; ++j) row_r2c(r + (size_t)j * nx, c + (size_t)j * nh, z, scr);
     }
 #pragma omp parallel
     {
-      std::vector<cd> col(ny), scr(std::max(nx, ny));
+      std::vector<C> col(ny), scr(std::max(nx, ny));
 #pragma omp for
       for (int k = 0; k < nh; ++k) {
         for (int j = 0; j < ny; ++j) col[j] = c[(size_t)j * nh + k];
@@ -475,10 +547,10 @@ struct FFT2 {
     }
   }
   // c[ny][nh] (Hermitian half) -> r[ny][nx], unnormalised; c is destroyed
-  void c2r(cd* c, double* r) const {
+  void c2r(C* c, T* r) const {
 #pragma omp parallel
     {
-      std::vector<cd> col(ny), scr(std::max(nx, ny));
+      std::vector<C> col(ny), scr(std::max(nx, ny));
 #pragma omp for
       for (int k = 0; k < nh; ++k) {
         for (int j = 0; j < ny; ++j) col[j] = c[(size_t)j * nh + k];
@@ -488,17 +560,9 @@ struct FFT2 {
     }
 #pragma omp parallel
     {
-      std::vector<cd> row(nx), scr(std::max(nx, ny));
+      std::vector<C> z(nx), scr(std::max(nx, ny));
 #pragma omp for
-      for (int j = 0; j < ny; ++j) {
-        for (int k = 0; k < nh; ++k) row[k] = c[(size_t)j * nh + k];
-        for (int k = nh; k < nx; ++k) row[k] = std::conj(c[(size_t)j * nh + (nx - k)]);
-        // FFTW c2r ignores the imaginary parts of the self-conjugate bins
-        row[0] = cd(row[0].real(), 0.0);
-        if (nx % 2 == 0) row[nx / 2] = cd(row[nx / 2].real(), 0.0);
-        fx.run(row.data(), +1, scr.data());
-        for (int i = 0; i < nx; ++i) r[(size_t)j * nx + i] = row[i].real();
-      }
+      for (int j = 0; j < ny; ++j) row_c2r(c + (size_t)j * nh, r + (size_t)j * nx, z, scr);
     }
   }
 };
@@ -583,8 +647,15 @@ struct Sim {
   std::vector<double> dz, il_space;
   double space_to_sul = 0, sul_mu = 1, head_mu = 1, fly_height = 0;
   int px, py, ph;  // FFT grid and half width
-  FFT2 fft;
+  FFT2<double> fft;
   std::vector<cd> nhat;  // [ks][ko][9][py][ph]
+  // FP32 FFT grids (the reference's default single-precision FFTW build): the
+  // tensor spectrum from the FP64 real tensor cast to float, the M grid, its
+  // spectrum and H in float; state and fields stay FP64
+  int fft_bits = 64;
+  FFT2<float> fft32;
+  std::vector<std::complex<float>> nhat32;
+  std::vector<double> n2d_real;  // the real tensor, kept to form either spectrum
   bool demag_on = true;
   std::vector<Layer> L;
   int in = 0;          // which m buffer is current (llg.f90 `in` toggle, 0 or 1)
@@ -606,8 +677,21 @@ struct Sim {
 static void build_spectrum(Sim* s, const double* n2d_real) {
   const int nl = s->nl;
   const size_t plane = (size_t)s->px * s->py, hplane = (size_t)s->ph * s->py;
+  s->n2d_real.assign(n2d_real, n2d_real + (size_t)nl * nl * 9 * plane);
+  if (s->fft_bits == 32) {
+    // demag.f90:255-267 with ffttr = single: the tensor cast to float, then its FFT
+    std::vector<float> rf(plane);
+    s->nhat32.assign((size_t)nl * nl * 9 * hplane, std::complex<float>(0, 0));
+    for (int p = 0; p < nl * nl * 9; ++p) {
+      for (size_t q = 0; q < plane; ++q) rf[q] = (float)n2d_real[p * plane + q];
+      s->fft32.r2c(rf.data(), &s->nhat32[p * hplane]);
+    }
+    s->nhat.clear();
+    return;
+  }
   s->nhat.assign((size_t)nl * nl * 9 * hplane, cd(0, 0));
   for (int p = 0; p < nl * nl * 9; ++p) s->fft.r2c(n2d_real + p * plane, &s->nhat[p * hplane]);
+  s->nhat32.clear();
 }
 
 // grain -> cell scatter of Ms*ms_scale*m (data.f90:322-390)
@@ -632,24 +716,42 @@ static void scatter_m(Sim* s, int buf, std::vector<double>& grid) {
 }
 
 // get_demag (demag.f90:33-135) + get_magnetostatic gather (field.f90:438-470)
-static void demag_from_grid(Sim* s, std::vector<double>& grid) {
-  const int nl = s->nl;
-  const size_t plane = (size_t)s->px * s->py, hplane = (size_t)s->ph * s->py;
-  std::vector<cd> X((size_t)nl * 3 * hplane), H((size_t)nl * 3 * hplane, cd(0, 0));
-  for (int p = 0; p < nl * 3; ++p) s->fft.r2c(&grid[p * plane], &X[p * hplane]);
+template <typename T>
+static void demag_conv(const FFT2<T>& fft, const std::vector<std::complex<T>>& nhat, int nl, size_t plane,
+                       size_t hplane, T* grid) {
+  using C = std::complex<T>;
+  std::vector<C> X((size_t)nl * 3 * hplane), H((size_t)nl * 3 * hplane, C(0, 0));
+  for (int p = 0; p < nl * 3; ++p) fft.r2c(&grid[p * plane], &X[p * hplane]);
   for (int ks = 0; ks < nl; ++ks)
     for (int ko = 0; ko < nl; ++ko) {
-      const cd* N = &s->nhat[((size_t)ks * nl + ko) * 9 * hplane];
+      const C* N = &nhat[((size_t)ks * nl + ko) * 9 * hplane];
       for (int a = 0; a < 3; ++a) {
-        cd* Ha = &H[((size_t)ko * 3 + a) * hplane];
+        C* Ha = &H[((size_t)ko * 3 + a) * hplane];
         for (int b = 0; b < 3; ++b) {
-          const cd* Nab = N + (size_t)(3 * a + b) * hplane;
-          const cd* Xb = &X[((size_t)ks * 3 + b) * hplane];
-          for (size_t q = 0; q < hplane; ++q) Ha[q] += Nab[q] * Xb[q];
+          const C* Nab = N + (size_t)(3 * a + b) * hplane;
+          const C* Xb = &X[((size_t)ks * 3 + b) * hplane];
+#pragma omp parallel for
+          for (size_t q = 0; q < hplane; ++q) Ha[q] += cmul(Nab[q], Xb[q]);
         }
       }
     }
-  for (int p = 0; p < nl * 3; ++p) s->fft.c2r(&H[p * hplane], &grid[p * plane]);
+  for (int p = 0; p < nl * 3; ++p) fft.c2r(&H[p * hplane], &grid[p * plane]);
+}
+
+static void demag_from_grid(Sim* s, std::vector<double>& grid) {
+  const int nl = s->nl;
+  const size_t plane = (size_t)s->px * s->py, hplane = (size_t)s->ph * s->py;
+  if (s->fft_bits == 32) {
+    // M grid, spectra and H in float (get_mag's real(., ffttr)), back to FP64 fields
+    std::vector<float> gf(grid.size());
+#pragma omp parallel for
+    for (size_t q = 0; q < grid.size(); ++q) gf[q] = (float)grid[q];
+    demag_conv<float>(s->fft32, s->nhat32, nl, plane, hplane, gf.data());
+#pragma omp parallel for
+    for (size_t q = 0; q < grid.size(); ++q) grid[q] = (double)gf[q];
+    return;
+  }
+  demag_conv<double>(s->fft, s->nhat, nl, plane, hplane, grid.data());
 }
 
 static void gather_demag(Sim* s, const std::vector<double>& grid) {
@@ -686,6 +788,7 @@ static void compute_demag(Sim* s, int buf) {
 // funct (applied.f90:328-377); Fortran mod(x,g) = x - int(x/g)*g
 static double funct(int f, double t, double g, double phase, double param, double duty,
                     double moddepth) {
+  if (f == 7) return 1.0;  // ROT with the rotation angles present, |gamma| != 1 (applied.f90:378-383)
   if (f == 1) return std::sin(t * g + phase);
   if (f == 2) return std::cos(t * g + phase);
   if (f == 3) return std::exp(t * g + phase);
@@ -835,6 +938,12 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
     for (int n = 0; n < Ly.N; ++n) {
       if (!Ly.do_grain[n]) continue;  // field.f90:199-233 (a frozen grain keeps its last field)
       double ha[3] = {sc * Ly.hdir[0], sc * Ly.hdir[1], sc * Ly.hdir[2]};
+      if (Ly.func == 7) {  // ROT: rot_fld's direction (cos, sin((2 gamma t + phase) acos(-1)), 0)
+        const double th = (2.0 * Ly.fgamma * t + Ly.phase) * std::acos(-1.0);
+        ha[0] = sc * std::cos(th);
+        ha[1] = sc * std::sin(th);
+        ha[2] = 0.0;
+      }
       if (Ly.tab)
         for (int a = 0; a < 3; ++a) ha[a] = hat[3 * n + a];
       if (Ly.head) {
@@ -1462,8 +1571,43 @@ static void push_zhang(Sim* s, int l, int type, int iter, double dt, double dt0,
   *mmag1 = mm;
 }
 
+// rotate_q (transform.f90:65-74): m -> w ** (0, m) ** w*
+static void ref_rotate_q(const double w[4], const double m[3], double t[3]) {
+  const double w1 = w[0] * w[0], w2 = w[1] * w[1], w3 = w[2] * w[2], w4 = w[3] * w[3];
+  t[0] = 2.0 * (m[2] * (w[0] * w[2] + w[1] * w[3]) + m[1] * (w[1] * w[2] - w[0] * w[3])) + m[0] * (w1 + w2 - w3 - w4);
+  t[1] = 2.0 * (m[0] * (w[0] * w[3] + w[1] * w[2]) + m[2] * (w[2] * w[3] - w[0] * w[1])) + m[1] * (w1 + w3 - w2 - w4);
+  t[2] = 2.0 * (m[1] * (w[0] * w[1] + w[2] * w[3]) + m[0] * (w[1] * w[3] - w[0] * w[2])) + m[2] * (w1 + w4 - w3 - w2);
+}
+
+// rotate_2 (transform.f90:97-115) as push_llg calls it (norm0 present, norm1 absent)
+static void ref_rotate_2(double theta0, const double u0[3], double theta1, const double u1[3], const double m[3],
+                         double t[3]) {
+  double st1 = 0.5 * theta1, st0 = 0.5 * theta0, ct0, ct1;
+  double t0[3] = {u0[0], u0[1], u0[2]};
+  ct0 = std::sqrt(t0[0] * t0[0] + t0[1] * t0[1] + t0[2] * t0[2]);
+  if (ct0 != 0.0) {
+    for (int a = 0; a < 3; ++a) t0[a] /= ct0;
+  } else {
+    t0[0] = 0.0; t0[1] = 0.0; t0[2] = 1.0;
+    st0 = 0.0;
+  }
+  const double* t1 = u1;
+  if (st0 == 0.0 && st0 == st1) {
+    for (int a = 0; a < 3; ++a) t[a] = m[a];
+    return;
+  }
+  ct1 = std::cos(st1); st1 = std::sin(st1);
+  ct0 = std::cos(st0); st0 = std::sin(st0);
+  const double w[4] = {ct0 * ct1 - (t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2]) * st0 * st1,
+                       t0[0] * ct1 * st0 + (t1[0] * ct0 + (t1[1] * t0[2] - t0[1] * t1[2]) * st0) * st1,
+                       t0[1] * ct1 * st0 + (t1[1] * ct0 + (t1[2] * t0[0] - t0[2] * t1[0]) * st0) * st1,
+                       t0[2] * ct1 * st0 + (t1[2] * ct0 + (t1[0] * t0[1] - t0[0] * t1[1]) * st0) * st1};
+  ref_rotate_q(w, m, t);
+}
+
 // push_llg (llg.f90:1066-1155): one stage for one layer.
-// Heun (type -3) branch :1122-1139, Boris/semi-implicit (|type|=2) :1109-1118.
+// Heun (type -3) branch :1122-1139, analytic rotations (|type| = 1)
+// :1093-1107, Boris/semi-implicit (|type| = 2) :1109-1118.
 static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, double* errmx_l,
                      double* errmx1_l, double* mmag1) {
   Layer& Ly = s->L[l];
@@ -1493,16 +1637,35 @@ static void push_llg(Sim* s, int l, int type, int iter, double dt, double dt0, d
         y = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
         if (y > em * ms2) em = y / ms2;
         double scale2 = Ly.alpha_scale[n] * Ly.alpha;
-        // |type| == 2: semi-implicit (Boris) push, llg.f90:1115-1118
-        double o[3] = {scale1 * h[0] - scale2 * m[0], scale1 * h[1] - scale2 * m[1],
-                       scale1 * h[2] - scale2 * m[2]};
-        double mo[3];
-        cross(m, o, mo);
-        double tt[3] = {m[0] + mo[0], m[1] + mo[1], m[2] + mo[2]};
-        double yy = 2.0 / (1.0 + o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
-        double to[3];
-        cross(tt, o, to);
-        for (int a = 0; a < 3; ++a) d[a] = yy * to[a];
+        if (std::abs(type) != 2) {
+          // analytic rotations (llg.f90:1093-1107): precession |scale11| about
+          // h, damping turn th0 - 2 atan(exp(scale11 scale2) tan(th0/2)) about m x o
+          double yv = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+          if (yv > 0.0) {
+            yv = std::sqrt(yv);
+            const double scale11 = 2.0 * scale1 * yv / (1.0 + scale2 * scale2);
+            const double o[3] = {h[0] / yv, h[1] / yv, h[2] / yv};
+            const double th0 = std::acos(std::min(1.0, std::max(-1.0, o[0] * m[0] + o[1] * m[1] + o[2] * m[2])));
+            double mo[3], r[3];
+            cross(m, o, mo);
+            ref_rotate_2(th0 - 2.0 * std::atan(std::exp(scale11 * scale2) * std::tan(0.5 * th0)), mo,
+                         std::abs(scale11), o, m, r);
+            for (int a = 0; a < 3; ++a) d[a] = r[a] - m[a];
+          } else {
+            d[0] = d[1] = d[2] = 0.0;
+          }
+        } else {
+          // |type| == 2: semi-implicit (Boris) push, llg.f90:1115-1118
+          double o[3] = {scale1 * h[0] - scale2 * m[0], scale1 * h[1] - scale2 * m[1],
+                         scale1 * h[2] - scale2 * m[2]};
+          double mo[3];
+          cross(m, o, mo);
+          double tt[3] = {m[0] + mo[0], m[1] + mo[1], m[2] + mo[2]};
+          double yy = 2.0 / (1.0 + o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+          double to[3];
+          cross(tt, o, to);
+          for (int a = 0; a < 3; ++a) d[a] = yy * to[a];
+        }
         em1 = std::max(em1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         for (int a = 0; a < 3; ++a) mnext[a] = m[a] + d[a];
       } else {
@@ -1822,12 +1985,12 @@ void orc_calculate_tensor(int nx, int ny, int nl, double dx, double dy, const do
 
 // ---- FFT probes (row-major [ny][nx] real, [ny][nx/2+1] complex interleaved) ----
 void orc_fft_r2c(int nx, int ny, const double* r, double* c) {
-  FFT2 f;
+  FFT2<double> f;
   f.init(nx, ny);
   f.r2c(r, reinterpret_cast<cd*>(c));
 }
 void orc_fft_c2r(int nx, int ny, const double* c_in, double* r) {
-  FFT2 f;
+  FFT2<double> f;
   f.init(nx, ny);
   std::vector<cd> c(reinterpret_cast<const cd*>(c_in),
                     reinterpret_cast<const cd*>(c_in) + (size_t)ny * (nx / 2 + 1));
@@ -1883,12 +2046,27 @@ void* orc_create(int nx, int ny, int nl, int boundary, int images, double dx, do
   s->py = boundary == 1 ? 2 * ny : ny;
   s->ph = s->px / 2 + 1;
   s->fft.init(s->px, s->py);
+  s->fft32.init(s->px, s->py);
   s->demag_on = demag_on != 0;
   s->L.resize(nl);
   return s;
 }
 
 void orc_destroy(void* h) { delete static_cast<Sim*>(h); }
+
+// FFT precision of the demag convolution: 64 (the FFTD=1 build) or 32 (the
+// default single-precision FFTW build); the spectrum is re-formed from the
+// real tensor if one is set
+int orc_set_fft_precision(void* h, int bits) {
+  Sim* s = static_cast<Sim*>(h);
+  if (bits != 32 && bits != 64) return 1;
+  s->fft_bits = bits;
+  if (!s->n2d_real.empty()) {
+    const std::vector<double> t = s->n2d_real;
+    build_spectrum(s, t.data());
+  }
+  return 0;
+}
 
 // {window nx, ny, origin i0, j0} (the whole grid and 0, 0 without a window)
 void orc_get_window(void* h, int* out4) {
@@ -1914,7 +2092,10 @@ int orc_set_window(void* h, int nxw, int nyw, double vx, double vy, double ox, d
   s->py = s->boundary == 1 ? 2 * fy : fy;
   s->ph = s->px / 2 + 1;
   s->fft.init(s->px, s->py);
+  s->fft32.init(s->px, s->py);
   s->nhat.clear();
+  s->nhat32.clear();
+  s->n2d_real.clear();
   return 0;
 }
 
@@ -2245,7 +2426,9 @@ void orc_eval_field(void* h, double t) {
 // traj: optional [nsteps][nl][3] vol-weighted <m> after each step.
 int orc_step(void* h, int nsteps, double dt, int type, double* stats_out, double* traj) {
   Sim* s = static_cast<Sim*>(h);
-  if (!(type == -3 || type == 2 || type == -2)) return 2;
+  if (!(type == -3 || type == 2 || type == -2 || type == 1 || type == -1)) return 2;
+  for (const Layer& Ly : s->L)
+    if (Ly.llb && std::abs(type) == 1) return 2;  // push_llb has no analytic rotation here
   update_do_grain(s, s->t);  // llg.f90:138
   for (int k = 0; k < nsteps; ++k) {
     heun_or_boris_step(s, dt, type);
@@ -2262,7 +2445,7 @@ int orc_step(void* h, int nsteps, double dt, int type, double* stats_out, double
 int orc_step_adaptive(void* h, int nsteps, int type, double dt_frac, double dt_max, const double* max_dm, double* dt,
                       double* max_dmdt, double* stats_out) {
   Sim* s = static_cast<Sim*>(h);
-  if (!(type == -3 || type == 2 || type == -2)) return 2;
+  if (!(type == -3 || type == 2 || type == -2 || type == 1 || type == -1)) return 2;
   if (s->wnx) return 3;  // fixed dt only with a moving window
   for (int k = 0; k < nsteps; ++k) adaptive_step(s, type, dt_frac, dt_max, max_dm, dt, max_dmdt);
   if (stats_out) std::memcpy(stats_out, &s->last, sizeof(Stats));
@@ -2290,7 +2473,7 @@ int orc_off_field(void* h, double zoff, double dzobs, double head_mu, double fly
     if (k != nl - 1) zob += s->il_space[k];
   }
   const double zot = zob + dzobs;
-  FFT2 f;
+  FFT2<double> f;
   f.init(nx, ny);
   std::vector<double> nn(9 * plane), t(9 * plane), grid(3 * plane);
   std::vector<cd> T(9 * hplane), X(3 * hplane), H(3 * hplane, cd(0, 0));

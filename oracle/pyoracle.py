@@ -87,6 +87,7 @@ def lib():
         L.orc_fft_c2r.argtypes = [i, i, P(d), P(d)]
         L.orc_demag_direct.argtypes = [i, i, i, P(d), P(d), i, P(i), i, P(d)]
         L.orc_set_threads.argtypes = [i]
+        L.orc_set_fft_precision.argtypes = [vp, i]
         L.orc_get_threads.restype = i
         L.orc_stats_size.restype = i
         assert L.orc_stats_size() == STATS_DTYPE.itemsize, "Stats layout mismatch"
@@ -222,7 +223,7 @@ class OracleSim:
     """CPU restatement driven like the GPU handle (mrm_b200.GpuSim)."""
 
     def __init__(self, medium, demag: bool = True, rng_mode: int = 1, seed: int = 1,
-                 tensor: np.ndarray | None = None):
+                 tensor: np.ndarray | None = None, fft_bits: int = 64):
         L = lib()
         self.medium = medium
         dz = f64(medium.dz)
@@ -231,6 +232,7 @@ class OracleSim:
                               medium.dx, medium.dy, _p(dz), _p(il), medium.space_to_sul,
                               medium.sul_mu, medium.head_mu, medium.fly_height, 1 if demag else 0)
         self._keep = []
+        assert L.orc_set_fft_precision(self.h, int(fft_bits)) == 0
         for l, lay in enumerate(medium.layers):
             arrs = [f64(lay.ms), f64(lay.vol), f64(lay.axis), f64(lay.hk), f64(lay.hk_scale),
                     f64(lay.ms_scale), f64(lay.alpha_scale)]
