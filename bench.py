@@ -375,6 +375,46 @@ def batched_leg(args, torch, local, rank, dist):
             "occupancy": occ, "shape": shape, "samples": len(hs)}
 
 
+GOLDEN_C2 = os.path.join(ROOT, "tests", "golden", "c2_mh.npz")
+
+
+def physics_leg(local):
+    """The Hc/Mr gate on the headline medium: the FP32 batched path over the
+    full 20,000-step ramp, one realisation per seed of the committed oracle
+    ensemble (tests/golden/c2_mh.npz, FP64 oracle, same medium and ramp), and
+    the relative error of the ensemble means of coercivity and remanence."""
+    from mrm_b200 import FP32
+    from mrm_b200.batch import Batch
+    if not os.path.exists(GOLDEN_C2):
+        return {"oracle_ensemble": "absent"}
+    g = np.load(GOLDEN_C2)
+    seeds = [int(x) for x in g["seeds"]]
+    b = Batch(FP32, local)
+    runs = []
+    for sd in seeds:
+        runs.append(b.add(make_medium(seed=1), dt=DT, thermal_seed=sd, tensor_from=runs[0] if runs else None))
+    hdir = np.array(make_medium(seed=1).layers[0].hdir)
+    hs, mhs = [], []
+    for _ in range(RAMP_STEPS // HEUN_PER_STEP):
+        b.step(HEUN_PER_STEP)
+        st = b.stats(runs)
+        hs.append(applied(float(st[0]["t"])))
+        mhs.append([float(x["mms_l"][0] @ hdir) for x in st])
+    b.close()
+    mh = np.array(mhs)
+    hm = [coercivity(hs, mh[:, i]) for i in range(len(seeds))]
+    hc = np.array([x[0] for x in hm], float)
+    mr = np.array([x[1] for x in hm], float)
+    return {"workload": f"{len(seeds)} realisations of the 65,536-grain medium (seeds {seeds}), full 2 ns ramp, "
+                        "FP32 batched path",
+            "hc_mean_oe": float(hc.mean()), "mr_mean": float(mr.mean()),
+            "oracle_hc_mean_oe": float(g["hc"].mean()), "oracle_mr_mean": float(g["mr"].mean()),
+            "hc_rel_err_vs_oracle_ensemble": float(hc.mean() / g["hc"].mean() - 1.0),
+            "mr_rel_err_vs_oracle_ensemble": float(mr.mean() / g["mr"].mean() - 1.0),
+            "oracle_hc_seed_spread_oe": float(np.std(g["hc"])),
+            "gate": "|rel err| <= 1 % for Hc and Mr"}
+
+
 def plain_leg(torch, local, precision, heun_chunk=100, total=RAMP_STEPS, flush_l2=True):
     """One plain single run of the 65,536-grain medium over the full ramp."""
     from mrm_b200 import GpuSim
@@ -680,6 +720,7 @@ def main():
         line["physics"].update({"hc_fp32_oe": p32["hc_oe"], "hc_fp64_oe": p64["hc_oe"], "hc_rel_err_fp32_vs_fp64": hc_err,
                                 "mr_fp32": p32["mr"], "mr_fp64": p64["mr"],
                                 "fp64_us_per_heun_step": p64["us_per_heun_step"]})
+        line["physics"]["vs_oracle"] = physics_leg(local)
         line["mix"] = mix_leg(torch, local)
         line["write"] = write_leg(torch, local)
         line["llb"] = llb_leg(torch, local)

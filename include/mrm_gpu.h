@@ -386,6 +386,13 @@ int mrm_batch_add(mrm_batch* b, const mrm_geom* geom, mrm_gpu** run);
 int mrm_batch_remove(mrm_batch* b, mrm_gpu* run);
 /* per-run time step and step budget: the run advances while step < step_end */
 int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active);
+/* Aligned start (no reference counterpart): the run idles through the first
+ * idle_steps steps of its next mrm_batch_step / _enqueue call, then steps on
+ * from where it is (state, time and thermal counters as without the delay),
+ * so that a budget of S steps ends on a call boundary of fixed length K when
+ * idle_steps = K - S mod K.  step_end stays where it is: the run executes
+ * the same steps, idle_steps later.  Once per run, before it starts stepping. */
+int mrm_batch_delay_run(mrm_gpu* run, int64_t idle_steps);
 /* Advances every active run by up to nsteps steps of llg_type (-3, 2 or -2). */
 int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type);
 /* Stats of each listed run at its last executed step that ended an

@@ -32,6 +32,11 @@ class BatchRun(_RunMixin):
         self.dt = dt
         self.step_end = step_end
 
+    def delay(self, idle_steps: int):
+        """Aligned start: the run idles through the first `idle_steps` steps of
+        the batch's next call, then executes its budget unchanged."""
+        self._check(_lib.load().mrm_batch_delay_run(self.h, int(idle_steps)))
+
 
 class Batch:
     def __init__(self, precision: int = _lib.FP32, device: int = 0):

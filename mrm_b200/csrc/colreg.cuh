@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) creg_kernel(const RunDev<float>* 
     const Task tk = tasks[i];
     const RunDev<float>& rd = runs[tk.x];
     if (!rd.active || !rd.demag) return false;
-    return (flags & kFlagForce) || rd.step + istep < rd.step_end;
+    return (flags & kFlagForce) || step_due(rd, rd.step + istep);
   };
   // thread 0: the tile of task i into the staging area (nothing for a task
   // without work), completing phase `ph` of bars[1]

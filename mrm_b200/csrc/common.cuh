@@ -150,6 +150,7 @@ struct RunDev {
   long long step_base;
   long long step;          // current step index (advanced by the advance kernel)
   long long step_end;      // the run advances while step < step_end
+  long long step_begin;    // and idles while step < step_begin (an aligned start inside a call)
   unsigned long long seed;
   int active;
   int stats_ok;            // set by the advance kernel: the chunk's last step was executed
@@ -177,6 +178,13 @@ constexpr int kFuncRot = 7;  // the ROT time function: an in-plane field rotatin
 // imaginary for xz, yz, zx, zy and odd in ky for xy, yx, yz, zy.
 constexpr int kImagMask = (1 << 2) | (1 << 5) | (1 << 6) | (1 << 7);
 constexpr int kOddMask = (1 << 1) | (1 << 3) | (1 << 5) | (1 << 7);
+
+// Whether a run executes step `step` of a call: inside its budget and past its
+// aligned start.
+template <typename R>
+MRM_HD bool step_due(const RunDev<R>& rd, long long step) {
+  return step >= rd.step_begin && step < rd.step_end;
+}
 
 // row task: (run, layer, first row, number of rows); column task: (run, first column, ncols, 0)
 using Task = int4;

@@ -943,7 +943,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // ---------------- wait for the previous kernel's results ----------------
   pdl_wait();
   const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
-  const bool run_it = (flags & kFlagForce) || step < rd.step_end;
+  const bool run_it = (flags & kFlagForce) || step_due(rd, step);
   if (threadIdx.x == 0) {
     if (run_it && inverse)
       for (int s = 0; s < nseq; ++s) {
@@ -1702,7 +1702,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) col_kernel(const RunDev<R>* __res
     mbar_arrive(&bars[0]);
   }
   pdl_wait();
-  const bool run_it = (flags & kFlagForce) || rd.step + istep < rd.step_end;
+  const bool run_it = (flags & kFlagForce) || step_due(rd, rd.step + istep);
   const bool ok = mbar_wait(&bars[0], 0);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) atomicOr(err, kErrBarrierTimeout);
@@ -1848,7 +1848,7 @@ __global__ void __launch_bounds__(256) commit_kernel(const RunDev<R>* __restrict
   if (!rd.active) return;
   pdl_wait();
   const long long step = *reinterpret_cast<const volatile long long*>(&rd.step) + istep;
-  if (!(flags & kFlagForce) && step >= rd.step_end) return;
+  if (!(flags & kFlagForce) && !step_due(rd, step)) return;
   const LayerDev<R>& L = rd.L[tk.y];
   // (a windowed run's task row is grid row wj0 + row from column wi0)
   const int n0 = rd.gnx ? (rd.wj0 + tk.z) * rd.gnx + rd.wi0 : tk.z * rd.nx, cnt = tk.w * rd.nx;

@@ -106,6 +106,7 @@ struct mrm_gpu {
   double tensor_resid = 0.0, tensor_kept = 0.0;
   double dt = 1e-13, t_base = 0.0;
   long long step_base = 0, step = 0, step_end = 0;
+  long long step_begin = -(long long)9e18;  // idles while step < step_begin (mrm_batch_delay_run)
   unsigned long long seed = 1;
   bool active = true;
   bool spec_valid = false;
@@ -480,6 +481,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
   d.step_base = r->step_base;
   d.step = r->step;
   d.step_end = r->step_end;
+  d.step_begin = r->step_begin;
   d.seed = r->seed;
   d.active = r->active ? 1 : 0;
   d.row_task0 = r->row_task0;
@@ -3112,12 +3114,27 @@ int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active) {
   if (!run) return MRM_ERR_ARG;
   if (!(dt > 0)) return set_err(&run->err, MRM_ERR_ARG, "dt must be > 0");
   if (dt != run->dt) {
-    run->t_base = run->t_base + (double)(run->step - run->step_base) * run->dt;
-    run->step_base = run->step;
+    // rebase the time at the run's next executed step (a delayed run's step
+    // counter sits below it)
+    const long long at = std::max(run->step, run->step_begin);
+    run->t_base = run->t_base + (double)(at - run->step_base) * run->dt;
+    run->step_base = at;
     run->dt = dt;
   }
   run->step_end = step_end;
   run->active = active != 0;
+  run->eng->desc_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_batch_delay_run(mrm_gpu* run, int64_t idle_steps) {
+  if (!run) return MRM_ERR_ARG;
+  if (idle_steps < 0) return set_err(&run->err, MRM_ERR_ARG, "idle_steps must be >= 0");
+  if (run->step < run->step_begin) return set_err(&run->err, MRM_ERR_ARG, "the run is already delayed");
+  // the step counter moves back by idle_steps and the run idles until it is
+  // back at its current step: state, time and thermal counters are unchanged
+  run->step_begin = run->step;
+  run->step -= idle_steps;
   run->eng->desc_dirty = true;
   return MRM_OK;
 }

@@ -8,9 +8,12 @@ start).  The server keeps one Batch resident on the GPU and loops:
    footprint (state, parameters, spectra, tensor) fits the HBM budget; a
    request's tensor spectrum is copied device-to-device from a per-geometry
    template instead of being rebuilt;
-3. advance every active run by K Heun steps in one launch sequence, with
-   K = min(chunk, the smallest remaining budget), so that budgets end on
-   call boundaries and each run's reductions describe its own last step;
+3. advance every active run by K = chunk Heun steps in one launch sequence.
+   A request of S steps is admitted with an aligned start: it idles through
+   the first K - S mod K steps of its first call (mrm_batch_delay_run), so
+   its budget ends on a call boundary and its reductions at the end of
+   every call describe its own last step, while every call keeps the full
+   chunk length (a run's trajectory is the same as without the delay);
 4. record each run's M(H) sample (time, applied field, m.h), retire finished
    runs (result + latency = finish - arrival) and free their memory.
 
@@ -41,13 +44,17 @@ from .workloads import DT, Request
 class _Active:
     __slots__ = ("req", "run", "fp", "admitted", "remaining", "samples")
 
-    def __init__(self, req, run, fp, admitted):
+    def __init__(self, req, run, fp, admitted, idle):
         self.req = req
         self.run = run
         self.fp = fp
         self.admitted = admitted
-        self.remaining = req.steps
+        self.remaining = req.steps + idle  # steps of the calls left, idle prefix included
         self.samples = []
+
+    @property
+    def steps_done(self) -> int:
+        return max(0, self.req.steps - self.remaining)
 
 
 def applied_field(req: Request, t: float) -> float:
@@ -73,8 +80,9 @@ class Server:
     """Continuous-batching scheduler over a Batch-like backend.
 
     backend: object with add(medium, dt, steps, thermal_seed, tensor_from) ->
-    run, remove(run), step(k), stats(runs), footprint(medium) -> bytes,
-    memory() -> (free, total); defaults to the GPU Batch.
+    run, delay(run, idle_steps), remove(run), step(k), stats(runs),
+    footprint(medium) -> bytes, memory() -> (free, total); defaults to the
+    GPU Batch.
     """
 
     def __init__(self, backend=None, precision: int = _lib.FP32, device: int = 0,
@@ -114,7 +122,10 @@ class Server:
         run = self.be.add(med, DT, req.steps, req.seed, tmpl)
         if tmpl is None:
             self.templates[key] = self.be.make_template(run)
-        return _Active(req, run, fp, now)
+        idle = (-req.steps) % self.chunk
+        if idle:
+            self.be.delay(run, idle)
+        return _Active(req, run, fp, now, idle)
 
     def _retire(self, a: Optional[_Active], req: Request, status: str, now: float, s=None) -> dict:
         """Result record of a request that leaves the server (a: its run, or
@@ -123,7 +134,7 @@ class Server:
         res = {"rid": req.rid, "kind": req.kind, "grains": req.grains, "steps": req.steps,
                "arrival": req.arrival, "admitted": a.admitted if a is not None else None,
                "finished": now, "latency": now - req.arrival, "status": status,
-               "steps_done": req.steps - (a.remaining if a is not None else req.steps),
+               "steps_done": a.steps_done if a is not None else 0,
                "samples": len(samples)}
         if s is not None:
             res["final_mave"] = np.asarray(s["mave"]).tolist()
@@ -177,8 +188,9 @@ class Server:
                 if pending:
                     self.sleep(max(0.0, min(pending[0].arrival - (self.clock() - t0), 0.01)))
                 continue
-            # one launch sequence for every active run; budgets end on call boundaries
-            k = min(self.chunk, min(a.remaining for a in active))
+            # one launch sequence of the full chunk for every active run; every
+            # budget ends on a call boundary (aligned starts)
+            k = self.chunk
             self.be.step(k)
             calls += 1
             st = self.be.stats([a.run for a in active])
@@ -229,6 +241,9 @@ class GpuBackend:
         run = self.batch.add(medium, dt=dt, steps=steps, thermal_seed=seed, tensor_from=template)
         run._hdir = np.array(medium.layers[0].hdir, float)
         return run
+
+    def delay(self, run, idle_steps):
+        run.delay(idle_steps)
 
     def make_template(self, run):
         t = self.lib_batch.add(run.medium, dt=DT, steps=0, demag=True, tensor_from=run)

@@ -57,6 +57,32 @@ def test_batch_step_budgets(gpulib):
     b.close()
 
 
+def test_batch_aligned_start(gpulib):
+    """A run delayed by K - S mod K idles through the head of its first call
+    and ends its S-step budget on the call boundary: state, time and the
+    call's reductions equal the run stepped alone; an undelayed neighbour is
+    unaffected."""
+    meds = _media()[:2]
+    b = Batch(FP64)
+    r0 = b.add(meds[0], dt=1e-13, steps=70, thermal_seed=9)
+    r1 = b.add(meds[1], dt=1e-13, steps=200, thermal_seed=9)
+    r0.delay(30)
+    b.step(100)
+    st = b.stats([r0, r1])
+    assert st[0]["step"] == 70 and st[1]["step"] == 100
+    b.step(100)
+    st2 = b.stats([r0, r1])
+    assert st2[0]["step"] == 70 and np.array_equal(st2[0]["mave"], st[0]["mave"])
+    for r, m, k, s in ((r0, meds[0], 70, st[0]), (r1, meds[1], 200, st2[1])):
+        g = GpuSim(m, precision=FP64, thermal_seed=9)
+        sg = g.step(k, 1e-13)
+        assert np.array_equal(r.get_state(0), g.get_state(0))
+        assert r.get_time()[1] == k
+        assert s["t"] == sg["t"] and np.array_equal(s["mave"], sg["mave"])
+        g.close()
+    b.close()
+
+
 def test_tensor_copy_matches_build(gpulib):
     m = media.mh_medium(32, seed=4)
     b = Batch(FP32)

@@ -11,6 +11,7 @@ class FakeRun:
         self.medium = medium
         self.budget = steps
         self.done = 0
+        self.idle = 0
 
 
 class FakeBackend:
@@ -38,6 +39,10 @@ class FakeBackend:
     def make_template(self, run):
         return object()
 
+    def delay(self, run, idle):
+        assert run.done == 0 and run.idle == 0 and 0 < idle
+        run.idle = idle
+
     def hdir(self, run):
         return np.array([0.0, 0.0, 1.0])
 
@@ -46,11 +51,13 @@ class FakeBackend:
         self.used -= self.footprint(run.medium)
 
     def step(self, k):
-        rem = [r.budget - r.done for r in self.runs]
-        assert k <= min(rem), "a call must not run past a budget"
+        # every budget ends on a call boundary: no run stops inside a call
+        for r in self.runs:
+            assert r.idle + (r.budget - r.done) >= k, "a call must not run past a budget"
         self.calls.append((k, len(self.runs)))
         for r in self.runs:
-            r.done += k
+            r.done += k - r.idle
+            r.idle = 0
         self.t += 1e-4 * k
 
     def stats(self, runs):
@@ -163,7 +170,27 @@ def test_cancellation_from_another_thread():
     be.step = step_and_cancel
     out = srv.run(reqs)
     res = {r["rid"]: r for r in out["results"]}
+    # 3000 steps are a multiple of the chunk: no idle prefix, three calls done
     assert res[0]["status"] == "cancelled" and res[0]["steps_done"] == 300
     assert res[2]["status"] == "cancelled" and res[2]["steps_done"] == 0 and res[2]["admitted"] is None
     assert res[1]["status"] == "done" and res[1]["step"] == 900
     assert out["cancelled"] == 2 and not be.runs
+
+
+def test_every_call_has_the_full_chunk():
+    """Aligned starts: budgets that are not multiples of the chunk idle through
+    the head of their first call, so every call runs the full chunk and each
+    request still executes exactly its own step count."""
+    reqs = [Request(0, 0.0, "mh", 32, 300.0, 1000, 1), Request(1, 0.0, "mh", 32, 300.0, 130, 2),
+            Request(2, 0.0, "write", 32, 300.0, 777, 3), Request(3, 0.0, "mh", 32, 300.0, 256, 4)]
+    be = FakeBackend(budget_bytes=10**12)
+    srv = Server(backend=be, chunk=128, clock=be.clock, sleep=be.sleep)
+    out = srv.run(reqs)
+    assert {k for k, _ in be.calls} == {128}
+    assert len(be.calls) == -(-1000 // 128)
+    res = {r["rid"]: r for r in out["results"]}
+    for q in reqs:
+        assert res[q.rid]["status"] == "done" and res[q.rid]["step"] == q.steps
+        assert res[q.rid]["steps_done"] == q.steps
+    # a request finishes after as many calls as its steps need
+    assert res[1]["finished"] < res[2]["finished"] < res[0]["finished"]
