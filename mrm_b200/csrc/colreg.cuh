@@ -29,165 +29,24 @@ namespace mrm {
 
 constexpr int kCregMinLg = 8, kCregMaxLg = 10;
 
-// Exchange-buffer swizzle in 8-byte elements: bits 0..3 xored with bits 3..6.
-// It is linear over xor, and for every stage's access pattern of a half warp
-// (16 consecutive threads, one register slot) it puts the 16 elements on
-// distinct bank pairs for N = 256 .. 2048 (checked by enumeration).
-MRM_HD constexpr int xswz(int p) { return p ^ ((p >> 3) & 15); }
-
-// Stage plan of an N = 2^LGN point column: S stages; stage 0 has radix
-// 2^R0 over the top R0 position bits, the others radix 8.  In stage s a
-// thread's eight elements differ in the three position bits from dbit(s)
-// (its register digit); the other bits are the thread index.
-template <int LGN>
-struct CregPlan {
-  static constexpr int N = 1 << LGN, NT = N / 8, S = (LGN + 2) / 3, R0 = LGN - 3 * (S - 1);
-  MRM_HD static constexpr int dbit(int s) { return s == 0 ? LGN - 3 : LGN - R0 - 3 * s; }
-  // log2 of the butterfly stride of stage s (the LGNS of its pass table)
-  MRM_HD static constexpr int lgd(int s) { return s == 0 ? LGN - R0 : dbit(s); }
-};
-
-// position of a thread's element 0 in a stage whose register digit starts at bit B
-template <int B>
-MRM_D int creg_base(int t) {
-  return (t & ((1 << B) - 1)) | ((t >> B) << (B + 3));
-}
-
-// forward radix-8 DFT of four inputs (inputs 4..7 are zero)
-MRM_D void dft8_half_in(Cx<float>* v) {
-  const float h = 0.70710678118654752440f;
-  Cx<float> e0 = v[0], e1 = v[1], e2 = v[2], e3 = v[3];
-  Cx<float> o0 = e0, o1 = cmul(e1, Cx<float>{h, -h}), o2 = cmul_i(e2, -1.f), o3 = cmul(e3, Cx<float>{-h, -h});
-  dft4<float, -1>(e0, e1, e2, e3);
-  dft4<float, -1>(o0, o1, o2, o3);
-  v[0] = e0;
-  v[2] = e1;
-  v[4] = e2;
-  v[6] = e3;
-  v[1] = o0;
-  v[3] = o1;
-  v[5] = o2;
-  v[7] = o3;
-}
-
-// The twiddles of a thread's butterflies in stage STAGE (shared by the three
-// components): w[jl * R + m] = e^{-2 pi i j0 m / L} for the radix-R
-// butterfly jl of the thread (one for radix 8; 8/R for a stage 0 of radix 2
-// or 4), m >= 1; none when the stage's stride is 1.
-template <int LGN, int STAGE>
-MRM_D void creg_twiddles(Cx<float> (&w)[8], int t, const Cx<float>* __restrict__ tw) {
-  using P = CregPlan<LGN>;
-  constexpr int LGD = P::lgd(STAGE), D = 1 << LGD, OFF = pass_tw_off(LGN, LGD);
-  constexpr int R = STAGE == 0 ? (1 << P::R0) : 8, NB = 8 / R;
-  if constexpr (D > 1) {
-#pragma unroll
-    for (int jl = 0; jl < NB; ++jl) {
-      const int j0 = STAGE == 0 ? t + (jl << (LGN - 3)) : (t & (D - 1));
-#pragma unroll
-      for (int m = 1; m < R; ++m) w[jl * R + m] = tw[OFF + (m - 1) * D + j0];
-    }
-  }
-}
-
-// Forward stage STAGE (decimation in frequency: butterfly, then twiddles) on
-// one component's eight elements; element k of the register digit is v[k].
-// HALF: positions >= N/2 are zero on input (stage 0).
-template <int LGN, int STAGE, bool HALF>
-MRM_D void creg_fwd(Cx<float> (&v)[8], const Cx<float> (&w)[8]) {
-  using P = CregPlan<LGN>;
-  constexpr int D = 1 << P::lgd(STAGE);
-  if constexpr (STAGE == 0 && P::R0 < 3) {
-    constexpr int R = 1 << P::R0, NB = 8 / R;
-#pragma unroll
-    for (int jl = 0; jl < NB; ++jl) {
-      Cx<float> u[R];
-#pragma unroll
-      for (int m = 0; m < R; ++m) u[m] = v[jl + NB * m];
-      if constexpr (HALF) {
-        if constexpr (R == 4) {
-          const Cx<float> a0 = u[0], a1 = u[1];
-          u[0] = cadd(a0, a1);
-          u[1] = cadd(a0, cmul_i(a1, -1.f));
-          u[2] = csub(a0, a1);
-          u[3] = cadd(a0, cmul_i(a1, 1.f));
-        } else {
-          u[1] = u[0];
-        }
-      } else {
-        if constexpr (R == 4) dft4<float, -1>(u[0], u[1], u[2], u[3]);
-        else dft2<float, -1>(u);
-      }
-#pragma unroll
-      for (int m = 1; m < R; ++m) u[m] = cmul(u[m], w[jl * R + m]);
-#pragma unroll
-      for (int m = 0; m < R; ++m) v[jl + NB * m] = u[m];
-    }
-  } else {
-    if constexpr (STAGE == 0 && HALF) dft8_half_in(v);
-    else dft8<float, -1>(v);
-    if constexpr (D > 1) {
-#pragma unroll
-      for (int m = 1; m < 8; ++m) v[m] = cmul(v[m], w[m]);
-    }
-  }
-}
-
-// Inverse stage STAGE (decimation in time: conjugate twiddles, then the
-// butterfly with the + sign), unnormalised, on one component.
-template <int LGN, int STAGE>
-MRM_D void creg_inv(Cx<float> (&v)[8], const Cx<float> (&w)[8]) {
-  using P = CregPlan<LGN>;
-  constexpr int D = 1 << P::lgd(STAGE);
-  if constexpr (STAGE == 0 && P::R0 < 3) {
-    constexpr int R = 1 << P::R0, NB = 8 / R;
-#pragma unroll
-    for (int jl = 0; jl < NB; ++jl) {
-      Cx<float> u[R];
-      u[0] = v[jl];
-#pragma unroll
-      for (int m = 1; m < R; ++m) u[m] = cmul(v[jl + NB * m], cconj(w[jl * R + m]));
-      if constexpr (R == 4) dft4<float, 1>(u[0], u[1], u[2], u[3]);
-      else dft2<float, 1>(u);
-#pragma unroll
-      for (int m = 0; m < R; ++m) v[jl + NB * m] = u[m];
-    }
-  } else {
-    if constexpr (D > 1) {
-#pragma unroll
-      for (int m = 1; m < 8; ++m) v[m] = cmul(v[m], cconj(w[m]));
-    }
-    dft8<float, 1>(v);
-  }
-}
-
-// barrier of one column's NT threads: the warp itself, or named barrier 1 + c
-template <int NT>
-MRM_D void creg_sync(int c) {
-  if constexpr (NT <= 32) {
-    __syncwarp();
-  } else {
-    asm volatile("bar.sync %0, %1;" ::"r"(c + 1), "n"(NT) : "memory");
-  }
-}
-
 // A stage over the three components in the column's buffer: each component's
 // eight elements at the thread's positions of the stage are read, transformed
 // and written back in place (no other thread touches them in this stage).
 template <int LGN, int STAGE, bool INV>
 MRM_D void creg_stage(Cx<float>* __restrict__ buf, int t, const Cx<float>* __restrict__ tw) {
-  using P = CregPlan<LGN>;
+  using P = RegPlan<LGN>;
   constexpr int B = P::dbit(STAGE);
   Cx<float> w[8];
-  creg_twiddles<LGN, STAGE>(w, t, tw);
-  const int a = xswz(creg_base<B>(t));
+  reg_twiddles<LGN, STAGE>(w, t, tw);
+  const int a = xswz(reg_base<B>(t));
 #pragma unroll 1
   for (int q = 0; q < 3; ++q) {
     Cx<float>* b = buf + q * P::N;
     Cx<float> v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = b[a ^ xswz(k << B)];
-    if constexpr (INV) creg_inv<LGN, STAGE>(v, w);
-    else creg_fwd<LGN, STAGE, false>(v, w);
+    if constexpr (INV) reg_inv<LGN, STAGE>(v, w);
+    else reg_fwd<LGN, STAGE, false>(v, w);
 #pragma unroll
     for (int k = 0; k < 8; ++k) b[a ^ xswz(k << B)] = v[k];
   }
@@ -250,7 +109,7 @@ MRM_HD constexpr int creg_smem(int tw_cap, int block, int stage_bytes) {
 template <int LGN, bool HALF, class AFTER>
 MRM_D void creg_body(const RunDev<float>& rd, int k, int t, int c, bool live, const Cx<float>* __restrict__ tw,
                      const Cx<float>* __restrict__ stg, Cx<float>* __restrict__ buf, const AFTER& staged_read) {
-  using P = CregPlan<LGN>;
+  using P = RegPlan<LGN>;
   constexpr int N = P::N, NT = P::NT, KIN = HALF ? 4 : 8;
   constexpr int B0 = P::dbit(0);
   const int ny = rd.ny, lgct = rd.lgct, cs = k & ((1 << lgct) - 1);
@@ -270,25 +129,25 @@ MRM_D void creg_body(const RunDev<float>& rd, int k, int t, int c, bool live, co
   staged_read();
   {
     Cx<float> w[8];
-    creg_twiddles<LGN, 0>(w, t, tw);
-    const int a = xswz(creg_base<B0>(t));
+    reg_twiddles<LGN, 0>(w, t, tw);
+    const int a = xswz(reg_base<B0>(t));
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       Cx<float> v[8];
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk) v[kk] = kk < KIN ? v0[q][kk] : Cx<float>{0.f, 0.f};
-      creg_fwd<LGN, 0, HALF>(v, w);
+      reg_fwd<LGN, 0, HALF>(v, w);
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk) buf[q * N + (a ^ xswz(kk << B0))] = v[kk];
     }
   }
   // the tensor slice: its loads land during the remaining forward stages
-  creg_sync<NT>(c);
+  reg_sync<NT>(c);
   creg_stage<LGN, 1, false>(buf, t, tw);
-  creg_sync<NT>(c);
+  reg_sync<NT>(c);
   creg_stage<LGN, 2, false>(buf, t, tw);
   if constexpr (P::S == 4) {
-    creg_sync<NT>(c);
+    reg_sync<NT>(c);
     creg_stage<LGN, 3, false>(buf, t, tw);
   }
   // the last stage's positions are the thread's own: no barrier before the product
@@ -299,24 +158,24 @@ MRM_D void creg_body(const RunDev<float>& rd, int k, int t, int c, bool live, co
   }
   if constexpr (P::S == 4) {
     creg_stage<LGN, 3, true>(buf, t, tw);
-    creg_sync<NT>(c);
+    reg_sync<NT>(c);
   }
   creg_stage<LGN, 2, true>(buf, t, tw);
-  creg_sync<NT>(c);
+  reg_sync<NT>(c);
   creg_stage<LGN, 1, true>(buf, t, tw);
-  creg_sync<NT>(c);
+  reg_sync<NT>(c);
   if (live) {
     // inverse stage 0 and the H^ rows, row-major [plane][ny][phs]
     Cx<float> w[8];
-    creg_twiddles<LGN, 0>(w, t, tw);
-    const int a = xswz(creg_base<B0>(t));
+    reg_twiddles<LGN, 0>(w, t, tw);
+    const int a = xswz(reg_base<B0>(t));
     Cx<float>* dst = spech + k;
 #pragma unroll 1
     for (int q = 0; q < 3; ++q) {
       Cx<float> v[8];
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk) v[kk] = buf[q * N + (a ^ xswz(kk << B0))];
-      creg_inv<LGN, 0>(v, w);
+      reg_inv<LGN, 0>(v, w);
 #pragma unroll
       for (int kk = 0; kk < KIN; ++kk) {
         const int j = t + kk * NT;
@@ -331,9 +190,10 @@ MRM_D void creg_body(const RunDev<float>& rd, int k, int t, int c, bool live, co
 template <int LGN, int BLOCK, class AFTER>
 MRM_D void creg_column(const RunDev<float>& rd, int k0, int nc, const Cx<float>* tw, Cx<float>* xb,
                        const Cx<float>* stg, const AFTER& staged_read) {
-  using P = CregPlan<LGN>;
+  using P = RegPlan<LGN>;
   static_assert(P::NT <= BLOCK && BLOCK % P::NT == 0, "a block holds whole columns");
   static_assert(P::NT >= 32, "a column is one or more whole warps");
+  static_assert(P::NT == 32 || BLOCK / P::NT <= 4, "named barriers 1..4");
   const int c = threadIdx.x / P::NT, t = threadIdx.x % P::NT;
   const bool live = c < nc;
   Cx<float>* buf = xb + c * 3 * P::N;

@@ -21,6 +21,7 @@
 #pragma once
 #include "common.cuh"
 #include "fft.cuh"
+#include "regfft.cuh"
 #include "philox.cuh"
 #include "tma.cuh"
 
@@ -808,6 +809,75 @@ MRM_HD int row_fft_smem(int lgpx, int rpb) {
   return (row_tw_count(lgpx) + 2 * rpb * 3 * seq_stride(M)) * (int)sizeof(Cx<R>);
 }
 
+// Register row transforms of a block's sequences (FP32 runs, 16 <= M <= 1024
+// points): sequence s (= 3 row + component) at s * cs in each buffer, one group
+// of M/8 threads per sequence, group g taking sequences g, g + G, ...
+// (G = BLOCK / (M/8)).  The choice depends on M alone, so every row shape
+// computes the same transform.
+MRM_HD constexpr bool rrow_len_ok(int lgM) { return lgM >= 4 && lgM <= 10; }
+
+template <int LGM, int BLOCK>
+MRM_D void rrow_inverse_block(const Cx<float>* X, Cx<float>* xb, Cx<float>* out, int cs, int nseq, int nz,
+                              const Cx<float>* __restrict__ twpost, const Cx<float>* __restrict__ twpass) {
+  constexpr int NT = 1 << (LGM - 3), G = BLOCK / NT;
+  static_assert(G >= 1 && BLOCK % NT == 0, "whole groups per block");
+  static_assert(NT <= 32 || G <= 4, "named barriers 1..4");
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+#pragma unroll 1
+  for (int s0 = 0; s0 < nseq; s0 += G) {
+    const int s = s0 + g;
+    if (s < nseq) rrow_inverse<LGM>(X + s * cs, xb + s * cs, out + s * cs, t, g, nz, twpost, twpass);
+  }
+}
+
+// POST(s, t, nt, Y): the group's spectrum post-processing of sequence s from
+// its natural-order Y (the group is synchronised before and after the call's
+// reads through the next sequence's barriers; Y is not written again).
+template <int LGM, bool HALF, int BLOCK, class POST>
+MRM_D void rrow_forward_block(Cx<float>* in, Cx<float>* xb, int cs, int nseq, const Cx<float>* __restrict__ twpass,
+                              const POST& post) {
+  constexpr int NT = 1 << (LGM - 3), G = BLOCK / NT;
+  static_assert(G >= 1 && BLOCK % NT == 0, "whole groups per block");
+  static_assert(NT <= 32 || G <= 4, "named barriers 1..4");
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+#pragma unroll 1
+  for (int s0 = 0; s0 < nseq; s0 += G) {
+    const int s = s0 + g;
+    if (s < nseq) {
+      rrow_forward<LGM, HALF>(in + s * cs, xb + s * cs, in + s * cs, t, g, twpass);
+      post(s, t, NT, in + s * cs);
+    }
+  }
+}
+
+template <int BLOCK, int LGMAX>
+MRM_D void rrow_inverse_any(int lgM, const Cx<float>* X, Cx<float>* xb, Cx<float>* out, int cs, int nseq, int nz,
+                            const Cx<float>* twpost, const Cx<float>* twpass) {
+  switch (lgM) {
+    case 4: rrow_inverse_block<4, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    case 5: rrow_inverse_block<5, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    case 6: rrow_inverse_block<6, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    case 7: if constexpr (LGMAX >= 8) rrow_inverse_block<7, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    case 8: if constexpr (LGMAX >= 9) rrow_inverse_block<8, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    case 9: if constexpr (LGMAX >= 10) rrow_inverse_block<9, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+    default: if constexpr (LGMAX >= 11) rrow_inverse_block<10, BLOCK>(X, xb, out, cs, nseq, nz, twpost, twpass); break;
+  }
+}
+
+template <int BLOCK, int LGMAX, bool HALF, class POST>
+MRM_D void rrow_forward_any(int lgM, Cx<float>* in, Cx<float>* xb, int cs, int nseq, const Cx<float>* twpass,
+                            const POST& post) {
+  switch (lgM) {
+    case 4: rrow_forward_block<4, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    case 5: rrow_forward_block<5, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    case 6: rrow_forward_block<6, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    case 7: if constexpr (LGMAX >= 8) rrow_forward_block<7, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    case 8: if constexpr (LGMAX >= 9) rrow_forward_block<8, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    case 9: if constexpr (LGMAX >= 10) rrow_forward_block<9, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+    default: if constexpr (LGMAX >= 11) rrow_forward_block<10, HALF, BLOCK>(in, xb, cs, nseq, twpass, post); break;
+  }
+}
+
 // Row kernel: one task = up to RPB grid rows of one layer of one run.
 //   kInit: forward row FFT of Ms*m (spectrum of the current state)
 //   kPred / kCorr: inverse row FFT of H^ -> H_demag, field assembly, Heun
@@ -988,7 +1058,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
   Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
-  if (inverse) {
+  // FP32 rows of 16..1024 complex points: the register transforms
+  constexpr bool kRegRowType = sizeof(R) == sizeof(float);
+  const bool regrow = kRegRowType && rrow_len_ok(lgM);
+  if (inverse && regrow) {
+    if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0))) return;
+    if constexpr (kRegRowType)
+      rrow_inverse_any<BLOCK, LGMAX>(lgM, bufB, bufA, bufB, cs, nseq, (nx + 1) >> 1, twpost, twpass);
+    __syncthreads();
+    Z = bufB;
+  } else if (inverse) {
     if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0))) return;
     const int tot = nseq * M;
     for (int idx = threadIdx.x; idx < tot; idx += BLOCK) {
@@ -1423,20 +1502,51 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   if (STAGE == kEval || rd.demag == 0) return;  // (reloaded: one register less across the loop)
 
   // ---------------- forward row transform of Ms*m -> spectrum columns ----------------
+  // (the register transforms of a row whose upper half is zero padding read
+  // only its lower half)
   const int two_m = 2 * M;
-  if (nx < two_m) {
+  const bool half_in = regrow && nx <= M;
+  const int zlim = half_in ? M : two_m;
+  if (nx < zlim) {
     for (int s = 0; s < nseq; ++s)
-      for (int i = nx + threadIdx.x; i < two_m; i += BLOCK) outr[s * rs + i] = (R)0;
+      for (int i = nx + threadIdx.x; i < zlim; i += BLOCK) outr[s * rs + i] = (R)0;
   }
   __syncthreads();
   Cx<R>* scratch = (W == bufA) ? bufB : bufA;
+  const int nys = rd.nys, lgct = rd.lgct, T = 1 << lgct, ntile = (ph + T - 1) >> lgct;
+  if constexpr (kRegRowType) {
+    if (regrow) {
+      // X[k] = e - i w^k o (w = e^{-2 pi i / px}) for the group's sequence:
+      // thread t takes k = t + j M/8 (and k = M), stored in column tiles of
+      // T = 2^lgct columns, each tile row by row
+      auto post = [&](int s, int t, int nt, const Cx<R>* Ys) {
+        const int row = s / 3, comp = s - 3 * row;
+        Cx<R>* dst = rd.specx + (size_t)(l * 3 + comp) * ntile * nys * T;
+#pragma unroll 1
+        for (int k = t; k <= M; k += nt) {
+          const Cx<R> yk = Ys[k & (M - 1)];
+          const Cx<R> ymk = cconj(Ys[(M - k) & (M - 1)]);
+          const Cx<R> e = cscale(cadd(yk, ymk), (R)0.5);
+          const Cx<R> o = cscale(csub(yk, ymk), (R)0.5);
+          const Cx<R> wo = cmul(twpost[k], o);
+          const long long at = (((long long)(k >> lgct) * nys + row0 + row) << lgct) + (k & (T - 1));
+          if (!MRM_CHECK((long long)(l * 3 + comp) * ntile * nys * T + at < (long long)rd.nl * 3 * ntile * nys * T,
+                         310, k))
+            continue;
+          dst[at] = csub(e, cmul_i(wo, (R)1));
+        }
+      };
+      if (half_in) rrow_forward_any<BLOCK, LGMAX, true>(lgM, W, scratch, cs, nseq, twpass, post);
+      else rrow_forward_any<BLOCK, LGMAX, false>(lgM, W, scratch, cs, nseq, twpass, post);
+      return;
+    }
+  }
   Cx<R>* Y = block_fft_c<R, -1, NBMAX, BLOCK, LGMAX - 1>(W, scratch, lgM, nseq, twpass);
   // X[k] = e - i w^k o (w = e^{-2 pi i / px}), stored in column tiles of T =
   // 2^lgct columns (one column task), each tile row by row: consecutive threads
   // take the T columns of a row, then the task's next rows, then the next tile
   const int lgr = nrows > 1 ? 32 - __clz(nrows - 1) : 0;
   const int rmask = (1 << lgr) - 1;
-  const int nys = rd.nys, lgct = rd.lgct, T = 1 << lgct, ntile = (ph + T - 1) >> lgct;
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) {
     Cx<R>* dst = rd.specx + (size_t)(l * 3 + comp) * ntile * nys * T;
