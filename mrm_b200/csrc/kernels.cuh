@@ -763,6 +763,38 @@ struct RowStage {
   int bytes;                    // total
 };
 
+// Loads from shared memory through a generic pointer that is known to point
+// there (ld.shared: the compiler need not prove the address space).
+MRM_D V4<float> lds_v4(const V4<float>* p) {
+  V4<float> v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(smem_u32(p)));
+  return v;
+}
+MRM_D V4<double> lds_v4(const V4<double>* p) {
+  V4<double> v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(smem_u32(p)));
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2 + 16];" : "=d"(v.z), "=d"(v.w) : "r"(smem_u32(p)));
+  return v;
+}
+MRM_D float lds_r(const float* p) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
+  return v;
+}
+MRM_D double lds_r(const double* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+  return v;
+}
+
+// compile-time value selecting a generic lambda's instantiation
+template <int V>
+struct IntC {
+  static constexpr int value = V;
+};
+
 // R-valued rows can be staged when a row is a whole number of 16-byte units
 template <typename R>
 MRM_HD bool rows_16b(int nx) { return ((long long)nx * (long long)sizeof(R)) % 16 == 0; }
@@ -1090,31 +1122,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[2], 0))) return;
 
   // ---------------- per-grain field + integrator stage ----------------
-  // row views: staged rows in shared memory, or the global arrays
-  const V4<R>* PB = staged ? reinterpret_cast<const V4<R>*>(stg + sp.pb) : L.pb + base;
-  const V4<R>* PA = (staged && sp.pa >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.pa) : L.pa + base;
-  const V4<R>* XS = (staged && sp.xst >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.xst) : L.xst + base;
-  const R* UC = (staged && sp.ucol >= 0) ? reinterpret_cast<const R*>(stg + sp.ucol) : (ucol ? L.ucol + base : nullptr);
-  const R* LC = (staged && sp.lcol >= 0) ? reinterpret_cast<const R*>(stg + sp.lcol) : (lcol ? L.lcol + base : nullptr);
-  const V4<R>* MF = staged ? reinterpret_cast<const V4<R>*>(stg + sp.mf) + sp.halo * nx : mfield + base;
-  const V4<R>* M0 = (staged && sp.m0 >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.m0) : L.m + base;
-  const V4<R>* DM = (staged && sp.dm >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.dm) : L.dm + base;
-  const V4<R>* HT = (staged && sp.ht >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.ht) : L.ht + base;
-  const V4<R>* VU = (staged && sp.vu >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.vu) : (ucol ? mother_u + base : nullptr);
-  const V4<R>* VL = (staged && sp.vl >= 0) ? reinterpret_cast<const V4<R>*>(stg + sp.vl) : (lcol ? mother_l + base : nullptr);
-  // field row rr in [-1, nrows] (lattice neighbours wrap periodically)
-  auto mf_row = [&](int rr) -> const V4<R>* {
-    if (staged) return MF + rr * nx;
-    if (win) {
-      int j = wj0 + row0 + rr;
-      j = j < 0 ? j + gny : (j >= gny ? j - gny : j);
-      return mfield + (size_t)j * gnx;
-    }
-    int j = row0 + rr;
-    j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
-    return mfield + (size_t)j * nx;
-  };
-
   const double t_now = rd.t_base + (double)(step - rd.step_base) * rd.dt;
   const double t_stage = (STAGE == kCorr) ? t_now + (mid ? 0.5 * rd.dt : rd.dt) : t_now;
   const double sc = ramp(L, t_stage);
@@ -1180,22 +1187,74 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 #pragma unroll
   for (int s = 0; s < (stats ? kNPart : 1); ++s) rec[s] = 0.0;
 
+  // The per-grain loop, compiled twice in the fast kernels without
+  // reductions: staged (the
+  // block's rows in shared memory: every row view is a shared-memory address
+  // known as such, and no global fallback is loaded) and unstaged.  Staged, the plan
+  // holds every row the loop reads: pa and the row field outside kInit, xst
+  // with the stencil, m0 and dm in kCorr, ht in kCorr with a thermal field,
+  // vu / vl with the columnar couplings (row_stage_plan); ucol / lcol rows
+  // are staged when a row is a whole number of 16-byte units.
+  auto grain_loop = [&](auto mode_c) {
+  // mode 1: staged, 0: unstaged, 2: decided at run time (the general kernels,
+  // whose larger loop bodies would spill more as two copies)
+  constexpr int MODE = decltype(mode_c)::value;
+  const bool ST = MODE == 2 ? staged : MODE == 1;
+  auto srow = [&](int off) { return reinterpret_cast<const V4<R>*>(stg + off); };
+  const V4<R>* PB = ST ? srow(sp.pb) : L.pb + base;
+  const V4<R>* PA = ST ? srow(sp.pa) : L.pa + base;
+  const V4<R>* XS = ST ? srow(sp.xst) : L.xst + base;
+  const R* UC = (ST && sp.ucol >= 0) ? reinterpret_cast<const R*>(stg + sp.ucol) : (ucol ? L.ucol + base : nullptr);
+  const R* LC = (ST && sp.lcol >= 0) ? reinterpret_cast<const R*>(stg + sp.lcol) : (lcol ? L.lcol + base : nullptr);
+  const V4<R>* MF = ST ? srow(sp.mf) + sp.halo * nx : mfield + base;
+  const V4<R>* M0 = ST ? srow(sp.m0) : L.m + base;
+  const V4<R>* DM = ST ? srow(sp.dm) : L.dm + base;
+  const V4<R>* HT = ST ? srow(sp.ht) : L.ht + base;
+  const V4<R>* VU = ST ? srow(sp.vu) : (ucol ? mother_u + base : nullptr);
+  const V4<R>* VL = ST ? srow(sp.vl) : (lcol ? mother_l + base : nullptr);
+  if (ST) {
+    MRM_CHECK(STAGE == kInit || sp.pa >= 0, 950, sp.pa);
+    MRM_CHECK(STAGE == kInit || !stencil || sp.xst >= 0, 951, sp.xst);
+    MRM_CHECK(STAGE != kCorr || (sp.m0 >= 0 && sp.dm >= 0 && (!thermal || sp.ht >= 0)), 952, sp.m0);
+    MRM_CHECK(STAGE == kInit || ((!ucol || sp.vu >= 0) && (!lcol || sp.vl >= 0)), 953, sp.vu);
+  }
+  // field row rr in [-1, nrows] (lattice neighbours wrap periodically)
+  auto mf_row = [&](int rr) -> const V4<R>* {
+    if (ST) return MF + rr * nx;
+    if (win) {
+      int j = wj0 + row0 + rr;
+      j = j < 0 ? j + gny : (j >= gny ? j - gny : j);
+      return mfield + (size_t)j * gnx;
+    }
+    int j = row0 + rr;
+    j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
+    return mfield + (size_t)j * nx;
+  };
+  // row-view loads: explicit shared-memory loads when staged
+  auto at4 = [&](const V4<R>* p, int i) -> V4<R> {
+    if constexpr (MODE == 1) return lds_v4(p + i);
+    else return p[i];
+  };
+  auto at1 = [&](const R* p, int i) -> R {
+    if constexpr (MODE == 1) return lds_r(p + i);
+    else return p[i];
+  };
   for (int idx = threadIdx.x; idx < ngr; idx += BLOCK) {
     const int rr = pow2x ? (idx >> lgnx) : idx / nx;
     const int i = idx - rr * nx;
     const int q = idx;                // index within the task's rows
     const int n = base + idx;         // grain index within the layer
-    const V4<R> pb = PB[q];
+    const V4<R> pb = at4(PB, q);
     const R mse = pb.x;  // Ms * ms_scale
     if (STAGE == kInit) {
-      const V4<R> mf = MF[q];
+      const V4<R> mf = at4(MF, q);
       outr[(rr * 3 + 0) * rs + i] = mse * mf.x;
       outr[(rr * 3 + 1) * rs + i] = mse * mf.y;
       outr[(rr * 3 + 2) * rs + i] = mse * mf.z;
       continue;
     }
-    const V4<R> mf = MF[q];
-    const V4<R> pa = PA[q];
+    const V4<R> mf = at4(MF, q);
+    const V4<R> pa = at4(PA, q);
     R hdx = 0, hdy = 0, hdz = 0;
     if (mapped) {
       const V4<R> g = L.cgrain ? L.hdm[n] : L.hd[n];
@@ -1203,9 +1262,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       hdy = g.y;
       hdz = g.z;
     } else if (use_hdr) {
-      hdx = hdr[(rr * 3 + 0) * rs + i];
-      hdy = hdr[(rr * 3 + 1) * rs + i];
-      hdz = hdr[(rr * 3 + 2) * rs + i];
+      hdx = at1(hdr, (rr * 3 + 0) * rs + i);
+      hdy = at1(hdr, (rr * 3 + 1) * rs + i);
+      hdz = at1(hdr, (rr * 3 + 2) * rs + i);
     }
     // applied field of this grain: the uniform part (plus the write head's in
     // the evaluation stage; the stepping stages carry it in hdx, hdz)
@@ -1266,13 +1325,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     }
     R ex = 0, ey = 0, ez = 0;
     if (stencil) {
-      const V4<R> c = XS[q];
+      const V4<R> c = at4(XS, q);
       const V4<R>* rowc = mf_row(rr);
       // (in a window the neighbours are the full grid's: row pointers at the
       // full rows' starts, the grid column wi0 + i)
       const int ci = wi0 + i;
       const int im = (ci == 0 ? gnx - 1 : ci - 1), ip = (ci == gnx - 1 ? 0 : ci + 1);
-      const V4<R> n0 = mf_row(rr - 1)[ci], n1 = rowc[im], n2 = rowc[ip], n3 = mf_row(rr + 1)[ci];
+      const V4<R> n0 = at4(mf_row(rr - 1), ci), n1 = at4(rowc, im), n2 = at4(rowc, ip), n3 = at4(mf_row(rr + 1), ci);
       ex = c.x * n0.x + c.y * n1.x + c.z * n2.x + c.w * n3.x;
       ey = c.x * n0.y + c.y * n1.y + c.z * n2.y + c.w * n3.y;
       ez = c.x * n0.z + c.y * n1.z + c.z * n2.z + c.w * n3.z;
@@ -1332,7 +1391,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         htz = s * gn[2];
         L.ht[n] = V4<R>{htx, hty, htz, (R)0};
       } else {
-        const V4<R> ht = HT[q];
+        const V4<R> ht = at4(HT, q);
         htx = ht.x;
         hty = ht.y;
         htz = ht.z;
@@ -1432,11 +1491,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         L.dm[n] = V4<R>{dx, dy, dz, (R)0};
         m0 = mf;
       } else {
-        const V4<R> d1 = DM[q];
+        const V4<R> d1 = at4(DM, q);
         dx = (R)0.5 * (dx + d1.x);
         dy = (R)0.5 * (dy + d1.y);
         dz = (R)0.5 * (dz + d1.z);
-        m0 = M0[q];
+        m0 = at4(M0, q);
       }
       mn.x = m0.x + dx;
       mn.y = m0.y + dy;
@@ -1495,6 +1554,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
                            (double)(ez + vz) * mf.z) * (double)mse;
       rec[kSlotE] += (e_d + (double)e_k + e_x) * v;
     }
+  }
+  };
+  if constexpr (GEN == 0 && !stats) {
+    if (staged) grain_loop(IntC<1>{});
+    else grain_loop(IntC<0>{});
+  } else {
+    grain_loop(IntC<2>{});
   }
   if constexpr (stats) {
     block_reduce_record(rec, sred, part + (size_t)blockIdx.x * kNPart);

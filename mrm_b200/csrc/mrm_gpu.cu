@@ -202,10 +202,22 @@ int set_err(std::string* dst, int code, const char* fmt, ...) {
     }                                                                                      \
   } while (0)
 
+// The engine streams are non-blocking: they do not wait for work on the
+// legacy default stream.  Zero-fills and uploads issued there therefore
+// complete before these helpers return (a cudaMemset is asynchronous, and a
+// pageable host-to-device cudaMemcpy may return before its DMA lands), so no
+// later kernel on an engine stream can overtake them.
 int dmalloc(std::string* errp, void** p, size_t bytes) {
   CK(cudaMalloc(p, bytes ? bytes : 16));
   CK(cudaMemset(*p, 0, bytes ? bytes : 16));
+  CK(cudaStreamSynchronize(cudaStreamLegacy));
   return MRM_OK;
+}
+
+cudaError_t h2d(void* dst, const void* src, size_t bytes) {
+  const cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(cudaStreamLegacy);
 }
 
 void dfree(void*& p) {
@@ -266,13 +278,13 @@ int engine_init(Engine* e, int prec, int dev) {
   if (prec == MRM_FP64) {
     int rc = dmalloc(errp, &e->d_tw, sizeof(double) * 2 * ntw);
     if (rc) return rc;
-    CK(cudaMemcpy(e->d_tw, tw.data(), sizeof(double) * 2 * ntw, cudaMemcpyHostToDevice));
+    CK(h2d(e->d_tw, tw.data(), sizeof(double) * 2 * ntw));
   } else {
     std::vector<float> twf(2 * ntw);
     for (size_t k = 0; k < 2 * ntw; ++k) twf[k] = (float)tw[k];
     int rc = dmalloc(errp, &e->d_tw, sizeof(float) * 2 * ntw);
     if (rc) return rc;
-    CK(cudaMemcpy(e->d_tw, twf.data(), sizeof(float) * 2 * ntw, cudaMemcpyHostToDevice));
+    CK(h2d(e->d_tw, twf.data(), sizeof(float) * 2 * ntw));
   }
   {
     int rc = dmalloc(errp, (void**)&e->d_err, 4 * sizeof(int));  // flags, first check code, its value
@@ -929,8 +941,9 @@ std::map<std::string, Shape>& tune_cache() {
   return c;
 }
 
-// Times each row shape (predictor + corrector launches) and each column
-// shape x columns per task on the batch itself and keeps the fastest.  The
+// Times each column shape x columns per task, then each row shape, on the
+// batch itself (one Heun step's chained launches, as the captured steps run
+// them) and keeps the fastest.  The
 // kernels run on the real state, which is saved before and restored after
 // (m and the stored field per layer; the spectra are re-established).
 template <typename R>
@@ -983,7 +996,17 @@ int autotune(Engine* e) {
     for (auto* r : e->runs) r->spec_valid = false;
     return establish_spectra<R>(e);
   };
-  const int reps = 4;
+  const int reps = 6;
+  // one Heun step's four launches, chained as in the captured steps (the
+  // shapes interact through the overlap of a kernel's tail with the next
+  // kernel's start)
+  auto heun_step = [&]() -> cudaError_t {
+    cudaError_t a = launch_row_e<R>(e, kPred, false, 0, kFlagForce, true);
+    cudaError_t b = launch_col_e<R>(e, 0, kFlagForce, true);
+    cudaError_t c = launch_row_e<R>(e, kCorr, false, 0, kFlagForce, true);
+    cudaError_t d = launch_col_e<R>(e, 0, kFlagForce, true);
+    return a != cudaSuccess ? a : b != cudaSuccess ? b : c != cudaSuccess ? c : d;
+  };
   // column shapes with the default row shape
   Shape best = {e->rowv, e->colv, e->cpt};
   float best_ms = 1e30f;
@@ -998,7 +1021,7 @@ int autotune(Engine* e) {
       e->err.clear();
       if (prepare() != MRM_OK) continue;
       float ms = 0;
-      int rc = time_it([&]() { return launch_col_e<R>(e, 0, kFlagForce, false); }, reps, &ms);
+      int rc = time_it(heun_step, reps, &ms);
       if (rc) return rc;
       if (ms < best_ms) {
         best_ms = ms;
@@ -1015,15 +1038,7 @@ int autotune(Engine* e) {
     e->err.clear();
     if (prepare() != MRM_OK) continue;
     float ms = 0;
-    int rc = time_it(
-        [&]() {
-          cudaError_t a = launch_row_e<R>(e, kPred, false, 0, kFlagForce, false);
-          cudaError_t b = launch_col_e<R>(e, 0, kFlagForce, false);
-          cudaError_t c = launch_row_e<R>(e, kCorr, false, 0, kFlagForce, false);
-          cudaError_t d = launch_col_e<R>(e, 0, kFlagForce, false);
-          return a != cudaSuccess ? a : b != cudaSuccess ? b : c != cudaSuccess ? c : d;
-        },
-        reps, &ms);
+    int rc = time_it(heun_step, reps, &ms);
     if (rc) return rc;
     if (ms < best_ms) {
       best_ms = ms;
@@ -1425,9 +1440,9 @@ int upload_csr(mrm_gpu* r, int n, const int32_t* index, const int32_t* grain, co
   if (rc) return rc;
   rc = dmalloc(errp, dcoef, sizeof(R) * std::max(nnz, 1));
   if (rc) return rc;
-  CK(cudaMemcpy(*didx, index, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(*dnbr, nb.data(), sizeof(int) * std::max(nnz, 1), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(*dcoef, cf.data(), sizeof(R) * std::max(nnz, 1), cudaMemcpyHostToDevice));
+  CK(h2d(*didx, index, sizeof(int) * (n + 1)));
+  CK(h2d(*dnbr, nb.data(), sizeof(int) * std::max(nnz, 1)));
+  CK(h2d(*dcoef, cf.data(), sizeof(R) * std::max(nnz, 1)));
   return MRM_OK;
 }
 
@@ -1506,9 +1521,9 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
     pv[4 * c + 3] = first ? 1.0 : 0.0;
   }
   LayerBufs& b = r->L[l];
-  CK(cudaMemcpy(b.pa, pa.data(), sizeof(R) * 4 * nc, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.pb, pb.data(), sizeof(R) * 4 * nc, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.pv, pv.data(), sizeof(double) * 4 * nc, cudaMemcpyHostToDevice));
+  CK(h2d(b.pa, pa.data(), sizeof(R) * 4 * nc));
+  CK(h2d(b.pb, pb.data(), sizeof(R) * 4 * nc));
+  CK(h2d(b.pv, pv.data(), sizeof(double) * 4 * nc));
   auto& hc = host_cache()[r];
   hc.resize(MRM_MAX_LAYERS);
   hc[l].ms_scale.assign(ms_scale, ms_scale + n);
@@ -1534,9 +1549,9 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
     if (!rc) rc = dmalloc(errp, &b.hdm, sizeof(R) * 4 * (size_t)nc);
     if (!rc) rc = dmalloc(errp, &b.hapm, sizeof(R) * 4 * (size_t)nc);
     if (rc) return rc;
-    CK(cudaMemcpy(b.cgrain, cg.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b.gci, g2ci, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b.gcs, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+    CK(h2d(b.cgrain, cg.data(), sizeof(int) * nc));
+    CK(h2d(b.gci, g2ci, sizeof(int) * (n + 1)));
+    CK(h2d(b.gcs, cells.data(), sizeof(int) * cells.size()));
   }
   if (!identity && hxi && hxg && hx) {
     // intralayer exchange of the grains, on every cell of each grain, with each
@@ -1583,7 +1598,7 @@ int upload_layer_t(mrm_gpu* r, int l, int n, const double* ms, const double* vol
     if (lattice) {
       int rc2 = dmalloc(errp, &b.xst, sizeof(R) * 4 * (size_t)n);
       if (rc2) return rc2;
-      CK(cudaMemcpy(b.xst, st.data(), sizeof(R) * 4 * (size_t)n, cudaMemcpyHostToDevice));
+      CK(h2d(b.xst, st.data(), sizeof(R) * 4 * (size_t)n));
     }
   } else {
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
@@ -1641,7 +1656,7 @@ int tensor_real(mrm_gpu* r, double* d_n2d) {
   void* d_pg = nullptr;
   int rc = dmalloc(errp, &d_pg, sizeof(PairGeom) * npair);
   if (rc) return rc;
-  CK(cudaMemcpy(d_pg, pg.data(), sizeof(PairGeom) * npair, cudaMemcpyHostToDevice));
+  CK(h2d(d_pg, pg.data(), sizeof(PairGeom) * npair));
   const int nimg = r->g.boundary == MRM_OPEN ? 0 : std::max(0, r->g.num_images);
   const long long total = (long long)npair * r->px * r->py;
   tensor_real_kernel<<<(unsigned)((total + 127) / 128), 128, 0, r->eng->st>>>(
@@ -1677,7 +1692,7 @@ int tensor_spectrum(mrm_gpu* r, const double* d_n2d) {
   }
   rc = dmalloc(errp, &d_tw64, sizeof(double) * 2 * kTwN);
   if (rc) return rc;
-  CK(cudaMemcpy(d_tw64, tw.data(), sizeof(double) * 2 * kTwN, cudaMemcpyHostToDevice));
+  CK(h2d(d_tw64, tw.data(), sizeof(double) * 2 * kTwN));
   const Cx<double>* tw64 = static_cast<const Cx<double>*>(d_tw64);
   const int M = r->px / 2;
   // two shared buffers of one padded-stride sequence each (fft.cuh)
@@ -1746,7 +1761,7 @@ int set_cubic_t(mrm_gpu* h, int layer, const double* cubic_axis) {
     int rc = dmalloc(errp, &b.cax, sizeof(R) * 12 * (size_t)n);
     if (rc) return rc;
   }
-  CK(cudaMemcpy(b.cax, v.data(), sizeof(R) * 12 * (size_t)n, cudaMemcpyHostToDevice));
+  CK(h2d(b.cax, v.data(), sizeof(R) * 12 * (size_t)n));
   return MRM_OK;
 }
 
@@ -1894,10 +1909,10 @@ int mrm_gpu_upload_interlayer(mrm_gpu* h, int layer, int side, const int32_t* in
     rc = dmalloc(errp, col, re * n);
     if (rc) return rc;
     if (h->g.precision == MRM_FP64) {
-      CK(cudaMemcpy(*col, cf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+      CK(h2d(*col, cf.data(), sizeof(double) * n));
     } else {
       std::vector<float> f(cf.begin(), cf.end());
-      CK(cudaMemcpy(*col, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+      CK(h2d(*col, f.data(), sizeof(float) * n));
     }
   }
   h->eng->desc_dirty = true;
@@ -2047,7 +2062,7 @@ int mrm_gpu_upload_tensor(mrm_gpu* h, const double* n2d, int nx_fft, int ny_fft)
   const size_t bytes = sizeof(double) * 9 * (size_t)h->nl * h->nl * h->px * h->py;
   int rc = dmalloc(errp, &d_n2d, bytes);
   if (rc) return rc;
-  CK(cudaMemcpy(d_n2d, n2d, bytes, cudaMemcpyHostToDevice));
+  CK(h2d(d_n2d, n2d, bytes));
   rc = tensor_spectrum(h, static_cast<const double*>(d_n2d));
   dfree(d_n2d);
   return rc;
@@ -2249,9 +2264,9 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
   td.t0 = t_origin;
   td.dx = h->g.dx;
   td.dy = h->g.dy;
-  CK(cudaMemcpy(b.tb_v, vfld, sizeof(double) * nv, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.tb_pos, pos.data(), sizeof(double) * pos.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.tab, &td, sizeof(TabDev), cudaMemcpyHostToDevice));
+  CK(h2d(b.tb_v, vfld, sizeof(double) * nv));
+  CK(h2d(b.tb_pos, pos.data(), sizeof(double) * pos.size()));
+  CK(h2d(b.tab, &td, sizeof(TabDev)));
   if (b.func == kFuncHead) {  // back to the default time scale (1)
     b.func = 0;
     b.scale = 1.0;
@@ -2321,8 +2336,8 @@ static int set_llb_mode(mrm_gpu* h, int layer, double spin, const double* tc, co
   d.mode = mode;
   d.meq_bs = meq_bs ? 1 : 0;
   d.garanin_tau = garanin_tau ? 1 : 0;
-  CK(cudaMemcpy(b.llbp, rec.data(), sizeof(V4<double>) * (size_t)nc, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.llb, &d, sizeof(LlbDev), cudaMemcpyHostToDevice));
+  CK(h2d(b.llbp, rec.data(), sizeof(V4<double>) * (size_t)nc));
+  CK(h2d(b.llb, &d, sizeof(LlbDev)));
   return MRM_OK;
 }
 
@@ -2334,7 +2349,7 @@ static int push_temp_profile(mrm_gpu* h, LayerBufs& b) {
   }
   CK(cudaSetDevice(h->eng->dev));
   CK(cudaStreamSynchronize(h->eng->st));
-  CK(cudaMemcpy(b.tprof, &b.tp, sizeof(TempDev), cudaMemcpyHostToDevice));
+  CK(h2d(b.tprof, &b.tp, sizeof(TempDev)));
   h->eng->desc_dirty = true;
   h->eng->tables_dirty = true;  // the general kernels
   return MRM_OK;
