@@ -201,9 +201,9 @@ int mrm_gpu_set_field_table(mrm_gpu* h, int layer, int nfx, int nfy, const doubl
  *   fx(i) = exp(-(((i + 1/2) dx + ref_x - vel_x (t - t_origin) - offset_x)/sigma_x)^(2 expn))
  * (y alike; sigma 0: flat; offsets below -1e200: the grid centre), s(t) the
  * profile's time scale (mrm_gpu_set_temp_function; default 1).  The grain's
- * temperature replaces the layer's in the thermal variance and in the LLB / MT
- * pushes (the temperature-scaling tables are not part of this path: Ms, Hk and
- * alpha scales stay inputs).  One grain per cell.  expn < 0 removes it.
+ * temperature replaces the layer's in the thermal variance, in the LLB / MT
+ * pushes and in the layer's temperature scaling (mrm_gpu_set_temp_scaling).
+ * One grain per cell.  expn < 0 removes it.
  * mrm_gpu_set_temp_function: s(t) = ((s_end - s_start) clamp((t - t_start) /
  * (t_end - t_start), 0, 1) + s_start) scale (func 0) or (amp f(t) + dc) scale
  * with f as in mrm_gpu_set_field_function (func 1..5). */
@@ -213,6 +213,35 @@ int mrm_gpu_set_temp_profile(mrm_gpu* h, int layer, double background, double dt
 int mrm_gpu_set_temp_function(mrm_gpu* h, int layer, int func, double t_start, double t_end, double s_start,
                               double s_end, double amp, double gamma, double phase, double param, double duty,
                               double moddepth, double dc, double scale);
+
+/* Temperature scaling of Ms, alpha and Hk on `layer` (set_temp_scaling and
+ * find_temp_scaling, temp_scaling.f90:37-50,365-433, applied at every field
+ * evaluation by get_applied, field.f90:527-595): with x = T/Tc of the grain
+ * (tc[n], field%tc; T its temperature at the evaluation),
+ *   ms_scale = clamp(|m|, 0, 1) (use_mag, the LLB magnitude), else
+ *              clamp(1 - x, 0, 1)^msexp (msexp >= 0), else the Ms table at x;
+ *   alpha_scale = the alpha table at x;  hk_scale = clamp(1 - x, 0, 1)^hkexp
+ *              (hkexp >= 0), else the Hk table at x;  a scale without a rule is 1.
+ * They enter as the reference's ms_scale, alpha_scale and hk_scale do: the
+ * demag source, the exchange terms (the neighbours' ms_scale), anisotropy,
+ * damping, the thermal variance and the reductions.  The layer must have been
+ * uploaded with unit scales (the reference's, which only this scaling
+ * changes), one grain per cell, no moving window, the lattice form of the
+ * exchange and columnar interlayer couplings (MRM_ERR_UNSUPPORTED /
+ * MRM_ERR_STATE otherwise).  tc NULL switches it off.  (No reference
+ * counterpart for the C form; the Fortran host calls it where it calls
+ * set_temp_scaling / init_temp_scaling.)
+ * mrm_gpu_set_temp_scaling_table: table `which` (1 Ms, 2 alpha, 3 Hk, 4 Hx)
+ * from n (temperature, scale) pairs as file_temp_scaling reads them
+ * (temp_scaling.f90:126-239), reduced as it reduces them (ordered, equal
+ * temperatures merged, equal end scales trimmed, temperatures above 5 taken
+ * as K and divided by the largest); a table of one node scales nothing; n = 0
+ * removes it.  The Hx table is kept but, as in the reference, scales nothing.
+ * mrm_gpu_get_temp_scaling_table: the reduced table (*n: room in, nodes out). */
+int mrm_gpu_set_temp_scaling(mrm_gpu* h, int layer, const double* tc, double msexp, double hkexp, int use_mag);
+int mrm_gpu_set_temp_scaling_table(mrm_gpu* h, int layer, int which, int n, const double* temp,
+                                   const double* scaling);
+int mrm_gpu_get_temp_scaling_table(const mrm_gpu* h, int layer, int which, int* n, double* temp, double* scaling);
 
 /* LLB integrator (llgp%llb; push_llb, llg.f90:916-1064, Heun branch
  * :1000-1047 and the |m| = 0 branch :1048-1060) on `layer`: spin S, per grain

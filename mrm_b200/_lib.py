@@ -39,7 +39,8 @@ EXPORTS = [
     "mrm_gpu_set_cubic_axes", "mrm_gpu_step_adaptive", "mrm_gpu_off_field", "mrm_gpu_set_field_table",
     "mrm_gpu_set_window", "mrm_gpu_get_window", "mrm_gpu_set_llb", "mrm_gpu_set_mag", "mrm_gpu_get_mag",
     "mrm_gpu_set_mt", "mrm_gpu_set_temp_profile", "mrm_gpu_set_temp_function",
-    "mrm_gpu_set_zhang",
+    "mrm_gpu_set_zhang", "mrm_gpu_set_temp_scaling", "mrm_gpu_set_temp_scaling_table",
+    "mrm_gpu_get_temp_scaling_table",
 ]
 
 
@@ -141,6 +142,9 @@ def load(path: str = LIB_PATH):
         "mrm_gpu_set_zhang": ([vp, i, d, pd, i, i], i),
         "mrm_gpu_set_temp_profile": ([vp, i, d, d, d, d, i, d, d, d, d, d, d, d], i),
         "mrm_gpu_set_temp_function": ([vp, i, i] + [d] * 12, i),
+        "mrm_gpu_set_temp_scaling": ([vp, i, pd, d, d, i], i),
+        "mrm_gpu_set_temp_scaling_table": ([vp, i, i, i, pd, pd], i),
+        "mrm_gpu_get_temp_scaling_table": ([vp, i, i, C.POINTER(C.c_int), pd, pd], i),
         "mrm_gpu_set_mag": ([vp, i, pd], i),
         "mrm_gpu_get_mag": ([vp, i, pd], i),
         "mrm_gpu_set_shape": ([vp, i, i, i], i),

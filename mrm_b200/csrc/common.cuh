@@ -81,6 +81,22 @@ struct TempDev {
   double t_start, t_end, s_start, s_end, scale, amp, fgamma, phase, param, duty, moddepth, dc;
 };
 
+// Temperature scaling of a layer (find_temp_scaling, temp_scaling.f90:365-433),
+// in device memory: the cells' Tc; power laws (1 - T/Tc)^e of Ms and Hk
+// (e < 0: none); Ms scaled by |m| instead (mag, the LLB magnitude); reduced
+// tables T/Tc -> scale of Ms, alpha and Hk (table k: nt[k] nodes at
+// tt + off[k], tv + off[k]; fewer than 2 nodes: none); floor_ms of the
+// thermal variance.  The layer was uploaded with unit scales, which these
+// replace at every field evaluation.
+struct TscDev {
+  const double* tc;
+  const double* tt;
+  const double* tv;
+  int off[3], nt[3];
+  double msexp, hkexp, floor_ms;
+  int mag;
+};
+
 // Per-layer device view of one run.  State vectors are float4/double4
 // "SoA of 4-vectors": (x,y,z,w) per grain for one 16/32-byte load (w of m and
 // mp: the magnitude |m| of the LLB integrator; unused otherwise).
@@ -132,6 +148,7 @@ struct LayerDev {
   const struct TabDev* tab;  // tabulated field profile (null: the uniform hdir applies)
   const LlbDev* llb;         // LLB integrator (null: LLG)
   const TempDev* tprof;      // temperature profile (null: the uniform temperature)
+  const TscDev* tsc;         // temperature scaling of Ms, alpha, Hk (null: the uploaded scales)
   double temperature;
   double gamma;
   int thermal;

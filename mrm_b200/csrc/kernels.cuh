@@ -204,6 +204,51 @@ MRM_D double temp_cell(const TempDev& P, double s, double t, int i, int j) {
   return P.bg + s * fy * fx;
 }
 
+// find_temp_scaling (temp_scaling.f90:365-430) for one cell.  A table at
+// x = T/Tc: its first scale at or below the first node, its last at or above
+// the last, linear in between (bisection on the nodes, :397-414).
+MRM_D double tsc_table(const double* tt, const double* tv, int n, double x) {
+  int k1 = 0, k2 = n - 1;
+  double y;
+  if (x <= tt[0]) {
+    y = 0.0;
+  } else if (x >= tt[k2]) {
+    y = 0.0;
+    k1 = k2;
+  } else {
+    while (k2 - k1 > 1) {
+      const int k = (k2 + k1 + 2) / 2 - 1;  // the midpoint of the 1-based indices
+      if (x < tt[k]) k2 = k;
+      else k1 = k;
+    }
+    y = fmax(0.0, fmin(1.0, (x - tt[k1]) / (tt[k2] - tt[k1])));
+  }
+  return tv[k1] + y * (tv[k2] - tv[k1]);
+}
+// Ms scale of cell n at temperature T (|m| = mag): |m| itself (use_mag_p),
+// the power law, the table, or 1
+MRM_D double tsc_ms(const TscDev& S, int n, double T, double mag) {
+  if (S.mag) return fmin(1.0, fmax(0.0, fabs(mag)));
+  if (S.msexp >= 0.0) return pow(fmin(1.0, fmax(0.0, 1.0 - T / S.tc[n])), S.msexp);
+  if (S.nt[0] > 1) return tsc_table(S.tt + S.off[0], S.tv + S.off[0], S.nt[0], T / S.tc[n]);
+  return 1.0;
+}
+MRM_D double tsc_alpha(const TscDev& S, int n, double T) {
+  return S.nt[1] > 1 ? tsc_table(S.tt + S.off[1], S.tv + S.off[1], S.nt[1], T / S.tc[n]) : 1.0;
+}
+MRM_D double tsc_hk(const TscDev& S, int n, double T) {
+  if (S.hkexp >= 0.0) return pow(fmin(1.0, fmax(0.0, 1.0 - T / S.tc[n])), S.hkexp);
+  if (S.nt[2] > 1) return tsc_table(S.tt + S.off[2], S.tv + S.off[2], S.nt[2], T / S.tc[n]);
+  return 1.0;
+}
+// temperature of cell (i, j) of a layer at time t: its profile's, or the uniform one
+template <typename R>
+MRM_D double layer_temp(const LayerDev<R>& L, double t, int i, int j) {
+  if (!L.tprof) return L.temperature;
+  const TempDev& P = *L.tprof;
+  return temp_cell(P, P.dtemp * temp_scale(P, t), t, i, j);
+}
+
 // Write head (func 6): gap-centre position and write polarity at time t
 template <typename R>
 MRM_D void head_state(const LayerDev<R>& L, double t, double* xh, double* pol) {
@@ -1244,17 +1289,43 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     const int i = idx - rr * nx;
     const int q = idx;                // index within the task's rows
     const int n = base + idx;         // grain index within the layer
-    const V4<R> pb = at4(PB, q);
-    const R mse = pb.x;  // Ms * ms_scale
+    V4<R> pb = at4(PB, q);
+    // (temperature scaling, level 2: the grain's grid cell)
+    const int gi = wi0 + i, gj = wj0 + row0 + rr;
     if (STAGE == kInit) {
       const V4<R> mf = at4(MF, q);
-      outr[(rr * 3 + 0) * rs + i] = mse * mf.x;
-      outr[(rr * 3 + 1) * rs + i] = mse * mf.y;
-      outr[(rr * 3 + 2) * rs + i] = mse * mf.z;
+      R ms0 = pb.x;  // Ms * ms_scale
+      if constexpr (GEN == 2)
+        if (L.tsc) ms0 = (R)((double)pb.x * tsc_ms(*L.tsc, n, layer_temp(L, t_stage, gi, gj), (double)mf.w));
+      outr[(rr * 3 + 0) * rs + i] = ms0 * mf.x;
+      outr[(rr * 3 + 1) * rs + i] = ms0 * mf.y;
+      outr[(rr * 3 + 2) * rs + i] = ms0 * mf.z;
       continue;
     }
     const V4<R> mf = at4(MF, q);
-    const V4<R> pa = at4(PA, q);
+    V4<R> pa = at4(PA, q);
+    // Temperature scaling (find_temp_scaling at this stage's field evaluation,
+    // temp_scaling.f90:365-430): the grain's Ms, alpha and Hk scales replace
+    // the unit scales the layer was uploaded with (in Ms * ms_scale, Hk *
+    // hk_scale, alpha * alpha_scale, and the thermal variance's
+    // alpha_scale / max(floor_ms, ms_scale), field.f90:418-421)
+    double sc_ms = 1.0, sc_al = 1.0;
+    if constexpr (GEN == 2) {
+      if (L.tsc) {
+        const TscDev& S = *L.tsc;
+        const double Tn = layer_temp(L, t_stage, gi, gj);
+        sc_ms = tsc_ms(S, n, Tn, (double)mf.w);
+        sc_al = tsc_alpha(S, n, Tn);
+        const double sh = tsc_hk(S, n, Tn);
+        pb.x = (R)((double)pb.x * sc_ms);
+        pb.y = (R)((double)pb.y * sh);
+        pa.w = (R)((double)pa.w * sh);
+        pb.z = (R)((double)pb.z * sc_al);
+        pb.w = sc_ms > 0.0 ? (R)((double)pb.w * sqrt(sc_al * fmax(S.floor_ms, 1.0) / fmax(S.floor_ms, sc_ms)))
+                           : (R)0;
+      }
+    }
+    const R mse = pb.x;  // Ms * ms_scale
     R hdx = 0, hdy = 0, hdz = 0;
     if (mapped) {
       const V4<R> g = L.cgrain ? L.hdm[n] : L.hd[n];
@@ -1325,13 +1396,25 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     }
     R ex = 0, ey = 0, ez = 0;
     if (stencil) {
-      const V4<R> c = at4(XS, q);
+      V4<R> c = at4(XS, q);
       const V4<R>* rowc = mf_row(rr);
       // (in a window the neighbours are the full grid's: row pointers at the
       // full rows' starts, the grid column wi0 + i)
       const int ci = wi0 + i;
       const int im = (ci == 0 ? gnx - 1 : ci - 1), ip = (ci == gnx - 1 ? 0 : ci + 1);
       const V4<R> n0 = at4(mf_row(rr - 1), ci), n1 = at4(rowc, im), n2 = at4(rowc, ip), n3 = at4(mf_row(rr + 1), ci);
+      if constexpr (GEN == 2) {
+        if (L.tsc) {
+          // hx(j) ms_scale(j) m(j) (get_intralayer_hx, field.f90:350-363) with the
+          // neighbours' scales at this evaluation (one grain per cell, no window)
+          const TscDev& S = *L.tsc;
+          const int jm = gj == 0 ? gny - 1 : gj - 1, jp = gj == gny - 1 ? 0 : gj + 1;
+          c.x = (R)((double)c.x * tsc_ms(S, jm * gnx + ci, layer_temp(L, t_stage, ci, jm), (double)n0.w));
+          c.y = (R)((double)c.y * tsc_ms(S, gj * gnx + im, layer_temp(L, t_stage, im, gj), (double)n1.w));
+          c.z = (R)((double)c.z * tsc_ms(S, gj * gnx + ip, layer_temp(L, t_stage, ip, gj), (double)n2.w));
+          c.w = (R)((double)c.w * tsc_ms(S, jp * gnx + ci, layer_temp(L, t_stage, ci, jp), (double)n3.w));
+        }
+      }
       ex = c.x * n0.x + c.y * n1.x + c.z * n2.x + c.w * n3.x;
       ey = c.x * n0.y + c.y * n1.y + c.z * n2.y + c.w * n3.y;
       ez = c.x * n0.z + c.y * n1.z + c.z * n2.z + c.w * n3.z;
@@ -1339,16 +1422,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
     }
     R vx = 0, vy = 0, vz = 0;
+    // (a columnar partner layer with temperature scaling: its grain's ms_scale
+    // at this evaluation, get_interlayer_hx field.f90:326-348)
+    auto col_scale = [&](const LayerDev<R>* Lo, R cf, R mag) -> R {
+      if constexpr (GEN == 2)
+        if (Lo->tsc) return (R)((double)cf * tsc_ms(*Lo->tsc, n, layer_temp(*Lo, t_stage, gi, gj), (double)mag));
+      return cf;
+    };
     if (ucol) {
-      const R cu = UC[q];
       const V4<R> vu = VU[q];
+      const R cu = col_scale(Lu, UC[q], vu.w);
       vx += cu * vu.x; vy += cu * vu.y; vz += cu * vu.z;
     } else if (L.uidx && Lu) {
       csr_sum<R>(L.uidx, L.unbr, L.ucoef, mother_u, n, vx, vy, vz);
     }
     if (lcol) {
-      const R cl = LC[q];
       const V4<R> vl = VL[q];
+      const R cl = col_scale(Ll, LC[q], vl.w);
       vx += cl * vl.x; vy += cl * vl.y; vz += cl * vl.z;
     } else if (L.lidx && Ll) {
       csr_sum<R>(L.lidx, L.lnbr, L.lcoef, mother_l, n, vx, vy, vz);
@@ -1380,11 +1470,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
         const int nt = L.cgrain ? max(0, L.cgrain[n]) : n;
         thermal_normals(rd.seed, (unsigned long long)l, (unsigned long long)step, (unsigned long long)nt, gn);
         R s = (GEN == 2 && L.tprof) ? (R)((double)pb.w * sqrt(Tg / rd.dt)) : pb.w * tfac;
-        if (GEN == 2 && L.llb && (double)mf.w != 1.0) {
-          // get_thermal with |m| != 1 (field.f90:416-417): the variance over
-          // max(floor_ms, |m|) instead of max(floor_ms, ms_scale)
+        if (GEN == 2 && L.llb) {
           const LlbDev& P = *L.llb;
-          s = (R)sqrt(P.p[n].z * Tg / (fmax(P.floor_ms, fabs((double)mf.w)) * rd.dt));
+          if (P.mode != 2) {
+            // LLB and MT runs: get_thermal with no_ms_p (get_fields, llg.f90:363-365;
+            // field.f90:414-415): alpha_scale T / (Ms V)
+            s = (R)sqrt(P.p[n].z * sc_al * Tg / rd.dt);
+          } else if ((double)mf.w != 1.0) {
+            // Zhang with |m| != 1 (field.f90:416-417): the variance over
+            // max(floor_ms, |m|) instead of max(floor_ms, ms_scale)
+            s = (R)sqrt(P.p[n].z * sc_al * Tg / (fmax(P.floor_ms, fabs((double)mf.w)) * rd.dt));
+          }
         }
         htx = s * gn[0];
         hty = s * gn[1];
@@ -1519,13 +1615,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
     if (!llb) mn.w = (R)0;
     if (STAGE == kPred) L.mp[n] = mn;
     else L.m[n] = mn;
-    outr[(rr * 3 + 0) * rs + i] = mse * mn.x;
-    outr[(rr * 3 + 1) * rs + i] = mse * mn.y;
-    outr[(rr * 3 + 2) * rs + i] = mse * mn.z;
+    // the demag source of the next field evaluation (Ms ms_scale m): with
+    // temperature scaling, the scale at that evaluation's time and state
+    R msrc = mse;
+    if constexpr (GEN == 2) {
+      if (L.tsc) {
+        const double t_src = (STAGE == kPred && mid) ? t_now + 0.5 * rd.dt : t_now + rd.dt;
+        msrc = (R)((double)at4(PB, q).x * tsc_ms(*L.tsc, n, layer_temp(L, t_src, gi, gj), (double)mn.w));
+      }
+    }
+    outr[(rr * 3 + 0) * rs + i] = msrc * mn.x;
+    outr[(rr * 3 + 1) * rs + i] = msrc * mn.y;
+    outr[(rr * 3 + 2) * rs + i] = msrc * mn.z;
 
     if constexpr (stats) {
       const V4<double> pv = L.pv[n];  // {vol, ms_scale, ms, 1}; (0, .., 0) on the extra cells of a grain
-      const double v = pv.x, w = pv.z * pv.y * v;
+      const double msc = (GEN == 2 && L.tsc) ? sc_ms : pv.y;  // ms_scale of this evaluation
+      const double v = pv.x, w = pv.z * msc * v;
       const double mx = mn.x, my = mn.y, mz = mn.z;
       rec[kSlotV] += v;
       rec[kSlotM + 0] += v * mx;
@@ -1545,7 +1651,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       rec[kSlotMaxTq] = fmax(rec[kSlotMaxTq], (double)tq2 / (pv.z * pv.z));
       rec[kSlotMaxD2] = fmax(rec[kSlotMaxD2], d2x >= 0.0 ? d2x : (double)(dx * dx + dy * dy + dz * dz));
       // mmag1: |m| ms_scale vol (push_llg, llg.f90:1152), |m| vol (push_llb, :1062)
-      rec[kSlotMmag] += llb ? (double)mn.w * v : sqrt(mx * mx + my * my + mz * mz) * pv.y * v;
+      rec[kSlotMmag] += llb ? (double)mn.w * v : sqrt(mx * mx + my * my + mz * mz) * msc * v;
       rec[kSlotVA] += v;  // volume of the grains pushed (do_grain)
       // energy at the evaluated state (field.f90:200, :360, :374, :339)
       const double e_d = -((double)mf.x * ((double)hdx + apx) + (double)mf.y * ((double)hdy + apy) +

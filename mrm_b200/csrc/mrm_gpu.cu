@@ -81,6 +81,16 @@ struct LayerBufs {
   // temperature profile (null tprof: the uniform temperature): device TempDev and its host copy
   void* tprof = nullptr;
   TempDev tp{};
+  // temperature scaling (null tsc: off): device TscDev, the cells' Tc, the
+  // concatenated tables; host copies of the settings and reduced tables
+  // (Ms, alpha, Hk, Hx)
+  void* tsc = nullptr;
+  void* tsc_tc = nullptr;
+  void* tsc_tab = nullptr;
+  bool tsc_on = false;
+  double tsc_msexp = -1.0, tsc_hkexp = -1.0;
+  int tsc_mag = 0;
+  std::vector<double> tsc_t[4], tsc_v[4];
 };
 
 struct Engine;
@@ -568,6 +578,7 @@ RunDev<R> make_desc(const mrm_gpu* r) {
     o.tab = static_cast<const TabDev*>(b.tab);
     o.llb = static_cast<const LlbDev*>(b.llb);
     o.tprof = static_cast<const TempDev*>(b.tprof);
+    o.tsc = static_cast<const TscDev*>(b.tsc);
   }
   return d;
 }
@@ -724,7 +735,7 @@ int build_tables(Engine* e) {
       e->has_head = e->has_head || r->L[l].func == kFuncHead || r->L[l].tab != nullptr;
       e->has_cubic = e->has_cubic || r->L[l].cax != nullptr;
       e->has_llb = e->has_llb || r->L[l].llb != nullptr;
-      e->has_tprof = e->has_tprof || r->L[l].tprof != nullptr;
+      e->has_tprof = e->has_tprof || r->L[l].tprof != nullptr || r->L[l].tsc != nullptr;
       e->mapped = e->mapped || r->L[l].cgrain != nullptr;
     }
   if (e->mapped && karlqvist_head)
@@ -1365,6 +1376,7 @@ void run_free(mrm_gpu* r) {
     dfree(b.cgrain); dfree(b.gci); dfree(b.gcs); dfree(b.hdm); dfree(b.hapm);
     dfree(b.tab); dfree(b.tb_v); dfree(b.tb_pos);
     dfree(b.llb); dfree(b.llbp); dfree(b.tprof);
+    dfree(b.tsc); dfree(b.tsc_tc); dfree(b.tsc_tab);
   }
 }
 
@@ -2398,6 +2410,155 @@ int mrm_gpu_set_temp_profile(mrm_gpu* h, int layer, double background, double dt
   return push_temp_profile(h, b);
 }
 
+// file_temp_scaling's reduction of a table as read (temp_scaling.f90:152-203):
+// ordered by temperature (ties keep their order), equal temperatures merged
+// pairwise from the top into the mean of their scales, an equal first pair
+// and an equal last pair of scales trimmed, and temperatures whose largest
+// exceeds 5 (a table in K) divided by it
+static void reduce_scaling_table(int n, const double* temp, const double* scaling, std::vector<double>& t_out,
+                                 std::vector<double>& v_out) {
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return temp[a] < temp[b]; });
+  std::vector<double> t(n), v(n);
+  for (int i = 0; i < n; ++i) {
+    t[i] = temp[ord[i]];
+    v[i] = scaling[ord[i]];
+  }
+  int merged = 0;
+  for (int i = n - 1; i >= 1; --i) {
+    if (t[i - 1] != t[i]) continue;
+    ++merged;
+    v[i - 1] = 0.5 * (v[i - 1] + v[i]);
+    for (int j = i + 1; j < n; ++j) {  // the entries above move down one place (to the table's end)
+      t[j - 1] = t[j];
+      v[j - 1] = v[j];
+    }
+  }
+  int m = std::max(1, n - merged);
+  if (m >= 2 && v[0] == v[1]) {
+    t.erase(t.begin());
+    v.erase(v.begin());
+    --m;
+  }
+  if (m > 1 && v[m - 2] == v[m - 1]) --m;
+  if (t[m - 1] > 5.0) {
+    const double top = t[m - 1];
+    for (int i = 0; i < m; ++i) t[i] /= top;
+  }
+  t_out.assign(t.begin(), t.begin() + m);
+  v_out.assign(v.begin(), v.begin() + m);
+}
+
+static int push_temp_scaling(mrm_gpu* h, LayerBufs& b) {
+  std::string* errp = &h->err;
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaStreamSynchronize(h->eng->st));
+  dfree(b.tsc);
+  dfree(b.tsc_tab);
+  h->eng->desc_dirty = true;
+  h->eng->tables_dirty = true;  // the level-2 kernels
+  if (!b.tsc_on) {
+    dfree(b.tsc_tc);
+    return MRM_OK;
+  }
+  TscDev d{};
+  // the tables of Ms, alpha and Hk (Hx's scales nothing in the reference)
+  std::vector<double> tt, tv;
+  for (int k = 0; k < 3; ++k) {
+    d.off[k] = (int)tt.size();
+    d.nt[k] = (int)b.tsc_t[k].size();
+    tt.insert(tt.end(), b.tsc_t[k].begin(), b.tsc_t[k].end());
+    tv.insert(tv.end(), b.tsc_v[k].begin(), b.tsc_v[k].end());
+  }
+  const size_t nt = std::max<size_t>(tt.size(), 1);
+  int rc = dmalloc(errp, &b.tsc_tab, sizeof(double) * 2 * nt);
+  if (!rc) rc = dmalloc(errp, &b.tsc, sizeof(TscDev));
+  if (rc) return rc;
+  double* tab_d = static_cast<double*>(b.tsc_tab);
+  if (!tt.empty()) {
+    CK(h2d(tab_d, tt.data(), sizeof(double) * tt.size()));
+    CK(h2d(tab_d + nt, tv.data(), sizeof(double) * tv.size()));
+  }
+  d.tc = static_cast<const double*>(b.tsc_tc);
+  d.tt = tab_d;
+  d.tv = tab_d + nt;
+  d.msexp = b.tsc_msexp;
+  d.hkexp = b.tsc_hkexp;
+  d.floor_ms = b.floor_ms;
+  d.mag = b.tsc_mag;
+  CK(h2d(b.tsc, &d, sizeof(TscDev)));
+  return MRM_OK;
+}
+
+int mrm_gpu_set_temp_scaling(mrm_gpu* h, int layer, const double* tc, double msexp, double hkexp, int use_mag) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  std::string* errp = &h->err;
+  LayerBufs& b = h->L[layer];
+  if (!tc) {
+    b.tsc_on = false;
+    return push_temp_scaling(h, b);
+  }
+  if (!b.uploaded) return set_err(errp, MRM_ERR_STATE, "upload layer %d first", layer);
+  const HostLayerCache& hc = host_cache()[h][layer];
+  if (!hc.cgrain.empty()) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs one grain per cell");
+  if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling with a moving demag window");
+  // the neighbours' ms_scale enters every exchange term: the lattice and columnar forms carry it per stage
+  if (b.xidx && !b.xst) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs the lattice form of the exchange");
+  if ((b.uidx && !b.ucol) || (b.lidx && !b.lcol) || (layer > 0 && h->L[layer - 1].lidx && !h->L[layer - 1].lcol) ||
+      (layer + 1 < h->nl && h->L[layer + 1].uidx && !h->L[layer + 1].ucol))
+    return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs columnar interlayer couplings");
+  for (int g = 0; g < b.ng; ++g) {
+    if (hc.ms_scale[g] != 1.0 || hc.hk_scale[g] != 1.0 || hc.alpha_scale[g] != 1.0)
+      return set_err(errp, MRM_ERR_STATE, "layer %d: temperature scaling replaces the scales; upload them as 1", layer);
+    if (!(tc[g] > 0)) return set_err(errp, MRM_ERR_ARG, "temperature scaling needs Tc > 0 (grain %d)", g);
+  }
+  CK(cudaSetDevice(h->eng->dev));
+  CK(cudaStreamSynchronize(h->eng->st));
+  dfree(b.tsc_tc);
+  int rc = dmalloc(errp, &b.tsc_tc, sizeof(double) * (size_t)b.ng);
+  if (rc) return rc;
+  CK(h2d(b.tsc_tc, tc, sizeof(double) * (size_t)b.ng));
+  b.tsc_on = true;
+  b.tsc_msexp = msexp;
+  b.tsc_hkexp = hkexp;
+  b.tsc_mag = use_mag ? 1 : 0;
+  return push_temp_scaling(h, b);
+}
+
+int mrm_gpu_set_temp_scaling_table(mrm_gpu* h, int layer, int which, int n, const double* temp,
+                                   const double* scaling) {
+  if (!h) return MRM_ERR_ARG;
+  if (layer < 0 || layer >= h->nl) return set_err(&h->err, MRM_ERR_ARG, "layer %d out of range", layer);
+  if (which < 1 || which > 4) return set_err(&h->err, MRM_ERR_ARG, "table %d: 1 Ms, 2 alpha, 3 Hk, 4 Hx", which);
+  if (n < 0 || (n > 0 && (!temp || !scaling))) return MRM_ERR_ARG;
+  LayerBufs& b = h->L[layer];
+  if (n == 0) {
+    b.tsc_t[which - 1].clear();
+    b.tsc_v[which - 1].clear();
+  } else {
+    reduce_scaling_table(n, temp, scaling, b.tsc_t[which - 1], b.tsc_v[which - 1]);
+  }
+  return b.tsc_on ? push_temp_scaling(h, b) : MRM_OK;
+}
+
+int mrm_gpu_get_temp_scaling_table(const mrm_gpu* h, int layer, int which, int* n, double* temp, double* scaling) {
+  if (!h || !n || layer < 0 || layer >= h->nl || which < 1 || which > 4) return MRM_ERR_ARG;
+  const LayerBufs& b = h->L[layer];
+  const int m = (int)b.tsc_t[which - 1].size();
+  if (*n < m) {
+    *n = m;
+    return MRM_ERR_ARG;
+  }
+  for (int i = 0; i < m; ++i) {
+    if (temp) temp[i] = b.tsc_t[which - 1][i];
+    if (scaling) scaling[i] = b.tsc_v[which - 1][i];
+  }
+  *n = m;
+  return MRM_OK;
+}
+
 int mrm_gpu_set_temp_function(mrm_gpu* h, int layer, int func, double t_start, double t_end, double s_start,
                               double s_end, double amp, double gamma, double phase, double param, double duty,
                               double moddepth, double dc, double scale) {
@@ -3275,7 +3436,8 @@ struct NoAllocDev {
 NoAllocDev g_noalloc_dev[kNoAllocMaxDev];
 std::mutex g_noalloc_mu;
 
-static_assert(sizeof(RunDev<float>) <= 4000, "run descriptor must fit in a kernel parameter block");
+// (kernel parameter blocks hold up to 32,764 bytes from CUDA 12.1 on sm_70 and later)
+static_assert(sizeof(RunDev<float>) <= 32000, "run descriptor must fit in a kernel parameter block");
 
 struct NoAllocLayout {
   size_t desc = 0, rtask = 0, ctask = 0, m = 0, hd = 0, hf = 0, specx = 0, spech = 0, total = 0;

@@ -79,6 +79,8 @@ class _RunMixin:
                 self.set_zhang(l, **lay.zhang)
             if getattr(lay, "temp_profile", None):
                 self.set_temp_profile(l, **lay.temp_profile)
+            if getattr(lay, "temp_scaling", None):
+                self.set_temp_scaling(l, **lay.temp_scaling)
             if getattr(lay, "cubic_axis", None) is not None:
                 self.set_cubic_axes(l, lay.cubic_axis)
             self.set_thermal(l, lay.thermal, lay.temperature, thermal_seed)
@@ -193,6 +195,32 @@ class _RunMixin:
                 float(tf.get("gamma", 0.0)), float(tf.get("phase", 0.0)), float(tf.get("param", 0.0)),
                 float(tf.get("duty", 0.0)), float(tf.get("moddepth", 0.0)), float(tf.get("dc", 0.0)),
                 float(tf.get("scale", 1.0))))
+
+    def set_temp_scaling(self, layer, tc, msexp=-1.0, hkexp=-1.0, use_mag=False, tables=None):
+        """Temperature scaling of Ms, alpha and Hk on `layer` (include/mrm_gpu.h
+        mrm_gpu_set_temp_scaling): per-grain Curie temperature `tc` (K), power-law
+        exponents (negative: none), Ms from |m| (`use_mag`), and `tables`
+        {which: (temperatures, scales)} with which 1 Ms, 2 alpha, 3 Hk, 4 Hx (as
+        read; reduced by the library).  tc None turns it off."""
+        L = _lib.load()
+        if tc is None:
+            self._check(L.mrm_gpu_set_temp_scaling(self.h, layer, None, 0.0, 0.0, 0))
+            return
+        t = f64(tc)
+        for which, (temps, scales) in (tables or {}).items():
+            tt, vv = f64(temps), f64(scales)
+            self._check(L.mrm_gpu_set_temp_scaling_table(self.h, layer, int(which), len(tt), fptr(tt), fptr(vv)))
+        self._check(L.mrm_gpu_set_temp_scaling(self.h, layer, fptr(t), float(msexp), float(hkexp),
+                                               1 if use_mag else 0))
+
+    def get_temp_scaling_table(self, layer, which):
+        """The reduced scaling table `which`: (T/Tc, scale)."""
+        L = _lib.load()
+        n = C.c_int(0)
+        L.mrm_gpu_get_temp_scaling_table(self.h, layer, int(which), C.byref(n), None, None)
+        tt, vv = np.zeros(max(n.value, 1)), np.zeros(max(n.value, 1))
+        self._check(L.mrm_gpu_get_temp_scaling_table(self.h, layer, int(which), C.byref(n), fptr(tt), fptr(vv)))
+        return tt[:n.value].copy(), vv[:n.value].copy()
 
     def set_zhang(self, layer, spin, lambda_ms, meq_bs=False, garanin_tau=False):
         """Zhang integrator on `layer` (include/mrm_gpu.h mrm_gpu_set_zhang)."""

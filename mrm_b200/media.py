@@ -96,6 +96,10 @@ class Layer:
     temp_profile: Optional[dict] = None
     # Zhang integrator (llgp%zhang): dict(spin, lambda_ms, meq_bs, garanin_tau)
     zhang: Optional[dict] = None
+    # temperature scaling of Ms, alpha, Hk: dict of GpuSim.set_temp_scaling's
+    # arguments (tc, msexp, hkexp, use_mag, tables) (include/mrm_gpu.h
+    # mrm_gpu_set_temp_scaling); the layer's scales are then uploaded as 1
+    temp_scaling: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -451,7 +455,8 @@ def llb_medium(side: int = 32, *, temperature: float = 600.0, tc: float = 700.0,
     (S + 1)) (the mean-field Tc of push_llb's Langevin form, lambda_m =
     lambdaMs (S+1)/S, is (g mu_B/k_B) S lambda_m / 3), under a constant
     reversing field of h_oe along the medium's field direction; the anisotropy
-    and Ms scales stay the inputs (Tc-free scaling)."""
+    and Ms scales stay the inputs (no temperature scaling unless the layer's
+    temp_scaling is set)."""
     med = mh_medium(side, seed=seed, boundary=boundary, temperature=temperature)
     rng = np.random.default_rng(seed + 1000)
     for lay in med.layers:

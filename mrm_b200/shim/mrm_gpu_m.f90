@@ -13,7 +13,10 @@ module mrm_gpu_m
   private
   public :: mrm_geom_t, mrm_stats_t, gpu_create, gpu_destroy, gpu_upload_layer, &
             gpu_upload_interlayer, gpu_build_tensor, gpu_upload_tensor, gpu_set_uniform_field, &
-            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_zhang, gpu_set_temp_profile, gpu_set_temp_function, gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
+            gpu_set_field_function, gpu_set_head_field, gpu_set_cubic_axes, gpu_step_adaptive, gpu_off_field, &
+            gpu_set_window, gpu_set_field_table, gpu_set_llb, gpu_set_mt, gpu_set_zhang, &
+            gpu_set_temp_profile, gpu_set_temp_function, gpu_set_temp_scaling, gpu_set_temp_scaling_table, &
+            gpu_set_mag, gpu_get_mag, gpu_set_thermal, gpu_set_state, gpu_get_state, &
             gpu_get_field, &
             gpu_set_time, gpu_step, gpu_last_error, gpu_push_m
 
@@ -130,6 +133,21 @@ module mrm_gpu_m
       integer(C_INT), value :: layer, meq_bs, garanin_tau
       real(C_DOUBLE), value :: spin
       real(C_DOUBLE), intent(in) :: lambda_ms(*)
+    end function
+    integer(C_INT) function c_set_temp_scaling(h, layer, tc, msexp, hkexp, use_mag) &
+        bind(C, name="mrm_gpu_set_temp_scaling")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, use_mag
+      real(C_DOUBLE), intent(in) :: tc(*)
+      real(C_DOUBLE), value :: msexp, hkexp
+    end function
+    integer(C_INT) function c_set_temp_scaling_table(h, layer, which, n, temp, scaling) &
+        bind(C, name="mrm_gpu_set_temp_scaling_table")
+      import :: C_INT, C_PTR, C_DOUBLE
+      type(C_PTR), value :: h
+      integer(C_INT), value :: layer, which, n
+      real(C_DOUBLE), intent(in) :: temp(*), scaling(*)
     end function
     integer(C_INT) function c_set_temp_profile(h, layer, bg, dtemp, sx, sy, expn, vx, vy, ox, oy, rx, ry, t0) &
         bind(C, name="mrm_gpu_set_temp_profile")
@@ -372,6 +390,25 @@ contains
     real(C_DOUBLE), intent(in) :: background, dtemp, sigma(2), vel(2), offset(2), ref(2), t_origin
     ok_p = ok(c_set_temp_profile(h, int(layer - 1, C_INT), background, dtemp, sigma(1), sigma(2), int(expn, C_INT), &
                                  vel(1), vel(2), offset(1), offset(2), ref(1), ref(2), t_origin))
+  end function
+  ! temp_scaling(layer)%p (include/mrm_gpu.h mrm_gpu_set_temp_scaling): field(layer)%tc,
+  ! %msexp, %hkexp, %use_mag_p; called where init_temp_scaling runs (grain.f90:54),
+  ! after the layer's uploads with its unit scales
+  logical function gpu_set_temp_scaling(h, layer, tc, msexp, hkexp, use_mag_p) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer
+    real(C_DOUBLE), intent(in) :: tc(:), msexp, hkexp
+    logical, intent(in) :: use_mag_p
+    ok_p = ok(c_set_temp_scaling(h, int(layer - 1, C_INT), tc, msexp, hkexp, merge(1_C_INT, 0_C_INT, use_mag_p)))
+  end function
+  ! file_temp_scaling's table indx (1 Ms, 2 alpha, 3 Hk, 4 Hx) as read: the
+  ! (temperature, scaling) pairs before the reduction, which the library applies
+  logical function gpu_set_temp_scaling_table(h, layer, indx, temp, scaling) result(ok_p)
+    type(C_PTR), intent(in) :: h
+    integer, intent(in) :: layer, indx
+    real(C_DOUBLE), intent(in) :: temp(:), scaling(:)
+    ok_p = ok(c_set_temp_scaling_table(h, int(layer - 1, C_INT), int(indx, C_INT), int(size(temp), C_INT), &
+                                       temp, scaling))
   end function
   ! set_temp's time scale of that profile (include/mrm_gpu.h mrm_gpu_set_temp_function)
   logical function gpu_set_temp_function(h, layer, func, t_start, t_end, s_start, s_end, amp, gamma, phase, param, &

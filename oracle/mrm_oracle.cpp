@@ -604,6 +604,16 @@ struct Layer {
   double tp_t_start = -1e22, tp_t_end = 1e22, tp_s_start = 1, tp_s_end = 1, tp_scale = 1, tp_amp = 0, tp_fgamma = 0,
          tp_phase = 0, tp_param = 0, tp_duty = 0, tp_moddepth = 0, tp_dc = 0;
   std::vector<double> temp;
+  // temperature scaling (temp_scaling_s, temp_scaling.f90:21-26; applied by
+  // find_temp_scaling :365-430 at every field evaluation): the grains' Tc
+  // (field%tc), power laws (1 - T/Tc)^e for Ms and Hk (negative: none), Ms
+  // from |m| (use_mag_p), and the reduced tables T/Tc -> scale of Ms, alpha,
+  // Hk and Hx (Hx's scale is computed but, as in the reference, used nowhere)
+  bool tsc = false;
+  std::vector<double> tsc_tc;
+  double tsc_msexp = -1.0, tsc_hkexp = -1.0;
+  bool tsc_mag = false;
+  std::vector<double> tsc_t[4], tsc_v[4];
   std::vector<double> m[2], dm, h, hthm, hdemag, happ;
   // schedule: uniform field x linear ramp (applied.f90:863-883)
   double hdir[3] = {0, 0, 0};
@@ -920,14 +930,104 @@ static void grain_temps(const Sim* s, Layer& Ly, double t) {
   }
 }
 
+// file_temp_scaling's reduction of a table as read (temp_scaling.f90:152-203):
+// sorted by temperature (ties keep their order), equal temperatures merged
+// pairwise from the top with the mean of their scales, an equal first pair of
+// scales and an equal last pair trimmed, and the temperatures divided by the
+// largest when it exceeds 5 (a table in K, normalised to T/Tc)
+void reduce_scaling_table(int n, const double* t_in, const double* v_in, std::vector<double>& t_out,
+                          std::vector<double>& v_out) {
+  std::vector<std::pair<double, double>> d(n);
+  for (int i = 0; i < n; ++i) d[i] = {t_in[i], v_in[i]};
+  std::stable_sort(d.begin(), d.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<double> t(n), v(n);
+  for (int i = 0; i < n; ++i) {
+    t[i] = d[i].first;
+    v[i] = d[i].second;
+  }
+  int k = 0;
+  for (int i = n - 1; i >= 1; --i)  // 1-based i = n .. 2
+    if (t[i - 1] == t[i]) {
+      ++k;
+      v[i - 1] = 0.5 * (v[i - 1] + v[i]);
+      for (int j = i + 1; j < n; ++j) {  // 1-based j = i+1 .. n: entry j moves to j-1
+        t[j - 1] = t[j];
+        v[j - 1] = v[j];
+      }
+    }
+  int m = std::max(1, n - k);
+  if (m >= 2 && v[0] == v[1]) {
+    for (int i = 1; i < m; ++i) {
+      t[i - 1] = t[i];
+      v[i - 1] = v[i];
+    }
+    --m;
+  }
+  if (m > 1 && v[m - 2] == v[m - 1]) --m;
+  if (t[m - 1] > 5.0) {
+    const double top = t[m - 1];
+    for (int i = 0; i < m; ++i) t[i] /= top;
+  }
+  t_out.assign(t.begin(), t.begin() + m);
+  v_out.assign(v.begin(), v.begin() + m);
+}
+
+// a scaling table at x = T/Tc: its first scale below the first node, its last
+// above the last, linear in between (bisection, temp_scaling.f90:397-414)
+static double table_scale(const std::vector<double>& tt, const std::vector<double>& vv, double x) {
+  const int n = (int)tt.size();
+  int k1 = 0, k2 = n - 1;
+  double y;
+  if (x <= tt[0]) {
+    y = 0.0;
+  } else if (x >= tt[k2]) {
+    y = 0.0;
+    k1 = k2;
+  } else {
+    while (k2 - k1 > 1) {
+      const int k = (k2 + k1 + 2) / 2 - 1;  // the reference's (k2 + k1) / 2 on 1-based indices
+      if (x < tt[k]) k2 = k;
+      else k1 = k;
+    }
+    y = std::max(0.0, std::min(1.0, (x - tt[k1]) / (tt[k2] - tt[k1])));
+  }
+  return vv[k1] + y * (vv[k2] - vv[k1]);
+}
+
+// find_temp_scaling (temp_scaling.f90:365-430): the grains' ms_scale,
+// alpha_scale and hk_scale from their temperature (the last grain_temps) and
+// Tc, or ms_scale from |m| of buffer buf; tables with one node scale nothing
+static void find_temp_scaling(Layer& Ly, int buf) {
+  if (!Ly.tsc) return;
+  std::vector<double>* val[3] = {&Ly.ms_scale, &Ly.alpha_scale, &Ly.hk_scale};
+  for (int i = 0; i < 3; ++i) {
+    std::vector<double>& v = *val[i];
+    if (i == 0 && Ly.tsc_mag) {
+      for (int n = 0; n < Ly.N; ++n) v[n] = std::min(1.0, std::max(0.0, std::abs(Ly.mag[buf][n])));
+    } else if ((i == 0 && Ly.tsc_msexp >= 0.0) || (i == 2 && Ly.tsc_hkexp >= 0.0)) {
+      const double e = i == 0 ? Ly.tsc_msexp : Ly.tsc_hkexp;
+      for (int n = 0; n < Ly.N; ++n)
+        v[n] = std::pow(std::min(1.0, std::max(0.0, 1.0 - Ly.temp[n] / Ly.tsc_tc[n])), e);
+    } else if (Ly.tsc_t[i].size() > 1) {
+      for (int n = 0; n < Ly.N; ++n)
+        if (Ly.do_grain[n]) v[n] = table_scale(Ly.tsc_t[i], Ly.tsc_v[i], Ly.temp[n] / Ly.tsc_tc[n]);
+    }
+  }
+}
+
 // get_field (field.f90:160-273) for the LLG path; energy per grain summed into *energy
 static void get_field(Sim* s, double t, int buf, double* energy) {
+  // get_applied first (field.f90:183): the grains' temperatures and their
+  // scaling, which the demag source already uses
+  for (int l = 0; l < s->nl; ++l) {
+    grain_temps(s, s->L[l], t);
+    find_temp_scaling(s->L[l], buf);
+  }
   compute_demag(s, buf);
   double e_tot = 0.0;
   for (int l = 0; l < s->nl; ++l) {
     Layer& Ly = s->L[l];
     double sc = Ly.head ? 0.0 : ramp_scale(Ly, t);
-    grain_temps(s, Ly, t);
     std::vector<double> hat;
     if (Ly.tab) table_field(s, Ly, t, sc, hat);
     const double* m = Ly.m[buf].data();
@@ -1025,7 +1125,9 @@ static void get_field(Sim* s, double t, int buf, double* energy) {
   if (energy) *energy = e_tot;
 }
 
-// get_thermal (field.f90:397-436), LLG branch (mag == 1, ms_scale > 0)
+// get_thermal (field.f90:397-436).  The LLB and MT runs draw it with no_ms_p
+// (get_fields, llg.f90:363-365: llgp%llb or llgp%mt), the others through the
+// |m| and ms_scale branches.
 static void get_thermal(Sim* s) {
   const double kB = 1.380662e-16;
   for (int l = 0; l < s->nl; ++l) {
@@ -1039,7 +1141,9 @@ static void get_thermal(Sim* s) {
       if (!Ly.do_grain[n]) continue;
       double x = 0.0;
       const double Tn = Ly.temp.empty() ? Ly.temperature : Ly.temp[n];  // field(i)%temp(n)
-      if (Ly.mag[s->in][n] != 1.0)  // field.f90:416-417
+      if (Ly.llb && Ly.mode != 2)  // no_ms_p (field.f90:414-415)
+        x = Ly.alpha_scale[n] * Tn / (Ly.ms[n] * Ly.vol[n]);
+      else if (Ly.mag[s->in][n] != 1.0)  // field.f90:416-417
         x = Ly.alpha_scale[n] * Tn / (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, std::abs(Ly.mag[s->in][n])));
       else if (Ly.ms_scale[n] > 0.0)
         x = Ly.alpha_scale[n] * Tn / (Ly.ms[n] * Ly.vol[n] * std::max(Ly.floor_ms, Ly.ms_scale[n]));
@@ -2349,6 +2453,61 @@ int orc_set_mt(void* h, int l, double spin, const double* lam_ms, int meq_bs, in
 }
 
 // LLB on layer l (mrm_gpu_set_llb's arguments; tc NULL: off)
+// set_temp_scaling (temp_scaling.f90:37-50) with the grains' Tc: msexp / hkexp
+// < 0 leave those power laws off; tc null switches the scaling off
+int orc_set_temp_scaling(void* h, int l, const double* tc, double msexp, double hkexp, int use_mag) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  Layer& Ly = s->L[l];
+  Ly.tsc = tc != nullptr;
+  if (!tc) return 0;
+  Ly.tsc_tc.assign(tc, tc + Ly.N);
+  Ly.tsc_msexp = msexp;
+  Ly.tsc_hkexp = hkexp;
+  Ly.tsc_mag = use_mag != 0;
+  return 0;
+}
+
+// file_temp_scaling's table which (1 Ms, 2 alpha, 3 Hk, 4 Hx) as read; n = 0 removes it
+int orc_set_temp_scaling_table(void* h, int l, int which, int n, const double* temp, const double* scaling) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl || which < 1 || which > 4 || n < 0) return 1;
+  Layer& Ly = s->L[l];
+  if (n == 0) {
+    Ly.tsc_t[which - 1].clear();
+    Ly.tsc_v[which - 1].clear();
+    return 0;
+  }
+  reduce_scaling_table(n, temp, scaling, Ly.tsc_t[which - 1], Ly.tsc_v[which - 1]);
+  return 0;
+}
+
+// the reduced table (for tests): *n on input the room, on output the nodes
+int orc_get_temp_scaling_table(void* h, int l, int which, int* n, double* temp, double* scaling) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl || which < 1 || which > 4) return 1;
+  const Layer& Ly = s->L[l];
+  const int m = (int)Ly.tsc_t[which - 1].size();
+  if (*n < m) return 2;
+  for (int i = 0; i < m; ++i) {
+    temp[i] = Ly.tsc_t[which - 1][i];
+    scaling[i] = Ly.tsc_v[which - 1][i];
+  }
+  *n = m;
+  return 0;
+}
+
+// the layer's scales after the last field evaluation (for tests): ms, alpha, hk per grain
+int orc_get_scales(void* h, int l, double* ms_scale, double* alpha_scale, double* hk_scale) {
+  Sim* s = static_cast<Sim*>(h);
+  if (l < 0 || l >= s->nl) return 1;
+  const Layer& Ly = s->L[l];
+  std::copy(Ly.ms_scale.begin(), Ly.ms_scale.end(), ms_scale);
+  std::copy(Ly.alpha_scale.begin(), Ly.alpha_scale.end(), alpha_scale);
+  std::copy(Ly.hk_scale.begin(), Ly.hk_scale.end(), hk_scale);
+  return 0;
+}
+
 int orc_set_llb(void* h, int l, double spin, const double* tc, const double* lam_ms) {
   Sim* s = static_cast<Sim*>(h);
   if (l < 0 || l >= s->nl) return 1;

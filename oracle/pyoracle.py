@@ -61,6 +61,10 @@ def lib():
         L.orc_set_mt.argtypes = [vp, i, d, P(d), i, i, i]
         L.orc_set_temp_profile.argtypes = [vp, i, d, d, d, d, i, d, d, d, d, d, d, d]
         L.orc_set_temp_function.argtypes = [vp, i, i] + [d] * 12
+        L.orc_set_temp_scaling.argtypes = [vp, i, P(d), d, d, i]
+        L.orc_set_temp_scaling_table.argtypes = [vp, i, i, i, P(d), P(d)]
+        L.orc_get_temp_scaling_table.argtypes = [vp, i, i, P(i), P(d), P(d)]
+        L.orc_get_scales.argtypes = [vp, i, P(d), P(d), P(d)]
         L.orc_get_temp.argtypes = [vp, i, P(d)]
         L.orc_set_mag.argtypes = [vp, i, P(d)]
         L.orc_get_mag.argtypes = [vp, i, P(d)]
@@ -272,6 +276,9 @@ class OracleSim:
             tp = getattr(lay, "temp_profile", None)
             if tp:
                 self.set_temp_profile(l, **tp)
+            ts = getattr(lay, "temp_scaling", None)
+            if ts:
+                self.set_temp_scaling(l, **ts)
             L.orc_set_thermal(self.h, l, 1 if lay.thermal else 0, lay.temperature, rng_mode, seed)
             cub = getattr(lay, "cubic_axis", None)
             if cub is not None:
@@ -364,6 +371,32 @@ class OracleSim:
         if time:
             a = _temp_function_args(time)
             assert lib().orc_set_temp_function(self.h, layer, *a) == 0
+
+    def set_temp_scaling(self, layer, tc, msexp=-1.0, hkexp=-1.0, use_mag=False, tables=None):
+        """Temperature scaling (GpuSim.set_temp_scaling's arguments; tc None: off)."""
+        if tc is None:
+            assert lib().orc_set_temp_scaling(self.h, layer, None, 0.0, 0.0, 0) == 0
+            return
+        t = f64(tc)
+        self._keep.append(t)
+        assert lib().orc_set_temp_scaling(self.h, layer, _p(t), float(msexp), float(hkexp), int(bool(use_mag))) == 0
+        for which, (temps, scales) in (tables or {}).items():
+            tt, vv = f64(temps), f64(scales)
+            assert lib().orc_set_temp_scaling_table(self.h, layer, int(which), len(tt), _p(tt), _p(vv)) == 0
+
+    def get_temp_scaling_table(self, layer, which):
+        """The reduced scaling table `which` (1 Ms, 2 alpha, 3 Hk, 4 Hx): (T/Tc, scale)."""
+        n = C.c_int(4096)
+        tt, vv = np.zeros(4096), np.zeros(4096)
+        assert lib().orc_get_temp_scaling_table(self.h, layer, int(which), C.byref(n), _p(tt), _p(vv)) == 0
+        return tt[:n.value].copy(), vv[:n.value].copy()
+
+    def get_scales(self, layer):
+        """ms_scale, alpha_scale, hk_scale per grain after the last field evaluation."""
+        N = self.medium.layers[layer].N
+        a, b, c = np.zeros(N), np.zeros(N), np.zeros(N)
+        assert lib().orc_get_scales(self.h, layer, _p(a), _p(b), _p(c)) == 0
+        return a, b, c
 
     def get_temp(self, layer):
         """Grain temperatures of the last field evaluation."""

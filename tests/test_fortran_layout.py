@@ -87,3 +87,17 @@ def test_bind_c_types_match_header(tmp_path):
             assert c[(ct, name)] == (off, nbytes), (ct, name, c[(ct, name)], (off, nbytes))
         assert c[(ct, "sizeof")] == size, (ct, c[(ct, "sizeof")], size)
         assert len(lay) == sum(1 for k in c if k[0] == ct and k[1] != "sizeof")
+
+
+def test_shim_source_form_and_bound_names():
+    """Free-form Fortran lines are at most 132 characters, and every bind(C)
+    name of the shim is a function the C header declares."""
+    import re
+    src = open(SHIM).read()
+    for k, line in enumerate(src.splitlines(), 1):
+        assert len(line) <= 132, f"line {k} has {len(line)} characters"
+    header = open(os.path.join(ROOT, "include", "mrm_gpu.h")).read()
+    bound = re.findall(r'bind\(C,\s*name="(\w+)"\)', src)
+    assert bound
+    for name in bound:
+        assert re.search(r"\b" + name + r"\s*\(", header), name
