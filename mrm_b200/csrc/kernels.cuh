@@ -1083,6 +1083,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       if (sp.xst >= 0) copy(&bars[0], stg + sp.xst, L.xst + base, base * v4b, nlay * v4b, nrows * v4row, 130);
       if (sp.ucol >= 0) copy(&bars[0], stg + sp.ucol, L.ucol + base, base * rb, nlay * rb, nrows * rrow, 140);
       if (sp.lcol >= 0) copy(&bars[0], stg + sp.lcol, L.lcol + base, base * rb, nlay * rb, nrows * rrow, 150);
+    } else if (!win && v4row % 16 == 0) {
+      // rows read at use: their parameter rows start for L2 now, and arrive
+      // while the inverse row transforms run
+      bulk_prefetch_l2(L.pb + base, (uint32_t)(nrows * v4row));
+      if (STAGE != kInit) {
+        bulk_prefetch_l2(L.pa + base, (uint32_t)(nrows * v4row));
+        if (stencil) bulk_prefetch_l2(L.xst + base, (uint32_t)(nrows * v4row));
+      }
     }
     mbar_arrive(&bars[0]);
   }
@@ -1100,6 +1108,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
              rd.phs * (int)cb, 200);
       }
     mbar_arrive(&bars[1]);
+    if (run_it && !staged && !win && v4row % 16 == 0) {
+      // the state rows of this stage (with the lattice neighbours' rows) for L2
+      bulk_prefetch_l2(mfield + base, (uint32_t)(nrows * v4row));
+      if (STAGE != kInit && stencil) {
+        const int jm = row0 == 0 ? ny - 1 : row0 - 1, jp = row0 + nrows == ny ? 0 : row0 + nrows;
+        bulk_prefetch_l2(mfield + (size_t)jm * nx, (uint32_t)v4row);
+        bulk_prefetch_l2(mfield + (size_t)jp * nx, (uint32_t)v4row);
+      }
+      if (STAGE == kCorr) {
+        bulk_prefetch_l2(L.m + base, (uint32_t)(nrows * v4row));
+        bulk_prefetch_l2(L.dm + base, (uint32_t)(nrows * v4row));
+        if (thermal) bulk_prefetch_l2(L.ht + base, (uint32_t)(nrows * v4row));
+      }
+    }
     if (run_it && staged) {
       if (sp.halo) {
         const int jm = row0 == 0 ? ny - 1 : row0 - 1, jp = row0 + nrows == ny ? 0 : row0 + nrows;

@@ -82,6 +82,12 @@ MRM_D bool mbar_wait(uint64_t* bar, uint32_t phase) {
   return false;
 }
 
+// bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned source) from
+// global memory into L2; nothing waits for it
+MRM_D void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // global -> shared bulk copy of `bytes` (multiple of 16) completing on `bar`
 MRM_D void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
