@@ -57,10 +57,12 @@ RAMP_STEPS = 20000  # 2 ns at 0.1 ps
 WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
             "512x512 zero-padded FFT demag, Heun 0.1 ps")
 
-# DRAM traffic per launch of each kernel in bytes per grain of the launch, for
-# the headline batch with its tuned shapes (ncu capture summarised in
-# profiles/batched_32x65536_launch_list.md)
-NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 140.6, "col": 70.2, "row_corr": 166.4}
+# DRAM traffic per launch of each kernel in bytes per grain of the launch:
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
+# headline batch (32 x 65,536 grains, row shape 1, the register column kernel
+# {128 threads, 4 blocks/SM}, one column per task), divided by its grains; a
+# kernel change calls for a new capture
+NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 140.3, "col": 29.8, "row_corr": 165.1}
 
 
 def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4, runs: int = 1,
@@ -695,7 +697,7 @@ def main():
                      "traffic": (NCU_TRAFFIC_BYTES_PER_GRAIN[dom] * nb * n
                                  if dom in NCU_TRAFFIC_BYTES_PER_GRAIN else None),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 32 x 65,536 "
-                                       "grains, row/column shapes 1/1, 2 columns per task",
+                                       "grains, row shape 1, register column kernel 128 x 4, 1 column per task",
                      "per_kernel_ms": per_kernel, "launches_per_heun_step": launches_per_heun,
                      "per_kernel_frac": {k: ab[k] / (v * 1e-3) / 1e9 / peak for k, v in per_kernel.items()},
                      "occupancy_blocks_per_sm": {"row": B["occupancy"][0], "col": B["occupancy"][1]},
