@@ -39,6 +39,21 @@ MRM_HD Cx<R> cscale(Cx<R> a, R s) { return {a.x * s, a.y * s}; }
 template <typename R>
 MRM_HD Cx<R> cmul_i(Cx<R> a, R s) { return {-s * a.y, s * a.x}; }
 
+// FP32 sums and differences on sm_100 as one paired add (FADD2: both lanes
+// rounded as two scalar adds would be), half the issue slots of the butterflies
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+template <>
+MRM_HD Cx<float> cadd<float>(Cx<float> a, Cx<float> b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return {r.x, r.y};
+}
+template <>
+MRM_HD Cx<float> csub<float>(Cx<float> a, Cx<float> b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(-b.x, -b.y));
+  return {r.x, r.y};
+}
+#endif
+
 // Tabulated (moving) field profile of a layer, in device memory: file_applied
 // + set + interpolate (applied.f90:711-813,1471-1520,1757-1776).  Values
 // v[c + 3 (i + nx j)] (Oe) at table nodes pos[i] (x), pos[nx + j] (y) (cm); the
