@@ -181,6 +181,7 @@ struct Engine {
   int part_cap = 0;
   StatsDev* d_stats = nullptr;
   StatsDev* h_stats = nullptr;  // pinned
+  int nslots = 0;               // runs in the current tables (stats slots 0 .. nslots-1)
   int stats_cap = 0;
   void* d_tw = nullptr;  // Cx<R>[tw_table_size()] (fft.cuh layout)
   bool tables_dirty = true;
@@ -798,6 +799,7 @@ int build_tables(Engine* e) {
   int rc = plan_smem<R>(e);
   if (rc) return rc;
   clear_graphs(e);
+  e->nslots = nr;
   e->tables_dirty = false;
   e->desc_dirty = true;
   return MRM_OK;
@@ -1343,8 +1345,7 @@ int run_alloc(mrm_gpu* r) {
   if (rc) return rc;
   rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
   if (rc) return rc;
-  rc = r->fft_big ? MRM_OK : tensor_alloc(r);
-  if (rc) return rc;
+  // (the tensor buffer comes with the first build or upload, or is shared)
   const size_t n = (size_t)r->g.nx * r->g.ny;
   for (int l = 0; l < r->nl; ++l) {
     LayerBufs& b = r->L[l];
@@ -2113,9 +2114,11 @@ int mrm_gpu_copy_tensor(mrm_gpu* dst, const mrm_gpu* src) {
   CK(cudaSetDevice(dst->eng->dev));
   // the same geometry has the same tensor: share the source's buffer (it is
   // only read from now on; a later build or upload on either run writes a
-  // buffer of its own)
+  // buffer of its own).  The source's tensor must be complete; the
+  // destination's own earlier buffer, if any, must be out of use before it
+  // is released (a fresh run has none, and nothing in flight reads it).
   CK(cudaStreamSynchronize(src->eng->st));
-  CK(cudaStreamSynchronize(dst->eng->st));
+  if (dst->tens_buf) CK(cudaStreamSynchronize(dst->eng->st));
   dst->tens_buf = src->tens_buf;
   dst->tens = src->tens;
   dst->tensor_ready = true;
@@ -3355,7 +3358,9 @@ int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats
   if (!b || (nruns > 0 && (!runs || !out))) return MRM_ERR_ARG;
   Engine* e = &b->eng;
   std::string* errp = &e->err;
-  const int nr = (int)e->runs.size();
+  // the slots of the tables the last steps ran with (runs added since then
+  // have none yet)
+  const int nr = e->nslots;
   if (!nr) return MRM_OK;
   CK(cudaSetDevice(e->dev));
   CK(cudaMemcpyAsync(e->h_stats, e->d_stats, sizeof(StatsDev) * nr, cudaMemcpyDeviceToHost, e->st));

@@ -8,7 +8,8 @@ start).  The server keeps one Batch resident on the GPU and loops:
    footprint (state, parameters, spectra, tensor) fits the HBM budget; a
    request's tensor spectrum is copied device-to-device from a per-geometry
    template instead of being rebuilt;
-3. advance every active run by K = chunk Heun steps in one launch sequence.
+3. advance every active run by K = chunk Heun steps in one launch sequence,
+   enqueued before step 2's admissions so that their host work overlaps it.
    A request of S steps is admitted with an aligned start: it idles through
    the first K - S mod K steps of its first call (mrm_batch_delay_run), so
    its budget ends on a call boundary and its reductions at the end of
@@ -17,8 +18,11 @@ start).  The server keeps one Batch resident on the GPU and loops:
 4. record each run's M(H) sample (time, applied field, m.h), retire finished
    runs (result + latency = finish - arrival) and free their memory.
 
-Requests that arrive while others are on the GPU are admitted as soon as
-memory frees up and join the next launch; a run's trajectory does not depend
+A request's medium (its grains, parameters and exchange lists, built on the
+host) is prepared by a worker thread as soon as the request arrives, while
+the GPU runs the current call (the launch releases the interpreter lock), so
+admission only uploads it.  Requests that arrive while others are on the
+GPU are admitted as soon as memory frees up and join the next launch; a run's trajectory does not depend
 on its neighbours (each run's kernels read only its own data), which the
 tests check bit for bit against the same request run alone.
 
@@ -31,6 +35,7 @@ runs continue unchanged.  Finished requests have status "done".
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import threading
 import time
 from typing import Callable, Dict, List, Optional
@@ -80,9 +85,9 @@ class Server:
     """Continuous-batching scheduler over a Batch-like backend.
 
     backend: object with add(medium, dt, steps, thermal_seed, tensor_from) ->
-    run, delay(run, idle_steps), remove(run), step(k), stats(runs),
-    footprint(medium) -> bytes, memory() -> (free, total); defaults to the
-    GPU Batch.
+    run, delay(run, idle_steps), remove(run), step(k) (or enqueue(k), which
+    returns at once), stats(runs) (waits for the call), footprint(medium) ->
+    bytes, memory() -> (free, total); defaults to the GPU Batch.
     """
 
     def __init__(self, backend=None, precision: int = _lib.FP32, device: int = 0,
@@ -110,6 +115,12 @@ class Server:
         boundary (queued or running); thread-safe."""
         with self._cancel_lock:
             self._cancelled.add(int(rid))
+
+    def _enqueue(self, k: int):
+        """Starts a call of k steps (the backend's asynchronous launch when it
+        has one; stats() then waits for it)."""
+        launch = getattr(self.be, "enqueue", None)
+        (launch or self.be.step)(k)
 
     def _take_cancelled(self) -> set:
         with self._cancel_lock:
@@ -156,10 +167,23 @@ class Server:
         results = []
         t0 = self.clock()
         calls = 0
+        # media of arrived requests, built on a worker thread (rid -> future)
+        prep = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        media = {}
+        try:
+            return self._loop(pending, queue, active, results, t0, calls, prep, media)
+        finally:
+            for f in media.values():
+                f.cancel()
+            prep.shutdown(wait=True)
+
+    def _loop(self, pending, queue, active, results, t0, calls, prep, media) -> dict:
         while pending or queue or active:
             now = self.clock() - t0
             while pending and pending[0].arrival <= now:
-                queue.append(pending.popleft())
+                q = pending.popleft()
+                queue.append(q)
+                media[q.rid] = prep.submit(q.medium)
             # cancellations and timeouts, at a call boundary: queued or running
             cancelled = self._take_cancelled()
             for rid in cancelled:
@@ -169,34 +193,41 @@ class Server:
             expired = lambda r: r.timeout is not None and now - r.arrival >= r.timeout  # noqa: E731
             for q in [q for q in queue if q.rid in cancelled or expired(q)]:
                 queue.remove(q)
+                media.pop(q.rid).cancel()
                 results.append(self._retire(None, q, "cancelled" if q.rid in cancelled else "timeout", now))
             for a in [a for a in active if a.req.rid in cancelled or expired(a.req)]:
                 active.remove(a)
                 results.append(self._retire(a, a.req, "cancelled" if a.req.rid in cancelled else "timeout", now))
+            # one launch sequence of the full chunk for the runs already on the
+            # device (every budget ends on a call boundary: aligned starts),
+            # enqueued before the admissions below, whose host work (uploads,
+            # the next requests' set-up) then overlaps it; runs admitted now
+            # join the next call
+            running = list(active)
+            k = self.chunk
+            if running:
+                self._enqueue(k)
+                calls += 1
             # admission, first come first served, by device footprint
             while queue and len(active) < self.max_active:
                 req = queue[0]
-                med = req.medium()
+                med = media[req.rid].result()
                 fp = self.be.footprint(med)
                 if active and self.used + fp > self.budget:
                     break
                 queue.popleft()
+                del media[req.rid]
                 a = self._admit(req, med, fp, self.clock() - t0)
                 self.used += a.fp
                 active.append(a)
-            if not active:
-                if pending:
+            if not running:
+                if not active and pending:
                     self.sleep(max(0.0, min(pending[0].arrival - (self.clock() - t0), 0.01)))
                 continue
-            # one launch sequence of the full chunk for every active run; every
-            # budget ends on a call boundary (aligned starts)
-            k = self.chunk
-            self.be.step(k)
-            calls += 1
-            st = self.be.stats([a.run for a in active])
+            st = self.be.stats([a.run for a in running])
             done_t = self.clock() - t0
             finished = []
-            for a, s in zip(active, st):
+            for a, s in zip(running, st):
                 a.remaining -= k
                 mh = float(np.asarray(s["mms_l"][0]) @ self.be.hdir(a.run))
                 a.samples.append((float(s["t"]), applied_field(a.req, float(s["t"])), mh,
@@ -258,6 +289,9 @@ class GpuBackend:
 
     def step(self, k: int):
         self.batch.step(k)
+
+    def enqueue(self, k: int):
+        self.batch.enqueue(k)
 
     def stats(self, runs):
         return self.batch.stats(runs)
