@@ -226,9 +226,8 @@ int mrm_gpu_set_temp_function(mrm_gpu* h, int layer, int func, double t_start, d
  * demag source, the exchange terms (the neighbours' ms_scale), anisotropy,
  * damping, the thermal variance and the reductions.  The layer must have been
  * uploaded with unit scales (the reference's, which only this scaling
- * changes), one grain per cell, no moving window, the lattice form of the
- * exchange and columnar interlayer couplings (MRM_ERR_UNSUPPORTED /
- * MRM_ERR_STATE otherwise).  tc NULL switches it off.  (No reference
+ * changes), with one grain per cell and no moving window
+ * (MRM_ERR_STATE / MRM_ERR_UNSUPPORTED otherwise).  tc NULL switches it off.  (No reference
  * counterpart for the C form; the Fortran host calls it where it calls
  * set_temp_scaling / init_temp_scaling.)
  * mrm_gpu_set_temp_scaling_table: table `which` (1 Ms, 2 alpha, 3 Hk, 4 Hx)

@@ -764,6 +764,22 @@ MRM_D void csr_sum(const int* __restrict__ idx, const int* __restrict__ nbr,
   }
 }
 
+// csr_sum with each neighbour's coefficient times scale(j, m_j) (temperature
+// scaling: the neighbour's ms_scale at this evaluation)
+template <typename R, class SCALE>
+MRM_D void csr_sum_scaled(const int* __restrict__ idx, const int* __restrict__ nbr, const R* __restrict__ cf,
+                          const V4<R>* __restrict__ mb, int n, const SCALE& scale, R& hx, R& hy, R& hz) {
+  const int q0 = __ldg(idx + n), q1 = __ldg(idx + n + 1);
+  for (int q = q0; q < q1; ++q) {
+    const int j = __ldg(nbr + q);
+    const V4<R> mj = mb[j];
+    const R c = (R)((double)__ldg(cf + q) * scale(j, mj));
+    hx += c * mj.x;
+    hy += c * mj.y;
+    hz += c * mj.z;
+  }
+}
+
 // stats record slots (sums except the two maxima)
 constexpr int kSlotV = 0, kSlotM = 1, kSlotM2 = 4, kSlotH = 7, kSlotWM = 10, kSlotW = 13,
               kSlotNup = 14, kSlotMaxTq = 15, kSlotMaxD2 = 16, kSlotMmag = 17, kSlotE = 18, kSlotVA = 19;
@@ -1441,11 +1457,33 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       ey = c.x * n0.y + c.y * n1.y + c.z * n2.y + c.w * n3.y;
       ez = c.x * n0.z + c.y * n1.z + c.z * n2.z + c.w * n3.z;
     } else if (L.xidx) {
-      csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
+      bool done = false;
+      if constexpr (GEN == 2) {
+        if (L.tsc) {
+          // hx(j) ms_scale(j) m(j) with the neighbours' scales (one grain per cell: j is a cell)
+          csr_sum_scaled<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, [&](int j, const V4<R>& mj) {
+            return tsc_ms(*L.tsc, j, layer_temp(L, t_stage, j % nx, j / nx), (double)mj.w);
+          }, ex, ey, ez);
+          done = true;
+        }
+      }
+      if (!done) csr_sum<R>(L.xidx, L.xnbr, L.xcoef, mfield, n, ex, ey, ez);
     }
     R vx = 0, vy = 0, vz = 0;
-    // (a columnar partner layer with temperature scaling: its grain's ms_scale
-    // at this evaluation, get_interlayer_hx field.f90:326-348)
+    // (an interlayer partner with temperature scaling: its grains' ms_scale at
+    // this evaluation, get_interlayer_hx field.f90:326-348)
+    auto csr_pair = [&](const LayerDev<R>* Lo, const int* idx, const int* nbr, const R* cf, const V4<R>* mo, R& ox,
+                        R& oy, R& oz) {
+      if constexpr (GEN == 2) {
+        if (Lo->tsc) {
+          csr_sum_scaled<R>(idx, nbr, cf, mo, n, [&](int j, const V4<R>& mj) {
+            return tsc_ms(*Lo->tsc, j, layer_temp(*Lo, t_stage, j % nx, j / nx), (double)mj.w);
+          }, ox, oy, oz);
+          return;
+        }
+      }
+      csr_sum<R>(idx, nbr, cf, mo, n, ox, oy, oz);
+    };
     auto col_scale = [&](const LayerDev<R>* Lo, R cf, R mag) -> R {
       if constexpr (GEN == 2)
         if (Lo->tsc) return (R)((double)cf * tsc_ms(*Lo->tsc, n, layer_temp(*Lo, t_stage, gi, gj), (double)mag));
@@ -1456,14 +1494,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
       const R cu = col_scale(Lu, UC[q], vu.w);
       vx += cu * vu.x; vy += cu * vu.y; vz += cu * vu.z;
     } else if (L.uidx && Lu) {
-      csr_sum<R>(L.uidx, L.unbr, L.ucoef, mother_u, n, vx, vy, vz);
+      csr_pair(Lu, L.uidx, L.unbr, L.ucoef, mother_u, vx, vy, vz);
     }
     if (lcol) {
       const V4<R> vl = VL[q];
       const R cl = col_scale(Ll, LC[q], vl.w);
       vx += cl * vl.x; vy += cl * vl.y; vz += cl * vl.z;
     } else if (L.lidx && Ll) {
-      csr_sum<R>(L.lidx, L.lnbr, L.lcoef, mother_l, n, vx, vy, vz);
+      csr_pair(Ll, L.lidx, L.lnbr, L.lcoef, mother_l, vx, vy, vz);
     }
     hx += ex + vx;
     hy += ey + vy;

@@ -2507,11 +2507,6 @@ int mrm_gpu_set_temp_scaling(mrm_gpu* h, int layer, const double* tc, double mse
   const HostLayerCache& hc = host_cache()[h][layer];
   if (!hc.cgrain.empty()) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs one grain per cell");
   if (h->wnx) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling with a moving demag window");
-  // the neighbours' ms_scale enters every exchange term: the lattice and columnar forms carry it per stage
-  if (b.xidx && !b.xst) return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs the lattice form of the exchange");
-  if ((b.uidx && !b.ucol) || (b.lidx && !b.lcol) || (layer > 0 && h->L[layer - 1].lidx && !h->L[layer - 1].lcol) ||
-      (layer + 1 < h->nl && h->L[layer + 1].uidx && !h->L[layer + 1].ucol))
-    return set_err(errp, MRM_ERR_UNSUPPORTED, "temperature scaling needs columnar interlayer couplings");
   for (int g = 0; g < b.ng; ++g) {
     if (hc.ms_scale[g] != 1.0 || hc.hk_scale[g] != 1.0 || hc.alpha_scale[g] != 1.0)
       return set_err(errp, MRM_ERR_STATE, "layer %d: temperature scaling replaces the scales; upload them as 1", layer);

@@ -3,7 +3,7 @@ oracle's find_temp_scaling (temp_scaling.f90:365-430): HAMR trajectories of
 an LLG layer (power laws and tables; Heun, the semi-implicit push and its
 midpoint form) and of an LLB layer (Ms from |m|) on the same Philox stream,
 the FP32 path, the batched form, the host library's table reduction and the
-combinations the path refuses."""
+combination the path refuses."""
 import numpy as np
 import pytest
 
@@ -114,13 +114,35 @@ def test_refusals(gpulib):
     med.layers[0].ms_scale[3] = 0.9  # the reference's scales start at 1 and only this scaling moves them
     with pytest.raises(MrmError, match="upload them as 1"):
         GpuSim(med, precision=FP64)
-    med = _hamr_llg(8, msexp=0.5)
-    lay = med.layers[0]
-    # a CSR exchange that the 4-neighbour lattice form cannot hold (grain 1
-    # also couples to its diagonal neighbour, 1-based grain nx + 2)
-    idx, gr, cf = lay.hx_index.copy(), lay.hx_grain.copy(), lay.hx.copy()
-    lay.hx_grain = np.insert(gr, idx[1], lay.nx + 2).astype(np.int32)
-    lay.hx = np.insert(cf, idx[1], 100.0)
-    lay.hx_index = np.concatenate([idx[:1], idx[1:] + 1]).astype(np.int32)
-    with pytest.raises(MrmError, match="lattice form"):
-        GpuSim(med, precision=FP64)
+
+
+def _csr_exchange(lay):
+    """A CSR exchange that the 4-neighbour lattice form cannot hold: every
+    grain also couples to its diagonal neighbour (i+1, j+1)."""
+    nx, ny = lay.nx, lay.ny
+    idx, gr, cf = lay.hx_index, lay.hx_grain, lay.hx
+    new_idx, new_gr, new_cf = [0], [], []
+    for g in range(lay.N):
+        i, j = g % nx, g // nx
+        new_gr.extend(gr[idx[g]:idx[g + 1]])
+        new_cf.extend(cf[idx[g]:idx[g + 1]])
+        new_gr.append(((j + 1) % ny) * nx + (i + 1) % nx + 1)
+        new_cf.append(120.0)
+        new_idx.append(len(new_gr))
+    lay.hx_index = np.array(new_idx, np.int32)
+    lay.hx_grain = np.array(new_gr, np.int32)
+    lay.hx = np.array(new_cf, float)
+
+
+def test_csr_exchange_fp64(oracle, gpulib):
+    """The neighbours' scales on the CSR form of the exchange."""
+    med = _hamr_llg(16, vel=FAST, msexp=0.35, tables={3: TABLES["kelvin"]})
+    _csr_exchange(med.layers[0])
+    orc, gpu = _pair(oracle, med, FP64)
+    for chunk in range(3):
+        orc.step(100, 1e-13)
+        gpu.step(100, 1e-13)
+        assert np.abs(gpu.get_state(0) - orc.get_state(0)).max() < 1e-8, chunk
+    assert (orc.get_scales(0)[0] == 0.0).any()
+    gpu.close()
+    orc.close()
