@@ -106,6 +106,7 @@ struct mrm_gpu {
   void* spech = nullptr;
   void* specx = nullptr;
   void* xfer = nullptr;  // 3 x N doubles: host <-> device transfers of one layer's state
+  void* slab = nullptr;  // one allocation holding xfer and every layer's per-grain arrays
   // tensor spectrum: runs whose tensor was copied from a run of the same
   // geometry share that run's buffer (tens_buf owns it; tens is its address),
   // so a batch of one geometry reads one tensor, which stays in L2
@@ -1343,21 +1344,29 @@ int run_alloc(mrm_gpu* r) {
   const size_t re = relem(r->g.precision);
   int rc = r->fft_big ? MRM_OK : spectra_alloc(r);
   if (rc) return rc;
-  rc = dmalloc(errp, &r->xfer, (size_t)r->g.nx * r->g.ny * 3 * sizeof(double));
-  if (rc) return rc;
   // (the tensor buffer comes with the first build or upload, or is shared)
+  // The transfer buffer and every layer's per-grain arrays live in one
+  // zero-filled allocation (256-byte aligned pieces): a run costs one
+  // allocation and one free of them instead of one per array.
   const size_t n = (size_t)r->g.nx * r->g.ny;
+  auto piece = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t v4 = piece(n * 4 * re), pv = piece(n * 4 * sizeof(double)), xf = piece(n * 3 * sizeof(double));
+  rc = dmalloc(errp, &r->slab, xf + (size_t)r->nl * (8 * v4 + pv));
+  if (rc) return rc;
+  unsigned char* at = static_cast<unsigned char*>(r->slab);
+  r->xfer = at;
+  at += xf;
   for (int l = 0; l < r->nl; ++l) {
     LayerBufs& b = r->L[l];
     b.n = (int)n;
     b.ng = (int)n;
     void** v4s[] = {&b.m, &b.mp, &b.dm, &b.hf, &b.hd, &b.ht, &b.pa, &b.pb};
     for (void** p : v4s) {
-      rc = dmalloc(errp, p, n * 4 * re);
-      if (rc) return rc;
+      *p = at;
+      at += v4;
     }
-    rc = dmalloc(errp, &b.pv, n * 4 * sizeof(double));
-    if (rc) return rc;
+    b.pv = at;
+    at += pv;
   }
   return MRM_OK;
 }
@@ -1365,11 +1374,12 @@ int run_alloc(mrm_gpu* r) {
 void run_free(mrm_gpu* r) {
   dfree(r->spech);
   dfree(r->specx);
-  dfree(r->xfer);
+  dfree(r->slab);  // xfer and the per-grain arrays
+  r->xfer = nullptr;
   tensor_release(r);
   for (int l = 0; l < MRM_MAX_LAYERS; ++l) {
     LayerBufs& b = r->L[l];
-    dfree(b.m); dfree(b.mp); dfree(b.dm); dfree(b.hf); dfree(b.hd); dfree(b.ht); dfree(b.pa); dfree(b.pb); dfree(b.pv);
+    b.m = b.mp = b.dm = b.hf = b.hd = b.ht = b.pa = b.pb = b.pv = nullptr;
     dfree(b.xidx); dfree(b.xnbr); dfree(b.xcoef);
     dfree(b.uidx); dfree(b.unbr); dfree(b.ucoef);
     dfree(b.lidx); dfree(b.lnbr); dfree(b.lcoef);
