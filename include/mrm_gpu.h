@@ -411,7 +411,17 @@ const char* mrm_batch_last_error(const mrm_batch* b);
 /* Creates a run inside the batch (same precision/device); configure it with
  * the mrm_gpu_* upload/set functions; it is freed by mrm_batch_remove. */
 int mrm_batch_add(mrm_batch* b, const mrm_geom* geom, mrm_gpu** run);
+/* Takes the run out of the batch after the batch's work in flight; the run
+ * handle is invalid on return.  Its device memory is released at the batch's
+ * next mrm_batch_stats, mrm_batch_step or mrm_batch_destroy. */
 int mrm_batch_remove(mrm_batch* b, mrm_gpu* run);
+/* Moves a run of batch src into batch dst (same precision and device; no
+ * reference counterpart): state, parameters, tensor and counters move with
+ * it, no device copy is made.  Waits for both batches' work in flight.  A
+ * server sets up arriving runs in a second batch, whose uploads and tensor
+ * builds then overlap the serving batch's steps, and moves them in between
+ * two calls. */
+int mrm_batch_adopt(mrm_batch* dst, mrm_batch* src, mrm_gpu* run);
 /* per-run time step and step budget: the run advances while step < step_end */
 int mrm_batch_set_run(mrm_gpu* run, double dt, int64_t step_end, int active);
 /* Aligned start (no reference counterpart): the run idles through the first

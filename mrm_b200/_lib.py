@@ -31,7 +31,8 @@ EXPORTS = [
     "mrm_gpu_get_field", "mrm_gpu_set_time", "mrm_gpu_get_time", "mrm_gpu_eval_field",
     "mrm_gpu_step", "mrm_gpu_enqueue_steps", "mrm_gpu_read_stats", "mrm_gpu_stream", "mrm_gpu_profile",
     "mrm_batch_enqueue", "mrm_batch_stream", "mrm_batch_create", "mrm_batch_destroy", "mrm_batch_last_error",
-    "mrm_batch_add", "mrm_batch_remove", "mrm_batch_set_run", "mrm_batch_delay_run", "mrm_batch_step", "mrm_batch_stats",
+    "mrm_batch_add", "mrm_batch_remove", "mrm_batch_adopt", "mrm_batch_set_run", "mrm_batch_delay_run",
+    "mrm_batch_step", "mrm_batch_stats",
     "mrm_run_footprint", "mrm_device_memory", "mrm_gpu_copy_tensor", "mrm_batch_occupancy",
     "mrm_gpu_set_field_function", "mrm_gpu_demag_noalloc", "mrm_batch_profile", "mrm_gpu_set_head_field",
     "mrm_gpu_set_shape", "mrm_gpu_set_autotune", "mrm_gpu_get_shape", "mrm_gpu_check_device",
@@ -119,6 +120,7 @@ def load(path: str = LIB_PATH):
         "mrm_batch_last_error": ([vp], C.c_char_p),
         "mrm_batch_add": ([vp, P(Geom), P(vp)], i),
         "mrm_batch_remove": ([vp, vp], i),
+        "mrm_batch_adopt": ([vp, vp, vp], i),
         "mrm_batch_set_run": ([vp, d, i64, i], i),
         "mrm_batch_delay_run": ([vp, i64], i),
         "mrm_batch_step": ([vp, i, i], i),

@@ -77,9 +77,20 @@ class Batch:
         return run
 
     def remove(self, run: BatchRun):
+        """Takes the run out; its device memory is released at the next
+        stats, step or close."""
         self._check(_lib.load().mrm_batch_remove(self.b, run.h))
         self.runs.remove(run)
         run.h = None
+
+    def adopt(self, run: BatchRun):
+        """Moves a run of another batch (same precision and device) into this
+        one, without a device copy."""
+        src = run.batch
+        self._check(_lib.load().mrm_batch_adopt(self.b, src.b, run.h))
+        src.runs.remove(run)
+        run.batch = self
+        self.runs.append(run)
 
     def step(self, nsteps: int, llg_type: int = -3):
         self._check(_lib.load().mrm_batch_step(self.b, int(nsteps), int(llg_type)))

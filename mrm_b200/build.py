@@ -21,7 +21,7 @@ SOURCES = (["csrc/mrm_gpu.cu", "csrc/k_col.cu"] + [f"csrc/k_row_f32_v{v}.cu" for
            [f"csrc/k_row_f64_v{v}.cu" for v in range(3)] + [f"csrc/k_col_f32_v{v}.cu" for v in range(3)] +
            [f"csrc/k_col_f64_v{v}.cu" for v in range(2)] + [f"csrc/k_creg_v{v}.cu" for v in range(3)])
 HEADERS = ["csrc/common.cuh", "csrc/fft.cuh", "csrc/kernels.cuh", "csrc/philox.cuh", "csrc/tensor.cuh",
-           "csrc/tma.cuh", "csrc/launch.h", "csrc/k_row.inc", "csrc/k_col.inc", "csrc/colreg.cuh", "csrc/k_creg.inc", "../include/mrm_gpu.h"]
+           "csrc/tma.cuh", "csrc/launch.h", "csrc/k_row.inc", "csrc/k_col.inc", "csrc/colreg.cuh", "csrc/regfft.cuh", "csrc/k_creg.inc", "../include/mrm_gpu.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 

@@ -147,6 +147,9 @@ struct Engine {
   int dev = 0;
   cudaStream_t st = nullptr;
   std::vector<mrm_gpu*> runs;
+  // removed runs whose device memory is released at the next stats, step or
+  // destroy (after the stream has passed their last use)
+  std::vector<mrm_gpu*> retired;
   void* d_runs = nullptr;  // RunDev<R>[cap]
   int runs_cap = 0;
   Task* d_rtasks = nullptr;
@@ -1478,6 +1481,18 @@ struct HostLayerCache {
 std::map<const mrm_gpu*, std::vector<HostLayerCache>>& host_cache() {
   static std::map<const mrm_gpu*, std::vector<HostLayerCache>> m;
   return m;
+}
+
+// Frees the runs mrm_batch_remove took out of the engine: the stream has
+// passed their last use (remove waited for the work then in flight, and later
+// work runs on tables without them)
+void release_retired(Engine* e) {
+  for (auto* r : e->retired) {
+    host_cache().erase(r);
+    run_free(r);
+    delete r;
+  }
+  e->retired.clear();
 }
 
 template <typename R>
@@ -3257,6 +3272,7 @@ int mrm_batch_destroy(mrm_batch* b) {
   if (!b) return MRM_OK;
   cudaSetDevice(b->eng.dev);
   cudaStreamSynchronize(b->eng.st);
+  release_retired(&b->eng);
   for (auto* r : b->eng.runs) {
     host_cache().erase(r);
     run_free(r);
@@ -3286,11 +3302,36 @@ int mrm_batch_remove(mrm_batch* b, mrm_gpu* run) {
   cudaStreamSynchronize(b->eng.st);
   auto& v = b->eng.runs;
   v.erase(std::remove(v.begin(), v.end(), run), v.end());
-  host_cache().erase(run);
-  run_free(run);
-  delete run;
+  // the frees wait for the next stats / step / destroy: a server removes
+  // finished runs between two calls, and their frees then overlap the next
+  // call instead of holding the device idle
+  run->slot = -1;
+  b->eng.retired.push_back(run);
   b->eng.tables_dirty = true;
   b->eng.desc_dirty = true;
+  return MRM_OK;
+}
+
+int mrm_batch_adopt(mrm_batch* dst, mrm_batch* src, mrm_gpu* run) {
+  if (!dst || !src || !run || run->eng != &src->eng) return MRM_ERR_ARG;
+  if (dst == src) return MRM_OK;
+  Engine* d = &dst->eng;
+  Engine* s = &src->eng;
+  std::string* errp = &d->err;
+  if (d->prec != s->prec || d->dev != s->dev)
+    return set_err(errp, MRM_ERR_ARG, "adopt: the batches differ in precision or device");
+  CK(cudaSetDevice(d->dev));
+  CK(cudaStreamSynchronize(s->st));  // the run's uploads and tensor build
+  CK(cudaStreamSynchronize(d->st));  // the tables below change at the next call
+  auto& v = s->runs;
+  v.erase(std::remove(v.begin(), v.end(), run), v.end());
+  s->tables_dirty = true;
+  s->desc_dirty = true;
+  run->eng = d;
+  run->slot = -1;
+  d->runs.push_back(run);
+  d->tables_dirty = true;
+  d->desc_dirty = true;
   return MRM_OK;
 }
 
@@ -3344,6 +3385,7 @@ int mrm_batch_step(mrm_batch* b, int nsteps, int llg_type) {
   if (rc) return rc;
   std::string* errp = &b->eng.err;
   CK(cudaStreamSynchronize(b->eng.st));
+  release_retired(&b->eng);
   return MRM_OK;
 }
 
@@ -3366,8 +3408,11 @@ int mrm_batch_stats(mrm_batch* b, int nruns, mrm_gpu* const* runs, mrm_gpu_stats
   // the slots of the tables the last steps ran with (runs added since then
   // have none yet)
   const int nr = e->nslots;
-  if (!nr) return MRM_OK;
   CK(cudaSetDevice(e->dev));
+  // removed runs: no work in flight reads them (they left the tables before
+  // it was enqueued), and their frees overlap it
+  release_retired(e);
+  if (!nr) return MRM_OK;
   CK(cudaMemcpyAsync(e->h_stats, e->d_stats, sizeof(StatsDev) * nr, cudaMemcpyDeviceToHost, e->st));
   CK(cudaStreamSynchronize(e->st));
   if (check_device_error(e)) return MRM_ERR_DEVICE;

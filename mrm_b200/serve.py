@@ -7,7 +7,10 @@ start).  The server keeps one Batch resident on the GPU and loops:
 2. admit queued requests first-come-first-served while their device
    footprint (state, parameters, spectra, tensor) fits the HBM budget; a
    request's tensor spectrum is copied device-to-device from a per-geometry
-   template instead of being rebuilt;
+   template instead of being rebuilt.  The GPU backend sets admitted runs up
+   in a second (staging) batch, whose uploads wait only for its own stream,
+   and moves them into the serving batch (mrm_batch_adopt, no copy) right
+   before its next call;
 3. advance every active run by K = chunk Heun steps in one launch sequence,
    enqueued before step 2's admissions so that their host work overlaps it.
    A request of S steps is admitted with an aligned start: it idles through
@@ -16,7 +19,8 @@ start).  The server keeps one Batch resident on the GPU and loops:
    every call describe its own last step, while every call keeps the full
    chunk length (a run's trajectory is the same as without the delay);
 4. record each run's M(H) sample (time, applied field, m.h), retire finished
-   runs (result + latency = finish - arrival) and free their memory.
+   runs (result + latency = finish - arrival) and free their memory (the
+   frees themselves run while the next call is on the GPU).
 
 A request's medium (its grains, parameters and exchange lists, built on the
 host) is prepared by a worker thread as soon as the request arrives, while
@@ -261,6 +265,11 @@ class GpuBackend:
         self.device = device
         self.batch = Batch(precision, device)
         self.lib_batch = Batch(precision, device)  # per-geometry tensor templates (never stepped)
+        # arriving runs are set up here (uploads, tensor copies or builds on
+        # this batch's stream, overlapping the serving batch's call in
+        # flight) and move into the serving batch before its next call
+        self.stage = Batch(precision, device)
+        self._staged = []
 
     def memory(self):
         return self._mem(self.device)
@@ -269,9 +278,15 @@ class GpuBackend:
         return self._fp(medium, self.precision)
 
     def add(self, medium, dt, steps, seed, template):
-        run = self.batch.add(medium, dt=dt, steps=steps, thermal_seed=seed, tensor_from=template)
+        run = self.stage.add(medium, dt=dt, steps=steps, thermal_seed=seed, tensor_from=template)
         run._hdir = np.array(medium.layers[0].hdir, float)
+        self._staged.append(run)
         return run
+
+    def _adopt(self):
+        for run in self._staged:
+            self.batch.adopt(run)
+        self._staged = []
 
     def delay(self, run, idle_steps):
         run.delay(idle_steps)
@@ -285,12 +300,19 @@ class GpuBackend:
         return run._hdir
 
     def remove(self, run):
-        self.batch.remove(run)
+        if run in self._staged:
+            self._staged.remove(run)
+            self.stage.remove(run)
+            self.stage.stats([])  # the staging batch never steps: release now
+        else:
+            self.batch.remove(run)
 
     def step(self, k: int):
+        self._adopt()
         self.batch.step(k)
 
     def enqueue(self, k: int):
+        self._adopt()
         self.batch.enqueue(k)
 
     def stats(self, runs):
@@ -301,4 +323,5 @@ class GpuBackend:
 
     def close(self):
         self.batch.close()
+        self.stage.close()
         self.lib_batch.close()

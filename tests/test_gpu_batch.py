@@ -83,6 +83,42 @@ def test_batch_aligned_start(gpulib):
     b.close()
 
 
+def test_adopted_run_matches_alone(gpulib):
+    """A run set up (uploads, tensor) in a second batch and moved into a
+    stepping batch between two of its calls, next to a run removed at the same
+    boundary, advances exactly like the run alone; the removed run's device
+    memory comes back at the batch's next stats."""
+    from mrm_b200.batch import device_memory
+    meds = _media()
+    b, stage = Batch(FP64), Batch(FP64)
+    r0 = b.add(meds[0], dt=1e-13, steps=60, thermal_seed=9)
+    r1 = b.add(meds[1], dt=1e-13, steps=120, thermal_seed=9)
+    b.step(60)
+    r2 = stage.add(meds[2], dt=1e-13, steps=60, thermal_seed=9)
+    assert stage.runs == [r2]
+    b.remove(r0)
+    b.adopt(r2)
+    assert stage.runs == [] and b.runs == [r1, r2] and r2.batch is b
+    b.step(60)
+    st = b.stats([r1, r2])
+    for r, m, k, s in ((r1, meds[1], 120, st[0]), (r2, meds[2], 60, st[1])):
+        g = GpuSim(m, precision=FP64, thermal_seed=9)
+        sg = g.step(k, 1e-13)
+        assert np.array_equal(r.get_state(0), g.get_state(0))
+        assert s["step"] == k and np.array_equal(s["mave"], sg["mave"])
+        g.close()
+    # a large run removed between calls: its memory is back after the next stats
+    big = b.add(media.mh_medium(512, seed=5), dt=1e-13, steps=16)
+    b.step(16)
+    free0, _ = device_memory(0)
+    b.remove(big)
+    b.stats([r1])
+    free1, _ = device_memory(0)
+    assert free1 - free0 > 48 * 1024 * 1024, (free0, free1)
+    stage.close()
+    b.close()
+
+
 def test_tensor_copy_matches_build(gpulib):
     m = media.mh_medium(32, seed=4)
     b = Batch(FP32)
