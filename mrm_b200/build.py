@@ -17,9 +17,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmrm_gpu.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = (["csrc/mrm_gpu.cu", "csrc/k_col.cu"] + [f"csrc/k_row_f32_v{v}.cu" for v in range(5)] +
-           [f"csrc/k_row_f64_v{v}.cu" for v in range(3)] + [f"csrc/k_col_f32_v{v}.cu" for v in range(3)] +
-           [f"csrc/k_col_f64_v{v}.cu" for v in range(2)] + [f"csrc/k_creg_v{v}.cu" for v in range(3)])
+# longest compiles first (the pool takes them in this order)
+SOURCES = ([f"csrc/k_row_f32_v{v}_g{g}.cu" for g in (2, 1, 0) for v in range(5)] +
+           [f"csrc/k_creg_v{v}.cu" for v in range(3)] + [f"csrc/k_row_f64_v{v}.cu" for v in range(3)] +
+           [f"csrc/k_col_f32_v{v}.cu" for v in range(3)] + [f"csrc/k_col_f64_v{v}.cu" for v in range(2)] +
+           ["csrc/mrm_gpu.cu", "csrc/k_col.cu", "csrc/k_row_split.cu"])
 HEADERS = ["csrc/common.cuh", "csrc/fft.cuh", "csrc/kernels.cuh", "csrc/philox.cuh", "csrc/tensor.cuh",
            "csrc/tma.cuh", "csrc/launch.h", "csrc/k_row.inc", "csrc/k_col.inc", "csrc/colreg.cuh", "csrc/regfft.cuh", "csrc/k_creg.inc", "../include/mrm_gpu.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

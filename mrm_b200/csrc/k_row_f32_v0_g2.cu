@@ -1,0 +1,6 @@
+// k_row_f32_v0_g2.cu -- FP32 row kernels of compiled shape 0 (launch.h),
+// level 2 (row_kernel's GEN).
+#define ROW_REAL float
+#define ROW_V 0
+#define ROW_GEN 2
+#include "k_row.inc"

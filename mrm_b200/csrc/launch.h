@@ -59,6 +59,15 @@ struct RowOps {
 };
 template <typename R, int V>
 const RowOps& row_ops();
+// the kernels of one level of a shape whose levels compile in translation
+// units of their own (the FP32 shapes: k_row_f32_v*_g*.cu, assembled into
+// row_ops by k_row_split.cu)
+struct RowGenOps {
+  cudaError_t (*launch)(int stage, bool stats, const RowLaunch& a, int istep, int flags);
+  const void* fn[6];
+};
+template <typename R, int V, int GEN>
+const RowGenOps& row_gen_ops();
 
 struct RowLaunch {
   cudaStream_t st;
