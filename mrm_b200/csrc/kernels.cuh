@@ -971,7 +971,8 @@ MRM_D void rrow_forward_any(int lgM, Cx<float>* in, Cx<float>* xb, int cs, int n
   }
 }
 
-// Row kernel: one task = up to RPB grid rows of one layer of one run.
+// Row kernel: one task = up to RPB grid rows of one layer of one run (more for
+// a run of short FP32 rows, packed by the host).
 //   kInit: forward row FFT of Ms*m (spectrum of the current state)
 //   kPred / kCorr: inverse row FFT of H^ -> H_demag, field assembly, Heun
 //                  stage, forward row FFT of Ms*m* / Ms*m_{n+1}
@@ -995,7 +996,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const Task tk = tasks[blockIdx.x];
   const RunDev<R>& rd = runs[tk.x];
   if (!rd.active) return;  // host-set, constant within a captured graph
-  if (rd.lgpx > LGMAX || tk.w > RPB) {  // shape not compiled into this variant (the host never picks it)
+  if (rd.lgpx > LGMAX) {  // shape not compiled into this variant (the host never picks it)
     if (threadIdx.x == 0) atomicOr(err, kErrShape);
     return;
   }
@@ -1013,6 +1014,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   const int gnx = win ? rd.gnx : nx, gny = win ? rd.gny : ny, wi0 = win ? rd.wi0 : 0, wj0 = win ? rd.wj0 : 0;
   const int lgpx = rd.lgpx, lgM = lgpx - 1, M = 1 << lgM, ph = M + 1;
   const int cs = seq_stride(M);  // complex stride of one sequence in shared memory
+  // FP32 rows of 16..1024 complex points: the register transforms, whose
+  // loops take any number of rows; a run of rows shorter than the launch's
+  // longest may then have more than RPB rows per task (the host packs them
+  // into the FFT buffers sized for the longest rows)
+  constexpr bool kRegRowType = sizeof(R) == sizeof(float);
+  const bool regrow = kRegRowType && rrow_len_ok(lgM);
+  const int rcap = (regrow && !win) ? max(RPB, nrows) : RPB;
   const int nseq = nrows * 3;
   const int ngr = nrows * nx;
   const LayerDev<R>& L = rd.L[l];
@@ -1023,17 +1031,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 
   Cx<R>* tws = reinterpret_cast<Cx<R>*>(smem_raw);  // post twiddles | pass tables
   const int ntw = row_tw_count(lgpx);
+  if (nrows > rcap || (long long)(ntw + 2 * rcap * 3 * cs) * (long long)sizeof(Cx<R>) >
+                          (long long)dynamic_smem_bytes()) {  // host bug: a task the buffers do not hold
+    if (threadIdx.x == 0) atomicOr(err, kErrShape);
+    return;
+  }
   Cx<R>* bufA = tws + ntw;
-  Cx<R>* bufB = bufA + RPB * 3 * cs;
+  Cx<R>* bufB = bufA + rcap * 3 * cs;
   // a layer under the moving write head gets its head field per grid column in
   // a table after the FFT buffers (the host reserves it), then the staging area
   // (its byte offset; 0: no head)
   // (a tabulated field profile gets its interpolation weights there instead)
   const bool ftab = GEN && STAGE != kInit && rd.L[tk.y].tab != nullptr;
   const int htab_off = GEN && (rd.L[tk.y].func == kFuncHead || ftab)
-                           ? (int)(reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) - smem_raw)
+                           ? (int)(reinterpret_cast<unsigned char*>(bufB + rcap * 3 * cs) - smem_raw)
                            : 0;
-  unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + RPB * 3 * cs) +
+  unsigned char* stg = reinterpret_cast<unsigned char*>(bufB + rcap * 3 * cs) +
                        (ftab ? field_table_bytes(rd.nx) : htab_off ? head_table_bytes<R>(rd.nx) : 0);
   if (htab_off && (long long)(stg - smem_raw) > (long long)dynamic_smem_bytes()) {  // host bug: no room reserved
     if (threadIdx.x == 0) atomicOr(err, kErrShape);
@@ -1173,9 +1186,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
 
   // ---------------- inverse row transform: H^ rows -> H_demag ----------------
   Cx<R>* Z = bufA;  // after the inverse: z[n] = x[2n] + i x[2n+1] per sequence
-  // FP32 rows of 16..1024 complex points: the register transforms
-  constexpr bool kRegRowType = sizeof(R) == sizeof(float);
-  const bool regrow = kRegRowType && rrow_len_ok(lgM);
   if (inverse && regrow) {
     if (leave_on_timeout(mbar_wait(&bars[0], 0) & mbar_wait(&bars[1], 0))) return;
     if constexpr (kRegRowType)

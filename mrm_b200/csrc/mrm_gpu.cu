@@ -409,6 +409,43 @@ int run_stage_bytes(const mrm_gpu* r, int stage, int rows) {
   return need;
 }
 
+// Packing of short rows: an FP32 run (register row transforms, no window,
+// head, field table or grain map) whose rows are shorter than the batch's
+// longest takes 2^k times the shape's rows per task, as many as the FFT
+// buffers sized for the longest rows hold, with at most as many grains per
+// task as the longest rows' tasks: its blocks then carry about as many points
+// as those of the longest rows instead of idling most of their threads.
+struct RowPackCap {
+  int fft = 0;     // FFT-buffer bytes of the launch (twiddles + two buffers)
+  int grains = 0;  // grains of the largest unpacked task
+};
+
+template <typename R>
+RowPackCap row_pack_cap(const Engine* e, int rpb) {
+  RowPackCap c;
+  for (auto* r : e->runs) {
+    c.fft = std::max(c.fft, row_fft_smem<R>(r->lgpx, rpb));
+    c.grains = std::max(c.grains, rows_per_task(r, rpb) * fnx(r));
+  }
+  return c;
+}
+
+bool row_packable(const mrm_gpu* r) {
+  if (r->g.precision != MRM_FP32 || r->wnx || !rrow_len_ok(r->lgpx - 1)) return false;
+  for (int l = 0; l < r->nl; ++l)
+    if (r->L[l].tab || r->L[l].func == kFuncHead || r->L[l].cgrain) return false;
+  return true;
+}
+
+template <typename R>
+int rows_per_task(const mrm_gpu* r, int rpb, const RowPackCap& c) {
+  int rows = rows_per_task(r, rpb);
+  if (!row_packable(r)) return rows;
+  while (2 * rows <= fny(r) && row_fft_smem<R>(r->lgpx, 2 * rows) <= c.fft && 2 * rows * fnx(r) <= c.grains)
+    rows *= 2;
+  return rows;
+}
+
 // row-kernel shared memory before the staging area: twiddles, FFT buffers and,
 // for a run with a layer under the write head, the head-field table (with a
 // tabulated field profile, its interpolation weights)
@@ -630,10 +667,11 @@ int plan_smem(Engine* e) {
   int need[kSlots] = {0, 0, 0, 0, 0, 0};
   size_t scol = 16;
   int tw_cap = 0, stage_bytes = 0;
+  const RowPackCap pack = row_pack_cap<R>(e, rv.rpb);
   for (auto* r : e->runs) {
     if (r->lgpx > rv.lgmax)
       return set_err(errp, MRM_ERR_UNSUPPORTED, "row shape %d does not cover %d-column FFT grids", e->rowv, r->px);
-    const int rows = rows_per_task(r, rv.rpb);
+    const int rows = rows_per_task<R>(r, rv.rpb, pack);
     fft = std::max(fft, row_fixed_smem<R>(r, rv.rpb));
     for (int q = 0; q < kSlots; ++q) need[q] = std::max(need[q], run_stage_bytes<R>(r, kSlotStage[q], rows));
     if (r->demag && r->tensor_ready) {
@@ -698,11 +736,12 @@ template <typename R>
 int build_tables(Engine* e) {
   std::string* errp = &e->err;
   const RowVariant rv = row_variant<R>(e->rowv);
+  const RowPackCap pack = row_pack_cap<R>(e, rv.rpb);
   std::vector<Task> rt, ct, ct2, stt;
   for (size_t i = 0; i < e->runs.size(); ++i) {
     mrm_gpu* r = e->runs[i];
     r->slot = (int)i;
-    const int rpt = rows_per_task(r, rv.rpb);
+    const int rpt = rows_per_task<R>(r, rv.rpb, pack);
     const int ny = fny(r);
     for (int l = 0; l < r->nl; ++l)
       for (int j = 0; j < ny; j += rpt) rt.push_back(make_int4((int)i, l, j, std::min(rpt, ny - j)));

@@ -119,6 +119,31 @@ def test_adopted_run_matches_alone(gpulib):
     b.close()
 
 
+def test_packed_short_rows_match_alone(gpulib):
+    """FP32 runs whose rows are shorter than the batch's longest get several
+    rows per row task (2 to 8 here, next to a 128-grain-wide run); every run,
+    a two-layer one and one with the STE time function among them, still
+    steps bit for bit as it does alone (where it has the longest rows)."""
+    from tests.helpers import two_layer
+    big = media.mh_medium(128, seed=31, temperature=300.0)
+    meds = [big, media.mh_medium(16, seed=32, temperature=300.0), media.mh_medium(32, seed=33, temperature=300.0),
+            two_layer(32, 16, seed=34, temperature=300.0), media.mh_medium(64, seed=35, temperature=300.0)]
+    lay = meds[4].layers[0]
+    lay.func, lay.amp, lay.fgamma, lay.param, lay.scale = 4, 12000.0, 2e-11, 1e-12, 1.0
+    b = Batch(FP32)
+    runs = [b.add(m, dt=1e-13, steps=64, thermal_seed=40 + i) for i, m in enumerate(meds)]
+    b.step(64)
+    st = b.stats(runs)
+    for i, (r, m) in enumerate(zip(runs, meds)):
+        g = GpuSim(m, precision=FP32, thermal_seed=40 + i)
+        sg = g.step(64, 1e-13)
+        for l in range(m.n_lay):
+            assert np.array_equal(r.get_state(l), g.get_state(l)), (i, l)
+        assert np.array_equal(st[i]["mave"], sg["mave"]), i
+        g.close()
+    b.close()
+
+
 def test_tensor_copy_matches_build(gpulib):
     m = media.mh_medium(32, seed=4)
     b = Batch(FP32)
