@@ -62,7 +62,7 @@ WORKLOAD = ("batched {b} x 65,536-grain M(H) ramp realisations, T=300 K, FP32, "
 # headline batch (32 x 65,536 grains, row shape 1, the register column kernel
 # {128 threads, 4 blocks/SM}, one column per task), divided by its grains; a
 # kernel change calls for a new capture
-NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 140.1, "col": 35.3, "row_corr": 164.4}
+NCU_TRAFFIC_BYTES_PER_GRAIN = {"row_pred": 141.0, "col": 35.7, "row_corr": 164.4}
 
 
 def algorithmic_bytes(nx: int, ny: int, px: int, py: int, nl: int = 1, fp: int = 4, runs: int = 1,
