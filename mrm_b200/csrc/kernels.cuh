@@ -1017,10 +1017,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) row_kernel(const RunDev<R>* __res
   // FP32 rows of 16..1024 complex points: the register transforms, whose
   // loops take any number of rows; a run of rows shorter than the launch's
   // longest may then have more than RPB rows per task (the host packs them
-  // into the FFT buffers sized for the longest rows)
+  // into the FFT buffers sized for the longest rows; not in level-2 batches)
   constexpr bool kRegRowType = sizeof(R) == sizeof(float);
   const bool regrow = kRegRowType && rrow_len_ok(lgM);
-  const int rcap = (regrow && !win) ? max(RPB, nrows) : RPB;
+  const int rcap = (GEN < 2 && regrow && !win) ? max(RPB, nrows) : RPB;
   const int nseq = nrows * 3;
   const int ngr = nrows * nx;
   const LayerDev<R>& L = rd.L[l];

@@ -424,6 +424,10 @@ template <typename R>
 RowPackCap row_pack_cap(const Engine* e, int rpb) {
   RowPackCap c;
   for (auto* r : e->runs) {
+    // a batch on the level-2 kernels (LLB / MT / Zhang, temperature profiles
+    // or scaling) packs nothing: those kernels keep RPB rows per task
+    for (int l = 0; l < r->nl; ++l)
+      if (r->L[l].llb || r->L[l].tprof || r->L[l].tsc) return RowPackCap{};
     c.fft = std::max(c.fft, row_fft_smem<R>(r->lgpx, rpb));
     c.grains = std::max(c.grains, rows_per_task(r, rpb) * fnx(r));
   }
