@@ -119,6 +119,22 @@ def test_adopted_run_matches_alone(gpulib):
     b.close()
 
 
+def test_adopt_refuses_other_precision(gpulib):
+    """A run moves only between batches of one precision and device; a refused
+    move leaves it where it was, still stepping."""
+    from mrm_b200 import MrmError
+    m = media.mh_medium(16, seed=36)
+    b32, b64 = Batch(FP32), Batch(FP64)
+    r = b64.add(m, dt=1e-13, steps=8)
+    with pytest.raises(MrmError):
+        b32.adopt(r)
+    assert b64.runs == [r] and b32.runs == [] and r.batch is b64
+    b64.step(8)
+    assert r.get_time()[1] == 8
+    b32.close()
+    b64.close()
+
+
 def test_packed_short_rows_match_alone(gpulib):
     """FP32 runs whose rows are shorter than the batch's longest get several
     rows per row task (2 to 8 here, next to a 128-grain-wide run); every run,
